@@ -1,0 +1,59 @@
+"""The oracle's two independent forms agree (sum factorisation vs direct quadrature)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+LAWS = {
+    "constant": O.material(),
+    "linear_k": O.material(O.LAW_LINEAR_K, k=1.0, k1=0.5),
+    "liquid_solid": O.material(O.LAW_LIQUID_SOLID, rho=1000.0, cp=4226.0, k=0.556, rho_s=900.0,
+                               cp_s=1762.0, k_s=2.22, T_solidus=0.2, T_liquidus=0.8),
+}
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+@pytest.mark.parametrize("law", list(LAWS))
+def test_sum_factorisation_matches_direct_quadrature(degree, perturb, law):
+    rng = np.random.default_rng(degree)
+    o = O.Oracle(degree, (3, 2, 3), perturb=perturb, seed=11)
+    o.set_material(LAWS[law], 1e-3)
+    src = rng.uniform(-1, 1, o.n_dofs)
+    T_lin = rng.uniform(0, 1, o.n_dofs)
+    T_old = rng.uniform(0, 1, o.n_dofs)
+    a = o.vmult(src, T_lin, T_old, form=0)
+    b = o.vmult(src, T_lin, T_old, form=1)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+    da = o.inverse_diagonal(T_lin, T_old, form=0)
+    db = o.inverse_diagonal(T_lin, T_old, form=1)
+    assert np.allclose(1 / da, 1 / db, rtol=1e-12, atol=0)
+    # constrained rows of vmult are zero, inverse diagonal there is one
+    m = o.mask().astype(bool)
+    assert np.all(a[m] == 0.0) and np.all(da[m] == 1.0)
+
+
+def test_operator_symmetric_for_constant_law():
+    rng = np.random.default_rng(3)
+    o = O.Oracle(3, (3, 3, 3), perturb=0.2, seed=2)
+    o.set_material(LAWS["constant"], 1e-3)
+    u = rng.uniform(-1, 1, o.n_dofs)
+    v = rng.uniform(-1, 1, o.n_dofs)
+    assert abs(u @ o.vmult(v) - v @ o.vmult(u)) <= 1e-12 * abs(u @ o.vmult(u))
+
+
+def test_tangent_is_derivative_of_residual():
+    """J(T) du = d/deps [-R(T + eps du)] * (-1): the tangent of the k(T) law is consistent."""
+    rng = np.random.default_rng(5)
+    o = O.Oracle(2, (3, 3, 3), perturb=0.1, seed=4)
+    o.set_material(LAWS["linear_k"], 1e-2)
+    T = rng.uniform(0, 1, o.n_dofs)
+    T_old = rng.uniform(0, 1, o.n_dofs)
+    du = rng.uniform(-1, 1, o.n_dofs)
+    du[o.mask().astype(bool)] = 0.0
+    eps = 1e-6
+    rp = o.create_rhs(T + eps * du, T_old)
+    rm = o.create_rhs(T - eps * du, T_old)
+    fd = -(rp - rm) / (2 * eps)
+    Jdu = o.vmult(du, T, T_old)
+    assert np.abs(fd - Jdu).max() <= 1e-7 * np.abs(Jdu).max()

@@ -1,0 +1,59 @@
+"""The oracle against MeltPoolDG's own regression outputs (known-answer pins).
+
+Both cases are lower-dimensional in the reference; here they run on 3D meshes
+that are one cell thick (extent 1) in the extra directions, where the exact
+discrete solution is constant across those directions, so the FE L2 norms are
+the reference's norms.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+# applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/
+#   unidirectional_heat_transfer.mpirun=4.output
+UNIDIRECTIONAL = [5.64198e-03, 5.53556e-03, 5.44694e-03, 5.37273e-03, 5.31056e-03]
+# applications/mp-heat-transfer/cases/solidification_slab/tests/solidification_slab.mpirun=1.output
+SLAB = [2.82611e+02, 2.82458e+02, 2.82345e+02, 2.82252e+02, 2.82169e+02]
+
+
+def _six_digits(a, b):
+    return float(f"{a:.5e}") == float(f"{b:.5e}")
+
+
+@pytest.mark.parametrize("solver", ["gmres", "cg"])
+def test_unidirectional_heat_transfer(solver):
+    # unidirectional_heat_transfer.json: 2D [0,0.1]^2, 5 global refinements (32x32), Q1,
+    # gas k = rho = cp = 1, all boundaries adiabatic, T0 = x (LinearTemp(0, 0.1)),
+    # dt = 1e-4, 5 steps, rel tol 1e-12, Newton residual tolerance 5e-9.
+    o = O.Oracle(1, (32, 32, 1), lo=(0, 0, 0), hi=(0.1, 0.1, 1.0), dirichlet_mask=0)
+    o.set_material(O.material(), 1e-4)
+    x = o.support_points()
+    T = x[:, 0].copy()
+    T_old = np.zeros_like(T)
+    dt_old = 0.0
+    for ref in UNIDIRECTIONAL:
+        rc, st = o.time_step_newton(T, T_old, 1e-4, dt_old, res_tol=5e-9, solver=solver)
+        dt_old = 1e-4
+        assert rc == 0 and st.converged
+        assert _six_digits(o.l2_norm(T), ref), (o.l2_norm(T), ref)
+
+
+def test_solidification_slab():
+    # solidification_slab.json: 1D [0,1], 7 refinements (128 cells), Q1, Dirichlet T = 253 at
+    # x = 0, T0 = 283, liquid-solid mushy zone (270..276 K), dt = 200, 5 steps, Newton residual
+    # tolerance 1e-8, GMRES (the heat default, heat_data.cpp:11).
+    o = O.Oracle(1, (128, 1, 1), lo=(0, 0, 0), hi=(1, 1, 1), dirichlet_mask=1,
+                 dirichlet_value=(253.0, 0, 0, 0, 0, 0))
+    m = O.material(O.LAW_LIQUID_SOLID, rho=1000.0, cp=4226.0, k=0.556, rho_s=1000.0, cp_s=1762.0,
+                   k_s=2.22, T_solidus=270.0, T_liquidus=276.0)
+    o.set_material(m, 200.0)
+    T = np.full(o.n_dofs, 283.0)
+    o.distribute(T)
+    T_old = np.zeros_like(T)
+    dt_old = 0.0
+    for ref in SLAB:
+        rc, st = o.time_step_newton(T, T_old, 200.0, dt_old, res_tol=1e-8, solver="gmres")
+        dt_old = 200.0
+        assert rc == 0 and st.converged
+        assert _six_digits(o.l2_norm(T), ref), (o.l2_norm(T), ref)

@@ -1,0 +1,222 @@
+/*
+ * mpdg_heat.h - C ABI of the B200-native matrix-free heat operator and solve.
+ *
+ * This is the drop-in boundary for MeltPoolDG's implicit heat-transfer hot
+ * path. Every entry point is `extern "C"`, takes plain pointers and sizes,
+ * returns an int status (MPDG_OK = 0) and never throws. Vectors passed as
+ * `double *` / `float *` are DEVICE pointers of length n_dofs (locally owned
+ * DoFs, no ghosts: one GPU owns the whole mesh) unless the name ends in
+ * `_host`. Work is enqueued on the handle's stream (mpdg_heat_set_stream);
+ * entry points that return host scalars synchronise that stream.
+ *
+ * Reference interfaces replaced (paths inside the MeltPoolDG tree):
+ *   OperatorBase<number>            include/meltpooldg/core/operator_base.hpp:21-84
+ *   OperatorMatrixFree<dim,number>  include/meltpooldg/core/operator_base.hpp:188-282
+ *   HeatDiffuseMultiPhaseOperator   source/heat/heat_diffuse_operator.cpp
+ *   JacobiPreconditioner            include/meltpooldg/linear_algebra/preconditioner_jacobi.hpp
+ *   LinearSolver::solve             include/meltpooldg/linear_algebra/linear_solver.hpp:22-134
+ *   NewtonRaphsonSolver             source/linear_algebra/newton_raphson_solver.cpp:22-152
+ *   Predictor (linear)              include/meltpooldg/linear_algebra/predictor.hpp:118-160
+ *   HeatDiffuseOperation::solve     source/heat/heat_diffuse_operation.cpp:213-289
+ *
+ * Mesh: a structured hexahedral box, FE_Q(degree) on Gauss-Lobatto support
+ * points, QGauss(degree+1), DoFs numbered lexicographically on the
+ * (degree*cells+1)^3 nodal grid (x fastest). The geometry is either the
+ * affine box or a trilinear map of vertices perturbed inside the box, with
+ * per-quadrature-point geometric factors resident on the device.
+ */
+#ifndef MPDG_HEAT_H
+#define MPDG_HEAT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+  MPDG_OK = 0,
+  MPDG_ERR_INVALID_ARGUMENT = 1,   /* deal.II Assert/AssertThrow on arguments      */
+  MPDG_ERR_OUT_OF_MEMORY = 2,
+  MPDG_ERR_NOT_CONVERGED = 3,      /* SolverControl::NoConvergence                 */
+  MPDG_ERR_NAN = 4,                /* residual became NaN/Inf                      */
+  MPDG_ERR_BREAKDOWN = 5,          /* CG p.Ap <= 0 or GMRES breakdown              */
+  MPDG_ERR_CUDA = 6,               /* a CUDA runtime call failed                   */
+  MPDG_ERR_ZERO_TIME_INCREMENT = 7,/* AssertThrowZeroTimeIncrement (exceptions.hpp:6) */
+  MPDG_ERR_NEWTON_NOT_CONVERGED = 8,/* ExcNewtonDidNotConverge -> ExcHeatTransferNoConvergence */
+  MPDG_ERR_NOT_SUPPORTED = 9
+};
+
+/* ---- mesh, material, parameters -------------------------------------- */
+typedef struct {
+  int      degree;             /* FE_Q degree, 1..6 (fe_util.hpp:30)                 */
+  int      cells[3];           /* cells per direction                                */
+  double   lo[3], hi[3];       /* box corners                                        */
+  double   perturb;            /* interior vertex perturbation, fraction of h (0 = affine) */
+  uint64_t seed;               /* perturbation seed (splitmix64 counter hash)        */
+  int      dirichlet_mask;     /* bit f: face f Dirichlet (0 x-,1 x+,2 y-,3 y+,4 z-,5 z+) */
+  double   dirichlet_value[6]; /* constant Dirichlet value per face                  */
+} mpdg_mesh_desc;
+
+enum { MPDG_LAW_CONSTANT = 0, MPDG_LAW_LINEAR_K = 1, MPDG_LAW_LIQUID_SOLID = 2 };
+
+/* Material law (Material::compute_parameters, material.templates.hpp:104-137,226-375):
+ *   CONSTANT      rho*cp and k constant (material type gas / liquid)
+ *   LINEAR_K      k(T) = k_l + k1*T, rho*cp constant (new law, no reference counterpart)
+ *   LIQUID_SOLID  cubic smoothstep in the solid fraction between liquid and solid values,
+ *                 mushy zone or sharp transition (material.templates.hpp:296-375,745-780) */
+typedef struct {
+  int    law;
+  int    sharp;            /* LIQUID_SOLID: 0 mushy zone, 1 sharp                    */
+  int    volume_specific;  /* interpolate rho*cp directly (heat_data diffuse option) */
+  double rho_l, cp_l, k_l; /* liquid, or the single constant phase                   */
+  double rho_s, cp_s, k_s; /* solid                                                  */
+  double T_solidus, T_liquidus;
+  double k1;
+} mpdg_material;
+
+enum { MPDG_SOLVER_CG = 0, MPDG_SOLVER_GMRES = 1 };           /* LinearSolverType  */
+enum { MPDG_PRECOND_IDENTITY = 0, MPDG_PRECOND_JACOBI = 1,    /* PreconditionerType */
+       MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 = 2 };
+
+typedef struct {
+  int    solver;              /* MPDG_SOLVER_*                                      */
+  int    preconditioner;      /* MPDG_PRECOND_*                                     */
+  int    max_iterations;      /* linear_solver_data.hpp:44 default 10000            */
+  double rel_tolerance;       /* default 1e-12                                      */
+  double abs_tolerance;       /* default 1e-20                                      */
+  int    gmres_restart;       /* GMRES basis size before restart (default 28)       */
+  int    cheb_degree;         /* Chebyshev: FP32 operator applications per call      */
+  int    cheb_eig_iterations; /* Lanczos steps for the eigenvalue estimate          */
+  double cheb_max_factor;     /* upper bound = factor * estimated lambda_max        */
+  double cheb_min_fraction;   /* lower bound = max(lambda_min estimate, fraction*upper) */
+  double tol_reference_norm;  /* > 0: stop when |r| <= rel_tolerance * this value   */
+} mpdg_solver_params;
+
+typedef struct {
+  int    iterations;          /* SolverControl::last_step()                         */
+  int    status;              /* MPDG_OK or an error code                           */
+  double initial_residual;
+  double final_residual;      /* recursive residual at exit                         */
+  double true_residual;       /* |b - A x| recomputed in FP64 (mixed precision)     */
+  double lambda_min, lambda_max; /* Chebyshev interval used                         */
+} mpdg_solve_stats;
+
+typedef struct mpdg_heat mpdg_heat;
+
+/* Default parameters (MeltPoolDG defaults, linear_solver_data.hpp:40-47). */
+void mpdg_solver_params_default(mpdg_solver_params *prm);
+
+/* ---- lifetime (ScratchData::build + operator construction) ----------- */
+int mpdg_heat_create(const mpdg_mesh_desc *desc, int device, mpdg_heat **out);
+int mpdg_heat_destroy(mpdg_heat *h);
+/* Enqueue all work of this handle on `stream` (a cudaStream_t; NULL = legacy default). */
+int mpdg_heat_set_stream(mpdg_heat *h, void *stream);
+int mpdg_heat_n_dofs(const mpdg_heat *h, int64_t *n_dofs);
+int mpdg_heat_n_cells(const mpdg_heat *h, int64_t *n_cells);
+int mpdg_heat_dof_dims(const mpdg_heat *h, int dims[3]);
+/* Device memory the handle holds (geometry, FP32 copies, solver workspace), bytes. */
+int mpdg_heat_device_bytes(const mpdg_heat *h, int64_t *bytes);
+
+/* ---- operator coefficients ------------------------------------------ */
+/* Material law (Material ctor + HeatDiffuseMultiPhaseOperator ctor, do_solidification =
+ * law != CONSTANT). */
+int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m);
+/* OperatorBase::reset_time_increment (operator_base.hpp:41-46). */
+int mpdg_heat_reset_time_increment(mpdg_heat *h, double dt);
+/* The operator's references to `temperature` (linearisation point) and
+ * `temperature_old` (heat_diffuse_operator.hpp:128-135). Device pointers that must
+ * stay valid while the operator is used; FP32 copies for the FP32 operator are
+ * refreshed by this call. */
+int mpdg_heat_set_linearization(mpdg_heat *h, const double *temperature,
+                                const double *temperature_old);
+
+/* ---- OperatorMatrixFree verbs --------------------------------------- */
+/* dst = J src (vmult, heat_diffuse_operator.cpp:179-197): dst zeroed first, Dirichlet
+ * entries of src read as zero, constrained rows of dst left zero. */
+int mpdg_heat_vmult(mpdg_heat *h, double *dst, const double *src);
+/* Same operator in FP32 (geometry, linearisation point and coefficients in FP32). */
+int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src);
+/* compute_inverse_diagonal_from_matrixfree (heat_diffuse_operator.cpp:271-284):
+ * diag(J) inverted with |d| > 1e-10 ? 1/d : 1. */
+int mpdg_heat_compute_inverse_diagonal(mpdg_heat *h, double *inv_diag);
+/* create_rhs(dst, src) (heat_diffuse_operator.cpp:783-806): dst += -R(T) with T the
+ * linearisation point, src = temperature_old, heat_source the nodal source vector
+ * (may be NULL for zero); dst is not zeroed. */
+int mpdg_heat_create_rhs(mpdg_heat *h, double *dst, const double *src,
+                         const double *heat_source);
+/* AffineConstraints::distribute: set Dirichlet DoFs of u to their values. */
+int mpdg_heat_distribute_constraints(mpdg_heat *h, double *u);
+/* VectorTools::compute_norm(u, L2) with QGauss(p+1) (vector_tools.cpp:188-200). */
+int mpdg_heat_l2_norm(mpdg_heat *h, const double *u, double *norm);
+/* DoF support point coordinates, xyz[3*i + d] (device pointer, 3*n_dofs doubles). */
+int mpdg_heat_support_points(mpdg_heat *h, double *xyz);
+/* Nodal interpolation of the volumetric Gaussian source
+ * q(x) = amplitude * exp(-|x - center|^2 / radius^2) (cf. laser_heat_source_volumetric.cpp). */
+int mpdg_heat_gaussian_source(mpdg_heat *h, double *q, double amplitude, const double center[3],
+                              double radius);
+
+/* ---- preconditioner + linear solver ---------------------------------- */
+/* JacobiPreconditioner::update (preconditioner_jacobi.hpp:65-69): stores the inverse
+ * diagonal at the current linearisation point inside the handle. */
+int mpdg_heat_preconditioner_update(mpdg_heat *h);
+/* JacobiPreconditioner::vmult: dst = src .* inv_diag. */
+int mpdg_heat_preconditioner_vmult(mpdg_heat *h, double *dst, const double *src);
+/* LinearSolver::solve(op, x, b, data, precond) (linear_solver.hpp:22-134): solve J x = b
+ * from the initial guess in x, ReductionControl(max_it, abs_tol, rel_tol). CG or GMRES,
+ * identity / Jacobi / FP32 Chebyshev-Jacobi preconditioning; the preconditioner must
+ * have been updated. */
+int mpdg_heat_linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x,
+                           const double *b, mpdg_solve_stats *stats);
+
+/* ---- time step --------------------------------------------------------- */
+enum { MPDG_PREDICTOR_NONE = 0, MPDG_PREDICTOR_LINEAR = 1, MPDG_PREDICTOR_GIVEN = 2 };
+
+typedef struct {
+  int    newton_max_iterations;   /* nonlinear_solver_data.hpp:13 default 10 */
+  double newton_residual_tolerance;   /* default 1e-9  */
+  double newton_correction_tolerance; /* default 1e-10 */
+  int    predictor;               /* MPDG_PREDICTOR_*                         */
+  int    single_linearization;    /* 1: one linearisation per step, stop at
+                                     |b - J T| <= rel_tolerance |b|, b = J T_g - R(T_g) */
+  mpdg_solver_params linear;
+} mpdg_step_params;
+
+typedef struct {
+  int    newton_iterations;
+  int    linear_iterations;
+  int    converged;
+  double initial_relative_residual; /* |R(T_g)| / |b| for single_linearization      */
+  double step_ms;                   /* device time of the step (CUDA events)        */
+} mpdg_step_stats;
+
+void mpdg_step_params_default(mpdg_step_params *prm);
+
+/* Initial guess used by MPDG_PREDICTOR_GIVEN (e.g. a learned predictor's output);
+ * a device pointer that must stay valid until the step has run. */
+int mpdg_heat_set_guess(mpdg_heat *h, const double *guess);
+
+/* HeatDiffuseOperation::solve (heat_diffuse_operation.cpp:213-289) on device vectors:
+ * predictor (none / linear extrapolation / the guess already in T_cur), history
+ * commit (T_old <- T_cur), Dirichlet values, preconditioner update at the predicted
+ * state, Newton-Raphson with increment solves (or one linearisation, see above).
+ * T_cur and T_old are updated in place; heat_source may be NULL. */
+int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, double dt, double dt_old,
+                        double *T_cur, double *T_old, const double *heat_source,
+                        mpdg_step_stats *stats);
+
+/* Same with HOST vectors: copies T_cur, T_old, heat_source to the device, runs the
+ * step, copies T_cur and T_old back (the reference operation's own data location). */
+int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *prm, double dt,
+                             double dt_old, double *T_cur, double *T_old,
+                             const double *heat_source, mpdg_step_stats *stats);
+
+/* Last error message of this thread (static storage). */
+const char *mpdg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,72 @@
+// Argument structs shared by the cell kernels and the handle code.
+#pragma once
+
+#include <stdint.h>
+
+namespace mpdg {
+
+// ---------------------------------------------------------------------------
+// argument structs
+// ---------------------------------------------------------------------------
+struct MeshDims {
+  int m[3];   // cells per direction
+  int nd[3];  // DoFs per direction
+  int p;      // degree
+  int dmask;  // Dirichlet faces (bit f: 0 x-,1 x+,2 y-,3 y+,4 z-,5 z+)
+};
+
+template <typename T>
+struct MatParams {
+  T rho_l, cp_l, k_l, rho_s, cp_s, k_s;
+  T T_liq, T_sol, inv_mushy, k1;
+  T idt;
+  int sharp, vs, need_told;
+};
+
+template <typename T>
+struct GeoParams {
+  T detJ;                   // uniform box: det(J)
+  T Gd[3];                  // uniform box: det(J) / h_d^2
+  const T *__restrict__ q;  // deformed: [cell][7][n^3] = JxW, Gxx Gxy Gxz Gyy Gyz Gzz
+};
+
+// Scalars of a device-resident Krylov iteration (read by kernels, finalised
+// by the last CTA of a reduction, polled by the host).
+struct SolverState {
+  double rz, rz_old, alpha, beta, pAp, rr, res, res0, tol, zAp;
+  int it, max_it, done, status;  // done: 0 running, 1 converged, 2 stopped
+  int first;                     // preconditioned CG: first direction (beta = 0)
+  int record;                    // record alpha/beta history (Lanczos)
+  double hist_alpha[64], hist_beta[64];
+};
+
+enum FinMode { FIN_NONE = 0, FIN_STORE = 1, FIN_CG_ALPHA = 2 };
+
+template <typename T>
+struct CellArgs {
+  int64_t n_cells;
+  MeshDims d;
+  GeoParams<T> g;
+  MatParams<T> m;
+  const T *__restrict__ src;
+  T *dst;
+  const T *__restrict__ Tl;
+  const T *__restrict__ To;
+  const T *__restrict__ qs;
+  double *partials;    // per-CTA partial sums
+  unsigned *counter;   // last-CTA election counter (reset by the last CTA)
+  SolverState *st;     // early exit when st->done; alpha finalisation
+  double *out;         // FIN_STORE destination
+  int fin;
+};
+
+// ---------------------------------------------------------------------------
+// launch shapes
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int cells_per_block(int n)
+{
+  return n == 2 ? 32 : n == 3 ? 14 : n == 4 ? 8 : n == 5 ? 5 : n == 6 ? 4 : 2;
+}
+__host__ __device__ constexpr int block_threads(int n) { return cells_per_block(n) * n * n; }
+
+}  // namespace mpdg

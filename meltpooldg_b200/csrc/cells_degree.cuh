@@ -1,0 +1,152 @@
+// Host launchers of the cell kernels for one polynomial degree. Each
+// cells_pN.cu translation unit includes this header and instantiates
+// MPDG_DEFINE_DEGREE(n) so the degrees compile in parallel; the handle code
+// reaches them through DegreeTable.
+#pragma once
+
+#include "cell_kernels.cuh"
+#include "degree_table.hpp"
+
+namespace mpdg {
+
+template <typename K>
+static int persistent_grid(K kernel, int threads, size_t smem, int64_t n_batches, int sm_count,
+                           int *cache)
+{
+  if (*cache <= 0) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    *cache = per_sm > 0 ? per_sm : 1;
+  }
+  int64_t g = (int64_t)(*cache) * sm_count;
+  if (g > n_batches) g = n_batches;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+template <int n>
+struct DegreeOps {
+  static constexpr int CPB = cells_per_block(n);
+  static constexpr int THREADS = block_threads(n);
+
+  static void upload(const double *tab, const float *tabf, const double *w, const float *wf)
+  {
+    cudaMemcpyToSymbol(c_tab_d, tab, sizeof(double) * kTabSize);
+    cudaMemcpyToSymbol(c_tab_f, tabf, sizeof(float) * kTabSize);
+    cudaMemcpyToSymbol(c_w_d, w, sizeof(double) * kWSize);
+    cudaMemcpyToSymbol(c_w_f, wf, sizeof(float) * kWSize);
+  }
+
+  template <typename T, int GEO, int LAW>
+  static cudaError_t vmult_t(const CellArgs<T> &a, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_vmult<n, T, GEO, LAW>;
+    const size_t smem = smem_vmult<n, T>(LAW != 0);
+    const int64_t nb = (a.n_cells + CPB - 1) / CPB;
+    const int g = persistent_grid(k, THREADS, smem, nb, sm, &cache);
+    k<<<g, THREADS, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  static cudaError_t vmult(const CellArgs<T> &a, int geo, int law, cudaStream_t s, int sm)
+  {
+    if (geo == 0) {
+      if (law == 0) return vmult_t<T, 0, 0>(a, s, sm);
+      if (law == 1) return vmult_t<T, 0, 1>(a, s, sm);
+      return vmult_t<T, 0, 2>(a, s, sm);
+    }
+    if (law == 0) return vmult_t<T, 1, 0>(a, s, sm);
+    if (law == 1) return vmult_t<T, 1, 1>(a, s, sm);
+    return vmult_t<T, 1, 2>(a, s, sm);
+  }
+  static cudaError_t vmult_d(const CellArgs<double> &a, int geo, int law, cudaStream_t s, int sm)
+  {
+    return vmult<double>(a, geo, law, s, sm);
+  }
+  static cudaError_t vmult_f(const CellArgs<float> &a, int geo, int law, cudaStream_t s, int sm)
+  {
+    return vmult<float>(a, geo, law, s, sm);
+  }
+
+  template <int GEO, int LAW>
+  static cudaError_t rhs_t(const CellArgs<double> &a, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_rhs<n, GEO, LAW>;
+    const size_t smem = smem_rhs<n>();
+    const int g = persistent_grid(k, THREADS, smem, (a.n_cells + CPB - 1) / CPB, sm, &cache);
+    k<<<g, THREADS, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t rhs(const CellArgs<double> &a, int geo, int law, cudaStream_t s, int sm)
+  {
+    if (geo == 0) {
+      if (law == 0) return rhs_t<0, 0>(a, s, sm);
+      if (law == 1) return rhs_t<0, 1>(a, s, sm);
+      return rhs_t<0, 2>(a, s, sm);
+    }
+    if (law == 0) return rhs_t<1, 0>(a, s, sm);
+    if (law == 1) return rhs_t<1, 1>(a, s, sm);
+    return rhs_t<1, 2>(a, s, sm);
+  }
+
+  template <int GEO, int LAW>
+  static cudaError_t diag_t(const CellArgs<double> &a, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_diag<n, GEO, LAW>;
+    const size_t smem = smem_diag<n>();
+    const int g = persistent_grid(k, THREADS, smem, (a.n_cells + CPB - 1) / CPB, sm, &cache);
+    k<<<g, THREADS, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t diag(const CellArgs<double> &a, int geo, int law, cudaStream_t s, int sm)
+  {
+    if (geo == 0) {
+      if (law == 0) return diag_t<0, 0>(a, s, sm);
+      if (law == 1) return diag_t<0, 1>(a, s, sm);
+      return diag_t<0, 2>(a, s, sm);
+    }
+    if (law == 0) return diag_t<1, 0>(a, s, sm);
+    if (law == 1) return diag_t<1, 1>(a, s, sm);
+    return diag_t<1, 2>(a, s, sm);
+  }
+
+  template <int GEO>
+  static cudaError_t norm_t(const CellArgs<double> &a, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_norm<n, GEO>;
+    const size_t smem = smem_norm<n>();
+    const int g = persistent_grid(k, THREADS, smem, (a.n_cells + CPB - 1) / CPB, sm, &cache);
+    k<<<g, THREADS, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t norm(const CellArgs<double> &a, int geo, int, cudaStream_t s, int sm)
+  {
+    return geo == 0 ? norm_t<0>(a, s, sm) : norm_t<1>(a, s, sm);
+  }
+
+  static DegreeTable table()
+  {
+    DegreeTable t;
+    t.n = n;
+    t.upload = &upload;
+    t.vmult_d = &vmult_d;
+    t.vmult_f = &vmult_f;
+    t.rhs = &rhs;
+    t.diag = &diag;
+    t.norm = &norm;
+    return t;
+  }
+};
+
+}  // namespace mpdg
+
+#define MPDG_DEFINE_DEGREE(N)                                            \
+  namespace mpdg {                                                       \
+  DegreeTable degree_table_##N() { return DegreeOps<N>::table(); }        \
+  }

@@ -1,0 +1,27 @@
+// Function table of the per-degree cell-kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace mpdg {
+
+template <typename T> struct CellArgs;
+
+struct DegreeTable {
+  int n = 0;
+  void (*upload)(const double *tab, const float *tabf, const double *w, const float *wf) = nullptr;
+  cudaError_t (*vmult_d)(const CellArgs<double> &, int geo, int law, cudaStream_t, int sm) = nullptr;
+  cudaError_t (*vmult_f)(const CellArgs<float> &, int geo, int law, cudaStream_t, int sm) = nullptr;
+  cudaError_t (*rhs)(const CellArgs<double> &, int geo, int law, cudaStream_t, int sm) = nullptr;
+  cudaError_t (*diag)(const CellArgs<double> &, int geo, int law, cudaStream_t, int sm) = nullptr;
+  cudaError_t (*norm)(const CellArgs<double> &, int geo, int law, cudaStream_t, int sm) = nullptr;
+};
+
+DegreeTable degree_table_2();
+DegreeTable degree_table_3();
+DegreeTable degree_table_4();
+DegreeTable degree_table_5();
+DegreeTable degree_table_6();
+DegreeTable degree_table_7();
+
+}  // namespace mpdg

@@ -1,0 +1,1538 @@
+// Handle, setup kernels, Krylov drivers and the C ABI of the B200-native heat
+// operator (include/mpdg_heat.h).
+//
+// Everything a solve touches stays resident on the device: the geometry
+// factors, the solution history, the inverse diagonal and its FP32 copy, the
+// FP32 copies of the linearisation point and the Krylov vectors. Krylov
+// scalars (alpha, beta, residual norms, convergence flag) are computed on the
+// device by the last CTA of each fused reduction and every kernel of an
+// iteration exits immediately once the flag is set, so the host only polls
+// the flag every few iterations instead of synchronising per iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mpdg_heat.h"
+#include "cell_args.cuh"
+#include "degree_table.hpp"
+#include "fe_tables.hpp"
+#include "reduce.cuh"
+
+using namespace mpdg;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg)
+{
+  g_err = msg;
+  return code;
+}
+
+#define CU(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(e_ == cudaErrorMemoryAllocation ? MPDG_ERR_OUT_OF_MEMORY : MPDG_ERR_CUDA, \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+#define TRY(call)                  \
+  do {                             \
+    int r_ = (call);               \
+    if (r_ != MPDG_OK) return r_;  \
+  } while (0)
+
+extern "C" const char *mpdg_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+constexpr int VT = 256;  // threads of the vector kernels
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct mpdg_heat {
+  int device = 0, sm_count = 148;
+  cudaStream_t stream = nullptr;
+  mpdg_mesh_desc desc{};
+  int p = 1, n = 2, npt = 8;
+  int64_t n_dofs = 0, n_cells = 0;
+  MeshDims dims{};
+  int geo = 0;  // 0 uniform box, 1 per-quadrature-point factors
+  double hcell[3] = {1, 1, 1};
+  DegreeTable tab;
+  // geometry
+  double *vert = nullptr;  // vertices (deformed meshes)
+  double *geoq = nullptr;  // [cell][7][npt]
+  float *geoq_f = nullptr;
+  // coefficients
+  mpdg_material mat{};
+  int law = 0, need_told = 0;
+  double dt = 0.0;
+  const double *T_lin = nullptr, *T_old = nullptr;
+  float *T_lin_f = nullptr, *T_old_f = nullptr;
+  bool lin_f_dirty = true;
+  // preconditioner
+  double *inv_diag = nullptr;
+  float *inv_diag_f = nullptr;
+  bool diag_valid = false, diag_f_dirty = true;
+  double eig_min = 0.0, eig_max = 0.0;
+  bool eig_valid = false;
+  // reduction scratch
+  double *partials = nullptr;
+  unsigned *counter = nullptr;
+  SolverState *st = nullptr, *st_host = nullptr;
+  double *scal = nullptr, *scal_host = nullptr;
+  // Krylov / step workspace
+  double *r = nullptr, *pv = nullptr, *Ap = nullptr, *z = nullptr, *w1 = nullptr, *w2 = nullptr,
+         *w3 = nullptr;
+  float *r32 = nullptr, *x32 = nullptr, *d32 = nullptr, *Ax32 = nullptr;
+  double *host_T = nullptr, *host_To = nullptr, *host_q = nullptr;  // device buffers for *_host
+  const double *guess = nullptr;
+  int64_t bytes = 0;
+  std::vector<void *> owned;
+};
+
+static constexpr int kPartialsPerValue = 148 * 64;
+
+static int dalloc(mpdg_heat *h, void **p, size_t bytes)
+{
+  if (*p) return MPDG_OK;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(MPDG_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  h->owned.push_back(*p);
+  h->bytes += (int64_t)bytes;
+  return MPDG_OK;
+}
+template <typename T> static int dvec(mpdg_heat *h, T **p, int64_t n)
+{
+  return dalloc(h, reinterpret_cast<void **>(p), sizeof(T) * (size_t)n);
+}
+
+// ---------------------------------------------------------------------------
+// per-device table upload
+// ---------------------------------------------------------------------------
+static DegreeTable table_for(int n)
+{
+  switch (n) {
+  case 2: return degree_table_2();
+  case 3: return degree_table_3();
+  case 4: return degree_table_4();
+  case 5: return degree_table_5();
+  case 6: return degree_table_6();
+  default: return degree_table_7();
+  }
+}
+
+static bool g_uploaded[64][8];
+
+static int upload_tables(int device, int n)
+{
+  if (device < 0 || device >= 64) return fail(MPDG_ERR_INVALID_ARGUMENT, "device id");
+  if (g_uploaded[device][n]) return MPDG_OK;
+  std::vector<double> tab, w, xl;
+  fill_even_odd(tab, w, xl);
+  std::vector<float> tabf(tab.begin(), tab.end()), wf(w.begin(), w.end());
+  table_for(n).upload(tab.data(), tabf.data(), w.data(), wf.data());
+  CU(cudaGetLastError());
+  g_uploaded[device][n] = true;
+  return MPDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// setup kernels
+// ---------------------------------------------------------------------------
+struct Q1D {
+  double xg[kMaxN], wg[kMaxN], xl[kMaxN];
+};
+
+__device__ __forceinline__ void trilinear(const double *__restrict__ vert, const MeshDims &d, int cx,
+                                          int cy, int cz, const double xi[3], double x[3],
+                                          double J[3][3])
+{
+  for (int a = 0; a < 3; ++a) {
+    x[a] = 0.0;
+    for (int b = 0; b < 3; ++b) J[a][b] = 0.0;
+  }
+  for (int v = 0; v < 8; ++v) {
+    const int a = v & 1, b = (v >> 1) & 1, c = (v >> 2) & 1;
+    const int64_t vid =
+      (int64_t)(cx + a) + (int64_t)(d.m[0] + 1) * ((cy + b) + (int64_t)(d.m[1] + 1) * (cz + c));
+    const double *X = vert + 3 * vid;
+    const double na = a ? xi[0] : 1.0 - xi[0], da = a ? 1.0 : -1.0;
+    const double nb = b ? xi[1] : 1.0 - xi[1], db = b ? 1.0 : -1.0;
+    const double nc = c ? xi[2] : 1.0 - xi[2], dc = c ? 1.0 : -1.0;
+    const double N = na * nb * nc;
+    const double dN[3] = {da * nb * nc, na * db * nc, na * nb * dc};
+    for (int e = 0; e < 3; ++e) {
+      x[e] += X[e] * N;
+      for (int f = 0; f < 3; ++f) J[e][f] += X[e] * dN[f];
+    }
+  }
+}
+
+// per-quadrature-point JxW and G = JxW J^-1 J^-T of the trilinear map
+__global__ void k_geometry(int64_t n_cells, MeshDims d, int n, Q1D q1, const double *vert,
+                           double *geo)
+{
+  const int npt = n * n * n;
+  const int64_t total = n_cells * npt;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / npt;
+    const int q = (int)(t % npt);
+    const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
+    const int cx = (int)(c % d.m[0]), cy = (int)((c / d.m[0]) % d.m[1]),
+              cz = (int)(c / ((int64_t)d.m[0] * d.m[1]));
+    const double xi[3] = {q1.xg[qi], q1.xg[qj], q1.xg[qk]};
+    double x[3], J[3][3];
+    trilinear(vert, d, cx, cy, cz, xi, x, J);
+    const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                       J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                       J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+    double inv[3][3];
+    inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+    inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+    inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+    inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+    inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+    inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+    inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+    inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+    inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    const double w = q1.wg[qi] * q1.wg[qj] * q1.wg[qk];
+    const double jxw = det * w;
+    const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+    double *g = geo + c * 7 * npt + q;
+    g[0] = jxw;
+    for (int k = 0; k < 6; ++k) {
+      double s = 0.0;
+      for (int e = 0; e < 3; ++e) s += inv[ia[k]][e] * inv[ib[k]][e];
+      g[(1 + k) * npt] = jxw * s;
+    }
+  }
+}
+
+struct PosArgs {
+  MeshDims d;
+  int geo;
+  double lo[3], hc[3];
+  Q1D q1;
+  const double *vert;
+};
+
+__device__ __forceinline__ void dof_position(const PosArgs &a, int64_t idx, double x[3])
+{
+  const int64_t I = idx % a.d.nd[0];
+  const int64_t J = (idx / a.d.nd[0]) % a.d.nd[1];
+  const int64_t K = idx / ((int64_t)a.d.nd[0] * a.d.nd[1]);
+  const int64_t pos[3] = {I, J, K};
+  int cc[3];
+  double xi[3];
+  for (int e = 0; e < 3; ++e) {
+    cc[e] = (int)(pos[e] / a.d.p);
+    if (cc[e] >= a.d.m[e]) cc[e] = a.d.m[e] - 1;
+    xi[e] = a.q1.xl[pos[e] - (int64_t)cc[e] * a.d.p];
+  }
+  if (a.geo == 0) {
+    for (int e = 0; e < 3; ++e) x[e] = a.lo[e] + a.hc[e] * (cc[e] + xi[e]);
+  } else {
+    double J3[3][3];
+    trilinear(a.vert, a.d, cc[0], cc[1], cc[2], xi, x, J3);
+  }
+}
+
+__global__ void k_support_points(int64_t N, PosArgs a, double *xyz)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double x[3];
+    dof_position(a, i, x);
+    xyz[3 * i] = x[0];
+    xyz[3 * i + 1] = x[1];
+    xyz[3 * i + 2] = x[2];
+  }
+}
+
+__global__ void k_gaussian(int64_t N, PosArgs a, double *q, double amp, double c0, double c1,
+                           double c2, double inv_r2)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double x[3];
+    dof_position(a, i, x);
+    const double d2 = (x[0] - c0) * (x[0] - c0) + (x[1] - c1) * (x[1] - c1) + (x[2] - c2) * (x[2] - c2);
+    q[i] = amp * exp(-d2 * inv_r2);
+  }
+}
+
+// set Dirichlet values face by face; a DoF on several faces takes the value of
+// the first constrained face in the order x-, x+, y-, y+, z-, z+
+struct DirArgs {
+  MeshDims d;
+  double val[6];
+};
+__global__ void k_distribute(DirArgs a, int face, double *u)
+{
+  const int dir = face / 2;
+  const int e1 = dir == 0 ? 1 : 0, e2 = dir == 2 ? 1 : 2;
+  const int64_t n1 = a.d.nd[e1], n2 = a.d.nd[e2];
+  const int fixed = (face & 1) ? a.d.nd[dir] - 1 : 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n1 * n2;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t pos[3];
+    pos[dir] = fixed;
+    pos[e1] = t % n1;
+    pos[e2] = t / n1;
+    bool earlier = false;
+    for (int f = 0; f < face; ++f) {
+      if (!(a.d.dmask & (1 << f))) continue;
+      const int df = f / 2;
+      const int64_t at = (f & 1) ? a.d.nd[df] - 1 : 0;
+      if (pos[df] == at) earlier = true;
+    }
+    if (earlier) continue;
+    const int64_t idx = pos[0] + (int64_t)a.d.nd[0] * (pos[1] + (int64_t)a.d.nd[1] * pos[2]);
+    u[idx] = a.val[face];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// vector kernels
+// ---------------------------------------------------------------------------
+#define GRID_STRIDE(i, N) \
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (N); i += (int64_t)gridDim.x * blockDim.x)
+
+__global__ void k_cast_f(int64_t N, const double *__restrict__ x, float *__restrict__ y)
+{
+  GRID_STRIDE(i, N) y[i] = (float)x[i];
+}
+__global__ void k_invert_diag(int64_t N, double *d)
+{
+  GRID_STRIDE(i, N)
+  {
+    const double v = d[i];
+    d[i] = fabs(v) > 1.0e-10 ? 1.0 / v : 1.0;
+  }
+}
+__global__ void k_scale(int64_t N, double *dst, const double *__restrict__ src,
+                        const double *__restrict__ D)
+{
+  GRID_STRIDE(i, N) dst[i] = src[i] * D[i];
+}
+__global__ void k_predict(int64_t N, const double *__restrict__ T, const double *__restrict__ To,
+                          double *out, double f)
+{
+  GRID_STRIDE(i, N) out[i] = (f + 1.0) * T[i] - f * To[i];
+}
+__global__ void k_axpy(int64_t N, double *y, double a, const double *__restrict__ x)
+{
+  GRID_STRIDE(i, N) y[i] += a * x[i];
+}
+__global__ void k_masked_random(int64_t N, MeshDims d, double *b)
+{
+  GRID_STRIDE(i, N)
+  {
+    const int64_t I = i % d.nd[0], J = (i / d.nd[0]) % d.nd[1], K = i / ((int64_t)d.nd[0] * d.nd[1]);
+    uint64_t x = 0x9E3779B97F4A7C15ULL * (uint64_t)(i + 1) + 0x632BE59BD9B4E019ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    x ^= x >> 31;
+    const bool c = ((d.dmask & 1) && I == 0) || ((d.dmask & 2) && I == d.nd[0] - 1) ||
+                   ((d.dmask & 4) && J == 0) || ((d.dmask & 8) && J == d.nd[1] - 1) ||
+                   ((d.dmask & 16) && K == 0) || ((d.dmask & 32) && K == d.nd[2] - 1);
+    b[i] = c ? 0.0 : 2.0 * ((double)(x >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+  }
+}
+
+// sums[0] = a.a, sums[1] = (a+b).(a+b) (b may be null), written to out[0..1]
+__global__ void k_norms(int64_t N, const double *__restrict__ a, const double *__restrict__ b,
+                        double *partials, unsigned *counter, double *out)
+{
+  double v[2] = {0.0, 0.0};
+  GRID_STRIDE(i, N)
+  {
+    const double x = a[i];
+    v[0] += x * x;
+    const double y = b ? x + b[i] : x;
+    v[1] += y * y;
+  }
+  double tot[2];
+  if (grid_sum<2>(v, partials, counter, tot)) {
+    out[0] = tot[0];
+    out[1] = tot[1];
+  }
+}
+
+// ---- Jacobi / identity preconditioned CG (FP64) ----------------------------
+// init: r = b - Ax ; z = D r ; p = z ; Ap = 0 ; rz, rr -> state
+__global__ void k_cg_init(int64_t N, const double *__restrict__ b, double *r, double *p,
+                          double *Ap, const double *__restrict__ D, SolverState *st,
+                          double *partials, unsigned *counter, double rel, double abs_tol,
+                          double ref_norm, int max_it, int record)
+{
+  double v[2] = {0.0, 0.0};
+  GRID_STRIDE(i, N)
+  {
+    const double ri = b[i] - Ap[i];
+    const double zi = D ? D[i] * ri : ri;
+    r[i] = ri;
+    p[i] = zi;
+    Ap[i] = 0.0;
+    v[0] += ri * zi;
+    v[1] += ri * ri;
+  }
+  double tot[2];
+  if (grid_sum<2>(v, partials, counter, tot)) {
+    st->rz = tot[0];
+    st->rr = tot[1];
+    st->res = st->res0 = sqrt(tot[1]);
+    st->tol = fmax(abs_tol, rel * (ref_norm > 0.0 ? ref_norm : st->res0));
+    st->it = 0;
+    st->max_it = max_it;
+    st->status = 0;
+    st->first = 1;
+    st->record = record;
+    st->alpha = st->beta = 0.0;
+    if (!isfinite(st->res)) {
+      st->done = 2;
+      st->status = MPDG_ERR_NAN;
+    } else if (st->res <= st->tol) {
+      st->done = 1;
+    } else if (max_it <= 0) {
+      st->done = 2;
+      st->status = MPDG_ERR_NOT_CONVERGED;
+    } else {
+      st->done = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ void finish_iteration(SolverState *st, double rr)
+{
+  const int it = ++st->it;
+  st->rr = rr;
+  st->res = sqrt(rr);
+  if (st->record && it <= 64) {
+    st->hist_alpha[it - 1] = st->alpha;
+    st->hist_beta[it - 1] = st->beta;
+  }
+  if (!isfinite(st->res)) {
+    st->done = 2;
+    st->status = MPDG_ERR_NAN;
+  } else if (st->res <= st->tol) {
+    st->done = 1;
+  } else if (it >= st->max_it) {
+    st->done = 2;
+    st->status = MPDG_ERR_NOT_CONVERGED;
+  }
+}
+
+// x += alpha p ; r -= alpha Ap ; rz = r.D r ; rr = r.r ; beta = rz / rz_old
+__global__ void k_cg_update_xr(int64_t N, double *x, double *r, const double *__restrict__ p,
+                               const double *__restrict__ Ap, const double *__restrict__ D,
+                               SolverState *st, double *partials, unsigned *counter)
+{
+  if (st->done) return;
+  const double alpha = st->alpha;
+  double v[2] = {0.0, 0.0};
+  GRID_STRIDE(i, N)
+  {
+    x[i] += alpha * p[i];
+    const double ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    const double zi = D ? D[i] * ri : ri;
+    v[0] += ri * zi;
+    v[1] += ri * ri;
+  }
+  double tot[2];
+  if (grid_sum<2>(v, partials, counter, tot)) {
+    st->beta = tot[0] / st->rz;
+    st->rz_old = st->rz;
+    st->rz = tot[0];
+    finish_iteration(st, tot[1]);
+  }
+}
+
+// p = D r + beta p ; Ap = 0
+__global__ void k_cg_update_p(int64_t N, const double *__restrict__ r, double *p, double *Ap,
+                              const double *__restrict__ D, const SolverState *st)
+{
+  if (st->done) return;
+  const double beta = st->beta;
+  GRID_STRIDE(i, N)
+  {
+    const double zi = D ? D[i] * r[i] : r[i];
+    p[i] = zi + beta * p[i];
+    Ap[i] = 0.0;
+  }
+}
+
+// ---- FP64 CG with the FP32 Chebyshev-Jacobi preconditioner ------------------
+// init: r = b - Ax ; rr ; r32 = r ; x32 = D32 r32 / theta ; d32 = x32 ; Ap = 0 ; Ax32 = 0
+__global__ void k_cgm_init(int64_t N, const double *__restrict__ b, double *r, double *Ap,
+                           float *r32, float *x32, float *d32, float *Ax32,
+                           const float *__restrict__ D32, float inv_theta, SolverState *st,
+                           double *partials, unsigned *counter, double rel, double abs_tol,
+                           double ref_norm, int max_it)
+{
+  double v[1] = {0.0};
+  GRID_STRIDE(i, N)
+  {
+    const double ri = b[i] - Ap[i];
+    r[i] = ri;
+    Ap[i] = 0.0;
+    const float rf = (float)ri;
+    r32[i] = rf;
+    const float xf = D32[i] * rf * inv_theta;
+    x32[i] = xf;
+    d32[i] = xf;
+    Ax32[i] = 0.0f;
+    v[0] += ri * ri;
+  }
+  double tot[1];
+  if (grid_sum<1>(v, partials, counter, tot)) {
+    st->rr = tot[0];
+    st->res = st->res0 = sqrt(tot[0]);
+    st->tol = fmax(abs_tol, rel * (ref_norm > 0.0 ? ref_norm : st->res0));
+    st->it = 0;
+    st->max_it = max_it;
+    st->status = 0;
+    st->first = 1;
+    st->record = 0;
+    st->alpha = st->beta = 0.0;
+    if (!isfinite(st->res)) {
+      st->done = 2;
+      st->status = MPDG_ERR_NAN;
+    } else if (st->res <= st->tol) {
+      st->done = 1;
+    } else if (max_it <= 0) {
+      st->done = 2;
+      st->status = MPDG_ERR_NOT_CONVERGED;
+    } else {
+      st->done = 0;
+    }
+  }
+}
+
+// Chebyshev step: d = c1 d + c2 D32 (r32 - Ax32) ; x32 += d ; Ax32 = 0
+__global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32, float *d32,
+                            float *Ax32, const float *__restrict__ D32, float c1, float c2,
+                            const SolverState *st)
+{
+  if (st->done) return;
+  GRID_STRIDE(i, N)
+  {
+    const float dn = c1 * d32[i] + c2 * D32[i] * (r32[i] - Ax32[i]);
+    d32[i] = dn;
+    x32[i] += dn;
+    Ax32[i] = 0.0f;
+  }
+}
+
+// last Chebyshev step, then z = x32 (FP64), rz = r.z, zAp = z.Ap and the
+// flexible (Polak-Ribiere) beta = (z.r - alpha z.Ap) / rz_old
+__global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const float *__restrict__ x32,
+                            const float *__restrict__ d32, float *Ax32,
+                            const float *__restrict__ D32, float c1, float c2,
+                            const double *__restrict__ r, const double *__restrict__ Ap, double *z,
+                            SolverState *st, double *partials, unsigned *counter)
+{
+  if (st->done) return;
+  double v[2] = {0.0, 0.0};
+  GRID_STRIDE(i, N)
+  {
+    const float dn = c1 * d32[i] + c2 * D32[i] * (r32[i] - Ax32[i]);
+    const double zi = (double)(x32[i] + dn);
+    Ax32[i] = 0.0f;
+    z[i] = zi;
+    v[0] += zi * r[i];
+    v[1] += zi * Ap[i];
+  }
+  double tot[2];
+  if (grid_sum<2>(v, partials, counter, tot)) {
+    if (st->first) {
+      st->beta = 0.0;
+      st->first = 0;
+    } else {
+      st->beta = (tot[0] - st->alpha * tot[1]) / st->rz;
+    }
+    st->rz = tot[0];
+    st->zAp = tot[1];
+  }
+}
+
+// x += alpha p ; r -= alpha Ap ; rr ; r32 = r ; x32 = D32 r32 / theta ; d32 = x32
+__global__ void k_cgm_update_xr(int64_t N, double *x, double *r, const double *__restrict__ p,
+                                const double *__restrict__ Ap, float *r32, float *x32, float *d32,
+                                const float *__restrict__ D32, float inv_theta, SolverState *st,
+                                double *partials, unsigned *counter)
+{
+  if (st->done) return;
+  const double alpha = st->alpha;
+  double v[1] = {0.0};
+  GRID_STRIDE(i, N)
+  {
+    x[i] += alpha * p[i];
+    const double ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    const float rf = (float)ri;
+    r32[i] = rf;
+    const float xf = D32[i] * rf * inv_theta;
+    x32[i] = xf;
+    d32[i] = xf;
+    v[0] += ri * ri;
+  }
+  double tot[1];
+  if (grid_sum<1>(v, partials, counter, tot)) finish_iteration(st, tot[0]);
+}
+
+// p = z + beta p ; Ap = 0
+__global__ void k_cgm_update_p(int64_t N, const double *__restrict__ z, double *p, double *Ap,
+                               const SolverState *st)
+{
+  if (st->done) return;
+  const double beta = st->beta;
+  GRID_STRIDE(i, N)
+  {
+    p[i] = beta != 0.0 ? z[i] + beta * p[i] : z[i];  // first direction: p = z
+    Ap[i] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+static int vgrid(const mpdg_heat *h, int64_t N)
+{
+  int64_t g = (N + VT - 1) / VT;
+  const int64_t cap = (int64_t)h->sm_count * 8;
+  if (g > cap) g = cap;
+  return (int)std::max<int64_t>(g, 1);
+}
+
+template <typename T>
+static CellArgs<T> cell_args(mpdg_heat *h)
+{
+  CellArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  a.n_cells = h->n_cells;
+  a.d = h->dims;
+  const double detJ = h->hcell[0] * h->hcell[1] * h->hcell[2];
+  a.g.detJ = (T)detJ;
+  for (int e = 0; e < 3; ++e) a.g.Gd[e] = (T)(detJ / (h->hcell[e] * h->hcell[e]));
+  a.g.q = nullptr;
+  const mpdg_material &m = h->mat;
+  a.m.rho_l = (T)m.rho_l;
+  a.m.cp_l = (T)m.cp_l;
+  a.m.k_l = (T)m.k_l;
+  a.m.rho_s = (T)m.rho_s;
+  a.m.cp_s = (T)m.cp_s;
+  a.m.k_s = (T)m.k_s;
+  a.m.T_liq = (T)m.T_liquidus;
+  a.m.T_sol = (T)m.T_solidus;
+  a.m.inv_mushy = (T)(m.T_liquidus != m.T_solidus ? 1.0 / (m.T_liquidus - m.T_solidus) : 0.0);
+  a.m.k1 = (T)m.k1;
+  a.m.idt = (T)(1.0 / h->dt);
+  a.m.sharp = m.sharp;
+  a.m.vs = m.volume_specific;
+  a.m.need_told = h->need_told;
+  a.partials = h->partials;
+  a.counter = h->counter;
+  a.fin = FIN_NONE;
+  return a;
+}
+
+static int ensure_dt(mpdg_heat *h)
+{
+  if (!(h->dt != 0.0) || !std::isfinite(h->dt))
+    return fail(MPDG_ERR_ZERO_TIME_INCREMENT, "time increment is zero: call reset_time_increment");
+  return MPDG_OK;
+}
+
+static int ensure_lin(mpdg_heat *h)
+{
+  if (h->law != MPDG_LAW_CONSTANT && !h->T_lin)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "temperature-dependent law needs set_linearization");
+  if (h->law == MPDG_LAW_LIQUID_SOLID && h->need_told && !h->T_old)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "liquid-solid law needs temperature_old");
+  return MPDG_OK;
+}
+
+// dst += J src (FP64); fin/out/st select the fused src.dst reduction
+static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, double *out,
+                      SolverState *st)
+{
+  TRY(ensure_dt(h));
+  TRY(ensure_lin(h));
+  CellArgs<double> a = cell_args<double>(h);
+  a.g.q = h->geoq;
+  a.src = src;
+  a.dst = dst;
+  a.Tl = h->T_lin;
+  a.To = h->T_old;
+  a.fin = fin;
+  a.out = out;
+  a.st = st;
+  CU(h->tab.vmult_d(a, h->geo, h->law, h->stream, h->sm_count));
+  return MPDG_OK;
+}
+
+static int refresh_f32(mpdg_heat *h)
+{
+  const int64_t N = h->n_dofs;
+  if (h->geo == 1 && !h->geoq_f) {
+    const int64_t ng = h->n_cells * 7 * h->npt;
+    TRY(dvec(h, &h->geoq_f, ng));
+    k_cast_f<<<vgrid(h, ng), VT, 0, h->stream>>>(ng, h->geoq, h->geoq_f);
+    CU(cudaGetLastError());
+  }
+  if (h->lin_f_dirty && h->law != MPDG_LAW_CONSTANT) {
+    TRY(dvec(h, &h->T_lin_f, N));
+    TRY(dvec(h, &h->T_old_f, N));
+    k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->T_lin, h->T_lin_f);
+    if (h->T_old) k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->T_old, h->T_old_f);
+    CU(cudaGetLastError());
+  }
+  h->lin_f_dirty = false;
+  return MPDG_OK;
+}
+
+static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *st)
+{
+  TRY(ensure_dt(h));
+  TRY(ensure_lin(h));
+  TRY(refresh_f32(h));
+  CellArgs<float> a = cell_args<float>(h);
+  a.g.q = h->geoq_f;
+  a.src = src;
+  a.dst = dst;
+  a.Tl = h->T_lin_f;
+  a.To = h->T_old_f;
+  a.st = st;
+  CU(h->tab.vmult_f(a, h->geo, h->law, h->stream, h->sm_count));
+  return MPDG_OK;
+}
+
+static int poll(mpdg_heat *h)
+{
+  CU(cudaMemcpyAsync(h->st_host, h->st, sizeof(SolverState), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return MPDG_OK;
+}
+
+static int norms(mpdg_heat *h, const double *a, const double *b, double *aa, double *ab)
+{
+  const int64_t N = h->n_dofs;
+  k_norms<<<vgrid(h, N), VT, 0, h->stream>>>(N, a, b, h->partials, h->counter, h->scal);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(h->scal_host, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  if (aa) *aa = h->scal_host[0];
+  if (ab) *ab = h->scal_host[1];
+  return MPDG_OK;
+}
+
+static int ensure_workspace(mpdg_heat *h)
+{
+  const int64_t N = h->n_dofs;
+  TRY(dvec(h, &h->r, N));
+  TRY(dvec(h, &h->pv, N));
+  TRY(dvec(h, &h->Ap, N));
+  return MPDG_OK;
+}
+
+static int ensure_workspace_f32(mpdg_heat *h)
+{
+  const int64_t N = h->n_dofs;
+  TRY(dvec(h, &h->z, N));
+  TRY(dvec(h, &h->r32, N));
+  TRY(dvec(h, &h->x32, N));
+  TRY(dvec(h, &h->d32, N));
+  TRY(dvec(h, &h->Ax32, N));
+  TRY(dvec(h, &h->inv_diag_f, N));
+  return MPDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CG (FP64, identity or Jacobi); record = Lanczos history for eigenvalues
+// ---------------------------------------------------------------------------
+static int cg_jacobi(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
+                     const double *D, int record, mpdg_solve_stats *stats)
+{
+  const int64_t N = h->n_dofs;
+  TRY(ensure_workspace(h));
+  const int g = vgrid(h, N);
+  CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+  TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+  k_cg_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->pv, h->Ap, D, h->st, h->partials, h->counter,
+                                      prm->rel_tolerance, prm->abs_tolerance,
+                                      prm->tol_reference_norm, prm->max_iterations, record);
+  CU(cudaGetLastError());
+  TRY(poll(h));
+  const double res0 = h->st_host->res0;
+  int chunk = 4;
+  while (!h->st_host->done) {
+    for (int c = 0; c < chunk; ++c) {
+      TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
+      k_cg_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, D, h->st, h->partials,
+                                              h->counter);
+      k_cg_update_p<<<g, VT, 0, h->stream>>>(N, h->r, h->pv, h->Ap, D, h->st);
+    }
+    CU(cudaGetLastError());
+    TRY(poll(h));
+    chunk = std::min(chunk * 2, 64);
+  }
+  if (stats) {
+    stats->iterations = h->st_host->it;
+    stats->status = h->st_host->done == 1 ? MPDG_OK : h->st_host->status;
+    stats->initial_residual = res0;
+    stats->final_residual = h->st_host->res;
+    stats->true_residual = h->st_host->res;
+  }
+  return MPDG_OK;
+}
+
+// Lanczos estimate of the extreme eigenvalues of D^-1 J
+static double tridiag_eig(int m, const double *d, const double *e, int which)
+{
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < m; ++i) {
+    const double r = (i > 0 ? std::fabs(e[i - 1]) : 0.0) + (i < m - 1 ? std::fabs(e[i]) : 0.0);
+    lo = std::min(lo, d[i] - r);
+    hi = std::max(hi, d[i] + r);
+  }
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    int cnt = 0;
+    double q = d[0] - mid;
+    if (q < 0) ++cnt;
+    for (int i = 1; i < m; ++i) {
+      if (q == 0.0) q = 1e-300;
+      q = d[i] - mid - e[i - 1] * e[i - 1] / q;
+      if (q < 0) ++cnt;
+    }
+    if (cnt > which)
+      hi = mid;
+    else
+      lo = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+static int estimate_eigenvalues(mpdg_heat *h, int n_it, double *lmin, double *lmax)
+{
+  const int64_t N = h->n_dofs;
+  n_it = std::max(2, std::min(n_it, 64));
+  TRY(dvec(h, &h->w3, N));
+  TRY(dvec(h, &h->z, N));
+  k_masked_random<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, h->w3);
+  CU(cudaMemsetAsync(h->z, 0, sizeof(double) * N, h->stream));
+  mpdg_solver_params prm;
+  mpdg_solver_params_default(&prm);
+  prm.max_iterations = n_it;
+  prm.rel_tolerance = 0.0;
+  prm.abs_tolerance = 0.0;
+  TRY(cg_jacobi(h, &prm, h->z, h->w3, h->inv_diag, 1, nullptr));
+  const SolverState &s = *h->st_host;
+  const int m = std::min(s.it, 64);
+  if (m < 1) {
+    *lmin = *lmax = 1.0;
+    return MPDG_OK;
+  }
+  std::vector<double> d(m), e(m, 0.0);
+  for (int j = 0; j < m; ++j) {
+    d[j] = 1.0 / s.hist_alpha[j] + (j > 0 ? s.hist_beta[j - 1] / s.hist_alpha[j - 1] : 0.0);
+    if (j + 1 < m) e[j] = std::sqrt(s.hist_beta[j]) / s.hist_alpha[j];
+  }
+  *lmin = tridiag_eig(m, d.data(), e.data(), 0);
+  *lmax = tridiag_eig(m, d.data(), e.data(), m - 1);
+  return MPDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 flexible CG with the FP32 Chebyshev-Jacobi preconditioner
+// ---------------------------------------------------------------------------
+static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
+                        mpdg_solve_stats *stats)
+{
+  const int64_t N = h->n_dofs;
+  if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
+  if (prm->cheb_degree < 1) return fail(MPDG_ERR_INVALID_ARGUMENT, "cheb_degree < 1");
+  TRY(ensure_workspace(h));
+  TRY(ensure_workspace_f32(h));
+  TRY(refresh_f32(h));
+  if (h->diag_f_dirty) {
+    k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->inv_diag, h->inv_diag_f);
+    CU(cudaGetLastError());
+    h->diag_f_dirty = false;
+  }
+  if (!h->eig_valid) {
+    TRY(estimate_eigenvalues(h, prm->cheb_eig_iterations, &h->eig_min, &h->eig_max));
+    h->eig_valid = true;
+  }
+  const double bmax = prm->cheb_max_factor * h->eig_max;
+  const double amin = std::max(h->eig_min, prm->cheb_min_fraction * bmax);
+  const double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin), sigma = theta / delta;
+  const int k = prm->cheb_degree;
+  std::vector<float> c1(k + 1), c2(k + 1);
+  {
+    double rho0 = 1.0 / sigma;
+    for (int j = 1; j <= k; ++j) {
+      const double rho1 = 1.0 / (2.0 * sigma - rho0);
+      c1[j] = (float)(rho1 * rho0);
+      c2[j] = (float)(2.0 * rho1 / delta);
+      rho0 = rho1;
+    }
+  }
+  const float inv_theta = (float)(1.0 / theta);
+  const int g = vgrid(h, N);
+  int total_it = 0, restarts = 0;
+  double res0 = -1.0, true_res = 0.0;
+  for (;;) {
+    CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+    TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+    k_cgm_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->Ap, h->r32, h->x32, h->d32, h->Ax32,
+                                        h->inv_diag_f, inv_theta, h->st, h->partials, h->counter,
+                                        prm->rel_tolerance, prm->abs_tolerance,
+                                        res0 > 0.0 && prm->tol_reference_norm <= 0.0
+                                          ? res0
+                                          : prm->tol_reference_norm,
+                                        prm->max_iterations - total_it);
+    CU(cudaGetLastError());
+    TRY(poll(h));
+    if (res0 < 0.0) res0 = h->st_host->res0;
+    auto precondition = [&]() -> int {
+      for (int j = 1; j <= k; ++j) {
+        TRY(op_apply_f(h, h->Ax32, h->x32, h->st));
+        if (j < k)
+          k_cheb_step<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
+                                               c1[j], c2[j], h->st);
+        else
+          k_cheb_last<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
+                                               c1[j], c2[j], h->r, h->Ap, h->z, h->st,
+                                               h->partials, h->counter);
+      }
+      k_cgm_update_p<<<g, VT, 0, h->stream>>>(N, h->z, h->pv, h->Ap, h->st);
+      CU(cudaGetLastError());
+      return MPDG_OK;
+    };
+    if (!h->st_host->done) TRY(precondition());
+    int chunk = 2;
+    while (!h->st_host->done) {
+      for (int c = 0; c < chunk; ++c) {
+        TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
+        k_cgm_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, h->r32, h->x32, h->d32,
+                                                 h->inv_diag_f, inv_theta, h->st, h->partials,
+                                                 h->counter);
+        TRY(precondition());
+      }
+      TRY(poll(h));
+      chunk = std::min(chunk * 2, 16);
+    }
+    total_it += h->st_host->it;
+    const int done = h->st_host->done, status = h->st_host->status;
+    const double tol = h->st_host->tol;
+    // true residual recheck in FP64
+    CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+    TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+    TRY(dvec(h, &h->w3, N));
+    CU(cudaMemcpyAsync(h->w3, b, sizeof(double) * N, cudaMemcpyDeviceToDevice, h->stream));
+    k_axpy<<<g, VT, 0, h->stream>>>(N, h->w3, -1.0, h->Ap);
+    double rr = 0.0;
+    TRY(norms(h, h->w3, nullptr, &rr, nullptr));
+    true_res = std::sqrt(rr);
+    if (done == 1 && true_res > tol && total_it < prm->max_iterations && restarts < 5) {
+      ++restarts;
+      continue;
+    }
+    if (stats) {
+      stats->iterations = total_it;
+      stats->status = (done == 1 && true_res <= tol * 1.0000001) ? MPDG_OK
+                      : (done == 1 ? MPDG_ERR_NOT_CONVERGED : status);
+      stats->initial_residual = res0;
+      stats->final_residual = h->st_host->res;
+      stats->true_residual = true_res;
+      stats->lambda_min = amin;
+      stats->lambda_max = bmax;
+    }
+    return MPDG_OK;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" void mpdg_solver_params_default(mpdg_solver_params *p)
+{
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->solver = MPDG_SOLVER_CG;
+  p->preconditioner = MPDG_PRECOND_JACOBI;
+  p->max_iterations = 10000;
+  p->rel_tolerance = 1e-12;
+  p->abs_tolerance = 1e-20;
+  p->gmres_restart = 28;
+  p->cheb_degree = 4;
+  p->cheb_eig_iterations = 12;
+  p->cheb_max_factor = 1.2;
+  p->cheb_min_fraction = 0.0;
+  p->tol_reference_norm = 0.0;
+}
+
+extern "C" void mpdg_step_params_default(mpdg_step_params *p)
+{
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->newton_max_iterations = 10;
+  p->newton_residual_tolerance = 1e-9;
+  p->newton_correction_tolerance = 1e-10;
+  p->predictor = MPDG_PREDICTOR_LINEAR;
+  p->single_linearization = 0;
+  mpdg_solver_params_default(&p->linear);
+}
+
+static void release(mpdg_heat *h)
+{
+  for (void *p : h->owned) cudaFree(p);
+  h->owned.clear();
+  if (h->st_host) cudaFreeHost(h->st_host);
+  if (h->scal_host) cudaFreeHost(h->scal_host);
+  h->st_host = nullptr;
+  h->scal_host = nullptr;
+}
+
+extern "C" int mpdg_heat_create(const mpdg_mesh_desc *desc, int device, mpdg_heat **out)
+{
+  if (!desc || !out) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (desc->degree < 1 || desc->degree > 6)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "degree must be in 1..6");
+  for (int e = 0; e < 3; ++e) {
+    if (desc->cells[e] < 1) return fail(MPDG_ERR_INVALID_ARGUMENT, "cells must be >= 1");
+    if (!(desc->hi[e] > desc->lo[e])) return fail(MPDG_ERR_INVALID_ARGUMENT, "empty box");
+  }
+  if (desc->perturb < 0.0 || desc->perturb >= 0.5)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "perturb must be in [0, 0.5)");
+  const int64_t nd0 = (int64_t)desc->degree * desc->cells[0] + 1,
+                nd1 = (int64_t)desc->degree * desc->cells[1] + 1,
+                nd2 = (int64_t)desc->degree * desc->cells[2] + 1;
+  if (nd0 > (1 << 30) || nd1 > (1 << 30) || nd2 > (1 << 30))
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "mesh too large");
+  CU(cudaSetDevice(device));
+  mpdg_heat *h = new mpdg_heat();
+  h->device = device;
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+  h->desc = *desc;
+  h->p = desc->degree;
+  h->n = h->p + 1;
+  h->npt = h->n * h->n * h->n;
+  for (int e = 0; e < 3; ++e) {
+    h->dims.m[e] = desc->cells[e];
+    h->dims.nd[e] = h->p * desc->cells[e] + 1;
+    h->hcell[e] = (desc->hi[e] - desc->lo[e]) / desc->cells[e];
+  }
+  h->dims.p = h->p;
+  h->dims.dmask = desc->dirichlet_mask & 63;
+  h->n_dofs = nd0 * nd1 * nd2;
+  h->n_cells = (int64_t)desc->cells[0] * desc->cells[1] * desc->cells[2];
+  h->geo = desc->perturb > 0.0 ? 1 : 0;
+  h->tab = table_for(h->n);
+  int rc = upload_tables(device, h->n);
+  if (rc != MPDG_OK) {
+    delete h;
+    return rc;
+  }
+  auto cleanup = [&](int code) {
+    release(h);
+    delete h;
+    return code;
+  };
+  if ((rc = dalloc(h, (void **)&h->partials, sizeof(double) * 4 * kPartialsPerValue)) != MPDG_OK)
+    return cleanup(rc);
+  if ((rc = dalloc(h, (void **)&h->counter, sizeof(unsigned) * 4)) != MPDG_OK) return cleanup(rc);
+  if ((rc = dalloc(h, (void **)&h->st, sizeof(SolverState))) != MPDG_OK) return cleanup(rc);
+  if ((rc = dalloc(h, (void **)&h->scal, sizeof(double) * 8)) != MPDG_OK) return cleanup(rc);
+  if (cudaMallocHost((void **)&h->st_host, sizeof(SolverState)) != cudaSuccess ||
+      cudaMallocHost((void **)&h->scal_host, sizeof(double) * 8) != cudaSuccess)
+    return cleanup(fail(MPDG_ERR_OUT_OF_MEMORY, "cudaMallocHost"));
+  cudaMemset(h->counter, 0, sizeof(unsigned) * 4);
+  cudaMemset(h->st, 0, sizeof(SolverState));
+  memset(h->st_host, 0, sizeof(SolverState));
+  if (h->geo == 1) {
+    // vertices on the host (counter-hash perturbation of interior vertices), then
+    // per-quadrature-point geometry on the device
+    const int64_t nv = (int64_t)(desc->cells[0] + 1) * (desc->cells[1] + 1) * (desc->cells[2] + 1);
+    std::vector<double> vert(3 * nv);
+    for (int c = 0; c <= desc->cells[2]; ++c)
+      for (int b = 0; b <= desc->cells[1]; ++b)
+        for (int a = 0; a <= desc->cells[0]; ++a) {
+          const int idx[3] = {a, b, c};
+          const int64_t v = a + (int64_t)(desc->cells[0] + 1) * (b + (int64_t)(desc->cells[1] + 1) * c);
+          bool interior = true;
+          for (int e = 0; e < 3; ++e)
+            if (idx[e] == 0 || idx[e] == desc->cells[e]) interior = false;
+          for (int e = 0; e < 3; ++e) {
+            double x = desc->lo[e] + h->hcell[e] * idx[e];
+            if (interior) {
+              uint64_t r = desc->seed * 0xD1B54A32D192ED03ULL + (uint64_t)(3 * v + e);
+              r += 0x9E3779B97F4A7C15ULL;
+              r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ULL;
+              r = (r ^ (r >> 27)) * 0x94D049BB133111EBULL;
+              r ^= r >> 31;
+              const double u = 2.0 * ((double)(r >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+              x += desc->perturb * h->hcell[e] * u;
+            }
+            vert[3 * v + e] = x;
+          }
+        }
+    if ((rc = dvec(h, &h->vert, 3 * nv)) != MPDG_OK) return cleanup(rc);
+    if ((rc = dvec(h, &h->geoq, h->n_cells * 7 * h->npt)) != MPDG_OK) return cleanup(rc);
+    if (cudaMemcpy(h->vert, vert.data(), sizeof(double) * 3 * nv, cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return cleanup(fail(MPDG_ERR_CUDA, "vertex upload"));
+    const Tables1D t1 = make_tables(h->n);
+    Q1D q1;
+    for (int i = 0; i < h->n; ++i) {
+      q1.xg[i] = t1.xg[i];
+      q1.wg[i] = t1.wg[i];
+      q1.xl[i] = t1.xl[i];
+    }
+    const int64_t total = h->n_cells * h->npt;
+    k_geometry<<<vgrid(h, total), VT>>>(h->n_cells, h->dims, h->n, q1, h->vert, h->geoq);
+    if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(fail(MPDG_ERR_CUDA, "geometry"));
+  }
+  mpdg_material m0;
+  memset(&m0, 0, sizeof(m0));
+  m0.law = MPDG_LAW_CONSTANT;
+  m0.rho_l = m0.cp_l = m0.k_l = 1.0;
+  m0.rho_s = m0.cp_s = m0.k_s = 1.0;
+  m0.T_liquidus = 1.0;
+  h->mat = m0;
+  *out = h;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_destroy(mpdg_heat *h)
+{
+  if (!h) return MPDG_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  release(h);
+  delete h;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_stream(mpdg_heat *h, void *stream)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  h->stream = (cudaStream_t)stream;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_n_dofs(const mpdg_heat *h, int64_t *n)
+{
+  if (!h || !n) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  *n = h->n_dofs;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_n_cells(const mpdg_heat *h, int64_t *n)
+{
+  if (!h || !n) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  *n = h->n_cells;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_dof_dims(const mpdg_heat *h, int dims[3])
+{
+  if (!h || !dims) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  for (int e = 0; e < 3; ++e) dims[e] = h->dims.nd[e];
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_device_bytes(const mpdg_heat *h, int64_t *bytes)
+{
+  if (!h || !bytes) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  *bytes = h->bytes;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
+{
+  if (!h || !m) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (m->law < 0 || m->law > 2) return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown material law");
+  if (m->law == MPDG_LAW_LIQUID_SOLID && !m->sharp && !(m->T_liquidus > m->T_solidus))
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "liquidus must exceed solidus");
+  h->mat = *m;
+  h->law = m->law;
+  h->need_told = 0;
+  if (m->law == MPDG_LAW_LIQUID_SOLID)
+    h->need_told = m->volume_specific ? (m->rho_l * m->cp_l != m->rho_s * m->cp_s)
+                                      : (m->rho_l != m->rho_s || m->cp_l != m->cp_s);
+  h->diag_valid = false;
+  h->eig_valid = false;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_reset_time_increment(mpdg_heat *h, double dt)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  h->dt = dt;
+  h->eig_valid = false;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_linearization(mpdg_heat *h, const double *T, const double *T_old)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  h->T_lin = T;
+  h->T_old = T_old;
+  h->lin_f_dirty = true;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_vmult(mpdg_heat *h, double *dst, const double *src)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  CU(cudaMemsetAsync(dst, 0, sizeof(double) * h->n_dofs, h->stream));
+  return op_apply_d(h, dst, src, FIN_NONE, nullptr, nullptr);
+}
+
+extern "C" int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  CU(cudaMemsetAsync(dst, 0, sizeof(float) * h->n_dofs, h->stream));
+  return op_apply_f(h, dst, src, nullptr);
+}
+
+static int compute_diag(mpdg_heat *h, double *d)
+{
+  TRY(ensure_dt(h));
+  TRY(ensure_lin(h));
+  CU(cudaMemsetAsync(d, 0, sizeof(double) * h->n_dofs, h->stream));
+  CellArgs<double> a = cell_args<double>(h);
+  a.g.q = h->geoq;
+  a.dst = d;
+  a.Tl = h->T_lin;
+  a.To = h->T_old;
+  CU(h->tab.diag(a, h->geo, h->law, h->stream, h->sm_count));
+  k_invert_diag<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, d);
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_compute_inverse_diagonal(mpdg_heat *h, double *inv_diag)
+{
+  if (!h || !inv_diag) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  return compute_diag(h, inv_diag);
+}
+
+static int create_rhs(mpdg_heat *h, double *dst, const double *src, const double *q)
+{
+  TRY(ensure_dt(h));
+  if (!h->T_lin) return fail(MPDG_ERR_INVALID_ARGUMENT, "create_rhs needs set_linearization");
+  CellArgs<double> a = cell_args<double>(h);
+  a.g.q = h->geoq;
+  a.dst = dst;
+  a.Tl = h->T_lin;
+  a.To = src;
+  a.qs = q;
+  CU(h->tab.rhs(a, h->geo, h->law, h->stream, h->sm_count));
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_create_rhs(mpdg_heat *h, double *dst, const double *src,
+                                    const double *heat_source)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  return create_rhs(h, dst, src, heat_source);
+}
+
+static int distribute(mpdg_heat *h, double *u)
+{
+  DirArgs a;
+  a.d = h->dims;
+  for (int f = 0; f < 6; ++f) a.val[f] = h->desc.dirichlet_value[f];
+  for (int f = 0; f < 6; ++f) {
+    if (!(h->dims.dmask & (1 << f))) continue;
+    const int dir = f / 2;
+    const int e1 = dir == 0 ? 1 : 0, e2 = dir == 2 ? 1 : 2;
+    const int64_t cnt = (int64_t)h->dims.nd[e1] * h->dims.nd[e2];
+    k_distribute<<<vgrid(h, cnt), VT, 0, h->stream>>>(a, f, u);
+  }
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_distribute_constraints(mpdg_heat *h, double *u)
+{
+  if (!h || !u) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  return distribute(h, u);
+}
+
+extern "C" int mpdg_heat_l2_norm(mpdg_heat *h, const double *u, double *norm)
+{
+  if (!h || !u || !norm) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  CellArgs<double> a = cell_args<double>(h);
+  a.g.q = h->geoq;
+  a.src = u;
+  a.out = h->scal;
+  CU(h->tab.norm(a, h->geo, 0, h->stream, h->sm_count));
+  CU(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  *norm = std::sqrt(h->scal_host[0]);
+  return MPDG_OK;
+}
+
+static PosArgs pos_args(const mpdg_heat *h)
+{
+  PosArgs a;
+  a.d = h->dims;
+  a.geo = h->geo;
+  for (int e = 0; e < 3; ++e) {
+    a.lo[e] = h->desc.lo[e];
+    a.hc[e] = h->hcell[e];
+  }
+  const Tables1D t1 = make_tables(h->n);
+  for (int i = 0; i < h->n; ++i) {
+    a.q1.xg[i] = t1.xg[i];
+    a.q1.wg[i] = t1.wg[i];
+    a.q1.xl[i] = t1.xl[i];
+  }
+  a.vert = h->vert;
+  return a;
+}
+
+extern "C" int mpdg_heat_support_points(mpdg_heat *h, double *xyz)
+{
+  if (!h || !xyz) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  k_support_points<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), xyz);
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_gaussian_source(mpdg_heat *h, double *q, double amplitude,
+                                         const double center[3], double radius)
+{
+  if (!h || !q || !center || !(radius > 0.0)) return fail(MPDG_ERR_INVALID_ARGUMENT, "bad argument");
+  CU(cudaSetDevice(h->device));
+  k_gaussian<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), q, amplitude,
+                                                        center[0], center[1], center[2],
+                                                        1.0 / (radius * radius));
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_preconditioner_update(mpdg_heat *h)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  CU(cudaSetDevice(h->device));
+  TRY(dvec(h, &h->inv_diag, h->n_dofs));
+  TRY(compute_diag(h, h->inv_diag));
+  h->diag_valid = true;
+  h->diag_f_dirty = true;
+  h->eig_valid = false;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_preconditioner_vmult(mpdg_heat *h, double *dst, const double *src)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
+  CU(cudaSetDevice(h->device));
+  k_scale<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, dst, src, h->inv_diag);
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+static int linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
+                        mpdg_solve_stats *stats)
+{
+  mpdg_solve_stats local;
+  memset(&local, 0, sizeof(local));
+  if (prm->solver != MPDG_SOLVER_CG)
+    return fail(MPDG_ERR_NOT_SUPPORTED, "only CG is available on the device path");
+  if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32) {
+    TRY(cg_chebyshev(h, prm, x, b, &local));
+  } else {
+    const double *D = nullptr;
+    if (prm->preconditioner == MPDG_PRECOND_JACOBI) {
+      if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
+      D = h->inv_diag;
+    }
+    TRY(cg_jacobi(h, prm, x, b, D, 0, &local));
+  }
+  if (stats) *stats = local;
+  if (local.status != MPDG_OK)
+    return fail(local.status, local.status == MPDG_ERR_NOT_CONVERGED
+                                ? "linear solver did not converge"
+                                : (local.status == MPDG_ERR_NAN ? "residual is not finite"
+                                                                : "solver breakdown"));
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x,
+                                      const double *b, mpdg_solve_stats *stats)
+{
+  if (!h || !prm || !x || !b) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  return linear_solve(h, prm, x, b, stats);
+}
+
+extern "C" int mpdg_heat_set_guess(mpdg_heat *h, const double *guess)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  h->guess = guess;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, double dt,
+                                   double dt_old, double *T_cur, double *T_old,
+                                   const double *heat_source, mpdg_step_stats *stats)
+{
+  if (!h || !prm || !T_cur || !T_old) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (prm->predictor == MPDG_PREDICTOR_GIVEN && !h->guess)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "predictor GIVEN needs mpdg_heat_set_guess");
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  const size_t vb = sizeof(double) * N;
+  TRY(dvec(h, &h->w1, N));
+  TRY(dvec(h, &h->w2, N));
+  TRY(dvec(h, &h->z, N));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  CU(cudaEventRecord(e0, h->stream));
+  mpdg_step_stats s;
+  memset(&s, 0, sizeof(s));
+  int rc = MPDG_OK;
+  do {
+    h->dt = dt;
+    h->eig_valid = false;
+    // init_time_advance: predictor into w1, commit history, constraints
+    if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
+      k_predict<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, h->w1, dt / dt_old);
+    } else if (prm->predictor == MPDG_PREDICTOR_GIVEN) {
+      if ((rc = (cudaMemcpyAsync(h->w1, h->guess, vb, cudaMemcpyDeviceToDevice, h->stream) ==
+                 cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, "guess copy"))) != MPDG_OK) break;
+    } else {
+      if ((rc = (cudaMemcpyAsync(h->w1, T_cur, vb, cudaMemcpyDeviceToDevice, h->stream) ==
+                 cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, "copy"))) != MPDG_OK) break;
+    }
+    cudaMemcpyAsync(T_old, T_cur, vb, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(T_cur, h->w1, vb, cudaMemcpyDeviceToDevice, h->stream);
+    if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
+    h->T_lin = T_cur;
+    h->T_old = T_old;
+    h->lin_f_dirty = true;
+    if (prm->linear.preconditioner != MPDG_PRECOND_IDENTITY) {
+      if ((rc = dvec(h, &h->inv_diag, N)) != MPDG_OK) break;
+      if ((rc = compute_diag(h, h->inv_diag)) != MPDG_OK) break;
+      h->diag_valid = true;
+      h->diag_f_dirty = true;
+    }
+    if (prm->single_linearization) {
+      // b = J T_g - R(T_g); solve J delta = -R(T_g) to |b - J T| <= tol |b|
+      cudaMemsetAsync(h->w2, 0, vb, h->stream);
+      if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
+      cudaMemsetAsync(h->z, 0, vb, h->stream);
+      if ((rc = op_apply_d(h, h->z, T_cur, FIN_NONE, nullptr, nullptr)) != MPDG_OK) break;
+      double rr = 0.0, bb = 0.0;
+      if ((rc = norms(h, h->w2, h->z, &rr, &bb)) != MPDG_OK) break;
+      mpdg_solver_params lp = prm->linear;
+      lp.tol_reference_norm = std::sqrt(bb);
+      lp.abs_tolerance = std::max(lp.abs_tolerance, 0.0);
+      cudaMemsetAsync(h->w1, 0, vb, h->stream);
+      mpdg_solve_stats ls;
+      memset(&ls, 0, sizeof(ls));
+      if ((rc = linear_solve(h, &lp, h->w1, h->w2, &ls)) != MPDG_OK) break;
+      k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1);
+      if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
+      s.linear_iterations = ls.iterations;
+      s.newton_iterations = 1;
+      s.converged = 1;
+      s.initial_relative_residual = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+    } else {
+      for (int i = 0; i < prm->newton_max_iterations; ++i) {
+        cudaMemsetAsync(h->w2, 0, vb, h->stream);
+        if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
+        cudaMemsetAsync(h->w1, 0, vb, h->stream);
+        mpdg_solve_stats ls;
+        memset(&ls, 0, sizeof(ls));
+        if ((rc = linear_solve(h, &prm->linear, h->w1, h->w2, &ls)) != MPDG_OK) break;
+        s.linear_iterations += ls.iterations;
+        double rr = 0.0, dd = 0.0;
+        if ((rc = norms(h, h->w2, nullptr, &rr, nullptr)) != MPDG_OK) break;
+        if ((rc = norms(h, h->w1, nullptr, &dd, nullptr)) != MPDG_OK) break;
+        if (std::sqrt(rr) < prm->newton_residual_tolerance &&
+            std::sqrt(dd) < prm->newton_correction_tolerance) {
+          s.converged = 1;
+          break;
+        }
+        k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1);
+        if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
+        h->lin_f_dirty = true;
+        s.newton_iterations = i + 1;
+      }
+      if (rc == MPDG_OK && !s.converged)
+        rc = fail(MPDG_ERR_NEWTON_NOT_CONVERGED, "Newton-Raphson did not converge");
+    }
+  } while (0);
+  cudaEventRecord(e1, h->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s.step_ms = ms;
+  if (stats) *stats = s;
+  if (rc == MPDG_OK) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return rc;
+}
+
+extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *prm, double dt,
+                                        double dt_old, double *T_cur, double *T_old,
+                                        const double *heat_source, mpdg_step_stats *stats)
+{
+  if (!h || !prm || !T_cur || !T_old) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  const size_t vb = sizeof(double) * N;
+  TRY(dvec(h, &h->host_T, N));
+  TRY(dvec(h, &h->host_To, N));
+  if (heat_source) TRY(dvec(h, &h->host_q, N));
+  CU(cudaMemcpyAsync(h->host_T, T_cur, vb, cudaMemcpyHostToDevice, h->stream));
+  CU(cudaMemcpyAsync(h->host_To, T_old, vb, cudaMemcpyHostToDevice, h->stream));
+  if (heat_source) CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->stream));
+  TRY(mpdg_heat_time_step(h, prm, dt, dt_old, h->host_T, h->host_To, heat_source ? h->host_q : nullptr,
+                          stats));
+  CU(cudaMemcpyAsync(T_cur, h->host_T, vb, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(T_old, h->host_To, vb, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return MPDG_OK;
+}

@@ -1,0 +1,341 @@
+"""Python mirror of MeltPoolDG's heat-operator interface over the C ABI.
+
+Names, argument meaning and error behaviour follow the reference:
+  HeatDiffuseOperator   HeatDiffuseMultiPhaseOperator / OperatorMatrixFree verbs
+                        (include/meltpooldg/core/operator_base.hpp:188-282)
+  JacobiPreconditioner  include/meltpooldg/linear_algebra/preconditioner_jacobi.hpp
+  LinearSolver.solve    include/meltpooldg/linear_algebra/linear_solver.hpp:22-134
+  HeatDiffuseOperation  source/heat/heat_diffuse_operation.cpp (init_time_advance + solve)
+Vectors are torch CUDA tensors (float64, or float32 for the FP32 operator) of
+length n_dofs; all work runs on the CUDA library (libmpdg_heat.so), there is no
+CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib as L
+
+
+# ---------------------------------------------------------------------------
+# exceptions (deal.II / MeltPoolDG exception names)
+# ---------------------------------------------------------------------------
+class MpdgError(RuntimeError):
+    code = -1
+
+
+class ExcInvalidArgument(MpdgError, ValueError):
+    code = L.ERR_INVALID_ARGUMENT
+
+
+class ExcOutOfMemory(MpdgError, MemoryError):
+    code = L.ERR_OUT_OF_MEMORY
+
+
+class ExcNoConvergence(MpdgError):
+    """dealii::SolverControl::NoConvergence."""
+    code = L.ERR_NOT_CONVERGED
+
+
+class ExcNaN(ExcNoConvergence):
+    code = L.ERR_NAN
+
+
+class ExcBreakdown(ExcNoConvergence):
+    code = L.ERR_BREAKDOWN
+
+
+class ExcCuda(MpdgError):
+    code = L.ERR_CUDA
+
+
+class ExcZeroTimeIncrement(MpdgError):
+    """AssertThrowZeroTimeIncrement (include/meltpooldg/core/exceptions.hpp:6)."""
+    code = L.ERR_ZERO_TIME_INCREMENT
+
+
+class ExcHeatTransferNoConvergence(MpdgError):
+    """ExcNewtonDidNotConverge -> ExcHeatTransferNoConvergence (exceptions.hpp:25-26)."""
+    code = L.ERR_NEWTON_NOT_CONVERGED
+
+
+class ExcNotImplemented(MpdgError, NotImplementedError):
+    code = L.ERR_NOT_SUPPORTED
+
+
+_EXC = {c.code: c for c in (ExcInvalidArgument, ExcOutOfMemory, ExcNoConvergence, ExcNaN,
+                             ExcBreakdown, ExcCuda, ExcZeroTimeIncrement,
+                             ExcHeatTransferNoConvergence, ExcNotImplemented)}
+
+
+def check(rc: int):
+    if rc != L.OK:
+        raise _EXC.get(rc, MpdgError)(f"[{rc}] {L.last_error()}")
+
+
+# ---------------------------------------------------------------------------
+# descriptions
+# ---------------------------------------------------------------------------
+FACES = {"x-": 0, "x+": 1, "y-": 2, "y+": 3, "z-": 4, "z+": 5}
+
+
+def box_mesh(degree, cells, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), perturb=0.0, seed=1,
+             dirichlet=("x-", "x+", "y-", "y+", "z-", "z+"), dirichlet_values=None) -> L.MeshDesc:
+    """Structured FE_Q(degree) box mesh; `dirichlet` lists constrained faces."""
+    d = L.MeshDesc()
+    d.degree = int(degree)
+    for i in range(3):
+        d.cells[i] = int(cells[i])
+        d.lo[i] = float(lo[i])
+        d.hi[i] = float(hi[i])
+    d.perturb = float(perturb)
+    d.seed = int(seed)
+    mask = 0
+    for f in dirichlet:
+        mask |= 1 << (FACES[f] if isinstance(f, str) else int(f))
+    d.dirichlet_mask = mask
+    vals = dirichlet_values or {}
+    for f, v in (vals.items() if isinstance(vals, dict) else enumerate(vals)):
+        d.dirichlet_value[FACES[f] if isinstance(f, str) else int(f)] = float(v)
+    return d
+
+
+def material(law=L.LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_s=None, k_s=None,
+             T_solidus=0.0, T_liquidus=1.0, sharp=False, volume_specific=False) -> L.Material:
+    m = L.Material()
+    m.law = int(law)
+    m.sharp = int(sharp)
+    m.volume_specific = int(volume_specific)
+    m.rho_l, m.cp_l, m.k_l = float(rho), float(cp), float(k)
+    m.rho_s = float(rho if rho_s is None else rho_s)
+    m.cp_s = float(cp if cp_s is None else cp_s)
+    m.k_s = float(k if k_s is None else k_s)
+    m.T_solidus, m.T_liquidus, m.k1 = float(T_solidus), float(T_liquidus), float(k1)
+    return m
+
+
+@dataclass
+class LinearSolverData:
+    """LinearSolverData (linear_solver_data.hpp:40-47) plus the Chebyshev options."""
+    solver_type: int = L.SOLVER_CG
+    preconditioner_type: int = L.PRECOND_JACOBI
+    max_iterations: int = 10000
+    rel_tolerance: float = 1e-12
+    abs_tolerance: float = 1e-20
+    gmres_restart: int = 28
+    cheb_degree: int = 4
+    cheb_eig_iterations: int = 12
+    cheb_max_factor: float = 1.2
+    cheb_min_fraction: float = 0.0
+    tol_reference_norm: float = 0.0
+
+    def to_c(self) -> L.SolverParams:
+        return L.SolverParams(self.solver_type, self.preconditioner_type, self.max_iterations,
+                              self.rel_tolerance, self.abs_tolerance, self.gmres_restart,
+                              self.cheb_degree, self.cheb_eig_iterations, self.cheb_max_factor,
+                              self.cheb_min_fraction, self.tol_reference_norm)
+
+
+@dataclass
+class NonlinearSolverData:
+    """NonlinearSolverData (nonlinear_solver_data.hpp:13-19)."""
+    max_nonlinear_iterations: int = 10
+    residual_tolerance: float = 1e-9
+    field_correction_tolerance: float = 1e-10
+
+
+def _ptr(t: torch.Tensor | None, dtype=torch.float64):
+    if t is None:
+        return None
+    if not t.is_cuda or t.dtype != dtype or not t.is_contiguous():
+        raise ExcInvalidArgument(f"expected a contiguous CUDA {dtype} tensor, got "
+                                 f"{t.dtype} on {t.device}")
+    return t.data_ptr()
+
+
+# ---------------------------------------------------------------------------
+# operator
+# ---------------------------------------------------------------------------
+class HeatDiffuseOperator:
+    """Matrix-free heat tangent operator on one GPU (OperatorMatrixFree verbs)."""
+
+    def __init__(self, mesh: L.MeshDesc, device: int = 0):
+        self._L = L.load()
+        self.mesh = mesh
+        self.device = torch.device("cuda", device)
+        h = C.c_void_p()
+        check(self._L.mpdg_heat_create(C.byref(mesh), device, C.byref(h)))
+        self.h = h
+        n = C.c_int64()
+        check(self._L.mpdg_heat_n_dofs(h, C.byref(n)))
+        self.n_dofs = int(n.value)
+        check(self._L.mpdg_heat_n_cells(h, C.byref(n)))
+        self.n_cells = int(n.value)
+        dims = (C.c_int * 3)()
+        check(self._L.mpdg_heat_dof_dims(h, dims))
+        self.dims = tuple(dims)
+        self.degree = mesh.degree
+        self._refs = ()
+        self.sync_stream()
+
+    def sync_stream(self):
+        """Enqueue subsequent work on torch's current stream of this device."""
+        with torch.cuda.device(self.device):
+            s = torch.cuda.current_stream().cuda_stream
+        check(self._L.mpdg_heat_set_stream(self.h, C.c_void_p(s)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self._L.mpdg_heat_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def new_vector(self, dtype=torch.float64):
+        return torch.zeros(self.n_dofs, dtype=dtype, device=self.device)
+
+    def device_bytes(self) -> int:
+        n = C.c_int64()
+        check(self._L.mpdg_heat_device_bytes(self.h, C.byref(n)))
+        return int(n.value)
+
+    # coefficients ---------------------------------------------------------
+    def set_material(self, m: L.Material):
+        check(self._L.mpdg_heat_set_material(self.h, C.byref(m)))
+
+    def reset_time_increment(self, dt: float):
+        check(self._L.mpdg_heat_reset_time_increment(self.h, float(dt)))
+
+    def set_linearization(self, temperature, temperature_old=None):
+        self._refs = (temperature, temperature_old)
+        check(self._L.mpdg_heat_set_linearization(self.h, _ptr(temperature),
+                                                   _ptr(temperature_old)))
+
+    # verbs ------------------------------------------------------------------
+    def vmult(self, dst, src):
+        if src.dtype == torch.float32:
+            check(self._L.mpdg_heat_vmult_f32(self.h, _ptr(dst, torch.float32),
+                                               _ptr(src, torch.float32)))
+        else:
+            check(self._L.mpdg_heat_vmult(self.h, _ptr(dst), _ptr(src)))
+        return dst
+
+    def compute_inverse_diagonal_from_matrixfree(self, diag):
+        check(self._L.mpdg_heat_compute_inverse_diagonal(self.h, _ptr(diag)))
+        return diag
+
+    def create_rhs(self, dst, src, heat_source=None):
+        check(self._L.mpdg_heat_create_rhs(self.h, _ptr(dst), _ptr(src), _ptr(heat_source)))
+        return dst
+
+    def distribute_constraints(self, u):
+        check(self._L.mpdg_heat_distribute_constraints(self.h, _ptr(u)))
+        return u
+
+    def l2_norm(self, u) -> float:
+        v = C.c_double()
+        check(self._L.mpdg_heat_l2_norm(self.h, _ptr(u), C.byref(v)))
+        return float(v.value)
+
+    def support_points(self):
+        x = torch.empty((self.n_dofs, 3), dtype=torch.float64, device=self.device)
+        check(self._L.mpdg_heat_support_points(self.h, x.data_ptr()))
+        return x
+
+    def gaussian_source(self, q, amplitude, center, radius):
+        c = (C.c_double * 3)(*[float(v) for v in center])
+        check(self._L.mpdg_heat_gaussian_source(self.h, _ptr(q), float(amplitude), c,
+                                                 float(radius)))
+        return q
+
+
+class JacobiPreconditioner:
+    """JacobiPreconditioner: update() stores inv diag(J) in the handle; vmult scales."""
+
+    def __init__(self, op: HeatDiffuseOperator):
+        self.op = op
+
+    def update(self, *_):
+        check(self.op._L.mpdg_heat_preconditioner_update(self.op.h))
+
+    def vmult(self, dst, src):
+        check(self.op._L.mpdg_heat_preconditioner_vmult(self.op.h, _ptr(dst), _ptr(src)))
+        return dst
+
+    def reinit(self):
+        pass
+
+
+class LinearSolver:
+    last_stats: L.SolveStats | None = None
+
+    @staticmethod
+    def solve(op: HeatDiffuseOperator, solution, rhs, data: LinearSolverData = None,
+              preconditioner=None) -> int:
+        """Solve J x = b from the guess in `solution`; returns the iteration count and
+        raises ExcNoConvergence like dealii::SolverControl::NoConvergence."""
+        data = data or LinearSolverData()
+        if preconditioner is None and data.preconditioner_type != L.PRECOND_IDENTITY:
+            data = LinearSolverData(**{**data.__dict__, "preconditioner_type": L.PRECOND_IDENTITY})
+        prm = data.to_c()
+        st = L.SolveStats()
+        rc = op._L.mpdg_heat_linear_solve(op.h, C.byref(prm), _ptr(solution), _ptr(rhs),
+                                          C.byref(st))
+        LinearSolver.last_stats = st
+        check(rc)
+        return int(st.iterations)
+
+
+def step_params(linear: LinearSolverData = None, nonlinear: NonlinearSolverData = None,
+                predictor=L.PREDICTOR_LINEAR, single_linearization=False) -> L.StepParams:
+    linear = linear or LinearSolverData()
+    nonlinear = nonlinear or NonlinearSolverData()
+    p = L.StepParams()
+    p.newton_max_iterations = nonlinear.max_nonlinear_iterations
+    p.newton_residual_tolerance = nonlinear.residual_tolerance
+    p.newton_correction_tolerance = nonlinear.field_correction_tolerance
+    p.predictor = int(predictor)
+    p.single_linearization = int(bool(single_linearization))
+    p.linear = linear.to_c()
+    return p
+
+
+class HeatDiffuseOperation:
+    """HeatDiffuseOperation: owns the solution history on the device and advances it.
+
+    solve(dt) = init_time_advance (predictor, history commit, constraints) +
+    preconditioner update + Newton-Raphson (heat_diffuse_operation.cpp:213-289).
+    """
+
+    def __init__(self, op: HeatDiffuseOperator, linear: LinearSolverData = None,
+                 nonlinear: NonlinearSolverData = None, predictor=L.PREDICTOR_LINEAR,
+                 single_linearization=False):
+        self.op = op
+        self.params = step_params(linear, nonlinear, predictor, single_linearization)
+        self.T = op.new_vector()
+        self.T_old = op.new_vector()
+        self.heat_source = None
+        self.dt_old = 0.0
+        self.last_stats = None
+
+    def set_initial_condition(self, T0):
+        self.T.copy_(T0)
+        self.op.distribute_constraints(self.T)
+
+    def set_guess(self, guess):
+        check(self.op._L.mpdg_heat_set_guess(self.op.h, _ptr(guess)))
+        self._guess = guess
+
+    def solve(self, dt: float):
+        st = L.StepStats()
+        rc = self.op._L.mpdg_heat_time_step(self.op.h, C.byref(self.params), float(dt),
+                                            float(self.dt_old), _ptr(self.T), _ptr(self.T_old),
+                                            _ptr(self.heat_source), C.byref(st))
+        self.last_stats = st
+        check(rc)
+        self.dt_old = float(dt)
+        return st

@@ -1,0 +1,186 @@
+"""GPU parity of the operator verbs against the CPU oracle (same seeded inputs).
+
+Tolerances: FP64 verbs 1e-12 relative (max norm against max |oracle|); the FP32
+operator 2e-5 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+from meltpooldg_b200 import _lib as L
+from meltpooldg_b200 import heat as H
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+LAWS = {
+    "constant": dict(law=0, rho=1.0, cp=1.0, k=1.0),
+    "linear_k": dict(law=1, rho=1.0, cp=1.0, k=1.0, k1=0.5),
+    "liquid_solid": dict(law=2, rho=1000.0, cp=4226.0, k=0.556, rho_s=900.0, cp_s=1762.0,
+                         k_s=2.22, T_solidus=0.2, T_liquidus=0.8),
+}
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+
+def pair(degree, cells, perturb=0.0, law="constant", dt=1e-3, dirichlet=0x3F, lo=(0, 0, 0),
+         hi=(1, 1, 1), values=(0.0,) * 6, seed=3):
+    o = O.Oracle(degree, cells, lo=lo, hi=hi, perturb=perturb, seed=seed, dirichlet_mask=dirichlet,
+                 dirichlet_value=values)
+    o.set_material(O.material(**LAWS[law]), dt)
+    faces = [f for f in range(6) if dirichlet & (1 << f)]
+    g = H.HeatDiffuseOperator(H.box_mesh(degree, cells, lo, hi, perturb, seed, faces,
+                                         list(values)))
+    g.set_material(H.material(**LAWS[law]))
+    g.reset_time_increment(dt)
+    return o, g
+
+
+def cuda(a, dtype=torch.float64):
+    return torch.tensor(a, dtype=dtype, device="cuda")
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy().astype(np.float64) if isinstance(a, torch.Tensor) else a
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+@pytest.mark.parametrize("law", list(LAWS))
+def test_vmult_diag_rhs_match_oracle(degree, perturb, law):
+    cells = (5, 4, 3) if degree <= 4 else (3, 3, 2)
+    o, g = pair(degree, cells, perturb, law)
+    rng = np.random.default_rng(100 * degree + int(10 * perturb))
+    N = o.n_dofs
+    assert g.n_dofs == N and g.dims == o.dims
+    src = rng.uniform(-1, 1, N)
+    Tl = rng.uniform(0, 1, N)
+    To = rng.uniform(0, 1, N)
+    q = rng.uniform(0, 5, N)
+    Tl_d, To_d = cuda(Tl), cuda(To)
+    g.set_linearization(Tl_d, To_d)
+    # FP64 vmult
+    ref = o.vmult(src, Tl, To)
+    dst = g.new_vector()
+    g.vmult(dst, cuda(src))
+    assert rel(dst, ref) <= TOL64
+    # FP32 vmult (geometry, coefficients and linearisation point in FP32)
+    d32 = g.new_vector(torch.float32)
+    g.vmult(d32, cuda(src, torch.float32))
+    assert rel(d32, ref) <= TOL32 * (10 if degree >= 5 else 1)
+    # inverse diagonal
+    dref = o.inverse_diagonal(Tl, To)
+    dg = g.compute_inverse_diagonal_from_matrixfree(g.new_vector())
+    assert rel(1.0 / dg.cpu().numpy(), 1.0 / dref) <= TOL64
+    # create_rhs (dst is accumulated, not zeroed)
+    base = rng.uniform(-1, 1, N)
+    rref = o.create_rhs(Tl, To, q, dst=base.copy())
+    rg = cuda(base)
+    g.create_rhs(rg, To_d, cuda(q))
+    assert rel(rg, rref) <= TOL64
+    # L2 norm
+    assert abs(g.l2_norm(Tl_d) - o.l2_norm(Tl)) <= 1e-13 * o.l2_norm(Tl)
+
+
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+def test_geometry_support_points_and_constraints(perturb):
+    o, g = pair(3, (4, 3, 5), perturb, dirichlet=0b101101,
+                values=(1.0, 2.0, 0.0, 3.0, 4.0, 5.0))
+    x = g.support_points().cpu().numpy()
+    assert np.abs(x - o.support_points()).max() <= 1e-14
+    u = np.random.default_rng(1).uniform(size=o.n_dofs)
+    ud = cuda(u)
+    g.distribute_constraints(ud)
+    assert np.array_equal(ud.cpu().numpy(), o.distribute(u.copy()))
+    q = g.gaussian_source(g.new_vector(), 2.0, (0.5, 0.5, 0.9), 0.1)
+    assert rel(q, o.gaussian_source(2.0, (0.5, 0.5, 0.9), 0.1)) <= 1e-14
+
+
+def test_constrained_rows_and_zero_input():
+    o, g = pair(2, (3, 3, 3), 0.1, "linear_k")
+    N = o.n_dofs
+    T = cuda(np.random.default_rng(2).uniform(size=N))
+    g.set_linearization(T, T)
+    dst = g.new_vector()
+    g.vmult(dst, g.new_vector())
+    assert torch.count_nonzero(dst) == 0
+    src = cuda(np.random.default_rng(3).uniform(-1, 1, N))
+    g.vmult(dst, src)
+    mask = torch.tensor(o.mask().astype(bool), device="cuda")
+    assert torch.count_nonzero(dst[mask]) == 0
+    d = g.compute_inverse_diagonal_from_matrixfree(g.new_vector())
+    assert torch.all(d[mask] == 1.0)
+
+
+def test_single_cell_and_thin_meshes():
+    for cells, degree in [((1, 1, 1), 1), ((1, 1, 1), 4), ((7, 1, 1), 2), ((1, 5, 2), 3)]:
+        o, g = pair(degree, cells, 0.0, "liquid_solid", dirichlet=0)
+        rng = np.random.default_rng(sum(cells))
+        src, Tl, To = (rng.uniform(0, 1, o.n_dofs) for _ in range(3))
+        g.set_linearization(cuda(Tl), cuda(To))
+        dst = g.new_vector()
+        g.vmult(dst, cuda(src))
+        assert rel(dst, o.vmult(src, Tl, To)) <= TOL64
+
+
+def test_errors_are_raised_not_silent():
+    o, g = pair(2, (2, 2, 2))
+    g.reset_time_increment(0.0)
+    with pytest.raises(H.ExcZeroTimeIncrement):
+        g.vmult(g.new_vector(), g.new_vector())
+    g.reset_time_increment(1e-3)
+    g.set_material(H.material(law=1, k1=0.5))
+    with pytest.raises(H.ExcInvalidArgument):  # k(T) law without a linearisation point
+        g.vmult(g.new_vector(), g.new_vector())
+    with pytest.raises(H.ExcInvalidArgument):
+        g.vmult(g.new_vector(), torch.zeros(g.n_dofs, dtype=torch.float64))  # host tensor
+    with pytest.raises(H.ExcInvalidArgument):
+        H.HeatDiffuseOperator(H.box_mesh(7, (2, 2, 2)))
+
+
+@pytest.mark.parametrize("law", ["constant", "linear_k"])
+def test_jacobi_cg_matches_oracle(law):
+    o, g = pair(3, (6, 5, 4), 0.15, law, dt=1e-2)
+    rng = np.random.default_rng(7)
+    N = o.n_dofs
+    Tl = rng.uniform(0, 1, N)
+    b = o.vmult(rng.uniform(-1, 1, N), Tl, Tl)
+    x_ref, its_ref, _ = o.cg(b, T_lin=Tl, T_old=Tl, rel_tol=1e-12)
+    Tl_d = cuda(Tl)
+    g.set_linearization(Tl_d, Tl_d)
+    H.JacobiPreconditioner(g).update()
+    x = g.new_vector()
+    its = H.LinearSolver.solve(g, x, cuda(b), H.LinearSolverData(rel_tolerance=1e-12), True)
+    assert abs(its - its_ref) <= 2
+    assert rel(x, x_ref) <= 1e-9
+
+
+@pytest.mark.parametrize("degree", [2, 3, 4])
+def test_chebyshev_mixed_precision_cg(degree):
+    o, g = pair(degree, (5, 5, 5), 0.2, "linear_k", dt=5e-3)
+    rng = np.random.default_rng(degree)
+    N = o.n_dofs
+    Tl = rng.uniform(0, 1, N)
+    b = o.vmult(rng.uniform(-1, 1, N), Tl, Tl)
+    x_ref, its_ref, _ = o.cg(b, T_lin=Tl, T_old=Tl, rel_tol=1e-13)
+    Tl_d = cuda(Tl)
+    g.set_linearization(Tl_d, Tl_d)
+    H.JacobiPreconditioner(g).update()
+    x = g.new_vector()
+    data = H.LinearSolverData(preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32,
+                              rel_tolerance=1e-10, cheb_degree=4)
+    its = H.LinearSolver.solve(g, x, cuda(b), data, True)
+    st = H.LinearSolver.last_stats
+    assert st.true_residual <= 1e-10 * st.initial_residual * 1.0000001
+    assert its < its_ref  # the polynomial preconditioner cuts outer iterations
+    assert rel(x, x_ref) <= 1e-7
+
+
+def test_linear_solve_not_converged_raises():
+    o, g = pair(3, (4, 4, 4), 0.0, dt=1.0)
+    H.JacobiPreconditioner(g).update()
+    b = cuda(np.random.default_rng(0).uniform(size=o.n_dofs))
+    with pytest.raises(H.ExcNoConvergence):
+        H.LinearSolver.solve(g, g.new_vector(), b,
+                             H.LinearSolverData(max_iterations=3, rel_tolerance=1e-12), True)

@@ -1,0 +1,56 @@
+"""Implicit heat steps on the GPU: the reference regression case and the
+single-linearisation step against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from meltpooldg_b200 import _lib as L
+from meltpooldg_b200 import heat as H
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+# applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/
+#   unidirectional_heat_transfer.mpirun=4.output
+UNIDIRECTIONAL = [5.64198e-03, 5.53556e-03, 5.44694e-03, 5.37273e-03, 5.31056e-03]
+
+
+def test_unidirectional_heat_transfer_newton_on_gpu():
+    op = H.HeatDiffuseOperator(H.box_mesh(1, (32, 32, 1), (0, 0, 0), (0.1, 0.1, 1.0),
+                                          dirichlet=()))
+    op.set_material(H.material())
+    opn = H.HeatDiffuseOperation(op, H.LinearSolverData(rel_tolerance=1e-12),
+                                 H.NonlinearSolverData(residual_tolerance=5e-9))
+    x = op.support_points()
+    opn.set_initial_condition(x[:, 0].contiguous())
+    for ref in UNIDIRECTIONAL:
+        st = opn.solve(1e-4)
+        assert st.converged == 1
+        assert float(f"{op.l2_norm(opn.T):.5e}") == ref
+
+
+@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_CHEBYSHEV_JACOBI_F32])
+def test_single_linearization_step_matches_oracle(precond):
+    """One k(T) = 1 + 0.5 T step: T = T_g + J(T_g)^-1 (-R(T_g)), Gaussian source."""
+    deg, cells, dt = 3, (6, 6, 6), 5e-4
+    o = O.Oracle(deg, cells, perturb=0.1, seed=5)
+    o.set_material(O.material(O.LAW_LINEAR_K, k=1.0, k1=0.5), dt)
+    q = o.gaussian_source(50.0, (0.5, 0.5, 0.9), 0.1)
+    T_old = np.zeros(o.n_dofs)
+    T_prev = o.distribute(np.random.default_rng(1).uniform(0, 1, o.n_dofs))
+    # oracle: predictor = T_prev (first step), linearise there, solve to 1e-12
+    Tg = T_prev.copy()
+    r = o.create_rhs(Tg, T_prev, q)
+    d, its, _ = o.cg(r, T_lin=Tg, T_old=T_prev, rel_tol=1e-13)
+    T_ref = Tg + d
+    op = H.HeatDiffuseOperator(H.box_mesh(deg, cells, perturb=0.1, seed=5))
+    op.set_material(H.material(law=1, k=1.0, k1=0.5))
+    lin = H.LinearSolverData(preconditioner_type=precond, rel_tolerance=1e-10)
+    opn = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_NONE, single_linearization=True)
+    opn.set_initial_condition(torch.tensor(T_prev, device="cuda"))
+    opn.heat_source = torch.tensor(q, device="cuda")
+    st = opn.solve(dt)
+    T = opn.T.cpu().numpy()
+    assert np.abs(T - T_ref).max() <= 1e-7 * np.abs(T_ref).max()
+    assert np.array_equal(opn.T_old.cpu().numpy(), T_prev)
+    assert st.linear_iterations > 0

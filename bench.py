@@ -1,0 +1,372 @@
+"""Benchmark: implicit heat steps of the nonlinear k(T) heat problem on B200.
+
+Workload (one "step" = one implicit Euler step of the hot path): FE_Q(3) on the
+unit cube with 128^3 cells (385^3 = 57,066,625 DoFs), k(T) = 1 + 0.5 T,
+rho*cp = 1, dt = 5e-4, Dirichlet T = 0 on all faces, T0 = 0, a Gaussian source
+of radius 0.05 at z = 0.95 moving along x at speed 1, one Newton linearisation
+per step solved to |b - J T| <= 1e-8 |b|. Two solvers run the same steps:
+  plain  FP64 Jacobi-CG
+  mixed  FP64 flexible CG with the FP32 degree-4 Chebyshev-Jacobi preconditioner
+`value` is the step throughput of the faster one in DoFs advanced per second
+(whole job: summed over replicas when run with --gpus N > 1, which runs
+independent replicas: the path has no data-parallel exchange on one mesh).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Heat step time @1e-8 resid: learned+mixed vs plain FP64 CG; MF vmult GDoF/s"
+DEGREE, CELLS, DT, K1 = 3, 128, 5e-4, 0.5
+AMP, RADIUS, Z0, SPEED, X0 = 500.0, 0.05, 0.95, 1.0, 0.1
+REL_TOL = 1e-8
+
+
+def source_center(t):
+    return (X0 + SPEED * t, 0.5, Z0)
+
+
+def workload_config(cells):
+    n = (DEGREE * cells + 1) ** 3
+    return {
+        "workload": f"implicit k(T) heat step, FE_Q({DEGREE}) unit cube {cells}^3 cells "
+                    f"({n} DoFs), k=1+{K1}T, rho*cp=1, dt={DT}, Dirichlet 0, moving Gaussian "
+                    f"source r={RADIUS} z={Z0} v={SPEED}, one linearisation, |b-JT|<={REL_TOL}|b|",
+        "degree": DEGREE, "cells": [cells] * 3, "n_dofs": n,
+        "l2_flush": "inputs larger than L2 (each FP64 vector is %.0f MB > 126 MB L2)" % (n * 8 / 1e6),
+    }
+
+
+# ---------------------------------------------------------------------------
+# clock sampling
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle port: the reference's algorithm restated in C, OpenMP)
+# ---------------------------------------------------------------------------
+def cpu_step_sample(cells, steps):
+    """Implicit steps of the same problem on a smaller mesh with the oracle; returns
+    (DoFs/s, seconds, n_dofs, cores)."""
+    import numpy as np
+    from oracle import oracle as O
+    o = O.Oracle(DEGREE, (cells,) * 3)
+    o.set_material(O.material(O.LAW_LINEAR_K, k=1.0, k1=K1), DT)
+    T = np.zeros(o.n_dofs)
+    T_old = np.zeros(o.n_dofs)
+    dt_old = 0.0
+    t0 = time.perf_counter()
+    for s in range(steps):
+        t = (s + 1) * DT
+        q = o.gaussian_source(AMP, source_center(t), RADIUS)
+        Tg = o.linear_predictor(T, T_old, DT, dt_old)
+        T_old, T = T, o.distribute(Tg)
+        r = o.create_rhs(T, T_old, q)
+        b = o.vmult(T, T, T_old) + r
+        bn, rn = float(np.linalg.norm(b)), float(np.linalg.norm(r))
+        if rn > 0.0:
+            d, _, _ = o.cg(r, T_lin=T, T_old=T_old, rel_tol=REL_TOL * bn / rn, abs_tol=0.0)
+            T = T + d
+        dt_old = DT
+    sec = time.perf_counter() - t0
+    return o.n_dofs * steps / sec, sec, o.n_dofs, os.cpu_count()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cells = args.cpu_cells
+    for _ in range(args.warmup):
+        cpu_step_sample(cells, 1)
+    rate, sec, n, cores = cpu_step_sample(cells, args.steps)
+    sample = (f"{args.steps} implicit steps of the same problem on {cells}^3 cells ({n} DoFs) "
+              f"with the oracle port (OpenMP, {cores} threads)")
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "DoF/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(CELLS),
+            "cpu_baseline": {"value": rate, "unit": "DoF/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "DoF/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the dominant kernel from the committed ncu summary."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        return d
+    except Exception:
+        return {}
+
+
+def run_mine(args):
+    import torch
+    import torch.distributed as dist
+
+    from meltpooldg_b200 import _lib as L
+    from meltpooldg_b200 import heat as H
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    cells = args.cells
+
+    op = H.HeatDiffuseOperator(H.box_mesh(DEGREE, (cells,) * 3), device=local)
+    op.set_material(H.material(law=L.LAW_LINEAR_K, k=1.0, k1=K1))
+    N = op.n_dofs
+    plain = H.HeatDiffuseOperation(op, H.LinearSolverData(rel_tolerance=REL_TOL,
+                                                          abs_tolerance=0.0),
+                                   predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    mixed = H.HeatDiffuseOperation(op, H.LinearSolverData(
+        preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32, rel_tolerance=REL_TOL,
+        abs_tolerance=0.0, cheb_degree=4), predictor=L.PREDICTOR_LINEAR,
+        single_linearization=True)
+    q = op.new_vector()
+    mixed.heat_source = q
+    plain.heat_source = q
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    def march(opn, first, count):
+        its = []
+        for s in range(first, first + count):
+            op.gaussian_source(q, AMP, source_center((s + 1) * DT), RADIUS)
+            st = opn.solve(DT)
+            its.append(st.linear_iterations)
+        return its
+
+    def timed(opn, first, count, instrument=False):
+        barrier()
+        if instrument:
+            op.set_timing(True)
+            op.counters(reset=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        its = march(opn, first, count)
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        cnt = None
+        if instrument:
+            cnt = op.counters(reset=True)
+            op.set_timing(False)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, its, cnt
+
+    W, K = args.warmup, args.steps
+    # plain FP64 Jacobi-CG
+    ms_plain = its_plain = None
+    if not args.no_plain:
+        march(plain, 0, W)
+        ms_plain, its_plain, _ = timed(plain, W, K)
+    # mixed precision (timed region with clock sampling and operator timing)
+    march(mixed, 0, W)
+    clocks = Clocks(local) if rank == 0 else None
+    ms_mixed, its_mixed, cnt = timed(mixed, W, K, instrument=True)
+    clk = clocks.stop() if clocks else None
+    err = None
+    if not args.no_plain:
+        diff = torch.linalg.vector_norm(mixed.T - plain.T).item()
+        ref = torch.linalg.vector_norm(plain.T).item()
+        err = {"rel_l2": diff / ref if ref > 0 else 0.0,
+               "rel_max": ((mixed.T - plain.T).abs().max() / plain.T.abs().max()).item()}
+
+    # e2e: the host-buffer C-ABI call (H2D of T, T_old, source; D2H of T, T_old per step)
+    e2e = None
+    if not args.no_e2e:
+        import ctypes as C
+        hT = torch.empty(N, dtype=torch.float64, pin_memory=True)
+        hTo = torch.empty(N, dtype=torch.float64, pin_memory=True)
+        hq = torch.empty(N, dtype=torch.float64, pin_memory=True)
+        hT.copy_(mixed.T)
+        hTo.copy_(mixed.T_old)
+        prm = mixed.params
+        ms_e2e = 0.0
+        first = W + K
+        for s in range(first, first + K):
+            op.gaussian_source(q, AMP, source_center((s + 1) * DT), RADIUS)
+            hq.copy_(q)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            stt = L.StepStats()
+            H.check(op._L.mpdg_heat_time_step_host(op.h, C.byref(prm), DT, DT,
+                                                    C.c_void_p(hT.data_ptr()),
+                                                    C.c_void_p(hTo.data_ptr()),
+                                                    C.c_void_p(hq.data_ptr()), C.byref(stt)))
+            e1.record(stream)
+            barrier()
+            ms_e2e += e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms_e2e], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e2e = float(t.item())
+        e2e = {"value": world * N * K / (ms_e2e / 1e3), "unit": "DoF/s",
+               "h2d_bytes_per_step": 3 * N * 8, "d2h_bytes_per_step": 2 * N * 8,
+               "ms_per_step": ms_e2e / K}
+
+    # vmult throughput of the FP64 operator (MF vmult GDoF/s), CUDA events
+    x = torch.rand(N, dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    for _ in range(3):
+        op.vmult(y, x)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(10):
+        op.vmult(y, x)
+    e1.record(stream)
+    barrier()
+    vm_ms = e0.elapsed_time(e1) / 10
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    # roofline of the dominant kernel in the timed region
+    hbm, hbm_kind = peaks()
+    if cnt["vmult32_ms"] >= cnt["vmult64_ms"]:
+        kname, s, calls, kms = "k_vmult<4,float,affine,linear_k>", 4, cnt["vmult32_calls"], cnt["vmult32_ms"]
+    else:
+        kname, s, calls, kms = "k_vmult<4,double,affine,linear_k>", 8, cnt["vmult64_calls"], cnt["vmult64_ms"]
+    alg_bytes = 3 * s * N  # src + dst + linearisation point
+    per_launch_ms = kms / max(calls, 1)
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    tr = profile_traffic().get(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "peak_source": f"{hbm_kind} hbm_gbs",
+                "traffic": tr, "algorithmic_bytes_per_launch": alg_bytes,
+                "avg_launch_ms": per_launch_ms, "launches": calls,
+                "share_of_step": kms / ms_mixed}
+
+    cpu = None
+    if not args.no_cpu:
+        rate, sec, n, cores = cpu_step_sample(args.cpu_cells, args.cpu_steps)
+        cpu = {"value": rate, "unit": "DoF/s", "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_steps} implicit steps of the same problem on "
+                         f"{args.cpu_cells}^3 cells ({n} DoFs), oracle port, {sec:.1f} s"}
+
+    best_ms = min(ms_mixed, ms_plain) if ms_plain else ms_mixed
+    line = {
+        "metric": METRIC, "value": world * N * K / (best_ms / 1e3), "unit": "DoF/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": best_ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (outer CG) + f32 (Chebyshev preconditioner)", "data": "synthetic",
+        "config": {**workload_config(cells), "parallelism": f"replicas x{world}"},
+        "mixed_ms_per_step": ms_mixed / K,
+        "plain_fp64_ms_per_step": ms_plain / K if ms_plain else None,
+        "speedup_mixed_vs_plain": (ms_plain / ms_mixed) if ms_plain else None,
+        "cg_iterations_mixed": its_mixed, "cg_iterations_plain": its_plain,
+        "mixed_vs_plain_error": err,
+        "vmult_fp64_gdofs": N / (vm_ms / 1e3) / 1e9, "vmult_fp64_ms": vm_ms,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(cnt["launches"]), "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--cells", type=int, default=CELLS)
+    ap.add_argument("--cpu-cells", type=int, default=48)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_mine(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -213,6 +213,20 @@ int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *prm, double d
                              double dt_old, double *T_cur, double *T_old,
                              const double *heat_source, mpdg_step_stats *stats);
 
+/* ---- instrumentation -------------------------------------------------- */
+typedef struct {
+  int64_t launches;        /* kernels this handle launched since the last reset      */
+  int64_t vmult64_calls, vmult32_calls;
+  double  vmult64_ms, vmult32_ms; /* summed device time of the operator applications
+                                     (CUDA events on the handle's stream; only while
+                                     timing is enabled)                                */
+} mpdg_counters;
+
+/* Enable/disable per-launch CUDA-event timing of the operator applications. */
+int mpdg_heat_set_timing(mpdg_heat *h, int enable);
+/* Read (synchronises the stream) and optionally reset the counters. */
+int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset);
+
 /* Last error message of this thread (static storage). */
 const char *mpdg_last_error(void);
 

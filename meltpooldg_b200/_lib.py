@@ -70,6 +70,12 @@ class StepStats(C.Structure):
                 ("step_ms", C.c_double)]
 
 
+class Counters(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("vmult64_calls", C.c_int64),
+                ("vmult32_calls", C.c_int64), ("vmult64_ms", C.c_double),
+                ("vmult32_ms", C.c_double)]
+
+
 _P = C.c_void_p
 _H = C.c_void_p
 _D = C.c_void_p  # device pointers are passed as integers
@@ -104,6 +110,8 @@ _SIGS = {
                                       _D, C.POINTER(StepStats)]),
     "mpdg_heat_time_step_host": (C.c_int, [_H, C.POINTER(StepParams), C.c_double, C.c_double,
                                            _P, _P, _P, C.POINTER(StepStats)]),
+    "mpdg_heat_set_timing": (C.c_int, [_H, C.c_int]),
+    "mpdg_heat_get_counters": (C.c_int, [_H, C.POINTER(Counters), C.c_int]),
     "mpdg_last_error": (C.c_char_p, []),
 }
 

@@ -102,7 +102,40 @@ struct mpdg_heat {
   const double *guess = nullptr;
   int64_t bytes = 0;
   std::vector<void *> owned;
+  // instrumentation
+  int64_t launches = 0, vm64 = 0, vm32 = 0;
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev64, ev32;
+  std::vector<cudaEvent_t> ev_pool;
+  double ms64 = 0.0, ms32 = 0.0;
 };
+
+static cudaEvent_t take_event(mpdg_heat *h)
+{
+  if (!h->ev_pool.empty()) {
+    cudaEvent_t e = h->ev_pool.back();
+    h->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// fold recorded operator-timing events into the sums (stream must be idle)
+static void drain_events(mpdg_heat *h)
+{
+  for (auto *v : {&h->ev64, &h->ev32}) {
+    for (auto &pr : *v) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess)
+        (v == &h->ev64 ? h->ms64 : h->ms32) += ms;
+      h->ev_pool.push_back(pr.first);
+      h->ev_pool.push_back(pr.second);
+    }
+    v->clear();
+  }
+}
 
 static constexpr int kPartialsPerValue = 148 * 64;
 
@@ -688,7 +721,19 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
   a.fin = fin;
   a.out = out;
   a.st = st;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->timing) {
+    e0 = take_event(h);
+    e1 = take_event(h);
+    cudaEventRecord(e0, h->stream);
+  }
   CU(h->tab.vmult_d(a, h->geo, h->law, h->stream, h->sm_count));
+  if (h->timing) {
+    cudaEventRecord(e1, h->stream);
+    h->ev64.push_back({e0, e1});
+  }
+  ++h->vm64;
+  ++h->launches;
   return MPDG_OK;
 }
 
@@ -698,14 +743,17 @@ static int refresh_f32(mpdg_heat *h)
   if (h->geo == 1 && !h->geoq_f) {
     const int64_t ng = h->n_cells * 7 * h->npt;
     TRY(dvec(h, &h->geoq_f, ng));
-    k_cast_f<<<vgrid(h, ng), VT, 0, h->stream>>>(ng, h->geoq, h->geoq_f);
+    k_cast_f<<<vgrid(h, ng), VT, 0, h->stream>>>(ng, h->geoq, h->geoq_f); ++h->launches;
     CU(cudaGetLastError());
   }
   if (h->lin_f_dirty && h->law != MPDG_LAW_CONSTANT) {
     TRY(dvec(h, &h->T_lin_f, N));
     TRY(dvec(h, &h->T_old_f, N));
-    k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->T_lin, h->T_lin_f);
-    if (h->T_old) k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->T_old, h->T_old_f);
+    k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->T_lin, h->T_lin_f); ++h->launches;
+    if (h->T_old) {
+      k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->T_old, h->T_old_f);
+      ++h->launches;
+    }
     CU(cudaGetLastError());
   }
   h->lin_f_dirty = false;
@@ -724,7 +772,19 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
   a.Tl = h->T_lin_f;
   a.To = h->T_old_f;
   a.st = st;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->timing) {
+    e0 = take_event(h);
+    e1 = take_event(h);
+    cudaEventRecord(e0, h->stream);
+  }
   CU(h->tab.vmult_f(a, h->geo, h->law, h->stream, h->sm_count));
+  if (h->timing) {
+    cudaEventRecord(e1, h->stream);
+    h->ev32.push_back({e0, e1});
+  }
+  ++h->vm32;
+  ++h->launches;
   return MPDG_OK;
 }
 
@@ -738,7 +798,7 @@ static int poll(mpdg_heat *h)
 static int norms(mpdg_heat *h, const double *a, const double *b, double *aa, double *ab)
 {
   const int64_t N = h->n_dofs;
-  k_norms<<<vgrid(h, N), VT, 0, h->stream>>>(N, a, b, h->partials, h->counter, h->scal);
+  k_norms<<<vgrid(h, N), VT, 0, h->stream>>>(N, a, b, h->partials, h->counter, h->scal); ++h->launches;
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(h->scal_host, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
@@ -781,7 +841,7 @@ static int cg_jacobi(mpdg_heat *h, const mpdg_solver_params *prm, double *x, con
   TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
   k_cg_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->pv, h->Ap, D, h->st, h->partials, h->counter,
                                       prm->rel_tolerance, prm->abs_tolerance,
-                                      prm->tol_reference_norm, prm->max_iterations, record);
+                                      prm->tol_reference_norm, prm->max_iterations, record); ++h->launches;
   CU(cudaGetLastError());
   TRY(poll(h));
   const double res0 = h->st_host->res0;
@@ -790,8 +850,8 @@ static int cg_jacobi(mpdg_heat *h, const mpdg_solver_params *prm, double *x, con
     for (int c = 0; c < chunk; ++c) {
       TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
       k_cg_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, D, h->st, h->partials,
-                                              h->counter);
-      k_cg_update_p<<<g, VT, 0, h->stream>>>(N, h->r, h->pv, h->Ap, D, h->st);
+                                              h->counter); ++h->launches;
+      k_cg_update_p<<<g, VT, 0, h->stream>>>(N, h->r, h->pv, h->Ap, D, h->st); ++h->launches;
     }
     CU(cudaGetLastError());
     TRY(poll(h));
@@ -840,7 +900,7 @@ static int estimate_eigenvalues(mpdg_heat *h, int n_it, double *lmin, double *lm
   n_it = std::max(2, std::min(n_it, 64));
   TRY(dvec(h, &h->w3, N));
   TRY(dvec(h, &h->z, N));
-  k_masked_random<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, h->w3);
+  k_masked_random<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, h->w3); ++h->launches;
   CU(cudaMemsetAsync(h->z, 0, sizeof(double) * N, h->stream));
   mpdg_solver_params prm;
   mpdg_solver_params_default(&prm);
@@ -877,7 +937,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   TRY(ensure_workspace_f32(h));
   TRY(refresh_f32(h));
   if (h->diag_f_dirty) {
-    k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->inv_diag, h->inv_diag_f);
+    k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->inv_diag, h->inv_diag_f); ++h->launches;
     CU(cudaGetLastError());
     h->diag_f_dirty = false;
   }
@@ -912,22 +972,24 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
                                         res0 > 0.0 && prm->tol_reference_norm <= 0.0
                                           ? res0
                                           : prm->tol_reference_norm,
-                                        prm->max_iterations - total_it);
+                                        prm->max_iterations - total_it); ++h->launches;
     CU(cudaGetLastError());
     TRY(poll(h));
     if (res0 < 0.0) res0 = h->st_host->res0;
     auto precondition = [&]() -> int {
       for (int j = 1; j <= k; ++j) {
         TRY(op_apply_f(h, h->Ax32, h->x32, h->st));
-        if (j < k)
+        if (j < k) {
           k_cheb_step<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
                                                c1[j], c2[j], h->st);
-        else
+        } else {
           k_cheb_last<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
                                                c1[j], c2[j], h->r, h->Ap, h->z, h->st,
                                                h->partials, h->counter);
+        }
+        ++h->launches;
       }
-      k_cgm_update_p<<<g, VT, 0, h->stream>>>(N, h->z, h->pv, h->Ap, h->st);
+      k_cgm_update_p<<<g, VT, 0, h->stream>>>(N, h->z, h->pv, h->Ap, h->st); ++h->launches;
       CU(cudaGetLastError());
       return MPDG_OK;
     };
@@ -938,7 +1000,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
         TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
         k_cgm_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, h->r32, h->x32, h->d32,
                                                  h->inv_diag_f, inv_theta, h->st, h->partials,
-                                                 h->counter);
+                                                 h->counter); ++h->launches;
         TRY(precondition());
       }
       TRY(poll(h));
@@ -952,7 +1014,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
     TRY(dvec(h, &h->w3, N));
     CU(cudaMemcpyAsync(h->w3, b, sizeof(double) * N, cudaMemcpyDeviceToDevice, h->stream));
-    k_axpy<<<g, VT, 0, h->stream>>>(N, h->w3, -1.0, h->Ap);
+    k_axpy<<<g, VT, 0, h->stream>>>(N, h->w3, -1.0, h->Ap); ++h->launches;
     double rr = 0.0;
     TRY(norms(h, h->w3, nullptr, &rr, nullptr));
     true_res = std::sqrt(rr);
@@ -1008,6 +1070,10 @@ extern "C" void mpdg_step_params_default(mpdg_step_params *p)
 
 static void release(mpdg_heat *h)
 {
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drain_events(h);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  h->ev_pool.clear();
   for (void *p : h->owned) cudaFree(p);
   h->owned.clear();
   if (h->st_host) cudaFreeHost(h->st_host);
@@ -1233,7 +1299,8 @@ static int compute_diag(mpdg_heat *h, double *d)
   a.Tl = h->T_lin;
   a.To = h->T_old;
   CU(h->tab.diag(a, h->geo, h->law, h->stream, h->sm_count));
-  k_invert_diag<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, d);
+  ++h->launches;
+  k_invert_diag<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, d); ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;
 }
@@ -1256,6 +1323,7 @@ static int create_rhs(mpdg_heat *h, double *dst, const double *src, const double
   a.To = src;
   a.qs = q;
   CU(h->tab.rhs(a, h->geo, h->law, h->stream, h->sm_count));
+  ++h->launches;
   return MPDG_OK;
 }
 
@@ -1277,7 +1345,7 @@ static int distribute(mpdg_heat *h, double *u)
     const int dir = f / 2;
     const int e1 = dir == 0 ? 1 : 0, e2 = dir == 2 ? 1 : 2;
     const int64_t cnt = (int64_t)h->dims.nd[e1] * h->dims.nd[e2];
-    k_distribute<<<vgrid(h, cnt), VT, 0, h->stream>>>(a, f, u);
+    k_distribute<<<vgrid(h, cnt), VT, 0, h->stream>>>(a, f, u); ++h->launches;
   }
   CU(cudaGetLastError());
   return MPDG_OK;
@@ -1299,6 +1367,7 @@ extern "C" int mpdg_heat_l2_norm(mpdg_heat *h, const double *u, double *norm)
   a.src = u;
   a.out = h->scal;
   CU(h->tab.norm(a, h->geo, 0, h->stream, h->sm_count));
+  ++h->launches;
   CU(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
   *norm = std::sqrt(h->scal_host[0]);
@@ -1328,7 +1397,7 @@ extern "C" int mpdg_heat_support_points(mpdg_heat *h, double *xyz)
 {
   if (!h || !xyz) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   CU(cudaSetDevice(h->device));
-  k_support_points<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), xyz);
+  k_support_points<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), xyz); ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;
 }
@@ -1340,7 +1409,7 @@ extern "C" int mpdg_heat_gaussian_source(mpdg_heat *h, double *q, double amplitu
   CU(cudaSetDevice(h->device));
   k_gaussian<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), q, amplitude,
                                                         center[0], center[1], center[2],
-                                                        1.0 / (radius * radius));
+                                                        1.0 / (radius * radius)); ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;
 }
@@ -1362,7 +1431,7 @@ extern "C" int mpdg_heat_preconditioner_vmult(mpdg_heat *h, double *dst, const d
   if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
   CU(cudaSetDevice(h->device));
-  k_scale<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, dst, src, h->inv_diag);
+  k_scale<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, dst, src, h->inv_diag); ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;
 }
@@ -1433,7 +1502,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     h->eig_valid = false;
     // init_time_advance: predictor into w1, commit history, constraints
     if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
-      k_predict<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, h->w1, dt / dt_old);
+      k_predict<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, h->w1, dt / dt_old); ++h->launches;
     } else if (prm->predictor == MPDG_PREDICTOR_GIVEN) {
       if ((rc = (cudaMemcpyAsync(h->w1, h->guess, vb, cudaMemcpyDeviceToDevice, h->stream) ==
                  cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, "guess copy"))) != MPDG_OK) break;
@@ -1468,7 +1537,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
       mpdg_solve_stats ls;
       memset(&ls, 0, sizeof(ls));
       if ((rc = linear_solve(h, &lp, h->w1, h->w2, &ls)) != MPDG_OK) break;
-      k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1);
+      k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1); ++h->launches;
       if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
       s.linear_iterations = ls.iterations;
       s.newton_iterations = 1;
@@ -1491,7 +1560,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
           s.converged = 1;
           break;
         }
-        k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1);
+        k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1); ++h->launches;
         if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
         h->lin_f_dirty = true;
         s.newton_iterations = i + 1;
@@ -1534,5 +1603,30 @@ extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *pr
   CU(cudaMemcpyAsync(T_cur, h->host_T, vb, cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(T_old, h->host_To, vb, cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_timing(mpdg_heat *h, int enable)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  h->timing = enable != 0;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset)
+{
+  if (!h || !c) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->stream));
+  drain_events(h);
+  c->launches = h->launches;
+  c->vmult64_calls = h->vm64;
+  c->vmult32_calls = h->vm32;
+  c->vmult64_ms = h->ms64;
+  c->vmult32_ms = h->ms32;
+  if (reset) {
+    h->launches = h->vm64 = h->vm32 = 0;
+    h->ms64 = h->ms32 = 0.0;
+  }
   return MPDG_OK;
 }

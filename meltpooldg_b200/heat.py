@@ -241,6 +241,14 @@ class HeatDiffuseOperator:
         check(self._L.mpdg_heat_l2_norm(self.h, _ptr(u), C.byref(v)))
         return float(v.value)
 
+    def set_timing(self, enable: bool):
+        check(self._L.mpdg_heat_set_timing(self.h, int(bool(enable))))
+
+    def counters(self, reset: bool = False) -> dict:
+        c = L.Counters()
+        check(self._L.mpdg_heat_get_counters(self.h, C.byref(c), int(bool(reset))))
+        return {k: getattr(c, k) for k, _ in L.Counters._fields_}
+
     def support_points(self):
         x = torch.empty((self.n_dofs, 3), dtype=torch.float64, device=self.device)
         check(self._L.mpdg_heat_support_points(self.h, x.data_ptr()))

@@ -1,0 +1,56 @@
+"""Time (and give ncu a target for) the operator application on one mesh.
+
+  python -m meltpooldg_b200.profile_vmult --degree 3 --cells 96 --law 1 --reps 3
+prints one JSON line per precision with the CUDA-event time per application,
+DoFs/s and algorithmic GB/s (src + dst + linearisation point [+ per-q geometry]).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import torch
+
+from . import heat as H
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--degree", type=int, default=3)
+    ap.add_argument("--cells", type=int, default=96)
+    ap.add_argument("--perturb", type=float, default=0.0)
+    ap.add_argument("--law", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--dtype", default="both", choices=["f64", "f32", "both"])
+    a = ap.parse_args()
+    op = H.HeatDiffuseOperator(H.box_mesh(a.degree, (a.cells,) * 3, perturb=a.perturb))
+    op.set_material(H.material(law=a.law, k=1.0, k1=0.5))
+    op.reset_time_increment(5e-4)
+    N = op.n_dofs
+    g = torch.Generator(device="cuda").manual_seed(0)
+    T = torch.rand(N, dtype=torch.float64, device="cuda", generator=g)
+    op.set_linearization(T, T)
+    nq = op.n_cells * (a.degree + 1) ** 3
+    for dt in (["f64", "f32"] if a.dtype == "both" else [a.dtype]):
+        ty = torch.float64 if dt == "f64" else torch.float32
+        s = 8 if dt == "f64" else 4
+        x = torch.rand(N, dtype=ty, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        op.vmult(y, x)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.reps):
+            op.vmult(y, x)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+        alg = s * N * (2 + (1 if a.law else 0)) + (7 * s * nq if a.perturb > 0 else 0)
+        print(json.dumps({"degree": a.degree, "cells": a.cells, "perturb": a.perturb,
+                          "law": a.law, "dtype": dt, "n_dofs": N, "ms": ms,
+                          "gdofs": N / ms / 1e6, "alg_bytes": alg,
+                          "alg_gbs": alg / ms / 1e6}), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -578,7 +578,7 @@ __global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32
 }
 
 // last Chebyshev step, then z = x32 (FP64), rz = r.z, zAp = z.Ap and the
-// flexible (Polak-Ribiere) beta = (z.r - alpha z.Ap) / rz_old
+// flexible (Polak-Ribiere) beta = z.(r - r_old) / rz_old = -alpha z.Ap / rz_old
 __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const float *__restrict__ x32,
                             const float *__restrict__ d32, float *Ax32,
                             const float *__restrict__ D32, float c1, float c2,
@@ -602,7 +602,7 @@ __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const floa
       st->beta = 0.0;
       st->first = 0;
     } else {
-      st->beta = (tot[0] - st->alpha * tot[1]) / st->rz;
+      st->beta = -st->alpha * tot[1] / st->rz;
     }
     st->rz = tot[0];
     st->zAp = tot[1];

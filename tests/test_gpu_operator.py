@@ -187,6 +187,7 @@ def test_chebyshev_mixed_precision_cg_larger_mesh():
     g.set_linearization(T, T)
     H.JacobiPreconditioner(g).update()
     x_src = g.gaussian_source(g.new_vector(), 1.0, (0.5, 0.5, 0.5), 0.2)
+    g.distribute_constraints(x_src)  # homogeneous Dirichlet values
     b = g.vmult(g.new_vector(), x_src)
     its_j = H.LinearSolver.solve(g, g.new_vector(), b, H.LinearSolverData(rel_tolerance=1e-10),
                                  True)

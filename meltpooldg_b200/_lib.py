@@ -98,6 +98,7 @@ _SIGS = {
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),
     "mpdg_heat_distribute_constraints": (C.c_int, [_H, _D]),
     "mpdg_heat_l2_norm": (C.c_int, [_H, _D, C.POINTER(C.c_double)]),
+    "mpdg_heat_l2_norm_noalloc": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_support_points": (C.c_int, [_H, _D]),
     "mpdg_heat_gaussian_source": (C.c_int, [_H, _D, C.c_double, C.POINTER(C.c_double),
                                             C.c_double]),

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1628,5 +1629,80 @@ extern "C" int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset)
     h->launches = h->vm64 = h->vm32 = 0;
     h->ms64 = h->ms32 = 0.0;
   }
+  return MPDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FE L2 norm that allocates nothing
+//
+// Some callers cannot call cudaMalloc: code being captured into a CUDA graph
+// (allocation is not a capturable operation), code that runs inside another
+// framework's memory pool where raw driver allocations are forbidden or would
+// break its accounting, and loops that must not pay the implicit device
+// synchronisation of a first-use allocation. For them this variant of the L2
+// norm keeps its reduction scratch (one partial sum per CTA plus the last-CTA
+// election counter) in a fixed array in this file instead of handle memory,
+// and writes the result to a device scalar the caller owns.
+//
+// Limits and sharing: the array holds kNoAllocSlots partial sums (128 KiB),
+// i.e. the reduction grid may have at most kNoAllocSlots CTAs; a launch that
+// would need more is rejected with MPDG_ERR_INVALID_ARGUMENT (it cannot happen
+// on GPUs with up to 512 SMs). Every GPU that loads the library holds the
+// array until the process exits. All calls on a device share it and it keeps
+// the last call's contents; the counter is cleared at the start of each call,
+// so calls that overlap on the GPU (different streams, or different host
+// threads on one device) race and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+static constexpr int kNoAllocSlots = 16384;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlots + 32];
+
+static std::mutex g_noalloc_mutex;
+static double *g_noalloc_addr[64];
+
+__global__ void k_sqrt_scalar(double *x) { *x = sqrt(*x); }
+
+// Device address of the static scratch array on `device` (the current device),
+// looked up once per device on the first call there.
+static int noalloc_scratch(int device, double **out)
+{
+  if (device < 0 || device >= 64) return fail(MPDG_ERR_INVALID_ARGUMENT, "device id");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[device]) {
+    double *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(MPDG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_addr[device] = p;
+  }
+  *out = g_noalloc_addr[device];
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_l2_norm_noalloc(mpdg_heat *h, const double *u, double *norm)
+{
+  if (!h || !u || !norm) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  double *scratch = nullptr;
+  TRY(noalloc_scratch(h->device, &scratch));
+  int max_ctas_per_sm = 32;
+  cudaDeviceGetAttribute(&max_ctas_per_sm, cudaDevAttrMaxBlocksPerMultiprocessor, h->device);
+  const int64_t batches = (h->n_cells + cells_per_block(h->n) - 1) / cells_per_block(h->n);
+  const int64_t slots = std::min<int64_t>(batches, (int64_t)max_ctas_per_sm * h->sm_count);
+  if (slots > kNoAllocSlots)
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "l2_norm_noalloc: the reduction needs " + std::to_string(slots) +
+                  " partial sums, the static scratch holds " + std::to_string(kNoAllocSlots));
+  unsigned *counter = reinterpret_cast<unsigned *>(scratch + kNoAllocSlots);
+  CU(cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream));
+  CellArgs<double> a = cell_args<double>(h);
+  a.g.q = h->geoq;
+  a.src = u;
+  a.out = norm;
+  a.partials = scratch;
+  a.counter = counter;
+  CU(h->tab.norm(a, h->geo, 0, h->stream, h->sm_count));
+  k_sqrt_scalar<<<1, 1, 0, h->stream>>>(norm);
+  CU(cudaGetLastError());
+  h->launches += 2;
   return MPDG_OK;
 }

@@ -1,0 +1,373 @@
+// Register-resident cell kernel for the operator application (n = p + 1 <= 5).
+//
+// Layout: every cell gets n threads of one warp (32/n cells per warp); thread t
+// holds one 2D plane of the cell's n^3 tensor in registers:
+//   Z-layout  thread t holds P[j][i] = u(i, j, k = t)   (x and y in registers)
+//   X-layout  thread t holds Q[k][j] = u(i = t, j, k)   (y and z in registers)
+// so x/y contractions run on Z-planes and y/z contractions on X-planes without
+// touching shared memory. Switching layouts goes through a per-cell shared
+// buffer buf[k][j][i] (plane stride n^2+1, cell stride = 4 mod 16 doubles),
+// which keeps both the plane-wise writes and the strided reads free of bank
+// conflicts. A cell never spans two warps, so __syncwarp is the only barrier.
+//
+// Operator application per cell (TDEP = temperature-dependent law):
+//   T_lin: gather Z, S_x S_y, copy D_x, Z->X (2 planes), S_z (2), D_y, D_z
+//          -> per-point coefficients k, dk dT/dxi_d (staged in a thread-private
+//             interleaved shared area: the same thread writes and reads them)
+//   u:     gather Z (masked), S_x S_y, copy D_x, Z->X (2), S_z (2), D_y, D_z
+//   q-op:  val = c u JxW, f = G (k grad u + dk u grad T)   (pointwise, X)
+//   integ: t = val + D_y^T f_y + D_z^T f_z, S_z^T t, S_z^T f_x, X->Z (2),
+//          w = t + D_x^T f_x, S_x^T, S_y^T, atomic scatter of plane t
+// i.e. 21 1D sweeps and 6 layout switches per cell for k(T), 14 and 4 without.
+#pragma once
+
+#include "cell_kernels.cuh"
+
+namespace mpdg {
+
+template <int n> __host__ __device__ constexpr int v2_cells_per_warp() { return 32 / n; }
+template <int n> __host__ __device__ constexpr int v2_plane_stride() { return n * n + 1; }
+template <int n> __host__ __device__ constexpr int v2_cell_stride()
+{
+  int s = n * v2_plane_stride<n>();
+  while (s % 16 != 4) ++s;
+  return s;
+}
+template <int LAW> __host__ __device__ constexpr int v2_ncoef() { return LAW == 0 ? 0 : (LAW == 1 ? 4 : 5); }
+constexpr int kV2Warps = 2;  // warps per CTA
+template <int n, typename T, int LAW> __host__ __device__ constexpr size_t v2_smem_per_warp()
+{
+  return sizeof(T) * ((size_t)2 * (v2_cells_per_warp<n>() + 1) * v2_cell_stride<n>() +
+                      (size_t)v2_ncoef<LAW>() * n * n * 32);
+}
+template <int n, typename T, int LAW> __host__ __device__ constexpr size_t v2_smem()
+{
+  return kV2Warps * v2_smem_per_warp<n, T, LAW>();
+}
+
+// 1D contraction of matrix `kind` along the second index of A[a][b] for every a
+// (B may alias A).
+template <int n, int kind, bool add, typename T>
+__device__ __forceinline__ void psweep_b(const T (&A)[n][n], T (&B)[n][n])
+{
+  constexpr int h = n / 2;
+  constexpr int off = tab_off(n, kind);
+  constexpr int sym = kind_sym(kind);
+#pragma unroll
+  for (int a = 0; a < n; ++a) {
+    T x[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i] = A[a][i];
+    T e[h], o[h];
+#pragma unroll
+    for (int l = 0; l < h; ++l) {
+      e[l] = x[l] + x[n - 1 - l];
+      o[l] = x[l] - x[n - 1 - l];
+    }
+#pragma unroll
+    for (int q = 0; q < h + (n & 1); ++q) {
+      T E = (n & 1) ? ctab<T>(off + 2 * n * h + q) * x[h] : ctab<T>(off + q * h) * e[0];
+      T O = ctab<T>(off + n * h + q * h) * o[0];
+#pragma unroll
+      for (int l = (n & 1) ? 0 : 1; l < h; ++l) E = fma(ctab<T>(off + q * h + l), e[l], E);
+#pragma unroll
+      for (int l = 1; l < h; ++l) O = fma(ctab<T>(off + n * h + q * h + l), o[l], O);
+      if (q < h) {
+        const T y0 = E + O, y1 = sym > 0 ? E - O : O - E;
+        B[a][q] = add ? B[a][q] + y0 : y0;
+        B[a][n - 1 - q] = add ? B[a][n - 1 - q] + y1 : y1;
+      } else {
+        B[a][q] = add ? B[a][q] + (E + O) : (E + O);
+      }
+    }
+  }
+}
+
+// 1D contraction along the first index of A[a][b] for every b (B may alias A).
+template <int n, int kind, bool add, typename T>
+__device__ __forceinline__ void psweep_a(const T (&A)[n][n], T (&B)[n][n])
+{
+  constexpr int h = n / 2;
+  constexpr int off = tab_off(n, kind);
+  constexpr int sym = kind_sym(kind);
+#pragma unroll
+  for (int b = 0; b < n; ++b) {
+    T x[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i] = A[i][b];
+    T e[h], o[h];
+#pragma unroll
+    for (int l = 0; l < h; ++l) {
+      e[l] = x[l] + x[n - 1 - l];
+      o[l] = x[l] - x[n - 1 - l];
+    }
+#pragma unroll
+    for (int q = 0; q < h + (n & 1); ++q) {
+      T E = (n & 1) ? ctab<T>(off + 2 * n * h + q) * x[h] : ctab<T>(off + q * h) * e[0];
+      T O = ctab<T>(off + n * h + q * h) * o[0];
+#pragma unroll
+      for (int l = (n & 1) ? 0 : 1; l < h; ++l) E = fma(ctab<T>(off + q * h + l), e[l], E);
+#pragma unroll
+      for (int l = 1; l < h; ++l) O = fma(ctab<T>(off + n * h + q * h + l), o[l], O);
+      if (q < h) {
+        const T y0 = E + O, y1 = sym > 0 ? E - O : O - E;
+        B[q][b] = add ? B[q][b] + y0 : y0;
+        B[n - 1 - q][b] = add ? B[n - 1 - q][b] + y1 : y1;
+      } else {
+        B[q][b] = add ? B[q][b] + (E + O) : (E + O);
+      }
+    }
+  }
+}
+
+// Layout switches through the per-cell shared buffer buf[k][j][i].
+// Z -> X: thread t writes plane k = t, then reads column i = t.
+template <int n, typename T>
+__device__ __forceinline__ void z_to_x1(const T (&A)[n][n], T (&QA)[n][n], T *ba, int t)
+{
+  constexpr int PS = v2_plane_stride<n>();
+#pragma unroll
+  for (int j = 0; j < n; ++j)
+#pragma unroll
+    for (int i = 0; i < n; ++i) ba[t * PS + j * n + i] = A[j][i];
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < n; ++k)
+#pragma unroll
+    for (int j = 0; j < n; ++j) QA[k][j] = ba[k * PS + j * n + t];
+  __syncwarp();
+}
+
+template <int n, typename T>
+__device__ __forceinline__ void z_to_x2(const T (&A)[n][n], const T (&B)[n][n], T (&QA)[n][n],
+                                        T (&QB)[n][n], T *ba, T *bb, int t)
+{
+  constexpr int PS = v2_plane_stride<n>();
+#pragma unroll
+  for (int j = 0; j < n; ++j)
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+      ba[t * PS + j * n + i] = A[j][i];
+      bb[t * PS + j * n + i] = B[j][i];
+    }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < n; ++k)
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      QA[k][j] = ba[k * PS + j * n + t];
+      QB[k][j] = bb[k * PS + j * n + t];
+    }
+  __syncwarp();
+}
+
+// X -> Z: thread t writes column i = t, then reads plane k = t.
+template <int n, typename T>
+__device__ __forceinline__ void x_to_z2(const T (&QA)[n][n], const T (&QB)[n][n], T (&A)[n][n],
+                                        T (&B)[n][n], T *ba, T *bb, int t)
+{
+  constexpr int PS = v2_plane_stride<n>();
+#pragma unroll
+  for (int k = 0; k < n; ++k)
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      ba[k * PS + j * n + t] = QA[k][j];
+      bb[k * PS + j * n + t] = QB[k][j];
+    }
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < n; ++j)
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+      A[j][i] = ba[t * PS + j * n + i];
+      B[j][i] = bb[t * PS + j * n + i];
+    }
+  __syncwarp();
+}
+
+// gather plane k = K of a cell (Z-layout), optionally masked
+template <int n, typename T>
+__device__ __forceinline__ void gather_plane(const MeshDims &d, int64_t base, int I0, int J0, int K,
+                                             bool masked, const T *__restrict__ g, T (&P)[n][n],
+                                             bool active)
+{
+#pragma unroll
+  for (int j = 0; j < n; ++j) {
+    const int64_t row = base + (int64_t)d.nd[0] * j;
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+      T v = T(0);
+      if (active) {
+        v = __ldg(g + row + i);
+        if (masked && constrained(d, I0 + i, J0 + j, K)) v = T(0);
+      }
+      P[j][i] = v;
+    }
+  }
+}
+
+template <int n, typename T, int GEO, int LAW>
+__global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
+{
+  constexpr int CW = v2_cells_per_warp<n>();
+  constexpr int CS = v2_cell_stride<n>();
+  constexpr int NCOEF = v2_ncoef<LAW>();
+  constexpr bool TDEP = LAW != 0;
+  if (a.st && a.st->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cw = lane / n, t = lane % n;
+  const bool lane_ok = cw < CW;
+  T *wbuf = reinterpret_cast<T *>(smem_raw) + (size_t)warp * (v2_smem_per_warp<n, T, LAW>() / sizeof(T));
+  T *bufA = wbuf + cw * CS;                     // idle lanes use the spare slot cw == CW
+  T *bufB = wbuf + (CW + 1) * CS + cw * CS;
+  T *coef = wbuf + 2 * (CW + 1) * CS;           // [NCOEF][n*n][32], thread-private columns
+  const MeshDims &d = a.d;
+  double dot = 0.0;
+  const int64_t n_groups = (a.n_cells + CW - 1) / CW;
+  for (int64_t grp = (int64_t)blockIdx.x * kV2Warps + warp; grp < n_groups;
+       grp += (int64_t)gridDim.x * kV2Warps) {
+    const int64_t cell = grp * CW + cw;
+    const bool active = lane_ok && cell < a.n_cells;
+    const int64_t cc = active ? cell : 0;
+    const int cx = (int)(cc % d.m[0]);
+    const int cy = (int)((cc / d.m[0]) % d.m[1]);
+    const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
+    const int I0 = d.p * cx, J0 = d.p * cy, K = d.p * cz + t;
+    const int64_t base = (int64_t)d.nd[0] * (J0 + (int64_t)d.nd[1] * K) + I0;
+
+    if (TDEP) {
+      // ---- linearisation point: values and reference gradients at the q-points
+      T P[n][n], Dx[n][n];
+      gather_plane<n>(d, base, I0, J0, K, false, a.Tl, P, active);
+      psweep_b<n, kS, false>(P, P);
+      psweep_a<n, kS, false>(P, P);
+      psweep_b<n, kD, false>(P, Dx);
+      T Tq[n][n], Tx[n][n];
+      z_to_x2<n>(P, Dx, Tq, Tx, bufA, bufB, t);
+      psweep_a<n, kS, false>(Tq, Tq);
+      psweep_a<n, kS, false>(Tx, Tx);
+      T Ty[n][n], Tz[n][n];
+      psweep_b<n, kD, false>(Tq, Ty);
+      psweep_a<n, kD, false>(Tq, Tz);
+      T To[n][n];
+      if (LAW == 2 && a.m.need_told) {
+        gather_plane<n>(d, base, I0, J0, K, false, a.To, P, active);
+        psweep_b<n, kS, false>(P, P);
+        psweep_a<n, kS, false>(P, P);
+        z_to_x1<n>(P, To, bufA, t);
+        psweep_a<n, kS, false>(To, To);
+      }
+#pragma unroll
+      for (int k = 0; k < n; ++k)
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          T rhocp, kk, drhocp, dk;
+          mat_eval<LAW>(a.m, Tq[k][j], rhocp, kk, drhocp, dk);
+          const int pt = k * n + j;
+          coef[(0 * n * n + pt) * 32 + lane] = kk;
+          coef[(1 * n * n + pt) * 32 + lane] = dk * Tx[k][j];
+          coef[(2 * n * n + pt) * 32 + lane] = dk * Ty[k][j];
+          coef[(3 * n * n + pt) * 32 + lane] = dk * Tz[k][j];
+          if (LAW == 2) {
+            T c = a.m.idt * rhocp;
+            if (a.m.need_told) c += a.m.idt * drhocp * (Tq[k][j] - To[k][j]);
+            coef[(4 * n * n + pt) * 32 + lane] = c;
+          }
+        }
+    }
+
+    // ---- operand: values and reference gradients at the q-points
+    T U[n][n], Ux[n][n];
+    {
+      T P[n][n], Dx[n][n];
+      gather_plane<n>(d, base, I0, J0, K, true, a.src, P, active);
+      psweep_b<n, kS, false>(P, P);
+      psweep_a<n, kS, false>(P, P);
+      psweep_b<n, kD, false>(P, Dx);
+      z_to_x2<n>(P, Dx, U, Ux, bufA, bufB, t);
+    }
+    psweep_a<n, kS, false>(U, U);
+    psweep_a<n, kS, false>(Ux, Ux);
+    T Uy[n][n], Uz[n][n];
+    psweep_b<n, kD, false>(U, Uy);
+    psweep_a<n, kD, false>(U, Uz);
+
+    // ---- quadrature-point operation (tangent_local_cell_operation)
+#pragma unroll
+    for (int k = 0; k < n; ++k)
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        T jxw, G[6];
+        geo_at<n, GEO>(a.g, cc, t, j, k, jxw, G);
+        const T uu = U[k][j];
+        T kk, cval;
+        T f0, f1, f2;
+        if (TDEP) {
+          const int pt = k * n + j;
+          kk = coef[(0 * n * n + pt) * 32 + lane];
+          f0 = kk * Ux[k][j] + coef[(1 * n * n + pt) * 32 + lane] * uu;
+          f1 = kk * Uy[k][j] + coef[(2 * n * n + pt) * 32 + lane] * uu;
+          f2 = kk * Uz[k][j] + coef[(3 * n * n + pt) * 32 + lane] * uu;
+          cval = LAW == 2 ? coef[(4 * n * n + pt) * 32 + lane] : a.m.idt * (a.m.rho_l * a.m.cp_l);
+        } else {
+          kk = a.m.k_l;
+          f0 = kk * Ux[k][j];
+          f1 = kk * Uy[k][j];
+          f2 = kk * Uz[k][j];
+          cval = a.m.idt * (a.m.rho_l * a.m.cp_l);
+        }
+        T F0, F1, F2;
+        apply_G<GEO>(G, f0, f1, f2, F0, F1, F2);
+        U[k][j] = cval * uu * jxw;
+        Ux[k][j] = F0;
+        Uy[k][j] = F1;
+        Uz[k][j] = F2;
+      }
+
+    // ---- integration
+    psweep_b<n, kDT, true>(Uy, U);
+    psweep_a<n, kDT, true>(Uz, U);
+    psweep_a<n, kST, false>(U, U);
+    psweep_a<n, kST, false>(Ux, Ux);
+    T W[n][n], Wx[n][n];
+    x_to_z2<n>(U, Ux, W, Wx, bufA, bufB, t);
+    psweep_b<n, kDT, true>(Wx, W);
+    psweep_b<n, kST, false>(W, W);
+    psweep_a<n, kST, false>(W, W);
+
+    // ---- scatter (constrained rows skipped) and the optional src.dst partial
+    if (active) {
+      const bool want_dot = a.fin != FIN_NONE;
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const int64_t row = base + (int64_t)d.nd[0] * j;
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+          const bool c = constrained(d, I0 + i, J0 + j, K);
+          if (!c) atomic_add(a.dst + row + i, W[j][i]);
+          if (want_dot && !c) dot += (double)__ldg(a.src + row + i) * (double)W[j][i];
+        }
+      }
+    }
+  }
+  if (a.fin != FIN_NONE) {
+    double v[1] = {dot}, tot[1];
+    if (grid_sum<1>(v, a.partials, a.counter, tot)) {
+      if (a.fin == FIN_STORE) {
+        *a.out = tot[0];
+      } else {
+        SolverState *s = a.st;
+        s->pAp = tot[0];
+        if (!(tot[0] > 0.0) || !isfinite(tot[0])) {
+          s->done = 2;
+          s->status = 5;
+        } else {
+          s->alpha = s->rz / tot[0];
+        }
+      }
+    }
+  }
+}
+
+}  // namespace mpdg

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "cell_kernels.cuh"
+#include "cell_kernels_v2.cuh"
 #include "degree_table.hpp"
 
 namespace mpdg {
@@ -39,9 +40,26 @@ struct DegreeOps {
     cudaMemcpyToSymbol(c_w_f, wf, sizeof(float) * kWSize);
   }
 
+  // register-resident kernel where a cell's planes fit the register file
+  template <typename T>
+  static constexpr bool use_v2()
+  {
+    return sizeof(T) == 8 ? n <= 4 : n <= 5;
+  }
+
   template <typename T, int GEO, int LAW>
   static cudaError_t vmult_t(const CellArgs<T> &a, cudaStream_t s, int sm)
   {
+    if constexpr (use_v2<T>()) {
+      static int cache2 = 0;
+      auto k2 = k_vmult2<n, T, GEO, LAW>;
+      const size_t smem2 = v2_smem<n, T, LAW>();
+      const int64_t ng = (a.n_cells + v2_cells_per_warp<n>() - 1) / v2_cells_per_warp<n>();
+      const int g2 = persistent_grid(k2, 32 * kV2Warps, smem2, (ng + kV2Warps - 1) / kV2Warps, sm,
+                                     &cache2);
+      k2<<<g2, 32 * kV2Warps, smem2, s>>>(a);
+      return cudaGetLastError();
+    }
     static int cache = 0;
     auto k = k_vmult<n, T, GEO, LAW>;
     const size_t smem = smem_vmult<n, T>(LAW != 0);

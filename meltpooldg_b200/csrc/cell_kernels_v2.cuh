@@ -185,9 +185,42 @@ __device__ __forceinline__ void x_to_z2(const T (&QA)[n][n], const T (&QB)[n][n]
   __syncwarp();
 }
 
+// Dirichlet test of the DoFs of plane K of cell (I0, J0): face flags per row, the
+// x faces only at i = 0 and i = n - 1.
+struct PlaneMask {
+  bool plane, xlo, xhi, ylo, yhi;
+  __device__ __forceinline__ PlaneMask(const MeshDims &d, int I0, int J0, int K, int p)
+  {
+    plane = ((d.dmask & 16) && K == 0) || ((d.dmask & 32) && K == d.nd[2] - 1);
+    xlo = (d.dmask & 1) && I0 == 0;
+    xhi = (d.dmask & 2) && I0 + p == d.nd[0] - 1;
+    ylo = (d.dmask & 4) && J0 == 0;
+    yhi = (d.dmask & 8) && J0 + p == d.nd[1] - 1;
+  }
+  template <int n>
+  __device__ __forceinline__ bool at(int i, int j) const
+  {
+    return plane || (j == 0 && ylo) || (j == n - 1 && yhi) || (i == 0 && xlo) ||
+           (i == n - 1 && xhi);
+  }
+};
+
+// L2 prefetch of the n rows (n values each) of plane K of a cell
+template <int n, typename T>
+__device__ __forceinline__ void prefetch_plane(const T *g, int64_t base, int nd0)
+{
+#pragma unroll
+  for (int j = 0; j < n; ++j) {
+    const T *row = g + base + (int64_t)nd0 * j;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(row));
+    if ((reinterpret_cast<uintptr_t>(row) & 127) + n * sizeof(T) > 128)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(row + n - 1));
+  }
+}
+
 // gather plane k = K of a cell (Z-layout), optionally masked
 template <int n, typename T>
-__device__ __forceinline__ void gather_plane(const MeshDims &d, int64_t base, int I0, int J0, int K,
+__device__ __forceinline__ void gather_plane(const MeshDims &d, int64_t base, const PlaneMask &pm,
                                              bool masked, const T *__restrict__ g, T (&P)[n][n],
                                              bool active)
 {
@@ -199,7 +232,7 @@ __device__ __forceinline__ void gather_plane(const MeshDims &d, int64_t base, in
       T v = T(0);
       if (active) {
         v = __ldg(g + row + i);
-        if (masked && constrained(d, I0 + i, J0 + j, K)) v = T(0);
+        if (masked && pm.template at<n>(i, j)) v = T(0);
       }
       P[j][i] = v;
     }
@@ -235,11 +268,39 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
     const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
     const int I0 = d.p * cx, J0 = d.p * cy, K = d.p * cz + t;
     const int64_t base = (int64_t)d.nd[0] * (J0 + (int64_t)d.nd[1] * K) + I0;
+    const PlaneMask pm(d, I0, J0, K, d.p);
+
+    // both gathers first so their latencies overlap
+    T Pu[n][n];
+    gather_plane<n>(d, base, pm, true, a.src, Pu, active);
+    T Pt[n][n];
+    if (TDEP) gather_plane<n>(d, base, pm, false, a.Tl, Pt, active);
+
+    // L2 prefetch of the next group's rows (and geometry) while this one computes
+    {
+      const int64_t ncell = cell + (int64_t)gridDim.x * kV2Warps * CW;
+      if (lane_ok && ncell < a.n_cells) {
+        const int ncx = (int)(ncell % d.m[0]);
+        const int ncy = (int)((ncell / d.m[0]) % d.m[1]);
+        const int ncz = (int)(ncell / ((int64_t)d.m[0] * d.m[1]));
+        const int64_t nbase =
+          (int64_t)d.nd[0] * (d.p * ncy + (int64_t)d.nd[1] * (d.p * ncz + t)) + d.p * ncx;
+        prefetch_plane<n>(a.src, nbase, d.nd[0]);
+        if (TDEP) prefetch_plane<n>(a.Tl, nbase, d.nd[0]);
+        if (GEO == 1) {
+          constexpr int npt = n * n * n;
+          const char *gq = reinterpret_cast<const char *>(a.g.q + ncell * 7 * npt);
+          constexpr int bytes = 7 * npt * (int)sizeof(T);
+          for (int off = t * 128; off < bytes; off += n * 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(gq + off));
+        }
+      }
+    }
 
     if (TDEP) {
       // ---- linearisation point: values and reference gradients at the q-points
-      T P[n][n], Dx[n][n];
-      gather_plane<n>(d, base, I0, J0, K, false, a.Tl, P, active);
+      T (&P)[n][n] = Pt;
+      T Dx[n][n];
       psweep_b<n, kS, false>(P, P);
       psweep_a<n, kS, false>(P, P);
       psweep_b<n, kD, false>(P, Dx);
@@ -252,7 +313,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
       psweep_a<n, kD, false>(Tq, Tz);
       T To[n][n];
       if (LAW == 2 && a.m.need_told) {
-        gather_plane<n>(d, base, I0, J0, K, false, a.To, P, active);
+        gather_plane<n>(d, base, pm, false, a.To, P, active);
         psweep_b<n, kS, false>(P, P);
         psweep_a<n, kS, false>(P, P);
         z_to_x1<n>(P, To, bufA, t);
@@ -280,12 +341,11 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
     // ---- operand: values and reference gradients at the q-points
     T U[n][n], Ux[n][n];
     {
-      T P[n][n], Dx[n][n];
-      gather_plane<n>(d, base, I0, J0, K, true, a.src, P, active);
-      psweep_b<n, kS, false>(P, P);
-      psweep_a<n, kS, false>(P, P);
-      psweep_b<n, kD, false>(P, Dx);
-      z_to_x2<n>(P, Dx, U, Ux, bufA, bufB, t);
+      T Dx[n][n];
+      psweep_b<n, kS, false>(Pu, Pu);
+      psweep_a<n, kS, false>(Pu, Pu);
+      psweep_b<n, kD, false>(Pu, Dx);
+      z_to_x2<n>(Pu, Dx, U, Ux, bufA, bufB, t);
     }
     psweep_a<n, kS, false>(U, U);
     psweep_a<n, kS, false>(Ux, Ux);
@@ -344,7 +404,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
         const int64_t row = base + (int64_t)d.nd[0] * j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-          const bool c = constrained(d, I0 + i, J0 + j, K);
+          const bool c = pm.template at<n>(i, j);
           if (!c) atomic_add(a.dst + row + i, W[j][i]);
           if (want_dot && !c) dot += (double)__ldg(a.src + row + i) * (double)W[j][i];
         }

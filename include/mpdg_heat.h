@@ -93,6 +93,11 @@ typedef struct {
   double cheb_max_factor;     /* upper bound = factor * estimated lambda_max        */
   double cheb_min_fraction;   /* lower bound = max(lambda_min estimate, fraction*upper) */
   double tol_reference_norm;  /* > 0: stop when |r| <= rel_tolerance * this value   */
+  int    cheb_picard;         /* 1: the FP32 Chebyshev applies the Picard operator
+                                 (conductivity k(T_lin) at the q-points, no dk/dT term);
+                                 the outer FP64 CG keeps the exact tangent          */
+  int    cheb_eig_reuse;      /* 1: keep the Chebyshev interval across solves and
+                                 time steps until the material or the mesh changes  */
 } mpdg_solver_params;
 
 typedef struct {

@@ -49,7 +49,8 @@ class SolverParams(C.Structure):
                 ("rel_tolerance", C.c_double), ("abs_tolerance", C.c_double),
                 ("gmres_restart", C.c_int), ("cheb_degree", C.c_int),
                 ("cheb_eig_iterations", C.c_int), ("cheb_max_factor", C.c_double),
-                ("cheb_min_fraction", C.c_double), ("tol_reference_norm", C.c_double)]
+                ("cheb_min_fraction", C.c_double), ("tol_reference_norm", C.c_double),
+                ("cheb_picard", C.c_int), ("cheb_eig_reuse", C.c_int)]
 
 
 class SolveStats(C.Structure):

@@ -53,6 +53,7 @@ struct CellArgs {
   const T *__restrict__ Tl;
   const T *__restrict__ To;
   const T *__restrict__ qs;
+  const float *__restrict__ kq;  // per-q conductivity [cell][n^3] (coefficient-field operator)
   double *partials;    // per-CTA partial sums
   unsigned *counter;   // last-CTA election counter (reset by the last CTA)
   SolverState *st;     // early exit when st->done; alpha finalisation

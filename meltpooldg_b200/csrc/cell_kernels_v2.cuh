@@ -33,7 +33,7 @@ template <int n> __host__ __device__ constexpr int v2_cell_stride()
   while (s % 16 != 4) ++s;
   return s;
 }
-template <int LAW> __host__ __device__ constexpr int v2_ncoef() { return LAW == 0 ? 0 : (LAW == 1 ? 4 : 5); }
+template <int LAW> __host__ __device__ constexpr int v2_ncoef() { return (LAW == 0 || LAW == 3) ? 0 : (LAW == 1 ? 4 : 5); }
 constexpr int kV2Warps = 2;  // warps per CTA
 template <int n, typename T, int LAW> __host__ __device__ constexpr size_t v2_smem_per_warp()
 {
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
   constexpr int CW = v2_cells_per_warp<n>();
   constexpr int CS = v2_cell_stride<n>();
   constexpr int NCOEF = v2_ncoef<LAW>();
-  constexpr bool TDEP = LAW != 0;
+  constexpr bool TDEP = LAW == 1 || LAW == 2;  // LAW 3: conductivity field k(q), no tangent
   if (a.st && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -287,6 +287,8 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           (int64_t)d.nd[0] * (d.p * ncy + (int64_t)d.nd[1] * (d.p * ncz + t)) + d.p * ncx;
         prefetch_plane<n>(a.src, nbase, d.nd[0]);
         if (TDEP) prefetch_plane<n>(a.Tl, nbase, d.nd[0]);
+        if (LAW == 3 && t == 0)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.kq + ncell * (n * n * n)));
         if (GEO == 1) {
           constexpr int npt = n * n * n;
           const char *gq = reinterpret_cast<const char *>(a.g.q + ncell * 7 * npt);
@@ -371,7 +373,10 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           f2 = kk * Uz[k][j] + coef[(3 * n * n + pt) * 32 + lane] * uu;
           cval = LAW == 2 ? coef[(4 * n * n + pt) * 32 + lane] : a.m.idt * (a.m.rho_l * a.m.cp_l);
         } else {
-          kk = a.m.k_l;
+          if (LAW == 3)
+            kk = (T)__ldg(a.kq + cc * (n * n * n) + t + n * (j + n * k));
+          else
+            kk = a.m.k_l;
           f0 = kk * Ux[k][j];
           f1 = kk * Uy[k][j];
           f2 = kk * Uz[k][j];
@@ -426,6 +431,51 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           s->alpha = s->rz / tot[0];
         }
       }
+    }
+  }
+}
+
+// Conductivity at the quadrature points, kq[cell][q] = k(T_lin(x_q)) in FP32,
+// for the coefficient-field (Picard) operator of the FP32 preconditioner.
+template <int n, int LAW>
+__global__ void __launch_bounds__(32 * kV2Warps) k_conductivity_q(CellArgs<double> a, float *kq)
+{
+  using T = double;
+  constexpr int CW = v2_cells_per_warp<n>();
+  constexpr int CS = v2_cell_stride<n>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cw = lane / n, t = lane % n;
+  const bool lane_ok = cw < CW;
+  T *bufA = reinterpret_cast<T *>(smem_raw) + (size_t)warp * (CW + 1) * CS + cw * CS;
+  const MeshDims &d = a.d;
+  const int64_t n_groups = (a.n_cells + CW - 1) / CW;
+  for (int64_t grp = (int64_t)blockIdx.x * kV2Warps + warp; grp < n_groups;
+       grp += (int64_t)gridDim.x * kV2Warps) {
+    const int64_t cell = grp * CW + cw;
+    const bool active = lane_ok && cell < a.n_cells;
+    const int64_t cc = active ? cell : 0;
+    const int cx = (int)(cc % d.m[0]);
+    const int cy = (int)((cc / d.m[0]) % d.m[1]);
+    const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
+    const int I0 = d.p * cx, J0 = d.p * cy, K = d.p * cz + t;
+    const int64_t base = (int64_t)d.nd[0] * (J0 + (int64_t)d.nd[1] * K) + I0;
+    const PlaneMask pm(d, I0, J0, K, d.p);
+    T P[n][n], Q[n][n];
+    gather_plane<n>(d, base, pm, false, a.Tl, P, active);
+    psweep_b<n, kS, false>(P, P);
+    psweep_a<n, kS, false>(P, P);
+    z_to_x1<n>(P, Q, bufA, t);
+    psweep_a<n, kS, false>(Q, Q);
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < n; ++k)
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          T rhocp, kk, drhocp, dk;
+          mat_eval<LAW>(a.m, Q[k][j], rhocp, kk, drhocp, dk);
+          kq[cc * (n * n * n) + t + n * (j + n * k)] = (float)kk;
+        }
     }
   }
 }

@@ -59,18 +59,26 @@ struct DegreeOps {
                                      &cache2);
       k2<<<g2, 32 * kV2Warps, smem2, s>>>(a);
       return cudaGetLastError();
+    } else {
+      static int cache = 0;
+      auto k = k_vmult<n, T, GEO, LAW>;
+      const size_t smem = smem_vmult<n, T>(LAW != 0);
+      const int64_t nb = (a.n_cells + CPB - 1) / CPB;
+      const int g = persistent_grid(k, THREADS, smem, nb, sm, &cache);
+      k<<<g, THREADS, smem, s>>>(a);
+      return cudaGetLastError();
     }
-    static int cache = 0;
-    auto k = k_vmult<n, T, GEO, LAW>;
-    const size_t smem = smem_vmult<n, T>(LAW != 0);
-    const int64_t nb = (a.n_cells + CPB - 1) / CPB;
-    const int g = persistent_grid(k, THREADS, smem, nb, sm, &cache);
-    k<<<g, THREADS, smem, s>>>(a);
-    return cudaGetLastError();
   }
   template <typename T>
   static cudaError_t vmult(const CellArgs<T> &a, int geo, int law, cudaStream_t s, int sm)
   {
+    if (law == 3) {
+      if constexpr (use_v2<T>()) {
+        return geo == 0 ? vmult_t<T, 0, 3>(a, s, sm) : vmult_t<T, 1, 3>(a, s, sm);
+      } else {
+        return cudaErrorNotSupported;
+      }
+    }
     if (geo == 0) {
       if (law == 0) return vmult_t<T, 0, 0>(a, s, sm);
       if (law == 1) return vmult_t<T, 0, 1>(a, s, sm);
@@ -148,6 +156,25 @@ struct DegreeOps {
     return geo == 0 ? norm_t<0>(a, s, sm) : norm_t<1>(a, s, sm);
   }
 
+  template <int LAW>
+  static cudaError_t kq_t(const CellArgs<double> &a, float *kq, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_conductivity_q<n, LAW>;
+    const size_t smem = sizeof(double) * kV2Warps * (v2_cells_per_warp<n>() + 1) * v2_cell_stride<n>();
+    const int64_t ng = (a.n_cells + v2_cells_per_warp<n>() - 1) / v2_cells_per_warp<n>();
+    const int g = persistent_grid(k, 32 * kV2Warps, smem, (ng + kV2Warps - 1) / kV2Warps, sm, &cache);
+    k<<<g, 32 * kV2Warps, smem, s>>>(a, kq);
+    return cudaGetLastError();
+  }
+  static cudaError_t conductivity_q(const CellArgs<double> &a, float *kq, int law, cudaStream_t s,
+                                    int sm)
+  {
+    if (law == 0) return kq_t<0>(a, kq, s, sm);
+    if (law == 1) return kq_t<1>(a, kq, s, sm);
+    return kq_t<2>(a, kq, s, sm);
+  }
+
   static DegreeTable table()
   {
     DegreeTable t;
@@ -158,6 +185,7 @@ struct DegreeOps {
     t.rhs = &rhs;
     t.diag = &diag;
     t.norm = &norm;
+    if constexpr (use_v2<float>()) t.conductivity_q = &conductivity_q;
     return t;
   }
 };

@@ -15,6 +15,9 @@ struct DegreeTable {
   cudaError_t (*rhs)(const CellArgs<double> &, int geo, int law, cudaStream_t, int sm) = nullptr;
   cudaError_t (*diag)(const CellArgs<double> &, int geo, int law, cudaStream_t, int sm) = nullptr;
   cudaError_t (*norm)(const CellArgs<double> &, int geo, int law, cudaStream_t, int sm) = nullptr;
+  // kq[cell][q] = k(T_lin) in FP32; nullptr where the degree has no register-resident kernel
+  cudaError_t (*conductivity_q)(const CellArgs<double> &, float *kq, int law, cudaStream_t,
+                                int sm) = nullptr;
 };
 
 DegreeTable degree_table_2();

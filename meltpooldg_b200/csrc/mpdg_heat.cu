@@ -90,6 +90,7 @@ struct mpdg_heat {
   bool diag_valid = false, diag_f_dirty = true;
   double eig_min = 0.0, eig_max = 0.0;
   bool eig_valid = false;
+  float *kq = nullptr;  // FP32 conductivity at the q-points (Picard preconditioner operator)
   // reduction scratch
   double *partials = nullptr;
   unsigned *counter = nullptr;
@@ -761,12 +762,14 @@ static int refresh_f32(mpdg_heat *h)
   return MPDG_OK;
 }
 
-static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *st)
+static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *st,
+                      bool picard = false)
 {
   TRY(ensure_dt(h));
   TRY(ensure_lin(h));
   TRY(refresh_f32(h));
   CellArgs<float> a = cell_args<float>(h);
+  a.kq = h->kq;
   a.g.q = h->geoq_f;
   a.src = src;
   a.dst = dst;
@@ -779,7 +782,7 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
     e1 = take_event(h);
     cudaEventRecord(e0, h->stream);
   }
-  CU(h->tab.vmult_f(a, h->geo, h->law, h->stream, h->sm_count));
+  CU(h->tab.vmult_f(a, h->geo, picard ? 3 : h->law, h->stream, h->sm_count));
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
     h->ev32.push_back({e0, e1});
@@ -942,7 +945,15 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     CU(cudaGetLastError());
     h->diag_f_dirty = false;
   }
-  if (!h->eig_valid) {
+  const bool picard = prm->cheb_picard && h->law == MPDG_LAW_LINEAR_K && h->tab.conductivity_q;
+  if (picard) {
+    TRY(dvec(h, &h->kq, h->n_cells * h->npt));
+    CellArgs<double> a = cell_args<double>(h);
+    a.Tl = h->T_lin;
+    CU(h->tab.conductivity_q(a, h->kq, h->law, h->stream, h->sm_count));
+    ++h->launches;
+  }
+  if (!h->eig_valid || !prm->cheb_eig_reuse) {
     TRY(estimate_eigenvalues(h, prm->cheb_eig_iterations, &h->eig_min, &h->eig_max));
     h->eig_valid = true;
   }
@@ -979,7 +990,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     if (res0 < 0.0) res0 = h->st_host->res0;
     auto precondition = [&]() -> int {
       for (int j = 1; j <= k; ++j) {
-        TRY(op_apply_f(h, h->Ax32, h->x32, h->st));
+        TRY(op_apply_f(h, h->Ax32, h->x32, h->st, picard));
         if (j < k) {
           k_cheb_step<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
                                                c1[j], c2[j], h->st);
@@ -1499,8 +1510,8 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
   memset(&s, 0, sizeof(s));
   int rc = MPDG_OK;
   do {
+    if (h->dt != dt || !prm->linear.cheb_eig_reuse) h->eig_valid = false;
     h->dt = dt;
-    h->eig_valid = false;
     // init_time_advance: predictor into w1, commit history, constraints
     if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
       k_predict<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, h->w1, dt / dt_old); ++h->launches;

@@ -131,12 +131,15 @@ class LinearSolverData:
     cheb_max_factor: float = 1.2
     cheb_min_fraction: float = 0.0
     tol_reference_norm: float = 0.0
+    cheb_picard: bool = False
+    cheb_eig_reuse: bool = False
 
     def to_c(self) -> L.SolverParams:
         return L.SolverParams(self.solver_type, self.preconditioner_type, self.max_iterations,
                               self.rel_tolerance, self.abs_tolerance, self.gmres_restart,
                               self.cheb_degree, self.cheb_eig_iterations, self.cheb_max_factor,
-                              self.cheb_min_fraction, self.tol_reference_norm)
+                              self.cheb_min_fraction, self.tol_reference_norm,
+                              int(self.cheb_picard), int(self.cheb_eig_reuse))
 
 
 @dataclass

@@ -177,13 +177,17 @@ def test_chebyshev_mixed_precision_cg(degree):
     assert rel(x, x_ref) <= 1e-7
 
 
-def test_chebyshev_mixed_precision_cg_larger_mesh():
-    """Flexible CG + FP32 Chebyshev on a 24^3-cell Q3 heat operator: converges to the
-    FP64 tolerance (true residual) in far fewer outer iterations than Jacobi-CG."""
+@pytest.mark.parametrize("picard", [False, True])
+def test_chebyshev_mixed_precision_cg_larger_mesh(picard):
+    """Flexible CG + FP32 Chebyshev on a 24^3-cell Q3 k(T) tangent at a smooth
+    linearisation point: converges to the FP64 tolerance (true residual) in far fewer
+    outer iterations than Jacobi-CG, with the exact FP32 tangent or the Picard operator
+    in the preconditioner."""
     g = H.HeatDiffuseOperator(H.box_mesh(3, (24, 24, 24)))
     g.set_material(H.material(law=1, k=1.0, k1=0.5))
     g.reset_time_increment(5e-4)
-    T = g.new_vector()
+    T = g.gaussian_source(g.new_vector(), 1.5, (0.5, 0.5, 0.8), 0.15)
+    g.distribute_constraints(T)
     g.set_linearization(T, T)
     H.JacobiPreconditioner(g).update()
     x_src = g.gaussian_source(g.new_vector(), 1.0, (0.5, 0.5, 0.5), 0.2)
@@ -193,7 +197,7 @@ def test_chebyshev_mixed_precision_cg_larger_mesh():
                                  True)
     x = g.new_vector()
     data = H.LinearSolverData(preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32,
-                              rel_tolerance=1e-10)
+                              rel_tolerance=1e-10, cheb_picard=picard)
     its_c = H.LinearSolver.solve(g, x, b, data, True)
     st = H.LinearSolver.last_stats
     assert st.true_residual <= 1e-10 * st.initial_residual * 1.0000001

@@ -31,6 +31,7 @@ METRIC = "Heat step time @1e-8 resid: learned+mixed vs plain FP64 CG; MF vmult G
 DEGREE, CELLS, DT, K1 = 3, 128, 5e-4, 0.5
 AMP, RADIUS, Z0, SPEED, X0 = 500.0, 0.05, 0.95, 1.0, 0.1
 REL_TOL = 1e-8
+CHEB_DEGREE = 6
 
 
 def source_center(t):
@@ -191,8 +192,8 @@ def run_mine(args):
                                    predictor=L.PREDICTOR_LINEAR, single_linearization=True)
     mixed = H.HeatDiffuseOperation(op, H.LinearSolverData(
         preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32, rel_tolerance=REL_TOL,
-        abs_tolerance=0.0, cheb_degree=4), predictor=L.PREDICTOR_LINEAR,
-        single_linearization=True)
+        abs_tolerance=0.0, cheb_degree=CHEB_DEGREE, cheb_picard=True, cheb_eig_reuse=True),
+        predictor=L.PREDICTOR_LINEAR, single_linearization=True)
     q = op.new_vector()
     mixed.heat_source = q
     plain.heat_source = q
@@ -233,16 +234,17 @@ def run_mine(args):
         return ms, its, cnt
 
     W, K = args.warmup, args.steps
-    # plain FP64 Jacobi-CG
-    ms_plain = its_plain = None
-    if not args.no_plain:
-        march(plain, 0, W)
-        ms_plain, its_plain, _ = timed(plain, W, K)
-    # mixed precision (timed region with clock sampling and operator timing)
+    # mixed precision first (timed region with clock sampling and operator timing)
     march(mixed, 0, W)
     clocks = Clocks(local) if rank == 0 else None
     ms_mixed, its_mixed, cnt = timed(mixed, W, K, instrument=True)
     clk = clocks.stop() if clocks else None
+    init_res = mixed.last_stats.initial_relative_residual
+    # plain FP64 Jacobi-CG on the same steps
+    ms_plain = its_plain = None
+    if not args.no_plain:
+        march(plain, 0, W)
+        ms_plain, its_plain, _ = timed(plain, W, K)
     err = None
     if not args.no_plain:
         diff = torch.linalg.vector_norm(mixed.T - plain.T).item()
@@ -305,11 +307,16 @@ def run_mine(args):
 
     # roofline of the dominant kernel in the timed region
     hbm, hbm_kind = peaks()
+    nq = op.n_cells * (DEGREE + 1) ** 3
     if cnt["vmult32_ms"] >= cnt["vmult64_ms"]:
-        kname, s, calls, kms = "k_vmult<4,float,affine,linear_k>", 4, cnt["vmult32_calls"], cnt["vmult32_ms"]
+        # FP32 Picard operator of the preconditioner: src + dst + conductivity per q-point
+        kname = "k_vmult2<4,float,affine,conductivity_field>"
+        calls, kms = cnt["vmult32_calls"], cnt["vmult32_ms"]
+        alg_bytes = 2 * 4 * N + 4 * nq
     else:
-        kname, s, calls, kms = "k_vmult<4,double,affine,linear_k>", 8, cnt["vmult64_calls"], cnt["vmult64_ms"]
-    alg_bytes = 3 * s * N  # src + dst + linearisation point
+        kname = "k_vmult2<4,double,affine,linear_k>"
+        calls, kms = cnt["vmult64_calls"], cnt["vmult64_ms"]
+        alg_bytes = 3 * 8 * N  # src + dst + linearisation point
     per_launch_ms = kms / max(calls, 1)
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     tr = profile_traffic().get(kname)
@@ -337,6 +344,11 @@ def run_mine(args):
         "plain_fp64_ms_per_step": ms_plain / K if ms_plain else None,
         "speedup_mixed_vs_plain": (ms_plain / ms_mixed) if ms_plain else None,
         "cg_iterations_mixed": its_mixed, "cg_iterations_plain": its_plain,
+        "initial_relative_residual_last_step": init_res,
+        "mixed_solver": {"outer": "FP64 flexible CG", "preconditioner":
+                         f"FP32 Chebyshev-Jacobi degree {CHEB_DEGREE}, Picard operator "
+                         "(k(T_lin) at the q-points), interval from 12 Lanczos steps reused "
+                         "across steps", "predictor": "linear extrapolation"},
         "mixed_vs_plain_error": err,
         "vmult_fp64_gdofs": N / (vm_ms / 1e3) / 1e9, "vmult_fp64_ms": vm_ms,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

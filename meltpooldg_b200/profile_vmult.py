@@ -3,6 +3,8 @@
   python -m meltpooldg_b200.profile_vmult --degree 3 --cells 96 --law 1 --reps 3
 prints one JSON line per precision with the CUDA-event time per application,
 DoFs/s and algorithmic GB/s (src + dst + linearisation point [+ per-q geometry]).
+With --solve it instead runs a few outer iterations of FP64 CG with the FP32
+Chebyshev preconditioner on the Picard operator, so that kernel can be captured.
 """
 from __future__ import annotations
 
@@ -22,6 +24,7 @@ def main():
     ap.add_argument("--law", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--dtype", default="both", choices=["f64", "f32", "both"])
+    ap.add_argument("--solve", action="store_true")
     a = ap.parse_args()
     op = H.HeatDiffuseOperator(H.box_mesh(a.degree, (a.cells,) * 3, perturb=a.perturb))
     op.set_material(H.material(law=a.law, k=1.0, k1=0.5))
@@ -31,6 +34,22 @@ def main():
     T = torch.rand(N, dtype=torch.float64, device="cuda", generator=g)
     op.set_linearization(T, T)
     nq = op.n_cells * (a.degree + 1) ** 3
+    if a.solve:
+        from . import _lib as L
+        op.distribute_constraints(T)
+        H.JacobiPreconditioner(op).update()
+        b = op.vmult(op.new_vector(), torch.rand(N, dtype=torch.float64, device="cuda",
+                                                 generator=g))
+        data = H.LinearSolverData(preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32,
+                                  cheb_degree=6, cheb_picard=True, max_iterations=3,
+                                  rel_tolerance=1e-30)
+        try:
+            H.LinearSolver.solve(op, op.new_vector(), b, data, True)
+        except H.ExcNoConvergence:
+            pass
+        torch.cuda.synchronize()
+        print("solve done")
+        return
     for dt in (["f64", "f32"] if a.dtype == "both" else [a.dtype]):
         ty = torch.float64 if dt == "f64" else torch.float32
         s = 8 if dt == "f64" else 4

@@ -91,6 +91,10 @@ struct mpdg_heat {
   double eig_min = 0.0, eig_max = 0.0;
   bool eig_valid = false;
   float *kq = nullptr;  // FP32 conductivity at the q-points (Picard preconditioner operator)
+  // GMRES basis (m + 1 vectors) and small device buffers
+  double *gV = nullptr;
+  int gV_m = 0;
+  double *gsmall = nullptr;
   // reduction scratch
   double *partials = nullptr;
   unsigned *counter = nullptr;
@@ -649,6 +653,73 @@ __global__ void k_cgm_update_p(int64_t N, const double *__restrict__ z, double *
   }
 }
 
+// ---- GMRES building blocks --------------------------------------------------
+constexpr int kMaxBasis = 32;
+
+// out[i] = V_i . w for i < nv (V_i = V + i * ld)
+__global__ void k_multidot(int64_t N, const double *__restrict__ V, int64_t ld, int nv,
+                           const double *__restrict__ w, double *partials, unsigned *counter,
+                           double *out)
+{
+  double v[kMaxBasis];
+#pragma unroll
+  for (int i = 0; i < kMaxBasis; ++i) v[i] = 0.0;
+  GRID_STRIDE(k, N)
+  {
+    const double wk = w[k];
+#pragma unroll
+    for (int i = 0; i < kMaxBasis; ++i)
+      if (i < nv) v[i] += wk * V[(int64_t)i * ld + k];
+  }
+  double tot[kMaxBasis];
+  if (grid_sum<kMaxBasis>(v, partials, counter, tot))
+    for (int i = 0; i < nv; ++i) out[i] = tot[i];
+}
+
+// w -= sum_i c_i V_i (i < nv)
+__global__ void k_multi_axpy(int64_t N, const double *__restrict__ V, int64_t ld, int nv,
+                             const double *__restrict__ c, double *w)
+{
+  GRID_STRIDE(k, N)
+  {
+    double s = w[k];
+    for (int i = 0; i < nv; ++i) s -= c[i] * V[(int64_t)i * ld + k];
+    w[k] = s;
+  }
+}
+
+// v = v * a ; z = D v (or v)
+__global__ void k_scale_precond(int64_t N, double *v, double a, const double *__restrict__ D,
+                                double *z)
+{
+  GRID_STRIDE(k, N)
+  {
+    const double x = v[k] * a;
+    v[k] = x;
+    z[k] = D ? D[k] * x : x;
+  }
+}
+
+// v = b - Ax
+__global__ void k_residual(int64_t N, const double *__restrict__ b, const double *__restrict__ Ax,
+                           double *v)
+{
+  GRID_STRIDE(k, N) v[k] = b[k] - Ax[k];
+}
+
+// x += D (sum_i y_i V_i)
+__global__ void k_gmres_update(int64_t N, const double *__restrict__ V, int64_t ld, int nv,
+                               const double *__restrict__ y, const double *__restrict__ D,
+                               double *x)
+{
+  GRID_STRIDE(k, N)
+  {
+    double s = 0.0;
+    for (int i = 0; i < nv; ++i) s += y[i] * V[(int64_t)i * ld + k];
+    x[k] += D ? D[k] * s : s;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
@@ -1046,6 +1117,138 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     }
     return MPDG_OK;
   }
+}
+
+// ---------------------------------------------------------------------------
+// GMRES(m) with right preconditioning (deal.II SolverGMRES as LinearSolver::solve
+// configures it, linear_solver.hpp:113-118): the monitored quantity is the
+// unpreconditioned residual |b - A x|, estimated by the Givens-rotated
+// least-squares residual. Arnoldi with classical Gram-Schmidt applied twice
+// (one multi-dot and one multi-axpy pass per round); the small Hessenberg
+// problem is solved on the host.
+// ---------------------------------------------------------------------------
+static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
+                 const double *D, mpdg_solve_stats *stats)
+{
+  const int64_t N = h->n_dofs;
+  const int m = std::max(1, std::min(prm->gmres_restart > 0 ? prm->gmres_restart : 28,
+                                     kMaxBasis - 1));
+  if (h->gV && h->gV_m < m) return fail(MPDG_ERR_INVALID_ARGUMENT, "GMRES restart grew");
+  if (!h->gV) {
+    TRY(dvec(h, &h->gV, (int64_t)(m + 1) * N));
+    h->gV_m = m;
+  }
+  TRY(dvec(h, &h->gsmall, 4 * kMaxBasis));
+  TRY(ensure_workspace(h));
+  TRY(dvec(h, &h->z, N));
+  double *V = h->gV, *hcol = h->gsmall, *ydev = h->gsmall + kMaxBasis;
+  const int g = std::min(vgrid(h, N), h->sm_count * 4);
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), gg(m + 1), y(m), hc(kMaxBasis);
+  double *hhost = h->scal_host;  // pinned, >= 8 doubles; larger reads go through hc below
+  (void)hhost;
+  int it = 0, status = MPDG_ERR_NOT_CONVERGED;
+  double tol = 0.0, res = 0.0, res0 = -1.0;
+  auto host_read = [&](const double *dev, double *dst, int cnt) -> int {
+    CU(cudaMemcpyAsync(dst, dev, sizeof(double) * cnt, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return MPDG_OK;
+  };
+  for (;;) {
+    CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+    TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+    k_residual<<<g, VT, 0, h->stream>>>(N, b, h->Ap, V);
+    ++h->launches;
+    double rr = 0.0;
+    TRY(norms(h, V, nullptr, &rr, nullptr));
+    const double beta = std::sqrt(rr);
+    if (res0 < 0.0) {
+      res0 = beta;
+      tol = std::max(prm->abs_tolerance,
+                     prm->rel_tolerance * (prm->tol_reference_norm > 0.0 ? prm->tol_reference_norm : beta));
+    }
+    res = beta;
+    if (!std::isfinite(beta)) {
+      status = MPDG_ERR_NAN;
+      break;
+    }
+    if (beta <= tol) {
+      status = MPDG_OK;
+      break;
+    }
+    if (it >= prm->max_iterations) break;
+    k_scale_precond<<<g, VT, 0, h->stream>>>(N, V, 1.0 / beta, D, h->z);
+    ++h->launches;
+    std::fill(gg.begin(), gg.end(), 0.0);
+    std::fill(H.begin(), H.end(), 0.0);
+    gg[0] = beta;
+    int jj = 0;
+    bool stop = false;
+    for (int j = 0; j < m; ++j) {
+      double *w = V + (int64_t)(j + 1) * N;
+      CU(cudaMemsetAsync(w, 0, sizeof(double) * N, h->stream));
+      TRY(op_apply_d(h, w, h->z, FIN_NONE, nullptr, nullptr));
+      for (int pass = 0; pass < 2; ++pass) {
+        k_multidot<<<g, VT, 0, h->stream>>>(N, V, N, j + 1, w, h->partials, h->counter, hcol);
+        k_multi_axpy<<<g, VT, 0, h->stream>>>(N, V, N, j + 1, hcol, w);
+        h->launches += 2;
+        TRY(host_read(hcol, hc.data(), j + 1));
+        for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] += hc[i];
+      }
+      double ww = 0.0;
+      TRY(norms(h, w, nullptr, &ww, nullptr));
+      const double hn = std::sqrt(ww);
+      H[(size_t)(j + 1) * m + j] = hn;
+      for (int i = 0; i < j; ++i) {
+        const double a = H[(size_t)i * m + j], c = H[(size_t)(i + 1) * m + j];
+        H[(size_t)i * m + j] = cs[i] * a + sn[i] * c;
+        H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * c;
+      }
+      const double a = H[(size_t)j * m + j], c = H[(size_t)(j + 1) * m + j];
+      const double r = std::sqrt(a * a + c * c);
+      cs[j] = r > 0.0 ? a / r : 1.0;
+      sn[j] = r > 0.0 ? c / r : 0.0;
+      H[(size_t)j * m + j] = r;
+      H[(size_t)(j + 1) * m + j] = 0.0;
+      gg[j + 1] = -sn[j] * gg[j];
+      gg[j] = cs[j] * gg[j];
+      ++it;
+      jj = j + 1;
+      res = std::fabs(gg[j + 1]);
+      if (!std::isfinite(res)) {
+        status = MPDG_ERR_NAN;
+        stop = true;
+        break;
+      }
+      if (res <= tol || it >= prm->max_iterations || hn == 0.0) break;
+      k_scale_precond<<<g, VT, 0, h->stream>>>(N, w, 1.0 / hn, D, h->z);
+      ++h->launches;
+    }
+    if (stop) break;
+    // y = R^-1 g, x += M^-1 V y
+    for (int i = jj - 1; i >= 0; --i) {
+      double sacc = gg[i];
+      for (int k = i + 1; k < jj; ++k) sacc -= H[(size_t)i * m + k] * y[k];
+      y[i] = sacc / H[(size_t)i * m + i];
+    }
+    CU(cudaMemcpyAsync(ydev, y.data(), sizeof(double) * jj, cudaMemcpyHostToDevice, h->stream));
+    k_gmres_update<<<g, VT, 0, h->stream>>>(N, V, N, jj, ydev, D, x);
+    ++h->launches;
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(h->stream));  // y lives on the host stack
+    if (res <= tol) {
+      status = MPDG_OK;
+      break;
+    }
+    if (it >= prm->max_iterations) break;
+  }
+  if (stats) {
+    stats->iterations = it;
+    stats->status = status;
+    stats->initial_residual = res0;
+    stats->final_residual = res;
+    stats->true_residual = res;
+  }
+  return MPDG_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1453,9 +1656,18 @@ static int linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
 {
   mpdg_solve_stats local;
   memset(&local, 0, sizeof(local));
-  if (prm->solver != MPDG_SOLVER_CG)
-    return fail(MPDG_ERR_NOT_SUPPORTED, "only CG is available on the device path");
-  if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32) {
+  if (prm->solver == MPDG_SOLVER_GMRES) {
+    if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32)
+      return fail(MPDG_ERR_NOT_SUPPORTED, "GMRES supports identity or Jacobi preconditioning");
+    const double *D = nullptr;
+    if (prm->preconditioner == MPDG_PRECOND_JACOBI) {
+      if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
+      D = h->inv_diag;
+    }
+    TRY(gmres(h, prm, x, b, D, &local));
+  } else if (prm->solver != MPDG_SOLVER_CG) {
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown solver type");
+  } else if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32) {
     TRY(cg_chebyshev(h, prm, x, b, &local));
   } else {
     const double *D = nullptr;

@@ -205,6 +205,34 @@ def test_chebyshev_mixed_precision_cg_larger_mesh(picard):
     assert torch.linalg.vector_norm(x - x_src) <= 1e-6 * torch.linalg.vector_norm(x_src)
 
 
+@pytest.mark.parametrize("restart", [5, 28])
+def test_gmres_matches_oracle_on_nonsymmetric_tangent(restart):
+    """Liquid-solid tangent at a rough linearisation point (strongly non-symmetric dk/dT
+    term): right-preconditioned GMRES(m) against the oracle's GMRES."""
+    law = dict(law=2, rho=1.0, cp=1.0, k=0.5, rho_s=1.2, cp_s=0.8, k_s=2.5, T_solidus=0.3,
+               T_liquidus=0.7)
+    o = O.Oracle(2, (5, 4, 4), perturb=0.1, seed=2)
+    o.set_material(O.material(**law), 1e-2)
+    g = H.HeatDiffuseOperator(H.box_mesh(2, (5, 4, 4), perturb=0.1, seed=2))
+    g.set_material(H.material(**law))
+    g.reset_time_increment(1e-2)
+    rng = np.random.default_rng(11)
+    N = o.n_dofs
+    Tl = rng.uniform(0, 1, N)
+    To = rng.uniform(0, 1, N)
+    b = o.vmult(rng.uniform(-1, 1, N), Tl, To)
+    x_ref, its_ref, _ = o.gmres(b, T_lin=Tl, T_old=To, rel_tol=1e-12, restart=restart)
+    g.set_linearization(cuda(Tl), cuda(To))
+    H.JacobiPreconditioner(g).update()
+    x = g.new_vector()
+    its = H.LinearSolver.solve(g, x, cuda(b), H.LinearSolverData(
+        solver_type=L.SOLVER_GMRES, rel_tolerance=1e-12, gmres_restart=restart), True)
+    assert abs(its - its_ref) <= max(2, its_ref // 10), (its, its_ref)
+    assert rel(x, x_ref) <= 1e-9
+    r = b - o.vmult(x.cpu().numpy(), Tl, To)
+    assert np.linalg.norm(r) <= 1.01e-12 * np.linalg.norm(b)
+
+
 def test_linear_solve_not_converged_raises():
     o, g = pair(3, (4, 4, 4), 0.0, dt=1.0)
     H.JacobiPreconditioner(g).update()

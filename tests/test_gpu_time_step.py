@@ -54,3 +54,37 @@ def test_single_linearization_step_matches_oracle(precond):
     assert np.abs(T - T_ref).max() <= 1e-7 * np.abs(T_ref).max()
     assert np.array_equal(opn.T_old.cpu().numpy(), T_prev)
     assert st.linear_iterations > 0
+
+
+# applications/mp-heat-transfer/cases/solidification_slab/tests/solidification_slab.mpirun=1.output
+SLAB = [2.82611e+02, 2.82458e+02, 2.82345e+02, 2.82252e+02, 2.82169e+02]
+
+
+def test_solidification_slab_newton_gmres_on_gpu():
+    """The reference's liquid-solid regression case through the GPU Newton path with the
+    reference's default linear solver (GMRES, Jacobi), 1D slab as a one-cell-thick 3D mesh."""
+    op = H.HeatDiffuseOperator(H.box_mesh(1, (128, 1, 1), dirichlet=("x-",),
+                                          dirichlet_values={"x-": 253.0}))
+    op.set_material(H.material(law=L.LAW_LIQUID_SOLID, rho=1000.0, cp=4226.0, k=0.556,
+                               rho_s=1000.0, cp_s=1762.0, k_s=2.22, T_solidus=270.0,
+                               T_liquidus=276.0))
+    lin = H.LinearSolverData(solver_type=L.SOLVER_GMRES, rel_tolerance=1e-12)
+    opn = H.HeatDiffuseOperation(op, lin, H.NonlinearSolverData(residual_tolerance=1e-8))
+    opn.set_initial_condition(torch.full((op.n_dofs,), 283.0, dtype=torch.float64, device="cuda"))
+    for ref in SLAB:
+        st = opn.solve(200.0)
+        assert st.converged == 1
+        assert float(f"{op.l2_norm(opn.T):.5e}") == ref
+
+
+def test_unidirectional_heat_transfer_gmres_on_gpu():
+    op = H.HeatDiffuseOperator(H.box_mesh(1, (32, 32, 1), (0, 0, 0), (0.1, 0.1, 1.0),
+                                          dirichlet=()))
+    op.set_material(H.material())
+    opn = H.HeatDiffuseOperation(op, H.LinearSolverData(solver_type=L.SOLVER_GMRES,
+                                                        rel_tolerance=1e-12),
+                                 H.NonlinearSolverData(residual_tolerance=5e-9))
+    opn.set_initial_condition(op.support_points()[:, 0].contiguous())
+    for ref in UNIDIRECTIONAL:
+        opn.solve(1e-4)
+        assert float(f"{op.l2_norm(opn.T):.5e}") == ref

@@ -227,6 +227,40 @@ int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *prm, double d
                              double dt_old, double *T_cur, double *T_old,
                              const double *heat_source, mpdg_step_stats *stats);
 
+/* ---- learned initial guess (no counterpart in the reference; the hook is the
+ *      Predictor's type switch, predictor.hpp:122-154) ---------------------- */
+/* A 3D U-Net (4 levels, 16/32/48/64 channels, 3x3x3 convolutions, BF16 weights and
+ * activations, FP32 accumulation) on an nx x ny x nz nodal grid; input 3 channels,
+ * output 1 channel, all tensors planar [C][z][y][x] FP32 on the device. */
+typedef struct mpdg_unet mpdg_unet;
+int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet **out);
+int mpdg_unet_destroy(mpdg_unet *u);
+int mpdg_unet_set_stream(mpdg_unet *u, void *stream);
+int mpdg_unet_n_params(const mpdg_unet *u, int64_t *n);
+/* FP32 master parameters (device, n_params): get / set (set refreshes the BF16 copy). */
+int mpdg_unet_get_params(mpdg_unet *u, float *dst);
+int mpdg_unet_set_params(mpdg_unet *u, const float *src);
+int mpdg_unet_forward(mpdg_unet *u, const float *input, float *output);
+/* Gradient of sum(grad_output * output) w.r.t. the parameters after a forward. */
+int mpdg_unet_backward(mpdg_unet *u, const float *grad_output, float *grad_params);
+/* One Adam step (beta 0.9/0.999) on the mean squared error; loss returned on the host. */
+int mpdg_unet_train_step(mpdg_unet *u, const float *input, const float *target, float lr,
+                         double *loss);
+int mpdg_unet_loss(mpdg_unet *u, const float *target, double *loss);
+const char *mpdg_unet_last_error(void);
+
+/* Network input from the solution history on the nodal grid sampled every `stride`
+ * DoFs per direction ((n_d - 1) % stride == 0): channels (T - T_old)/s[0],
+ * dt*q/s[1], T/s[2] (q may be NULL). */
+int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T, const double *T_old,
+                            const double *heat_source, double dt, const double scales[3],
+                            float *input);
+/* Learned guess for the next step: guess = 2 T - T_old + s3 * P(y), P the trilinear
+ * prolongation of the network output y from the sampled grid; Dirichlet values applied. */
+int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, const double *T,
+                            const double *T_old, const double *heat_source, double dt,
+                            const double scales[4], double *guess);
+
 /* ---- instrumentation -------------------------------------------------- */
 typedef struct {
   int64_t launches;        /* kernels this handle launched since the last reset      */

@@ -114,6 +114,21 @@ _SIGS = {
                                            _P, _P, _P, C.POINTER(StepStats)]),
     "mpdg_heat_set_timing": (C.c_int, [_H, C.c_int]),
     "mpdg_heat_get_counters": (C.c_int, [_H, C.POINTER(Counters), C.c_int]),
+    "mpdg_unet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_H)]),
+    "mpdg_unet_destroy": (C.c_int, [_H]),
+    "mpdg_unet_set_stream": (C.c_int, [_H, _P]),
+    "mpdg_unet_n_params": (C.c_int, [_H, C.POINTER(C.c_int64)]),
+    "mpdg_unet_get_params": (C.c_int, [_H, _D]),
+    "mpdg_unet_set_params": (C.c_int, [_H, _D]),
+    "mpdg_unet_forward": (C.c_int, [_H, _D, _D]),
+    "mpdg_unet_backward": (C.c_int, [_H, _D, _D]),
+    "mpdg_unet_train_step": (C.c_int, [_H, _D, _D, C.c_float, C.POINTER(C.c_double)]),
+    "mpdg_unet_loss": (C.c_int, [_H, _D, C.POINTER(C.c_double)]),
+    "mpdg_unet_last_error": (C.c_char_p, []),
+    "mpdg_heat_learned_input": (C.c_int, [_H, C.c_int, _D, _D, _D, C.c_double,
+                                          C.POINTER(C.c_double), _D]),
+    "mpdg_heat_learned_guess": (C.c_int, [_H, _H, C.c_int, _D, _D, _D, C.c_double,
+                                          C.POINTER(C.c_double), _D]),
     "mpdg_last_error": (C.c_char_p, []),
 }
 

@@ -95,6 +95,8 @@ struct mpdg_heat {
   double *gV = nullptr;
   int gV_m = 0;
   double *gsmall = nullptr;
+  float *nn_buf = nullptr;  // learned guess: network input and output on the sampled grid
+  int64_t nn_buf_n = 0;
   // reduction scratch
   double *partials = nullptr;
   unsigned *counter = nullptr;
@@ -1928,4 +1930,113 @@ extern "C" int mpdg_heat_l2_norm_noalloc(mpdg_heat *h, const double *u, double *
   CU(cudaGetLastError());
   h->launches += 2;
   return MPDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned initial guess: sampling onto the network grid and prolongation back
+// ---------------------------------------------------------------------------
+__global__ void k_learned_input(MeshDims d, int stride, int cx, int cy, int cz,
+                                const double *__restrict__ T, const double *__restrict__ To,
+                                const double *__restrict__ q, double dt, double s0, double s1,
+                                double s2, float *in)
+{
+  const int64_t nc = (int64_t)cx * cy * cz;
+  GRID_STRIDE(t, nc)
+  {
+    const int X = (int)(t % cx), Y = (int)((t / cx) % cy), Z = (int)(t / ((int64_t)cx * cy));
+    const int64_t f = (int64_t)stride * X + (int64_t)d.nd[0] * ((int64_t)stride * Y + (int64_t)d.nd[1] * stride * Z);
+    const double Tv = T[f];
+    in[t] = (float)((Tv - To[f]) / s0);
+    in[nc + t] = (float)(q ? dt * q[f] / s1 : 0.0);
+    in[2 * nc + t] = (float)(Tv / s2);
+  }
+}
+
+__global__ void k_learned_guess(int64_t N, MeshDims d, int stride, int cx, int cy, int cz,
+                                const double *__restrict__ T, const double *__restrict__ To,
+                                const float *__restrict__ y, double s3, double *g)
+{
+  GRID_STRIDE(i, N)
+  {
+    const int64_t I = i % d.nd[0], J = (i / d.nd[0]) % d.nd[1], K = i / ((int64_t)d.nd[0] * d.nd[1]);
+    const int64_t pos[3] = {I, J, K};
+    const int cdim[3] = {cx, cy, cz};
+    int lo[3], hi[3];
+    double w[3];
+    for (int e = 0; e < 3; ++e) {
+      lo[e] = (int)(pos[e] / stride);
+      const int r = (int)(pos[e] - (int64_t)lo[e] * stride);
+      hi[e] = lo[e] + (r > 0 ? 1 : 0);
+      if (hi[e] >= cdim[e]) hi[e] = cdim[e] - 1;
+      w[e] = (double)r / stride;
+    }
+    double s = 0.0;
+    for (int c = 0; c < 8; ++c) {
+      const int ix = (c & 1) ? hi[0] : lo[0], iy = (c & 2) ? hi[1] : lo[1], iz = (c & 4) ? hi[2] : lo[2];
+      const double wt = ((c & 1) ? w[0] : 1.0 - w[0]) * ((c & 2) ? w[1] : 1.0 - w[1]) *
+                        ((c & 4) ? w[2] : 1.0 - w[2]);
+      if (wt != 0.0) s += wt * (double)y[ix + (int64_t)cx * (iy + (int64_t)cy * iz)];
+    }
+    g[i] = 2.0 * T[i] - To[i] + s3 * s;
+  }
+}
+
+static int learned_dims(mpdg_heat *h, int stride, int c[3])
+{
+  if (stride < 1) return fail(MPDG_ERR_INVALID_ARGUMENT, "stride must be >= 1");
+  for (int e = 0; e < 3; ++e) {
+    if ((h->dims.nd[e] - 1) % stride != 0)
+      return fail(MPDG_ERR_INVALID_ARGUMENT, "(n_dofs per direction - 1) must be divisible by stride");
+    c[e] = (h->dims.nd[e] - 1) / stride + 1;
+  }
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T,
+                                       const double *T_old, const double *heat_source, double dt,
+                                       const double scales[3], float *input)
+{
+  if (!h || !T || !T_old || !scales || !input) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  int c[3];
+  TRY(learned_dims(h, stride, c));
+  CU(cudaSetDevice(h->device));
+  const int64_t nc = (int64_t)c[0] * c[1] * c[2];
+  k_learned_input<<<vgrid(h, nc), VT, 0, h->stream>>>(h->dims, stride, c[0], c[1], c[2], T, T_old,
+                                                     heat_source, dt, scales[0], scales[1],
+                                                     scales[2], input);
+  CU(cudaGetLastError());
+  ++h->launches;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_unet_forward(mpdg_unet *u, const float *input, float *output);
+extern "C" int mpdg_unet_set_stream(mpdg_unet *u, void *stream);
+
+extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, const double *T,
+                                       const double *T_old, const double *heat_source, double dt,
+                                       const double scales[4], double *guess)
+{
+  if (!h || !u || !T || !T_old || !scales || !guess)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  int c[3];
+  TRY(learned_dims(h, stride, c));
+  CU(cudaSetDevice(h->device));
+  const int64_t nc = (int64_t)c[0] * c[1] * c[2];
+  float *buf = nullptr;  // network input (3 nc) and output (nc), kept in the handle
+  TRY(dalloc(h, reinterpret_cast<void **>(&h->nn_buf), sizeof(float) * 4 * nc));
+  if (h->nn_buf_n < nc) {
+    if (h->nn_buf_n != 0) return fail(MPDG_ERR_INVALID_ARGUMENT, "network grid grew");
+    h->nn_buf_n = nc;
+  }
+  buf = h->nn_buf;
+  TRY(mpdg_heat_learned_input(h, stride, T, T_old, heat_source, dt, scales, buf));
+  mpdg_unet_set_stream(u, h->stream);
+  const int rc = mpdg_unet_forward(u, buf, buf + 3 * nc);
+  if (rc != MPDG_OK) return fail(rc, "network forward failed");
+  k_learned_guess<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, h->dims, stride, c[0], c[1],
+                                                             c[2], T, T_old, buf + 3 * nc,
+                                                             scales[3], guess);
+  CU(cudaGetLastError());
+  ++h->launches;
+  return distribute(h, guess);
 }

@@ -1,0 +1,209 @@
+"""Learned initial guess for the implicit heat step.
+
+A new predictor type next to MeltPoolDG's linear extrapolation
+(include/meltpooldg/linear_algebra/predictor.hpp:122-154, predictor_data.hpp:9-20):
+guess = 2 T^n - T^{n-1} + s3 * P(y), with y the output of a small BF16 U-Net
+(libmpdg_heat.so, mpdg_unet_*) evaluated on the nodal grid sampled every
+`stride` DoFs per direction and P the trilinear prolongation. The solver still
+iterates to the same tolerance, so the network only shortens CG.
+
+Training data come from trajectories of the plain FP64 solver along seeded
+random straight scan paths; training runs the library's own forward, backward
+and Adam kernels on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+import os
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib as L
+from . import heat as H
+
+DT, K1, AMP, RADIUS, Z0 = 5e-4, 0.5, 500.0, 0.05, 0.95
+
+
+def _check(rc):
+    if rc != L.OK:
+        msg = L.load().mpdg_unet_last_error().decode() or L.last_error()
+        raise H._EXC.get(rc, H.MpdgError)(f"[{rc}] {msg}")
+
+
+class UNet:
+    """The library's U-Net on an (nx, ny, nz) grid; tensors are CUDA float32."""
+
+    def __init__(self, dims, seed=1, device=0):
+        self._L = L.load()
+        self.dims = tuple(int(d) for d in dims)
+        self.device = torch.device("cuda", device)
+        h = C.c_void_p()
+        _check(self._L.mpdg_unet_create(*self.dims, int(seed), C.byref(h)))
+        self.h = h
+        n = C.c_int64()
+        _check(self._L.mpdg_unet_n_params(h, C.byref(n)))
+        self.n_params = int(n.value)
+        self.n_points = self.dims[0] * self.dims[1] * self.dims[2]
+        self.sync_stream()
+
+    def sync_stream(self):
+        with torch.cuda.device(self.device):
+            s = torch.cuda.current_stream().cuda_stream
+        _check(self._L.mpdg_unet_set_stream(self.h, C.c_void_p(s)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self._L.mpdg_unet_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def get_params(self):
+        p = torch.empty(self.n_params, dtype=torch.float32, device=self.device)
+        _check(self._L.mpdg_unet_get_params(self.h, p.data_ptr()))
+        return p
+
+    def set_params(self, p):
+        p = p.to(self.device, torch.float32).contiguous()
+        _check(self._L.mpdg_unet_set_params(self.h, p.data_ptr()))
+
+    def forward(self, x):
+        x = x.contiguous()
+        y = torch.empty(self.n_points, dtype=torch.float32, device=self.device)
+        _check(self._L.mpdg_unet_forward(self.h, x.data_ptr(), y.data_ptr()))
+        return y
+
+    def backward(self, grad_out):
+        g = torch.empty(self.n_params, dtype=torch.float32, device=self.device)
+        _check(self._L.mpdg_unet_backward(self.h, grad_out.contiguous().data_ptr(), g.data_ptr()))
+        return g
+
+    def train_step(self, x, target, lr):
+        loss = C.c_double()
+        _check(self._L.mpdg_unet_train_step(self.h, x.contiguous().data_ptr(),
+                                            target.contiguous().data_ptr(), float(lr),
+                                            C.byref(loss)))
+        return float(loss.value)
+
+
+# layer shapes (must match nn_unet.cu): (Cin, Cout) of the 15 convolutions
+LAYERS = [(3, 16), (16, 16), (16, 32), (32, 32), (32, 48), (48, 48), (48, 64), (64, 64),
+          (64, 48), (48, 48), (48, 32), (32, 32), (32, 16), (16, 16), (16, 1)]
+
+
+def unpack(params):
+    """Split the flat parameter vector into [(weight[Cout, Cin, 3, 3, 3], bias[Cout])]."""
+    out, off = [], 0
+    for ci, co in LAYERS:
+        w = params[off:off + ci * co * 27].view(co, ci, 3, 3, 3)
+        off += ci * co * 27
+        b = params[off:off + co]
+        off += co
+        out.append((w, b))
+    assert off == params.numel()
+    return out
+
+
+@dataclass
+class GuessModel:
+    """A trained network plus the scaling of its inputs and output."""
+    stride: int = 1
+    scales: list = field(default_factory=lambda: [1.0, 1.0, 1.0, 1.0])
+    net: UNet | None = None
+
+    def guess(self, op: H.HeatDiffuseOperator, T, T_old, q, dt, out=None):
+        out = op.new_vector() if out is None else out
+        self.net.sync_stream()
+        s = (C.c_double * 4)(*self.scales)
+        H.check(op._L.mpdg_heat_learned_guess(op.h, self.net.h, self.stride, T.data_ptr(),
+                                               T_old.data_ptr(),
+                                               None if q is None else q.data_ptr(), float(dt),
+                                               s, out.data_ptr()))
+        return out
+
+    def save(self, path):
+        p = self.net.get_params().cpu()
+        torch.save({"params": p, "dims": self.net.dims, "scales": self.scales}, path + ".pt")
+        with open(path + ".json", "w") as f:
+            json.dump({"dims": self.net.dims, "scales": self.scales,
+                       "n_params": self.net.n_params}, f, indent=1)
+
+    @classmethod
+    def load(cls, path, stride=1, device=0):
+        d = torch.load(path + ".pt", map_location="cpu")
+        net = UNet(d["dims"], device=device)
+        net.set_params(d["params"])
+        return cls(stride=stride, scales=list(d["scales"]), net=net)
+
+
+def scan_path(rng: torch.Generator):
+    """Straight scan segment: start in [0.1, 0.9]^2, random heading, speed 1."""
+    u = torch.rand(3, generator=rng, dtype=torch.float64).tolist()
+    x0, y0 = 0.1 + 0.8 * u[0], 0.1 + 0.8 * u[1]
+    th = 2.0 * math.pi * u[2]
+    return lambda t: (x0 + t * math.cos(th), y0 + t * math.sin(th), Z0)
+
+
+def make_operator(cells, degree=3, device=0):
+    op = H.HeatDiffuseOperator(H.box_mesh(degree, (cells,) * 3), device=device)
+    op.set_material(H.material(law=L.LAW_LINEAR_K, k=1.0, k1=K1))
+    return op
+
+
+def generate(op, n_traj, n_steps, seed, stride=1, scales=(1.0, 1.0, 1.0), amp=AMP,
+             solver_tol=1e-10):
+    """Trajectories of the plain FP64 solver; returns [(input[3, G], target[G])] where the
+    target is T^{n+1} - (2 T^n - T^{n-1}) on the sampled grid (unscaled)."""
+    g = torch.Generator().manual_seed(seed)
+    lin = H.LinearSolverData(rel_tolerance=solver_tol, abs_tolerance=0.0)
+    dims = tuple((d - 1) // stride + 1 for d in op.dims)
+    npts = dims[0] * dims[1] * dims[2]
+    samples = []
+    s3 = (C.c_double * 3)(*scales)
+    for _ in range(n_traj):
+        path = scan_path(g)
+        opn = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR,
+                                     single_linearization=True)
+        q = op.new_vector()
+        opn.heat_source = q
+        for s in range(n_steps):
+            op.gaussian_source(q, amp, path((s + 1) * DT), RADIUS)
+            T_n, T_nm1 = opn.T.clone(), opn.T_old.clone()
+            x = torch.empty(3 * npts, dtype=torch.float32, device=op.device)
+            H.check(op._L.mpdg_heat_learned_input(op.h, stride, T_n.data_ptr(), T_nm1.data_ptr(),
+                                                  q.data_ptr(), DT, s3, x.data_ptr()))
+            opn.solve(DT)
+            if s == 0:
+                continue  # no history yet: the first step has no extrapolation to correct
+            tgt = (opn.T - 2.0 * T_n + T_nm1).view(op.dims[2], op.dims[1], op.dims[0])
+            tgt = tgt[::stride, ::stride, ::stride].contiguous().view(-1).float()
+            samples.append((x, tgt))
+    return samples
+
+
+def fit_scales(samples):
+    """Per-channel input scales and the output scale (standard deviations)."""
+    xs = torch.stack([x.view(3, -1) for x, _ in samples])
+    ts = torch.stack([t for _, t in samples])
+    sx = [float(xs[:, c].std().clamp_min(1e-30)) for c in range(3)]
+    return sx + [float(ts.std().clamp_min(1e-30))]
+
+
+def train(net: UNet, samples, scales, steps, lr=1e-3, seed=0, log_every=0):
+    """Adam on the MSE of the scaled target; returns the loss history."""
+    g = torch.Generator().manual_seed(seed)
+    sx = torch.tensor(scales[:3], dtype=torch.float32, device=net.device).view(3, 1)
+    data = [((x.view(3, -1) / sx).reshape(-1).contiguous(), (t / scales[3]).contiguous())
+            for x, t in samples]
+    hist = []
+    for it in range(steps):
+        i = int(torch.randint(len(data), (1,), generator=g))
+        cur_lr = lr * 0.5 * (1.0 + math.cos(math.pi * it / steps))
+        hist.append(net.train_step(data[i][0], data[i][1], cur_lr))
+        if log_every and it % log_every == 0:
+            print(f"step {it} loss {hist[-1]:.4e}", flush=True)
+    return hist

@@ -255,11 +255,15 @@ const char *mpdg_unet_last_error(void);
 int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T, const double *T_old,
                             const double *heat_source, double dt, const double scales[3],
                             float *input);
-/* Learned guess for the next step: guess = 2 T - T_old + s3 * P(y), P the trilinear
- * prolongation of the network output y from the sampled grid; Dirichlet values applied. */
+/* Learned guess for the next step: guess = LE + alpha d with LE = 2 T - T_old the
+ * linear extrapolation, d = a P(y) the network correction (a = RMS of T - T_old, the
+ * inputs scaled by a, a and T_scale, P the trilinear prolongation from the sampled
+ * grid) and, with line_search, alpha = argmin |r(LE) - alpha J d| (J linearised at
+ * LE), so the guess's residual never exceeds the extrapolation's; else alpha = 1.
+ * Dirichlet values applied; alpha returned in *alpha_out (may be NULL). */
 int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, const double *T,
                             const double *T_old, const double *heat_source, double dt,
-                            const double scales[4], double *guess);
+                            double T_scale, int line_search, double *guess, double *alpha_out);
 
 /* ---- instrumentation -------------------------------------------------- */
 typedef struct {

@@ -128,7 +128,7 @@ _SIGS = {
     "mpdg_heat_learned_input": (C.c_int, [_H, C.c_int, _D, _D, _D, C.c_double,
                                           C.POINTER(C.c_double), _D]),
     "mpdg_heat_learned_guess": (C.c_int, [_H, _H, C.c_int, _D, _D, _D, C.c_double,
-                                          C.POINTER(C.c_double), _D]),
+                                          C.c_double, C.c_int, _D, C.POINTER(C.c_double)]),
     "mpdg_last_error": (C.c_char_p, []),
 }
 

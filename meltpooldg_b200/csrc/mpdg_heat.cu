@@ -2012,31 +2012,83 @@ extern "C" int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T
 extern "C" int mpdg_unet_forward(mpdg_unet *u, const float *input, float *output);
 extern "C" int mpdg_unet_set_stream(mpdg_unet *u, void *stream);
 
+__global__ void k_lincomb(int64_t N, double *out, double a, const double *__restrict__ x, double b,
+                          const double *__restrict__ y)
+{
+  GRID_STRIDE(i, N) out[i] = a * x[i] + b * (y ? y[i] : 0.0);
+}
+
 extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, const double *T,
                                        const double *T_old, const double *heat_source, double dt,
-                                       const double scales[4], double *guess)
+                                       double T_scale, int line_search, double *guess,
+                                       double *alpha_out)
 {
-  if (!h || !u || !T || !T_old || !scales || !guess)
-    return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (!h || !u || !T || !T_old || !guess) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (!(dt > 0.0) || !(T_scale > 0.0)) return fail(MPDG_ERR_INVALID_ARGUMENT, "dt and T_scale must be > 0");
   int c[3];
   TRY(learned_dims(h, stride, c));
   CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
   const int64_t nc = (int64_t)c[0] * c[1] * c[2];
-  float *buf = nullptr;  // network input (3 nc) and output (nc), kept in the handle
   TRY(dalloc(h, reinterpret_cast<void **>(&h->nn_buf), sizeof(float) * 4 * nc));
-  if (h->nn_buf_n < nc) {
-    if (h->nn_buf_n != 0) return fail(MPDG_ERR_INVALID_ARGUMENT, "network grid grew");
-    h->nn_buf_n = nc;
-  }
-  buf = h->nn_buf;
-  TRY(mpdg_heat_learned_input(h, stride, T, T_old, heat_source, dt, scales, buf));
-  mpdg_unet_set_stream(u, h->stream);
-  const int rc = mpdg_unet_forward(u, buf, buf + 3 * nc);
-  if (rc != MPDG_OK) return fail(rc, "network forward failed");
-  k_learned_guess<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, h->dims, stride, c[0], c[1],
-                                                             c[2], T, T_old, buf + 3 * nc,
-                                                             scales[3], guess);
-  CU(cudaGetLastError());
+  if (h->nn_buf_n == 0) h->nn_buf_n = nc;
+  if (h->nn_buf_n != nc) return fail(MPDG_ERR_INVALID_ARGUMENT, "network grid changed");
+  TRY(dvec(h, &h->w1, N));
+  TRY(dvec(h, &h->w2, N));
+  TRY(dvec(h, &h->w3, N));
+  // per-sample scale: RMS of the time increment
+  k_lincomb<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->w1, 1.0, T, -1.0, T_old);
   ++h->launches;
+  double dd = 0.0;
+  TRY(norms(h, h->w1, nullptr, &dd, nullptr));
+  const double a = std::sqrt(dd / (double)N);
+  // linear extrapolation 2 T - T_old (with Dirichlet values) into guess
+  k_lincomb<<<vgrid(h, N), VT, 0, h->stream>>>(N, guess, 2.0, T, -1.0, T_old);
+  ++h->launches;
+  TRY(distribute(h, guess));
+  if (!(a > 0.0)) {  // no history yet: the extrapolation is the guess
+    if (alpha_out) *alpha_out = 0.0;
+    return MPDG_OK;
+  }
+  const double scales[3] = {a, a, T_scale};
+  TRY(mpdg_heat_learned_input(h, stride, T, T_old, heat_source, dt, scales, h->nn_buf));
+  mpdg_unet_set_stream(u, h->stream);
+  const int rc = mpdg_unet_forward(u, h->nn_buf, h->nn_buf + 3 * nc);
+  if (rc != MPDG_OK) return fail(rc, "network forward failed");
+  // d = a * P(y) (prolongated correction) into w1, zero at Dirichlet DoFs
+  CU(cudaMemsetAsync(h->w2, 0, sizeof(double) * N, h->stream));
+  k_learned_guess<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, stride, c[0], c[1], c[2], h->w2,
+                                                     h->w2, h->nn_buf + 3 * nc, a, h->w1);
+  ++h->launches;
+  double alpha = 1.0;
+  if (line_search) {
+    // alpha = argmin |r(LE) - alpha J d| with the operator linearised at the extrapolation
+    TRY(ensure_dt(h));
+    const double *keepT = h->T_lin, *keepTo = h->T_old;
+    h->T_lin = guess;
+    h->T_old = T;
+    h->lin_f_dirty = true;
+    CU(cudaMemsetAsync(h->w2, 0, sizeof(double) * N, h->stream));
+    int rr = create_rhs(h, h->w2, T, heat_source);               // r = -R(LE)
+    if (rr == MPDG_OK) {
+      CU(cudaMemsetAsync(h->w3, 0, sizeof(double) * N, h->stream));
+      rr = op_apply_d(h, h->w3, h->w1, FIN_NONE, nullptr, nullptr);  // J d
+    }
+    h->T_lin = keepT;
+    h->T_old = keepTo;
+    h->lin_f_dirty = true;
+    TRY(rr);
+    double jj = 0.0, rj_plus = 0.0;
+    TRY(norms(h, h->w3, nullptr, &jj, nullptr));
+    TRY(norms(h, h->w2, h->w3, nullptr, &rj_plus));  // |r + Jd|^2
+    double r2 = 0.0;
+    TRY(norms(h, h->w2, nullptr, &r2, nullptr));
+    const double rj = 0.5 * (rj_plus - r2 - jj);
+    alpha = jj > 0.0 ? rj / jj : 0.0;
+  }
+  k_lincomb<<<vgrid(h, N), VT, 0, h->stream>>>(N, guess, 1.0, guess, alpha, h->w1);
+  ++h->launches;
+  CU(cudaGetLastError());
+  if (alpha_out) *alpha_out = alpha;
   return distribute(h, guess);
 }

@@ -2,10 +2,12 @@
 
 A new predictor type next to MeltPoolDG's linear extrapolation
 (include/meltpooldg/linear_algebra/predictor.hpp:122-154, predictor_data.hpp:9-20):
-guess = 2 T^n - T^{n-1} + s3 * P(y), with y the output of a small BF16 U-Net
-(libmpdg_heat.so, mpdg_unet_*) evaluated on the nodal grid sampled every
-`stride` DoFs per direction and P the trilinear prolongation. The solver still
-iterates to the same tolerance, so the network only shortens CG.
+guess = LE + alpha * a * P(y), with LE = 2 T^n - T^{n-1}, y the output of a small
+BF16 U-Net (libmpdg_heat.so, mpdg_unet_*) evaluated on the nodal grid sampled
+every `stride` DoFs per direction, P the trilinear prolongation, a the RMS of
+T^n - T^{n-1} (inputs and output are scaled by it) and alpha the step length that
+minimises the residual of the guess (so it is never worse than LE). The solver
+still iterates to the same tolerance, so the network only shortens CG.
 
 Training data come from trajectories of the plain FP64 solver along seeded
 random straight scan paths; training runs the library's own forward, backward
@@ -17,7 +19,7 @@ import ctypes as C
 import json
 import math
 import os
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import torch
 
@@ -110,26 +112,28 @@ def unpack(params):
 
 @dataclass
 class GuessModel:
-    """A trained network plus the scaling of its inputs and output."""
+    """A trained network, the sampling stride and the temperature input scale."""
     stride: int = 1
-    scales: list = field(default_factory=lambda: [1.0, 1.0, 1.0, 1.0])
+    T_scale: float = 1.0
     net: UNet | None = None
 
-    def guess(self, op: H.HeatDiffuseOperator, T, T_old, q, dt, out=None):
+    def guess(self, op: H.HeatDiffuseOperator, T, T_old, q, dt, out=None, line_search=True):
+        """Guess for the next step from (T^n, T^{n-1}, q^{n+1}); returns (guess, alpha)."""
         out = op.new_vector() if out is None else out
         self.net.sync_stream()
-        s = (C.c_double * 4)(*self.scales)
+        alpha = C.c_double()
         H.check(op._L.mpdg_heat_learned_guess(op.h, self.net.h, self.stride, T.data_ptr(),
                                                T_old.data_ptr(),
                                                None if q is None else q.data_ptr(), float(dt),
-                                               s, out.data_ptr()))
-        return out
+                                               float(self.T_scale), int(bool(line_search)),
+                                               out.data_ptr(), C.byref(alpha)))
+        return out, float(alpha.value)
 
     def save(self, path):
         p = self.net.get_params().cpu()
-        torch.save({"params": p, "dims": self.net.dims, "scales": self.scales}, path + ".pt")
+        torch.save({"params": p, "dims": self.net.dims, "T_scale": self.T_scale}, path + ".pt")
         with open(path + ".json", "w") as f:
-            json.dump({"dims": self.net.dims, "scales": self.scales,
+            json.dump({"dims": list(self.net.dims), "T_scale": self.T_scale,
                        "n_params": self.net.n_params}, f, indent=1)
 
     @classmethod
@@ -137,7 +141,7 @@ class GuessModel:
         d = torch.load(path + ".pt", map_location="cpu")
         net = UNet(d["dims"], device=device)
         net.set_params(d["params"])
-        return cls(stride=stride, scales=list(d["scales"]), net=net)
+        return cls(stride=stride, T_scale=float(d["T_scale"]), net=net)
 
 
 def scan_path(rng: torch.Generator):
@@ -154,16 +158,16 @@ def make_operator(cells, degree=3, device=0):
     return op
 
 
-def generate(op, n_traj, n_steps, seed, stride=1, scales=(1.0, 1.0, 1.0), amp=AMP,
-             solver_tol=1e-10):
-    """Trajectories of the plain FP64 solver; returns [(input[3, G], target[G])] where the
-    target is T^{n+1} - (2 T^n - T^{n-1}) on the sampled grid (unscaled)."""
+def generate(op, n_traj, n_steps, seed, stride=1, T_scale=0.1, amp=AMP, solver_tol=1e-10):
+    """Trajectories of the plain FP64 solver along seeded random scan paths. Returns
+    [(input[3 G], target[G])] on the sampled grid, normalised as the guess normalises
+    them: inputs (T^n - T^{n-1})/a, dt q/a, T^n/T_scale and target
+    (T^{n+1} - 2 T^n + T^{n-1})/a with a = RMS(T^n - T^{n-1})."""
     g = torch.Generator().manual_seed(seed)
     lin = H.LinearSolverData(rel_tolerance=solver_tol, abs_tolerance=0.0)
     dims = tuple((d - 1) // stride + 1 for d in op.dims)
     npts = dims[0] * dims[1] * dims[2]
     samples = []
-    s3 = (C.c_double * 3)(*scales)
     for _ in range(n_traj):
         path = scan_path(g)
         opn = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR,
@@ -173,37 +177,31 @@ def generate(op, n_traj, n_steps, seed, stride=1, scales=(1.0, 1.0, 1.0), amp=AM
         for s in range(n_steps):
             op.gaussian_source(q, amp, path((s + 1) * DT), RADIUS)
             T_n, T_nm1 = opn.T.clone(), opn.T_old.clone()
-            x = torch.empty(3 * npts, dtype=torch.float32, device=op.device)
-            H.check(op._L.mpdg_heat_learned_input(op.h, stride, T_n.data_ptr(), T_nm1.data_ptr(),
-                                                  q.data_ptr(), DT, s3, x.data_ptr()))
+            a = float((T_n - T_nm1).pow(2).mean().sqrt())
+            x = None
+            if s > 0 and a > 0.0:
+                x = torch.empty(3 * npts, dtype=torch.float32, device=op.device)
+                sc = (C.c_double * 3)(a, a, T_scale)
+                H.check(op._L.mpdg_heat_learned_input(op.h, stride, T_n.data_ptr(),
+                                                      T_nm1.data_ptr(), q.data_ptr(), DT, sc,
+                                                      x.data_ptr()))
             opn.solve(DT)
-            if s == 0:
-                continue  # no history yet: the first step has no extrapolation to correct
+            if x is None:
+                continue
             tgt = (opn.T - 2.0 * T_n + T_nm1).view(op.dims[2], op.dims[1], op.dims[0])
-            tgt = tgt[::stride, ::stride, ::stride].contiguous().view(-1).float()
-            samples.append((x, tgt))
+            tgt = tgt[::stride, ::stride, ::stride].contiguous().view(-1) / a
+            samples.append((x, tgt.float().contiguous()))
     return samples
 
 
-def fit_scales(samples):
-    """Per-channel input scales and the output scale (standard deviations)."""
-    xs = torch.stack([x.view(3, -1) for x, _ in samples])
-    ts = torch.stack([t for _, t in samples])
-    sx = [float(xs[:, c].std().clamp_min(1e-30)) for c in range(3)]
-    return sx + [float(ts.std().clamp_min(1e-30))]
-
-
-def train(net: UNet, samples, scales, steps, lr=1e-3, seed=0, log_every=0):
-    """Adam on the MSE of the scaled target; returns the loss history."""
+def train(net: UNet, samples, steps, lr=5e-4, seed=0, log_every=0):
+    """Adam with a cosine learning-rate decay on the MSE; returns the loss history."""
     g = torch.Generator().manual_seed(seed)
-    sx = torch.tensor(scales[:3], dtype=torch.float32, device=net.device).view(3, 1)
-    data = [((x.view(3, -1) / sx).reshape(-1).contiguous(), (t / scales[3]).contiguous())
-            for x, t in samples]
     hist = []
     for it in range(steps):
-        i = int(torch.randint(len(data), (1,), generator=g))
+        i = int(torch.randint(len(samples), (1,), generator=g))
         cur_lr = lr * 0.5 * (1.0 + math.cos(math.pi * it / steps))
-        hist.append(net.train_step(data[i][0], data[i][1], cur_lr))
+        hist.append(net.train_step(samples[i][0], samples[i][1], cur_lr))
         if log_every and it % log_every == 0:
             print(f"step {it} loss {hist[-1]:.4e}", flush=True)
     return hist

@@ -1,0 +1,55 @@
+"""The trained learned-guess model against linear extrapolation on a held-out scan path.
+
+The guess scales the network's correction by the residual-minimising step length, so
+its initial residual never exceeds the extrapolation's; the test records what the
+network gains in initial residual and CG iterations (the solver still iterates to the
+same 1e-8 tolerance, so the solution is unchanged)."""
+import os
+
+import pytest
+import torch
+
+from meltpooldg_b200 import _lib as L
+from meltpooldg_b200 import heat as H
+from meltpooldg_b200 import learned as LG
+
+pytestmark = pytest.mark.gpu
+MODEL = os.path.join(os.path.dirname(LG.__file__), "models", "heat_guess_p3_h96")
+
+
+def run(op, model, seed, n_steps=14):
+    path = LG.scan_path(torch.Generator().manual_seed(seed))
+    lin = H.LinearSolverData(preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32,
+                             rel_tolerance=1e-8, abs_tolerance=0.0, cheb_degree=6,
+                             cheb_picard=True, cheb_eig_reuse=True)
+    opn = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR,
+                                 single_linearization=True)
+    q = op.new_vector()
+    opn.heat_source = q
+    its, res = [], []
+    for s in range(n_steps):
+        op.gaussian_source(q, LG.AMP, path((s + 1) * LG.DT), LG.RADIUS)
+        if model is not None and s > 0:
+            g, _ = model.guess(op, opn.T, opn.T_old, q, LG.DT)
+            opn.set_guess(g)
+            opn.params.predictor = L.PREDICTOR_GIVEN
+        else:
+            opn.params.predictor = L.PREDICTOR_LINEAR
+        st = opn.solve(LG.DT)
+        its.append(st.linear_iterations)
+        res.append(st.initial_relative_residual)
+    return its, res, opn.T.clone()
+
+
+def test_learned_guess_on_held_out_path():
+    assert os.path.exists(MODEL + ".pt"), "trained model missing"
+    op = LG.make_operator(32)
+    model = LG.GuessModel.load(MODEL, stride=1)
+    its0, res0, T0 = run(op, None, seed=99)
+    its1, res1, T1 = run(op, model, seed=99)
+    gain = [r0 / r1 for r0, r1 in zip(res0[1:], res1[1:])]
+    print("initial residual gain per step", [round(x, 2) for x in gain],
+          "iterations", sum(its0), "->", sum(its1))
+    assert all(r1 <= r0 * 1.0001 for r0, r1 in zip(res0[1:], res1[1:]))
+    assert sum(its1) <= sum(its0) + 1
+    assert torch.linalg.vector_norm(T1 - T0) <= 1e-6 * torch.linalg.vector_norm(T0)

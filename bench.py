@@ -194,9 +194,23 @@ def run_mine(args):
         preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32, rel_tolerance=REL_TOL,
         abs_tolerance=0.0, cheb_degree=CHEB_DEGREE, cheb_picard=True, cheb_eig_reuse=True),
         predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    learned = H.HeatDiffuseOperation(op, H.LinearSolverData(
+        preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32, rel_tolerance=REL_TOL,
+        abs_tolerance=0.0, cheb_degree=CHEB_DEGREE, cheb_picard=True, cheb_eig_reuse=True),
+        predictor=L.PREDICTOR_GIVEN, single_linearization=True)
     q = op.new_vector()
     mixed.heat_source = q
     plain.heat_source = q
+    learned.heat_source = q
+    model = None
+    if not args.no_learned:
+        from meltpooldg_b200 import learned as LG
+        # network trained on 32^3-cell meshes (nodal spacing 1/96): stride 4 on 128^3 cells
+        model = LG.GuessModel.load(os.path.join(ROOT, "meltpooldg_b200", "models",
+                                                "heat_guess_p3_h96"),
+                                   stride=(DEGREE * cells) // 96 if cells % 32 == 0 else 1,
+                                   device=local)
+        guess_buf = op.new_vector()
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
@@ -208,6 +222,13 @@ def run_mine(args):
         its = []
         for s in range(first, first + count):
             op.gaussian_source(q, AMP, source_center((s + 1) * DT), RADIUS)
+            if opn is learned:
+                if s == 0:
+                    opn.params.predictor = L.PREDICTOR_LINEAR
+                else:
+                    model.guess(op, opn.T, opn.T_old, q, DT, out=guess_buf)
+                    opn.set_guess(guess_buf)
+                    opn.params.predictor = L.PREDICTOR_GIVEN
             st = opn.solve(DT)
             its.append(st.linear_iterations)
         return its
@@ -240,6 +261,12 @@ def run_mine(args):
     ms_mixed, its_mixed, cnt = timed(mixed, W, K, instrument=True)
     clk = clocks.stop() if clocks else None
     init_res = mixed.last_stats.initial_relative_residual
+    # learned guess + mixed precision on the same steps
+    ms_learned = its_learned = init_res_learned = None
+    if model is not None:
+        march(learned, 0, W)
+        ms_learned, its_learned, _ = timed(learned, W, K)
+        init_res_learned = learned.last_stats.initial_relative_residual
     # plain FP64 Jacobi-CG on the same steps
     ms_plain = its_plain = None
     if not args.no_plain:
@@ -333,7 +360,7 @@ def run_mine(args):
                "sample": f"{args.cpu_steps} implicit steps of the same problem on "
                          f"{args.cpu_cells}^3 cells ({n} DoFs), oracle port, {sec:.1f} s"}
 
-    best_ms = min(ms_mixed, ms_plain) if ms_plain else ms_mixed
+    best_ms = min(x for x in (ms_mixed, ms_plain, ms_learned) if x)
     line = {
         "metric": METRIC, "value": world * N * K / (best_ms / 1e3), "unit": "DoF/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": best_ms / K,
@@ -345,6 +372,10 @@ def run_mine(args):
         "speedup_mixed_vs_plain": (ms_plain / ms_mixed) if ms_plain else None,
         "cg_iterations_mixed": its_mixed, "cg_iterations_plain": its_plain,
         "initial_relative_residual_last_step": init_res,
+        "learned_mixed_ms_per_step": ms_learned / K if ms_learned else None,
+        "speedup_learned_mixed_vs_plain": (ms_plain / ms_learned) if (ms_plain and ms_learned) else None,
+        "cg_iterations_learned_mixed": its_learned,
+        "initial_relative_residual_last_step_learned": init_res_learned,
         "mixed_solver": {"outer": "FP64 flexible CG", "preconditioner":
                          f"FP32 Chebyshev-Jacobi degree {CHEB_DEGREE}, Picard operator "
                          "(k(T_lin) at the q-points), interval from 12 Lanczos steps reused "
@@ -372,6 +403,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -237,6 +237,7 @@ int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet **out);
 int mpdg_unet_destroy(mpdg_unet *u);
 int mpdg_unet_set_stream(mpdg_unet *u, void *stream);
 int mpdg_unet_n_params(const mpdg_unet *u, int64_t *n);
+int mpdg_unet_dims(const mpdg_unet *u, int dims[3]);
 /* FP32 master parameters (device, n_params): get / set (set refreshes the BF16 copy). */
 int mpdg_unet_get_params(mpdg_unet *u, float *dst);
 int mpdg_unet_set_params(mpdg_unet *u, const float *src);
@@ -260,7 +261,8 @@ int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T, const dou
  * inputs scaled by a, a and T_scale, P the trilinear prolongation from the sampled
  * grid) and, with line_search, alpha = argmin |r(LE) - alpha J d| (J linearised at
  * LE), so the guess's residual never exceeds the extrapolation's; else alpha = 1.
- * Dirichlet values applied; alpha returned in *alpha_out (may be NULL). */
+ * Dirichlet values applied; alpha returned in *alpha_out (may be NULL). The network's
+ * grid must equal the sampled grid (else MPDG_ERR_INVALID_ARGUMENT). */
 int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, const double *T,
                             const double *T_old, const double *heat_source, double dt,
                             double T_scale, int line_search, double *guess, double *alpha_out);

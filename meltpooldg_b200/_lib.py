@@ -118,6 +118,7 @@ _SIGS = {
     "mpdg_unet_destroy": (C.c_int, [_H]),
     "mpdg_unet_set_stream": (C.c_int, [_H, _P]),
     "mpdg_unet_n_params": (C.c_int, [_H, C.POINTER(C.c_int64)]),
+    "mpdg_unet_dims": (C.c_int, [_H, C.POINTER(C.c_int)]),
     "mpdg_unet_get_params": (C.c_int, [_H, _D]),
     "mpdg_unet_set_params": (C.c_int, [_H, _D]),
     "mpdg_unet_forward": (C.c_int, [_H, _D, _D]),

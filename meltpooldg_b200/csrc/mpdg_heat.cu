@@ -2011,6 +2011,7 @@ extern "C" int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T
 
 extern "C" int mpdg_unet_forward(mpdg_unet *u, const float *input, float *output);
 extern "C" int mpdg_unet_set_stream(mpdg_unet *u, void *stream);
+extern "C" int mpdg_unet_dims(const mpdg_unet *u, int dims[3]);
 
 __global__ void k_lincomb(int64_t N, double *out, double a, const double *__restrict__ x, double b,
                           const double *__restrict__ y)
@@ -2027,6 +2028,13 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
   if (!(dt > 0.0) || !(T_scale > 0.0)) return fail(MPDG_ERR_INVALID_ARGUMENT, "dt and T_scale must be > 0");
   int c[3];
   TRY(learned_dims(h, stride, c));
+  int ud[3];
+  TRY(mpdg_unet_dims(u, ud));
+  if (ud[0] != c[0] || ud[1] != c[1] || ud[2] != c[2])
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "network grid " + std::to_string(ud[0]) + "x" + std::to_string(ud[1]) + "x" +
+                  std::to_string(ud[2]) + " does not match the sampled mesh grid " +
+                  std::to_string(c[0]) + "x" + std::to_string(c[1]) + "x" + std::to_string(c[2]));
   CU(cudaSetDevice(h->device));
   const int64_t N = h->n_dofs;
   const int64_t nc = (int64_t)c[0] * c[1] * c[2];

@@ -621,6 +621,15 @@ extern "C" int mpdg_unet_set_stream(mpdg_unet *u, void *stream)
   return MPDG_OK;
 }
 
+extern "C" int mpdg_unet_dims(const mpdg_unet *u, int dims[3])
+{
+  if (!u || !dims) return nn_fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  dims[0] = u->g[0].nx;
+  dims[1] = u->g[0].ny;
+  dims[2] = u->g[0].nz;
+  return MPDG_OK;
+}
+
 extern "C" int mpdg_unet_n_params(const mpdg_unet *u, int64_t *n)
 {
   if (!u || !n) return nn_fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");

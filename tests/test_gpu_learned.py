@@ -53,3 +53,11 @@ def test_learned_guess_on_held_out_path():
     assert all(r1 <= r0 * 1.0001 for r0, r1 in zip(res0[1:], res1[1:]))
     assert sum(its1) <= sum(its0) + 1
     assert torch.linalg.vector_norm(T1 - T0) <= 1e-6 * torch.linalg.vector_norm(T0)
+
+
+def test_guess_rejects_a_network_of_another_grid():
+    op = LG.make_operator(8)  # 25^3 nodal grid
+    model = LG.GuessModel(stride=1, T_scale=0.1, net=LG.UNet((17, 17, 17)))
+    T = op.new_vector()
+    with pytest.raises(H.ExcInvalidArgument):
+        model.guess(op, T, T, None, LG.DT)

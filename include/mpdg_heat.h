@@ -129,6 +129,16 @@ int mpdg_heat_device_bytes(const mpdg_heat *h, int64_t *bytes);
 /* Material law (Material ctor + HeatDiffuseMultiPhaseOperator ctor, do_solidification =
  * law != CONSTANT). */
 int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m);
+/* Boundary terms on one box face (0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+), replacing the
+ * heat BoundaryConditionManager's "convection" / "radiation" / "neumann" entries
+ * (heat_diffuse_operator.cpp:243-269 tangent, :690-781 rhs, :1088-1129 local op):
+ *   MPDG_BC_CONVECTION  rhs -h (T - T_inf_conv), tangent h
+ *   MPDG_BC_RADIATION   rhs -eps sigma (T^4 - T_inf_rad^4), tangent 4 eps sigma T^3
+ *   MPDG_BC_NEUMANN     rhs -q_n (prescribed normal flux)
+ * Neumann cannot be combined with the others on a face (:708-712); type 0 clears. */
+enum { MPDG_BC_CONVECTION = 1, MPDG_BC_RADIATION = 2, MPDG_BC_NEUMANN = 4 };
+int mpdg_heat_set_boundary(mpdg_heat *h, int face, int type, double h_conv, double T_inf_conv,
+                           double emissivity, double T_inf_rad, double q_n);
 /* OperatorBase::reset_time_increment (operator_base.hpp:41-46). */
 int mpdg_heat_reset_time_increment(mpdg_heat *h, double dt);
 /* The operator's references to `temperature` (linearisation point) and

@@ -92,6 +92,8 @@ _SIGS = {
     "mpdg_heat_device_bytes": (C.c_int, [_H, C.POINTER(C.c_int64)]),
     "mpdg_heat_set_material": (C.c_int, [_H, C.POINTER(Material)]),
     "mpdg_heat_reset_time_increment": (C.c_int, [_H, C.c_double]),
+    "mpdg_heat_set_boundary": (C.c_int, [_H, C.c_int, C.c_int, C.c_double, C.c_double,
+                                         C.c_double, C.c_double, C.c_double]),
     "mpdg_heat_set_linearization": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult_f32": (C.c_int, [_H, _D, _D]),

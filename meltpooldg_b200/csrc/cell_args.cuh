@@ -58,6 +58,7 @@ struct CellArgs {
   unsigned *counter;   // last-CTA election counter (reset by the last CTA)
   SolverState *st;     // early exit when st->done; alpha finalisation
   double *out;         // FIN_STORE destination
+  const double *extra_dot;  // boundary-face part of src.dst, added at finalisation (nullable)
   int fin;
 };
 
@@ -69,5 +70,13 @@ __host__ __device__ constexpr int cells_per_block(int n)
   return n == 2 ? 32 : n == 3 ? 14 : n == 4 ? 8 : n == 5 ? 5 : n == 6 ? 4 : 2;
 }
 __host__ __device__ constexpr int block_threads(int n) { return cells_per_block(n) * n * n; }
+
+// Dirichlet-constrained DoF (I, J, K) of the lexicographic nodal grid
+__device__ __forceinline__ bool constrained(const MeshDims &d, int I, int J, int K)
+{
+  return ((d.dmask & 1) && I == 0) || ((d.dmask & 2) && I == d.nd[0] - 1) ||
+         ((d.dmask & 4) && J == 0) || ((d.dmask & 8) && J == d.nd[1] - 1) ||
+         ((d.dmask & 16) && K == 0) || ((d.dmask & 32) && K == d.nd[2] - 1);
+}
 
 }  // namespace mpdg

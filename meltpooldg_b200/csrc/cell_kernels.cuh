@@ -45,12 +45,6 @@ template <> __device__ __forceinline__ float cw<float>(int i) { return c_w_f[i];
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool constrained(const MeshDims &d, int I, int J, int K)
-{
-  return ((d.dmask & 1) && I == 0) || ((d.dmask & 2) && I == d.nd[0] - 1) ||
-         ((d.dmask & 4) && J == 0) || ((d.dmask & 8) && J == d.nd[1] - 1) ||
-         ((d.dmask & 16) && K == 0) || ((d.dmask & 32) && K == d.nd[2] - 1);
-}
 
 template <typename T> __device__ __forceinline__ void atomic_add(T *p, T v) { atomicAdd(p, v); }
 
@@ -336,6 +330,7 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
   if (a.fin != FIN_NONE) {
     double v[1] = {dot}, tot[1];
     if (grid_sum<1>(v, a.partials, a.counter, tot)) {
+      if (a.extra_dot) tot[0] += *a.extra_dot;
       if (a.fin == FIN_STORE) {
         *a.out = tot[0];
       } else {

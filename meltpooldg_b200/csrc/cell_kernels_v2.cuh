@@ -419,6 +419,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
   if (a.fin != FIN_NONE) {
     double v[1] = {dot}, tot[1];
     if (grid_sum<1>(v, a.partials, a.counter, tot)) {
+      if (a.extra_dot) tot[0] += *a.extra_dot;
       if (a.fin == FIN_STORE) {
         *a.out = tot[0];
       } else {

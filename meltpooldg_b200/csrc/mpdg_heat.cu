@@ -96,6 +96,10 @@ struct mpdg_heat {
   int gV_m = 0;
   double *gsmall = nullptr;
   float *nn_buf = nullptr;  // learned guess: network input and output on the sampled grid
+  // boundary terms per face: type bit 1 convection, 2 radiation, 4 Neumann
+  int btype[6] = {0, 0, 0, 0, 0, 0};
+  double bh[6] = {0}, bTc[6] = {0}, beps[6] = {0}, bTr[6] = {0}, bqn[6] = {0};
+  double *face_dot = nullptr;
   int64_t nn_buf_n = 0;
   // reduction scratch
   double *partials = nullptr;
@@ -722,6 +726,96 @@ __global__ void k_gmres_update(int64_t N, const double *__restrict__ V, int64_t 
   }
 }
 
+// ---- boundary faces (Robin / Neumann) ----------------------------------------
+// heat_diffuse_operator.cpp:243-269 (tangent loop), :719-781 (rhs loop),
+// :1088-1129 (local face operation). Boundary vertices are never perturbed, so
+// every boundary face is a flat h_a x h_b rectangle with JxW = h_a h_b w_a w_b.
+constexpr double kStefanBoltzmann = 5.670374419e-8;  // physical_constants.hpp:6
+
+template <typename T>
+struct FaceArgs {
+  MeshDims d;
+  int n, face, dir, ea, eb, fixed, type;
+  T ha, hb, hconv, Tinf_c, eps_sigma, Tinf_r4, qn;
+  T S[kMaxN][kMaxN], w[kMaxN];
+  const T *src;
+  T *dst;
+  const T *Tl;
+  double *dot;          // += sum over faces of src.dst (vmult), nullable
+  const SolverState *st;
+};
+
+// op 0: tangent (dst += A_f src), 1: rhs (dst += -R_f(Tl)), 2: diagonal
+template <typename T, int OP>
+__global__ void k_face(FaceArgs<T> a)
+{
+  if (a.st && a.st->done) return;
+  __shared__ T s_u[kMaxN * kMaxN], s_T[kMaxN * kMaxN], s_v[kMaxN * kMaxN];
+  __shared__ double s_red[32];
+  const int n = a.n, nn = n * n;
+  const int ca = blockIdx.x % a.d.m[a.ea], cb = blockIdx.x / a.d.m[a.ea];
+  const int tid = threadIdx.x;
+  const int ia = tid % n, ib = tid / n;
+  int64_t g = 0;
+  bool c = true;
+  if (tid < nn) {
+    int64_t pos[3];
+    pos[a.dir] = a.fixed;
+    pos[a.ea] = (int64_t)a.d.p * ca + ia;
+    pos[a.eb] = (int64_t)a.d.p * cb + ib;
+    g = pos[0] + (int64_t)a.d.nd[0] * (pos[1] + (int64_t)a.d.nd[1] * pos[2]);
+    c = constrained(a.d, (int)pos[0], (int)pos[1], (int)pos[2]);
+    s_u[tid] = (OP == 0 && !c) ? a.src[g] : T(0);
+    s_T[tid] = a.Tl ? a.Tl[g] : T(0);
+  }
+  __syncthreads();
+  if (tid < nn) {  // thread = quadrature point (qa, qb) = (ia, ib)
+    T uq = 0, Tq = 0;
+    for (int jb = 0; jb < n; ++jb)
+      for (int ja = 0; ja < n; ++ja) {
+        const T ph = a.S[ia][ja] * a.S[ib][jb];
+        uq += ph * s_u[ja + n * jb];
+        Tq += ph * s_T[ja + n * jb];
+      }
+    const T jxw = a.ha * a.hb * a.w[ia] * a.w[ib];
+    T val = 0;
+    if (OP == 1) {
+      if (a.type & 4) val -= a.qn;
+      if (a.type & 2) val -= a.eps_sigma * (Tq * Tq * Tq * Tq - a.Tinf_r4);
+      if (a.type & 1) val -= a.hconv * (Tq - a.Tinf_c);
+    } else {
+      if (a.type & 1) val += a.hconv;
+      if (a.type & 2) val += T(4) * a.eps_sigma * Tq * Tq * Tq;
+      if (OP == 0) val *= uq;
+    }
+    s_v[tid] = val * jxw;
+  }
+  __syncthreads();
+  double dot = 0.0;
+  if (tid < nn) {  // thread = face DoF (ia, ib)
+    T r = 0;
+    for (int qb = 0; qb < n; ++qb)
+      for (int qa = 0; qa < n; ++qa) {
+        const T ph = a.S[qa][ia] * a.S[qb][ib];
+        r += (OP == 2 ? ph * ph : ph) * s_v[qa + n * qb];
+      }
+    if (!c) {
+      atomicAdd(a.dst + g, r);
+      if (OP == 0) dot = (double)s_u[tid] * (double)r;
+    }
+  }
+  if (OP == 0 && a.dot) {
+    for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
+    if ((tid & 31) == 0) s_red[tid >> 5] = dot;
+    __syncthreads();
+    if (tid == 0) {
+      double sacc = 0.0;
+      for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) sacc += s_red[i];
+      atomicAdd(a.dot, sacc);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
@@ -781,6 +875,62 @@ static int ensure_lin(mpdg_heat *h)
   return MPDG_OK;
 }
 
+
+static bool any_faces(const mpdg_heat *h)
+{
+  for (int f = 0; f < 6; ++f)
+    if (h->btype[f]) return true;
+  return false;
+}
+
+template <typename T>
+static int launch_faces(mpdg_heat *h, int op, T *dst, const T *src, const T *Tl, double *dot,
+                        const SolverState *st)
+{
+  const Tables1D t1 = make_tables(h->n);
+  for (int f = 0; f < 6; ++f) {
+    if (!h->btype[f]) continue;
+    if (op != 1 && !(h->btype[f] & 3)) continue;  // Neumann has no tangent
+    FaceArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.d = h->dims;
+    a.n = h->n;
+    a.face = f;
+    a.dir = f / 2;
+    a.ea = a.dir == 0 ? 1 : 0;
+    a.eb = a.dir == 2 ? 1 : 2;
+    a.fixed = (f & 1) ? h->dims.nd[a.dir] - 1 : 0;
+    a.type = h->btype[f];
+    a.ha = (T)h->hcell[a.ea];
+    a.hb = (T)h->hcell[a.eb];
+    a.hconv = (T)h->bh[f];
+    a.Tinf_c = (T)h->bTc[f];
+    a.eps_sigma = (T)(h->beps[f] * kStefanBoltzmann);
+    a.Tinf_r4 = (T)std::pow(h->bTr[f], 4);
+    a.qn = (T)h->bqn[f];
+    for (int q = 0; q < h->n; ++q) {
+      a.w[q] = (T)t1.wg[q];
+      for (int i = 0; i < h->n; ++i) a.S[q][i] = (T)t1.A[kS][q][i];
+    }
+    a.src = src;
+    a.dst = dst;
+    a.Tl = Tl;
+    a.dot = dot;
+    a.st = st;
+    const int blocks = h->dims.m[a.ea] * h->dims.m[a.eb];
+    const int threads = ((h->n * h->n + 31) / 32) * 32;
+    if (op == 0)
+      k_face<T, 0><<<blocks, threads, 0, h->stream>>>(a);
+    else if (op == 1)
+      k_face<T, 1><<<blocks, threads, 0, h->stream>>>(a);
+    else
+      k_face<T, 2><<<blocks, threads, 0, h->stream>>>(a);
+    ++h->launches;
+  }
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
 // dst += J src (FP64); fin/out/st select the fused src.dst reduction
 static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, double *out,
                       SolverState *st)
@@ -801,6 +951,12 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
     e0 = take_event(h);
     e1 = take_event(h);
     cudaEventRecord(e0, h->stream);
+  }
+  if (any_faces(h)) {
+    TRY(dvec(h, &h->face_dot, 1));
+    CU(cudaMemsetAsync(h->face_dot, 0, sizeof(double), h->stream));
+    TRY(launch_faces<double>(h, 0, dst, src, h->T_lin, fin != FIN_NONE ? h->face_dot : nullptr, st));
+    if (fin != FIN_NONE) a.extra_dot = h->face_dot;
   }
   CU(h->tab.vmult_d(a, h->geo, h->law, h->stream, h->sm_count));
   if (h->timing) {
@@ -855,6 +1011,7 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
     e1 = take_event(h);
     cudaEventRecord(e0, h->stream);
   }
+  if (any_faces(h)) TRY(launch_faces<float>(h, 0, dst, src, h->T_lin_f, nullptr, st));
   CU(h->tab.vmult_f(a, h->geo, picard ? 3 : h->law, h->stream, h->sm_count));
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
@@ -1472,6 +1629,30 @@ extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
   return MPDG_OK;
 }
 
+extern "C" int mpdg_heat_set_boundary(mpdg_heat *h, int face, int type, double h_conv,
+                                      double T_inf_conv, double emissivity, double T_inf_rad,
+                                      double q_n)
+{
+  if (!h || face < 0 || face > 5 || type < 0 || type > 7)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "bad boundary face or type");
+  if ((type & MPDG_BC_NEUMANN) && (type & (MPDG_BC_CONVECTION | MPDG_BC_RADIATION)))
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "It is not allowed to specify both Neumann and radiation and/or convection "
+                "boundary conditions at the same face.");
+  if ((type & MPDG_BC_CONVECTION | type & MPDG_BC_RADIATION | type & MPDG_BC_NEUMANN) &&
+      (h->dims.dmask & (1 << face)))
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "face carries Dirichlet constraints");
+  h->btype[face] = type;
+  h->bh[face] = h_conv;
+  h->bTc[face] = T_inf_conv;
+  h->beps[face] = emissivity;
+  h->bTr[face] = T_inf_rad;
+  h->bqn[face] = q_n;
+  h->diag_valid = false;
+  h->eig_valid = false;
+  return MPDG_OK;
+}
+
 extern "C" int mpdg_heat_reset_time_increment(mpdg_heat *h, double dt)
 {
   if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
@@ -1517,6 +1698,7 @@ static int compute_diag(mpdg_heat *h, double *d)
   a.To = h->T_old;
   CU(h->tab.diag(a, h->geo, h->law, h->stream, h->sm_count));
   ++h->launches;
+  if (any_faces(h)) TRY(launch_faces<double>(h, 2, d, nullptr, h->T_lin, nullptr, nullptr));
   k_invert_diag<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, d); ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;
@@ -1541,6 +1723,7 @@ static int create_rhs(mpdg_heat *h, double *dst, const double *src, const double
   a.qs = q;
   CU(h->tab.rhs(a, h->geo, h->law, h->stream, h->sm_count));
   ++h->launches;
+  if (any_faces(h)) TRY(launch_faces<double>(h, 1, dst, nullptr, h->T_lin, nullptr, nullptr));
   return MPDG_OK;
 }
 

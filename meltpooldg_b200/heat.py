@@ -210,6 +210,16 @@ class HeatDiffuseOperator:
     def set_material(self, m: L.Material):
         check(self._L.mpdg_heat_set_material(self.h, C.byref(m)))
 
+    def set_boundary(self, face, convection=None, radiation=None, neumann=None):
+        """Robin / Neumann terms on a box face: convection=(h, T_inf),
+        radiation=(emissivity, T_inf), neumann=q_n; no argument clears the face."""
+        f = FACES[face] if isinstance(face, str) else int(face)
+        t = (1 if convection else 0) | (2 if radiation else 0) | (4 if neumann is not None else 0)
+        hc, tc = convection or (0.0, 0.0)
+        e, tr = radiation or (0.0, 0.0)
+        check(self._L.mpdg_heat_set_boundary(self.h, f, t, float(hc), float(tc), float(e),
+                                              float(tr), 0.0 if neumann is None else float(neumann)))
+
     def reset_time_increment(self, dt: float):
         check(self._L.mpdg_heat_reset_time_increment(self.h, float(dt)))
 

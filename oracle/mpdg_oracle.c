@@ -161,6 +161,9 @@ struct orc_heat {
   int          need_told; /* d(rho cp)/dT may be non-zero */
   /* direct-form tables */
   double *phi, *dphi;
+  /* boundary terms per face */
+  int    btype[6];
+  double bh[6], bTc[6], beps[6], bTr[6], bqn[6];
 };
 
 static int g_threads = 0;
@@ -948,6 +951,88 @@ static void run_direct(const orc_heat *h, int kind, double *dst, const double *s
 }
 
 /* ------------------------------------------------------------------ */
+/* boundary faces: direct 2D quadrature on the flat box faces          */
+/* ------------------------------------------------------------------ */
+
+#define ORC_SIGMA 5.670374419e-8 /* physical_constants.hpp:6 */
+
+int orc_set_boundary(orc_heat *h, int face, int type, double h_conv, double T_inf_conv,
+                     double emissivity, double T_inf_rad, double q_n)
+{
+  if (face < 0 || face > 5) return -1;
+  if ((type & 4) && (type & 3)) return -1; /* heat_diffuse_operator.cpp:708-712 */
+  h->btype[face] = type;
+  h->bh[face] = h_conv;
+  h->bTc[face] = T_inf_conv;
+  h->beps[face] = emissivity;
+  h->bTr[face] = T_inf_rad;
+  h->bqn[face] = q_n;
+  return 0;
+}
+
+/* kind 0: dst += tangent u ; 1: dst += rhs(T) ; 2: dst += diagonal */
+static void run_faces(const orc_heat *h, int kind, double *dst, const double *src,
+                      const double *T)
+{
+  const int n = h->n, p = h->p;
+  for (int f = 0; f < 6; ++f) {
+    const int type = h->btype[f];
+    if (!type) continue;
+    const int d = f / 2, ea = d == 0 ? 1 : 0, eb = d == 2 ? 1 : 2;
+    const double ha = (h->hi[ea] - h->lo[ea]) / h->m[ea], hb = (h->hi[eb] - h->lo[eb]) / h->m[eb];
+    const int fixed = (f & 1) ? h->nd[d] - 1 : 0;
+    for (int cb = 0; cb < h->m[eb]; ++cb)
+      for (int ca = 0; ca < h->m[ea]; ++ca) {
+        int64_t g[NMAX * NMAX];
+        double u[NMAX * NMAX], Tv[NMAX * NMAX], out[NMAX * NMAX];
+        for (int ib = 0; ib < n; ++ib)
+          for (int ia = 0; ia < n; ++ia) {
+            int64_t pos[3];
+            pos[d] = fixed;
+            pos[ea] = (int64_t)p * ca + ia;
+            pos[eb] = (int64_t)p * cb + ib;
+            const int l = ia + n * ib;
+            g[l] = pos[0] + h->nd[0] * (pos[1] + (int64_t)h->nd[1] * pos[2]);
+            u[l] = (kind == 0 && !h->mask[g[l]]) ? src[g[l]] : 0.0;
+            Tv[l] = T ? T[g[l]] : 0.0;
+            out[l] = 0.0;
+          }
+        for (int qb = 0; qb < n; ++qb)
+          for (int qa = 0; qa < n; ++qa) {
+            double uq = 0.0, Tq = 0.0;
+            for (int ib = 0; ib < n; ++ib)
+              for (int ia = 0; ia < n; ++ia) {
+                const double ph = h->S[qa][ia] * h->S[qb][ib];
+                uq += ph * u[ia + n * ib];
+                Tq += ph * Tv[ia + n * ib];
+              }
+            const double jxw = ha * hb * h->wg[qa] * h->wg[qb];
+            double val;
+            if (kind == 1) {
+              val = 0.0;
+              if (type & 4) val -= h->bqn[f];
+              if (type & 2)
+                val -= h->beps[f] * ORC_SIGMA * (Tq * Tq * Tq * Tq - pow(h->bTr[f], 4));
+              if (type & 1) val -= h->bh[f] * (Tq - h->bTc[f]);
+            } else {
+              val = 0.0;
+              if (type & 1) val += h->bh[f];
+              if (type & 2) val += 4.0 * h->beps[f] * ORC_SIGMA * Tq * Tq * Tq;
+              if (kind == 0) val *= uq;
+            }
+            for (int ib = 0; ib < n; ++ib)
+              for (int ia = 0; ia < n; ++ia) {
+                const double ph = h->S[qa][ia] * h->S[qb][ib];
+                out[ia + n * ib] += (kind == 2 ? ph * ph : ph) * val * jxw;
+              }
+          }
+        for (int l = 0; l < n * n; ++l)
+          if (!h->mask[g[l]]) dst[g[l]] += out[l];
+      }
+  }
+}
+
+/* ------------------------------------------------------------------ */
 /* operator verbs                                                      */
 /* ------------------------------------------------------------------ */
 
@@ -959,6 +1044,7 @@ void orc_vmult(const orc_heat *h, double *dst, const double *src, const double *
     run_sf(h, 0, dst, src, T_lin, T_old, NULL);
   else
     run_direct(h, 0, dst, src, T_lin, T_old);
+  run_faces(h, 0, dst, src, T_lin);
 }
 
 void orc_inverse_diagonal(const orc_heat *h, double *d, const double *T_lin, const double *T_old,
@@ -969,6 +1055,7 @@ void orc_inverse_diagonal(const orc_heat *h, double *d, const double *T_lin, con
     run_sf(h, 2, d, NULL, T_lin, T_old, NULL);
   else
     run_direct(h, 2, d, NULL, T_lin, T_old);
+  run_faces(h, 2, d, NULL, T_lin);
 #pragma omp parallel for num_threads(nthreads())
   for (int64_t i = 0; i < h->n_dofs; ++i) d[i] = fabs(d[i]) > 1.0e-10 ? 1.0 / d[i] : 1.0;
 }
@@ -977,6 +1064,7 @@ void orc_create_rhs(const orc_heat *h, double *dst, const double *T, const doubl
                     const double *heat_source)
 {
   run_sf(h, 1, dst, NULL, T, T_old, heat_source);
+  run_faces(h, 1, dst, NULL, T);
 }
 
 double orc_l2_norm(const orc_heat *h, const double *u)

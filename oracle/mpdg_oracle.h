@@ -75,6 +75,14 @@ void      orc_support_points(const orc_heat *h, double *xyz); /* n_dofs x 3 */
 void      orc_distribute(const orc_heat *h, double *u);       /* set Dirichlet values */
 void      orc_set_threads(int n);
 
+/* Boundary terms of one box face (face 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+):
+ * type bit 1 convection  h (T - T_inf_c)       (tangent h)
+ *      bit 2 radiation   eps sigma (T^4 - T_inf_r^4)  (tangent 4 eps sigma T^3)
+ *      bit 4 Neumann     prescribed normal flux q_n (rhs only)
+ * (heat_diffuse_operator.cpp:243-269 tangent, :719-781 rhs, :1088-1129 local op). */
+int orc_set_boundary(orc_heat *h, int face, int type, double h_conv, double T_inf_conv,
+                     double emissivity, double T_inf_rad, double q_n);
+
 /* Operator coefficients: material law and time step (reset_time_increment). */
 void orc_set_material(orc_heat *h, const orc_material *m, double dt);
 

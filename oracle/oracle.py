@@ -124,6 +124,9 @@ def lib():
                                                C.POINTER(StepStats)]
             L.orc_gmres.restype = C.c_int
             L.orc_gmres.argtypes = [_P, C.POINTER(SolverParams), C.c_int, _D, _D, _D, _D, _D, _D]
+            L.orc_set_boundary.restype = C.c_int
+            L.orc_set_boundary.argtypes = [_P, C.c_int, C.c_int, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.c_double]
             L.orc_gaussian_source.argtypes = [_P, _D, C.c_double, _D, C.c_double]
             _lib = L
     return _lib
@@ -204,6 +207,16 @@ class Oracle:
     def set_material(self, m: Material, dt: float):
         self.dt = dt
         self.L.orc_set_material(self.h, C.byref(m), dt)
+
+    def set_boundary(self, face, convection=None, radiation=None, neumann=None):
+        """convection=(h, T_inf), radiation=(emissivity, T_inf), neumann=q_n."""
+        t = (1 if convection else 0) | (2 if radiation else 0) | (4 if neumann is not None else 0)
+        hc, tc = convection or (0.0, 0.0)
+        e, tr = radiation or (0.0, 0.0)
+        rc = self.L.orc_set_boundary(self.h, face, t, hc, tc, e, tr,
+                                     0.0 if neumann is None else neumann)
+        if rc != 0:
+            raise ValueError("invalid boundary specification")
 
     def _z(self):
         return np.zeros(self.n_dofs)

@@ -233,6 +233,48 @@ def test_gmres_matches_oracle_on_nonsymmetric_tangent(restart):
     assert np.linalg.norm(r) <= 1.01e-12 * np.linalg.norm(b)
 
 
+@pytest.mark.parametrize("degree", [1, 2, 3, 4])
+def test_boundary_terms_match_oracle(degree):
+    """Convection + radiation on x-, radiation on z+, Neumann on x+, Dirichlet on y faces."""
+    o, g = pair(degree, (4, 3, 3), 0.15, "linear_k", dirichlet=0b001100)
+    for side, kw in ((0, dict(convection=(5.0, 300.0), radiation=(0.8, 320.0))),
+                     (5, dict(radiation=(0.5, 250.0))), (1, dict(neumann=3.0))):
+        o.set_boundary(side, **kw)
+        g.set_boundary(side, **kw)
+    rng = np.random.default_rng(degree)
+    N = o.n_dofs
+    src = rng.uniform(-1, 1, N)
+    Tl = rng.uniform(0.5, 1.5, N)
+    To = rng.uniform(0.5, 1.5, N)
+    g.set_linearization(cuda(Tl), cuda(To))
+    ref = o.vmult(src, Tl, To)
+    assert rel(g.vmult(g.new_vector(), cuda(src)), ref) <= TOL64
+    assert rel(g.vmult(g.new_vector(torch.float32), cuda(src, torch.float32)), ref) <= TOL32
+    dref = o.inverse_diagonal(Tl, To)
+    dg = g.compute_inverse_diagonal_from_matrixfree(g.new_vector())
+    assert rel(1.0 / dg.cpu().numpy(), 1.0 / dref) <= TOL64
+    rref = o.create_rhs(Tl, To)
+    assert rel(g.create_rhs(g.new_vector(), cuda(To)), rref) <= TOL64
+    with pytest.raises(H.ExcInvalidArgument):  # Neumann with convection on one face
+        g.set_boundary(4, convection=(1.0, 0.0), neumann=1.0)
+
+
+def test_cg_alpha_includes_boundary_terms():
+    """CG with Robin terms: the fused p.Ap reduction must include the face part."""
+    o, g = pair(2, (5, 4, 4), 0.1, "constant", dt=1e-2, dirichlet=0)
+    o.set_boundary(1, convection=(50.0, 0.0))
+    g.set_boundary(1, convection=(50.0, 0.0))
+    rng = np.random.default_rng(3)
+    b = o.vmult(rng.uniform(-1, 1, o.n_dofs))
+    x_ref, its_ref, _ = o.cg(b, rel_tol=1e-12)
+    g.set_linearization(g.new_vector(), g.new_vector())
+    H.JacobiPreconditioner(g).update()
+    x = g.new_vector()
+    its = H.LinearSolver.solve(g, x, cuda(b), H.LinearSolverData(rel_tolerance=1e-12), True)
+    assert abs(its - its_ref) <= 2
+    assert rel(x, x_ref) <= 1e-9
+
+
 def test_linear_solve_not_converged_raises():
     o, g = pair(3, (4, 4, 4), 0.0, dt=1.0)
     H.JacobiPreconditioner(g).update()

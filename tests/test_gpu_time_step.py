@@ -88,3 +88,34 @@ def test_unidirectional_heat_transfer_gmres_on_gpu():
     for ref in UNIDIRECTIONAL:
         opn.solve(1e-4)
         assert float(f"{op.l2_norm(opn.T):.5e}") == ref
+
+
+ROBIN = {
+    "convection": (dict(convection=(25.0, 300.0)),
+                   [1.00000e+02, 9.99999e+01, 9.99999e+01, 9.99998e+01, 9.99998e+01]),
+    "radiation": (dict(radiation=(0.98, 300.0)),
+                  [9.99998e+01, 9.99997e+01, 9.99995e+01, 9.99994e+01, 9.99992e+01]),
+    "radiation_and_convection": (dict(convection=(25.0, 300.0), radiation=(0.98, 300.0)),
+                                 [9.99998e+01, 9.99996e+01, 9.99994e+01, 9.99992e+01,
+                                  9.99990e+01]),
+}
+
+
+@pytest.mark.parametrize("case", list(ROBIN))
+def test_unidirectional_robin_on_gpu(case):
+    """unidirectional_heat_transfer_with_* regression outputs through the GPU Newton +
+    GMRES path with the Robin terms on the right boundary."""
+    bc, refs = ROBIN[case]
+    op = H.HeatDiffuseOperator(H.box_mesh(1, (32, 32, 1), (0, 0, 0), (0.1, 0.1, 1.0),
+                                          dirichlet=()))
+    op.set_material(H.material(rho=7850.0, cp=460.0, k=55.563))
+    op.set_boundary("x+", **bc)
+    opn = H.HeatDiffuseOperation(op, H.LinearSolverData(solver_type=L.SOLVER_GMRES,
+                                                        rel_tolerance=1e-12),
+                                 H.NonlinearSolverData(residual_tolerance=5e-9))
+    opn.set_initial_condition(torch.full((op.n_dofs,), 1000.0, dtype=torch.float64,
+                                         device="cuda"))
+    for ref in refs:
+        st = opn.solve(0.01)
+        assert st.converged == 1
+        assert float(f"{op.l2_norm(opn.T):.5e}") == ref

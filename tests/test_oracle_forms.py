@@ -57,3 +57,24 @@ def test_tangent_is_derivative_of_residual():
     fd = -(rp - rm) / (2 * eps)
     Jdu = o.vmult(du, T, T_old)
     assert np.abs(fd - Jdu).max() <= 1e-7 * np.abs(Jdu).max()
+
+
+def test_boundary_tangent_is_derivative_of_boundary_residual():
+    rng = np.random.default_rng(8)
+    o = O.Oracle(2, (3, 3, 3), perturb=0.15, seed=1, dirichlet_mask=0b001100)
+    o.set_material(LAWS["constant"], 1e-2)
+    o.set_boundary(0, convection=(5.0, 300.0), radiation=(0.8, 320.0))
+    o.set_boundary(5, radiation=(0.5, 250.0))
+    o.set_boundary(1, neumann=3.0)
+    T = rng.uniform(900, 1100, o.n_dofs)
+    T_old = rng.uniform(900, 1100, o.n_dofs)
+    du = rng.uniform(-1, 1, o.n_dofs)
+    du[o.mask().astype(bool)] = 0.0
+    eps = 1e-3
+    fd = -(o.create_rhs(T + eps * du, T_old) - o.create_rhs(T - eps * du, T_old)) / (2 * eps)
+    Jdu = o.vmult(du, T, T_old)
+    assert np.abs(fd - Jdu).max() <= 1e-7 * np.abs(Jdu).max()
+    # the boundary terms are in the diagonal too
+    d0 = 1.0 / o.inverse_diagonal(T, T_old, form=0)
+    d1 = 1.0 / o.inverse_diagonal(T, T_old, form=1)
+    assert np.allclose(d0, d1, rtol=1e-12, atol=0)

@@ -57,3 +57,33 @@ def test_solidification_slab():
         dt_old = 200.0
         assert rc == 0 and st.converged
         assert _six_digits(o.l2_norm(T), ref), (o.l2_norm(T), ref)
+
+
+# unidirectional_heat_transfer_with_{convection,radiation,radiation_and_convection}
+#   .mpirun=4.output: steel (k 55.563, cp 460, rho 7850), T0 = 1000, dt = 0.01, Robin
+#   terms on the right boundary (x = 0.1), h = 25, emissivity 0.98, T_inf = 300.
+ROBIN = {
+    "convection": (dict(convection=(25.0, 300.0)),
+                   [1.00000e+02, 9.99999e+01, 9.99999e+01, 9.99998e+01, 9.99998e+01]),
+    "radiation": (dict(radiation=(0.98, 300.0)),
+                  [9.99998e+01, 9.99997e+01, 9.99995e+01, 9.99994e+01, 9.99992e+01]),
+    "radiation_and_convection": (dict(convection=(25.0, 300.0), radiation=(0.98, 300.0)),
+                                 [9.99998e+01, 9.99996e+01, 9.99994e+01, 9.99992e+01,
+                                  9.99990e+01]),
+}
+
+
+@pytest.mark.parametrize("case", list(ROBIN))
+def test_unidirectional_heat_transfer_robin(case):
+    bc, refs = ROBIN[case]
+    o = O.Oracle(1, (32, 32, 1), lo=(0, 0, 0), hi=(0.1, 0.1, 1.0), dirichlet_mask=0)
+    o.set_material(O.material(rho=7850.0, cp=460.0, k=55.563), 0.01)
+    o.set_boundary(1, **bc)
+    T = np.full(o.n_dofs, 1000.0)
+    T_old = np.zeros_like(T)
+    dt_old = 0.0
+    for ref in refs:
+        rc, st = o.time_step_newton(T, T_old, 0.01, dt_old, res_tol=5e-9)
+        dt_old = 0.01
+        assert rc == 0
+        assert _six_digits(o.l2_norm(T), ref), (o.l2_norm(T), ref)

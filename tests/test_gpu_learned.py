@@ -56,7 +56,9 @@ def test_learned_guess_on_held_out_path():
     # measured on this pool: 1.1-2.1x smaller initial residual but no fewer CG iterations
     # (132 -> 134); the solver iterates to the same tolerance, so at most a few more
     assert sum(its1) <= 1.05 * sum(its0) + 1
-    assert torch.linalg.vector_norm(T1 - T0) <= 1e-6 * torch.linalg.vector_norm(T0)
+    # both runs stop at |b - J T| <= 1e-8 |b| from different guesses, so the fields may
+    # differ by up to ~cond(J) * 1e-8 per step (measured 6e-6 after 14 steps)
+    assert torch.linalg.vector_norm(T1 - T0) <= 5e-5 * torch.linalg.vector_norm(T0)
 
 
 def test_guess_rejects_a_network_of_another_grid():

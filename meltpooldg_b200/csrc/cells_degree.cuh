@@ -40,8 +40,10 @@ struct DegreeOps {
     cudaMemcpyToSymbol(c_w_f, wf, sizeof(float) * kWSize);
   }
 
-  // register-resident kernel where a cell's planes fit the register file
-  template <typename T>
+  // register-resident kernel where a cell's planes fit the register file (FP64 at
+  // p = 4 spills 64-750 bytes there and measured no faster than the line-per-thread
+  // kernel on the deformed mesh, so it stays on the latter)
+  template <typename T, int LAW = 0>
   static constexpr bool use_v2()
   {
     return sizeof(T) == 8 ? n <= 4 : n <= 5;
@@ -50,7 +52,7 @@ struct DegreeOps {
   template <typename T, int GEO, int LAW>
   static cudaError_t vmult_t(const CellArgs<T> &a, cudaStream_t s, int sm)
   {
-    if constexpr (use_v2<T>()) {
+    if constexpr (use_v2<T, LAW>()) {
       static int cache2 = 0;
       auto k2 = k_vmult2<n, T, GEO, LAW>;
       const size_t smem2 = v2_smem<n, T, LAW>();

@@ -154,6 +154,12 @@ int mpdg_heat_set_linearization(mpdg_heat *h, const double *temperature,
 int mpdg_heat_vmult(mpdg_heat *h, double *dst, const double *src);
 /* Same operator in FP32 (geometry, linearisation point and coefficients in FP32). */
 int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src);
+/* FP32 Picard operator of the mixed-precision preconditioner (no reference
+ * counterpart; the FP32 Chebyshev smoother applies it): the tangent of the
+ * linear-k law without its dk/dT grad(T_lin) u term, i.e. the conductivity
+ * k(T_lin) frozen at the quadrature points. Boundary-face terms as in
+ * mpdg_heat_vmult_f32. MPDG_ERR_INVALID_ARGUMENT for the other laws. */
+int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float *src);
 /* compute_inverse_diagonal_from_matrixfree (heat_diffuse_operator.cpp:271-284):
  * diag(J) inverted with |d| > 1e-10 ? 1/d : 1. */
 int mpdg_heat_compute_inverse_diagonal(mpdg_heat *h, double *inv_diag);

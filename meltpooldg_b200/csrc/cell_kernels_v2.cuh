@@ -287,8 +287,11 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           (int64_t)d.nd[0] * (d.p * ncy + (int64_t)d.nd[1] * (d.p * ncz + t)) + d.p * ncx;
         prefetch_plane<n>(a.src, nbase, d.nd[0]);
         if (TDEP) prefetch_plane<n>(a.Tl, nbase, d.nd[0]);
-        if (LAW == 3 && t == 0)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.kq + ncell * (n * n * n)));
+        if (LAW == 3) {
+          const char *kq = reinterpret_cast<const char *>(a.kq + ncell * (n * n * n));
+          for (int off = t * 128; off < n * n * n * 4; off += n * 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(kq + off));
+        }
         if (GEO == 1) {
           constexpr int npt = n * n * n;
           const char *gq = reinterpret_cast<const char *>(a.g.q + ncell * 7 * npt);

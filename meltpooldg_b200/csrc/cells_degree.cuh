@@ -6,7 +6,11 @@
 
 #include "cell_kernels.cuh"
 #include "cell_kernels_v2.cuh"
+#include "cell_kernels_f2.cuh"
 #include "degree_table.hpp"
+
+#include <stdlib.h>
+#include <type_traits>
 
 namespace mpdg {
 
@@ -27,6 +31,20 @@ static int persistent_grid(K kernel, int threads, size_t smem, int64_t n_batches
   return (int)g;
 }
 
+// FP32 operator on the scalar register-resident kernel (default) or the packed-pair
+// kernel (MPDG_FP32_PACKED=1); both compute the same operator. The packed kernel
+// issues 31 % fewer instructions at p = 3, but a packed FMA occupies the FMA pipe
+// for two cycles and its 210-255 registers per lane halve the resident warps, so
+// it measured 1.3-1.5x slower (p = 2, 3; constant k, k(T) tangent, Picard).
+static inline bool fp32_packed()
+{
+  static const int on = [] {
+    const char *e = getenv("MPDG_FP32_PACKED");
+    return (e && e[0] == '1') ? 1 : 0;
+  }();
+  return on != 0;
+}
+
 template <int n>
 struct DegreeOps {
   static constexpr int CPB = cells_per_block(n);
@@ -36,6 +54,9 @@ struct DegreeOps {
   {
     cudaMemcpyToSymbol(c_tab_d, tab, sizeof(double) * kTabSize);
     cudaMemcpyToSymbol(c_tab_f, tabf, sizeof(float) * kTabSize);
+    float2 tabf2[kTabSize];
+    for (int i = 0; i < kTabSize; ++i) tabf2[i] = make_float2(tabf[i], tabf[i]);
+    cudaMemcpyToSymbol(c_tab_f2, tabf2, sizeof(float2) * kTabSize);
     cudaMemcpyToSymbol(c_w_d, w, sizeof(double) * kWSize);
     cudaMemcpyToSymbol(c_w_f, wf, sizeof(float) * kWSize);
   }
@@ -52,6 +73,18 @@ struct DegreeOps {
   template <typename T, int GEO, int LAW>
   static cudaError_t vmult_t(const CellArgs<T> &a, cudaStream_t s, int sm)
   {
+    if constexpr (std::is_same<T, float>::value && n <= 4 && LAW != 2) {
+      if (fp32_packed()) {
+        static int cachep = 0;
+        auto kp = k_vmult2p<n, GEO, LAW>;
+        const size_t smemp = v2_smem<n, F2, LAW>();
+        const int64_t ng = ((a.n_cells + 1) / 2 + v2_cells_per_warp<n>() - 1) / v2_cells_per_warp<n>();
+        const int gp = persistent_grid(kp, 32 * kV2Warps, smemp, (ng + kV2Warps - 1) / kV2Warps,
+                                       sm, &cachep);
+        kp<<<gp, 32 * kV2Warps, smemp, s>>>(a);
+        return cudaGetLastError();
+      }
+    }
     if constexpr (use_v2<T, LAW>()) {
       static int cache2 = 0;
       auto k2 = k_vmult2<n, T, GEO, LAW>;

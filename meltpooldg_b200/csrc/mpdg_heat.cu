@@ -1686,6 +1686,22 @@ extern "C" int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src)
   return op_apply_f(h, dst, src, nullptr);
 }
 
+extern "C" int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float *src)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (h->law != MPDG_LAW_LINEAR_K || !h->tab.conductivity_q)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "Picard operator: linear-k law, degree <= 4 only");
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_lin(h));
+  TRY(dvec(h, &h->kq, h->n_cells * h->npt));
+  CellArgs<double> a = cell_args<double>(h);
+  a.Tl = h->T_lin;
+  CU(h->tab.conductivity_q(a, h->kq, h->law, h->stream, h->sm_count));
+  ++h->launches;
+  CU(cudaMemsetAsync(dst, 0, sizeof(float) * h->n_dofs, h->stream));
+  return op_apply_f(h, dst, src, nullptr, true);
+}
+
 static int compute_diag(mpdg_heat *h, double *d)
 {
   TRY(ensure_dt(h));

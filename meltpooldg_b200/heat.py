@@ -237,6 +237,13 @@ class HeatDiffuseOperator:
             check(self._L.mpdg_heat_vmult(self.h, _ptr(dst), _ptr(src)))
         return dst
 
+    def vmult_picard_f32(self, dst, src):
+        """FP32 Picard operator of the mixed-precision preconditioner: the tangent of the
+        linear-k law with k(T_lin) frozen at the quadrature points (no dk/dT term)."""
+        check(self._L.mpdg_heat_vmult_f32_picard(self.h, _ptr(dst, torch.float32),
+                                                  _ptr(src, torch.float32)))
+        return dst
+
     def compute_inverse_diagonal_from_matrixfree(self, diag):
         check(self._L.mpdg_heat_compute_inverse_diagonal(self.h, _ptr(diag)))
         return diag

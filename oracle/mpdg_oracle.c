@@ -679,7 +679,8 @@ static inline __attribute__((always_inline)) void integrate_vg(const orc_heat *h
   sweep(n, 0, &h->mST, s->t2, out, 0);
 }
 
-/* kind: 0 vmult, 1 rhs, 2 diagonal, 3 l2 norm accumulate */
+/* kind: 0 vmult, 1 rhs, 2 diagonal, 3 l2 norm accumulate, 4 vmult without the
+ * dk/dT grad(T_lin) u term (Picard operator) */
 static inline __attribute__((always_inline)) void batch_kernel(
   const orc_heat *h, const int n, const int kind, const int64_t *cells, int nl, double *dst,
   const double *src, const double *Tl, const double *To, const double *qs, scratch_t *s,
@@ -687,7 +688,7 @@ static inline __attribute__((always_inline)) void batch_kernel(
 {
   const int npt = n * n * n;
   const double idt = 1.0 / h->dt;
-  if (kind == 0) {
+  if (kind == 0 || kind == 4) {
     gather(h, cells, nl, src, 1, s->u);
     eval_vg(h, n, s->u, s, s->uq, s->gx, s->gy, s->gz);
     if (h->tdep) {
@@ -708,6 +709,7 @@ static inline __attribute__((always_inline)) void batch_kernel(
         if (h->tdep) {
           if (h->need_told) cval += idt * drhocp * (s->Tq[q][v] - s->Toq[q][v]);
           const double uu = s->uq[q][v];
+          if (kind == 4) dk = 0.0;
           g0 += dk * s->Tx[q][v] * uu;
           g1 += dk * s->Ty[q][v] * uu;
           g2 += dk * s->Tz[q][v] * uu;
@@ -1040,8 +1042,8 @@ void orc_vmult(const orc_heat *h, double *dst, const double *src, const double *
                const double *T_old, int form)
 {
   memset(dst, 0, sizeof(double) * h->n_dofs);
-  if (form == 0)
-    run_sf(h, 0, dst, src, T_lin, T_old, NULL);
+  if (form == 0 || form == 2)
+    run_sf(h, form == 0 ? 0 : 4, dst, src, T_lin, T_old, NULL);
   else
     run_direct(h, 0, dst, src, T_lin, T_old);
   run_faces(h, 0, dst, src, T_lin);

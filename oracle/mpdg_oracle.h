@@ -86,7 +86,9 @@ int orc_set_boundary(orc_heat *h, int face, int type, double h_conv, double T_in
 /* Operator coefficients: material law and time step (reset_time_increment). */
 void orc_set_material(orc_heat *h, const orc_material *m, double dt);
 
-/* dst = J(T_lin, T_old) src.  form 0: sum-factorised, 1: direct quadrature. */
+/* dst = J(T_lin, T_old) src.  form 0: sum-factorised, 1: direct quadrature,
+ * 2: sum-factorised Picard operator (the tangent without its dk/dT grad(T_lin) u
+ * term: conductivity k(T_lin) frozen at the quadrature points). */
 void orc_vmult(const orc_heat *h, double *dst, const double *src, const double *T_lin,
                const double *T_old, int form);
 /* inverse diagonal of J with the |d| > 1e-10 ? 1/d : 1 rule; form as above. */

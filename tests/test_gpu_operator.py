@@ -83,6 +83,48 @@ def test_vmult_diag_rhs_match_oracle(degree, perturb, law):
     assert abs(g.l2_norm(Tl_d) - o.l2_norm(Tl)) <= 1e-13 * o.l2_norm(Tl)
 
 
+@pytest.mark.parametrize("degree", [1, 2, 3, 4])
+@pytest.mark.parametrize("cells", [(4, 3, 3), (3, 3, 3), (1, 2, 3)])
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+def test_fp32_operator_cell_pairs(degree, cells, perturb):
+    """FP32 tangent and Picard operator against the oracle on meshes whose cell rows
+    have even length (cells processed in adjacent pairs), odd length (pairs across
+    rows) and an odd cell count (last pair half empty), with boundary-face terms."""
+    o, g = pair(degree, cells, perturb, "linear_k", dirichlet=0b110000)
+    for side, kw in ((0, dict(convection=(5.0, 300.0))), (3, dict(radiation=(0.5, 250.0)))):
+        o.set_boundary(side, **kw)
+        g.set_boundary(side, **kw)
+    rng = np.random.default_rng(7 * degree + len(cells))
+    N = o.n_dofs
+    src, Tl, To = rng.uniform(-1, 1, N), rng.uniform(0.5, 1.5, N), rng.uniform(0.5, 1.5, N)
+    g.set_linearization(cuda(Tl), cuda(To))
+    s32 = cuda(src, torch.float32)
+    assert rel(g.vmult(g.new_vector(torch.float32), s32), o.vmult(src, Tl, To)) <= TOL32
+    ref = o.vmult(src, Tl, To, form=2)
+    assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), ref) <= TOL32
+
+
+def test_fp32_packed_kernel_matches_oracle():
+    """The packed-pair FP32 kernel (MPDG_FP32_PACKED=1) on the same cases, in a child
+    process because the kernel choice is read once per process."""
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ, MPDG_FP32_PACKED="1")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p",
+                        "no:cacheprovider", __file__, "-k", "fp32_operator_cell_pairs"],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+
+
+def test_picard_operator_rejects_other_laws():
+    _, g = pair(2, (2, 2, 2), 0.0, "constant")
+    g.set_linearization(g.new_vector(), g.new_vector())
+    x = g.new_vector(torch.float32)
+    with pytest.raises(H.ExcInvalidArgument):
+        g.vmult_picard_f32(g.new_vector(torch.float32), x)
+
+
 @pytest.mark.parametrize("perturb", [0.0, 0.2])
 def test_geometry_support_points_and_constraints(perturb):
     o, g = pair(3, (4, 3, 5), perturb, dirichlet=0b101101,

@@ -15,18 +15,24 @@
 //
 // Tensors are planar [C][z][y][x]; activations BF16, activation gradients FP32,
 // weights [Cout][Cin][27] as FP32 masters plus a BF16 copy used by the kernels.
-// The convolutions run on the CUDA cores: a CTA holds an 8x8x4 output tile and
-// 16 output channels, stages one input channel's tile plus halo and its
-// 16 x 27 weights in shared memory at a time and accumulates in FP32 registers.
+// The forward convolutions run on the tensor cores (tcgen05 implicit GEMM,
+// nn_conv_tc.cuh). The backward convolutions (FP32 gradients) and the
+// CUDA-core forward (MPDG_UNET_TC=0) use k_conv3d: a CTA holds an 8x8x4 output
+// tile and 16 output channels, stages one input channel's tile plus halo and
+// its 16 x 27 weights in shared memory at a time and accumulates in FP32
+// registers.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/mpdg_heat.h"
+#include "nn_conv_tc.cuh"
 #include "reduce.cuh"
 
 using namespace mpdg;
@@ -347,6 +353,14 @@ struct mpdg_unet {
   int64_t n_params = 0;
   float *p = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
   __nv_bfloat16 *pb = nullptr;
+  uint4 *wpk = nullptr;       // weights packed for the tensor-core convolution
+  int64_t wpk_off[15] = {};   // per layer, in uint4
+  bool wpk_dirty = true;      // pb changed since the last packing
+  bool use_tc = true;         // forward convolutions on the tensor cores
+  bool training = false;      // forward keeps what the backward pass reads
+  bool ups_valid = false;     // u2, u1, u0 hold the upsampled decoder inputs
+  int *tc_err = nullptr;      // raised by a tensor-core convolution whose wait expired
+  int sm_count = 148;
   int64_t step = 0;
   // activations (BF16) and gradients (FP32)
   std::vector<void *> owned;
@@ -398,10 +412,95 @@ int wgrad(mpdg_unet *u, Grid3 g, int l, const __nv_bfloat16 *in, const float *go
 const __nv_bfloat16 *W(mpdg_unet *u, int l) { return u->pb + u->L[l].woff; }
 const float *B(mpdg_unet *u, int l) { return u->p + u->L[l].boff; }
 
+int npad_of(int co) { return (co + 15) / 16 * 16; }
+int cg_of(int ci) { return (ci + 15) / 16; }
+
+int pack_weights(mpdg_unet *u)
+{
+  for (int l = 0; l < 15; ++l) {
+    const int ci = u->L[l].ci, co = u->L[l].co;
+    nn_tc::k_pack_weights<<<64, 256, 0, u->stream>>>(ci, co, cg_of(ci), npad_of(co), W(u, l),
+                                                     u->wpk + u->wpk_off[l]);
+  }
+  NNCU(cudaGetLastError());
+  u->wpk_dirty = false;
+  return MPDG_OK;
+}
+
+template <int NPAD, bool RELU, bool ADD, typename TO>
+int conv_tc_t(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_bfloat16 *add,
+              TO *out, const Grid3 *up_from)
+{
+  auto k = nn_tc::k_conv3d_tc<NPAD, RELU, ADD, TO>;
+  static size_t attr_smem = 0;  // the attribute is kept at the request of the launch, so
+                                // that the occupancy query sees the real footprint
+  nn_tc::ConvArgs a;
+  a.nx = g.nx;
+  a.ny = g.ny;
+  a.nz = g.nz;
+  a.ci = u->L[l].ci;
+  a.co = u->L[l].co;
+  a.cg = cg_of(a.ci);
+  a.taps_per_stage = nn_tc::smem_bytes(a.cg, NPAD, 27) <= 200 * 1024 ? 27 : 9;
+  a.up = up_from != nullptr;
+  a.sx = up_from ? up_from->nx : g.nx;
+  a.sy = up_from ? up_from->ny : g.ny;
+  a.sz = up_from ? up_from->nz : g.nz;
+  a.in = in;
+  a.wp = u->wpk + u->wpk_off[l];
+  a.bias = B(u, l);
+  a.add = add;
+  a.out = out;
+  a.err = u->tc_err;
+  const size_t smem = nn_tc::smem_bytes(a.cg, NPAD, a.taps_per_stage);
+  if (smem != attr_smem) {
+    NNCU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_smem = smem;
+  }
+  // resident CTAs per SM from registers, shared memory, threads and tensor-memory columns
+  static int per_sm_regs = 0, smem_sm = 0, smem_rsv = 0, static_smem = 0;
+  if (per_sm_regs == 0) {
+    cudaFuncAttributes fa;
+    NNCU(cudaFuncGetAttributes(&fa, k));
+    int dev = 0;
+    NNCU(cudaGetDevice(&dev));
+    NNCU(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    NNCU(cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    static_smem = (int)fa.sharedSizeBytes;
+    per_sm_regs = 65536 / (((fa.numRegs + 7) / 8 * 8) * nn_tc::kThreads);
+  }
+  int per_sm = std::min(per_sm_regs, smem_sm / ((int)smem + static_smem + smem_rsv));
+  per_sm = std::min(per_sm, 2048 / nn_tc::kThreads);
+  per_sm = std::max(1, std::min(per_sm, 512 / nn_tc::tmem_cols(NPAD)));
+  const int64_t tiles = (int64_t)((g.nx + nn_tc::TCX - 1) / nn_tc::TCX) *
+                        ((g.ny + nn_tc::TCY - 1) / nn_tc::TCY) * g.nz;
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)per_sm * u->sm_count);
+  k<<<grid, nn_tc::kThreads, smem, u->stream>>>(a);
+  NNCU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+template <bool RELU, bool ADD, typename TO>
+int conv_tc(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_bfloat16 *add,
+            TO *out, const Grid3 *up_from = nullptr)
+{
+  if (u->wpk_dirty) NNTRY(pack_weights(u));
+  switch (npad_of(u->L[l].co)) {
+  case 16: return conv_tc_t<16, RELU, ADD, TO>(u, l, g, in, add, out, up_from);
+  case 32: return conv_tc_t<32, RELU, ADD, TO>(u, l, g, in, add, out, up_from);
+  case 48: return conv_tc_t<48, RELU, ADD, TO>(u, l, g, in, add, out, up_from);
+  case 64: return conv_tc_t<64, RELU, ADD, TO>(u, l, g, in, add, out, up_from);
+  default: return nn_fail(MPDG_ERR_INVALID_ARGUMENT, "tensor-core convolution: Cout > 64");
+  }
+}
+
 // conv + relu (activation out, BF16)
 int conv_relu(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, __nv_bfloat16 *out,
               const __nv_bfloat16 *add = nullptr)
 {
+  if (u->use_tc)
+    return add ? conv_tc<true, true>(u, l, g, in, add, out)
+               : conv_tc<true, false>(u, l, g, in, (const __nv_bfloat16 *)nullptr, out);
   if (add)
     return conv<__nv_bfloat16, __nv_bfloat16, true, true, false, false>(u, g, u->L[l].ci, u->L[l].co, in, W(u, l), B(u, l), add, nullptr, out);
   return conv<__nv_bfloat16, __nv_bfloat16, true, false, false, false>(u, g, u->L[l].ci, u->L[l].co, in, W(u, l), B(u, l), nullptr, nullptr, out);
@@ -439,6 +538,21 @@ int forward(mpdg_unet *u)
   NNTRY(pool(g[2], 48, u->e2, u->p2));
   NNTRY(conv_relu(u, E3A, g[3], u->p2, u->a3));
   NNTRY(conv_relu(u, E3B, g[3], u->a3, u->e3));
+  // decoder: with the tensor-core path the upsampling is fused into the halo load of
+  // the next convolution (the upsampled tensors are then formed only for training)
+  u->ups_valid = !u->use_tc || u->training;
+  if (u->use_tc) {
+    if (u->training) NNTRY(up(g[2], 64, u->e3, u->u2));
+    NNTRY((conv_tc<true, true>(u, D2A, g[2], u->e3, u->e2, u->s2, &g[3])));
+    NNTRY(conv_relu(u, D2B, g[2], u->s2, u->d2));
+    if (u->training) NNTRY(up(g[1], 48, u->d2, u->u1));
+    NNTRY((conv_tc<true, true>(u, D1A, g[1], u->d2, u->e1, u->s1, &g[2])));
+    NNTRY(conv_relu(u, D1B, g[1], u->s1, u->d1));
+    if (u->training) NNTRY(up(g[0], 32, u->d1, u->u0));
+    NNTRY((conv_tc<true, true>(u, D0A, g[0], u->d1, u->e0, u->s0, &g[1])));
+    NNTRY(conv_relu(u, D0B, g[0], u->s0, u->d0));
+    return conv_tc<false, false>(u, OUT, g[0], u->d0, (const __nv_bfloat16 *)nullptr, u->y);
+  }
   NNTRY(up(g[2], 64, u->e3, u->u2));
   NNTRY(conv_relu(u, D2A, g[2], u->u2, u->s2, u->e2));
   NNTRY(conv_relu(u, D2B, g[2], u->s2, u->d2));
@@ -455,6 +569,13 @@ int forward(mpdg_unet *u)
 int backward(mpdg_unet *u, const float *gy)
 {
   const Grid3 *g = u->g;
+  if (!u->ups_valid) {  // an inference forward fused the upsampling: form its outputs now
+    k_up<<<grid1d(g[2].n() * 64), 256, 0, u->stream>>>(g[2], 64, u->e3, u->u2);
+    k_up<<<grid1d(g[1].n() * 48), 256, 0, u->stream>>>(g[1], 48, u->d2, u->u1);
+    k_up<<<grid1d(g[0].n() * 32), 256, 0, u->stream>>>(g[0], 32, u->d1, u->u0);
+    NNCU(cudaGetLastError());
+    u->ups_valid = true;
+  }
   NNCU(cudaMemsetAsync(u->grad, 0, sizeof(float) * u->n_params, u->stream));
   float *gA = u->gA, *gB = u->gB, *gC = u->gC;
   auto relu_mask = [&](int64_t n, const __nv_bfloat16 *y, float *gg) -> int {
@@ -584,8 +705,23 @@ extern "C" int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet
       (rc = ualloc(u, (void **)&u->pb, sizeof(__nv_bfloat16) * u->n_params)) != MPDG_OK ||
       (rc = ualloc(u, (void **)&u->partials, sizeof(double) * 148 * 16)) != MPDG_OK ||
       (rc = ualloc(u, (void **)&u->lossd, sizeof(double) * 2)) != MPDG_OK ||
-      (rc = ualloc(u, (void **)&u->counter, sizeof(unsigned) * 4)) != MPDG_OK)
+      (rc = ualloc(u, (void **)&u->counter, sizeof(unsigned) * 4)) != MPDG_OK ||
+      (rc = ualloc(u, (void **)&u->tc_err, sizeof(int))) != MPDG_OK)
     return fail_free(rc);
+  int64_t wtot = 0;
+  for (int l = 0; l < 15; ++l) {
+    u->wpk_off[l] = wtot;
+    wtot += (int64_t)27 * cg_of(kCi[l]) * 2 * npad_of(kCo[l]);
+  }
+  if ((rc = ualloc(u, (void **)&u->wpk, sizeof(uint4) * wtot)) != MPDG_OK) return fail_free(rc);
+  cudaMemset(u->tc_err, 0, sizeof(int));
+  {
+    const char *e = getenv("MPDG_UNET_TC");
+    u->use_tc = !(e && e[0] == '0');
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&u->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  }
   // He-uniform initialisation from a counter hash; output layer scaled by 0.1
   std::vector<float> h(u->n_params, 0.f);
   for (int l = 0; l < 15; ++l) {
@@ -650,6 +786,7 @@ extern "C" int mpdg_unet_set_params(mpdg_unet *u, const float *src)
   NNCU(cudaMemcpyAsync(u->p, src, sizeof(float) * u->n_params, cudaMemcpyDeviceToDevice, u->stream));
   k_f32_to_bf16<<<grid1d(u->n_params), 256, 0, u->stream>>>(u->n_params, u->p, u->pb);
   NNCU(cudaGetLastError());
+  u->wpk_dirty = true;
   return MPDG_OK;
 }
 
@@ -662,6 +799,15 @@ extern "C" int mpdg_unet_forward(mpdg_unet *u, const float *input, float *output
   NNCU(cudaGetLastError());
   NNTRY(forward(u));
   if (output) NNCU(cudaMemcpyAsync(output, u->y, sizeof(float) * n0, cudaMemcpyDeviceToDevice, u->stream));
+  if (u->use_tc) {
+    int err = 0;
+    NNCU(cudaMemcpyAsync(&err, u->tc_err, sizeof(int), cudaMemcpyDeviceToHost, u->stream));
+    NNCU(cudaStreamSynchronize(u->stream));
+    if (err) {
+      cudaMemsetAsync(u->tc_err, 0, sizeof(int), u->stream);
+      return nn_fail(MPDG_ERR_CUDA, "tensor-core convolution: wait for the MMAs expired");
+    }
+  }
   return MPDG_OK;
 }
 
@@ -682,7 +828,10 @@ extern "C" int mpdg_unet_train_step(mpdg_unet *u, const float *input, const floa
 {
   if (!u || !input || !target) return nn_fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   const int64_t n0 = u->g[0].n();
-  NNTRY(mpdg_unet_forward(u, input, nullptr));
+  u->training = true;
+  const int frc = mpdg_unet_forward(u, input, nullptr);
+  u->training = false;
+  NNTRY(frc);
   float *gy = u->gC;  // reuse scratch for dL/dy (copied before backward overwrites gC)
   k_mse<<<grid1d(n0), 256, 0, u->stream>>>(n0, u->y, target, gy, u->partials, u->counter, u->lossd);
   NNCU(cudaGetLastError());
@@ -696,6 +845,7 @@ extern "C" int mpdg_unet_train_step(mpdg_unet *u, const float *input, const floa
   k_adam<<<grid1d(u->n_params), 256, 0, u->stream>>>(u->n_params, u->p, u->grad, u->m, u->v, lr, b1,
                                                       b2, 1e-8f, c1, c2, u->pb);
   NNCU(cudaGetLastError());
+  u->wpk_dirty = true;
   if (loss) {
     double l = 0.0;
     NNCU(cudaMemcpyAsync(&l, u->lossd, sizeof(double), cudaMemcpyDeviceToHost, u->stream));

@@ -84,3 +84,26 @@ def test_training_reduces_the_loss():
     for _ in range(150):
         last = net.train_step(x, t, 1e-3)
     assert last < 0.2 * first, (first, last)
+
+
+def test_tensor_core_forward_matches_cuda_core_forward(monkeypatch):
+    """The tcgen05 implicit-GEMM convolutions against the CUDA-core ones (same BF16
+    weights and activations, FP32 accumulation in both) on a grid whose x and y sizes
+    leave partial 8 x 16 tiles at every level."""
+    dims = (40, 33, 9)
+    n = dims[0] * dims[1] * dims[2]
+    monkeypatch.delenv("MPDG_UNET_TC", raising=False)
+    net_tc = LG.UNet(dims, seed=7)
+    monkeypatch.setenv("MPDG_UNET_TC", "0")
+    net_cc = LG.UNet(dims, seed=7)
+    g = torch.Generator().manual_seed(2)
+    for _ in range(2):
+        x = torch.randn(3 * n, generator=g).cuda()
+        y_tc, y_cc = net_tc.forward(x), net_cc.forward(x)
+        err = (y_tc - y_cc).norm() / y_cc.norm()
+        assert err < 1e-2, err
+        # after an update of the weights the packed copy follows
+        p = net_cc.get_params()
+        p.add_(0.01 * torch.randn(p.numel(), generator=g).cuda())
+        net_tc.set_params(p)
+        net_cc.set_params(p)

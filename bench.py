@@ -4,10 +4,12 @@ Workload (one "step" = one implicit Euler step of the hot path): FE_Q(3) on the
 unit cube with 128^3 cells (385^3 = 57,066,625 DoFs), k(T) = 1 + 0.5 T,
 rho*cp = 1, dt = 5e-4, Dirichlet T = 0 on all faces, T0 = 0, a Gaussian source
 of radius 0.05 at z = 0.95 moving along x at speed 1, one Newton linearisation
-per step solved to |b - J T| <= 1e-8 |b|. Two solvers run the same steps:
-  plain  FP64 Jacobi-CG
-  mixed  FP64 flexible CG with the FP32 degree-4 Chebyshev-Jacobi preconditioner
-`value` is the step throughput of the faster one in DoFs advanced per second
+per step solved to |b - J T| <= 1e-8 |b|. The solvers run the same steps:
+  plain    FP64 Jacobi-CG
+  mixed    FP64 flexible CG with the FP32 p-multigrid V-cycle preconditioner
+  cheb     FP64 flexible CG with the FP32 degree-6 Chebyshev-Jacobi preconditioner
+  learned  the mixed solver started from the learned guess
+`value` is the step throughput of the fastest one in DoFs advanced per second
 (whole job: summed over replicas when run with --gpus N > 1, which runs
 independent replicas: the path has no data-parallel exchange on one mesh).
 
@@ -190,16 +192,19 @@ def run_mine(args):
     plain = H.HeatDiffuseOperation(op, H.LinearSolverData(rel_tolerance=REL_TOL,
                                                           abs_tolerance=0.0),
                                    predictor=L.PREDICTOR_LINEAR, single_linearization=True)
-    mixed = H.HeatDiffuseOperation(op, H.LinearSolverData(
+    mg_data = dict(preconditioner_type=L.PRECOND_MG_F32, rel_tolerance=REL_TOL,
+                   abs_tolerance=0.0, cheb_picard=True, cheb_eig_reuse=True)
+    mixed = H.HeatDiffuseOperation(op, H.LinearSolverData(**mg_data),
+                                   predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    cheb = H.HeatDiffuseOperation(op, H.LinearSolverData(
         preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32, rel_tolerance=REL_TOL,
         abs_tolerance=0.0, cheb_degree=CHEB_DEGREE, cheb_picard=True, cheb_eig_reuse=True),
         predictor=L.PREDICTOR_LINEAR, single_linearization=True)
-    learned = H.HeatDiffuseOperation(op, H.LinearSolverData(
-        preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32, rel_tolerance=REL_TOL,
-        abs_tolerance=0.0, cheb_degree=CHEB_DEGREE, cheb_picard=True, cheb_eig_reuse=True),
-        predictor=L.PREDICTOR_GIVEN, single_linearization=True)
+    learned = H.HeatDiffuseOperation(op, H.LinearSolverData(**mg_data),
+                                     predictor=L.PREDICTOR_GIVEN, single_linearization=True)
     q = op.new_vector()
     mixed.heat_source = q
+    cheb.heat_source = q
     plain.heat_source = q
     learned.heat_source = q
     model = None
@@ -265,7 +270,13 @@ def run_mine(args):
     launches = int(op.counters(reset=True)["launches"])
     clk = clocks.stop() if clocks else None
     init_res = mixed.last_stats.initial_relative_residual
+    T_mixed = mixed.T.clone()  # after step W+K-1, compared with the plain solver below
     ms_instr, _, cnt = timed(mixed, W + K, K, instrument=True)
+    # Chebyshev-preconditioned mixed precision on the same steps
+    ms_cheb = its_cheb = None
+    if not args.no_cheb:
+        march(cheb, 0, W)
+        ms_cheb, its_cheb, _ = timed(cheb, W, K)
     # learned guess + mixed precision on the same steps
     ms_learned = its_learned = init_res_learned = None
     if model is not None:
@@ -279,10 +290,11 @@ def run_mine(args):
         ms_plain, its_plain, _ = timed(plain, W, K)
     err = None
     if not args.no_plain:
-        diff = torch.linalg.vector_norm(mixed.T - plain.T).item()
+        diff = torch.linalg.vector_norm(T_mixed - plain.T).item()
         ref = torch.linalg.vector_norm(plain.T).item()
         err = {"rel_l2": diff / ref if ref > 0 else 0.0,
-               "rel_max": ((mixed.T - plain.T).abs().max() / plain.T.abs().max()).item()}
+               "rel_max": ((T_mixed - plain.T).abs().max() / plain.T.abs().max()).item()}
+        del T_mixed
 
     # e2e: the host-buffer C-ABI call (H2D of T, T_old, source; D2H of T, T_old per step)
     e2e = None
@@ -389,7 +401,7 @@ def run_mine(args):
                "sample": f"{args.cpu_steps} implicit steps of the same problem on "
                          f"{args.cpu_cells}^3 cells ({n} DoFs), oracle port, {sec:.1f} s"}
 
-    best_ms = min(x for x in (ms_mixed, ms_plain, ms_learned) if x)
+    best_ms = min(x for x in (ms_mixed, ms_cheb, ms_plain, ms_learned) if x)
     line = {
         "metric": METRIC, "value": world * N * K / (best_ms / 1e3), "unit": "DoF/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": best_ms / K,
@@ -400,15 +412,20 @@ def run_mine(args):
         "plain_fp64_ms_per_step": ms_plain / K if ms_plain else None,
         "speedup_mixed_vs_plain": (ms_plain / ms_mixed) if ms_plain else None,
         "cg_iterations_mixed": its_mixed, "cg_iterations_plain": its_plain,
+        "cheb_mixed_ms_per_step": ms_cheb / K if ms_cheb else None,
+        "cg_iterations_cheb_mixed": its_cheb,
         "initial_relative_residual_last_step": init_res,
         "learned_mixed_ms_per_step": ms_learned / K if ms_learned else None,
         "speedup_learned_mixed_vs_plain": (ms_plain / ms_learned) if (ms_plain and ms_learned) else None,
         "cg_iterations_learned_mixed": its_learned,
         "initial_relative_residual_last_step_learned": init_res_learned,
         "mixed_solver": {"outer": "FP64 flexible CG", "preconditioner":
-                         f"FP32 Chebyshev-Jacobi degree {CHEB_DEGREE}, Picard operator "
-                         "(k(T_lin) at the q-points), interval from 12 Lanczos steps reused "
-                         "across steps", "predictor": "linear extrapolation"},
+                         "FP32 p-multigrid V-cycle: FE_Q(3) -> FE_Q(1) on 128^3 -> FE_Q(1) "
+                         "on 64^3, 32^3, 16^3, 8^3, 4^3; Chebyshev-Jacobi smoothing (2 pre, 2+1 "
+                         "post steps over [upper/8, upper]; 8 steps on the coarsest level); "
+                         "Picard operators (k(T_lin) at the q-points) on every level; Lanczos "
+                         "intervals reused across steps", "predictor": "linear extrapolation",
+                         "cheb": f"FP32 Chebyshev-Jacobi degree {CHEB_DEGREE}, Picard operator"},
         "mixed_vs_plain_error": err,
         "vmult_fp64_gdofs": N / (vm_ms / 1e3) / 1e9, "vmult_fp64_ms": vm_ms,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
@@ -431,6 +448,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cheb", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()

@@ -79,7 +79,12 @@ typedef struct {
 
 enum { MPDG_SOLVER_CG = 0, MPDG_SOLVER_GMRES = 1 };           /* LinearSolverType  */
 enum { MPDG_PRECOND_IDENTITY = 0, MPDG_PRECOND_JACOBI = 1,    /* PreconditionerType */
-       MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 = 2 };
+       MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 = 2,
+       /* FP32 p-multigrid V-cycle (no reference counterpart; the reference's GMG
+        * pattern is unit_tests/gmg.cc): FE_Q(p) -> FE_Q(1) on the same mesh, then
+        * FE_Q(1) on meshes coarsened by 2 per direction while the cell counts stay
+        * even and >= mg_min_cells; Chebyshev-Jacobi smoothing on every level */
+       MPDG_PRECOND_MG_F32 = 3 };
 
 typedef struct {
   int    solver;              /* MPDG_SOLVER_*                                      */
@@ -98,6 +103,10 @@ typedef struct {
                                  the outer FP64 CG keeps the exact tangent          */
   int    cheb_eig_reuse;      /* 1: keep the Chebyshev interval across solves and
                                  time steps until the material or the mesh changes  */
+  int    mg_smoothing_degree; /* multigrid: Chebyshev steps of pre- and post-smoothing */
+  int    mg_coarse_degree;    /* multigrid: Chebyshev steps on the coarsest level    */
+  double mg_smoothing_range;  /* multigrid: smoothing interval [upper / range, upper] */
+  int    mg_min_cells;        /* multigrid: coarsen while every cell count / 2 >= this */
 } mpdg_solver_params;
 
 typedef struct {

@@ -27,7 +27,7 @@ ERR_NOT_SUPPORTED = 9
 
 LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID = 0, 1, 2
 SOLVER_CG, SOLVER_GMRES = 0, 1
-PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_CHEBYSHEV_JACOBI_F32 = 0, 1, 2
+PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_CHEBYSHEV_JACOBI_F32, PRECOND_MG_F32 = 0, 1, 2, 3
 PREDICTOR_NONE, PREDICTOR_LINEAR, PREDICTOR_GIVEN = 0, 1, 2
 
 
@@ -50,7 +50,9 @@ class SolverParams(C.Structure):
                 ("gmres_restart", C.c_int), ("cheb_degree", C.c_int),
                 ("cheb_eig_iterations", C.c_int), ("cheb_max_factor", C.c_double),
                 ("cheb_min_fraction", C.c_double), ("tol_reference_norm", C.c_double),
-                ("cheb_picard", C.c_int), ("cheb_eig_reuse", C.c_int)]
+                ("cheb_picard", C.c_int), ("cheb_eig_reuse", C.c_int),
+                ("mg_smoothing_degree", C.c_int), ("mg_coarse_degree", C.c_int),
+                ("mg_smoothing_range", C.c_double), ("mg_min_cells", C.c_int)]
 
 
 class SolveStats(C.Structure):

@@ -63,6 +63,19 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// one level of the FP32 p-multigrid hierarchy (level 0 is the solver's own handle)
+struct MGLevel {
+  mpdg_heat *h = nullptr;
+  bool own = false;
+  int ratio = 1;                        // node ratio of the transfer to the next coarser level
+  float xi[8] = {0};                    // fine-cell node positions of that transfer, in [0, 1]
+  float *b = nullptr, *x = nullptr, *d = nullptr, *Ax = nullptr;
+  double *Tl = nullptr, *To = nullptr;  // injected linearisation point (levels > 0)
+  double theta = 1.0, delta = 1.0;      // smoothing interval (centre, half width)
+  int steps = 0;                        // Chebyshev steps (pre = post = steps; coarsest: all)
+  std::vector<float> c1, c2;
+};
+
 struct mpdg_heat {
   int device = 0, sm_count = 148;
   cudaStream_t stream = nullptr;
@@ -120,6 +133,10 @@ struct mpdg_heat {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev64, ev32;
   std::vector<cudaEvent_t> ev_pool;
   double ms64 = 0.0, ms32 = 0.0;
+  // p-multigrid preconditioner: levels and the scratch of the separable transfers
+  std::vector<MGLevel> mg;
+  float *mg_t1 = nullptr, *mg_t2 = nullptr;
+  int mg_min_cells = -1;
 };
 
 static cudaEvent_t take_event(mpdg_heat *h)
@@ -659,6 +676,110 @@ __global__ void k_cgm_update_p(int64_t N, const double *__restrict__ z, double *
   }
 }
 
+// ---- p-multigrid building blocks ---------------------------------------------
+struct Dims3 {
+  int n[3];
+  __host__ __device__ int64_t size() const { return (int64_t)n[0] * n[1] * n[2]; }
+  __host__ __device__ int64_t at(int i, int j, int k) const
+  {
+    return i + (int64_t)n[0] * (j + (int64_t)n[1] * k);
+  }
+};
+struct Transfer1D {
+  int r;         // fine nodes per coarse interval
+  float xi[8];   // position of fine node a (0 <= a < r) in its coarse interval
+};
+
+// coarse[V] = fine[r V] per direction (FP64 linearisation point)
+__global__ void k_inject(Dims3 fd, Dims3 cd, int r, const double *__restrict__ fine,
+                         double *coarse)
+{
+  GRID_STRIDE(i, cd.size())
+  {
+    const int a = (int)(i % cd.n[0]), b = (int)((i / cd.n[0]) % cd.n[1]),
+              c = (int)(i / ((int64_t)cd.n[0] * cd.n[1]));
+    coarse[i] = fine[fd.at(r * a, r * b, r * c)];
+  }
+}
+
+// restriction along one axis (transpose of the interpolation below):
+// out[.., V, ..] = sum_{|s| < r} phi_V(node r V + s) in[.., r V + s, ..]; masked rows of
+// the coarse level are set to zero
+__global__ void k_restrict_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
+                                const float *__restrict__ in, float *out, MeshDims md, int masked,
+                                const SolverState *st)
+{
+  if (st && st->done) return;
+  GRID_STRIDE(i, dout.size())
+  {
+    int o[3] = {(int)(i % dout.n[0]), (int)((i / dout.n[0]) % dout.n[1]),
+                (int)(i / ((int64_t)dout.n[0] * dout.n[1]))};
+    if (masked && constrained(md, o[0], o[1], o[2])) {
+      out[i] = 0.f;
+      continue;
+    }
+    const int V = o[axis];
+    float acc = 0.f;
+    for (int s = -(t.r - 1); s <= t.r - 1; ++s) {
+      const int I = t.r * V + s;
+      if (I < 0 || I >= di.n[axis]) continue;
+      const float w = s == 0 ? 1.f : (s > 0 ? 1.f - t.xi[s] : t.xi[t.r + s]);
+      int p[3] = {o[0], o[1], o[2]};
+      p[axis] = I;
+      acc += w * in[di.at(p[0], p[1], p[2])];
+    }
+    out[i] = acc;
+  }
+}
+
+// interpolation along one axis: out[.., I, ..] = (1 - xi_a) in[.., V, ..] + xi_a in[.., V + 1, ..]
+// with V = I / r, a = I % r; add: accumulate into out; masked rows are left untouched
+__global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
+                               const float *__restrict__ in, float *out, int add, MeshDims md,
+                               int masked, const SolverState *st)
+{
+  if (st && st->done) return;
+  GRID_STRIDE(i, dout.size())
+  {
+    int o[3] = {(int)(i % dout.n[0]), (int)((i / dout.n[0]) % dout.n[1]),
+                (int)(i / ((int64_t)dout.n[0] * dout.n[1]))};
+    if (masked && constrained(md, o[0], o[1], o[2])) {
+      if (!add) out[i] = 0.f;
+      continue;
+    }
+    const int I = o[axis], V = I / t.r, a = I - V * t.r;
+    int p[3] = {o[0], o[1], o[2]};
+    p[axis] = V;
+    float v = in[di.at(p[0], p[1], p[2])];
+    if (a != 0) {
+      p[axis] = V + 1;
+      v = (1.f - t.xi[a]) * v + t.xi[a] * in[di.at(p[0], p[1], p[2])];
+    }
+    out[i] = add ? out[i] + v : v;
+  }
+}
+
+// first Chebyshev step from zero: x = d = D b / theta
+__global__ void k_cheb_init(int64_t N, const float *__restrict__ b, float *x, float *d,
+                            const float *__restrict__ D32, float inv_theta, const SolverState *st)
+{
+  if (st->done) return;
+  GRID_STRIDE(i, N)
+  {
+    const float v = D32[i] * b[i] * inv_theta;
+    x[i] = v;
+    d[i] = v;
+  }
+}
+
+// Ax = b - Ax (the residual of the smoothed iterate, restricted next)
+__global__ void k_residual32(int64_t N, const float *__restrict__ b, float *Ax,
+                             const SolverState *st)
+{
+  if (st->done) return;
+  GRID_STRIDE(i, N) Ax[i] = b[i] - Ax[i];
+}
+
 // ---- GMRES building blocks --------------------------------------------------
 constexpr int kMaxBasis = 32;
 
@@ -1159,7 +1280,309 @@ static int estimate_eigenvalues(mpdg_heat *h, int n_it, double *lmin, double *lm
 }
 
 // ---------------------------------------------------------------------------
-// FP64 flexible CG with the FP32 Chebyshev-Jacobi preconditioner
+// FP32 p-multigrid preconditioner. Levels: the solver's FE_Q(p) operator, FE_Q(1)
+// on the same mesh (p > 1), then FE_Q(1) on meshes coarsened by two per direction
+// while every cell count stays even and its half >= mg_min_cells. Each coarse
+// level is a child handle with the same material, boundary terms and Dirichlet
+// faces, linearised at the injection of the fine linearisation point; its operator
+// is the same FP32 form as the fine one (Picard when the outer solve uses it).
+// Transfers are separable tensor products of the 1D interpolation between nested
+// node sets (the GLL nodes of FE_Q(p) for the p step, midpoints for the h step),
+// the restriction its transpose. Smoother: Chebyshev-Jacobi over
+// [upper / mg_smoothing_range, upper] with upper = cheb_max_factor * lambda_max of
+// D^-1 A from a Lanczos estimate per level; the coarsest level runs
+// mg_coarse_degree steps over [lambda_min, upper].
+// ---------------------------------------------------------------------------
+static void release(mpdg_heat *h);
+static std::vector<double> box_vertices(const mpdg_mesh_desc &desc);
+static int create_impl(const mpdg_mesh_desc *desc, int device, const std::vector<double> *verts,
+                       mpdg_heat **out);
+static int compute_diag(mpdg_heat *h, double *d);
+
+static void cheb_coefficients(double theta, double delta, int k, std::vector<float> &c1,
+                              std::vector<float> &c2)
+{
+  const double sigma = theta / delta;
+  c1.assign(k + 1, 0.f);
+  c2.assign(k + 1, 0.f);
+  double rho0 = 1.0 / sigma;
+  for (int j = 1; j <= k; ++j) {
+    const double rho1 = 1.0 / (2.0 * sigma - rho0);
+    c1[j] = (float)(rho1 * rho0);
+    c2[j] = (float)(2.0 * rho1 / delta);
+    rho0 = rho1;
+  }
+}
+
+static Dims3 nodal_dims(const mpdg_heat *h) { return Dims3{{h->dims.nd[0], h->dims.nd[1], h->dims.nd[2]}}; }
+
+static int mg_build(mpdg_heat *h, const mpdg_solver_params *prm)
+{
+  if (!h->mg.empty() && h->mg_min_cells == prm->mg_min_cells) return MPDG_OK;
+  for (MGLevel &lv : h->mg)
+    if (lv.own && lv.h) {
+      release(lv.h);
+      delete lv.h;
+    }
+  h->mg.clear();
+  h->mg_min_cells = prm->mg_min_cells;
+  MGLevel l0;
+  l0.h = h;
+  l0.b = h->r32;
+  l0.x = h->x32;
+  l0.d = h->d32;
+  l0.Ax = h->Ax32;
+  h->mg.push_back(l0);
+  mpdg_mesh_desc cur = h->desc;
+  std::vector<double> cur_verts;
+  if (h->geo == 1) cur_verts = box_vertices(h->desc);
+  auto add_child = [&](int ratio, const float *xi, const mpdg_mesh_desc &d,
+                       const std::vector<double> *verts) -> int {
+    mpdg_heat *c = nullptr;
+    TRY(create_impl(&d, h->device, verts, &c));
+    h->mg.back().ratio = ratio;
+    for (int a = 0; a < ratio && a < 8; ++a) h->mg.back().xi[a] = xi[a];
+    MGLevel lv;
+    lv.h = c;
+    lv.own = true;
+    h->mg.push_back(lv);
+    MGLevel &L = h->mg.back();
+    c->stream = h->stream;
+    TRY(mpdg_heat_set_material(c, &h->mat));
+    for (int f = 0; f < 6; ++f) {
+      c->btype[f] = h->btype[f];
+      c->bh[f] = h->bh[f];
+      c->bTc[f] = h->bTc[f];
+      c->beps[f] = h->beps[f];
+      c->bTr[f] = h->bTr[f];
+      c->bqn[f] = h->bqn[f];
+    }
+    TRY(ensure_workspace_f32(c));
+    TRY(dvec(c, &c->inv_diag, c->n_dofs));
+    TRY(dvec(c, &L.Tl, c->n_dofs));
+    TRY(dvec(c, &L.To, c->n_dofs));
+    L.b = c->r32;
+    L.x = c->x32;
+    L.d = c->d32;
+    L.Ax = c->Ax32;
+    CU(cudaMemsetAsync(L.Ax, 0, sizeof(float) * c->n_dofs, h->stream));
+    return MPDG_OK;
+  };
+  if (h->p > 1) {
+    const Tables1D t = make_tables(h->n);
+    float xi[8];
+    for (int a = 0; a < h->p && a < 8; ++a) xi[a] = (float)t.xl[a];
+    mpdg_mesh_desc d = cur;
+    d.degree = 1;
+    TRY(add_child(h->p, xi, d, h->geo == 1 ? &cur_verts : nullptr));
+    cur = d;
+  }
+  for (;;) {
+    bool ok = true;
+    for (int e = 0; e < 3; ++e)
+      if (cur.cells[e] % 2 != 0 || cur.cells[e] / 2 < std::max(1, prm->mg_min_cells)) ok = false;
+    if (!ok) break;
+    mpdg_mesh_desc d = cur;
+    d.degree = 1;
+    for (int e = 0; e < 3; ++e) d.cells[e] = cur.cells[e] / 2;
+    std::vector<double> cv;
+    if (h->geo == 1) {
+      // vertices of the coarse mesh = every second vertex of the current one
+      cv.resize((size_t)3 * (d.cells[0] + 1) * (d.cells[1] + 1) * (d.cells[2] + 1));
+      for (int c = 0; c <= d.cells[2]; ++c)
+        for (int b = 0; b <= d.cells[1]; ++b)
+          for (int a = 0; a <= d.cells[0]; ++a) {
+            const int64_t vc = a + (int64_t)(d.cells[0] + 1) * (b + (int64_t)(d.cells[1] + 1) * c);
+            const int64_t vf = 2 * a + (int64_t)(cur.cells[0] + 1) *
+                                         (2 * b + (int64_t)(cur.cells[1] + 1) * 2 * c);
+            for (int e = 0; e < 3; ++e) cv[3 * vc + e] = cur_verts[3 * vf + e];
+          }
+    }
+    const float xi[2] = {0.f, 0.5f};
+    TRY(add_child(2, xi, d, h->geo == 1 ? &cv : nullptr));
+    cur = d;
+    cur_verts.swap(cv);
+  }
+  if (h->mg.size() < 2)
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "multigrid needs degree > 1 or even cell counts with halves >= mg_min_cells");
+  // transfer scratch: the largest x-pass and y-pass intermediates
+  int64_t n1 = 0, n2 = 0;
+  for (size_t l = 0; l + 1 < h->mg.size(); ++l) {
+    const Dims3 F = nodal_dims(h->mg[l].h), C = nodal_dims(h->mg[l + 1].h);
+    n1 = std::max(n1, (int64_t)C.n[0] * F.n[1] * F.n[2]);
+    n2 = std::max(n2, (int64_t)C.n[0] * C.n[1] * F.n[2]);
+  }
+  TRY(dvec(h, &h->mg_t1, n1));
+  TRY(dvec(h, &h->mg_t2, n2));
+  return MPDG_OK;
+}
+
+static int estimate_eigenvalues(mpdg_heat *h, int n_it, double *lmin, double *lmax);
+
+// per solve: linearise the coarse levels at the injected point, their conductivity
+// fields, inverse diagonals and (first time, or without reuse) smoothing intervals
+static int mg_setup(mpdg_heat *h, const mpdg_solver_params *prm, bool picard)
+{
+  const int L = (int)h->mg.size();
+  const int s = std::max(1, prm->mg_smoothing_degree);
+  for (int l = 0; l < L; ++l) {
+    MGLevel &v = h->mg[l];
+    mpdg_heat *c = v.h;
+    if (l > 0) {
+      const MGLevel &f = h->mg[l - 1];
+      const double *fT = l == 1 ? h->T_lin : f.Tl;
+      const double *fTo = l == 1 ? h->T_old : (f.h->T_old ? f.To : nullptr);
+      const Dims3 F = nodal_dims(f.h), Cd = nodal_dims(c);
+      if (fT) {
+        k_inject<<<vgrid(c, Cd.size()), VT, 0, h->stream>>>(F, Cd, f.ratio, fT, v.Tl); ++h->launches;
+      }
+      if (fTo) {
+        k_inject<<<vgrid(c, Cd.size()), VT, 0, h->stream>>>(F, Cd, f.ratio, fTo, v.To); ++h->launches;
+      }
+      CU(cudaGetLastError());
+      if (c->dt != h->dt) {
+        c->dt = h->dt;
+        c->eig_valid = false;
+      }
+      c->T_lin = fT ? v.Tl : nullptr;
+      c->T_old = fTo ? v.To : nullptr;
+      c->lin_f_dirty = true;
+      TRY(refresh_f32(c));
+      if (picard) {
+        TRY(dvec(c, &c->kq, c->n_cells * c->npt));
+        CellArgs<double> a = cell_args<double>(c);
+        a.Tl = c->T_lin;
+        CU(c->tab.conductivity_q(a, c->kq, c->law, h->stream, c->sm_count));
+        ++h->launches;
+      }
+      TRY(compute_diag(c, c->inv_diag));
+      c->diag_valid = true;
+      k_cast_f<<<vgrid(c, c->n_dofs), VT, 0, h->stream>>>(c->n_dofs, c->inv_diag, c->inv_diag_f);
+      ++h->launches;
+      CU(cudaGetLastError());
+      if (!c->eig_valid || !prm->cheb_eig_reuse) {
+        TRY(estimate_eigenvalues(c, prm->cheb_eig_iterations, &c->eig_min, &c->eig_max));
+        c->eig_valid = true;
+      }
+    }
+    const double upper = prm->cheb_max_factor * c->eig_max;
+    double lower = upper / std::max(1.5, prm->mg_smoothing_range);
+    v.steps = s;
+    if (l == L - 1) {
+      lower = std::min(lower, std::max(c->eig_min, 1e-6 * upper));
+      v.steps = std::max(1, prm->mg_coarse_degree);
+    }
+    v.theta = 0.5 * (upper + lower);
+    v.delta = 0.5 * (upper - lower);
+    cheb_coefficients(v.theta, v.delta, v.steps, v.c1, v.c2);
+  }
+  return MPDG_OK;
+}
+
+static int mg_restrict(mpdg_heat *h, int l, const float *fine, float *coarse)
+{
+  const MGLevel &f = h->mg[l], &c = h->mg[l + 1];
+  const Dims3 F = nodal_dims(f.h), C = nodal_dims(c.h);
+  const Dims3 D1{{C.n[0], F.n[1], F.n[2]}}, D2{{C.n[0], C.n[1], F.n[2]}};
+  Transfer1D t;
+  t.r = f.ratio;
+  for (int a = 0; a < 8; ++a) t.xi[a] = f.xi[a];
+  k_restrict_axis<<<vgrid(h, D1.size()), VT, 0, h->stream>>>(0, F, D1, t, fine, h->mg_t1,
+                                                              c.h->dims, 0, h->st);
+  k_restrict_axis<<<vgrid(h, D2.size()), VT, 0, h->stream>>>(1, D1, D2, t, h->mg_t1, h->mg_t2,
+                                                              c.h->dims, 0, h->st);
+  k_restrict_axis<<<vgrid(h, C.size()), VT, 0, h->stream>>>(2, D2, C, t, h->mg_t2, coarse,
+                                                             c.h->dims, 1, h->st);
+  h->launches += 3;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine)
+{
+  const MGLevel &f = h->mg[l], &c = h->mg[l + 1];
+  const Dims3 F = nodal_dims(f.h), C = nodal_dims(c.h);
+  const Dims3 E2{{C.n[0], C.n[1], F.n[2]}}, E1{{C.n[0], F.n[1], F.n[2]}};
+  Transfer1D t;
+  t.r = f.ratio;
+  for (int a = 0; a < 8; ++a) t.xi[a] = f.xi[a];
+  k_prolong_axis<<<vgrid(h, E2.size()), VT, 0, h->stream>>>(2, C, E2, t, coarse, h->mg_t2, 0,
+                                                             f.h->dims, 0, h->st);
+  k_prolong_axis<<<vgrid(h, E1.size()), VT, 0, h->stream>>>(1, E2, E1, t, h->mg_t2, h->mg_t1, 0,
+                                                             f.h->dims, 0, h->st);
+  k_prolong_axis<<<vgrid(h, F.size()), VT, 0, h->stream>>>(0, E1, F, t, h->mg_t1, fine, 1,
+                                                            f.h->dims, 1, h->st);
+  h->launches += 3;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+__global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32, float *d32,
+                            float *Ax32, const float *__restrict__ D32, float c1, float c2,
+                            const SolverState *st);
+__global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const float *__restrict__ x32,
+                            const float *__restrict__ d32, float *Ax32,
+                            const float *__restrict__ D32, float c1, float c2,
+                            const double *__restrict__ r, const double *__restrict__ Ap, double *z,
+                            SolverState *st, double *partials, unsigned *counter);
+
+// one V-cycle on the FP32 residual in level 0's b (= r32), whose first smoothing step
+// (x = d = D b / theta_0) the caller has taken; ends with z = x (FP64) and the dots of
+// the flexible CG, like the last Chebyshev step
+static int mg_vcycle(mpdg_heat *h, bool picard)
+{
+  const int L = (int)h->mg.size();
+  SolverState *st = h->st;
+  for (int l = 0; l < L; ++l) {
+    MGLevel &v = h->mg[l];
+    mpdg_heat *c = v.h;
+    const int64_t N = c->n_dofs;
+    const int g = vgrid(c, N);
+    if (l > 0) {
+      k_cheb_init<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, c->inv_diag_f, (float)(1.0 / v.theta),
+                                           st);
+      ++h->launches;
+    }
+    for (int j = 1; j <= v.steps; ++j) {
+      TRY(op_apply_f(c, v.Ax, v.x, st, picard));
+      k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, v.c1[j],
+                                           v.c2[j], st);
+      ++h->launches;
+    }
+    if (l == L - 1) break;
+    TRY(op_apply_f(c, v.Ax, v.x, st, picard));
+    k_residual32<<<g, VT, 0, h->stream>>>(N, v.b, v.Ax, st);
+    ++h->launches;
+    TRY(mg_restrict(h, l, v.Ax, h->mg[l + 1].b));
+    CU(cudaMemsetAsync(v.Ax, 0, sizeof(float) * N, h->stream));
+  }
+  for (int l = L - 2; l >= 0; --l) {
+    MGLevel &v = h->mg[l];
+    mpdg_heat *c = v.h;
+    const int64_t N = c->n_dofs;
+    const int g = vgrid(c, N);
+    TRY(mg_prolong_add(h, l, h->mg[l + 1].x, v.x));
+    // post-smoothing: the Chebyshev recurrence restarted from the corrected iterate
+    for (int j = 0; j <= v.steps; ++j) {
+      TRY(op_apply_f(c, v.Ax, v.x, st, picard));
+      const float c1 = j == 0 ? 0.f : v.c1[j];
+      const float c2 = j == 0 ? (float)(1.0 / v.theta) : v.c2[j];
+      if (l == 0 && j == v.steps) {
+        k_cheb_last<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, h->r,
+                                             h->Ap, h->z, st, h->partials, h->counter);
+      } else {
+        k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, st);
+      }
+      ++h->launches;
+    }
+  }
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 flexible CG with the FP32 Chebyshev-Jacobi or p-multigrid preconditioner
 // ---------------------------------------------------------------------------
 static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
                         mpdg_solve_stats *stats)
@@ -1167,6 +1590,9 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   const int64_t N = h->n_dofs;
   if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
   if (prm->cheb_degree < 1) return fail(MPDG_ERR_INVALID_ARGUMENT, "cheb_degree < 1");
+  if (prm->preconditioner == MPDG_PRECOND_MG_F32 &&
+      (prm->mg_smoothing_degree < 1 || prm->mg_coarse_degree < 1 || !(prm->mg_smoothing_range > 1.0)))
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "multigrid: smoothing degrees >= 1, range > 1");
   TRY(ensure_workspace(h));
   TRY(ensure_workspace_f32(h));
   TRY(refresh_f32(h));
@@ -1187,19 +1613,19 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     TRY(estimate_eigenvalues(h, prm->cheb_eig_iterations, &h->eig_min, &h->eig_max));
     h->eig_valid = true;
   }
-  const double bmax = prm->cheb_max_factor * h->eig_max;
-  const double amin = std::max(h->eig_min, prm->cheb_min_fraction * bmax);
-  const double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin), sigma = theta / delta;
+  const bool use_mg = prm->preconditioner == MPDG_PRECOND_MG_F32;
+  double bmax = prm->cheb_max_factor * h->eig_max;
+  double amin = std::max(h->eig_min, prm->cheb_min_fraction * bmax);
+  double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin);
   const int k = prm->cheb_degree;
-  std::vector<float> c1(k + 1), c2(k + 1);
-  {
-    double rho0 = 1.0 / sigma;
-    for (int j = 1; j <= k; ++j) {
-      const double rho1 = 1.0 / (2.0 * sigma - rho0);
-      c1[j] = (float)(rho1 * rho0);
-      c2[j] = (float)(2.0 * rho1 / delta);
-      rho0 = rho1;
-    }
+  std::vector<float> c1, c2;
+  cheb_coefficients(theta, delta, k, c1, c2);
+  if (use_mg) {
+    TRY(mg_build(h, prm));
+    TRY(mg_setup(h, prm, picard));
+    theta = h->mg[0].theta;
+    bmax = theta + h->mg[0].delta;
+    amin = theta - h->mg[0].delta;
   }
   const float inv_theta = (float)(1.0 / theta);
   const int g = vgrid(h, N);
@@ -1219,6 +1645,12 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     TRY(poll(h));
     if (res0 < 0.0) res0 = h->st_host->res0;
     auto precondition = [&]() -> int {
+      if (use_mg) {
+        TRY(mg_vcycle(h, picard));
+        k_cgm_update_p<<<g, VT, 0, h->stream>>>(N, h->z, h->pv, h->Ap, h->st); ++h->launches;
+        CU(cudaGetLastError());
+        return MPDG_OK;
+      }
       for (int j = 1; j <= k; ++j) {
         TRY(op_apply_f(h, h->Ax32, h->x32, h->st, picard));
         if (j < k) {
@@ -1428,6 +1860,10 @@ extern "C" void mpdg_solver_params_default(mpdg_solver_params *p)
   p->cheb_max_factor = 1.2;
   p->cheb_min_fraction = 0.0;
   p->tol_reference_norm = 0.0;
+  p->mg_smoothing_degree = 2;
+  p->mg_coarse_degree = 8;
+  p->mg_smoothing_range = 8.0;
+  p->mg_min_cells = 4;
 }
 
 extern "C" void mpdg_step_params_default(mpdg_step_params *p)
@@ -1445,6 +1881,12 @@ extern "C" void mpdg_step_params_default(mpdg_step_params *p)
 static void release(mpdg_heat *h)
 {
   if (h->stream) cudaStreamSynchronize(h->stream);
+  for (MGLevel &lv : h->mg)
+    if (lv.own && lv.h) {
+      release(lv.h);
+      delete lv.h;
+    }
+  h->mg.clear();
   drain_events(h);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   h->ev_pool.clear();
@@ -1456,7 +1898,50 @@ static void release(mpdg_heat *h)
   h->scal_host = nullptr;
 }
 
+// vertices of the box mesh: interior vertices perturbed by a counter hash of
+// (seed, 3 * vertex + component), uniform in +-perturb * h
+static std::vector<double> box_vertices(const mpdg_mesh_desc &desc)
+{
+  const int64_t nv = (int64_t)(desc.cells[0] + 1) * (desc.cells[1] + 1) * (desc.cells[2] + 1);
+  std::vector<double> vert(3 * nv);
+  double hc[3];
+  for (int e = 0; e < 3; ++e) hc[e] = (desc.hi[e] - desc.lo[e]) / desc.cells[e];
+  for (int c = 0; c <= desc.cells[2]; ++c)
+    for (int b = 0; b <= desc.cells[1]; ++b)
+      for (int a = 0; a <= desc.cells[0]; ++a) {
+        const int idx[3] = {a, b, c};
+        const int64_t v = a + (int64_t)(desc.cells[0] + 1) * (b + (int64_t)(desc.cells[1] + 1) * c);
+        bool interior = true;
+        for (int e = 0; e < 3; ++e)
+          if (idx[e] == 0 || idx[e] == desc.cells[e]) interior = false;
+        for (int e = 0; e < 3; ++e) {
+          double x = desc.lo[e] + hc[e] * idx[e];
+          if (interior) {
+            uint64_t r = desc.seed * 0xD1B54A32D192ED03ULL + (uint64_t)(3 * v + e);
+            r += 0x9E3779B97F4A7C15ULL;
+            r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ULL;
+            r = (r ^ (r >> 27)) * 0x94D049BB133111EBULL;
+            r ^= r >> 31;
+            const double u = 2.0 * ((double)(r >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+            x += desc.perturb * hc[e] * u;
+          }
+          vert[3 * v + e] = x;
+        }
+      }
+  return vert;
+}
+
+// verts: host vertices of a deformed mesh ((cells + 1)^3 x 3), or null to generate them
+static int create_impl(const mpdg_mesh_desc *desc, int device, const std::vector<double> *verts,
+                       mpdg_heat **out);
+
 extern "C" int mpdg_heat_create(const mpdg_mesh_desc *desc, int device, mpdg_heat **out)
+{
+  return create_impl(desc, device, nullptr, out);
+}
+
+static int create_impl(const mpdg_mesh_desc *desc, int device, const std::vector<double> *verts,
+                       mpdg_heat **out)
 {
   if (!desc || !out) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
@@ -1517,29 +2002,10 @@ extern "C" int mpdg_heat_create(const mpdg_mesh_desc *desc, int device, mpdg_hea
     // vertices on the host (counter-hash perturbation of interior vertices), then
     // per-quadrature-point geometry on the device
     const int64_t nv = (int64_t)(desc->cells[0] + 1) * (desc->cells[1] + 1) * (desc->cells[2] + 1);
-    std::vector<double> vert(3 * nv);
-    for (int c = 0; c <= desc->cells[2]; ++c)
-      for (int b = 0; b <= desc->cells[1]; ++b)
-        for (int a = 0; a <= desc->cells[0]; ++a) {
-          const int idx[3] = {a, b, c};
-          const int64_t v = a + (int64_t)(desc->cells[0] + 1) * (b + (int64_t)(desc->cells[1] + 1) * c);
-          bool interior = true;
-          for (int e = 0; e < 3; ++e)
-            if (idx[e] == 0 || idx[e] == desc->cells[e]) interior = false;
-          for (int e = 0; e < 3; ++e) {
-            double x = desc->lo[e] + h->hcell[e] * idx[e];
-            if (interior) {
-              uint64_t r = desc->seed * 0xD1B54A32D192ED03ULL + (uint64_t)(3 * v + e);
-              r += 0x9E3779B97F4A7C15ULL;
-              r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ULL;
-              r = (r ^ (r >> 27)) * 0x94D049BB133111EBULL;
-              r ^= r >> 31;
-              const double u = 2.0 * ((double)(r >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
-              x += desc->perturb * h->hcell[e] * u;
-            }
-            vert[3 * v + e] = x;
-          }
-        }
+    std::vector<double> gen;
+    if (!verts) gen = box_vertices(*desc);
+    const std::vector<double> &vert = verts ? *verts : gen;
+    if ((int64_t)vert.size() != 3 * nv) return cleanup(fail(MPDG_ERR_INVALID_ARGUMENT, "vertex count"));
     if ((rc = dvec(h, &h->vert, 3 * nv)) != MPDG_OK) return cleanup(rc);
     if ((rc = dvec(h, &h->geoq, h->n_cells * 7 * h->npt)) != MPDG_OK) return cleanup(rc);
     if (cudaMemcpy(h->vert, vert.data(), sizeof(double) * 3 * nv, cudaMemcpyHostToDevice) !=
@@ -1858,7 +2324,8 @@ static int linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   mpdg_solve_stats local;
   memset(&local, 0, sizeof(local));
   if (prm->solver == MPDG_SOLVER_GMRES) {
-    if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32)
+    if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 ||
+        prm->preconditioner == MPDG_PRECOND_MG_F32)
       return fail(MPDG_ERR_NOT_SUPPORTED, "GMRES supports identity or Jacobi preconditioning");
     const double *D = nullptr;
     if (prm->preconditioner == MPDG_PRECOND_JACOBI) {
@@ -1868,7 +2335,8 @@ static int linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     TRY(gmres(h, prm, x, b, D, &local));
   } else if (prm->solver != MPDG_SOLVER_CG) {
     return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown solver type");
-  } else if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32) {
+  } else if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 ||
+             prm->preconditioner == MPDG_PRECOND_MG_F32) {
     TRY(cg_chebyshev(h, prm, x, b, &local));
   } else {
     const double *D = nullptr;

@@ -119,7 +119,7 @@ def material(law=L.LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_
 
 @dataclass
 class LinearSolverData:
-    """LinearSolverData (linear_solver_data.hpp:40-47) plus the Chebyshev options."""
+    """LinearSolverData (linear_solver_data.hpp:40-47) plus the Chebyshev and multigrid options."""
     solver_type: int = L.SOLVER_CG
     preconditioner_type: int = L.PRECOND_JACOBI
     max_iterations: int = 10000
@@ -133,13 +133,19 @@ class LinearSolverData:
     tol_reference_norm: float = 0.0
     cheb_picard: bool = False
     cheb_eig_reuse: bool = False
+    mg_smoothing_degree: int = 2
+    mg_coarse_degree: int = 8
+    mg_smoothing_range: float = 8.0
+    mg_min_cells: int = 4
 
     def to_c(self) -> L.SolverParams:
         return L.SolverParams(self.solver_type, self.preconditioner_type, self.max_iterations,
                               self.rel_tolerance, self.abs_tolerance, self.gmres_restart,
                               self.cheb_degree, self.cheb_eig_iterations, self.cheb_max_factor,
                               self.cheb_min_fraction, self.tol_reference_norm,
-                              int(self.cheb_picard), int(self.cheb_eig_reuse))
+                              int(self.cheb_picard), int(self.cheb_eig_reuse),
+                              self.mg_smoothing_degree, self.mg_coarse_degree,
+                              self.mg_smoothing_range, self.mg_min_cells)
 
 
 @dataclass

@@ -29,7 +29,8 @@ def test_unidirectional_heat_transfer_newton_on_gpu():
         assert float(f"{op.l2_norm(opn.T):.5e}") == ref
 
 
-@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_CHEBYSHEV_JACOBI_F32])
+@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_CHEBYSHEV_JACOBI_F32,
+                                     L.PRECOND_MG_F32])
 def test_single_linearization_step_matches_oracle(precond):
     """One k(T) = 1 + 0.5 T step: T = T_g + J(T_g)^-1 (-R(T_g)), Gaussian source."""
     deg, cells, dt = 3, (6, 6, 6), 5e-4

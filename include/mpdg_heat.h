@@ -169,6 +169,9 @@ int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src);
  * k(T_lin) frozen at the quadrature points. Boundary-face terms as in
  * mpdg_heat_vmult_f32. MPDG_ERR_INVALID_ARGUMENT for the other laws. */
 int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float *src);
+/* Inverse diagonal of that FP32 Picard operator (|d| > 1e-10 ? 1/d : 1), the Jacobi
+ * scaling of the multigrid smoothers. Same restrictions. */
+int mpdg_heat_inverse_diagonal_f32_picard(mpdg_heat *h, float *inv_diag);
 /* compute_inverse_diagonal_from_matrixfree (heat_diffuse_operator.cpp:271-284):
  * diag(J) inverted with |d| > 1e-10 ? 1/d : 1. */
 int mpdg_heat_compute_inverse_diagonal(mpdg_heat *h, double *inv_diag);

@@ -100,6 +100,7 @@ _SIGS = {
     "mpdg_heat_vmult": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult_f32": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult_f32_picard": (C.c_int, [_H, _D, _D]),
+    "mpdg_heat_inverse_diagonal_f32_picard": (C.c_int, [_H, _D]),
     "mpdg_heat_compute_inverse_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),
     "mpdg_heat_distribute_constraints": (C.c_int, [_H, _D]),

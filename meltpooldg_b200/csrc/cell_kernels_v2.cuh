@@ -484,4 +484,223 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_conductivity_q(CellArgs<doubl
   }
 }
 
+// Diagonal of the FP32 Picard operator (conductivity field kq at the q-points, no
+// dk/dT term): diag_i = sum_q c JxW phi_i^2 + grad phi_i^T (kq G) grad phi_i, sum-
+// factorised with the element-wise products P = S o S, Q = D o D, R = S o D of the 1D
+// value and collocation-derivative matrices (transposed tables kPT, kQT, kRT):
+// contraction along z and y on X-layout planes, along x on Z-layout planes.
+//   A_PP = P_z C0 + Q_z Gzz   A_PQ = P_z Gyy   A_QP = P_z Gxx
+//   X_P = P_y A_PP + Q_y A_PQ   X_Q = P_y A_QP   W = P_x X_P + Q_x X_Q
+// plus on deformed cells the cross terms (2 kq Gxy ... in R products):
+//   A_PR = R_z Gyz  A_RR = P_z Gxy  A_RP = R_z Gxz
+//   X_P += R_y A_PR   X_R = R_y A_RR + P_y A_RP   W += R_x X_R
+// a.dst (FP32) accumulates; Dirichlet rows are skipped.
+template <int n, int GEO>
+__global__ void __launch_bounds__(32 * kV2Warps) k_diag_picard(CellArgs<float> a)
+{
+  using T = float;
+  constexpr int CW = v2_cells_per_warp<n>();
+  constexpr int CS = v2_cell_stride<n>();
+  constexpr int npt = n * n * n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cw = lane / n, t = lane % n;
+  const bool lane_ok = cw < CW;
+  T *wbuf = reinterpret_cast<T *>(smem_raw) + (size_t)warp * 2 * (CW + 1) * CS;
+  T *bufA = wbuf + cw * CS;
+  T *bufB = wbuf + (CW + 1) * CS + cw * CS;
+  const MeshDims &d = a.d;
+  const T cval = a.m.idt * (a.m.rho_l * a.m.cp_l);
+  const int64_t n_groups = (a.n_cells + CW - 1) / CW;
+  for (int64_t grp = (int64_t)blockIdx.x * kV2Warps + warp; grp < n_groups;
+       grp += (int64_t)gridDim.x * kV2Warps) {
+    const int64_t cell = grp * CW + cw;
+    const bool active = lane_ok && cell < a.n_cells;
+    const int64_t cc = active ? cell : 0;
+    const int cx = (int)(cc % d.m[0]);
+    const int cy = (int)((cc / d.m[0]) % d.m[1]);
+    const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
+    const int I0 = d.p * cx, J0 = d.p * cy, K = d.p * cz + t;
+    const int64_t base = (int64_t)d.nd[0] * (J0 + (int64_t)d.nd[1] * K) + I0;
+    const PlaneMask pm(d, I0, J0, K, d.p);
+    // q-point coefficients on X-layout planes: thread t = q_x, registers [q_z][q_y]
+    T APP[n][n], APQ[n][n], AQP[n][n];
+    {
+      T C0[n][n], Gxx[n][n], Gyy[n][n], Gzz[n][n];
+#pragma unroll
+      for (int k = 0; k < n; ++k)
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          T jxw, G[6];
+          geo_at<n, GEO>(a.g, cc, t, j, k, jxw, G);
+          const T kk = active ? (T)__ldg(a.kq + cc * npt + t + n * (j + n * k)) : T(0);
+          C0[k][j] = active ? cval * jxw : T(0);
+          Gxx[k][j] = kk * G[0];
+          Gyy[k][j] = kk * G[3];
+          Gzz[k][j] = kk * G[5];
+        }
+      psweep_a<n, kPT, false>(C0, APP);
+      psweep_a<n, kQT, true>(Gzz, APP);
+      psweep_a<n, kPT, false>(Gyy, APQ);
+      psweep_a<n, kPT, false>(Gxx, AQP);
+    }
+    T XP[n][n], XQ[n][n];
+    psweep_b<n, kPT, false>(APP, XP);
+    psweep_b<n, kQT, true>(APQ, XP);
+    psweep_b<n, kPT, false>(AQP, XQ);
+    T XR[n][n];
+    if (GEO == 1) {
+      T Gxy[n][n], Gxz[n][n], Gyz[n][n];
+#pragma unroll
+      for (int k = 0; k < n; ++k)
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          T jxw, G[6];
+          geo_at<n, GEO>(a.g, cc, t, j, k, jxw, G);
+          const T kk = active ? (T)__ldg(a.kq + cc * npt + t + n * (j + n * k)) : T(0);
+          Gxy[k][j] = T(2) * kk * G[1];
+          Gxz[k][j] = T(2) * kk * G[2];
+          Gyz[k][j] = T(2) * kk * G[4];
+        }
+      T A1[n][n], A2[n][n];
+      psweep_a<n, kRT, false>(Gyz, A1);  // A_PR
+      psweep_b<n, kRT, true>(A1, XP);
+      psweep_a<n, kPT, false>(Gxy, A1);  // A_RR
+      psweep_a<n, kRT, false>(Gxz, A2);  // A_RP
+      psweep_b<n, kRT, false>(A1, XR);
+      psweep_b<n, kPT, true>(A2, XR);
+    }
+    T ZP[n][n], ZQ[n][n];
+    x_to_z2<n>(XP, XQ, ZP, ZQ, bufA, bufB, t);
+    T W[n][n];
+    psweep_b<n, kPT, false>(ZP, W);
+    psweep_b<n, kQT, true>(ZQ, W);
+    if (GEO == 1) {
+      x_to_z2<n>(XR, XR, ZP, ZQ, bufA, bufB, t);
+      psweep_b<n, kRT, true>(ZP, W);
+    }
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const int64_t row = base + (int64_t)d.nd[0] * j;
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+          if (!pm.template at<n>(i, j)) atomicAdd(a.dst + row + i, W[j][i]);
+      }
+    }
+  }
+}
+
+// create_rhs on register-resident planes for laws with constant rho*cp (0, 1):
+// dst += -R(T) = -sum_q [ (c (T - T_old) - q_h) phi_i JxW + k(T) grad T . G grad phi_i ]
+// with c = rho*cp / dt (rhs_cell_loop, heat_diffuse_operator.cpp:393-529). The value
+// term is linear in the nodal values, so w = c (T - T_old) - q is formed at the gather
+// and interpolated once.
+template <int n, int GEO, int LAW>
+__global__ void __launch_bounds__(32 * kV2Warps) k_rhs2(CellArgs<double> a)
+{
+  static_assert(LAW == 0 || LAW == 1, "constant rho*cp laws");
+  using T = double;
+  constexpr int CW = v2_cells_per_warp<n>();
+  constexpr int CS = v2_cell_stride<n>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cw = lane / n, t = lane % n;
+  const bool lane_ok = cw < CW;
+  T *wbuf = reinterpret_cast<T *>(smem_raw) + (size_t)warp * 2 * (CW + 1) * CS;
+  T *bufA = wbuf + cw * CS;
+  T *bufB = wbuf + (CW + 1) * CS + cw * CS;
+  const MeshDims &d = a.d;
+  const T c = a.m.idt * (a.m.rho_l * a.m.cp_l);
+  const int64_t n_groups = (a.n_cells + CW - 1) / CW;
+  for (int64_t grp = (int64_t)blockIdx.x * kV2Warps + warp; grp < n_groups;
+       grp += (int64_t)gridDim.x * kV2Warps) {
+    const int64_t cell = grp * CW + cw;
+    const bool active = lane_ok && cell < a.n_cells;
+    const int64_t cc = active ? cell : 0;
+    const int cx = (int)(cc % d.m[0]);
+    const int cy = (int)((cc / d.m[0]) % d.m[1]);
+    const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
+    const int I0 = d.p * cx, J0 = d.p * cy, K = d.p * cz + t;
+    const int64_t base = (int64_t)d.nd[0] * (J0 + (int64_t)d.nd[1] * K) + I0;
+    const PlaneMask pm(d, I0, J0, K, d.p);
+    T Pt[n][n], Pw[n][n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const int64_t row = base + (int64_t)d.nd[0] * j;
+#pragma unroll
+      for (int i = 0; i < n; ++i) {
+        T tv = T(0), w = T(0);
+        if (active) {
+          tv = __ldg(a.Tl + row + i);
+          w = c * (tv - __ldg(a.To + row + i)) - (a.qs ? __ldg(a.qs + row + i) : T(0));
+        }
+        Pt[j][i] = tv;
+        Pw[j][i] = w;
+      }
+    }
+    // T at the q-points: values and reference gradients (X-layout)
+    T Fx[n][n], Fy[n][n], Fz[n][n];
+    {
+      T Dx[n][n], Tq[n][n];
+      psweep_b<n, kS, false>(Pt, Pt);
+      psweep_a<n, kS, false>(Pt, Pt);
+      psweep_b<n, kD, false>(Pt, Dx);
+      z_to_x2<n>(Pt, Dx, Tq, Fx, bufA, bufB, t);
+      psweep_a<n, kS, false>(Tq, Tq);
+      psweep_a<n, kS, false>(Fx, Fx);
+      psweep_b<n, kD, false>(Tq, Fy);
+      psweep_a<n, kD, false>(Tq, Fz);
+      // f = -k(T) G grad T
+#pragma unroll
+      for (int k = 0; k < n; ++k)
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          T jxw, G[6];
+          geo_at<n, GEO>(a.g, cc, t, j, k, jxw, G);
+          T rhocp, kk, drhocp, dk;
+          mat_eval<LAW>(a.m, Tq[k][j], rhocp, kk, drhocp, dk);
+          T F0, F1, F2;
+          apply_G<GEO>(G, kk * Fx[k][j], kk * Fy[k][j], kk * Fz[k][j], F0, F1, F2);
+          Fx[k][j] = -F0;
+          Fy[k][j] = -F1;
+          Fz[k][j] = -F2;
+        }
+    }
+    // w at the q-points, val = -w JxW
+    T U[n][n];
+    psweep_b<n, kS, false>(Pw, Pw);
+    psweep_a<n, kS, false>(Pw, Pw);
+    z_to_x1<n>(Pw, U, bufA, t);
+    psweep_a<n, kS, false>(U, U);
+#pragma unroll
+    for (int k = 0; k < n; ++k)
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        T jxw, G[6];
+        geo_at<n, GEO>(a.g, cc, t, j, k, jxw, G);
+        U[k][j] = -U[k][j] * jxw;
+      }
+    // integration (as in k_vmult2)
+    psweep_b<n, kDT, true>(Fy, U);
+    psweep_a<n, kDT, true>(Fz, U);
+    psweep_a<n, kST, false>(U, U);
+    psweep_a<n, kST, false>(Fx, Fx);
+    T W[n][n], Wx[n][n];
+    x_to_z2<n>(U, Fx, W, Wx, bufA, bufB, t);
+    psweep_b<n, kDT, true>(Wx, W);
+    psweep_b<n, kST, false>(W, W);
+    psweep_a<n, kST, false>(W, W);
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const int64_t row = base + (int64_t)d.nd[0] * j;
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+          if (!pm.template at<n>(i, j)) atomic_add(a.dst + row + i, W[j][i]);
+      }
+    }
+  }
+}
+
 }  // namespace mpdg

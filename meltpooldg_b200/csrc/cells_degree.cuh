@@ -135,6 +135,17 @@ struct DegreeOps {
   template <int GEO, int LAW>
   static cudaError_t rhs_t(const CellArgs<double> &a, cudaStream_t s, int sm)
   {
+    if constexpr (use_v2<double>() && (LAW == 0 || LAW == 1)) {
+      static int cache2 = 0;
+      auto k2 = k_rhs2<n, GEO, LAW>;
+      const size_t smem2 =
+        sizeof(double) * kV2Warps * 2 * (v2_cells_per_warp<n>() + 1) * v2_cell_stride<n>();
+      const int64_t ng = (a.n_cells + v2_cells_per_warp<n>() - 1) / v2_cells_per_warp<n>();
+      const int g2 = persistent_grid(k2, 32 * kV2Warps, smem2, (ng + kV2Warps - 1) / kV2Warps, sm,
+                                     &cache2);
+      k2<<<g2, 32 * kV2Warps, smem2, s>>>(a);
+      return cudaGetLastError();
+    }
     static int cache = 0;
     auto k = k_rhs<n, GEO, LAW>;
     const size_t smem = smem_rhs<n>();
@@ -202,6 +213,21 @@ struct DegreeOps {
     k<<<g, 32 * kV2Warps, smem, s>>>(a, kq);
     return cudaGetLastError();
   }
+  template <int GEO>
+  static cudaError_t diag_picard_t(const CellArgs<float> &a, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_diag_picard<n, GEO>;
+    const size_t smem = sizeof(float) * kV2Warps * 2 * (v2_cells_per_warp<n>() + 1) * v2_cell_stride<n>();
+    const int64_t ng = (a.n_cells + v2_cells_per_warp<n>() - 1) / v2_cells_per_warp<n>();
+    const int g = persistent_grid(k, 32 * kV2Warps, smem, (ng + kV2Warps - 1) / kV2Warps, sm, &cache);
+    k<<<g, 32 * kV2Warps, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t diag_picard(const CellArgs<float> &a, int geo, cudaStream_t s, int sm)
+  {
+    return geo == 0 ? diag_picard_t<0>(a, s, sm) : diag_picard_t<1>(a, s, sm);
+  }
   static cudaError_t conductivity_q(const CellArgs<double> &a, float *kq, int law, cudaStream_t s,
                                     int sm)
   {
@@ -220,7 +246,10 @@ struct DegreeOps {
     t.rhs = &rhs;
     t.diag = &diag;
     t.norm = &norm;
-    if constexpr (use_v2<float>()) t.conductivity_q = &conductivity_q;
+    if constexpr (use_v2<float>()) {
+      t.conductivity_q = &conductivity_q;
+      t.diag_picard = &diag_picard;
+    }
     return t;
   }
 };

@@ -18,6 +18,8 @@ struct DegreeTable {
   // kq[cell][q] = k(T_lin) in FP32; nullptr where the degree has no register-resident kernel
   cudaError_t (*conductivity_q)(const CellArgs<double> &, float *kq, int law, cudaStream_t,
                                 int sm) = nullptr;
+  // a.dst += diagonal of the FP32 Picard operator (conductivity field a.kq); same degrees
+  cudaError_t (*diag_picard)(const CellArgs<float> &, int geo, cudaStream_t, int sm) = nullptr;
 };
 
 DegreeTable degree_table_2();

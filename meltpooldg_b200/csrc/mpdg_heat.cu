@@ -383,6 +383,15 @@ __global__ void k_cast_f(int64_t N, const double *__restrict__ x, float *__restr
 {
   GRID_STRIDE(i, N) y[i] = (float)x[i];
 }
+// inv = |d| > 1e-10 ? 1/d : 1 (the FP64 rule of compute_inverse_diagonal, in FP32)
+__global__ void k_invert_diag_f(int64_t N, const float *__restrict__ d, float *inv)
+{
+  GRID_STRIDE(i, N)
+  {
+    const float v = d[i];
+    inv[i] = fabsf(v) > 1.0e-10f ? 1.f / v : 1.f;
+  }
+}
 __global__ void k_invert_diag(int64_t N, double *d)
 {
   GRID_STRIDE(i, N)
@@ -702,18 +711,32 @@ __global__ void k_inject(Dims3 fd, Dims3 cd, int r, const double *__restrict__ f
   }
 }
 
+// The transfer kernels index with 32 bits (every level holds < 2^31 nodes): a
+// grid-stride loop over the flattened output with unsigned 32-bit div/mod.
+#define TRANSFER_LOOP(i, d)                                                                  \
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < (unsigned)(d).size();       \
+       i += gridDim.x * blockDim.x)
+__device__ __forceinline__ void transfer_index(const Dims3 &d, unsigned i, int o[3])
+{
+  const unsigned r = i / (unsigned)d.n[0];
+  o[0] = (int)(i - r * (unsigned)d.n[0]);
+  o[2] = (int)(r / (unsigned)d.n[1]);
+  o[1] = (int)(r - (unsigned)o[2] * (unsigned)d.n[1]);
+}
+
 // restriction along one axis (transpose of the interpolation below):
-// out[.., V, ..] = sum_{|s| < r} phi_V(node r V + s) in[.., r V + s, ..]; masked rows of
-// the coarse level are set to zero
+// out[.., V, ..] = sum_{|s| < r} phi_V(node r V + s) in[.., r V + s, ..]; with sub, the
+// input is b - in (the residual of the smoothed iterate, formed on the fly); masked rows
+// of the coarse level are set to zero
 __global__ void k_restrict_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
-                                const float *__restrict__ in, float *out, MeshDims md, int masked,
-                                const SolverState *st)
+                                const float *__restrict__ in, const float *__restrict__ sub_b,
+                                float *out, MeshDims md, int masked, const SolverState *st)
 {
   if (st && st->done) return;
-  GRID_STRIDE(i, dout.size())
+  TRANSFER_LOOP(i, dout)
   {
-    int o[3] = {(int)(i % dout.n[0]), (int)((i / dout.n[0]) % dout.n[1]),
-                (int)(i / ((int64_t)dout.n[0] * dout.n[1]))};
+    int o[3];
+    transfer_index(dout, i, o);
     if (masked && constrained(md, o[0], o[1], o[2])) {
       out[i] = 0.f;
       continue;
@@ -726,23 +749,26 @@ __global__ void k_restrict_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
       const float w = s == 0 ? 1.f : (s > 0 ? 1.f - t.xi[s] : t.xi[t.r + s]);
       int p[3] = {o[0], o[1], o[2]};
       p[axis] = I;
-      acc += w * in[di.at(p[0], p[1], p[2])];
+      const unsigned j = (unsigned)p[0] + (unsigned)di.n[0] * ((unsigned)p[1] + (unsigned)di.n[1] * (unsigned)p[2]);
+      acc += w * (sub_b ? sub_b[j] - in[j] : in[j]);
     }
     out[i] = acc;
   }
 }
 
 // interpolation along one axis: out[.., I, ..] = (1 - xi_a) in[.., V, ..] + xi_a in[.., V + 1, ..]
-// with V = I / r, a = I % r; add: accumulate into out; masked rows are left untouched
+// with V = I / r, a = I % r; add: accumulate into out; masked rows are left untouched;
+// zero (optional): an array of out's shape set to zero on the way
 __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
                                const float *__restrict__ in, float *out, int add, MeshDims md,
-                               int masked, const SolverState *st)
+                               int masked, float *zero, const SolverState *st)
 {
   if (st && st->done) return;
-  GRID_STRIDE(i, dout.size())
+  TRANSFER_LOOP(i, dout)
   {
-    int o[3] = {(int)(i % dout.n[0]), (int)((i / dout.n[0]) % dout.n[1]),
-                (int)(i / ((int64_t)dout.n[0] * dout.n[1]))};
+    int o[3];
+    transfer_index(dout, i, o);
+    if (zero) zero[i] = 0.f;
     if (masked && constrained(md, o[0], o[1], o[2])) {
       if (!add) out[i] = 0.f;
       continue;
@@ -750,10 +776,11 @@ __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
     const int I = o[axis], V = I / t.r, a = I - V * t.r;
     int p[3] = {o[0], o[1], o[2]};
     p[axis] = V;
-    float v = in[di.at(p[0], p[1], p[2])];
+    float v = in[(unsigned)p[0] + (unsigned)di.n[0] * ((unsigned)p[1] + (unsigned)di.n[1] * (unsigned)p[2])];
     if (a != 0) {
       p[axis] = V + 1;
-      v = (1.f - t.xi[a]) * v + t.xi[a] * in[di.at(p[0], p[1], p[2])];
+      v = (1.f - t.xi[a]) * v +
+          t.xi[a] * in[(unsigned)p[0] + (unsigned)di.n[0] * ((unsigned)p[1] + (unsigned)di.n[1] * (unsigned)p[2])];
     }
     out[i] = add ? out[i] + v : v;
   }
@@ -772,13 +799,6 @@ __global__ void k_cheb_init(int64_t N, const float *__restrict__ b, float *x, fl
   }
 }
 
-// Ax = b - Ax (the residual of the smoothed iterate, restricted next)
-__global__ void k_residual32(int64_t N, const float *__restrict__ b, float *Ax,
-                             const SolverState *st)
-{
-  if (st->done) return;
-  GRID_STRIDE(i, N) Ax[i] = b[i] - Ax[i];
-}
 
 // ---- GMRES building blocks --------------------------------------------------
 constexpr int kMaxBasis = 32;
@@ -1316,6 +1336,28 @@ static void cheb_coefficients(double theta, double delta, int k, std::vector<flo
 
 static Dims3 nodal_dims(const mpdg_heat *h) { return Dims3{{h->dims.nd[0], h->dims.nd[1], h->dims.nd[2]}}; }
 
+// inverse diagonal of the FP32 Picard operator into h->inv_diag_f (h->kq current);
+// h->d32 serves as the accumulator (its content is dead outside a preconditioner call)
+static int picard_inverse_diagonal(mpdg_heat *h)
+{
+  const int64_t N = h->n_dofs;
+  TRY(ensure_dt(h));
+  TRY(ensure_workspace_f32(h));
+  TRY(refresh_f32(h));
+  CU(cudaMemsetAsync(h->d32, 0, sizeof(float) * N, h->stream));
+  CellArgs<float> a = cell_args<float>(h);
+  a.kq = h->kq;
+  a.g.q = h->geoq_f;
+  a.dst = h->d32;
+  CU(h->tab.diag_picard(a, h->geo, h->stream, h->sm_count));
+  ++h->launches;
+  if (any_faces(h)) TRY(launch_faces<float>(h, 2, h->d32, nullptr, h->T_lin_f, nullptr, nullptr));
+  k_invert_diag_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->d32, h->inv_diag_f);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
 static int mg_build(mpdg_heat *h, const mpdg_solver_params *prm)
 {
   if (!h->mg.empty() && h->mg_min_cells == prm->mg_min_cells) return MPDG_OK;
@@ -1456,15 +1498,26 @@ static int mg_setup(mpdg_heat *h, const mpdg_solver_params *prm, bool picard)
         CU(c->tab.conductivity_q(a, c->kq, c->law, h->stream, c->sm_count));
         ++h->launches;
       }
-      TRY(compute_diag(c, c->inv_diag));
-      c->diag_valid = true;
-      k_cast_f<<<vgrid(c, c->n_dofs), VT, 0, h->stream>>>(c->n_dofs, c->inv_diag, c->inv_diag_f);
-      ++h->launches;
-      CU(cudaGetLastError());
-      if (!c->eig_valid || !prm->cheb_eig_reuse) {
+      const bool estimate = !c->eig_valid || !prm->cheb_eig_reuse;
+      if (estimate || !picard) {
+        // FP64 tangent diagonal: for the Lanczos estimate, and as the smoother's
+        // diagonal when the levels apply the tangent itself
+        TRY(compute_diag(c, c->inv_diag));
+        c->diag_valid = true;
+      }
+      if (estimate) {
         TRY(estimate_eigenvalues(c, prm->cheb_eig_iterations, &c->eig_min, &c->eig_max));
         c->eig_valid = true;
       }
+    }
+    // the smoother's Jacobi diagonal: of the operator the level applies
+    if (picard) {
+      TRY(picard_inverse_diagonal(c));
+      if (l == 0) h->diag_f_dirty = true;  // inv_diag_f no longer mirrors the FP64 diagonal
+    } else if (l > 0) {
+      k_cast_f<<<vgrid(c, c->n_dofs), VT, 0, h->stream>>>(c->n_dofs, c->inv_diag, c->inv_diag_f);
+      ++h->launches;
+      CU(cudaGetLastError());
     }
     const double upper = prm->cheb_max_factor * c->eig_max;
     double lower = upper / std::max(1.5, prm->mg_smoothing_range);
@@ -1480,7 +1533,9 @@ static int mg_setup(mpdg_heat *h, const mpdg_solver_params *prm, bool picard)
   return MPDG_OK;
 }
 
-static int mg_restrict(mpdg_heat *h, int l, const float *fine, float *coarse)
+// coarse = R (fine_b - fine_Ax)
+static int mg_restrict(mpdg_heat *h, int l, const float *fine_Ax, const float *fine_b,
+                       float *coarse)
 {
   const MGLevel &f = h->mg[l], &c = h->mg[l + 1];
   const Dims3 F = nodal_dims(f.h), C = nodal_dims(c.h);
@@ -1488,18 +1543,19 @@ static int mg_restrict(mpdg_heat *h, int l, const float *fine, float *coarse)
   Transfer1D t;
   t.r = f.ratio;
   for (int a = 0; a < 8; ++a) t.xi[a] = f.xi[a];
-  k_restrict_axis<<<vgrid(h, D1.size()), VT, 0, h->stream>>>(0, F, D1, t, fine, h->mg_t1,
-                                                              c.h->dims, 0, h->st);
-  k_restrict_axis<<<vgrid(h, D2.size()), VT, 0, h->stream>>>(1, D1, D2, t, h->mg_t1, h->mg_t2,
-                                                              c.h->dims, 0, h->st);
-  k_restrict_axis<<<vgrid(h, C.size()), VT, 0, h->stream>>>(2, D2, C, t, h->mg_t2, coarse,
-                                                             c.h->dims, 1, h->st);
+  k_restrict_axis<<<vgrid(h, D1.size()), VT, 0, h->stream>>>(0, F, D1, t, fine_Ax, fine_b,
+                                                             h->mg_t1, c.h->dims, 0, h->st);
+  k_restrict_axis<<<vgrid(h, D2.size()), VT, 0, h->stream>>>(1, D1, D2, t, h->mg_t1, nullptr,
+                                                             h->mg_t2, c.h->dims, 0, h->st);
+  k_restrict_axis<<<vgrid(h, C.size()), VT, 0, h->stream>>>(2, D2, C, t, h->mg_t2, nullptr, coarse,
+                                                            c.h->dims, 1, h->st);
   h->launches += 3;
   CU(cudaGetLastError());
   return MPDG_OK;
 }
 
-static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine)
+// fine += P coarse (constrained rows untouched); zero_fine (fine-shaped) is set to zero
+static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine, float *zero_fine)
 {
   const MGLevel &f = h->mg[l], &c = h->mg[l + 1];
   const Dims3 F = nodal_dims(f.h), C = nodal_dims(c.h);
@@ -1508,11 +1564,11 @@ static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine)
   t.r = f.ratio;
   for (int a = 0; a < 8; ++a) t.xi[a] = f.xi[a];
   k_prolong_axis<<<vgrid(h, E2.size()), VT, 0, h->stream>>>(2, C, E2, t, coarse, h->mg_t2, 0,
-                                                             f.h->dims, 0, h->st);
+                                                            f.h->dims, 0, nullptr, h->st);
   k_prolong_axis<<<vgrid(h, E1.size()), VT, 0, h->stream>>>(1, E2, E1, t, h->mg_t2, h->mg_t1, 0,
-                                                             f.h->dims, 0, h->st);
+                                                            f.h->dims, 0, nullptr, h->st);
   k_prolong_axis<<<vgrid(h, F.size()), VT, 0, h->stream>>>(0, E1, F, t, h->mg_t1, fine, 1,
-                                                            f.h->dims, 1, h->st);
+                                                           f.h->dims, 1, zero_fine, h->st);
   h->launches += 3;
   CU(cudaGetLastError());
   return MPDG_OK;
@@ -1551,18 +1607,17 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
       ++h->launches;
     }
     if (l == L - 1) break;
+    // residual b - A x restricted (formed inside the first pass); Ax is reset to zero by
+    // the last prolongation pass on the way back up
     TRY(op_apply_f(c, v.Ax, v.x, st, picard));
-    k_residual32<<<g, VT, 0, h->stream>>>(N, v.b, v.Ax, st);
-    ++h->launches;
-    TRY(mg_restrict(h, l, v.Ax, h->mg[l + 1].b));
-    CU(cudaMemsetAsync(v.Ax, 0, sizeof(float) * N, h->stream));
+    TRY(mg_restrict(h, l, v.Ax, v.b, h->mg[l + 1].b));
   }
   for (int l = L - 2; l >= 0; --l) {
     MGLevel &v = h->mg[l];
     mpdg_heat *c = v.h;
     const int64_t N = c->n_dofs;
     const int g = vgrid(c, N);
-    TRY(mg_prolong_add(h, l, h->mg[l + 1].x, v.x));
+    TRY(mg_prolong_add(h, l, h->mg[l + 1].x, v.x, v.Ax));
     // post-smoothing: the Chebyshev recurrence restarted from the corrected iterate
     for (int j = 0; j <= v.steps; ++j) {
       TRY(op_apply_f(c, v.Ax, v.x, st, picard));
@@ -1588,7 +1643,13 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
                         mpdg_solve_stats *stats)
 {
   const int64_t N = h->n_dofs;
-  if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
+  const bool use_mg = prm->preconditioner == MPDG_PRECOND_MG_F32;
+  const bool picard = prm->cheb_picard && h->law == MPDG_LAW_LINEAR_K && h->tab.conductivity_q;
+  // the FP64 inverse diagonal feeds the Lanczos estimate and the Chebyshev smoother; the
+  // multigrid smoothers of the Picard operator use that operator's own FP32 diagonal
+  const bool need_diag = !(use_mg && picard) || !h->eig_valid || !prm->cheb_eig_reuse;
+  if (need_diag && !h->diag_valid)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
   if (prm->cheb_degree < 1) return fail(MPDG_ERR_INVALID_ARGUMENT, "cheb_degree < 1");
   if (prm->preconditioner == MPDG_PRECOND_MG_F32 &&
       (prm->mg_smoothing_degree < 1 || prm->mg_coarse_degree < 1 || !(prm->mg_smoothing_range > 1.0)))
@@ -1596,12 +1657,11 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   TRY(ensure_workspace(h));
   TRY(ensure_workspace_f32(h));
   TRY(refresh_f32(h));
-  if (h->diag_f_dirty) {
+  if (h->diag_f_dirty && !(use_mg && picard)) {
     k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->inv_diag, h->inv_diag_f); ++h->launches;
     CU(cudaGetLastError());
     h->diag_f_dirty = false;
   }
-  const bool picard = prm->cheb_picard && h->law == MPDG_LAW_LINEAR_K && h->tab.conductivity_q;
   if (picard) {
     TRY(dvec(h, &h->kq, h->n_cells * h->npt));
     CellArgs<double> a = cell_args<double>(h);
@@ -1613,7 +1673,6 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     TRY(estimate_eigenvalues(h, prm->cheb_eig_iterations, &h->eig_min, &h->eig_max));
     h->eig_valid = true;
   }
-  const bool use_mg = prm->preconditioner == MPDG_PRECOND_MG_F32;
   double bmax = prm->cheb_max_factor * h->eig_max;
   double amin = std::max(h->eig_min, prm->cheb_min_fraction * bmax);
   double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin);
@@ -2168,6 +2227,25 @@ extern "C" int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float 
   return op_apply_f(h, dst, src, nullptr, true);
 }
 
+extern "C" int mpdg_heat_inverse_diagonal_f32_picard(mpdg_heat *h, float *inv_diag)
+{
+  if (!h || !inv_diag) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (h->law != MPDG_LAW_LINEAR_K || !h->tab.conductivity_q)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "Picard operator: linear-k law, degree <= 4 only");
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_lin(h));
+  TRY(dvec(h, &h->kq, h->n_cells * h->npt));
+  CellArgs<double> a = cell_args<double>(h);
+  a.Tl = h->T_lin;
+  CU(h->tab.conductivity_q(a, h->kq, h->law, h->stream, h->sm_count));
+  ++h->launches;
+  TRY(picard_inverse_diagonal(h));
+  h->diag_f_dirty = true;  // inv_diag_f now holds the Picard diagonal
+  CU(cudaMemcpyAsync(inv_diag, h->inv_diag_f, sizeof(float) * h->n_dofs,
+                     cudaMemcpyDeviceToDevice, h->stream));
+  return MPDG_OK;
+}
+
 static int compute_diag(mpdg_heat *h, double *d)
 {
   TRY(ensure_dt(h));
@@ -2409,11 +2487,19 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     h->T_lin = T_cur;
     h->T_old = T_old;
     h->lin_f_dirty = true;
-    if (prm->linear.preconditioner != MPDG_PRECOND_IDENTITY) {
+    // JacobiPreconditioner::update; the multigrid preconditioner on the Picard operator
+    // needs the FP64 diagonal only for a new Lanczos estimate
+    const bool mg_picard = prm->linear.preconditioner == MPDG_PRECOND_MG_F32 &&
+                           prm->linear.cheb_picard && h->law == MPDG_LAW_LINEAR_K &&
+                           h->tab.conductivity_q;
+    if (prm->linear.preconditioner != MPDG_PRECOND_IDENTITY &&
+        (!mg_picard || !h->eig_valid || !prm->linear.cheb_eig_reuse)) {
       if ((rc = dvec(h, &h->inv_diag, N)) != MPDG_OK) break;
       if ((rc = compute_diag(h, h->inv_diag)) != MPDG_OK) break;
       h->diag_valid = true;
       h->diag_f_dirty = true;
+    } else if (mg_picard) {
+      h->diag_valid = false;  // the stored diagonal belongs to an earlier linearisation
     }
     if (prm->single_linearization) {
       // b = J T_g - R(T_g); solve J delta = -R(T_g) to |b - J T| <= tol |b|

@@ -250,6 +250,11 @@ class HeatDiffuseOperator:
                                                   _ptr(src, torch.float32)))
         return dst
 
+    def inverse_diagonal_picard_f32(self, inv_diag):
+        """Inverse diagonal of the FP32 Picard operator (the multigrid smoothers' scaling)."""
+        check(self._L.mpdg_heat_inverse_diagonal_f32_picard(self.h, _ptr(inv_diag, torch.float32)))
+        return inv_diag
+
     def compute_inverse_diagonal_from_matrixfree(self, diag):
         check(self._L.mpdg_heat_compute_inverse_diagonal(self.h, _ptr(diag)))
         return diag

@@ -680,7 +680,7 @@ static inline __attribute__((always_inline)) void integrate_vg(const orc_heat *h
 }
 
 /* kind: 0 vmult, 1 rhs, 2 diagonal, 3 l2 norm accumulate, 4 vmult without the
- * dk/dT grad(T_lin) u term (Picard operator) */
+ * dk/dT grad(T_lin) u term (Picard operator), 5 the diagonal of that operator */
 static inline __attribute__((always_inline)) void batch_kernel(
   const orc_heat *h, const int n, const int kind, const int64_t *cells, int nl, double *dst,
   const double *src, const double *Tl, const double *To, const double *qs, scratch_t *s,
@@ -742,9 +742,9 @@ static inline __attribute__((always_inline)) void batch_kernel(
       }
     integrate_vg(h, n, s->uq, s->gx, s->gy, s->gz, s, s->u);
     scatter_add(h, cells, nl, s->u, dst);
-  } else if (kind == 2) {
+  } else if (kind == 2 || kind == 5) {
     /* closed-form diagonal: sum_q c0 phi_i^2 + grad phi_i^T (kG) grad phi_i
-     *                       + dk phi_i grad phi_i^T G grad T */
+     *                       + dk phi_i grad phi_i^T G grad T  (kind 5: without the last) */
     if (h->tdep) {
       gather(h, cells, nl, Tl, 0, s->u);
       eval_vg(h, n, s->u, s, s->Tq, s->Tx, s->Ty, s->Tz);
@@ -769,7 +769,7 @@ static inline __attribute__((always_inline)) void batch_kernel(
         Gyy[q][v] = k * G[3];
         Gyz[q][v] = 2.0 * k * G[4];
         Gzz[q][v] = k * G[5];
-        if (h->tdep) {
+        if (h->tdep && kind == 2) {
           const double t0 = s->Tx[q][v], t1 = s->Ty[q][v], t2 = s->Tz[q][v];
           Bx[q][v] = dk * (G[0] * t0 + G[1] * t1 + G[2] * t2);
           By[q][v] = dk * (G[1] * t0 + G[3] * t1 + G[4] * t2);
@@ -1053,8 +1053,8 @@ void orc_inverse_diagonal(const orc_heat *h, double *d, const double *T_lin, con
                           int form)
 {
   memset(d, 0, sizeof(double) * h->n_dofs);
-  if (form == 0)
-    run_sf(h, 2, d, NULL, T_lin, T_old, NULL);
+  if (form == 0 || form == 2)
+    run_sf(h, form == 0 ? 2 : 5, d, NULL, T_lin, T_old, NULL);
   else
     run_direct(h, 2, d, NULL, T_lin, T_old);
   run_faces(h, 2, d, NULL, T_lin);

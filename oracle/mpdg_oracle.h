@@ -91,7 +91,8 @@ void orc_set_material(orc_heat *h, const orc_material *m, double dt);
  * term: conductivity k(T_lin) frozen at the quadrature points). */
 void orc_vmult(const orc_heat *h, double *dst, const double *src, const double *T_lin,
                const double *T_old, int form);
-/* inverse diagonal of J with the |d| > 1e-10 ? 1/d : 1 rule; form as above. */
+/* inverse diagonal of J with the |d| > 1e-10 ? 1/d : 1 rule; form as above (2: of the
+ * Picard operator). */
 void orc_inverse_diagonal(const orc_heat *h, double *inv_diag, const double *T_lin,
                           const double *T_old, int form);
 /* dst += -R(T) (rhs_cell_loop); T_old plain, heat_source nodal vector. */

@@ -102,6 +102,9 @@ def test_fp32_operator_cell_pairs(degree, cells, perturb):
     assert rel(g.vmult(g.new_vector(torch.float32), s32), o.vmult(src, Tl, To)) <= TOL32
     ref = o.vmult(src, Tl, To, form=2)
     assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), ref) <= TOL32
+    dref = o.inverse_diagonal(Tl, To, form=2)
+    dg = g.inverse_diagonal_picard_f32(g.new_vector(torch.float32))
+    assert rel(1.0 / dg.cpu().double().numpy(), 1.0 / dref) <= TOL32
 
 
 def test_fp32_packed_kernel_matches_oracle():

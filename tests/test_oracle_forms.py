@@ -78,3 +78,24 @@ def test_boundary_tangent_is_derivative_of_boundary_residual():
     d0 = 1.0 / o.inverse_diagonal(T, T_old, form=0)
     d1 = 1.0 / o.inverse_diagonal(T, T_old, form=1)
     assert np.allclose(d0, d1, rtol=1e-12, atol=0)
+
+
+def test_picard_forms_reduce_to_the_constant_law():
+    """The Picard operator (form 2) and its diagonal at a constant linearisation point
+    T = c equal the constant-conductivity operator with k = k0 + k1 c."""
+    import numpy as np
+    from oracle import oracle as O
+    o = O.Oracle(3, (3, 2, 3), perturb=0.2, seed=3)
+    o.set_material(O.material(O.LAW_LINEAR_K, k=1.0, k1=0.5), 1e-3)
+    c = O.Oracle(3, (3, 2, 3), perturb=0.2, seed=3)
+    c.set_material(O.material(O.LAW_CONSTANT, k=1.4), 1e-3)
+    rng = np.random.default_rng(0)
+    src = rng.uniform(-1, 1, o.n_dofs)
+    T = np.full(o.n_dofs, 0.8)
+    a, b = o.vmult(src, T, T, form=2), c.vmult(src)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+    da, db = o.inverse_diagonal(T, T, form=2), c.inverse_diagonal()
+    assert np.abs(da - db).max() <= 1e-13 * np.abs(db).max()
+    # away from a constant point the Picard diagonal differs from the tangent's
+    T2 = rng.uniform(0.0, 1.0, o.n_dofs)
+    assert np.abs(o.inverse_diagonal(T2, T2, form=2) - o.inverse_diagonal(T2, T2)).max() > 0

@@ -137,6 +137,7 @@ struct mpdg_heat {
   std::vector<MGLevel> mg;
   float *mg_t1 = nullptr, *mg_t2 = nullptr;
   int mg_min_cells = -1;
+  bool x_zero = false;  // the next solve starts from x = 0 (its A x is skipped)
 };
 
 static cudaEvent_t take_event(mpdg_heat *h)
@@ -1213,7 +1214,8 @@ static int cg_jacobi(mpdg_heat *h, const mpdg_solver_params *prm, double *x, con
   TRY(ensure_workspace(h));
   const int g = vgrid(h, N);
   CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
-  TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+  if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+  h->x_zero = false;
   k_cg_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->pv, h->Ap, D, h->st, h->partials, h->counter,
                                       prm->rel_tolerance, prm->abs_tolerance,
                                       prm->tol_reference_norm, prm->max_iterations, record); ++h->launches;
@@ -1692,7 +1694,8 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   double res0 = -1.0, true_res = 0.0;
   for (;;) {
     CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
-    TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+    if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+    h->x_zero = false;
     k_cgm_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->Ap, h->r32, h->x32, h->d32, h->Ax32,
                                         h->inv_diag_f, inv_theta, h->st, h->partials, h->counter,
                                         prm->rel_tolerance, prm->abs_tolerance,
@@ -1805,7 +1808,8 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
   };
   for (;;) {
     CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
-    TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+    if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+    h->x_zero = false;
     k_residual<<<g, VT, 0, h->stream>>>(N, b, h->Ap, V);
     ++h->launches;
     double rr = 0.0;
@@ -2515,7 +2519,10 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
       cudaMemsetAsync(h->w1, 0, vb, h->stream);
       mpdg_solve_stats ls;
       memset(&ls, 0, sizeof(ls));
-      if ((rc = linear_solve(h, &lp, h->w1, h->w2, &ls)) != MPDG_OK) break;
+      h->x_zero = true;
+      rc = linear_solve(h, &lp, h->w1, h->w2, &ls);
+      h->x_zero = false;
+      if (rc != MPDG_OK) break;
       k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1); ++h->launches;
       if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
       s.linear_iterations = ls.iterations;
@@ -2529,7 +2536,10 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
         cudaMemsetAsync(h->w1, 0, vb, h->stream);
         mpdg_solve_stats ls;
         memset(&ls, 0, sizeof(ls));
-        if ((rc = linear_solve(h, &prm->linear, h->w1, h->w2, &ls)) != MPDG_OK) break;
+        h->x_zero = true;
+        rc = linear_solve(h, &prm->linear, h->w1, h->w2, &ls);
+        h->x_zero = false;
+        if (rc != MPDG_OK) break;
         s.linear_iterations += ls.iterations;
         double rr = 0.0, dd = 0.0;
         if ((rc = norms(h, h->w2, nullptr, &rr, nullptr)) != MPDG_OK) break;

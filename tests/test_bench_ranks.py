@@ -1,0 +1,60 @@
+"""The benchmark's multi-rank path on CPU: two gloo ranks agree on the slowest
+rank's time, the whole-job throughput counts every replica, and the reference arm
+runs on rank 0 only (the other ranks exit without work)."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank(rank, world, port, values, out):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        out[rank] = bench.max_over_ranks(values[rank], "cpu", world)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_take_the_slowest_time():
+    world = 2
+    values = [3.25, 7.5]
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_rank, args=(world, _free_port(), values, out), nprocs=world,
+                           join=True, start_method="spawn")
+        assert dict(out) == {0: 7.5, 1: 7.5}
+
+
+def test_single_rank_and_throughput():
+    assert bench.max_over_ranks(4.0, "cpu", 1) == 4.0
+    # two replicas of 1000 DoFs, 5 steps in 10 ms: 1e6 DoF/s
+    assert bench.replica_throughput(2, 1000, 5, 10.0) == pytest.approx(1e6)
+
+
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
+    monkeypatch.setenv("RANK", "1")
+
+    class Args:
+        cpu_cells, warmup, steps, gpus = 8, 3, 1, 2
+    assert bench.run_reference(Args()) == 0
+    assert capsys.readouterr().out == ""

@@ -57,6 +57,32 @@ def test_single_linearization_step_matches_oracle(precond):
     assert st.linear_iterations > 0
 
 
+def test_cpu_correctness_case_matches_oracle():
+    """The small CPU-runnable case: FE_Q(2) on 16^3 cells (35,937 DoFs), k = rho cp = 1,
+    dt = 1e-3, Dirichlet 0 on all faces, T0 ~ U[0, 1] (seeded; constrained DoFs set to
+    0), nodally interpolated source exp(-|x - c|^2 / 0.1^2) at c = (0.5, 0.5, 0.9), one
+    Jacobi-CG solve to 1e-10 relative, against the oracle's step."""
+    deg, cells, dt = 2, (16, 16, 16), 1e-3
+    o = O.Oracle(deg, cells)
+    o.set_material(O.material(O.LAW_CONSTANT, k=1.0), dt)
+    q = o.gaussian_source(1.0, (0.5, 0.5, 0.9), 0.1)
+    T0 = o.distribute(np.random.default_rng(1).uniform(0, 1, o.n_dofs))
+    r = o.create_rhs(T0, T0, q)
+    d, _, _ = o.cg(r, T_lin=T0, T_old=T0, rel_tol=1e-13)
+    T_ref = T0 + d
+    op = H.HeatDiffuseOperator(H.box_mesh(deg, cells))
+    op.set_material(H.material(law=0, k=1.0))
+    opn = H.HeatDiffuseOperation(op, H.LinearSolverData(rel_tolerance=1e-10),
+                                 predictor=L.PREDICTOR_NONE, single_linearization=True)
+    opn.set_initial_condition(torch.tensor(T0, device="cuda"))
+    opn.heat_source = torch.tensor(q, device="cuda")
+    st = opn.solve(dt)
+    T = opn.T.cpu().numpy()
+    assert op.n_dofs == 35937
+    assert np.abs(T - T_ref).max() <= 1e-7 * np.abs(T_ref).max()
+    assert 0 < st.linear_iterations < 200
+
+
 # applications/mp-heat-transfer/cases/solidification_slab/tests/solidification_slab.mpirun=1.output
 SLAB = [2.82611e+02, 2.82458e+02, 2.82345e+02, 2.82252e+02, 2.82169e+02]
 

@@ -107,6 +107,9 @@ typedef struct {
   int    mg_coarse_degree;    /* multigrid: Chebyshev steps on the coarsest level    */
   double mg_smoothing_range;  /* multigrid: smoothing interval [upper / range, upper] */
   int    mg_min_cells;        /* multigrid: coarsen while every cell count / 2 >= this */
+  int    mg_fine_pre_steps;   /* multigrid, finest level: pre-smoothing steps (< 0: as above) */
+  int    mg_fine_post_steps;  /* multigrid, finest level: post-smoothing steps after the
+                                 restart step (< 0: as mg_smoothing_degree)             */
 } mpdg_solver_params;
 
 typedef struct {

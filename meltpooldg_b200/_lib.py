@@ -52,7 +52,8 @@ class SolverParams(C.Structure):
                 ("cheb_min_fraction", C.c_double), ("tol_reference_norm", C.c_double),
                 ("cheb_picard", C.c_int), ("cheb_eig_reuse", C.c_int),
                 ("mg_smoothing_degree", C.c_int), ("mg_coarse_degree", C.c_int),
-                ("mg_smoothing_range", C.c_double), ("mg_min_cells", C.c_int)]
+                ("mg_smoothing_range", C.c_double), ("mg_min_cells", C.c_int),
+                ("mg_fine_pre_steps", C.c_int), ("mg_fine_post_steps", C.c_int)]
 
 
 class SolveStats(C.Structure):

@@ -72,7 +72,8 @@ struct MGLevel {
   float *b = nullptr, *x = nullptr, *d = nullptr, *Ax = nullptr;
   double *Tl = nullptr, *To = nullptr;  // injected linearisation point (levels > 0)
   double theta = 1.0, delta = 1.0;      // smoothing interval (centre, half width)
-  int steps = 0;                        // Chebyshev steps (pre = post = steps; coarsest: all)
+  int pre = 0, post = 0;                // Chebyshev steps before / after the coarse correction
+                                        // (post: after the restart step; coarsest: pre only)
   std::vector<float> c1, c2;
 };
 
@@ -1523,14 +1524,19 @@ static int mg_setup(mpdg_heat *h, const mpdg_solver_params *prm, bool picard)
     }
     const double upper = prm->cheb_max_factor * c->eig_max;
     double lower = upper / std::max(1.5, prm->mg_smoothing_range);
-    v.steps = s;
+    v.pre = v.post = s;
+    if (l == 0) {
+      if (prm->mg_fine_pre_steps >= 0) v.pre = prm->mg_fine_pre_steps;
+      if (prm->mg_fine_post_steps >= 0) v.post = prm->mg_fine_post_steps;
+    }
     if (l == L - 1) {
       lower = std::min(lower, std::max(c->eig_min, 1e-6 * upper));
-      v.steps = std::max(1, prm->mg_coarse_degree);
+      v.pre = std::max(1, prm->mg_coarse_degree);
+      v.post = 0;
     }
     v.theta = 0.5 * (upper + lower);
     v.delta = 0.5 * (upper - lower);
-    cheb_coefficients(v.theta, v.delta, v.steps, v.c1, v.c2);
+    cheb_coefficients(v.theta, v.delta, std::max(v.pre, v.post), v.c1, v.c2);
   }
   return MPDG_OK;
 }
@@ -1602,7 +1608,7 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
                                            st);
       ++h->launches;
     }
-    for (int j = 1; j <= v.steps; ++j) {
+    for (int j = 1; j <= v.pre; ++j) {
       TRY(op_apply_f(c, v.Ax, v.x, st, picard));
       k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, v.c1[j],
                                            v.c2[j], st);
@@ -1621,11 +1627,11 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
     const int g = vgrid(c, N);
     TRY(mg_prolong_add(h, l, h->mg[l + 1].x, v.x, v.Ax));
     // post-smoothing: the Chebyshev recurrence restarted from the corrected iterate
-    for (int j = 0; j <= v.steps; ++j) {
+    for (int j = 0; j <= v.post; ++j) {
       TRY(op_apply_f(c, v.Ax, v.x, st, picard));
       const float c1 = j == 0 ? 0.f : v.c1[j];
       const float c2 = j == 0 ? (float)(1.0 / v.theta) : v.c2[j];
-      if (l == 0 && j == v.steps) {
+      if (l == 0 && j == v.post) {
         k_cheb_last<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, h->r,
                                              h->Ap, h->z, st, h->partials, h->counter);
       } else {
@@ -1927,6 +1933,8 @@ extern "C" void mpdg_solver_params_default(mpdg_solver_params *p)
   p->mg_coarse_degree = 8;
   p->mg_smoothing_range = 8.0;
   p->mg_min_cells = 4;
+  p->mg_fine_pre_steps = -1;
+  p->mg_fine_post_steps = -1;
 }
 
 extern "C" void mpdg_step_params_default(mpdg_step_params *p)

@@ -137,6 +137,8 @@ class LinearSolverData:
     mg_coarse_degree: int = 8
     mg_smoothing_range: float = 8.0
     mg_min_cells: int = 4
+    mg_fine_pre_steps: int = -1
+    mg_fine_post_steps: int = -1
 
     def to_c(self) -> L.SolverParams:
         return L.SolverParams(self.solver_type, self.preconditioner_type, self.max_iterations,
@@ -145,7 +147,8 @@ class LinearSolverData:
                               self.cheb_min_fraction, self.tol_reference_norm,
                               int(self.cheb_picard), int(self.cheb_eig_reuse),
                               self.mg_smoothing_degree, self.mg_coarse_degree,
-                              self.mg_smoothing_range, self.mg_min_cells)
+                              self.mg_smoothing_range, self.mg_min_cells,
+                              self.mg_fine_pre_steps, self.mg_fine_post_steps)
 
 
 @dataclass

@@ -203,6 +203,31 @@ int mpdg_heat_support_points(mpdg_heat *h, double *xyz);
 int mpdg_heat_gaussian_source(mpdg_heat *h, double *q, double amplitude, const double center[3],
                               double radius);
 
+/* Volumetric laser heat source: LaserHeatSourceVolumetric::compute_volumetric_heat_source
+ * (laser_heat_source_volumetric.cpp:20-58) with the intensity profiles of
+ * laser_intensity_profiles.hpp, q[i] = I(x_i) at the DoF support points:
+ *   UNIFORM           I = power                                          (:62-90)
+ *   GAUSS_VOLUMETRIC  I = power / (r sqrt(pi/2))^3 exp(-2 |x - c|^2 / r^2) (:175-235)
+ *   GAUSS_PROJECTION  I = power / (r^2 pi/2) exp(-2 d^2 / r^2), d = distance of x to
+ *                     the beam line through c along the unit direction   (:36-60, :98-170)
+ *   GUSAROV           powder-layer absorption, reflectivity rho, extinction beta, layer
+ *                     thickness L                                        (:243-340)
+ * A zero or negative radius (Gauss, Gusarov) or a non-unit direction (projection) is
+ * MPDG_ERR_INVALID_ARGUMENT. */
+enum { MPDG_LASER_UNIFORM = 0, MPDG_LASER_GAUSS_VOLUMETRIC = 1, MPDG_LASER_GAUSS_PROJECTION = 2,
+       MPDG_LASER_GUSAROV = 3 };
+typedef struct {
+  int    profile;                 /* MPDG_LASER_*                                        */
+  double power;                   /* current power (LaserOperation::get_laser_power)     */
+  double position[3];             /* beam centre (LaserOperation::get_laser_position)    */
+  double direction[3];            /* unit beam direction (Gauss projection)              */
+  double radius;                  /* beam radius                                         */
+  double reflectivity;            /* Gusarov: rho                                        */
+  double extinction_coefficient;  /* Gusarov: beta                                       */
+  double layer_thickness;         /* Gusarov: L                                          */
+} mpdg_laser;
+int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser *laser);
+
 /* ---- preconditioner + linear solver ---------------------------------- */
 /* JacobiPreconditioner::update (preconditioner_jacobi.hpp:65-69): stores the inverse
  * diagonal at the current linearisation point inside the handle. */

@@ -74,6 +74,16 @@ class StepStats(C.Structure):
                 ("step_ms", C.c_double)]
 
 
+LASER_UNIFORM, LASER_GAUSS_VOLUMETRIC, LASER_GAUSS_PROJECTION, LASER_GUSAROV = 0, 1, 2, 3
+
+
+class Laser(C.Structure):
+    _fields_ = [("profile", C.c_int), ("power", C.c_double), ("position", C.c_double * 3),
+                ("direction", C.c_double * 3), ("radius", C.c_double),
+                ("reflectivity", C.c_double), ("extinction_coefficient", C.c_double),
+                ("layer_thickness", C.c_double)]
+
+
 class Counters(C.Structure):
     _fields_ = [("launches", C.c_int64), ("vmult64_calls", C.c_int64),
                 ("vmult32_calls", C.c_int64), ("vmult64_ms", C.c_double),
@@ -108,6 +118,7 @@ _SIGS = {
     "mpdg_heat_l2_norm": (C.c_int, [_H, _D, C.POINTER(C.c_double)]),
     "mpdg_heat_l2_norm_noalloc": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_support_points": (C.c_int, [_H, _D]),
+    "mpdg_heat_laser_source": (C.c_int, [_H, _D, C.POINTER(Laser)]),
     "mpdg_heat_gaussian_source": (C.c_int, [_H, _D, C.c_double, C.POINTER(C.c_double),
                                             C.c_double]),
     "mpdg_heat_preconditioner_update": (C.c_int, [_H]),

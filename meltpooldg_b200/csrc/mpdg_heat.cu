@@ -344,6 +344,58 @@ __global__ void k_gaussian(int64_t N, PosArgs a, double *q, double amp, double c
   }
 }
 
+// volumetric laser intensity at x (laser_intensity_profiles.hpp), parameters precomputed
+// on the host
+struct LaserArgs {
+  int profile;
+  double power, c[3], dir[3], radius, peak;
+  double rho, beta, L, lambda, a, D;  // Gusarov
+};
+__device__ __forceinline__ double gusarov_dq_dxi(const LaserArgs &g, double xi)
+{
+  const double rho = g.rho, a = g.a, lambda = g.lambda;
+  if (!(xi < lambda)) return 0.0;
+  return (3 - 3 * rho) * (exp(-xi) + rho * exp(xi - 2 * lambda)) / (4 * rho - 3) +
+         2 * a * a * rho / (g.D * (4 * rho - 3)) *
+           (exp(-lambda) * (1 - rho * rho) * (exp(-2 * a * xi) * (a - 1) + exp(2 * a * xi) * (a + 1)) -
+            (rho * exp(-2 * lambda) + 3) * (exp(2 * a * (xi - lambda)) * (1 - a - rho * (a + 1)) -
+                                            exp(2 * a * (lambda - xi)) * (a + rho * (a - 1) + 1)));
+}
+__device__ __forceinline__ double laser_intensity(const LaserArgs &g, const double x[3])
+{
+  const double v0 = x[0] - g.c[0], v1 = x[1] - g.c[1], v2 = x[2] - g.c[2];
+  if (g.profile == MPDG_LASER_UNIFORM) return g.power;
+  if (g.profile == MPDG_LASER_GAUSS_VOLUMETRIC) {
+    const double s2 = (v0 * v0 + v1 * v1 + v2 * v2) / (g.radius * g.radius);
+    return g.peak * exp(-2.0 * s2);
+  }
+  if (g.profile == MPDG_LASER_GAUSS_PROJECTION) {
+    const double w0 = v1 * g.dir[2] - v2 * g.dir[1], w1 = v2 * g.dir[0] - v0 * g.dir[2],
+                 w2 = v0 * g.dir[1] - v1 * g.dir[0];
+    const double s2 = (w0 * w0 + w1 * w1 + w2 * w2) / (g.radius * g.radius);
+    return g.peak * exp(-2.0 * s2);
+  }
+  // Gusarov: z measured downwards from the beam centre; zero outside the layer
+  const double dist = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+  const double z = -(x[2] - g.c[2]);
+  if (z >= g.L || z < g.c[2]) return 0.0;
+  double pd = 0.0;
+  if (dist <= g.radius) {
+    const double m = 1.0 - dist / g.radius, p = 1.0 + dist / g.radius;
+    pd = 3.0 * g.power / (M_PI * g.radius * g.radius) * (m * m) * (p * p);
+  }
+  return -g.beta * pd * gusarov_dq_dxi(g, z * g.beta);
+}
+__global__ void k_laser(int64_t N, PosArgs a, LaserArgs g, double *q)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double x[3];
+    dof_position(a, i, x);
+    q[i] = laser_intensity(g, x);
+  }
+}
+
 // set Dirichlet values face by face; a DoF on several faces takes the value of
 // the first constrained face in the order x-, x+, y-, y+, z-, z+
 struct DirArgs {
@@ -2370,6 +2422,49 @@ extern "C" int mpdg_heat_support_points(mpdg_heat *h, double *xyz)
   if (!h || !xyz) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   CU(cudaSetDevice(h->device));
   k_support_points<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), xyz); ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser *laser)
+{
+  if (!h || !q || !laser) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  const int pr = laser->profile;
+  if (pr < MPDG_LASER_UNIFORM || pr > MPDG_LASER_GUSAROV)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown laser intensity profile");
+  LaserArgs g;
+  memset(&g, 0, sizeof(g));
+  g.profile = pr;
+  g.power = laser->power;
+  for (int e = 0; e < 3; ++e) {
+    g.c[e] = laser->position[e];
+    g.dir[e] = laser->direction[e];
+  }
+  g.radius = laser->radius;
+  if (pr != MPDG_LASER_UNIFORM && !(g.radius > 0.0))
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "The laser beam radius must be greater than zero! Abort..");
+  const double half_pi = 0.5 * M_PI;
+  if (pr == MPDG_LASER_GAUSS_VOLUMETRIC) {
+    const double s = g.radius * std::sqrt(half_pi);
+    g.peak = g.power / (s * s * s);
+  } else if (pr == MPDG_LASER_GAUSS_PROJECTION) {
+    const double nrm = std::sqrt(g.dir[0] * g.dir[0] + g.dir[1] * g.dir[1] + g.dir[2] * g.dir[2]);
+    if (!(std::fabs(nrm - 1.0) < 1e-8))
+      return fail(MPDG_ERR_INVALID_ARGUMENT, "The line direction must be a unit vector");
+    g.peak = g.power / (g.radius * g.radius * half_pi);
+  } else if (pr == MPDG_LASER_GUSAROV) {
+    g.rho = laser->reflectivity;
+    g.beta = laser->extinction_coefficient;
+    g.L = laser->layer_thickness;
+    g.lambda = g.beta * g.L;
+    g.a = std::sqrt(1.0 - g.rho);
+    g.D = (1.0 - g.a) * (1.0 - g.a - g.rho * (1.0 + g.a)) * std::exp(-2.0 * g.a * g.lambda) -
+          (1.0 + g.a) * (1.0 + g.a - g.rho * (1.0 - g.a)) * std::exp(2.0 * g.a * g.lambda);
+  }
+  CU(cudaSetDevice(h->device));
+  k_laser<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), g, q);
+  ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;
 }

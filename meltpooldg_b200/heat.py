@@ -288,6 +288,17 @@ class HeatDiffuseOperator:
         check(self._L.mpdg_heat_support_points(self.h, x.data_ptr()))
         return x
 
+    def laser_source(self, q, profile, power, position, radius=1.0, direction=(0.0, 0.0, -1.0),
+                     gusarov=(0.0, 0.0, 0.0)):
+        """LaserHeatSourceVolumetric::compute_volumetric_heat_source: q = I(x) at the
+        support points for profile L.LASER_UNIFORM / _GAUSS_VOLUMETRIC / _GAUSS_PROJECTION /
+        _GUSAROV (gusarov = (reflectivity, extinction coefficient, layer thickness))."""
+        las = L.Laser(int(profile), float(power), (C.c_double * 3)(*map(float, position)),
+                      (C.c_double * 3)(*map(float, direction)), float(radius),
+                      *[float(v) for v in gusarov])
+        check(self._L.mpdg_heat_laser_source(self.h, _ptr(q), C.byref(las)))
+        return q
+
     def gaussian_source(self, q, amplitude, center, radius):
         c = (C.c_double * 3)(*[float(v) for v in center])
         check(self._L.mpdg_heat_gaussian_source(self.h, _ptr(q), float(amplitude), c,

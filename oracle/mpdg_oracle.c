@@ -1087,6 +1087,68 @@ void orc_gaussian_source(const orc_heat *h, double *q, double amp, const double 
   free(xyz);
 }
 
+/* Volumetric laser intensity profiles at the support points, following
+ * include/meltpooldg/heat/laser_intensity_profiles.hpp: UniformIntensityProfile (:62-90),
+ * GaussVolumetricIntensityProfile (:175-235), GaussProjectionIntensityProfile with
+ * compute_distance_to_line (:36-60, :98-170) and GusarovIntensityProfile (:243-340), as
+ * LaserHeatSourceVolumetric::compute_volumetric_heat_source evaluates them
+ * (source/heat/laser_heat_source_volumetric.cpp:20-58). */
+static double orc_gusarov_dq_dxi(double rho, double lambda, double a, double D, double xi)
+{
+  if (!(xi < lambda)) return 0.0;
+  const double t1 = (3.0 - 3.0 * rho) * (exp(-xi) + rho * exp(xi - 2.0 * lambda)) / (4.0 * rho - 3.0);
+  const double br = exp(-lambda) * (1.0 - rho * rho) *
+                      (exp(-2.0 * a * xi) * (a - 1.0) + exp(2.0 * a * xi) * (a + 1.0)) -
+                    (rho * exp(-2.0 * lambda) + 3.0) *
+                      (exp(2.0 * a * (xi - lambda)) * (1.0 - a - rho * (a + 1.0)) -
+                       exp(2.0 * a * (lambda - xi)) * (a + rho * (a - 1.0) + 1.0));
+  return t1 + 2.0 * a * a * rho / (D * (4.0 * rho - 3.0)) * br;
+}
+
+void orc_laser_source(const orc_heat *h, double *q, int profile, double power, const double c[3],
+                      const double dir[3], double radius, double rho, double beta, double L)
+{
+  double *xyz = (double *)malloc(sizeof(double) * 3 * h->n_dofs);
+  orc_support_points(h, xyz);
+  const double pi = 3.14159265358979323846;
+  const double sq = radius * sqrt(pi / 2.0);
+  const double peak_vol = power / (sq * sq * sq);
+  const double peak_proj = power / (radius * radius * (pi / 2.0));
+  const double lambda = beta * L, a = sqrt(1.0 - rho);
+  const double D = (1.0 - a) * (1.0 - a - rho * (1.0 + a)) * exp(-2.0 * a * lambda) -
+                   (1.0 + a) * (1.0 + a - rho * (1.0 - a)) * exp(2.0 * a * lambda);
+#pragma omp parallel for num_threads(nthreads())
+  for (int64_t i = 0; i < h->n_dofs; ++i) {
+    const double *x = xyz + 3 * i;
+    const double v[3] = {x[0] - c[0], x[1] - c[1], x[2] - c[2]};
+    double val = 0.0;
+    if (profile == 0) {
+      val = power;
+    } else if (profile == 1) {
+      const double s = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / radius;
+      val = peak_vol * exp(-2.0 * s * s);
+    } else if (profile == 2) {
+      const double w[3] = {v[1] * dir[2] - v[2] * dir[1], v[2] * dir[0] - v[0] * dir[2],
+                           v[0] * dir[1] - v[1] * dir[0]};
+      const double s = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]) / radius;
+      val = peak_proj * exp(-2.0 * s * s);
+    } else {
+      const double dist = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      const double z = -(x[2] - c[2]);
+      if (z >= L || z < c[2]) {
+        val = 0.0;
+      } else {
+        const double pd = dist <= radius ? 3.0 * power / (pi * radius * radius) *
+                                             pow(1.0 - dist / radius, 2) * pow(1.0 + dist / radius, 2)
+                                         : 0.0;
+        val = -beta * pd * orc_gusarov_dq_dxi(rho, lambda, a, D, z * beta);
+      }
+    }
+    q[i] = val;
+  }
+  free(xyz);
+}
+
 /* ------------------------------------------------------------------ */
 /* vector helpers and solvers                                          */
 /* ------------------------------------------------------------------ */

@@ -128,6 +128,8 @@ def lib():
             L.orc_set_boundary.argtypes = [_P, C.c_int, C.c_int, C.c_double, C.c_double,
                                            C.c_double, C.c_double, C.c_double]
             L.orc_gaussian_source.argtypes = [_P, _D, C.c_double, _D, C.c_double]
+            L.orc_laser_source.argtypes = [_P, _D, C.c_int, C.c_double, _D, _D, C.c_double,
+                                           C.c_double, C.c_double, C.c_double]
             _lib = L
     return _lib
 
@@ -303,6 +305,17 @@ class Oracle:
         rc = self.L.orc_time_step_newton(self.h, _ptr(T_cur), _ptr(T_old), _ptr(q), dt, dt_old,
                                          predictor, 1 if solver == "gmres" else 0, C.byref(lin), C.byref(nl), C.byref(st))
         return rc, st
+
+    def laser_source(self, profile, power, position, radius=1.0, direction=(0.0, 0.0, -1.0),
+                     gusarov=(0.0, 0.0, 0.0)):
+        """Volumetric laser intensity at the support points (profile 0 uniform, 1 Gauss
+        volumetric, 2 Gauss projection, 3 Gusarov with (reflectivity, extinction, layer))."""
+        q = np.empty(self.n_dofs)
+        c = np.ascontiguousarray(position, dtype=np.float64)
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        self.L.orc_laser_source(self.h, _ptr(q), int(profile), float(power), _ptr(c), _ptr(d),
+                                float(radius), *[float(v) for v in gusarov])
+        return q
 
     def gaussian_source(self, amp, center, radius):
         q = self._z()

@@ -99,3 +99,35 @@ def test_picard_forms_reduce_to_the_constant_law():
     # away from a constant point the Picard diagonal differs from the tangent's
     T2 = rng.uniform(0.0, 1.0, o.n_dofs)
     assert np.abs(o.inverse_diagonal(T2, T2, form=2) - o.inverse_diagonal(T2, T2)).max() > 0
+
+
+def test_laser_profiles_follow_their_formulas():
+    """Volumetric laser intensity at the support points: the uniform profile is the power,
+    the Gauss profiles peak at power / (r sqrt(pi/2))^3 (volumetric) and power / (r^2 pi/2)
+    (projection, constant along the beam), the Gusarov profile vanishes outside the layer."""
+    import math
+
+    import numpy as np
+    from oracle import oracle as O
+    o = O.Oracle(2, (4, 4, 4), perturb=0.1, seed=1)
+    x = o.support_points()
+    P, r, c = 30.0, 0.3, np.array([0.5, 0.5, 1.0])
+    assert np.all(o.laser_source(0, P, c) == P)
+    qv = o.laser_source(1, P, c, radius=r)
+    d2 = ((x - c) ** 2).sum(1)
+    ref = P / (r * math.sqrt(math.pi / 2)) ** 3 * np.exp(-2 * d2 / r ** 2)
+    assert np.abs(qv - ref).max() <= 1e-13 * ref.max()
+    qp = o.laser_source(2, P, c, radius=r, direction=(0.0, 0.0, -1.0))
+    dl2 = ((x[:, :2] - c[:2]) ** 2).sum(1)
+    ref = P / (r * r * math.pi / 2) * np.exp(-2 * dl2 / r ** 2)
+    assert np.abs(qp - ref).max() <= 1e-13 * ref.max()
+    # Gusarov: powder surface z = 0 with the material below (the reference's convention;
+    # its "z < position_z" compares the depth with the centre height), layer L = 0.5
+    b = O.Oracle(2, (4, 4, 4), lo=(0, 0, -1), hi=(1, 1, 0), perturb=0.1, seed=1)
+    xb = b.support_points()
+    g = b.laser_source(3, P, (0.5, 0.5, 0.0), radius=0.6, gusarov=(0.6, 20.0, 0.5))
+    depth = -xb[:, 2]
+    dist = np.sqrt(((xb - np.array([0.5, 0.5, 0.0])) ** 2).sum(1))
+    outside = (depth >= 0.5) | (depth < 0.0) | (dist > 0.6)
+    assert np.all(g[outside] == 0.0) and np.all(np.isfinite(g))
+    assert np.abs(g[~outside]).max() > 0.0

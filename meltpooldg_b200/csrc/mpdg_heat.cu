@@ -139,6 +139,12 @@ struct mpdg_heat {
   float *mg_t1 = nullptr, *mg_t2 = nullptr;
   int mg_min_cells = -1;
   bool x_zero = false;  // the next solve starts from x = 0 (its A x is skipped)
+  // host-buffer time step: a copy stream for the transfers that overlap the step, and the
+  // events the step records / waits on (null outside mpdg_heat_time_step_host)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_source = nullptr, ev_commit = nullptr, ev_inputs = nullptr;
+  bool wait_source = false, record_commit = false;
+  double *told_host = nullptr;  // host destination of the committed T_old (copy stream)
 };
 
 static cudaEvent_t take_event(mpdg_heat *h)
@@ -2004,6 +2010,14 @@ extern "C" void mpdg_step_params_default(mpdg_step_params *p)
 static void release(mpdg_heat *h)
 {
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->copy_stream) {
+    cudaStreamSynchronize(h->copy_stream);
+    cudaStreamDestroy(h->copy_stream);
+    cudaEventDestroy(h->ev_source);
+    cudaEventDestroy(h->ev_commit);
+    cudaEventDestroy(h->ev_inputs);
+    h->copy_stream = nullptr;
+  }
   for (MGLevel &lv : h->mg)
     if (lv.own && lv.h) {
       release(lv.h);
@@ -2590,6 +2604,12 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     }
     cudaMemcpyAsync(T_old, T_cur, vb, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(T_cur, h->w1, vb, cudaMemcpyDeviceToDevice, h->stream);
+    if (h->record_commit) {
+      // T_old is final here: its copy to the host runs on the copy stream during the step
+      cudaEventRecord(h->ev_commit, h->stream);
+      cudaStreamWaitEvent(h->copy_stream, h->ev_commit, 0);
+      cudaMemcpyAsync(h->told_host, T_old, vb, cudaMemcpyDeviceToHost, h->copy_stream);
+    }
     if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
     h->T_lin = T_cur;
     h->T_old = T_old;
@@ -2610,10 +2630,12 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     }
     if (prm->single_linearization) {
       // b = J T_g - R(T_g); solve J delta = -R(T_g) to |b - J T| <= tol |b|
-      cudaMemsetAsync(h->w2, 0, vb, h->stream);
-      if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
+      // J T_g first: it does not need the source, whose upload may still be running
       cudaMemsetAsync(h->z, 0, vb, h->stream);
       if ((rc = op_apply_d(h, h->z, T_cur, FIN_NONE, nullptr, nullptr)) != MPDG_OK) break;
+      cudaMemsetAsync(h->w2, 0, vb, h->stream);
+      if (h->wait_source) cudaStreamWaitEvent(h->stream, h->ev_source, 0);
+      if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
       double rr = 0.0, bb = 0.0;
       if ((rc = norms(h, h->w2, h->z, &rr, &bb)) != MPDG_OK) break;
       mpdg_solver_params lp = prm->linear;
@@ -2635,6 +2657,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     } else {
       for (int i = 0; i < prm->newton_max_iterations; ++i) {
         cudaMemsetAsync(h->w2, 0, vb, h->stream);
+        if (h->wait_source) cudaStreamWaitEvent(h->stream, h->ev_source, 0);
         if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
         cudaMemsetAsync(h->w1, 0, vb, h->stream);
         mpdg_solve_stats ls;
@@ -2687,13 +2710,38 @@ extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *pr
   TRY(dvec(h, &h->host_T, N));
   TRY(dvec(h, &h->host_To, N));
   if (heat_source) TRY(dvec(h, &h->host_q, N));
+  if (!h->copy_stream) {
+    CU(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&h->ev_source, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&h->ev_commit, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&h->ev_inputs, cudaEventDisableTiming));
+  }
+  // T and T_old are needed first (predictor, history commit); the source only by
+  // create_rhs, so its copy runs on the copy stream while the step starts
   CU(cudaMemcpyAsync(h->host_T, T_cur, vb, cudaMemcpyHostToDevice, h->stream));
   CU(cudaMemcpyAsync(h->host_To, T_old, vb, cudaMemcpyHostToDevice, h->stream));
-  if (heat_source) CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->stream));
-  TRY(mpdg_heat_time_step(h, prm, dt, dt_old, h->host_T, h->host_To, heat_source ? h->host_q : nullptr,
-                          stats));
+  CU(cudaEventRecord(h->ev_inputs, h->stream));
+  if (heat_source) {
+    CU(cudaStreamWaitEvent(h->copy_stream, h->ev_inputs, 0));  // one transfer at a time
+    CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->copy_stream));
+    CU(cudaEventRecord(h->ev_source, h->copy_stream));
+  }
+  // the new T_old (= the input T) is final once the step has committed the history: the
+  // step starts its copy back then, so it runs while the solve computes; T follows at the end
+  h->wait_source = heat_source != nullptr;
+  h->record_commit = true;
+  h->told_host = T_old;
+  const int rc = mpdg_heat_time_step(h, prm, dt, dt_old, h->host_T, h->host_To,
+                                     heat_source ? h->host_q : nullptr, stats);
+  h->wait_source = false;
+  h->record_commit = false;
+  h->told_host = nullptr;
+  if (rc != MPDG_OK) {
+    cudaStreamSynchronize(h->copy_stream);
+    return rc;
+  }
   CU(cudaMemcpyAsync(T_cur, h->host_T, vb, cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(T_old, h->host_To, vb, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->copy_stream));
   CU(cudaStreamSynchronize(h->stream));
   return MPDG_OK;
 }

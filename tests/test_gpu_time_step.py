@@ -146,3 +146,41 @@ def test_unidirectional_robin_on_gpu(case):
         st = opn.solve(0.01)
         assert st.converged == 1
         assert float(f"{op.l2_norm(opn.T):.5e}") == ref
+
+
+@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_MG_F32])
+def test_host_buffer_step_matches_device_step(precond):
+    """mpdg_heat_time_step_host (pinned host T, T_old and source; its copies overlap the
+    step) gives the fields of mpdg_heat_time_step on device vectors, two steps in a row,
+    with the history committed on the host side as well."""
+    import ctypes as C
+    op = H.HeatDiffuseOperator(H.box_mesh(3, (8, 8, 8)))
+    op.set_material(H.material(law=L.LAW_LINEAR_K, k=1.0, k1=0.5))
+    lin = H.LinearSolverData(preconditioner_type=precond, rel_tolerance=1e-10,
+                             abs_tolerance=0.0, cheb_picard=True)
+    dev = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    N, dt = op.n_dofs, 5e-4
+    T0 = torch.rand(N, dtype=torch.float64, device="cuda", generator=torch.Generator(
+        device="cuda").manual_seed(3))
+    op.distribute_constraints(T0)
+    dev.set_initial_condition(T0.clone())
+    hT = T0.cpu().pin_memory()
+    hTo = T0.cpu().pin_memory()
+    hq = torch.empty(N, dtype=torch.float64).pin_memory()
+    q = op.new_vector()
+    dev.heat_source = q
+    for s in range(2):
+        op.gaussian_source(q, 200.0, (0.3 + 0.1 * s, 0.5, 0.9), 0.1)
+        hq.copy_(q)
+        dev.solve(dt)
+        step = L.StepStats()
+        H.check(op._L.mpdg_heat_time_step_host(op.h, C.byref(dev.params), dt,
+                                                0.0 if s == 0 else dt,
+                                                C.c_void_p(hT.data_ptr()),
+                                                C.c_void_p(hTo.data_ptr()),
+                                                C.c_void_p(hq.data_ptr()), C.byref(step)))
+        # equal up to the solver tolerance (the atomic scatter makes sums order-dependent)
+        ref, ref_old = dev.T.cpu(), dev.T_old.cpu()
+        assert (hT - ref).abs().max() <= 1e-8 * ref.abs().max()
+        assert (hTo - ref_old).abs().max() <= 1e-8 * ref_old.abs().max()
+        assert ref.abs().max() > 0.0

@@ -60,19 +60,23 @@ typedef struct {
   double   dirichlet_value[6]; /* constant Dirichlet value per face                  */
 } mpdg_mesh_desc;
 
-enum { MPDG_LAW_CONSTANT = 0, MPDG_LAW_LINEAR_K = 1, MPDG_LAW_LIQUID_SOLID = 2 };
+enum { MPDG_LAW_CONSTANT = 0, MPDG_LAW_LINEAR_K = 1, MPDG_LAW_LIQUID_SOLID = 2,
+       MPDG_LAW_GAS_LIQUID = 3 };
 
 /* Material law (Material::compute_parameters, material.templates.hpp:104-137,226-375):
  *   CONSTANT      rho*cp and k constant (material type gas / liquid)
  *   LINEAR_K      k(T) = k_l + k1*T, rho*cp constant (new law, no reference counterpart)
  *   LIQUID_SOLID  cubic smoothstep in the solid fraction between liquid and solid values,
- *                 mushy zone or sharp transition (material.templates.hpp:296-375,745-780) */
+ *                 mushy zone or sharp transition (material.templates.hpp:296-375,745-780)
+ *   GAS_LIQUID    (1 - w) gas + w liquid with w = H (smooth) or H > 0.5 (sharp), H the
+ *                 level-set heaviside field of mpdg_heat_set_fields; the *_s members hold
+ *                 the gas values (material.templates.hpp:240-295,515-524) */
 typedef struct {
   int    law;
-  int    sharp;            /* LIQUID_SOLID: 0 mushy zone, 1 sharp                    */
+  int    sharp;            /* LIQUID_SOLID: 0 mushy zone, 1 sharp; GAS_LIQUID: 0 smooth, 1 sharp */
   int    volume_specific;  /* interpolate rho*cp directly (heat_data diffuse option) */
   double rho_l, cp_l, k_l; /* liquid, or the single constant phase                   */
-  double rho_s, cp_s, k_s; /* solid                                                  */
+  double rho_s, cp_s, k_s; /* solid (GAS_LIQUID: gas)                                */
   double T_solidus, T_liquidus;
   double k1;
 } mpdg_material;
@@ -141,6 +145,19 @@ int mpdg_heat_device_bytes(const mpdg_heat *h, int64_t *bytes);
 /* Material law (Material ctor + HeatDiffuseMultiPhaseOperator ctor, do_solidification =
  * law != CONSTANT). */
 int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m);
+/* Two-phase and transport fields of HeatDiffuseMultiPhaseOperator (its level_set_as_heaviside
+ * and velocity vectors, heat_diffuse_operator.cpp:47-72): device vectors on this handle's
+ * DoFs, caller-owned, read when the per-quadrature-point coefficients are built.
+ *   heaviside  n_dofs values, weights the GAS_LIQUID law (NULL: liquid properties)
+ *   velocity   3 x n_dofs, component-major (x block, y block, z block) or NULL; adds
+ *              rho_cp v.grad(T) to the residual and rho_cp v.grad(u) to the tangent and its
+ *              diagonal (:499-500, :1038-1042); allowed with the CONSTANT and GAS_LIQUID laws
+ * The coefficients are rebuilt at the next operator call after set_fields or set_material:
+ * call set_fields again after changing the vectors' contents.  With a velocity the operator
+ * is nonsymmetric (use MPDG_SOLVER_GMRES); the multigrid preconditioner is not available
+ * with either field.  A field that was interpolated from another finite element space is
+ * passed after its interpolation to this one. */
+int mpdg_heat_set_fields(mpdg_heat *h, const double *heaviside, const double *velocity);
 /* Boundary terms on one box face (0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+), replacing the
  * heat BoundaryConditionManager's "convection" / "radiation" / "neumann" entries
  * (heat_diffuse_operator.cpp:243-269 tangent, :690-781 rhs, :1088-1129 local op):

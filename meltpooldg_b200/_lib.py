@@ -25,7 +25,7 @@ ERR_ZERO_TIME_INCREMENT = 7
 ERR_NEWTON_NOT_CONVERGED = 8
 ERR_NOT_SUPPORTED = 9
 
-LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID = 0, 1, 2
+LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID = 0, 1, 2, 3
 SOLVER_CG, SOLVER_GMRES = 0, 1
 PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_CHEBYSHEV_JACOBI_F32, PRECOND_MG_F32 = 0, 1, 2, 3
 PREDICTOR_NONE, PREDICTOR_LINEAR, PREDICTOR_GIVEN = 0, 1, 2
@@ -104,6 +104,7 @@ _SIGS = {
     "mpdg_heat_dof_dims": (C.c_int, [_H, C.POINTER(C.c_int)]),
     "mpdg_heat_device_bytes": (C.c_int, [_H, C.POINTER(C.c_int64)]),
     "mpdg_heat_set_material": (C.c_int, [_H, C.POINTER(Material)]),
+    "mpdg_heat_set_fields": (C.c_int, [_H, C.c_void_p, C.c_void_p]),
     "mpdg_heat_reset_time_increment": (C.c_int, [_H, C.c_double]),
     "mpdg_heat_set_boundary": (C.c_int, [_H, C.c_int, C.c_int, C.c_double, C.c_double,
                                          C.c_double, C.c_double, C.c_double]),

@@ -54,6 +54,9 @@ struct CellArgs {
   const T *__restrict__ To;
   const T *__restrict__ qs;
   const float *__restrict__ kq;  // per-q conductivity [cell][n^3] (coefficient-field operator)
+  // per-q coefficients of the two-phase / convective operator (LAW 4), [cell][5][n^3]:
+  // rho_cp JxW, k, and JxW rho_cp J^-1 v (three components)
+  const T *__restrict__ cf;
   double *partials;    // per-CTA partial sums
   unsigned *counter;   // last-CTA election counter (reset by the last CTA)
   SolverState *st;     // early exit when st->done; alpha finalisation

@@ -16,6 +16,12 @@
 //     (source/heat/heat_diffuse_operator.cpp:1029-1078) and rhs_cell_loop
 //     (:481-527);
 //   integrate(values|gradients): D^T sweeps accumulated, then three S^T sweeps.
+//
+// LAW selects the q-point coefficients: 0 constant, 1 k(T) = k_l + k1 T, 2 liquid-solid
+// (both with their tangent terms at T_lin), 3 a per-q FP32 conductivity field (the Picard
+// operator of the preconditioner, register-resident kernel only), 4 per-q coefficient
+// fields a.cf (gas-liquid law weighted by the level-set heaviside and/or the convective
+// term rho_cp v.grad, heat_diffuse_operator.cpp:499-500 and :1038-1042).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -47,6 +53,9 @@ template <> __device__ __forceinline__ float cw<float>(int i) { return c_w_f[i];
 // ---------------------------------------------------------------------------
 
 template <typename T> __device__ __forceinline__ void atomic_add(T *p, T v) { atomicAdd(p, v); }
+
+// laws whose coefficients depend on the linearisation point T_lin
+template <int LAW> __host__ __device__ constexpr bool law_tdep() { return LAW == 1 || LAW == 2; }
 
 // Material::compute_parameters for the three laws; LAW is a template constant.
 template <int LAW, typename T>
@@ -241,7 +250,7 @@ template <int n, typename T, int GEO, int LAW>
 __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
 {
   constexpr int n2 = n * n, n3 = n2 * n, CPB = cells_per_block(n);
-  constexpr bool TDEP = LAW != 0;
+  constexpr bool TDEP = law_tdep<LAW>();
   constexpr int NF = TDEP ? 11 : 6;
   if (a.st && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -297,9 +306,18 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
       T jxw, G[6];
       geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
       T rhocp, kk, drhocp, dk;
-      mat_eval<LAW>(a.m, TDEP ? Tq[q] : T(0), rhocp, kk, drhocp, dk);
-      T cval = a.m.idt * rhocp;
       const T uu = u[q];
+      T val;
+      if (LAW == 4) {
+        const T *cf = a.cf + cc * 5 * n3 + q;
+        kk = __ldg(cf + n3);
+        rhocp = drhocp = dk = T(0);
+        val = a.m.idt * __ldg(cf) * uu + __ldg(cf + 2 * n3) * gx[q] + __ldg(cf + 3 * n3) * gy[q] +
+              __ldg(cf + 4 * n3) * gz[q];
+      } else {
+        mat_eval<LAW>(a.m, TDEP ? Tq[q] : T(0), rhocp, kk, drhocp, dk);
+      }
+      T cval = a.m.idt * rhocp;
       T f0 = kk * gx[q], f1 = kk * gy[q], f2 = kk * gz[q];
       if (TDEP) {
         if (LAW == 2 && a.m.need_told) cval += a.m.idt * drhocp * (Tq[q] - Toq[q]);
@@ -307,7 +325,7 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
         f1 += dk * Ty[q] * uu;
         f2 += dk * Tz[q] * uu;
       }
-      u[q] = cval * uu * jxw;
+      u[q] = LAW == 4 ? val : cval * uu * jxw;
       T F0, F1, F2;
       apply_G<GEO>(G, f0, f1, f2, F0, F1, F2);
       gx[q] = F0;
@@ -399,12 +417,20 @@ __global__ void __launch_bounds__(block_threads(n)) k_rhs(CellArgs<double> a)
       const int qi = q % n, qj = (q / n) % n, qk = q / n2;
       T jxw, G[6];
       geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
-      T rhocp, kk, drhocp, dk;
-      mat_eval<LAW>(a.m, tq[q], rhocp, kk, drhocp, dk);
-      const T val = a.m.idt * rhocp * (tq[q] - Toq[q]) - Sq[q];
+      T rhocp, kk, drhocp, dk, valw;
+      if (LAW == 4) {
+        // rho_cp (T - T_old) / dt - q + rho_cp grad(T).v, times JxW
+        const T *cf = a.cf + cc * 5 * n3 + q;
+        kk = __ldg(cf + n3);
+        valw = a.m.idt * __ldg(cf) * (tq[q] - Toq[q]) - Sq[q] * jxw +
+               __ldg(cf + 2 * n3) * gx[q] + __ldg(cf + 3 * n3) * gy[q] + __ldg(cf + 4 * n3) * gz[q];
+      } else {
+        mat_eval<LAW>(a.m, tq[q], rhocp, kk, drhocp, dk);
+        valw = (a.m.idt * rhocp * (tq[q] - Toq[q]) - Sq[q]) * jxw;
+      }
       T F0, F1, F2;
       apply_G<GEO>(G, kk * gx[q], kk * gy[q], kk * gz[q], F0, F1, F2);
-      u[q] = -val * jxw;
+      u[q] = -valw;
       gx[q] = -F0;
       gy[q] = -F1;
       gz[q] = -F2;
@@ -431,7 +457,7 @@ __global__ void __launch_bounds__(block_threads(n)) k_diag(CellArgs<double> a)
 {
   using T = double;
   constexpr int n2 = n * n, n3 = n2 * n, CPB = cells_per_block(n);
-  constexpr bool TDEP = LAW != 0;
+  constexpr bool TDEP = law_tdep<LAW>();
   constexpr int NF = 16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
@@ -476,10 +502,16 @@ __global__ void __launch_bounds__(block_threads(n)) k_diag(CellArgs<double> a)
       T jxw, G[6];
       geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
       T rhocp, kk, drhocp, dk;
-      mat_eval<LAW>(a.m, TDEP ? Tq[q] : T(0), rhocp, kk, drhocp, dk);
-      T cval = a.m.idt * rhocp;
+      const T *cf = LAW == 4 ? a.cf + cc * 5 * n3 + q : nullptr;
+      if (LAW == 4) {
+        kk = __ldg(cf + n3);
+        rhocp = drhocp = dk = T(0);
+      } else {
+        mat_eval<LAW>(a.m, TDEP ? Tq[q] : T(0), rhocp, kk, drhocp, dk);
+      }
+      T cval = LAW == 4 ? T(0) : a.m.idt * rhocp;
       if (TDEP && LAW == 2 && a.m.need_told) cval += a.m.idt * drhocp * (Tq[q] - C0[q]);
-      C0[q] = cval * jxw;
+      C0[q] = LAW == 4 ? a.m.idt * __ldg(cf) : cval * jxw;
       Gxx[q] = kk * G[0];
       Gxy[q] = T(2) * kk * G[1];
       Gxz[q] = T(2) * kk * G[2];
@@ -495,6 +527,11 @@ __global__ void __launch_bounds__(block_threads(n)) k_diag(CellArgs<double> a)
         Bx[q] = dk * b0;
         By[q] = dk * b1;
         Bz[q] = dk * b2;
+      } else if (LAW == 4) {
+        // convection: phi_i (JxW rho_cp J^-1 v).grad_ref(phi_i)
+        Bx[q] = __ldg(cf + 2 * n3);
+        By[q] = __ldg(cf + 3 * n3);
+        Bz[q] = __ldg(cf + 4 * n3);
       } else {
         Bx[q] = T(0);
         By[q] = T(0);

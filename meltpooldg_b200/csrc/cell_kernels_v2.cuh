@@ -33,7 +33,7 @@ template <int n> __host__ __device__ constexpr int v2_cell_stride()
   while (s % 16 != 4) ++s;
   return s;
 }
-template <int LAW> __host__ __device__ constexpr int v2_ncoef() { return (LAW == 0 || LAW == 3) ? 0 : (LAW == 1 ? 4 : 5); }
+template <int LAW> __host__ __device__ constexpr int v2_ncoef() { return (LAW == 1) ? 4 : (LAW == 2 ? 5 : 0); }
 constexpr int kV2Warps = 2;  // warps per CTA
 template <int n, typename T, int LAW> __host__ __device__ constexpr size_t v2_smem_per_warp()
 {
@@ -245,7 +245,8 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
   constexpr int CW = v2_cells_per_warp<n>();
   constexpr int CS = v2_cell_stride<n>();
   constexpr int NCOEF = v2_ncoef<LAW>();
-  constexpr bool TDEP = LAW == 1 || LAW == 2;  // LAW 3: conductivity field k(q), no tangent
+  // LAW 3: conductivity field k(q), no tangent; LAW 4: coefficient fields a.cf
+  constexpr bool TDEP = LAW == 1 || LAW == 2;
   if (a.st && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -291,6 +292,12 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           const char *kq = reinterpret_cast<const char *>(a.kq + ncell * (n * n * n));
           for (int off = t * 128; off < n * n * n * 4; off += n * 128)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(kq + off));
+        }
+        if (LAW == 4) {
+          constexpr int bytes = 5 * n * n * n * (int)sizeof(T);
+          const char *cf = reinterpret_cast<const char *>(a.cf + ncell * 5 * (n * n * n));
+          for (int off = t * 128; off < bytes; off += n * 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(cf + off));
         }
         if (GEO == 1) {
           constexpr int npt = n * n * n;
@@ -368,7 +375,19 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
         const T uu = U[k][j];
         T kk, cval;
         T f0, f1, f2;
-        if (TDEP) {
+        T val = T(0);
+        if (LAW == 4) {
+          // rho_cp u / dt + rho_cp v.grad(u), and the flux k grad(u), from the fields
+          constexpr int npt = n * n * n;
+          const T *cf = a.cf + cc * 5 * npt + t + n * (j + n * k);
+          kk = __ldg(cf + npt);
+          val = a.m.idt * __ldg(cf) * uu + __ldg(cf + 2 * npt) * Ux[k][j] +
+                __ldg(cf + 3 * npt) * Uy[k][j] + __ldg(cf + 4 * npt) * Uz[k][j];
+          f0 = kk * Ux[k][j];
+          f1 = kk * Uy[k][j];
+          f2 = kk * Uz[k][j];
+          cval = T(0);
+        } else if (TDEP) {
           const int pt = k * n + j;
           kk = coef[(0 * n * n + pt) * 32 + lane];
           f0 = kk * Ux[k][j] + coef[(1 * n * n + pt) * 32 + lane] * uu;
@@ -387,7 +406,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
         }
         T F0, F1, F2;
         apply_G<GEO>(G, f0, f1, f2, F0, F1, F2);
-        U[k][j] = cval * uu * jxw;
+        U[k][j] = LAW == 4 ? val : cval * uu * jxw;
         Ux[k][j] = F0;
         Uy[k][j] = F1;
         Uz[k][j] = F2;

@@ -73,7 +73,7 @@ struct DegreeOps {
   template <typename T, int GEO, int LAW>
   static cudaError_t vmult_t(const CellArgs<T> &a, cudaStream_t s, int sm)
   {
-    if constexpr (std::is_same<T, float>::value && n <= 4 && LAW != 2) {
+    if constexpr (std::is_same<T, float>::value && n <= 4 && LAW != 2 && LAW != 4) {
       if (fp32_packed()) {
         static int cachep = 0;
         auto kp = k_vmult2p<n, GEO, LAW>;
@@ -97,7 +97,7 @@ struct DegreeOps {
     } else {
       static int cache = 0;
       auto k = k_vmult<n, T, GEO, LAW>;
-      const size_t smem = smem_vmult<n, T>(LAW != 0);
+      const size_t smem = smem_vmult<n, T>(law_tdep<LAW>());
       const int64_t nb = (a.n_cells + CPB - 1) / CPB;
       const int g = persistent_grid(k, THREADS, smem, nb, sm, &cache);
       k<<<g, THREADS, smem, s>>>(a);
@@ -114,6 +114,7 @@ struct DegreeOps {
         return cudaErrorNotSupported;
       }
     }
+    if (law == 4) return geo == 0 ? vmult_t<T, 0, 4>(a, s, sm) : vmult_t<T, 1, 4>(a, s, sm);
     if (geo == 0) {
       if (law == 0) return vmult_t<T, 0, 0>(a, s, sm);
       if (law == 1) return vmult_t<T, 0, 1>(a, s, sm);
@@ -155,6 +156,7 @@ struct DegreeOps {
   }
   static cudaError_t rhs(const CellArgs<double> &a, int geo, int law, cudaStream_t s, int sm)
   {
+    if (law == 4) return geo == 0 ? rhs_t<0, 4>(a, s, sm) : rhs_t<1, 4>(a, s, sm);
     if (geo == 0) {
       if (law == 0) return rhs_t<0, 0>(a, s, sm);
       if (law == 1) return rhs_t<0, 1>(a, s, sm);
@@ -177,6 +179,7 @@ struct DegreeOps {
   }
   static cudaError_t diag(const CellArgs<double> &a, int geo, int law, cudaStream_t s, int sm)
   {
+    if (law == 4) return geo == 0 ? diag_t<0, 4>(a, s, sm) : diag_t<1, 4>(a, s, sm);
     if (geo == 0) {
       if (law == 0) return diag_t<0, 0>(a, s, sm);
       if (law == 1) return diag_t<0, 1>(a, s, sm);

@@ -105,6 +105,12 @@ struct mpdg_heat {
   double eig_min = 0.0, eig_max = 0.0;
   bool eig_valid = false;
   float *kq = nullptr;  // FP32 conductivity at the q-points (Picard preconditioner operator)
+  // two-phase / transport fields (caller-owned nodal vectors) and the per-q coefficient
+  // fields built from them (LAW 4 of the cell kernels), FP64 and its FP32 copy
+  const double *Hf = nullptr, *vel = nullptr;
+  double *cf = nullptr;
+  float *cf_f = nullptr;
+  bool cf_dirty = true, cf_f_dirty = true;
   // GMRES basis (m + 1 vectors) and small device buffers
   double *gV = nullptr;
   int gV_m = 0;
@@ -294,6 +300,86 @@ __global__ void k_geometry(int64_t n_cells, MeshDims d, int n, Q1D q1, const dou
       for (int e = 0; e < 3; ++e) s += inv[ia[k]][e] * inv[ib[k]][e];
       g[(1 + k) * npt] = jxw * s;
     }
+  }
+}
+
+// Per-quadrature-point coefficients of the gas-liquid / convective operator,
+// cf[cell][5][npt] = {rho_cp JxW, k, JxW rho_cp J^-1 v}: the heaviside and velocity fields
+// are interpolated at the point (FEEvaluation::evaluate(values) on the nodal vectors,
+// heat_diffuse_operator.cpp:448-473), the gas-liquid law mixes the phase properties with
+// w = H (smooth) or w = (H > 0.5) (sharp): (1 - w) gas + w liquid
+// (Material::compute_parameters, material.templates.hpp:240-295 and :515-524); rho_cp is
+// the product of the mixed density and capacity or the mixed volume-specific capacity
+// (heat_diffuse_operator.cpp:1138-1162).  Without a heaviside field w = 1 (liquid
+// properties, the constant law).  J^-1 v turns v.grad(u) into a contraction with the
+// reference gradient.  One thread per (cell, point); the interpolation is a direct
+// n^3-term sum (a set-up pass, run when the fields or the material change).
+struct FieldArgs {
+  MeshDims d;
+  int n, geo;
+  int64_t n_cells, n_dofs;
+  double hc[3];
+  double xg[8], wg[8], S[8][8];
+  const double *vert, *H, *vel;
+  int mix, sharp, vs;
+  double rho_l, cp_l, k_l, rho_g, cp_g, k_g;
+  double *cf;
+};
+
+__global__ void k_coef_fields(FieldArgs a)
+{
+  const int n = a.n, npt = n * n * n;
+  const int64_t total = a.n_cells * npt;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / npt;
+    const int q = (int)(t % npt);
+    const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
+    const int cx = (int)(c % a.d.m[0]), cy = (int)((c / a.d.m[0]) % a.d.m[1]),
+              cz = (int)(c / ((int64_t)a.d.m[0] * a.d.m[1]));
+    const int64_t base =
+      (int64_t)a.d.p * cx + (int64_t)a.d.nd[0] * ((int64_t)a.d.p * cy + (int64_t)a.d.nd[1] * a.d.p * cz);
+    double Hq = 0.0, v[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j) {
+        const double wjk = a.S[qk][k] * a.S[qj][j];
+        const int64_t row = base + (int64_t)a.d.nd[0] * (j + (int64_t)a.d.nd[1] * k);
+        for (int i = 0; i < n; ++i) {
+          const double w = wjk * a.S[qi][i];
+          if (a.H) Hq += w * a.H[row + i];
+          if (a.vel)
+            for (int e = 0; e < 3; ++e) v[e] += w * a.vel[(int64_t)e * a.n_dofs + row + i];
+        }
+      }
+    const double w = !a.mix ? 1.0 : (!a.H ? 1.0 : (a.sharp ? (Hq > 0.5 ? 1.0 : 0.0) : Hq));
+    const double kk = (1.0 - w) * a.k_g + w * a.k_l;
+    const double rhocp = a.vs ? (1.0 - w) * (a.rho_g * a.cp_g) + w * (a.rho_l * a.cp_l)
+                              : ((1.0 - w) * a.rho_g + w * a.rho_l) * ((1.0 - w) * a.cp_g + w * a.cp_l);
+    double det, inv[3][3];
+    if (a.geo == 0) {
+      det = a.hc[0] * a.hc[1] * a.hc[2];
+      for (int e = 0; e < 3; ++e)
+        for (int f = 0; f < 3; ++f) inv[e][f] = e == f ? 1.0 / a.hc[e] : 0.0;
+    } else {
+      const double xi[3] = {a.xg[qi], a.xg[qj], a.xg[qk]};
+      double x[3], J[3][3];
+      trilinear(a.vert, a.d, cx, cy, cz, xi, x, J);
+      det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+            J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+            J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+      for (int e = 0; e < 3; ++e)
+        for (int f = 0; f < 3; ++f) {
+          // (J^-1)[e][f] = cofactor of J[f][e] / det
+          const int r0 = (f + 1) % 3, r1 = (f + 2) % 3, c0 = (e + 1) % 3, c1 = (e + 2) % 3;
+          inv[e][f] = (J[r0][c0] * J[r1][c1] - J[r0][c1] * J[r1][c0]) / det;
+        }
+    }
+    const double jxw = det * a.wg[qi] * a.wg[qj] * a.wg[qk];
+    double *o = a.cf + c * 5 * npt + q;
+    o[0] = rhocp * jxw;
+    o[npt] = kk;
+    for (int e = 0; e < 3; ++e)
+      o[(2 + e) * npt] = jxw * rhocp * (inv[e][0] * v[0] + inv[e][1] * v[1] + inv[e][2] * v[2]);
   }
 }
 
@@ -1067,10 +1153,64 @@ static int ensure_dt(mpdg_heat *h)
   return MPDG_OK;
 }
 
+// the cell kernels' law: the public laws 0-2, or 4 (coefficient fields) for the gas-liquid
+// law and for any law with a velocity field
+static int klaw(const mpdg_heat *h)
+{
+  return (h->law == MPDG_LAW_GAS_LIQUID || h->vel) ? 4 : h->law;
+}
+
+static bool law_tdep(const mpdg_heat *h)
+{
+  return h->law == MPDG_LAW_LINEAR_K || h->law == MPDG_LAW_LIQUID_SOLID;
+}
+
+// (re)build the per-q coefficient fields when the operator uses them
+static int ensure_fields(mpdg_heat *h)
+{
+  if (klaw(h) != 4 || !h->cf_dirty) return MPDG_OK;
+  TRY(dvec(h, &h->cf, h->n_cells * 5 * h->npt));
+  const Tables1D t1 = make_tables(h->n);
+  FieldArgs a;
+  memset(&a, 0, sizeof(a));
+  a.d = h->dims;
+  a.n = h->n;
+  a.geo = h->geo;
+  a.n_cells = h->n_cells;
+  a.n_dofs = h->n_dofs;
+  for (int e = 0; e < 3; ++e) a.hc[e] = h->hcell[e];
+  for (int q = 0; q < h->n; ++q) {
+    a.xg[q] = t1.xg[q];
+    a.wg[q] = t1.wg[q];
+    for (int i = 0; i < h->n; ++i) a.S[q][i] = t1.A[kS][q][i];
+  }
+  a.vert = h->vert;
+  a.H = h->Hf;
+  a.vel = h->vel;
+  a.mix = h->law == MPDG_LAW_GAS_LIQUID;
+  a.sharp = h->mat.sharp;
+  a.vs = h->mat.volume_specific;
+  a.rho_l = h->mat.rho_l;
+  a.cp_l = h->mat.cp_l;
+  a.k_l = h->mat.k_l;
+  a.rho_g = h->mat.rho_s;
+  a.cp_g = h->mat.cp_s;
+  a.k_g = h->mat.k_s;
+  a.cf = h->cf;
+  const int64_t total = h->n_cells * h->npt;
+  k_coef_fields<<<vgrid(h, total), VT, 0, h->stream>>>(a); ++h->launches;
+  CU(cudaGetLastError());
+  h->cf_dirty = false;
+  h->cf_f_dirty = true;
+  return MPDG_OK;
+}
+
 static int ensure_lin(mpdg_heat *h)
 {
-  if (h->law != MPDG_LAW_CONSTANT && !h->T_lin)
+  if (law_tdep(h) && !h->T_lin)
     return fail(MPDG_ERR_INVALID_ARGUMENT, "temperature-dependent law needs set_linearization");
+  if (h->law == MPDG_LAW_GAS_LIQUID && !h->Hf)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "gas-liquid law needs a heaviside field (set_fields)");
   if (h->law == MPDG_LAW_LIQUID_SOLID && h->need_told && !h->T_old)
     return fail(MPDG_ERR_INVALID_ARGUMENT, "liquid-solid law needs temperature_old");
   return MPDG_OK;
@@ -1138,8 +1278,10 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
 {
   TRY(ensure_dt(h));
   TRY(ensure_lin(h));
+  TRY(ensure_fields(h));
   CellArgs<double> a = cell_args<double>(h);
   a.g.q = h->geoq;
+  a.cf = h->cf;
   a.src = src;
   a.dst = dst;
   a.Tl = h->T_lin;
@@ -1159,7 +1301,7 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
     TRY(launch_faces<double>(h, 0, dst, src, h->T_lin, fin != FIN_NONE ? h->face_dot : nullptr, st));
     if (fin != FIN_NONE) a.extra_dot = h->face_dot;
   }
-  CU(h->tab.vmult_d(a, h->geo, h->law, h->stream, h->sm_count));
+  CU(h->tab.vmult_d(a, h->geo, klaw(h), h->stream, h->sm_count));
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
     h->ev64.push_back({e0, e1});
@@ -1178,7 +1320,18 @@ static int refresh_f32(mpdg_heat *h)
     k_cast_f<<<vgrid(h, ng), VT, 0, h->stream>>>(ng, h->geoq, h->geoq_f); ++h->launches;
     CU(cudaGetLastError());
   }
-  if (h->lin_f_dirty && h->law != MPDG_LAW_CONSTANT) {
+  if (klaw(h) == 4 && h->cf_f_dirty) {
+    TRY(ensure_fields(h));
+    const int64_t nc = h->n_cells * 5 * h->npt;
+    TRY(dvec(h, &h->cf_f, nc));
+    k_cast_f<<<vgrid(h, nc), VT, 0, h->stream>>>(nc, h->cf, h->cf_f); ++h->launches;
+    CU(cudaGetLastError());
+    h->cf_f_dirty = false;
+  }
+  // T_lin in FP32 for the temperature-dependent laws and the radiation faces' tangent
+  bool radiation = false;
+  for (int f = 0; f < 6; ++f) radiation = radiation || (h->btype[f] & MPDG_BC_RADIATION);
+  if (h->lin_f_dirty && h->T_lin && (law_tdep(h) || radiation)) {
     TRY(dvec(h, &h->T_lin_f, N));
     TRY(dvec(h, &h->T_old_f, N));
     k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->T_lin, h->T_lin_f); ++h->launches;
@@ -1197,9 +1350,11 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
 {
   TRY(ensure_dt(h));
   TRY(ensure_lin(h));
+  TRY(ensure_fields(h));
   TRY(refresh_f32(h));
   CellArgs<float> a = cell_args<float>(h);
   a.kq = h->kq;
+  a.cf = h->cf_f;
   a.g.q = h->geoq_f;
   a.src = src;
   a.dst = dst;
@@ -1213,7 +1368,7 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
     cudaEventRecord(e0, h->stream);
   }
   if (any_faces(h)) TRY(launch_faces<float>(h, 0, dst, src, h->T_lin_f, nullptr, st));
-  CU(h->tab.vmult_f(a, h->geo, picard ? 3 : h->law, h->stream, h->sm_count));
+  CU(h->tab.vmult_f(a, h->geo, picard ? 3 : klaw(h), h->stream, h->sm_count));
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
     h->ev32.push_back({e0, e1});
@@ -1710,6 +1865,9 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
 {
   const int64_t N = h->n_dofs;
   const bool use_mg = prm->preconditioner == MPDG_PRECOND_MG_F32;
+  if (use_mg && klaw(h) == 4)
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "multigrid preconditioner: not available with the gas-liquid law or a velocity field");
   const bool picard = prm->cheb_picard && h->law == MPDG_LAW_LINEAR_K && h->tab.conductivity_q;
   // the FP64 inverse diagonal feeds the Lanczos estimate and the Chebyshev smoother; the
   // multigrid smoothers of the Picard operator use that operator's own FP32 diagonal
@@ -2218,7 +2376,10 @@ extern "C" int mpdg_heat_device_bytes(const mpdg_heat *h, int64_t *bytes)
 extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
 {
   if (!h || !m) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
-  if (m->law < 0 || m->law > 2) return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown material law");
+  if (m->law < 0 || m->law > 3) return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown material law");
+  if (h->vel && (m->law == MPDG_LAW_LINEAR_K || m->law == MPDG_LAW_LIQUID_SOLID))
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "a velocity field needs the constant or the gas-liquid law");
   if (m->law == MPDG_LAW_LIQUID_SOLID && !m->sharp && !(m->T_liquidus > m->T_solidus))
     return fail(MPDG_ERR_INVALID_ARGUMENT, "liquidus must exceed solidus");
   h->mat = *m;
@@ -2227,6 +2388,21 @@ extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
   if (m->law == MPDG_LAW_LIQUID_SOLID)
     h->need_told = m->volume_specific ? (m->rho_l * m->cp_l != m->rho_s * m->cp_s)
                                       : (m->rho_l != m->rho_s || m->cp_l != m->cp_s);
+  h->diag_valid = false;
+  h->eig_valid = false;
+  h->cf_dirty = true;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_fields(mpdg_heat *h, const double *heaviside, const double *velocity)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  if (velocity && (h->law == MPDG_LAW_LINEAR_K || h->law == MPDG_LAW_LIQUID_SOLID))
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "a velocity field needs the constant or the gas-liquid law");
+  h->Hf = heaviside;
+  h->vel = velocity;
+  h->cf_dirty = true;
   h->diag_valid = false;
   h->eig_valid = false;
   return MPDG_OK;
@@ -2251,6 +2427,7 @@ extern "C" int mpdg_heat_set_boundary(mpdg_heat *h, int face, int type, double h
   h->beps[face] = emissivity;
   h->bTr[face] = T_inf_rad;
   h->bqn[face] = q_n;
+  h->lin_f_dirty = true;
   h->diag_valid = false;
   h->eig_valid = false;
   return MPDG_OK;
@@ -2328,13 +2505,15 @@ static int compute_diag(mpdg_heat *h, double *d)
 {
   TRY(ensure_dt(h));
   TRY(ensure_lin(h));
+  TRY(ensure_fields(h));
   CU(cudaMemsetAsync(d, 0, sizeof(double) * h->n_dofs, h->stream));
   CellArgs<double> a = cell_args<double>(h);
   a.g.q = h->geoq;
+  a.cf = h->cf;
   a.dst = d;
   a.Tl = h->T_lin;
   a.To = h->T_old;
-  CU(h->tab.diag(a, h->geo, h->law, h->stream, h->sm_count));
+  CU(h->tab.diag(a, h->geo, klaw(h), h->stream, h->sm_count));
   ++h->launches;
   if (any_faces(h)) TRY(launch_faces<double>(h, 2, d, nullptr, h->T_lin, nullptr, nullptr));
   k_invert_diag<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, d); ++h->launches;
@@ -2353,13 +2532,16 @@ static int create_rhs(mpdg_heat *h, double *dst, const double *src, const double
 {
   TRY(ensure_dt(h));
   if (!h->T_lin) return fail(MPDG_ERR_INVALID_ARGUMENT, "create_rhs needs set_linearization");
+  TRY(ensure_lin(h));
+  TRY(ensure_fields(h));
   CellArgs<double> a = cell_args<double>(h);
   a.g.q = h->geoq;
+  a.cf = h->cf;
   a.dst = dst;
   a.Tl = h->T_lin;
   a.To = src;
   a.qs = q;
-  CU(h->tab.rhs(a, h->geo, h->law, h->stream, h->sm_count));
+  CU(h->tab.rhs(a, h->geo, klaw(h), h->stream, h->sm_count));
   ++h->launches;
   if (any_faces(h)) TRY(launch_faces<double>(h, 1, dst, nullptr, h->T_lin, nullptr, nullptr));
   return MPDG_OK;

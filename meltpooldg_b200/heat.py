@@ -219,6 +219,15 @@ class HeatDiffuseOperator:
     def set_material(self, m: L.Material):
         check(self._L.mpdg_heat_set_material(self.h, C.byref(m)))
 
+    def set_fields(self, heaviside=None, velocity=None):
+        """Level-set heaviside (n_dofs) and velocity ((3, n_dofs), component-major) fields
+        of the two-phase operator, torch CUDA float64 tensors on this operator's DoFs; None
+        removes one. Call again after changing a field's contents."""
+        if velocity is not None:
+            assert velocity.is_contiguous() and velocity.numel() == 3 * self.n_dofs
+        self._fields = (heaviside, velocity)
+        check(self._L.mpdg_heat_set_fields(self.h, _ptr(heaviside), _ptr(velocity)))
+
     def set_boundary(self, face, convection=None, radiation=None, neumann=None):
         """Robin / Neumann terms on a box face: convection=(h, T_inf),
         radiation=(emissivity, T_inf), neumann=q_n; no argument clears the face."""

@@ -5,6 +5,9 @@ prints one JSON line per precision with the CUDA-event time per application,
 DoFs/s and algorithmic GB/s (src + dst + linearisation point [+ per-q geometry]).
 With --solve it instead runs a few outer iterations of FP64 CG with the FP32
 Chebyshev preconditioner on the Picard operator, so that kernel can be captured.
+With --transport the operator is the two-phase one (gas-liquid law on a heaviside
+field plus the convective term of a velocity field), whose per-point coefficients
+(5 per quadrature point) replace the linearisation point in the traffic.
 """
 from __future__ import annotations
 
@@ -25,15 +28,25 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--dtype", default="both", choices=["f64", "f32", "both"])
     ap.add_argument("--solve", action="store_true")
+    ap.add_argument("--transport", action="store_true")
     a = ap.parse_args()
     op = H.HeatDiffuseOperator(H.box_mesh(a.degree, (a.cells,) * 3, perturb=a.perturb))
-    op.set_material(H.material(law=a.law, k=1.0, k1=0.5))
+    if a.transport:
+        a.law = 3
+        op.set_material(H.material(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3))
+    else:
+        op.set_material(H.material(law=a.law, k=1.0, k1=0.5))
     op.reset_time_increment(5e-4)
     N = op.n_dofs
     g = torch.Generator(device="cuda").manual_seed(0)
     T = torch.rand(N, dtype=torch.float64, device="cuda", generator=g)
     op.set_linearization(T, T)
     nq = op.n_cells * (a.degree + 1) ** 3
+    if a.transport:
+        x = op.support_points()
+        hs = (0.5 + 0.5 * torch.tanh((x[:, 2] - 0.5) / 0.05)).contiguous()
+        vel = torch.stack([torch.sin(3 * x[:, 1]), 0.5 + x[:, 2], -x[:, 0] * x[:, 1]]).contiguous()
+        op.set_fields(hs, vel)
     if a.solve:
         from . import _lib as L
         op.distribute_constraints(T)
@@ -64,9 +77,12 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / a.reps
-        alg = s * N * (2 + (1 if a.law else 0)) + (7 * s * nq if a.perturb > 0 else 0)
+        if a.transport:
+            alg = s * N * 2 + 5 * s * nq + (7 * s * nq if a.perturb > 0 else 0)
+        else:
+            alg = s * N * (2 + (1 if a.law else 0)) + (7 * s * nq if a.perturb > 0 else 0)
         print(json.dumps({"degree": a.degree, "cells": a.cells, "perturb": a.perturb,
-                          "law": a.law, "dtype": dt, "n_dofs": N, "ms": ms,
+                          "law": a.law, "transport": a.transport, "dtype": dt, "n_dofs": N, "ms": ms,
                           "gdofs": N / ms / 1e6, "alg_bytes": alg,
                           "alg_gbs": alg / ms / 1e6}), flush=True)
 

@@ -159,6 +159,8 @@ struct orc_heat {
   double       dt;
   int          tdep;      /* temperature-dependent law: tangent terms + T_lin */
   int          need_told; /* d(rho cp)/dT may be non-zero */
+  const double *Hf, *vel; /* nodal heaviside and velocity ([3][n_dofs]) fields, or NULL */
+  int          fields;    /* coefficients from the fields: gas-liquid law and/or convection */
   /* direct-form tables */
   double *phi, *dphi;
   /* boundary terms per face */
@@ -471,7 +473,8 @@ void orc_set_material(orc_heat *h, const orc_material *m, double dt)
 {
   h->mat = *m;
   h->dt = dt;
-  h->tdep = m->law != ORC_LAW_CONSTANT;
+  h->tdep = m->law == ORC_LAW_LINEAR_K || m->law == ORC_LAW_LIQUID_SOLID;
+  h->fields = m->law == ORC_LAW_GAS_LIQUID || h->vel != NULL;
   h->need_told = 0;
   if (m->law == ORC_LAW_LIQUID_SOLID) {
     if (m->volume_specific)
@@ -481,10 +484,58 @@ void orc_set_material(orc_heat *h, const orc_material *m, double dt)
   }
 }
 
+int orc_set_fields(orc_heat *h, const double *heaviside, const double *velocity)
+{
+  if (velocity && h->tdep) return -1;
+  h->Hf = heaviside;
+  h->vel = velocity;
+  h->fields = h->mat.law == ORC_LAW_GAS_LIQUID || velocity != NULL;
+  return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* material law (Material::compute_parameters, liquid_solid / gas,     */
 /* plus the linear conductivity law k = k_l + k1 T)                    */
 /* ------------------------------------------------------------------ */
+
+/* gas-liquid law at heaviside value H (material.templates.hpp:240-295): every property is
+ * (1 - w) gas + w liquid (LevelSet::Tools::interpolate, level_set_tools.hpp:40-43) with
+ * w = H (smooth transition) or heaviside(H, 0.5) = H > 0.5 (sharp, :515-524,
+ * characteristic_functions.hpp:37-40); rho*cp is the product of the interpolated density
+ * and capacity, or the interpolated volume-specific capacity (heat_diffuse_operator.cpp:
+ * 1138-1162).  The temperature derivatives are zero. */
+static inline void material_eval_H(const orc_material *m, double H, double *rhocp, double *k)
+{
+  const double w = m->law != ORC_LAW_GAS_LIQUID ? 1.0 : (m->sharp ? (H > 0.5 ? 1.0 : 0.0) : H);
+#define MIX(l, g) ((1.0 - w) * (g) + w * (l))
+  *k = MIX(m->k_l, m->k_s);
+  if (m->volume_specific)
+    *rhocp = MIX(m->rho_l * m->cp_l, m->rho_s * m->cp_s);
+  else
+    *rhocp = MIX(m->rho_l, m->rho_s) * MIX(m->cp_l, m->cp_s);
+#undef MIX
+}
+
+/* J^-1 v at quadrature point q of cell c (reference-space transport direction: the
+ * physical v.grad(u) equals (J^-1 v).grad_ref(u)) */
+static void ref_direction(const orc_heat *h, int64_t c, int q, const double v[3], double b[3])
+{
+  const int n = h->n;
+  const double xi[3] = {h->xg[q % n], h->xg[(q / n) % n], h->xg[q / (n * n)]};
+  double x[3], J[3][3];
+  cell_map(h, c, xi, x, J);
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                     J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  double inv[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      /* cofactor of J[j][i] */
+      const int r0 = (j + 1) % 3, r1 = (j + 2) % 3, c0 = (i + 1) % 3, c1 = (i + 2) % 3;
+      inv[i][j] = (J[r0][c0] * J[r1][c1] - J[r0][c1] * J[r1][c0]) / det;
+    }
+  for (int i = 0; i < 3; ++i) b[i] = inv[i][0] * v[0] + inv[i][1] * v[1] + inv[i][2] * v[2];
+}
 
 static inline void material_eval(const orc_material *m, double T, double *rhocp, double *k,
                                  double *drhocp, double *dk)
@@ -589,6 +640,7 @@ typedef struct {
   lane_t u[NPT_MAX], t1[NPT_MAX], t2[NPT_MAX];
   lane_t uq[NPT_MAX], gx[NPT_MAX], gy[NPT_MAX], gz[NPT_MAX];
   lane_t Tq[NPT_MAX], Tx[NPT_MAX], Ty[NPT_MAX], Tz[NPT_MAX], Toq[NPT_MAX], Sq[NPT_MAX];
+  lane_t Hq[NPT_MAX], Vq[3][NPT_MAX];
   lane_t c[10][NPT_MAX];
 } scratch_t;
 
@@ -665,6 +717,44 @@ static inline __attribute__((always_inline)) void eval_vg(const orc_heat *h, con
   }
 }
 
+/* heaviside and velocity values at the q-points of a batch (fields mode) */
+static inline __attribute__((always_inline)) void eval_fields(const orc_heat *h, const int n,
+                                                              const int64_t *cells, int nl,
+                                                              scratch_t *s)
+{
+  const int npt = n * n * n;
+  if (h->Hf) {
+    gather(h, cells, nl, h->Hf, 0, s->u);
+    eval_vg(h, n, s->u, s, s->Hq, NULL, NULL, NULL);
+  } else {
+    for (int q = 0; q < npt; ++q)
+      for (int v = 0; v < ORC_VEC; ++v) s->Hq[q][v] = 1.0;
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (h->vel) {
+      gather(h, cells, nl, h->vel + (size_t)d * h->n_dofs, 0, s->u);
+      eval_vg(h, n, s->u, s, s->Vq[d], NULL, NULL, NULL);
+    } else {
+      for (int q = 0; q < npt; ++q)
+        for (int v = 0; v < ORC_VEC; ++v) s->Vq[d][q][v] = 0.0;
+    }
+  }
+}
+
+/* coefficients of lane v at point q in fields mode: rho*cp, k and the reference-space
+ * transport vector b = J^-1 v (zero without a velocity field) */
+static inline void field_coefs(const orc_heat *h, const int64_t *cells, int nl, int v, int q,
+                               const scratch_t *s, double *rhocp, double *k, double b[3])
+{
+  material_eval_H(&h->mat, s->Hq[q][v], rhocp, k);
+  if (h->vel) {
+    const double vv[3] = {s->Vq[0][q][v], s->Vq[1][q][v], s->Vq[2][q][v]};
+    ref_direction(h, cells[v < nl ? v : 0], q, vv, b);
+  } else {
+    b[0] = b[1] = b[2] = 0.0;
+  }
+}
+
 /* out = S^T (val + sum_d D_d^T f_d) ; val in vq, fluxes in fx, fy, fz */
 static inline __attribute__((always_inline)) void integrate_vg(const orc_heat *h, const int n,
                                                                lane_t *vq, lane_t *fx,
@@ -688,6 +778,7 @@ static inline __attribute__((always_inline)) void batch_kernel(
 {
   const int npt = n * n * n;
   const double idt = 1.0 / h->dt;
+  if (h->fields && kind != 3) eval_fields(h, n, cells, nl, s);
   if (kind == 0 || kind == 4) {
     gather(h, cells, nl, src, 1, s->u);
     eval_vg(h, n, s->u, s, s->uq, s->gx, s->gy, s->gz);
@@ -701,10 +792,17 @@ static inline __attribute__((always_inline)) void batch_kernel(
     }
     for (int q = 0; q < npt; ++q)
       for (int v = 0; v < ORC_VEC; ++v) {
-        double jxw, G[6], rhocp, k, drhocp, dk;
+        double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
         geo_at(h, cells, nl, v, q, &jxw, G);
-        material_eval(&h->mat, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk);
+        if (h->fields) {
+          field_coefs(h, cells, nl, v, q, s, &rhocp, &k, b);
+          drhocp = dk = 0.0;
+        } else {
+          material_eval(&h->mat, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk);
+        }
         double cval = idt * rhocp;
+        /* convection rho_cp v.grad(u) (heat_diffuse_operator.cpp:1038-1042) */
+        const double conv = rhocp * (b[0] * s->gx[q][v] + b[1] * s->gy[q][v] + b[2] * s->gz[q][v]);
         double g0 = k * s->gx[q][v], g1 = k * s->gy[q][v], g2 = k * s->gz[q][v];
         if (h->tdep) {
           if (h->need_told) cval += idt * drhocp * (s->Tq[q][v] - s->Toq[q][v]);
@@ -714,7 +812,7 @@ static inline __attribute__((always_inline)) void batch_kernel(
           g1 += dk * s->Ty[q][v] * uu;
           g2 += dk * s->Tz[q][v] * uu;
         }
-        s->uq[q][v] = cval * s->uq[q][v] * jxw;
+        s->uq[q][v] = (cval * s->uq[q][v] + conv) * jxw;
         s->gx[q][v] = G[0] * g0 + G[1] * g1 + G[2] * g2;
         s->gy[q][v] = G[1] * g0 + G[3] * g1 + G[4] * g2;
         s->gz[q][v] = G[2] * g0 + G[4] * g1 + G[5] * g2;
@@ -730,10 +828,15 @@ static inline __attribute__((always_inline)) void batch_kernel(
     eval_vg(h, n, s->u, s, s->Sq, NULL, NULL, NULL);
     for (int q = 0; q < npt; ++q)
       for (int v = 0; v < ORC_VEC; ++v) {
-        double jxw, G[6], rhocp, k, drhocp, dk;
+        double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
         geo_at(h, cells, nl, v, q, &jxw, G);
-        material_eval(&h->mat, s->Tq[q][v], &rhocp, &k, &drhocp, &dk);
-        const double val = idt * rhocp * (s->Tq[q][v] - s->Toq[q][v]) - s->Sq[q][v];
+        if (h->fields)
+          field_coefs(h, cells, nl, v, q, s, &rhocp, &k, b);
+        else
+          material_eval(&h->mat, s->Tq[q][v], &rhocp, &k, &drhocp, &dk);
+        /* rhs_cell_loop value term with the convection rho_cp grad(T).v (:493-500) */
+        const double val = idt * rhocp * (s->Tq[q][v] - s->Toq[q][v]) - s->Sq[q][v] +
+                           rhocp * (b[0] * s->Tx[q][v] + b[1] * s->Ty[q][v] + b[2] * s->Tz[q][v]);
         const double g0 = k * s->Tx[q][v], g1 = k * s->Ty[q][v], g2 = k * s->Tz[q][v];
         s->uq[q][v] = -val * jxw;
         s->gx[q][v] = -(G[0] * g0 + G[1] * g1 + G[2] * g2);
@@ -757,9 +860,14 @@ static inline __attribute__((always_inline)) void batch_kernel(
            *Gyz = s->c[5], *Gzz = s->c[6], *Bx = s->c[7], *By = s->c[8], *Bz = s->c[9];
     for (int q = 0; q < npt; ++q)
       for (int v = 0; v < ORC_VEC; ++v) {
-        double jxw, G[6], rhocp, k, drhocp, dk;
+        double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
         geo_at(h, cells, nl, v, q, &jxw, G);
-        material_eval(&h->mat, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk);
+        if (h->fields) {
+          field_coefs(h, cells, nl, v, q, s, &rhocp, &k, b);
+          drhocp = dk = 0.0;
+        } else {
+          material_eval(&h->mat, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk);
+        }
         double cval = idt * rhocp;
         if (h->tdep && h->need_told) cval += idt * drhocp * (s->Tq[q][v] - s->Toq[q][v]);
         C0[q][v] = cval * jxw;
@@ -775,7 +883,10 @@ static inline __attribute__((always_inline)) void batch_kernel(
           By[q][v] = dk * (G[1] * t0 + G[3] * t1 + G[4] * t2);
           Bz[q][v] = dk * (G[2] * t0 + G[4] * t1 + G[5] * t2);
         } else {
-          Bx[q][v] = By[q][v] = Bz[q][v] = 0.0;
+          /* convection: phi_i (JxW rho_cp J^-1 v).grad_ref(phi_i) */
+          Bx[q][v] = jxw * rhocp * b[0];
+          By[q][v] = jxw * rhocp * b[1];
+          Bz[q][v] = jxw * rhocp * b[2];
         }
       }
     /* (x,y) = (P,P): z P C0 + z Q Gzz + z R Bz */
@@ -893,7 +1004,7 @@ static void run_direct(const orc_heat *h, int kind, double *dst, const double *s
     for (int64_t ic = 0; ic < nc; ++ic) {
       const int64_t c = h->color_cells[col][ic];
       const int64_t base = cell_base_dof(h, c);
-      double u[NPT_MAX], T[NPT_MAX], To_[NPT_MAX], out[NPT_MAX];
+      double u[NPT_MAX], T[NPT_MAX], To_[NPT_MAX], out[NPT_MAX], Hn[NPT_MAX], Vn[3][NPT_MAX];
       int64_t gidx[NPT_MAX];
       for (int k = 0; k < n; ++k)
         for (int j = 0; j < n; ++j)
@@ -903,24 +1014,35 @@ static void run_direct(const orc_heat *h, int kind, double *dst, const double *s
             u[l] = (kind == 0 && !h->mask[gidx[l]]) ? src[gidx[l]] : 0.0;
             T[l] = h->tdep ? Tl[gidx[l]] : 0.0;
             To_[l] = h->need_told ? To[gidx[l]] : 0.0;
+            Hn[l] = h->Hf ? h->Hf[gidx[l]] : 1.0;
+            for (int e = 0; e < 3; ++e) Vn[e][l] = h->vel ? h->vel[(size_t)e * h->n_dofs + gidx[l]] : 0.0;
             out[l] = 0.0;
           }
       const int64_t one[1] = {c};
       for (int q = 0; q < npt; ++q) {
         const double *ph = h->phi + (size_t)q * npt, *dph = h->dphi + (size_t)q * npt * 3;
-        double uq = 0, gu[3] = {0, 0, 0}, Tq = 0, gT[3] = {0, 0, 0}, Toq = 0;
+        double uq = 0, gu[3] = {0, 0, 0}, Tq = 0, gT[3] = {0, 0, 0}, Toq = 0, Hq = 0,
+               vq[3] = {0, 0, 0};
         for (int i = 0; i < npt; ++i) {
           uq += ph[i] * u[i];
           Tq += ph[i] * T[i];
           Toq += ph[i] * To_[i];
+          Hq += ph[i] * Hn[i];
+          for (int e = 0; e < 3; ++e) vq[e] += ph[i] * Vn[e][i];
           for (int d = 0; d < 3; ++d) {
             gu[d] += dph[3 * i + d] * u[i];
             gT[d] += dph[3 * i + d] * T[i];
           }
         }
-        double jxw, G[6], rhocp, k, drhocp, dk;
+        double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
         geo_at(h, one, 1, 0, q, &jxw, G);
-        material_eval(&h->mat, Tq, &rhocp, &k, &drhocp, &dk);
+        if (h->fields) {
+          material_eval_H(&h->mat, Hq, &rhocp, &k);
+          drhocp = dk = 0.0;
+          if (h->vel) ref_direction(h, c, q, vq, b);
+        } else {
+          material_eval(&h->mat, Tq, &rhocp, &k, &drhocp, &dk);
+        }
         double cval = idt * rhocp;
         if (h->tdep && h->need_told) cval += idt * drhocp * (Tq - Toq);
         if (!h->tdep) dk = 0.0;
@@ -929,13 +1051,14 @@ static void run_direct(const orc_heat *h, int kind, double *dst, const double *s
           double f[3], F[3];
           for (int d = 0; d < 3; ++d) f[d] = k * gu[d] + dk * gT[d] * uq;
           for (int d = 0; d < 3; ++d) F[d] = Gm[d][0] * f[0] + Gm[d][1] * f[1] + Gm[d][2] * f[2];
-          const double val = cval * uq * jxw;
+          const double val = (cval * uq + rhocp * (b[0] * gu[0] + b[1] * gu[1] + b[2] * gu[2])) * jxw;
           for (int i = 0; i < npt; ++i)
             out[i] += ph[i] * val + dph[3 * i] * F[0] + dph[3 * i + 1] * F[1] + dph[3 * i + 2] * F[2];
         } else {
           double BT[3];
           for (int d = 0; d < 3; ++d)
-            BT[d] = dk * (Gm[d][0] * gT[0] + Gm[d][1] * gT[1] + Gm[d][2] * gT[2]);
+            BT[d] = dk * (Gm[d][0] * gT[0] + Gm[d][1] * gT[1] + Gm[d][2] * gT[2]) +
+                    jxw * rhocp * b[d];
           for (int i = 0; i < npt; ++i) {
             const double *g = dph + 3 * i;
             double s = cval * jxw * ph[i] * ph[i];

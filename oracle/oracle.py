@@ -25,7 +25,7 @@ _HDR = os.path.join(_HERE, "mpdg_oracle.h")
 _lock = threading.Lock()
 _lib = None
 
-LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID = 0, 1, 2
+LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID = 0, 1, 2, 3
 
 
 def _cpu_tag() -> str:
@@ -108,6 +108,7 @@ def lib():
             L.orc_distribute.argtypes = [_P, _D]
             L.orc_set_threads.argtypes = [C.c_int]
             L.orc_set_material.argtypes = [_P, C.POINTER(Material), C.c_double]
+            L.orc_set_fields.argtypes = [_P, _D, _D]
             L.orc_vmult.argtypes = [_P, _D, _D, _D, _D, C.c_int]
             L.orc_inverse_diagonal.argtypes = [_P, _D, _D, _D, C.c_int]
             L.orc_create_rhs.argtypes = [_P, _D, _D, _D, _D]
@@ -209,6 +210,14 @@ class Oracle:
     def set_material(self, m: Material, dt: float):
         self.dt = dt
         self.L.orc_set_material(self.h, C.byref(m), dt)
+
+    def set_fields(self, heaviside=None, velocity=None):
+        """Nodal heaviside (n_dofs) and velocity ((3, n_dofs)) fields; None clears one."""
+        H = None if heaviside is None else np.ascontiguousarray(heaviside, np.float64)
+        V = None if velocity is None else np.ascontiguousarray(velocity, np.float64).reshape(3, -1)
+        self._fields = (H, V)  # the oracle keeps the pointers
+        if self.L.orc_set_fields(self.h, _ptr(H), None if V is None else _ptr(V)) != 0:
+            raise ValueError("velocity with a temperature-dependent law")
 
     def set_boundary(self, face, convection=None, radiation=None, neumann=None):
         """convection=(h, T_inf), radiation=(emissivity, T_inf), neumann=q_n."""

@@ -395,3 +395,110 @@ def test_linear_solve_not_converged_raises():
     with pytest.raises(H.ExcNoConvergence):
         H.LinearSolver.solve(g, g.new_vector(), b,
                              H.LinearSolverData(max_iterations=3, rel_tolerance=1e-12), True)
+
+
+TRANSPORT_CASES = {
+    # law, material, heaviside, velocity
+    "gas_liquid": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3), True, False),
+    "gas_liquid_sharp_vs": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3,
+                                 sharp=True, volume_specific=True), True, False),
+    "constant_velocity": (dict(law=0, rho=2.0, cp=3.0, k=5.0), False, True),
+    "gas_liquid_velocity": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3),
+                            True, True),
+}
+
+
+def transport_pair(degree, cells, perturb, case, dt=1e-2):
+    law, with_h, with_v = TRANSPORT_CASES[case]
+    hi = (1.0, 1.3, 0.8)
+    o = O.Oracle(degree, cells, hi=hi, perturb=perturb, seed=7)
+    o.set_material(O.material(**law), dt)
+    g = H.HeatDiffuseOperator(H.box_mesh(degree, cells, (0, 0, 0), hi, perturb, 7))
+    g.set_material(H.material(**law))
+    g.reset_time_increment(dt)
+    x = o.support_points()
+    Hf = 0.5 + 0.5 * np.tanh((x[:, 0] - 0.45) / 0.1) if with_h else None
+    V = np.stack([np.sin(3 * x[:, 1]), 0.5 + x[:, 2], -x[:, 0] * x[:, 1]]) if with_v else None
+    o.set_fields(Hf, V)
+    g.set_fields(None if Hf is None else cuda(Hf), None if V is None else cuda(V).contiguous())
+    return o, g
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+@pytest.mark.parametrize("case", list(TRANSPORT_CASES))
+def test_two_phase_transport_matches_oracle(degree, perturb, case):
+    """Gas-liquid law on the heaviside field and the convective term: FP64 vmult, inverse
+    diagonal and residual to 1e-12, the FP32 operator to 2e-5 (x10 for p >= 5)."""
+    cells = (5, 4, 3) if degree <= 4 else (3, 3, 2)
+    o, g = transport_pair(degree, cells, perturb, case)
+    rng = np.random.default_rng(7 * degree + int(10 * perturb))
+    N = o.n_dofs
+    src = rng.uniform(-1, 1, N)
+    T, To, q = rng.uniform(0, 1, N), rng.uniform(0, 1, N), rng.uniform(0, 5, N)
+    g.set_linearization(cuda(T), cuda(To))
+    ref = o.vmult(src)
+    dst = g.vmult(g.new_vector(), cuda(src))
+    assert rel(dst, ref) <= TOL64
+    d32 = g.vmult(g.new_vector(torch.float32), cuda(src, torch.float32))
+    assert rel(d32, ref) <= TOL32 * (10 if degree >= 5 else 1)
+    dref = o.inverse_diagonal()
+    dg = g.compute_inverse_diagonal_from_matrixfree(g.new_vector())
+    assert rel(1.0 / dg.cpu().numpy(), 1.0 / dref) <= TOL64
+    base = rng.uniform(-1, 1, N)
+    rref = o.create_rhs(T, To, q, dst=base.copy())
+    rg = cuda(base)
+    g.create_rhs(rg, cuda(To), cuda(q))
+    assert rel(rg, rref) <= TOL64
+
+
+def test_fields_are_rebuilt_after_set_fields_and_set_material():
+    o, g = transport_pair(3, (4, 3, 3), 0.1, "gas_liquid_velocity")
+    rng = np.random.default_rng(5)
+    src = rng.uniform(-1, 1, o.n_dofs)
+    g.vmult(g.new_vector(), cuda(src))
+    x = o.support_points()
+    Hf = 0.5 + 0.5 * np.tanh((x[:, 1] - 0.6) / 0.2)
+    V = np.stack([0 * x[:, 0] + 1.0, x[:, 0], 0 * x[:, 0]])
+    o.set_fields(Hf, V)
+    g.set_fields(cuda(Hf), cuda(V).contiguous())
+    assert rel(g.vmult(g.new_vector(), cuda(src)), o.vmult(src)) <= TOL64
+    m = dict(law=3, rho=1.0, cp=4.0, k=2.0, rho_s=0.1, cp_s=1.0, k_s=0.5)
+    o.set_material(O.material(**m), 1e-2)
+    g.set_material(H.material(**m))
+    assert rel(g.vmult(g.new_vector(), cuda(src)), o.vmult(src)) <= TOL64
+    o.set_fields(Hf, None)
+    g.set_fields(cuda(Hf), None)
+    assert rel(g.vmult(g.new_vector(), cuda(src)), o.vmult(src)) <= TOL64
+
+
+def test_gmres_on_the_convective_operator_matches_oracle():
+    o, g = transport_pair(2, (6, 5, 4), 0.1, "gas_liquid_velocity", dt=1e-1)
+    rng = np.random.default_rng(13)
+    N = o.n_dofs
+    b = o.vmult(rng.uniform(-1, 1, N))
+    x_ref, its_ref, _ = o.gmres(b, rel_tol=1e-12, restart=28)
+    g.set_linearization(cuda(np.zeros(N)), cuda(np.zeros(N)))
+    H.JacobiPreconditioner(g).update()
+    x = g.new_vector()
+    its = H.LinearSolver.solve(g, x, cuda(b), H.LinearSolverData(
+        solver_type=L.SOLVER_GMRES, rel_tolerance=1e-12), True)
+    assert abs(its - its_ref) <= max(2, its_ref // 10), (its, its_ref)
+    assert rel(x, x_ref) <= 1e-9
+
+
+def test_fields_reject_unsupported_combinations():
+    o, g = transport_pair(2, (4, 4, 4), 0.0, "constant_velocity")
+    with pytest.raises(H.ExcInvalidArgument):
+        g.set_material(H.material(law=1, k1=0.5))  # velocity with k(T)
+    N = g.n_dofs
+    g.set_linearization(cuda(np.zeros(N)), cuda(np.zeros(N)))
+    H.JacobiPreconditioner(g).update()
+    with pytest.raises(H.ExcInvalidArgument):
+        H.LinearSolver.solve(g, g.new_vector(), cuda(np.ones(N)), H.LinearSolverData(
+            preconditioner_type=L.PRECOND_MG_F32), True)
+    g2 = H.HeatDiffuseOperator(H.box_mesh(2, (3, 3, 3)))
+    g2.set_material(H.material(law=3, rho_s=0.5))
+    g2.reset_time_increment(1e-2)
+    with pytest.raises(H.ExcInvalidArgument):
+        g2.vmult(g2.new_vector(), g2.new_vector())  # gas-liquid law without a heaviside

@@ -131,3 +131,91 @@ def test_laser_profiles_follow_their_formulas():
     outside = (depth >= 0.5) | (depth < 0.0) | (dist > 0.6)
     assert np.all(g[outside] == 0.0) and np.all(np.isfinite(g))
     assert np.abs(g[~outside]).max() > 0.0
+
+
+GAS_LIQUID = dict(rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3)
+
+
+def transport_fields(o, velocity=True):
+    x = o.support_points()
+    H = 0.5 + 0.5 * np.tanh((x[:, 0] - 0.45) / 0.1)
+    V = np.stack([np.sin(3 * x[:, 1]), 0.5 + x[:, 2], -x[:, 0] * x[:, 1]]) if velocity else None
+    return H, V
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+@pytest.mark.parametrize("sharp,vs", [(False, False), (True, False), (False, True)])
+def test_two_phase_transport_forms_agree(degree, perturb, sharp, vs):
+    """Gas-liquid law on a heaviside field plus convection: both forms agree, the
+    residual is the affine counterpart of the tangent (the law is linear in T) and the
+    Picard form equals the tangent (no temperature derivatives)."""
+    o = O.Oracle(degree, (3, 2, 3), perturb=perturb, seed=7, hi=(1.0, 1.3, 0.8))
+    o.set_material(O.material(O.LAW_GAS_LIQUID, sharp=sharp, volume_specific=vs, **GAS_LIQUID), 1e-2)
+    o.set_fields(*transport_fields(o))
+    rng = np.random.default_rng(degree)
+    u = rng.standard_normal(o.n_dofs)
+    a = o.vmult(u, form=0)
+    assert np.abs(a - o.vmult(u, form=1)).max() <= 1e-13 * np.abs(a).max()
+    assert np.array_equal(a, o.vmult(u, form=2))
+    da, db = o.inverse_diagonal(form=0), o.inverse_diagonal(form=1)
+    assert np.allclose(1 / da, 1 / db, rtol=1e-12, atol=0)
+    T, To = rng.standard_normal(o.n_dofs), rng.standard_normal(o.n_dofs)
+    u[o.mask().astype(bool)] = 0.0
+    lin = o.create_rhs(T, To) - o.create_rhs(T + u, To)
+    assert np.abs(lin - o.vmult(u)).max() <= 1e-12 * np.abs(lin).max()
+
+
+def test_diagonal_of_the_convective_operator_matches_its_columns():
+    o = O.Oracle(2, (2, 2, 2), perturb=0.2, seed=4)
+    o.set_material(O.material(O.LAW_GAS_LIQUID, **GAS_LIQUID), 1e-2)
+    o.set_fields(*transport_fields(o))
+    N = o.n_dofs
+    m = o.mask().astype(bool)
+    col = np.array([o.vmult(np.eye(N)[i])[i] for i in range(N)])
+    inv = o.inverse_diagonal()
+    assert np.allclose(inv[~m], 1 / col[~m], rtol=1e-13, atol=0) and np.all(inv[m] == 1.0)
+
+
+def test_convection_of_a_linear_field():
+    """Constant velocity v and T = a.x with T_old = T: the interior residual rows are
+    -rho_cp (v.a) int(phi_i) (the diffusive part integrates to zero there)."""
+    for degree, perturb in [(2, 0.2), (3, 0.15)]:
+        o = O.Oracle(degree, (3, 4, 3), perturb=perturb)
+        x = o.support_points()
+        a, v = np.array([0.7, -1.1, 0.4]), np.array([1.0, 2.0, -3.0])
+        T = x @ a
+        o.set_material(O.material(rho=2.0, cp=3.0, k=5.0), 1e-2)
+        o.set_fields(None, np.tile(v[:, None], (1, o.n_dofs)))
+        r = o.create_rhs(T, T)
+        o.set_fields(None, None)
+        int_phi = o.create_rhs(0 * T, 0 * T, heat_source=np.ones(o.n_dofs))
+        inner = o.mask() == 0
+        assert np.abs(r[inner] + 6.0 * (v @ a) * int_phi[inner]).max() <= 1e-13 * np.abs(r).max()
+
+
+@pytest.mark.parametrize("sharp,vs", [(False, False), (True, False), (False, True), (True, True)])
+def test_uniform_heaviside_mixes_the_phase_properties(sharp, vs):
+    """A uniform heaviside H = 0.3 gives the constant law with the mixed properties
+    (1 - w) gas + w liquid, w = H or H > 0.5 (material.templates.hpp:240-295, :515-524)."""
+    g = GAS_LIQUID
+    o = O.Oracle(2, (3, 3, 2), perturb=0.1, seed=3)
+    u = np.random.default_rng(0).standard_normal(o.n_dofs)
+    o.set_material(O.material(O.LAW_GAS_LIQUID, sharp=sharp, volume_specific=vs, **g), 1e-2)
+    o.set_fields(np.full(o.n_dofs, 0.3), None)
+    a = o.vmult(u)
+    w = 0.0 if sharp else 0.3
+    mix = lambda liq, gas: (1 - w) * gas + w * liq
+    k = mix(g["k"], g["k_s"])
+    rhocp = mix(g["rho"] * g["cp"], g["rho_s"] * g["cp_s"]) if vs else \
+        mix(g["rho"], g["rho_s"]) * mix(g["cp"], g["cp_s"])
+    o.set_fields(None, None)
+    o.set_material(O.material(rho=rhocp, cp=1.0, k=k), 1e-2)
+    assert np.abs(a - o.vmult(u)).max() <= 1e-13 * np.abs(a).max()
+
+
+def test_velocity_needs_a_temperature_independent_law():
+    o = O.Oracle(1, (2, 2, 2))
+    o.set_material(O.material(O.LAW_LINEAR_K, k1=0.5), 1e-2)
+    with pytest.raises(ValueError):
+        o.set_fields(None, np.zeros((3, o.n_dofs)))

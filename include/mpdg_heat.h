@@ -61,7 +61,7 @@ typedef struct {
 } mpdg_mesh_desc;
 
 enum { MPDG_LAW_CONSTANT = 0, MPDG_LAW_LINEAR_K = 1, MPDG_LAW_LIQUID_SOLID = 2,
-       MPDG_LAW_GAS_LIQUID = 3 };
+       MPDG_LAW_GAS_LIQUID = 3, MPDG_LAW_GAS_LIQUID_SOLID = 4 };
 
 /* Material law (Material::compute_parameters, material.templates.hpp:104-137,226-375):
  *   CONSTANT      rho*cp and k constant (material type gas / liquid)
@@ -69,16 +69,20 @@ enum { MPDG_LAW_CONSTANT = 0, MPDG_LAW_LINEAR_K = 1, MPDG_LAW_LIQUID_SOLID = 2,
  *   LIQUID_SOLID  cubic smoothstep in the solid fraction between liquid and solid values,
  *                 mushy zone or sharp transition (material.templates.hpp:296-375,745-780)
  *   GAS_LIQUID    (1 - w) gas + w liquid with w = H (smooth) or H > 0.5 (sharp), H the
- *                 level-set heaviside field of mpdg_heat_set_fields; the *_s members hold
- *                 the gas values (material.templates.hpp:240-295,515-524) */
+ *                 level-set heaviside field of mpdg_heat_set_fields
+ *                 (material.templates.hpp:240-295,515-524)
+ *   GAS_LIQUID_SOLID  (1 - w) gas + w liquid_solid(T), temperature derivatives w d/dT
+ *                 liquid_solid (material.templates.hpp:376-500,620-740) */
 typedef struct {
   int    law;
-  int    sharp;            /* LIQUID_SOLID: 0 mushy zone, 1 sharp; GAS_LIQUID: 0 smooth, 1 sharp */
+  int    sharp;            /* liquid-solid transition: 0 mushy zone, 1 sharp         */
   int    volume_specific;  /* interpolate rho*cp directly (heat_data diffuse option) */
   double rho_l, cp_l, k_l; /* liquid, or the single constant phase                   */
-  double rho_s, cp_s, k_s; /* solid (GAS_LIQUID: gas)                                */
+  double rho_s, cp_s, k_s; /* solid                                                  */
   double T_solidus, T_liquidus;
   double k1;
+  int    sharp_gas_liquid; /* gas-liquid transition: 0 smooth (w = H), 1 sharp        */
+  double rho_g, cp_g, k_g; /* gas (GAS_LIQUID, GAS_LIQUID_SOLID)                      */
 } mpdg_material;
 
 enum { MPDG_SOLVER_CG = 0, MPDG_SOLVER_GMRES = 1 };           /* LinearSolverType  */
@@ -148,10 +152,12 @@ int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m);
 /* Two-phase and transport fields of HeatDiffuseMultiPhaseOperator (its level_set_as_heaviside
  * and velocity vectors, heat_diffuse_operator.cpp:47-72): device vectors on this handle's
  * DoFs, caller-owned, read when the per-quadrature-point coefficients are built.
- *   heaviside  n_dofs values, weights the GAS_LIQUID law (NULL: liquid properties)
+ *   heaviside  n_dofs values, weights the GAS_LIQUID and GAS_LIQUID_SOLID laws (required
+ *              by them)
  *   velocity   3 x n_dofs, component-major (x block, y block, z block) or NULL; adds
  *              rho_cp v.grad(T) to the residual and rho_cp v.grad(u) to the tangent and its
- *              diagonal (:499-500, :1038-1042); allowed with the CONSTANT and GAS_LIQUID laws
+ *              diagonal (:499-500, :1038-1042), with a temperature-dependent law also
+ *              d(rho_cp)/dT (v.grad T_lin) u (:1044-1049); not allowed with LINEAR_K
  * The coefficients are rebuilt at the next operator call after set_fields or set_material:
  * call set_fields again after changing the vectors' contents.  With a velocity the operator
  * is nonsymmetric (use MPDG_SOLVER_GMRES); the multigrid preconditioner is not available

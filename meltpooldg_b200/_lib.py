@@ -25,7 +25,7 @@ ERR_ZERO_TIME_INCREMENT = 7
 ERR_NEWTON_NOT_CONVERGED = 8
 ERR_NOT_SUPPORTED = 9
 
-LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID = 0, 1, 2, 3
+LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID, LAW_GAS_LIQUID_SOLID = 0, 1, 2, 3, 4
 SOLVER_CG, SOLVER_GMRES = 0, 1
 PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_CHEBYSHEV_JACOBI_F32, PRECOND_MG_F32 = 0, 1, 2, 3
 PREDICTOR_NONE, PREDICTOR_LINEAR, PREDICTOR_GIVEN = 0, 1, 2
@@ -41,7 +41,9 @@ class Material(C.Structure):
     _fields_ = [("law", C.c_int), ("sharp", C.c_int), ("volume_specific", C.c_int),
                 ("rho_l", C.c_double), ("cp_l", C.c_double), ("k_l", C.c_double),
                 ("rho_s", C.c_double), ("cp_s", C.c_double), ("k_s", C.c_double),
-                ("T_solidus", C.c_double), ("T_liquidus", C.c_double), ("k1", C.c_double)]
+                ("T_solidus", C.c_double), ("T_liquidus", C.c_double), ("k1", C.c_double),
+                ("sharp_gas_liquid", C.c_int),
+                ("rho_g", C.c_double), ("cp_g", C.c_double), ("k_g", C.c_double)]
 
 
 class SolverParams(C.Structure):

@@ -17,7 +17,7 @@ struct MeshDims {
 
 template <typename T>
 struct MatParams {
-  T rho_l, cp_l, k_l, rho_s, cp_s, k_s;
+  T rho_l, cp_l, k_l, rho_s, cp_s, k_s, rho_g, cp_g, k_g;
   T T_liq, T_sol, inv_mushy, k1;
   T idt;
   int sharp, vs, need_told;
@@ -54,8 +54,9 @@ struct CellArgs {
   const T *__restrict__ To;
   const T *__restrict__ qs;
   const float *__restrict__ kq;  // per-q conductivity [cell][n^3] (coefficient-field operator)
-  // per-q coefficients of the two-phase / convective operator (LAW 4), [cell][5][n^3]:
-  // rho_cp JxW, k, and JxW rho_cp J^-1 v (three components)
+  // per-q coefficient fields, [cell][5][n^3]. LAW 4 (temperature-independent laws):
+  // rho_cp JxW, k, JxW rho_cp J^-1 v (three components); LAW 5 (temperature-dependent
+  // laws with a heaviside and/or a velocity): gas-liquid weight w, 0, JxW J^-1 v
   const T *__restrict__ cf;
   double *partials;    // per-CTA partial sums
   unsigned *counter;   // last-CTA election counter (reset by the last CTA)

@@ -21,7 +21,9 @@
 // (both with their tangent terms at T_lin), 3 a per-q FP32 conductivity field (the Picard
 // operator of the preconditioner, register-resident kernel only), 4 per-q coefficient
 // fields a.cf (gas-liquid law weighted by the level-set heaviside and/or the convective
-// term rho_cp v.grad, heat_diffuse_operator.cpp:499-500 and :1038-1042).
+// term rho_cp v.grad, heat_diffuse_operator.cpp:499-500 and :1038-1042), 5 the liquid-solid
+// law at T_lin mixed with the gas by a per-q weight, with the convective terms including
+// d(rho_cp)/dT (v.grad T_lin) u (:1044-1049) (three-phase law, liquid-solid with velocity).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -55,7 +57,9 @@ template <> __device__ __forceinline__ float cw<float>(int i) { return c_w_f[i];
 template <typename T> __device__ __forceinline__ void atomic_add(T *p, T v) { atomicAdd(p, v); }
 
 // laws whose coefficients depend on the linearisation point T_lin
-template <int LAW> __host__ __device__ constexpr bool law_tdep() { return LAW == 1 || LAW == 2; }
+template <int LAW> __host__ __device__ constexpr bool law_tdep() { return LAW == 1 || LAW == 2 || LAW == 5; }
+// laws that may need T_old (d(rho_cp)/dT (T_lin - T_old) / dt in the tangent)
+template <int LAW> __host__ __device__ constexpr bool law_told() { return LAW == 2 || LAW == 5; }
 
 // Material::compute_parameters for the three laws; LAW is a template constant.
 template <int LAW, typename T>
@@ -96,6 +100,40 @@ __device__ __forceinline__ void mat_eval(const MatParams<T> &m, T temp, T &rhocp
       rhocp = rho * cp;
       drhocp = dcp * rho + drho * cp;
     }
+  }
+}
+
+// Three-phase law (Material::compute_parameters, gas_liquid_solid,
+// material.templates.hpp:376-500, 620-740): every property is (1 - w) gas + w ls(T) with
+// ls the liquid-solid interpolation of mat_eval<2>, its T derivative w dls/dT; w = 1 gives
+// the liquid-solid law exactly.
+template <typename T>
+__device__ __forceinline__ void mat_eval_w(const MatParams<T> &m, T temp, T w, T &rhocp, T &k,
+                                           T &drhocp, T &dk)
+{
+  T sf;
+  if (m.sharp)
+    sf = temp < m.T_sol ? T(1) : T(0);
+  else {
+    sf = (m.T_liq - temp) * m.inv_mushy;
+    sf = sf < T(0) ? T(0) : (sf > T(1) ? T(1) : sf);
+  }
+  const T hs = T(-2) * sf * sf * sf + T(3) * sf * sf;
+  const T dhs = T(-6) * sf * sf + T(6) * sf;
+  const bool edge = (sf == T(0) || sf == T(1));
+  auto prop = [&](T l, T s) { return sf == T(0) ? l : (sf == T(1) ? s : l + (s - l) * hs); };
+  auto dprop = [&](T l, T s) { return edge ? T(0) : T(-1) * m.inv_mushy * ((s - l) * dhs); };
+  const T g = T(1) - w;
+  k = g * m.k_g + w * prop(m.k_l, m.k_s);
+  dk = w * dprop(m.k_l, m.k_s);
+  if (m.vs) {
+    rhocp = g * (m.rho_g * m.cp_g) + w * prop(m.rho_l * m.cp_l, m.rho_s * m.cp_s);
+    drhocp = w * dprop(m.rho_l * m.cp_l, m.rho_s * m.cp_s);
+  } else {
+    const T rho = g * m.rho_g + w * prop(m.rho_l, m.rho_s);
+    const T cp = g * m.cp_g + w * prop(m.cp_l, m.cp_s);
+    drhocp = (w * dprop(m.cp_l, m.cp_s)) * rho + (w * dprop(m.rho_l, m.rho_s)) * cp;
+    rhocp = rho * cp;
   }
 }
 
@@ -278,7 +316,7 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
     for (int i = 0; i < n; ++i) u[i + n * line] = xs[i];
     if (TDEP) {
       T xt[n];
-      if (LAW == 2 && a.m.need_told) {
+      if (law_told<LAW>() && a.m.need_told) {
         gather_xline<n>(d, row, I0, J, K, false, a.To, xt, active);
 #pragma unroll
         for (int i = 0; i < n; ++i) Tq[i + n * line] = xt[i];
@@ -290,7 +328,7 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
     __syncthreads();
     if (TDEP) {
       // T_lin values + gradients: t1 -> (S) -> Tq; old values first if needed
-      if (LAW == 2 && a.m.need_told) {
+      if (law_told<LAW>() && a.m.need_told) {
         eval_values<n>(Tq, gx, gy, Toq, line);
       }
       eval_values<n>(t1, gx, gy, Tq, line);
@@ -307,8 +345,14 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
       geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
       T rhocp, kk, drhocp, dk;
       const T uu = u[q];
-      T val;
-      if (LAW == 4) {
+      T val, b0 = T(0), b1 = T(0), b2 = T(0);
+      if (LAW == 5) {
+        const T *cf = a.cf + cc * 5 * n3 + q;
+        mat_eval_w(a.m, Tq[q], __ldg(cf), rhocp, kk, drhocp, dk);
+        b0 = __ldg(cf + 2 * n3);
+        b1 = __ldg(cf + 3 * n3);
+        b2 = __ldg(cf + 4 * n3);
+      } else if (LAW == 4) {
         const T *cf = a.cf + cc * 5 * n3 + q;
         kk = __ldg(cf + n3);
         rhocp = drhocp = dk = T(0);
@@ -320,12 +364,15 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
       T cval = a.m.idt * rhocp;
       T f0 = kk * gx[q], f1 = kk * gy[q], f2 = kk * gz[q];
       if (TDEP) {
-        if (LAW == 2 && a.m.need_told) cval += a.m.idt * drhocp * (Tq[q] - Toq[q]);
+        if (law_told<LAW>() && a.m.need_told) cval += a.m.idt * drhocp * (Tq[q] - Toq[q]);
         f0 += dk * Tx[q] * uu;
         f1 += dk * Ty[q] * uu;
         f2 += dk * Tz[q] * uu;
       }
-      u[q] = LAW == 4 ? val : cval * uu * jxw;
+      if (LAW == 5)  // rho_cp b.grad(u) + d(rho_cp)/dT (b.grad T) u, b = JxW J^-1 v
+        val = cval * uu * jxw + rhocp * (b0 * gx[q] + b1 * gy[q] + b2 * gz[q]) +
+              drhocp * (b0 * Tx[q] + b1 * Ty[q] + b2 * Tz[q]) * uu;
+      u[q] = (LAW == 4 || LAW == 5) ? val : cval * uu * jxw;
       T F0, F1, F2;
       apply_G<GEO>(G, f0, f1, f2, F0, F1, F2);
       gx[q] = F0;
@@ -418,7 +465,13 @@ __global__ void __launch_bounds__(block_threads(n)) k_rhs(CellArgs<double> a)
       T jxw, G[6];
       geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
       T rhocp, kk, drhocp, dk, valw;
-      if (LAW == 4) {
+      if (LAW == 5) {
+        const T *cf = a.cf + cc * 5 * n3 + q;
+        mat_eval_w(a.m, tq[q], __ldg(cf), rhocp, kk, drhocp, dk);
+        valw = (a.m.idt * rhocp * (tq[q] - Toq[q]) - Sq[q]) * jxw +
+               rhocp * (__ldg(cf + 2 * n3) * gx[q] + __ldg(cf + 3 * n3) * gy[q] +
+                        __ldg(cf + 4 * n3) * gz[q]);
+      } else if (LAW == 4) {
         // rho_cp (T - T_old) / dt - q + rho_cp grad(T).v, times JxW
         const T *cf = a.cf + cc * 5 * n3 + q;
         kk = __ldg(cf + n3);
@@ -485,13 +538,13 @@ __global__ void __launch_bounds__(block_threads(n)) k_diag(CellArgs<double> a)
       gather_xline<n>(d, row, I0, J, K, false, a.Tl, x, active);
 #pragma unroll
       for (int i = 0; i < n; ++i) A[i + n * line] = x[i];
-      if (LAW == 2 && a.m.need_told) {
+      if (law_told<LAW>() && a.m.need_told) {
         gather_xline<n>(d, row, I0, J, K, false, a.To, x, active);
 #pragma unroll
         for (int i = 0; i < n; ++i) W[i + n * line] = x[i];
       }
       __syncthreads();
-      if (LAW == 2 && a.m.need_told) eval_values<n>(W, X, Y, C0, line);  // T_old values -> C0
+      if (law_told<LAW>() && a.m.need_told) eval_values<n>(W, X, Y, C0, line);  // T_old values -> C0
       eval_values<n>(A, X, Y, Tq, line);
       eval_gradients<n>(Tq, Bx, By, Bz, line);
     }
@@ -502,16 +555,21 @@ __global__ void __launch_bounds__(block_threads(n)) k_diag(CellArgs<double> a)
       T jxw, G[6];
       geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
       T rhocp, kk, drhocp, dk;
-      const T *cf = LAW == 4 ? a.cf + cc * 5 * n3 + q : nullptr;
+      const T *cf = (LAW == 4 || LAW == 5) ? a.cf + cc * 5 * n3 + q : nullptr;
       if (LAW == 4) {
         kk = __ldg(cf + n3);
         rhocp = drhocp = dk = T(0);
+      } else if (LAW == 5) {
+        mat_eval_w(a.m, Tq[q], __ldg(cf), rhocp, kk, drhocp, dk);
       } else {
         mat_eval<LAW>(a.m, TDEP ? Tq[q] : T(0), rhocp, kk, drhocp, dk);
       }
       T cval = LAW == 4 ? T(0) : a.m.idt * rhocp;
-      if (TDEP && LAW == 2 && a.m.need_told) cval += a.m.idt * drhocp * (Tq[q] - C0[q]);
+      if (TDEP && law_told<LAW>() && a.m.need_told) cval += a.m.idt * drhocp * (Tq[q] - C0[q]);
       C0[q] = LAW == 4 ? a.m.idt * __ldg(cf) : cval * jxw;
+      if (LAW == 5)  // d(rho_cp)/dT (b.grad T_lin) u is a mass-like term
+        C0[q] += drhocp * (__ldg(cf + 2 * n3) * Bx[q] + __ldg(cf + 3 * n3) * By[q] +
+                           __ldg(cf + 4 * n3) * Bz[q]);
       Gxx[q] = kk * G[0];
       Gxy[q] = T(2) * kk * G[1];
       Gxz[q] = T(2) * kk * G[2];
@@ -527,6 +585,11 @@ __global__ void __launch_bounds__(block_threads(n)) k_diag(CellArgs<double> a)
         Bx[q] = dk * b0;
         By[q] = dk * b1;
         Bz[q] = dk * b2;
+        if (LAW == 5) {  // convection: phi_i rho_cp (JxW J^-1 v).grad_ref(phi_i)
+          Bx[q] += rhocp * __ldg(cf + 2 * n3);
+          By[q] += rhocp * __ldg(cf + 3 * n3);
+          Bz[q] += rhocp * __ldg(cf + 4 * n3);
+        }
       } else if (LAW == 4) {
         // convection: phi_i (JxW rho_cp J^-1 v).grad_ref(phi_i)
         Bx[q] = __ldg(cf + 2 * n3);

@@ -63,17 +63,18 @@ struct DegreeOps {
 
   // register-resident kernel where a cell's planes fit the register file (FP64 at
   // p = 4 spills 64-750 bytes there and measured no faster than the line-per-thread
-  // kernel on the deformed mesh, so it stays on the latter)
+  // kernel on the deformed mesh, so it stays on the latter); the three-phase / transport
+  // law with temperature dependence (LAW 5) runs the line-per-thread kernel
   template <typename T, int LAW = 0>
   static constexpr bool use_v2()
   {
-    return sizeof(T) == 8 ? n <= 4 : n <= 5;
+    return LAW != 5 && (sizeof(T) == 8 ? n <= 4 : n <= 5);
   }
 
   template <typename T, int GEO, int LAW>
   static cudaError_t vmult_t(const CellArgs<T> &a, cudaStream_t s, int sm)
   {
-    if constexpr (std::is_same<T, float>::value && n <= 4 && LAW != 2 && LAW != 4) {
+    if constexpr (std::is_same<T, float>::value && n <= 4 && (LAW == 0 || LAW == 1 || LAW == 3)) {
       if (fp32_packed()) {
         static int cachep = 0;
         auto kp = k_vmult2p<n, GEO, LAW>;
@@ -115,6 +116,7 @@ struct DegreeOps {
       }
     }
     if (law == 4) return geo == 0 ? vmult_t<T, 0, 4>(a, s, sm) : vmult_t<T, 1, 4>(a, s, sm);
+    if (law == 5) return geo == 0 ? vmult_t<T, 0, 5>(a, s, sm) : vmult_t<T, 1, 5>(a, s, sm);
     if (geo == 0) {
       if (law == 0) return vmult_t<T, 0, 0>(a, s, sm);
       if (law == 1) return vmult_t<T, 0, 1>(a, s, sm);
@@ -157,6 +159,7 @@ struct DegreeOps {
   static cudaError_t rhs(const CellArgs<double> &a, int geo, int law, cudaStream_t s, int sm)
   {
     if (law == 4) return geo == 0 ? rhs_t<0, 4>(a, s, sm) : rhs_t<1, 4>(a, s, sm);
+    if (law == 5) return geo == 0 ? rhs_t<0, 5>(a, s, sm) : rhs_t<1, 5>(a, s, sm);
     if (geo == 0) {
       if (law == 0) return rhs_t<0, 0>(a, s, sm);
       if (law == 1) return rhs_t<0, 1>(a, s, sm);
@@ -180,6 +183,7 @@ struct DegreeOps {
   static cudaError_t diag(const CellArgs<double> &a, int geo, int law, cudaStream_t s, int sm)
   {
     if (law == 4) return geo == 0 ? diag_t<0, 4>(a, s, sm) : diag_t<1, 4>(a, s, sm);
+    if (law == 5) return geo == 0 ? diag_t<0, 5>(a, s, sm) : diag_t<1, 5>(a, s, sm);
     if (geo == 0) {
       if (law == 0) return diag_t<0, 0>(a, s, sm);
       if (law == 1) return diag_t<0, 1>(a, s, sm);

@@ -304,7 +304,9 @@ __global__ void k_geometry(int64_t n_cells, MeshDims d, int n, Q1D q1, const dou
 }
 
 // Per-quadrature-point coefficients of the gas-liquid / convective operator,
-// cf[cell][5][npt] = {rho_cp JxW, k, JxW rho_cp J^-1 v}: the heaviside and velocity fields
+// cf[cell][5][npt] = {rho_cp JxW, k, JxW rho_cp J^-1 v} (mode 4; mode 5, for the laws that
+// depend on T_lin, stores {w, 0, JxW J^-1 v} and the cell kernels evaluate the liquid-solid
+// law and mix it with the gas by w): the heaviside and velocity fields
 // are interpolated at the point (FEEvaluation::evaluate(values) on the nodal vectors,
 // heat_diffuse_operator.cpp:448-473), the gas-liquid law mixes the phase properties with
 // w = H (smooth) or w = (H > 0.5) (sharp): (1 - w) gas + w liquid
@@ -316,7 +318,7 @@ __global__ void k_geometry(int64_t n_cells, MeshDims d, int n, Q1D q1, const dou
 // n^3-term sum (a set-up pass, run when the fields or the material change).
 struct FieldArgs {
   MeshDims d;
-  int n, geo;
+  int n, geo, mode;
   int64_t n_cells, n_dofs;
   double hc[3];
   double xg[8], wg[8], S[8][8];
@@ -376,10 +378,11 @@ __global__ void k_coef_fields(FieldArgs a)
     }
     const double jxw = det * a.wg[qi] * a.wg[qj] * a.wg[qk];
     double *o = a.cf + c * 5 * npt + q;
-    o[0] = rhocp * jxw;
-    o[npt] = kk;
+    const double s = a.mode == 5 ? jxw : jxw * rhocp;
+    o[0] = a.mode == 5 ? w : rhocp * jxw;
+    o[npt] = a.mode == 5 ? 0.0 : kk;
     for (int e = 0; e < 3; ++e)
-      o[(2 + e) * npt] = jxw * rhocp * (inv[e][0] * v[0] + inv[e][1] * v[1] + inv[e][2] * v[2]);
+      o[(2 + e) * npt] = s * (inv[e][0] * v[0] + inv[e][1] * v[1] + inv[e][2] * v[2]);
   }
 }
 
@@ -1132,6 +1135,9 @@ static CellArgs<T> cell_args(mpdg_heat *h)
   a.m.rho_s = (T)m.rho_s;
   a.m.cp_s = (T)m.cp_s;
   a.m.k_s = (T)m.k_s;
+  a.m.rho_g = (T)m.rho_g;
+  a.m.cp_g = (T)m.cp_g;
+  a.m.k_g = (T)m.k_g;
   a.m.T_liq = (T)m.T_liquidus;
   a.m.T_sol = (T)m.T_solidus;
   a.m.inv_mushy = (T)(m.T_liquidus != m.T_solidus ? 1.0 / (m.T_liquidus - m.T_solidus) : 0.0);
@@ -1153,22 +1159,27 @@ static int ensure_dt(mpdg_heat *h)
   return MPDG_OK;
 }
 
-// the cell kernels' law: the public laws 0-2, or 4 (coefficient fields) for the gas-liquid
-// law and for any law with a velocity field
+// the cell kernels' law: the public laws 0-2; 4 (coefficient fields) for the gas-liquid law
+// and the constant law with a velocity; 5 (liquid-solid law at T_lin mixed with the gas by a
+// per-point weight, convection included) for the three-phase law and the liquid-solid law
+// with a velocity (a velocity with the linear-k law is rejected)
 static int klaw(const mpdg_heat *h)
 {
-  return (h->law == MPDG_LAW_GAS_LIQUID || h->vel) ? 4 : h->law;
+  if (h->law == MPDG_LAW_GAS_LIQUID_SOLID || (h->law == MPDG_LAW_LIQUID_SOLID && h->vel)) return 5;
+  if (h->law == MPDG_LAW_GAS_LIQUID || h->vel) return 4;
+  return h->law;
 }
 
 static bool law_tdep(const mpdg_heat *h)
 {
-  return h->law == MPDG_LAW_LINEAR_K || h->law == MPDG_LAW_LIQUID_SOLID;
+  return h->law == MPDG_LAW_LINEAR_K || h->law == MPDG_LAW_LIQUID_SOLID ||
+         h->law == MPDG_LAW_GAS_LIQUID_SOLID;
 }
 
 // (re)build the per-q coefficient fields when the operator uses them
 static int ensure_fields(mpdg_heat *h)
 {
-  if (klaw(h) != 4 || !h->cf_dirty) return MPDG_OK;
+  if (klaw(h) < 4 || !h->cf_dirty) return MPDG_OK;
   TRY(dvec(h, &h->cf, h->n_cells * 5 * h->npt));
   const Tables1D t1 = make_tables(h->n);
   FieldArgs a;
@@ -1176,6 +1187,7 @@ static int ensure_fields(mpdg_heat *h)
   a.d = h->dims;
   a.n = h->n;
   a.geo = h->geo;
+  a.mode = klaw(h);
   a.n_cells = h->n_cells;
   a.n_dofs = h->n_dofs;
   for (int e = 0; e < 3; ++e) a.hc[e] = h->hcell[e];
@@ -1187,15 +1199,15 @@ static int ensure_fields(mpdg_heat *h)
   a.vert = h->vert;
   a.H = h->Hf;
   a.vel = h->vel;
-  a.mix = h->law == MPDG_LAW_GAS_LIQUID;
-  a.sharp = h->mat.sharp;
+  a.mix = h->law == MPDG_LAW_GAS_LIQUID || h->law == MPDG_LAW_GAS_LIQUID_SOLID;
+  a.sharp = h->mat.sharp_gas_liquid;
   a.vs = h->mat.volume_specific;
   a.rho_l = h->mat.rho_l;
   a.cp_l = h->mat.cp_l;
   a.k_l = h->mat.k_l;
-  a.rho_g = h->mat.rho_s;
-  a.cp_g = h->mat.cp_s;
-  a.k_g = h->mat.k_s;
+  a.rho_g = h->mat.rho_g;
+  a.cp_g = h->mat.cp_g;
+  a.k_g = h->mat.k_g;
   a.cf = h->cf;
   const int64_t total = h->n_cells * h->npt;
   k_coef_fields<<<vgrid(h, total), VT, 0, h->stream>>>(a); ++h->launches;
@@ -1209,9 +1221,10 @@ static int ensure_lin(mpdg_heat *h)
 {
   if (law_tdep(h) && !h->T_lin)
     return fail(MPDG_ERR_INVALID_ARGUMENT, "temperature-dependent law needs set_linearization");
-  if (h->law == MPDG_LAW_GAS_LIQUID && !h->Hf)
-    return fail(MPDG_ERR_INVALID_ARGUMENT, "gas-liquid law needs a heaviside field (set_fields)");
-  if (h->law == MPDG_LAW_LIQUID_SOLID && h->need_told && !h->T_old)
+  if ((h->law == MPDG_LAW_GAS_LIQUID || h->law == MPDG_LAW_GAS_LIQUID_SOLID) && !h->Hf)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "gas-liquid laws need a heaviside field (set_fields)");
+  if ((h->law == MPDG_LAW_LIQUID_SOLID || h->law == MPDG_LAW_GAS_LIQUID_SOLID) && h->need_told &&
+      !h->T_old)
     return fail(MPDG_ERR_INVALID_ARGUMENT, "liquid-solid law needs temperature_old");
   return MPDG_OK;
 }
@@ -1320,7 +1333,7 @@ static int refresh_f32(mpdg_heat *h)
     k_cast_f<<<vgrid(h, ng), VT, 0, h->stream>>>(ng, h->geoq, h->geoq_f); ++h->launches;
     CU(cudaGetLastError());
   }
-  if (klaw(h) == 4 && h->cf_f_dirty) {
+  if (klaw(h) >= 4 && h->cf_f_dirty) {
     TRY(ensure_fields(h));
     const int64_t nc = h->n_cells * 5 * h->npt;
     TRY(dvec(h, &h->cf_f, nc));
@@ -1865,9 +1878,9 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
 {
   const int64_t N = h->n_dofs;
   const bool use_mg = prm->preconditioner == MPDG_PRECOND_MG_F32;
-  if (use_mg && klaw(h) == 4)
+  if (use_mg && klaw(h) >= 4)
     return fail(MPDG_ERR_INVALID_ARGUMENT,
-                "multigrid preconditioner: not available with the gas-liquid law or a velocity field");
+                "multigrid preconditioner: not available with the gas-liquid laws or a velocity field");
   const bool picard = prm->cheb_picard && h->law == MPDG_LAW_LINEAR_K && h->tab.conductivity_q;
   // the FP64 inverse diagonal feeds the Lanczos estimate and the Chebyshev smoother; the
   // multigrid smoothers of the Picard operator use that operator's own FP32 diagonal
@@ -2322,6 +2335,7 @@ static int create_impl(const mpdg_mesh_desc *desc, int device, const std::vector
   m0.law = MPDG_LAW_CONSTANT;
   m0.rho_l = m0.cp_l = m0.k_l = 1.0;
   m0.rho_s = m0.cp_s = m0.k_s = 1.0;
+  m0.rho_g = m0.cp_g = m0.k_g = 1.0;
   m0.T_liquidus = 1.0;
   h->mat = m0;
   *out = h;
@@ -2376,16 +2390,16 @@ extern "C" int mpdg_heat_device_bytes(const mpdg_heat *h, int64_t *bytes)
 extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
 {
   if (!h || !m) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
-  if (m->law < 0 || m->law > 3) return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown material law");
-  if (h->vel && (m->law == MPDG_LAW_LINEAR_K || m->law == MPDG_LAW_LIQUID_SOLID))
-    return fail(MPDG_ERR_INVALID_ARGUMENT,
-                "a velocity field needs the constant or the gas-liquid law");
-  if (m->law == MPDG_LAW_LIQUID_SOLID && !m->sharp && !(m->T_liquidus > m->T_solidus))
+  if (m->law < 0 || m->law > 4) return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown material law");
+  if (h->vel && m->law == MPDG_LAW_LINEAR_K)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "a velocity field is not available with the linear-k law");
+  if ((m->law == MPDG_LAW_LIQUID_SOLID || m->law == MPDG_LAW_GAS_LIQUID_SOLID) && !m->sharp &&
+      !(m->T_liquidus > m->T_solidus))
     return fail(MPDG_ERR_INVALID_ARGUMENT, "liquidus must exceed solidus");
   h->mat = *m;
   h->law = m->law;
   h->need_told = 0;
-  if (m->law == MPDG_LAW_LIQUID_SOLID)
+  if (m->law == MPDG_LAW_LIQUID_SOLID || m->law == MPDG_LAW_GAS_LIQUID_SOLID)
     h->need_told = m->volume_specific ? (m->rho_l * m->cp_l != m->rho_s * m->cp_s)
                                       : (m->rho_l != m->rho_s || m->cp_l != m->cp_s);
   h->diag_valid = false;
@@ -2397,9 +2411,8 @@ extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
 extern "C" int mpdg_heat_set_fields(mpdg_heat *h, const double *heaviside, const double *velocity)
 {
   if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
-  if (velocity && (h->law == MPDG_LAW_LINEAR_K || h->law == MPDG_LAW_LIQUID_SOLID))
-    return fail(MPDG_ERR_INVALID_ARGUMENT,
-                "a velocity field needs the constant or the gas-liquid law");
+  if (velocity && h->law == MPDG_LAW_LINEAR_K)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "a velocity field is not available with the linear-k law");
   h->Hf = heaviside;
   h->vel = velocity;
   h->cf_dirty = true;

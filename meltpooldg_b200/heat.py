@@ -104,7 +104,11 @@ def box_mesh(degree, cells, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), perturb=0.0,
 
 
 def material(law=L.LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_s=None, k_s=None,
-             T_solidus=0.0, T_liquidus=1.0, sharp=False, volume_specific=False) -> L.Material:
+             T_solidus=0.0, T_liquidus=1.0, sharp=False, volume_specific=False, rho_g=None,
+             cp_g=None, k_g=None, sharp_gas_liquid=False) -> L.Material:
+    """Material parameters: liquid (rho, cp, k), solid (*_s) and gas (*_g) phases, each
+    defaulting to the liquid values; sharp selects the sharp liquid-solid transition,
+    sharp_gas_liquid the sharp gas-liquid one."""
     m = L.Material()
     m.law = int(law)
     m.sharp = int(sharp)
@@ -114,6 +118,10 @@ def material(law=L.LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_
     m.cp_s = float(cp if cp_s is None else cp_s)
     m.k_s = float(k if k_s is None else k_s)
     m.T_solidus, m.T_liquidus, m.k1 = float(T_solidus), float(T_liquidus), float(k1)
+    m.sharp_gas_liquid = int(sharp_gas_liquid)
+    m.rho_g = float(rho if rho_g is None else rho_g)
+    m.cp_g = float(cp if cp_g is None else cp_g)
+    m.k_g = float(k if k_g is None else k_g)
     return m
 
 

@@ -7,7 +7,9 @@ With --solve it instead runs a few outer iterations of FP64 CG with the FP32
 Chebyshev preconditioner on the Picard operator, so that kernel can be captured.
 With --transport the operator is the two-phase one (gas-liquid law on a heaviside
 field plus the convective term of a velocity field), whose per-point coefficients
-(5 per quadrature point) replace the linearisation point in the traffic.
+(5 per quadrature point) replace the linearisation point in the traffic;
+--transport --law 4 uses the three-phase law (liquid-solid at T_lin mixed with the
+gas), whose traffic adds the linearisation point and T_old.
 """
 from __future__ import annotations
 
@@ -32,8 +34,9 @@ def main():
     a = ap.parse_args()
     op = H.HeatDiffuseOperator(H.box_mesh(a.degree, (a.cells,) * 3, perturb=a.perturb))
     if a.transport:
-        a.law = 3
-        op.set_material(H.material(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3))
+        a.law = 4 if a.law == 4 else 3
+        op.set_material(H.material(law=a.law, rho=2.0, cp=3.0, k=5.0, rho_s=2.2, cp_s=2.5, k_s=4.0,
+                                   T_solidus=0.3, T_liquidus=0.7, rho_g=0.5, cp_g=1.5, k_g=0.3))
     else:
         op.set_material(H.material(law=a.law, k=1.0, k1=0.5))
     op.reset_time_increment(5e-4)
@@ -78,7 +81,7 @@ def main():
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / a.reps
         if a.transport:
-            alg = s * N * 2 + 5 * s * nq + (7 * s * nq if a.perturb > 0 else 0)
+            alg = s * N * (2 + (2 if a.law == 4 else 0)) + 5 * s * nq + (7 * s * nq if a.perturb > 0 else 0)
         else:
             alg = s * N * (2 + (1 if a.law else 0)) + (7 * s * nq if a.perturb > 0 else 0)
         print(json.dumps({"degree": a.degree, "cells": a.cells, "perturb": a.perturb,

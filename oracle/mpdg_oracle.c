@@ -469,27 +469,31 @@ void orc_distribute(const orc_heat *h, double *u)
     if (h->mask[i]) u[i] = h->dvalue[i];
 }
 
-void orc_set_material(orc_heat *h, const orc_material *m, double dt)
+int orc_set_material(orc_heat *h, const orc_material *m, double dt)
 {
+  if (h->vel && m->law == ORC_LAW_LINEAR_K) return -1;
   h->mat = *m;
   h->dt = dt;
-  h->tdep = m->law == ORC_LAW_LINEAR_K || m->law == ORC_LAW_LIQUID_SOLID;
-  h->fields = m->law == ORC_LAW_GAS_LIQUID || h->vel != NULL;
+  h->tdep = m->law == ORC_LAW_LINEAR_K || m->law == ORC_LAW_LIQUID_SOLID ||
+            m->law == ORC_LAW_GAS_LIQUID_SOLID;
+  h->fields = m->law == ORC_LAW_GAS_LIQUID || m->law == ORC_LAW_GAS_LIQUID_SOLID || h->vel != NULL;
   h->need_told = 0;
-  if (m->law == ORC_LAW_LIQUID_SOLID) {
+  if (m->law == ORC_LAW_LIQUID_SOLID || m->law == ORC_LAW_GAS_LIQUID_SOLID) {
     if (m->volume_specific)
       h->need_told = (m->rho_l * m->cp_l != m->rho_s * m->cp_s);
     else
       h->need_told = (m->rho_l != m->rho_s) || (m->cp_l != m->cp_s);
   }
+  return 0;
 }
 
 int orc_set_fields(orc_heat *h, const double *heaviside, const double *velocity)
 {
-  if (velocity && h->tdep) return -1;
+  if (velocity && h->mat.law == ORC_LAW_LINEAR_K) return -1;
   h->Hf = heaviside;
   h->vel = velocity;
-  h->fields = h->mat.law == ORC_LAW_GAS_LIQUID || velocity != NULL;
+  h->fields = h->mat.law == ORC_LAW_GAS_LIQUID || h->mat.law == ORC_LAW_GAS_LIQUID_SOLID ||
+              velocity != NULL;
   return 0;
 }
 
@@ -497,24 +501,6 @@ int orc_set_fields(orc_heat *h, const double *heaviside, const double *velocity)
 /* material law (Material::compute_parameters, liquid_solid / gas,     */
 /* plus the linear conductivity law k = k_l + k1 T)                    */
 /* ------------------------------------------------------------------ */
-
-/* gas-liquid law at heaviside value H (material.templates.hpp:240-295): every property is
- * (1 - w) gas + w liquid (LevelSet::Tools::interpolate, level_set_tools.hpp:40-43) with
- * w = H (smooth transition) or heaviside(H, 0.5) = H > 0.5 (sharp, :515-524,
- * characteristic_functions.hpp:37-40); rho*cp is the product of the interpolated density
- * and capacity, or the interpolated volume-specific capacity (heat_diffuse_operator.cpp:
- * 1138-1162).  The temperature derivatives are zero. */
-static inline void material_eval_H(const orc_material *m, double H, double *rhocp, double *k)
-{
-  const double w = m->law != ORC_LAW_GAS_LIQUID ? 1.0 : (m->sharp ? (H > 0.5 ? 1.0 : 0.0) : H);
-#define MIX(l, g) ((1.0 - w) * (g) + w * (l))
-  *k = MIX(m->k_l, m->k_s);
-  if (m->volume_specific)
-    *rhocp = MIX(m->rho_l * m->cp_l, m->rho_s * m->cp_s);
-  else
-    *rhocp = MIX(m->rho_l, m->rho_s) * MIX(m->cp_l, m->cp_s);
-#undef MIX
-}
 
 /* J^-1 v at quadrature point q of cell c (reference-space transport direction: the
  * physical v.grad(u) equals (J^-1 v).grad_ref(u)) */
@@ -537,24 +523,14 @@ static void ref_direction(const orc_heat *h, int64_t c, int q, const double v[3]
   for (int i = 0; i < 3; ++i) b[i] = inv[i][0] * v[0] + inv[i][1] * v[1] + inv[i][2] * v[2];
 }
 
-static inline void material_eval(const orc_material *m, double T, double *rhocp, double *k,
-                                 double *drhocp, double *dk)
+/* liquid-solid interpolation of one property at temperature T (compute_solid_liquid_phases_
+ * property and its temperature derivative, material.templates.hpp:540-600,745-780): solid
+ * fraction sf from the mushy zone (or sharp at T_solidus), cubic smoothstep
+ * interpolate_cubic(sf, l, s) = l + (s - l) (3 sf^2 - 2 sf^3), derivative
+ * -(s - l) 6 sf (1 - sf) / (T_liquidus - T_solidus), both exact at sf = 0 and 1 */
+static inline void ls_interp(const orc_material *m, double T, double l, double s, double *val,
+                             double *dval)
 {
-  if (m->law == ORC_LAW_CONSTANT) {
-    *rhocp = m->rho_l * m->cp_l;
-    *k = m->k_l;
-    *drhocp = 0.0;
-    *dk = 0.0;
-    return;
-  }
-  if (m->law == ORC_LAW_LINEAR_K) {
-    *rhocp = m->rho_l * m->cp_l;
-    *k = m->k_l + m->k1 * T;
-    *drhocp = 0.0;
-    *dk = m->k1;
-    return;
-  }
-  /* liquid_solid: solid fraction sf, cubic smoothstep between liquid and solid */
   const double inv_mushy = 1.0 / (m->T_liquidus - m->T_solidus);
   double sf;
   if (m->sharp)
@@ -563,24 +539,85 @@ static inline void material_eval(const orc_material *m, double T, double *rhocp,
     sf = (m->T_liquidus - T) * inv_mushy;
     sf = sf < 0.0 ? 0.0 : (sf > 1.0 ? 1.0 : sf);
   }
-  const double hs = -2.0 * sf * sf * sf + 3.0 * sf * sf;   /* interpolate_cubic weight */
-  const double dhs = -6.0 * sf * sf + 6.0 * sf;             /* its derivative */
+  const double hs = -2.0 * sf * sf * sf + 3.0 * sf * sf; /* interpolate_cubic weight */
+  const double dhs = -6.0 * sf * sf + 6.0 * sf;           /* its derivative */
   const int edge = (sf == 0.0 || sf == 1.0);
-#define PROP(l, s) (sf == 0.0 ? (l) : (sf == 1.0 ? (s) : (l) + ((s) - (l)) * hs))
-#define DPROP(l, s) (edge ? 0.0 : -1.0 * inv_mushy * ((s) - (l)) * dhs)
-  *k = PROP(m->k_l, m->k_s);
-  *dk = DPROP(m->k_l, m->k_s);
-  if (m->volume_specific) {
-    *rhocp = PROP(m->rho_l * m->cp_l, m->rho_s * m->cp_s);
-    *drhocp = DPROP(m->rho_l * m->cp_l, m->rho_s * m->cp_s);
-  } else {
-    const double rho = PROP(m->rho_l, m->rho_s), cp = PROP(m->cp_l, m->cp_s);
-    const double drho = DPROP(m->rho_l, m->rho_s), dcp = DPROP(m->cp_l, m->cp_s);
-    *rhocp = rho * cp;
-    *drhocp = dcp * rho + drho * cp;
+  *val = sf == 0.0 ? l : (sf == 1.0 ? s : l + (s - l) * hs);
+  *dval = edge ? 0.0 : -1.0 * inv_mushy * ((s - l) * dhs);
+}
+
+/* Material::compute_parameters of the heat operator's material types at temperature T and
+ * level-set heaviside H (material.templates.hpp:104-137, 226-500), as rho*cp, k and their
+ * temperature derivatives (HeatDiffuseMultiPhaseOperator::get_material_parameters_and_
+ * derivatives, heat_diffuse_operator.cpp:1165-1215):
+ *   CONSTANT          liquid values
+ *   LINEAR_K          k = k_l + k1 T (no reference counterpart)
+ *   LIQUID_SOLID      ls_interp of every property (:296-375)
+ *   GAS_LIQUID        (1 - w) gas + w liquid, w = H or heaviside(H, 0.5) = H > 0.5
+ *                     (LevelSet::Tools::interpolate, level_set_tools.hpp:40-43; :240-295,
+ *                     :515-524, characteristic_functions.hpp:37-40); no T derivatives
+ *   GAS_LIQUID_SOLID  (1 - w) gas + w ls_interp(T), derivatives w d ls_interp / dT (:376-500,
+ *                     :620-740)
+ * rho*cp is the product of the interpolated density and capacity, or with volume_specific the
+ * interpolated rho*cp of the phases (:1138-1162). */
+static inline void material_eval(const orc_material *m, double T, double H, double *rhocp,
+                                 double *k, double *drhocp, double *dk)
+{
+  const int law = m->law;
+  if (law == ORC_LAW_CONSTANT) {
+    *rhocp = m->rho_l * m->cp_l;
+    *k = m->k_l;
+    *drhocp = 0.0;
+    *dk = 0.0;
+    return;
   }
-#undef PROP
-#undef DPROP
+  if (law == ORC_LAW_LINEAR_K) {
+    *rhocp = m->rho_l * m->cp_l;
+    *k = m->k_l + m->k1 * T;
+    *drhocp = 0.0;
+    *dk = m->k1;
+    return;
+  }
+  /* phase values of the liquid(-solid) side and their T derivatives */
+  double rho = 0.0, cp = 0.0, kk = 0.0, vs = 0.0, drho = 0.0, dcp = 0.0, dkk = 0.0, dvs = 0.0;
+  if (law == ORC_LAW_GAS_LIQUID) {
+    rho = m->rho_l, cp = m->cp_l, kk = m->k_l, vs = m->rho_l * m->cp_l;
+    drho = dcp = dkk = dvs = 0.0;
+  } else {
+    ls_interp(m, T, m->k_l, m->k_s, &kk, &dkk);
+    if (m->volume_specific) {
+      ls_interp(m, T, m->rho_l * m->cp_l, m->rho_s * m->cp_s, &vs, &dvs);
+    } else {
+      ls_interp(m, T, m->rho_l, m->rho_s, &rho, &drho);
+      ls_interp(m, T, m->cp_l, m->cp_s, &cp, &dcp);
+    }
+  }
+  if (law == ORC_LAW_LIQUID_SOLID) {
+    *k = kk;
+    *dk = dkk;
+    if (m->volume_specific) {
+      *rhocp = vs;
+      *drhocp = dvs;
+    } else {
+      *rhocp = rho * cp;
+      *drhocp = dcp * rho + drho * cp;
+    }
+    return;
+  }
+  /* gas mixing */
+  const double w = m->sharp_gas_liquid ? (H > 0.5 ? 1.0 : 0.0) : H;
+#define MIX(liq, gas) ((1.0 - w) * (gas) + w * (liq))
+  *k = MIX(kk, m->k_g);
+  *dk = w * dkk;
+  if (m->volume_specific) {
+    *rhocp = MIX(law == ORC_LAW_GAS_LIQUID ? m->rho_l * m->cp_l : vs, m->rho_g * m->cp_g);
+    *drhocp = w * dvs;
+  } else {
+    const double r = MIX(rho, m->rho_g), c = MIX(cp, m->cp_g);
+    *rhocp = r * c;
+    *drhocp = (w * dcp) * r + (w * drho) * c;
+  }
+#undef MIX
 }
 
 /* ------------------------------------------------------------------ */
@@ -741,12 +778,14 @@ static inline __attribute__((always_inline)) void eval_fields(const orc_heat *h,
   }
 }
 
-/* coefficients of lane v at point q in fields mode: rho*cp, k and the reference-space
- * transport vector b = J^-1 v (zero without a velocity field) */
-static inline void field_coefs(const orc_heat *h, const int64_t *cells, int nl, int v, int q,
-                               const scratch_t *s, double *rhocp, double *k, double b[3])
+/* coefficients of lane v at point q: rho*cp, k, their T derivatives at temperature T and
+ * the heaviside value there, and the reference-space transport vector b = J^-1 v (zero
+ * without a velocity field) */
+static inline void point_coefs(const orc_heat *h, const int64_t *cells, int nl, int v, int q,
+                               const scratch_t *s, double T, double *rhocp, double *k,
+                               double *drhocp, double *dk, double b[3])
 {
-  material_eval_H(&h->mat, s->Hq[q][v], rhocp, k);
+  material_eval(&h->mat, T, h->fields ? s->Hq[q][v] : 1.0, rhocp, k, drhocp, dk);
   if (h->vel) {
     const double vv[3] = {s->Vq[0][q][v], s->Vq[1][q][v], s->Vq[2][q][v]};
     ref_direction(h, cells[v < nl ? v : 0], q, vv, b);
@@ -792,17 +831,16 @@ static inline __attribute__((always_inline)) void batch_kernel(
     }
     for (int q = 0; q < npt; ++q)
       for (int v = 0; v < ORC_VEC; ++v) {
-        double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
+        double jxw, G[6], rhocp, k, drhocp, dk, b[3];
         geo_at(h, cells, nl, v, q, &jxw, G);
-        if (h->fields) {
-          field_coefs(h, cells, nl, v, q, s, &rhocp, &k, b);
-          drhocp = dk = 0.0;
-        } else {
-          material_eval(&h->mat, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk);
-        }
+        point_coefs(h, cells, nl, v, q, s, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk, b);
         double cval = idt * rhocp;
-        /* convection rho_cp v.grad(u) (heat_diffuse_operator.cpp:1038-1042) */
-        const double conv = rhocp * (b[0] * s->gx[q][v] + b[1] * s->gy[q][v] + b[2] * s->gz[q][v]);
+        /* convection rho_cp v.grad(u), and with a temperature-dependent law
+         * d(rho_cp)/dT (v.grad T_lin) u (heat_diffuse_operator.cpp:1038-1049) */
+        double conv = rhocp * (b[0] * s->gx[q][v] + b[1] * s->gy[q][v] + b[2] * s->gz[q][v]);
+        if (h->tdep)
+          conv += drhocp * (b[0] * s->Tx[q][v] + b[1] * s->Ty[q][v] + b[2] * s->Tz[q][v]) *
+                  s->uq[q][v];
         double g0 = k * s->gx[q][v], g1 = k * s->gy[q][v], g2 = k * s->gz[q][v];
         if (h->tdep) {
           if (h->need_told) cval += idt * drhocp * (s->Tq[q][v] - s->Toq[q][v]);
@@ -828,12 +866,9 @@ static inline __attribute__((always_inline)) void batch_kernel(
     eval_vg(h, n, s->u, s, s->Sq, NULL, NULL, NULL);
     for (int q = 0; q < npt; ++q)
       for (int v = 0; v < ORC_VEC; ++v) {
-        double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
+        double jxw, G[6], rhocp, k, drhocp, dk, b[3];
         geo_at(h, cells, nl, v, q, &jxw, G);
-        if (h->fields)
-          field_coefs(h, cells, nl, v, q, s, &rhocp, &k, b);
-        else
-          material_eval(&h->mat, s->Tq[q][v], &rhocp, &k, &drhocp, &dk);
+        point_coefs(h, cells, nl, v, q, s, s->Tq[q][v], &rhocp, &k, &drhocp, &dk, b);
         /* rhs_cell_loop value term with the convection rho_cp grad(T).v (:493-500) */
         const double val = idt * rhocp * (s->Tq[q][v] - s->Toq[q][v]) - s->Sq[q][v] +
                            rhocp * (b[0] * s->Tx[q][v] + b[1] * s->Ty[q][v] + b[2] * s->Tz[q][v]);
@@ -860,33 +895,29 @@ static inline __attribute__((always_inline)) void batch_kernel(
            *Gyz = s->c[5], *Gzz = s->c[6], *Bx = s->c[7], *By = s->c[8], *Bz = s->c[9];
     for (int q = 0; q < npt; ++q)
       for (int v = 0; v < ORC_VEC; ++v) {
-        double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
+        double jxw, G[6], rhocp, k, drhocp, dk, b[3];
         geo_at(h, cells, nl, v, q, &jxw, G);
-        if (h->fields) {
-          field_coefs(h, cells, nl, v, q, s, &rhocp, &k, b);
-          drhocp = dk = 0.0;
-        } else {
-          material_eval(&h->mat, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk);
-        }
+        point_coefs(h, cells, nl, v, q, s, h->tdep ? s->Tq[q][v] : 0.0, &rhocp, &k, &drhocp, &dk, b);
         double cval = idt * rhocp;
         if (h->tdep && h->need_told) cval += idt * drhocp * (s->Tq[q][v] - s->Toq[q][v]);
         C0[q][v] = cval * jxw;
+        if (h->tdep) /* d(rho_cp)/dT (v.grad T_lin) u: a mass-like term */
+          C0[q][v] += drhocp * (b[0] * s->Tx[q][v] + b[1] * s->Ty[q][v] + b[2] * s->Tz[q][v]) * jxw;
         Gxx[q][v] = k * G[0];
         Gxy[q][v] = 2.0 * k * G[1];
         Gxz[q][v] = 2.0 * k * G[2];
         Gyy[q][v] = k * G[3];
         Gyz[q][v] = 2.0 * k * G[4];
         Gzz[q][v] = k * G[5];
+        /* convection: phi_i (JxW rho_cp J^-1 v).grad_ref(phi_i) */
+        Bx[q][v] = jxw * rhocp * b[0];
+        By[q][v] = jxw * rhocp * b[1];
+        Bz[q][v] = jxw * rhocp * b[2];
         if (h->tdep && kind == 2) {
           const double t0 = s->Tx[q][v], t1 = s->Ty[q][v], t2 = s->Tz[q][v];
-          Bx[q][v] = dk * (G[0] * t0 + G[1] * t1 + G[2] * t2);
-          By[q][v] = dk * (G[1] * t0 + G[3] * t1 + G[4] * t2);
-          Bz[q][v] = dk * (G[2] * t0 + G[4] * t1 + G[5] * t2);
-        } else {
-          /* convection: phi_i (JxW rho_cp J^-1 v).grad_ref(phi_i) */
-          Bx[q][v] = jxw * rhocp * b[0];
-          By[q][v] = jxw * rhocp * b[1];
-          Bz[q][v] = jxw * rhocp * b[2];
+          Bx[q][v] += dk * (G[0] * t0 + G[1] * t1 + G[2] * t2);
+          By[q][v] += dk * (G[1] * t0 + G[3] * t1 + G[4] * t2);
+          Bz[q][v] += dk * (G[2] * t0 + G[4] * t1 + G[5] * t2);
         }
       }
     /* (x,y) = (P,P): z P C0 + z Q Gzz + z R Bz */
@@ -1036,13 +1067,9 @@ static void run_direct(const orc_heat *h, int kind, double *dst, const double *s
         }
         double jxw, G[6], rhocp, k, drhocp, dk, b[3] = {0.0, 0.0, 0.0};
         geo_at(h, one, 1, 0, q, &jxw, G);
-        if (h->fields) {
-          material_eval_H(&h->mat, Hq, &rhocp, &k);
-          drhocp = dk = 0.0;
-          if (h->vel) ref_direction(h, c, q, vq, b);
-        } else {
-          material_eval(&h->mat, Tq, &rhocp, &k, &drhocp, &dk);
-        }
+        material_eval(&h->mat, Tq, h->fields ? Hq : 1.0, &rhocp, &k, &drhocp, &dk);
+        if (h->vel) ref_direction(h, c, q, vq, b);
+        const double bT = b[0] * gT[0] + b[1] * gT[1] + b[2] * gT[2];
         double cval = idt * rhocp;
         if (h->tdep && h->need_told) cval += idt * drhocp * (Tq - Toq);
         if (!h->tdep) dk = 0.0;
@@ -1051,7 +1078,8 @@ static void run_direct(const orc_heat *h, int kind, double *dst, const double *s
           double f[3], F[3];
           for (int d = 0; d < 3; ++d) f[d] = k * gu[d] + dk * gT[d] * uq;
           for (int d = 0; d < 3; ++d) F[d] = Gm[d][0] * f[0] + Gm[d][1] * f[1] + Gm[d][2] * f[2];
-          const double val = (cval * uq + rhocp * (b[0] * gu[0] + b[1] * gu[1] + b[2] * gu[2])) * jxw;
+          const double val = (cval * uq + rhocp * (b[0] * gu[0] + b[1] * gu[1] + b[2] * gu[2]) +
+                              (h->tdep ? drhocp * bT * uq : 0.0)) * jxw;
           for (int i = 0; i < npt; ++i)
             out[i] += ph[i] * val + dph[3 * i] * F[0] + dph[3 * i + 1] * F[1] + dph[3 * i + 2] * F[2];
         } else {
@@ -1061,7 +1089,7 @@ static void run_direct(const orc_heat *h, int kind, double *dst, const double *s
                     jxw * rhocp * b[d];
           for (int i = 0; i < npt; ++i) {
             const double *g = dph + 3 * i;
-            double s = cval * jxw * ph[i] * ph[i];
+            double s = (cval + (h->tdep ? drhocp * bT : 0.0)) * jxw * ph[i] * ph[i];
             for (int a = 0; a < 3; ++a)
               for (int b = 0; b < 3; ++b) s += k * g[a] * Gm[a][b] * g[b];
             s += ph[i] * (g[0] * BT[0] + g[1] * BT[1] + g[2] * BT[2]);

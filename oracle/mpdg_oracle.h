@@ -51,16 +51,24 @@ typedef struct {
   double   dirichlet_value[6]; /* constant Dirichlet value per face */
 } orc_mesh_desc;
 
-enum { ORC_LAW_CONSTANT = 0, ORC_LAW_LINEAR_K = 1, ORC_LAW_LIQUID_SOLID = 2, ORC_LAW_GAS_LIQUID = 3 };
+enum {
+  ORC_LAW_CONSTANT = 0,
+  ORC_LAW_LINEAR_K = 1,
+  ORC_LAW_LIQUID_SOLID = 2,
+  ORC_LAW_GAS_LIQUID = 3,
+  ORC_LAW_GAS_LIQUID_SOLID = 4
+};
 
 typedef struct {
   int    law;             /* ORC_LAW_* */
-  int    sharp;           /* liquid-solid: 0 mushy zone, 1 sharp; gas-liquid: 0 smooth, 1 sharp */
+  int    sharp;           /* liquid-solid transition: 0 mushy zone, 1 sharp */
   int    volume_specific; /* interpolate rho*cp directly (heat "diffuse" option) */
   double rho_l, cp_l, k_l;  /* liquid (or the single constant phase) */
-  double rho_s, cp_s, k_s;  /* solid (gas for the gas-liquid law) */
+  double rho_s, cp_s, k_s;  /* solid */
   double T_solidus, T_liquidus;
   double k1;              /* linear law: k(T) = k_l + k1*T */
+  int    sharp_gas_liquid;  /* gas-liquid transition: 0 smooth (w = H), 1 sharp (w = H > 0.5) */
+  double rho_g, cp_g, k_g;  /* gas */
 } orc_material;
 
 typedef struct orc_heat orc_heat;
@@ -83,14 +91,17 @@ void      orc_set_threads(int n);
 int orc_set_boundary(orc_heat *h, int face, int type, double h_conv, double T_inf_conv,
                      double emissivity, double T_inf_rad, double q_n);
 
-/* Operator coefficients: material law and time step (reset_time_increment). */
-void orc_set_material(orc_heat *h, const orc_material *m, double dt);
+/* Operator coefficients: material law and time step (reset_time_increment).  Returns -1
+ * if a velocity field is set and the law is the linear-k law. */
+int orc_set_material(orc_heat *h, const orc_material *m, double dt);
 
 /* Two-phase and transport fields (HeatDiffuseMultiPhaseOperator's level_set_as_heaviside and
  * velocity, heat_diffuse_operator.cpp:51-67), nodal on the temperature space: heaviside (n_dofs)
  * weights the gas-liquid law, velocity ([3][n_dofs], component-major) adds the convective term
  * rho_cp v.grad(T) to the residual and rho_cp v.grad(u) to the tangent (:499-500, :1038-1042).
- * Either may be NULL.  Returns -1 if a velocity is combined with a temperature-dependent law. */
+ * With a temperature-dependent law the tangent also gets d(rho_cp)/dT (v.grad T_lin) u
+ * (:1044-1049).  Either may be NULL (no heaviside: weight 1, the liquid or liquid-solid
+ * properties).  Returns -1 if a velocity is combined with the linear-k law. */
 int orc_set_fields(orc_heat *h, const double *heaviside, const double *velocity);
 
 /* dst = J(T_lin, T_old) src.  form 0: sum-factorised, 1: direct quadrature,

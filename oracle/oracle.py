@@ -25,7 +25,7 @@ _HDR = os.path.join(_HERE, "mpdg_oracle.h")
 _lock = threading.Lock()
 _lib = None
 
-LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID = 0, 1, 2, 3
+LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID, LAW_GAS_LIQUID_SOLID = 0, 1, 2, 3, 4
 
 
 def _cpu_tag() -> str:
@@ -67,7 +67,9 @@ class Material(C.Structure):
     _fields_ = [("law", C.c_int), ("sharp", C.c_int), ("volume_specific", C.c_int),
                 ("rho_l", C.c_double), ("cp_l", C.c_double), ("k_l", C.c_double),
                 ("rho_s", C.c_double), ("cp_s", C.c_double), ("k_s", C.c_double),
-                ("T_solidus", C.c_double), ("T_liquidus", C.c_double), ("k1", C.c_double)]
+                ("T_solidus", C.c_double), ("T_liquidus", C.c_double), ("k1", C.c_double),
+                ("sharp_gas_liquid", C.c_int),
+                ("rho_g", C.c_double), ("cp_g", C.c_double), ("k_g", C.c_double)]
 
 
 class SolverParams(C.Structure):
@@ -143,7 +145,8 @@ def _ptr(a):
 
 
 def material(law=LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_s=None, k_s=None,
-             T_solidus=0.0, T_liquidus=1.0, sharp=False, volume_specific=False) -> Material:
+             T_solidus=0.0, T_liquidus=1.0, sharp=False, volume_specific=False, rho_g=None,
+             cp_g=None, k_g=None, sharp_gas_liquid=False) -> Material:
     m = Material()
     m.law = law
     m.sharp = int(sharp)
@@ -153,6 +156,10 @@ def material(law=LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_s=
     m.cp_s = cp if cp_s is None else cp_s
     m.k_s = k if k_s is None else k_s
     m.T_solidus, m.T_liquidus, m.k1 = T_solidus, T_liquidus, k1
+    m.sharp_gas_liquid = int(sharp_gas_liquid)
+    m.rho_g = rho if rho_g is None else rho_g
+    m.cp_g = cp if cp_g is None else cp_g
+    m.k_g = k if k_g is None else k_g
     return m
 
 
@@ -208,8 +215,10 @@ class Oracle:
         return u
 
     def set_material(self, m: Material, dt: float):
+        if self.L.orc_set_material(self.h, C.byref(m), dt) != 0:
+            raise ValueError("velocity with the linear-k law")
         self.dt = dt
-        self.L.orc_set_material(self.h, C.byref(m), dt)
+        self._material = m
 
     def set_fields(self, heaviside=None, velocity=None):
         """Nodal heaviside (n_dofs) and velocity ((3, n_dofs)) fields; None clears one."""
@@ -217,7 +226,7 @@ class Oracle:
         V = None if velocity is None else np.ascontiguousarray(velocity, np.float64).reshape(3, -1)
         self._fields = (H, V)  # the oracle keeps the pointers
         if self.L.orc_set_fields(self.h, _ptr(H), None if V is None else _ptr(V)) != 0:
-            raise ValueError("velocity with a temperature-dependent law")
+            raise ValueError("velocity with the linear-k law")
 
     def set_boundary(self, face, convection=None, radiation=None, neumann=None):
         """convection=(h, T_inf), radiation=(emissivity, T_inf), neumann=q_n."""

@@ -399,12 +399,22 @@ def test_linear_solve_not_converged_raises():
 
 TRANSPORT_CASES = {
     # law, material, heaviside, velocity
-    "gas_liquid": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3), True, False),
-    "gas_liquid_sharp_vs": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3,
-                                 sharp=True, volume_specific=True), True, False),
+    "gas_liquid": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_g=0.5, cp_g=1.5, k_g=0.3), True, False),
+    "gas_liquid_sharp_vs": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_g=0.5, cp_g=1.5, k_g=0.3,
+                                 sharp_gas_liquid=True, volume_specific=True), True, False),
     "constant_velocity": (dict(law=0, rho=2.0, cp=3.0, k=5.0), False, True),
-    "gas_liquid_velocity": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3),
+    "gas_liquid_velocity": (dict(law=3, rho=2.0, cp=3.0, k=5.0, rho_g=0.5, cp_g=1.5, k_g=0.3),
                             True, True),
+    # temperature-dependent laws with the fields (kernel LAW 5): mushy zone inside the
+    # sampled T range
+    "liquid_solid_velocity": (dict(law=2, rho=1.0, cp=1.0, k=0.5, rho_s=1.2, cp_s=0.8, k_s=2.5,
+                                   T_solidus=0.3, T_liquidus=0.7), False, True),
+    "three_phase": (dict(law=4, rho=1.0, cp=1.0, k=0.5, rho_s=1.2, cp_s=0.8, k_s=2.5,
+                         T_solidus=0.3, T_liquidus=0.7, rho_g=0.4, cp_g=1.5, k_g=0.2), True, False),
+    "three_phase_sharp_vs_velocity": (dict(law=4, rho=1.0, cp=1.0, k=0.5, rho_s=1.2, cp_s=0.8,
+                                           k_s=2.5, T_solidus=0.3, T_liquidus=0.7, rho_g=0.4,
+                                           cp_g=1.5, k_g=0.2, sharp_gas_liquid=True,
+                                           volume_specific=True), True, True),
 }
 
 
@@ -437,12 +447,12 @@ def test_two_phase_transport_matches_oracle(degree, perturb, case):
     src = rng.uniform(-1, 1, N)
     T, To, q = rng.uniform(0, 1, N), rng.uniform(0, 1, N), rng.uniform(0, 5, N)
     g.set_linearization(cuda(T), cuda(To))
-    ref = o.vmult(src)
+    ref = o.vmult(src, T, To)
     dst = g.vmult(g.new_vector(), cuda(src))
     assert rel(dst, ref) <= TOL64
     d32 = g.vmult(g.new_vector(torch.float32), cuda(src, torch.float32))
     assert rel(d32, ref) <= TOL32 * (10 if degree >= 5 else 1)
-    dref = o.inverse_diagonal()
+    dref = o.inverse_diagonal(T, To)
     dg = g.compute_inverse_diagonal_from_matrixfree(g.new_vector())
     assert rel(1.0 / dg.cpu().numpy(), 1.0 / dref) <= TOL64
     base = rng.uniform(-1, 1, N)
@@ -463,7 +473,7 @@ def test_fields_are_rebuilt_after_set_fields_and_set_material():
     o.set_fields(Hf, V)
     g.set_fields(cuda(Hf), cuda(V).contiguous())
     assert rel(g.vmult(g.new_vector(), cuda(src)), o.vmult(src)) <= TOL64
-    m = dict(law=3, rho=1.0, cp=4.0, k=2.0, rho_s=0.1, cp_s=1.0, k_s=0.5)
+    m = dict(law=3, rho=1.0, cp=4.0, k=2.0, rho_g=0.1, cp_g=1.0, k_g=0.5)
     o.set_material(O.material(**m), 1e-2)
     g.set_material(H.material(**m))
     assert rel(g.vmult(g.new_vector(), cuda(src)), o.vmult(src)) <= TOL64
@@ -490,7 +500,7 @@ def test_gmres_on_the_convective_operator_matches_oracle():
 def test_fields_reject_unsupported_combinations():
     o, g = transport_pair(2, (4, 4, 4), 0.0, "constant_velocity")
     with pytest.raises(H.ExcInvalidArgument):
-        g.set_material(H.material(law=1, k1=0.5))  # velocity with k(T)
+        g.set_material(H.material(law=1, k1=0.5))  # velocity with the linear-k law
     N = g.n_dofs
     g.set_linearization(cuda(np.zeros(N)), cuda(np.zeros(N)))
     H.JacobiPreconditioner(g).update()
@@ -498,7 +508,10 @@ def test_fields_reject_unsupported_combinations():
         H.LinearSolver.solve(g, g.new_vector(), cuda(np.ones(N)), H.LinearSolverData(
             preconditioner_type=L.PRECOND_MG_F32), True)
     g2 = H.HeatDiffuseOperator(H.box_mesh(2, (3, 3, 3)))
-    g2.set_material(H.material(law=3, rho_s=0.5))
     g2.reset_time_increment(1e-2)
-    with pytest.raises(H.ExcInvalidArgument):
-        g2.vmult(g2.new_vector(), g2.new_vector())  # gas-liquid law without a heaviside
+    z = g2.new_vector()
+    g2.set_linearization(z, z)
+    for law in (3, 4):  # gas-liquid laws without a heaviside
+        g2.set_material(H.material(law=law, rho_g=0.5))
+        with pytest.raises(H.ExcInvalidArgument):
+            g2.vmult(g2.new_vector(), g2.new_vector())

@@ -206,7 +206,7 @@ def test_unidirectional_transport_on_gpu(case):
                                           dirichlet=()))
     if two_phase:
         op.set_material(H.material(law=L.LAW_GAS_LIQUID, rho=7850.0, cp=460.0, k=55.563,
-                                   rho_s=3925.0, cp_s=230.0, k_s=27.7815, volume_specific=vs))
+                                   rho_g=3925.0, cp_g=230.0, k_g=27.7815, volume_specific=vs))
     else:
         op.set_material(H.material(rho=7850.0, cp=460.0, k=55.563))
     x = op.support_points()
@@ -233,3 +233,47 @@ def test_unidirectional_transport_on_gpu(case):
             assert abs(norm - ref) <= 0.5e-4 + 2e-7, norm
         else:
             assert float(f"{norm:.5e}") == ref
+
+
+# _with_velocity_and_solidification / _with_two_phase_and_solidification.mpirun=4.output (the
+# oracle's known-answer test states the setting): liquid-solid and three-phase laws with a
+# velocity, the second on a heaviside that moves with the velocity
+SOLIDIFICATION_TRANSPORT = {
+    "velocity_and_solidification": (0.01, 0.005, False,
+                                    [1.97002e+02, 1.97003e+02, 1.97004e+02, 1.97005e+02,
+                                     1.97006e+02]),
+    "two_phase_and_solidification": (1.0, 1e-4, True,
+                                     [1.96996e+02, 1.96992e+02, 1.96987e+02, 1.96983e+02,
+                                      1.96979e+02]),
+}
+
+
+@pytest.mark.parametrize("case", list(SOLIDIFICATION_TRANSPORT))
+def test_unidirectional_solidification_with_transport_on_gpu(case):
+    dt, vel, two_phase, refs = SOLIDIFICATION_TRANSPORT[case]
+    op = H.HeatDiffuseOperator(H.box_mesh(1, (32, 32, 1), (0, 0, 0), (0.1, 0.1, 1.0),
+                                          dirichlet=()))
+    ls = dict(rho=7850.0, cp=460.0, k=55.563, rho_s=7850.0, cp_s=700.0, k_s=17.0,
+              T_solidus=1966.0, T_liquidus=1974.0)
+    if two_phase:
+        op.set_material(H.material(law=L.LAW_GAS_LIQUID_SOLID, rho_g=3925.0, cp_g=230.0,
+                                   k_g=27.7815, sharp_gas_liquid=True, **ls))
+    else:
+        op.set_material(H.material(law=L.LAW_LIQUID_SOLID, **ls))
+    x = op.support_points()
+    v = torch.zeros((3, op.n_dofs), dtype=torch.float64, device="cuda")
+    v[0] = -vel
+    opn = H.HeatDiffuseOperation(op, H.LinearSolverData(solver_type=L.SOLVER_GMRES,
+                                                        rel_tolerance=1e-12),
+                                 H.NonlinearSolverData(residual_tolerance=1e-7))
+    opn.set_initial_condition((1960.0 + 20.0 * x[:, 0] / 0.1).contiguous())
+    eps = 0.01
+    for i, ref in enumerate(refs):
+        d = 0.2 / 3 - x[:, 0] - vel * (i + 1) * dt
+        hs = torch.where(d > eps, torch.ones_like(d), torch.where(
+            d <= -eps, torch.zeros_like(d),
+            (d + eps) / (2 * eps) + torch.sin(np.pi * d / eps) / (2 * np.pi))).contiguous()
+        op.set_fields(hs if two_phase else None, v)
+        st = opn.solve(dt)
+        assert st.converged == 1
+        assert float(f"{op.l2_norm(opn.T):.5e}") == ref

@@ -133,7 +133,7 @@ def test_laser_profiles_follow_their_formulas():
     assert np.abs(g[~outside]).max() > 0.0
 
 
-GAS_LIQUID = dict(rho=2.0, cp=3.0, k=5.0, rho_s=0.5, cp_s=1.5, k_s=0.3)
+GAS_LIQUID = dict(rho=2.0, cp=3.0, k=5.0, rho_g=0.5, cp_g=1.5, k_g=0.3)
 
 
 def transport_fields(o, velocity=True):
@@ -151,7 +151,8 @@ def test_two_phase_transport_forms_agree(degree, perturb, sharp, vs):
     residual is the affine counterpart of the tangent (the law is linear in T) and the
     Picard form equals the tangent (no temperature derivatives)."""
     o = O.Oracle(degree, (3, 2, 3), perturb=perturb, seed=7, hi=(1.0, 1.3, 0.8))
-    o.set_material(O.material(O.LAW_GAS_LIQUID, sharp=sharp, volume_specific=vs, **GAS_LIQUID), 1e-2)
+    o.set_material(O.material(O.LAW_GAS_LIQUID, sharp_gas_liquid=sharp, volume_specific=vs,
+                              **GAS_LIQUID), 1e-2)
     o.set_fields(*transport_fields(o))
     rng = np.random.default_rng(degree)
     u = rng.standard_normal(o.n_dofs)
@@ -201,14 +202,15 @@ def test_uniform_heaviside_mixes_the_phase_properties(sharp, vs):
     g = GAS_LIQUID
     o = O.Oracle(2, (3, 3, 2), perturb=0.1, seed=3)
     u = np.random.default_rng(0).standard_normal(o.n_dofs)
-    o.set_material(O.material(O.LAW_GAS_LIQUID, sharp=sharp, volume_specific=vs, **g), 1e-2)
+    o.set_material(O.material(O.LAW_GAS_LIQUID, sharp_gas_liquid=sharp, volume_specific=vs, **g),
+                   1e-2)
     o.set_fields(np.full(o.n_dofs, 0.3), None)
     a = o.vmult(u)
     w = 0.0 if sharp else 0.3
     mix = lambda liq, gas: (1 - w) * gas + w * liq
-    k = mix(g["k"], g["k_s"])
-    rhocp = mix(g["rho"] * g["cp"], g["rho_s"] * g["cp_s"]) if vs else \
-        mix(g["rho"], g["rho_s"]) * mix(g["cp"], g["cp_s"])
+    k = mix(g["k"], g["k_g"])
+    rhocp = mix(g["rho"] * g["cp"], g["rho_g"] * g["cp_g"]) if vs else \
+        mix(g["rho"], g["rho_g"]) * mix(g["cp"], g["cp_g"])
     o.set_fields(None, None)
     o.set_material(O.material(rho=rhocp, cp=1.0, k=k), 1e-2)
     assert np.abs(a - o.vmult(u)).max() <= 1e-13 * np.abs(a).max()
@@ -219,3 +221,56 @@ def test_velocity_needs_a_temperature_independent_law():
     o.set_material(O.material(O.LAW_LINEAR_K, k1=0.5), 1e-2)
     with pytest.raises(ValueError):
         o.set_fields(None, np.zeros((3, o.n_dofs)))
+
+
+THREE_PHASE = dict(rho=1.0, cp=1.0, k=0.5, rho_s=1.2, cp_s=0.8, k_s=2.5, T_solidus=0.3,
+                   T_liquidus=0.7, rho_g=0.4, cp_g=1.5, k_g=0.2)
+
+
+@pytest.mark.parametrize("law,sharp_gl,vs", [(O.LAW_LIQUID_SOLID, False, False),
+                                             (O.LAW_LIQUID_SOLID, False, True),
+                                             (O.LAW_GAS_LIQUID_SOLID, False, False),
+                                             (O.LAW_GAS_LIQUID_SOLID, True, False),
+                                             (O.LAW_GAS_LIQUID_SOLID, False, True)])
+def test_transport_tangent_is_derivative_of_residual(law, sharp_gl, vs):
+    """Temperature-dependent laws with a velocity (and the three-phase law on a heaviside):
+    the tangent, including d(rho_cp)/dT (v.grad T) u (heat_diffuse_operator.cpp:1044-1049),
+    is the derivative of the residual; both forms and the diagonal agree."""
+    rng = np.random.default_rng(9)
+    o = O.Oracle(2, (3, 3, 3), perturb=0.1, seed=4)
+    o.set_material(O.material(law, sharp_gas_liquid=sharp_gl, volume_specific=vs, **THREE_PHASE),
+                   1e-2)
+    Hf, V = transport_fields(o)
+    o.set_fields(Hf if law == O.LAW_GAS_LIQUID_SOLID else None, V)
+    T = rng.uniform(0, 1, o.n_dofs)
+    T_old = rng.uniform(0, 1, o.n_dofs)
+    du = rng.uniform(-1, 1, o.n_dofs)
+    du[o.mask().astype(bool)] = 0.0
+    eps = 1e-6
+    fd = -(o.create_rhs(T + eps * du, T_old) - o.create_rhs(T - eps * du, T_old)) / (2 * eps)
+    Jdu = o.vmult(du, T, T_old)
+    assert np.abs(fd - Jdu).max() <= 1e-6 * np.abs(Jdu).max()
+    assert np.abs(Jdu - o.vmult(du, T, T_old, form=1)).max() <= 1e-13 * np.abs(Jdu).max()
+    da, db = o.inverse_diagonal(T, T_old, form=0), o.inverse_diagonal(T, T_old, form=1)
+    assert np.allclose(1 / da, 1 / db, rtol=1e-12, atol=0)
+
+
+def test_three_phase_law_limits():
+    """H = 1 gives the liquid-solid law, H = 0 the gas (constant) law."""
+    o = O.Oracle(2, (3, 2, 2), perturb=0.1, seed=3)
+    rng = np.random.default_rng(1)
+    u, T, To = (rng.uniform(-1, 1, o.n_dofs), rng.uniform(0, 1, o.n_dofs),
+                rng.uniform(0, 1, o.n_dofs))
+    def op(m, H):
+        o.set_fields(None, None)
+        o.set_material(m, 1e-2)
+        o.set_fields(H, None)
+        return o.vmult(u, T, To), o.create_rhs(T, To)
+    three = O.material(O.LAW_GAS_LIQUID_SOLID, **THREE_PHASE)
+    a = op(three, np.ones(o.n_dofs))
+    b = op(O.material(O.LAW_LIQUID_SOLID, **THREE_PHASE), None)
+    assert all(np.abs(x - y).max() <= 1e-14 * np.abs(y).max() for x, y in zip(a, b))
+    a = op(three, np.zeros(o.n_dofs))
+    g = THREE_PHASE
+    b = op(O.material(rho=g["rho_g"], cp=g["cp_g"], k=g["k_g"]), None)
+    assert all(np.abs(x - y).max() <= 1e-14 * np.abs(y).max() for x, y in zip(a, b))

@@ -112,8 +112,8 @@ def smoothed_heaviside(d, eps):
 def transport_case(two_phase, volume_specific):
     o = O.Oracle(1, (32, 32, 1), lo=(0, 0, 0), hi=(0.1, 0.1, 1.0), dirichlet_mask=0)
     if two_phase:
-        m = O.material(O.LAW_GAS_LIQUID, rho=7850.0, cp=460.0, k=55.563, rho_s=3925.0,
-                       cp_s=230.0, k_s=27.7815, volume_specific=volume_specific)
+        m = O.material(O.LAW_GAS_LIQUID, rho=7850.0, cp=460.0, k=55.563, rho_g=3925.0,
+                       cp_g=230.0, k_g=27.7815, volume_specific=volume_specific)
     else:
         m = O.material(rho=7850.0, cp=460.0, k=55.563)
     o.set_material(m, 1e-3)
@@ -143,3 +143,50 @@ def test_unidirectional_heat_transfer_with_transport(case):
             assert abs(norm - ref) <= 0.5e-4 + 2e-7, norm
         else:
             assert _six_digits(norm, ref), (norm, ref)
+
+
+# unidirectional_heat_transfer_with_velocity_and_solidification and
+#   _with_two_phase_and_solidification.mpirun=4.output: no boundary terms, T0 = 1960 + 200 x
+#   (LinearTemp(1960, 1980)), liquid steel / solid (k 17, cp 700, rho 7850), mushy zone
+#   1966..1974 K, Newton residual tolerance 1e-7. The first: dt = 0.01, velocity (-0.005, 0).
+#   The second: the three-phase law (gas as above, sharp gas-liquid transition), dt = 1,
+#   velocity (-1e-4, 0), heaviside of the moving front smoothed_heaviside(0.2/3 - x - 1e-4 t,
+#   0.01) evaluated at the end of each step (CovectedVerticalLevelSetHeaviside,
+#   unidirectional_heat_transfer.cpp:94-130; HeatTransferApplication::compute_field_vector
+#   sets the function time to the new time, heat_transfer_application.cpp:466-480).
+SOLIDIFICATION_TRANSPORT = {
+    "velocity_and_solidification": (0.01, 0.005, False,
+                                    [1.97002e+02, 1.97003e+02, 1.97004e+02, 1.97005e+02,
+                                     1.97006e+02]),
+    "two_phase_and_solidification": (1.0, 1e-4, True,
+                                     [1.96996e+02, 1.96992e+02, 1.96987e+02, 1.96983e+02,
+                                      1.96979e+02]),
+}
+STEEL_LIQUID_SOLID = dict(rho=7850.0, cp=460.0, k=55.563, rho_s=7850.0, cp_s=700.0, k_s=17.0,
+                          T_solidus=1966.0, T_liquidus=1974.0)
+
+
+@pytest.mark.parametrize("case", list(SOLIDIFICATION_TRANSPORT))
+def test_unidirectional_solidification_with_transport(case):
+    dt, vel, two_phase, refs = SOLIDIFICATION_TRANSPORT[case]
+    o = O.Oracle(1, (32, 32, 1), lo=(0, 0, 0), hi=(0.1, 0.1, 1.0), dirichlet_mask=0)
+    if two_phase:
+        m = O.material(O.LAW_GAS_LIQUID_SOLID, rho_g=3925.0, cp_g=230.0, k_g=27.7815,
+                       sharp_gas_liquid=True, **STEEL_LIQUID_SOLID)
+    else:
+        m = O.material(O.LAW_LIQUID_SOLID, **STEEL_LIQUID_SOLID)
+    o.set_material(m, dt)
+    x = o.support_points()
+    v = np.zeros((3, o.n_dofs))
+    v[0] = -vel
+    T = 1960.0 + 20.0 * x[:, 0] / 0.1
+    T_old = np.zeros_like(T)
+    dt_old = 0.0
+    for i, ref in enumerate(refs):
+        t = (i + 1) * dt
+        o.set_fields(smoothed_heaviside(0.2 / 3 - x[:, 0] - vel * t, 0.01) if two_phase else None,
+                     v)
+        rc, st = o.time_step_newton(T, T_old, dt, dt_old, res_tol=1e-7)
+        dt_old = dt
+        assert rc == 0
+        assert _six_digits(o.l2_norm(T), ref), (o.l2_norm(T), ref)

@@ -313,7 +313,10 @@ def run_mine(args):
                "rel_max": ((T_mixed - plain.T).abs().max() / plain.T.abs().max()).item()}
         del T_mixed
 
-    # e2e: the host-buffer C-ABI call (H2D of T, T_old, source; D2H of T, T_old per step)
+    # e2e: host-buffer C-ABI steps. Headline: the history resident on the device as
+    # HeatDiffuseOperation keeps it (loaded once before the timed steps), each step uploads
+    # its host source and downloads the new T. Also reported: the stateless call that copies
+    # T, T_old and the source in and T, T_old out every step.
     e2e = None
     if not args.no_e2e:
         import ctypes as C
@@ -323,8 +326,28 @@ def run_mine(args):
         hT.copy_(T_W)  # the headline's steps W .. W+K-1 again, from the same state
         hTo.copy_(T_old_W)
         prm = mixed.params
-        ms_e2e = 0.0
         first = W
+        H.check(op._L.mpdg_heat_load_history(op.h, C.c_void_p(hT.data_ptr()),
+                                             C.c_void_p(hTo.data_ptr())))
+        ms_res = 0.0
+        for s in range(first, first + K):
+            op.gaussian_source(q, AMP, source_center((s + 1) * DT), RADIUS)
+            hq.copy_(q)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            stt = L.StepStats()
+            H.check(op._L.mpdg_heat_time_step_resident(op.h, C.byref(prm), DT, DT,
+                                                        C.c_void_p(hq.data_ptr()),
+                                                        C.c_void_p(hT.data_ptr()),
+                                                        C.byref(stt)))
+            e1.record(stream)
+            barrier()
+            ms_res += e0.elapsed_time(e1)
+        ms_res = max_over_ranks(ms_res, dev, world)
+        hT.copy_(T_W)
+        hTo.copy_(T_old_W)
+        ms_e2e = 0.0
         for s in range(first, first + K):
             op.gaussian_source(q, AMP, source_center((s + 1) * DT), RADIUS)
             hq.copy_(q)
@@ -340,9 +363,15 @@ def run_mine(args):
             barrier()
             ms_e2e += e0.elapsed_time(e1)
         ms_e2e = max_over_ranks(ms_e2e, dev, world)
-        e2e = {"value": replica_throughput(world, N, K, ms_e2e), "unit": "DoF/s",
-               "h2d_bytes_per_step": 3 * N * 8, "d2h_bytes_per_step": 2 * N * 8,
-               "ms_per_step": ms_e2e / K}
+        e2e = {"value": replica_throughput(world, N, K, ms_res), "unit": "DoF/s",
+               "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
+               "ms_per_step": ms_res / K,
+               "api": "mpdg_heat_time_step_resident (history resident on the device, loaded "
+                      "once; per step: host source in, new T out, pinned buffers)",
+               "stateless": {"value": replica_throughput(world, N, K, ms_e2e), "unit": "DoF/s",
+                             "h2d_bytes_per_step": 3 * N * 8, "d2h_bytes_per_step": 2 * N * 8,
+                             "ms_per_step": ms_e2e / K,
+                             "api": "mpdg_heat_time_step_host (T, T_old, source in; T, T_old out)"}}
 
     # vmult throughput of the FP64 operator (MF vmult GDoF/s), CUDA events
     x = torch.rand(N, dtype=torch.float64, device=dev)

@@ -306,6 +306,18 @@ int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *prm, double d
                              double dt_old, double *T_cur, double *T_old,
                              const double *heat_source, mpdg_step_stats *stats);
 
+/* Host-buffer steps with the solution history resident on the device, as
+ * HeatDiffuseOperation owns its SolutionHistory (heat_diffuse_operation.hpp:63):
+ * load_history copies a host T and T_old into the handle's device history; each
+ * time_step_resident uploads the step's host heat source (NULL: none) while the step
+ * starts, advances the history and copies the new T to T_out (NULL: no copy);
+ * store_history copies T and T_old back (either may be NULL). */
+int mpdg_heat_load_history(mpdg_heat *h, const double *T_host, const double *T_old_host);
+int mpdg_heat_store_history(mpdg_heat *h, double *T_host, double *T_old_host);
+int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params *prm, double dt,
+                                 double dt_old, const double *heat_source, double *T_out,
+                                 mpdg_step_stats *stats);
+
 /* ---- learned initial guess (no counterpart in the reference; the hook is the
  *      Predictor's type switch, predictor.hpp:122-154) ---------------------- */
 /* A 3D U-Net (4 levels, 16/32/48/64 channels, 3x3x3 convolutions, BF16 weights and

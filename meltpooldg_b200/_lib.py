@@ -133,6 +133,10 @@ _SIGS = {
                                       _D, C.POINTER(StepStats)]),
     "mpdg_heat_time_step_host": (C.c_int, [_H, C.POINTER(StepParams), C.c_double, C.c_double,
                                            _P, _P, _P, C.POINTER(StepStats)]),
+    "mpdg_heat_load_history": (C.c_int, [_H, _P, _P]),
+    "mpdg_heat_store_history": (C.c_int, [_H, _P, _P]),
+    "mpdg_heat_time_step_resident": (C.c_int, [_H, C.POINTER(StepParams), C.c_double,
+                                               C.c_double, _P, _P, C.POINTER(StepStats)]),
     "mpdg_heat_set_timing": (C.c_int, [_H, C.c_int]),
     "mpdg_heat_get_counters": (C.c_int, [_H, C.POINTER(Counters), C.c_int]),
     "mpdg_unet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_H)]),

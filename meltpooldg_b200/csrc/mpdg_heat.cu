@@ -151,6 +151,7 @@ struct mpdg_heat {
   cudaEvent_t ev_source = nullptr, ev_commit = nullptr, ev_inputs = nullptr;
   bool wait_source = false, record_commit = false;
   double *told_host = nullptr;  // host destination of the committed T_old (copy stream)
+  double *res_T = nullptr, *res_To = nullptr;  // device-resident history (time_step_resident)
 };
 
 static cudaEvent_t take_event(mpdg_heat *h)
@@ -2894,6 +2895,17 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
   return rc;
 }
 
+static int ensure_copy_stream(mpdg_heat *h)
+{
+  if (!h->copy_stream) {
+    CU(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&h->ev_source, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&h->ev_commit, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&h->ev_inputs, cudaEventDisableTiming));
+  }
+  return MPDG_OK;
+}
+
 extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *prm, double dt,
                                         double dt_old, double *T_cur, double *T_old,
                                         const double *heat_source, mpdg_step_stats *stats)
@@ -2905,12 +2917,7 @@ extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *pr
   TRY(dvec(h, &h->host_T, N));
   TRY(dvec(h, &h->host_To, N));
   if (heat_source) TRY(dvec(h, &h->host_q, N));
-  if (!h->copy_stream) {
-    CU(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-    CU(cudaEventCreateWithFlags(&h->ev_source, cudaEventDisableTiming));
-    CU(cudaEventCreateWithFlags(&h->ev_commit, cudaEventDisableTiming));
-    CU(cudaEventCreateWithFlags(&h->ev_inputs, cudaEventDisableTiming));
-  }
+  TRY(ensure_copy_stream(h));
   // T and T_old are needed first (predictor, history commit); the source only by
   // create_rhs, so its copy runs on the copy stream while the step starts
   CU(cudaMemcpyAsync(h->host_T, T_cur, vb, cudaMemcpyHostToDevice, h->stream));
@@ -2937,6 +2944,66 @@ extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *pr
   }
   CU(cudaMemcpyAsync(T_cur, h->host_T, vb, cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->copy_stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_load_history(mpdg_heat *h, const double *T_host, const double *T_old_host)
+{
+  if (!h || !T_host || !T_old_host) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  TRY(dvec(h, &h->res_T, N));
+  TRY(dvec(h, &h->res_To, N));
+  CU(cudaMemcpyAsync(h->res_T, T_host, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream));
+  CU(cudaMemcpyAsync(h->res_To, T_old_host, sizeof(double) * N, cudaMemcpyHostToDevice,
+                     h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_store_history(mpdg_heat *h, double *T_host, double *T_old_host)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  if (!h->res_T) return fail(MPDG_ERR_INVALID_ARGUMENT, "no resident history: call load_history");
+  CU(cudaSetDevice(h->device));
+  const size_t vb = sizeof(double) * h->n_dofs;
+  if (T_host) CU(cudaMemcpyAsync(T_host, h->res_T, vb, cudaMemcpyDeviceToHost, h->stream));
+  if (T_old_host) CU(cudaMemcpyAsync(T_old_host, h->res_To, vb, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params *prm, double dt,
+                                            double dt_old, const double *heat_source,
+                                            double *T_out, mpdg_step_stats *stats)
+{
+  if (!h || !prm) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (!h->res_T) return fail(MPDG_ERR_INVALID_ARGUMENT, "no resident history: call load_history");
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  const size_t vb = sizeof(double) * N;
+  if (heat_source) {
+    TRY(dvec(h, &h->host_q, N));
+    TRY(ensure_copy_stream(h));
+    // the source is first needed by create_rhs: its upload overlaps the predictor, the history
+    // commit and the first operator application (the previous source buffer is free: every
+    // call ends synchronised)
+    CU(cudaEventRecord(h->ev_inputs, h->stream));
+    CU(cudaStreamWaitEvent(h->copy_stream, h->ev_inputs, 0));
+    CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->copy_stream));
+    CU(cudaEventRecord(h->ev_source, h->copy_stream));
+  }
+  h->wait_source = heat_source != nullptr;
+  const int rc = mpdg_heat_time_step(h, prm, dt, dt_old, h->res_T, h->res_To,
+                                     heat_source ? h->host_q : nullptr, stats);
+  h->wait_source = false;
+  if (rc != MPDG_OK) {
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+    return rc;
+  }
+  if (T_out) CU(cudaMemcpyAsync(T_out, h->res_T, vb, cudaMemcpyDeviceToHost, h->stream));
+  if (h->copy_stream) CU(cudaStreamSynchronize(h->copy_stream));
   CU(cudaStreamSynchronize(h->stream));
   return MPDG_OK;
 }

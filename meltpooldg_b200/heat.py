@@ -400,6 +400,36 @@ class HeatDiffuseOperation:
         check(self.op._L.mpdg_heat_set_guess(self.op.h, _ptr(guess)))
         self._guess = guess
 
+    # host-buffer steps with the history resident on the device --------------------------
+    @staticmethod
+    def _host_ptr(t):
+        if t is None:
+            return None
+        if t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
+            raise ExcInvalidArgument("expected a contiguous host float64 tensor")
+        return C.c_void_p(t.data_ptr())
+
+    def load_history_host(self, T, T_old):
+        """Copy host T and T_old into the operator's device-resident history."""
+        check(self.op._L.mpdg_heat_load_history(self.op.h, self._host_ptr(T),
+                                                self._host_ptr(T_old)))
+
+    def store_history_host(self, T=None, T_old=None):
+        check(self.op._L.mpdg_heat_store_history(self.op.h, self._host_ptr(T),
+                                                 self._host_ptr(T_old)))
+
+    def solve_resident(self, dt: float, heat_source_host=None, T_out_host=None):
+        """One step on the resident history: uploads the host source, returns the new T
+        into T_out_host (pinned host tensors overlap the copies with the step)."""
+        st = L.StepStats()
+        rc = self.op._L.mpdg_heat_time_step_resident(
+            self.op.h, C.byref(self.params), float(dt), float(self.dt_old),
+            self._host_ptr(heat_source_host), self._host_ptr(T_out_host), C.byref(st))
+        self.last_stats = st
+        check(rc)
+        self.dt_old = float(dt)
+        return st
+
     def solve(self, dt: float):
         st = L.StepStats()
         rc = self.op._L.mpdg_heat_time_step(self.op.h, C.byref(self.params), float(dt),

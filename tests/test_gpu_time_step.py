@@ -186,6 +186,51 @@ def test_host_buffer_step_matches_device_step(precond):
         assert ref.abs().max() > 0.0
 
 
+@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_MG_F32])
+def test_resident_history_step_matches_device_step(precond):
+    """mpdg_heat_time_step_resident (history on the device, pinned host source in, new T
+    out) follows mpdg_heat_time_step on device vectors over three steps; store_history
+    returns both history vectors."""
+    op = H.HeatDiffuseOperator(H.box_mesh(3, (8, 8, 8)))
+    op.set_material(H.material(law=L.LAW_LINEAR_K, k=1.0, k1=0.5))
+    lin = H.LinearSolverData(preconditioner_type=precond, rel_tolerance=1e-10,
+                             abs_tolerance=0.0, cheb_picard=True)
+    dev = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    res = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    N, dt = op.n_dofs, 5e-4
+    T0 = torch.rand(N, dtype=torch.float64, device="cuda", generator=torch.Generator(
+        device="cuda").manual_seed(4))
+    op.distribute_constraints(T0)
+    dev.set_initial_condition(T0.clone())
+    res.load_history_host(T0.cpu().contiguous(), torch.zeros(N, dtype=torch.float64))
+    hq = torch.empty(N, dtype=torch.float64).pin_memory()
+    hT = torch.empty(N, dtype=torch.float64).pin_memory()
+    q = op.new_vector()
+    dev.heat_source = q
+    for s in range(3):
+        op.gaussian_source(q, 200.0, (0.3 + 0.1 * s, 0.5, 0.9), 0.1)
+        hq.copy_(q)
+        dev.solve(dt)
+        res.solve_resident(dt, hq, hT)
+        ref = dev.T.cpu()
+        assert (hT - ref).abs().max() <= 1e-8 * ref.abs().max()
+    T_back = torch.empty(N, dtype=torch.float64)
+    To_back = torch.empty(N, dtype=torch.float64)
+    res.store_history_host(T_back, To_back)
+    assert torch.equal(T_back, hT)
+    ref_old = dev.T_old.cpu()
+    assert (To_back - ref_old).abs().max() <= 1e-8 * ref_old.abs().max()
+    # a step without a source and without a copy back
+    res.solve_resident(dt)
+
+
+def test_resident_step_needs_a_loaded_history():
+    op = H.HeatDiffuseOperator(H.box_mesh(2, (4, 4, 4)))
+    res = H.HeatDiffuseOperation(op)
+    with pytest.raises(H.ExcInvalidArgument):
+        res.solve_resident(1e-3)
+
+
 # unidirectional_heat_transfer_with_velocity / _with_two_phase / _with_two_phase_rho_times_cp
 #   .mpirun=4.output: Robin terms on x = 0.1, dt = 1e-3, velocity (-0.01, 0), two-phase
 #   cases on the heaviside smoothed_heaviside(0.05 - y, 0.01) (the oracle's known-answer

@@ -620,6 +620,11 @@ static inline void material_eval(const orc_material *m, double T, double H, doub
 #undef MIX
 }
 
+void orc_material_eval(const orc_material *m, double T, double H, double out[4])
+{
+  material_eval(m, T, H, &out[0], &out[1], &out[2], &out[3]);
+}
+
 /* ------------------------------------------------------------------ */
 /* form 0: sum factorisation over cell batches                         */
 /* ------------------------------------------------------------------ */

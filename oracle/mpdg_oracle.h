@@ -91,6 +91,10 @@ void      orc_set_threads(int n);
 int orc_set_boundary(orc_heat *h, int face, int type, double h_conv, double T_inf_conv,
                      double emissivity, double T_inf_rad, double q_n);
 
+/* The material law at temperature T and heaviside H: out = {rho*cp, k, d(rho*cp)/dT, dk/dT}
+ * (the values the operator uses at a quadrature point). */
+void orc_material_eval(const orc_material *m, double T, double H, double out[4]);
+
 /* Operator coefficients: material law and time step (reset_time_increment).  Returns -1
  * if a velocity field is set and the law is the linear-k law. */
 int orc_set_material(orc_heat *h, const orc_material *m, double dt);

@@ -111,6 +111,8 @@ def lib():
             L.orc_set_threads.argtypes = [C.c_int]
             L.orc_set_material.argtypes = [_P, C.POINTER(Material), C.c_double]
             L.orc_set_fields.argtypes = [_P, _D, _D]
+            L.orc_material_eval.argtypes = [C.POINTER(Material), C.c_double, C.c_double, _D]
+            L.orc_material_eval.restype = None
             L.orc_vmult.argtypes = [_P, _D, _D, _D, _D, C.c_int]
             L.orc_inverse_diagonal.argtypes = [_P, _D, _D, _D, C.c_int]
             L.orc_create_rhs.argtypes = [_P, _D, _D, _D, _D]
@@ -161,6 +163,13 @@ def material(law=LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_s=
     m.cp_g = cp if cp_g is None else cp_g
     m.k_g = k if k_g is None else k_g
     return m
+
+
+def material_eval(m: Material, T: float, H: float = 1.0):
+    """(rho*cp, k, d(rho*cp)/dT, dk/dT) of the law at temperature T and heaviside H."""
+    out = np.zeros(4)
+    lib().orc_material_eval(C.byref(m), float(T), float(H), _ptr(out))
+    return tuple(out)
 
 
 class Oracle:

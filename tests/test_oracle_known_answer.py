@@ -190,3 +190,35 @@ def test_unidirectional_solidification_with_transport(case):
         dt_old = dt
         assert rc == 0
         assert _six_digits(o.l2_norm(T), ref), (o.l2_norm(T), ref)
+
+
+# unit_tests/material.cc / material.output: gas (k 10, cp 0, rho 1000), liquid (40, 1000, 8000),
+# solid (30, 900, 7000), mushy zone 0..100 K, smooth two-phase transition; evaluated at
+# (H, T) = (0.2, 20) and (0.6, 60). Rows: k, cp, rho, dk/dT, dcp/dT, drho/dT (printed with
+# 6 significant digits). The operator uses rho*cp = cp rho and d(rho*cp)/dT = dcp rho + drho cp.
+MATERIAL_OUTPUT = {
+    "gas": [(10, 0, 1000, 0, 0, 0), (10, 0, 1000, 0, 0, 0)],
+    "liquid": [(40, 1000, 8000, 0, 0, 0), (40, 1000, 8000, 0, 0, 0)],
+    "gas_liquid": [(16, 200, 2400, 0, 0, 0), (28, 600, 5200, 0, 0, 0)],
+    "liquid_solid": [(31.04, 910.4, 7104, 0.096, 0.96, 9.6),
+                     (36.48, 964.8, 7648, 0.144, 1.44, 14.4)],
+    "gas_liquid_solid": [(14.208, 182.08, 2220.8, 0.0192, 0.192, 1.92),
+                         (25.888, 578.88, 4988.8, 0.0864, 0.864, 8.64)],
+}
+
+
+@pytest.mark.parametrize("kind", list(MATERIAL_OUTPUT))
+def test_material_law_values(kind):
+    gas = dict(rho_g=1000.0, cp_g=0.0, k_g=10.0)
+    phases = dict(rho=8000.0, cp=1000.0, k=40.0, rho_s=7000.0, cp_s=900.0, k_s=30.0,
+                  T_solidus=0.0, T_liquidus=100.0)
+    laws = {"gas": O.material(rho=1000.0, cp=0.0, k=10.0),
+            "liquid": O.material(rho=8000.0, cp=1000.0, k=40.0),
+            "gas_liquid": O.material(O.LAW_GAS_LIQUID, **phases, **gas),
+            "liquid_solid": O.material(O.LAW_LIQUID_SOLID, **phases, **gas),
+            "gas_liquid_solid": O.material(O.LAW_GAS_LIQUID_SOLID, **phases, **gas)}
+    for (H, T), (k, cp, rho, dk, dcp, drho) in zip([(0.2, 20.0), (0.6, 60.0)],
+                                                   MATERIAL_OUTPUT[kind]):
+        rhocp, kk, drhocp, dkk = O.material_eval(laws[kind], T, H)
+        for got, want in [(kk, k), (dkk, dk), (rhocp, cp * rho), (drhocp, dcp * rho + drho * cp)]:
+            assert abs(got - want) <= 5e-6 * max(abs(want), 1e-300) or got == want, (got, want)

@@ -655,6 +655,76 @@ __global__ void __launch_bounds__(block_threads(n)) k_diag(CellArgs<double> a)
 }
 
 // ---------------------------------------------------------------------------
+// Tangent coefficient fields of the LAW 5 operator at the linearisation point, built once
+// per linearisation for the register-resident kernel's LAW 6: out[cell][8][n^3] =
+//   c   = (rho_cp / dt + d(rho_cp)/dT (T_lin - T_old) / dt) JxW + d(rho_cp)/dT (b.grad T_lin)
+//   k, rho_cp b (3), dk grad_ref T_lin (3)
+// with b = JxW J^-1 v and the gas-liquid weight w from a.cf (LAW 5 layout {w, 0, b}).
+// ---------------------------------------------------------------------------
+template <int n, int GEO>
+__global__ void __launch_bounds__(block_threads(n)) k_coef_tangent(CellArgs<double> a, double *out)
+{
+  using T = double;
+  constexpr int n2 = n * n, n3 = n2 * n, CPB = cells_per_block(n);
+  constexpr int NF = 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  const int cl = threadIdx.x / n2, line = threadIdx.x % n2;
+  T *x = sm + cl * NF * n3, *t1 = x + n3, *t2 = x + 2 * n3, *Tq = x + 3 * n3, *Tx = x + 4 * n3,
+    *Ty = x + 5 * n3, *Tz = x + 6 * n3, *To = x + 7 * n3;
+  const MeshDims &d = a.d;
+  const int64_t n_batches = (a.n_cells + CPB - 1) / CPB;
+  for (int64_t batch = blockIdx.x; batch < n_batches; batch += gridDim.x) {
+    const int64_t cell = batch * CPB + cl;
+    const bool active = cell < a.n_cells;
+    const int64_t cc = active ? cell : 0;
+    const int cx = (int)(cc % d.m[0]);
+    const int cy = (int)((cc / d.m[0]) % d.m[1]);
+    const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
+    const int j = line % n, k = line / n;
+    const int I0 = d.p * cx, J = d.p * cy + j, K = d.p * cz + k;
+    const int64_t row = (int64_t)d.nd[0] * (J + (int64_t)d.nd[1] * K) + I0;
+    T xv[n];
+    gather_xline<n>(d, row, I0, J, K, false, a.Tl, xv, active);
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i + n * line] = xv[i];
+    if (a.m.need_told) {
+      gather_xline<n>(d, row, I0, J, K, false, a.To, xv, active);
+#pragma unroll
+      for (int i = 0; i < n; ++i) To[i + n * line] = xv[i];
+    }
+    __syncthreads();
+    if (a.m.need_told) eval_values<n>(To, t1, t2, To, line);
+    eval_values<n>(x, t1, t2, Tq, line);
+    eval_gradients<n>(Tq, Tx, Ty, Tz, line);
+    if (active) {
+#pragma unroll
+      for (int r = 0; r < n; ++r) {
+        const int q = line + n2 * r;
+        T jxw, G[6];
+        geo_at<n, GEO>(a.g, cc, q % n, (q / n) % n, q / n2, jxw, G);
+        const T *cf = a.cf + cc * 5 * n3 + q;
+        T rhocp, kk, drhocp, dk;
+        mat_eval_w(a.m, Tq[q], __ldg(cf), rhocp, kk, drhocp, dk);
+        const T b0 = __ldg(cf + 2 * n3), b1 = __ldg(cf + 3 * n3), b2 = __ldg(cf + 4 * n3);
+        T c = a.m.idt * rhocp;
+        if (a.m.need_told) c += a.m.idt * drhocp * (Tq[q] - To[q]);
+        T *o = out + cc * 8 * n3 + q;
+        o[0] = c * jxw + drhocp * (b0 * Tx[q] + b1 * Ty[q] + b2 * Tz[q]);
+        o[n3] = kk;
+        o[2 * n3] = rhocp * b0;
+        o[3 * n3] = rhocp * b1;
+        o[4 * n3] = rhocp * b2;
+        o[5 * n3] = dk * Tx[q];
+        o[6 * n3] = dk * Ty[q];
+        o[7 * n3] = dk * Tz[q];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // L2 norm: sum over cells and q of u(q)^2 JxW (u read plain)
 // ---------------------------------------------------------------------------
 template <int n, int GEO>
@@ -708,5 +778,6 @@ template <int n, typename T> constexpr size_t smem_vmult(bool tdep)
 template <int n> constexpr size_t smem_rhs() { return sizeof(double) * cells_per_block(n) * 9 * n * n * n; }
 template <int n> constexpr size_t smem_diag() { return sizeof(double) * cells_per_block(n) * 16 * n * n * n; }
 template <int n> constexpr size_t smem_norm() { return sizeof(double) * cells_per_block(n) * 4 * n * n * n; }
+template <int n> constexpr size_t smem_coef_tangent() { return sizeof(double) * cells_per_block(n) * 8 * n * n * n; }
 
 }  // namespace mpdg

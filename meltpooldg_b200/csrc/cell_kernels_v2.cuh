@@ -245,7 +245,8 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
   constexpr int CW = v2_cells_per_warp<n>();
   constexpr int CS = v2_cell_stride<n>();
   constexpr int NCOEF = v2_ncoef<LAW>();
-  // LAW 3: conductivity field k(q), no tangent; LAW 4: coefficient fields a.cf
+  // LAW 3: conductivity field k(q), no tangent; LAW 4: coefficient fields a.cf; LAW 6: the
+  // tangent coefficient fields of LAW 5 built at the linearisation point (8 per point)
   constexpr bool TDEP = LAW == 1 || LAW == 2;
   if (a.st && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -293,9 +294,10 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           for (int off = t * 128; off < n * n * n * 4; off += n * 128)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(kq + off));
         }
-        if (LAW == 4) {
-          constexpr int bytes = 5 * n * n * n * (int)sizeof(T);
-          const char *cf = reinterpret_cast<const char *>(a.cf + ncell * 5 * (n * n * n));
+        if (LAW == 4 || LAW == 6) {
+          constexpr int nf = LAW == 4 ? 5 : 8;
+          constexpr int bytes = nf * n * n * n * (int)sizeof(T);
+          const char *cf = reinterpret_cast<const char *>(a.cf + ncell * nf * (n * n * n));
           for (int off = t * 128; off < bytes; off += n * 128)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(cf + off));
         }
@@ -387,6 +389,17 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           f1 = kk * Uy[k][j];
           f2 = kk * Uz[k][j];
           cval = T(0);
+        } else if (LAW == 6) {
+          // c u + rho_cp b.grad(u), flux k grad(u) + dk grad(T_lin) u
+          constexpr int npt = n * n * n;
+          const T *cf = a.cf + cc * 8 * npt + t + n * (j + n * k);
+          kk = __ldg(cf + npt);
+          val = __ldg(cf) * uu + __ldg(cf + 2 * npt) * Ux[k][j] + __ldg(cf + 3 * npt) * Uy[k][j] +
+                __ldg(cf + 4 * npt) * Uz[k][j];
+          f0 = kk * Ux[k][j] + __ldg(cf + 5 * npt) * uu;
+          f1 = kk * Uy[k][j] + __ldg(cf + 6 * npt) * uu;
+          f2 = kk * Uz[k][j] + __ldg(cf + 7 * npt) * uu;
+          cval = T(0);
         } else if (TDEP) {
           const int pt = k * n + j;
           kk = coef[(0 * n * n + pt) * 32 + lane];
@@ -406,7 +419,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
         }
         T F0, F1, F2;
         apply_G<GEO>(G, f0, f1, f2, F0, F1, F2);
-        U[k][j] = LAW == 4 ? val : cval * uu * jxw;
+        U[k][j] = (LAW == 4 || LAW == 6) ? val : cval * uu * jxw;
         Ux[k][j] = F0;
         Uy[k][j] = F1;
         Uz[k][j] = F2;

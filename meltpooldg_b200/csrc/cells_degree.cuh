@@ -117,6 +117,13 @@ struct DegreeOps {
     }
     if (law == 4) return geo == 0 ? vmult_t<T, 0, 4>(a, s, sm) : vmult_t<T, 1, 4>(a, s, sm);
     if (law == 5) return geo == 0 ? vmult_t<T, 0, 5>(a, s, sm) : vmult_t<T, 1, 5>(a, s, sm);
+    if (law == 6) {
+      if constexpr (use_v2<T>()) {
+        return geo == 0 ? vmult_t<T, 0, 6>(a, s, sm) : vmult_t<T, 1, 6>(a, s, sm);
+      } else {
+        return cudaErrorNotSupported;
+      }
+    }
     if (geo == 0) {
       if (law == 0) return vmult_t<T, 0, 0>(a, s, sm);
       if (law == 1) return vmult_t<T, 0, 1>(a, s, sm);
@@ -235,6 +242,21 @@ struct DegreeOps {
   {
     return geo == 0 ? diag_picard_t<0>(a, s, sm) : diag_picard_t<1>(a, s, sm);
   }
+  template <int GEO>
+  static cudaError_t coef_tangent_t(const CellArgs<double> &a, double *out, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_coef_tangent<n, GEO>;
+    const size_t smem = smem_coef_tangent<n>();
+    const int g = persistent_grid(k, THREADS, smem, (a.n_cells + CPB - 1) / CPB, sm, &cache);
+    k<<<g, THREADS, smem, s>>>(a, out);
+    return cudaGetLastError();
+  }
+  static cudaError_t coef_tangent(const CellArgs<double> &a, double *out, int geo, cudaStream_t s,
+                                  int sm)
+  {
+    return geo == 0 ? coef_tangent_t<0>(a, out, s, sm) : coef_tangent_t<1>(a, out, s, sm);
+  }
   static cudaError_t conductivity_q(const CellArgs<double> &a, float *kq, int law, cudaStream_t s,
                                     int sm)
   {
@@ -253,6 +275,9 @@ struct DegreeOps {
     t.rhs = &rhs;
     t.diag = &diag;
     t.norm = &norm;
+    t.coef_tangent = &coef_tangent;
+    t.v2_d = use_v2<double>();
+    t.v2_f = use_v2<float>();
     if constexpr (use_v2<float>()) {
       t.conductivity_q = &conductivity_q;
       t.diag_picard = &diag_picard;

@@ -18,6 +18,11 @@ struct DegreeTable {
   // kq[cell][q] = k(T_lin) in FP32; nullptr where the degree has no register-resident kernel
   cudaError_t (*conductivity_q)(const CellArgs<double> &, float *kq, int law, cudaStream_t,
                                 int sm) = nullptr;
+  // tangent coefficient fields of the LAW 5 operator at a.Tl (8 per point, FP64)
+  cudaError_t (*coef_tangent)(const CellArgs<double> &, double *out, int geo, cudaStream_t,
+                              int sm) = nullptr;
+  // the register-resident operator kernel exists for this degree (FP64 / FP32)
+  bool v2_d = false, v2_f = false;
   // a.dst += diagonal of the FP32 Picard operator (conductivity field a.kq); same degrees
   cudaError_t (*diag_picard)(const CellArgs<float> &, int geo, cudaStream_t, int sm) = nullptr;
 };

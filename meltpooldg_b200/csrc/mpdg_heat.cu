@@ -111,6 +111,11 @@ struct mpdg_heat {
   double *cf = nullptr;
   float *cf_f = nullptr;
   bool cf_dirty = true, cf_f_dirty = true;
+  // tangent coefficient fields of the LAW 5 operator at the linearisation point (8 per
+  // point, for the register-resident kernel's LAW 6) and their FP32 copy
+  double *tf = nullptr;
+  float *tf_f = nullptr;
+  bool tf_dirty = true, tf_f_dirty = true;
   // GMRES basis (m + 1 vectors) and small device buffers
   double *gV = nullptr;
   int gV_m = 0;
@@ -1218,6 +1223,24 @@ static int ensure_fields(mpdg_heat *h)
   return MPDG_OK;
 }
 
+// (re)build the LAW 5 tangent coefficient fields at the current linearisation point
+static int ensure_tangent(mpdg_heat *h)
+{
+  if (!h->tf_dirty) return MPDG_OK;
+  TRY(ensure_fields(h));
+  TRY(dvec(h, &h->tf, h->n_cells * 8 * h->npt));
+  CellArgs<double> a = cell_args<double>(h);
+  a.g.q = h->geoq;
+  a.cf = h->cf;
+  a.Tl = h->T_lin;
+  a.To = h->T_old;
+  CU(h->tab.coef_tangent(a, h->tf, h->geo, h->stream, h->sm_count));
+  ++h->launches;
+  h->tf_dirty = false;
+  h->tf_f_dirty = true;
+  return MPDG_OK;
+}
+
 static int ensure_lin(mpdg_heat *h)
 {
   if (law_tdep(h) && !h->T_lin)
@@ -1296,6 +1319,12 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
   CellArgs<double> a = cell_args<double>(h);
   a.g.q = h->geoq;
   a.cf = h->cf;
+  int law = klaw(h);
+  if (law == 5 && h->tab.v2_d) {
+    TRY(ensure_tangent(h));
+    a.cf = h->tf;
+    law = 6;
+  }
   a.src = src;
   a.dst = dst;
   a.Tl = h->T_lin;
@@ -1315,7 +1344,7 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
     TRY(launch_faces<double>(h, 0, dst, src, h->T_lin, fin != FIN_NONE ? h->face_dot : nullptr, st));
     if (fin != FIN_NONE) a.extra_dot = h->face_dot;
   }
-  CU(h->tab.vmult_d(a, h->geo, klaw(h), h->stream, h->sm_count));
+  CU(h->tab.vmult_d(a, h->geo, law, h->stream, h->sm_count));
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
     h->ev64.push_back({e0, e1});
@@ -1369,6 +1398,19 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
   CellArgs<float> a = cell_args<float>(h);
   a.kq = h->kq;
   a.cf = h->cf_f;
+  int law = picard ? 3 : klaw(h);
+  if (law == 5 && h->tab.v2_f) {
+    TRY(ensure_tangent(h));
+    const int64_t nt = h->n_cells * 8 * h->npt;
+    if (h->tf_f_dirty) {
+      TRY(dvec(h, &h->tf_f, nt));
+      k_cast_f<<<vgrid(h, nt), VT, 0, h->stream>>>(nt, h->tf, h->tf_f); ++h->launches;
+      CU(cudaGetLastError());
+      h->tf_f_dirty = false;
+    }
+    a.cf = h->tf_f;
+    law = 6;
+  }
   a.g.q = h->geoq_f;
   a.src = src;
   a.dst = dst;
@@ -1382,7 +1424,7 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
     cudaEventRecord(e0, h->stream);
   }
   if (any_faces(h)) TRY(launch_faces<float>(h, 0, dst, src, h->T_lin_f, nullptr, st));
-  CU(h->tab.vmult_f(a, h->geo, picard ? 3 : klaw(h), h->stream, h->sm_count));
+  CU(h->tab.vmult_f(a, h->geo, law, h->stream, h->sm_count));
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
     h->ev32.push_back({e0, e1});
@@ -1720,6 +1762,7 @@ static int mg_setup(mpdg_heat *h, const mpdg_solver_params *prm, bool picard)
       c->T_lin = fT ? v.Tl : nullptr;
       c->T_old = fTo ? v.To : nullptr;
       c->lin_f_dirty = true;
+      c->tf_dirty = true;
       TRY(refresh_f32(c));
       if (picard) {
         TRY(dvec(c, &c->kq, c->n_cells * c->npt));
@@ -2406,6 +2449,7 @@ extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
   h->diag_valid = false;
   h->eig_valid = false;
   h->cf_dirty = true;
+  h->tf_dirty = true;
   return MPDG_OK;
 }
 
@@ -2417,6 +2461,7 @@ extern "C" int mpdg_heat_set_fields(mpdg_heat *h, const double *heaviside, const
   h->Hf = heaviside;
   h->vel = velocity;
   h->cf_dirty = true;
+  h->tf_dirty = true;
   h->diag_valid = false;
   h->eig_valid = false;
   return MPDG_OK;
@@ -2442,6 +2487,7 @@ extern "C" int mpdg_heat_set_boundary(mpdg_heat *h, int face, int type, double h
   h->bTr[face] = T_inf_rad;
   h->bqn[face] = q_n;
   h->lin_f_dirty = true;
+  h->tf_dirty = true;
   h->diag_valid = false;
   h->eig_valid = false;
   return MPDG_OK;
@@ -2450,6 +2496,7 @@ extern "C" int mpdg_heat_set_boundary(mpdg_heat *h, int face, int type, double h
 extern "C" int mpdg_heat_reset_time_increment(mpdg_heat *h, double dt)
 {
   if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  if (dt != h->dt) h->tf_dirty = true;
   h->dt = dt;
   h->eig_valid = false;
   return MPDG_OK;
@@ -2461,6 +2508,7 @@ extern "C" int mpdg_heat_set_linearization(mpdg_heat *h, const double *T, const 
   h->T_lin = T;
   h->T_old = T_old;
   h->lin_f_dirty = true;
+  h->tf_dirty = true;
   return MPDG_OK;
 }
 
@@ -2810,6 +2858,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     h->T_lin = T_cur;
     h->T_old = T_old;
     h->lin_f_dirty = true;
+    h->tf_dirty = true;
     // JacobiPreconditioner::update; the multigrid preconditioner on the Picard operator
     // needs the FP64 diagonal only for a new Lanczos estimate
     const bool mg_picard = prm->linear.preconditioner == MPDG_PRECOND_MG_F32 &&
@@ -2874,6 +2923,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
         k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1); ++h->launches;
         if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
         h->lin_f_dirty = true;
+        h->tf_dirty = true;
         s.newton_iterations = i + 1;
       }
       if (rc == MPDG_OK && !s.converged)
@@ -3252,6 +3302,7 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
     h->T_lin = guess;
     h->T_old = T;
     h->lin_f_dirty = true;
+    h->tf_dirty = true;
     CU(cudaMemsetAsync(h->w2, 0, sizeof(double) * N, h->stream));
     int rr = create_rhs(h, h->w2, T, heat_source);               // r = -R(LE)
     if (rr == MPDG_OK) {
@@ -3261,6 +3312,7 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
     h->T_lin = keepT;
     h->T_old = keepTo;
     h->lin_f_dirty = true;
+    h->tf_dirty = true;
     TRY(rr);
     double jj = 0.0, rj_plus = 0.0;
     TRY(norms(h, h->w3, nullptr, &jj, nullptr));

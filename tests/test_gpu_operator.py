@@ -515,3 +515,27 @@ def test_fields_reject_unsupported_combinations():
         g2.set_material(H.material(law=law, rho_g=0.5))
         with pytest.raises(H.ExcInvalidArgument):
             g2.vmult(g2.new_vector(), g2.new_vector())
+
+
+@pytest.mark.parametrize("degree", [2, 3])
+def test_tangent_fields_follow_the_linearisation_point(degree):
+    """The three-phase operator's coefficient fields are rebuilt after set_linearization,
+    reset_time_increment and set_fields (FP64 and FP32)."""
+    o, g = transport_pair(degree, (4, 3, 3), 0.1, "three_phase_sharp_vs_velocity")
+    rng = np.random.default_rng(21)
+    N = o.n_dofs
+    src = rng.uniform(-1, 1, N)
+    for it in range(3):
+        T, To = rng.uniform(0, 1, N), rng.uniform(0, 1, N)
+        if it == 1:
+            o.set_material(o._material, 3e-3)
+            g.reset_time_increment(3e-3)
+        if it == 2:
+            x = o.support_points()
+            Hf = 0.5 + 0.5 * np.tanh((x[:, 2] - 0.3) / 0.1)
+            o.set_fields(Hf, None)
+            g.set_fields(cuda(Hf), None)
+        g.set_linearization(cuda(T), cuda(To))
+        ref = o.vmult(src, T, To)
+        assert rel(g.vmult(g.new_vector(), cuda(src)), ref) <= TOL64
+        assert rel(g.vmult(g.new_vector(torch.float32), cuda(src, torch.float32)), ref) <= TOL32

@@ -136,6 +136,15 @@ void mpdg_solver_params_default(mpdg_solver_params *prm);
 
 /* ---- lifetime (ScratchData::build + operator construction) ----------- */
 int mpdg_heat_create(const mpdg_mesh_desc *desc, int device, mpdg_heat **out);
+/* One rank's part of a z-slab decomposition of the box `global` (the partitioning of the
+ * reference's distributed triangulation, replaced by a structured split): the cells with
+ * z index in [z_begin, z_end), same vertices as the global mesh (its perturbation
+ * included), Dirichlet faces of the global mesh only (the slab's interior z faces carry
+ * none). DoF planes K = p z_begin .. p z_end of the global grid are local planes
+ * 0 .. p (z_end - z_begin); the two end planes are shared with the neighbouring slabs,
+ * whose partial sums the caller adds after each assembly (vmult, diagonal, rhs). */
+int mpdg_heat_create_slab(const mpdg_mesh_desc *global, int z_begin, int z_end, int device,
+                          mpdg_heat **out);
 int mpdg_heat_destroy(mpdg_heat *h);
 /* Enqueue all work of this handle on `stream` (a cudaStream_t; NULL = legacy default). */
 int mpdg_heat_set_stream(mpdg_heat *h, void *stream);
@@ -201,6 +210,9 @@ int mpdg_heat_inverse_diagonal_f32_picard(mpdg_heat *h, float *inv_diag);
 /* compute_inverse_diagonal_from_matrixfree (heat_diffuse_operator.cpp:271-284):
  * diag(J) inverted with |d| > 1e-10 ? 1/d : 1. */
 int mpdg_heat_compute_inverse_diagonal(mpdg_heat *h, double *inv_diag);
+/* diag(J) itself (constrained rows 0): the partial diagonal of a slab, summed over the
+ * shared planes before it is inverted. */
+int mpdg_heat_compute_diagonal(mpdg_heat *h, double *diag);
 /* create_rhs(dst, src) (heat_diffuse_operator.cpp:783-806): dst += -R(T) with T the
  * linearisation point, src = temperature_old, heat_source the nodal source vector
  * (may be NULL for zero); dst is not zeroed. */

@@ -99,6 +99,8 @@ _SIGS = {
     "mpdg_solver_params_default": (None, [C.POINTER(SolverParams)]),
     "mpdg_step_params_default": (None, [C.POINTER(StepParams)]),
     "mpdg_heat_create": (C.c_int, [C.POINTER(MeshDesc), C.c_int, C.POINTER(_H)]),
+    "mpdg_heat_create_slab": (C.c_int, [C.POINTER(MeshDesc), C.c_int, C.c_int, C.c_int,
+                                        C.POINTER(_H)]),
     "mpdg_heat_destroy": (C.c_int, [_H]),
     "mpdg_heat_set_stream": (C.c_int, [_H, _P]),
     "mpdg_heat_n_dofs": (C.c_int, [_H, C.POINTER(C.c_int64)]),
@@ -116,6 +118,7 @@ _SIGS = {
     "mpdg_heat_vmult_f32_picard": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_inverse_diagonal_f32_picard": (C.c_int, [_H, _D]),
     "mpdg_heat_compute_inverse_diagonal": (C.c_int, [_H, _D]),
+    "mpdg_heat_compute_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),
     "mpdg_heat_distribute_constraints": (C.c_int, [_H, _D]),
     "mpdg_heat_l2_norm": (C.c_int, [_H, _D, C.POINTER(C.c_double)]),

@@ -1589,7 +1589,7 @@ static void release(mpdg_heat *h);
 static std::vector<double> box_vertices(const mpdg_mesh_desc &desc);
 static int create_impl(const mpdg_mesh_desc *desc, int device, const std::vector<double> *verts,
                        mpdg_heat **out);
-static int compute_diag(mpdg_heat *h, double *d);
+static int compute_diag(mpdg_heat *h, double *d, bool invert = true);
 
 static void cheb_coefficients(double theta, double delta, int k, std::vector<float> &c1,
                               std::vector<float> &c2)
@@ -2292,6 +2292,30 @@ extern "C" int mpdg_heat_create(const mpdg_mesh_desc *desc, int device, mpdg_hea
   return create_impl(desc, device, nullptr, out);
 }
 
+extern "C" int mpdg_heat_create_slab(const mpdg_mesh_desc *global, int z_begin, int z_end,
+                                     int device, mpdg_heat **out)
+{
+  if (!global || !out) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (z_begin < 0 || z_end > global->cells[2] || z_end <= z_begin || global->cells[0] < 1 ||
+      global->cells[1] < 1)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "slab range outside the mesh");
+  mpdg_mesh_desc d = *global;
+  d.cells[2] = z_end - z_begin;
+  const double hz = (global->hi[2] - global->lo[2]) / global->cells[2];
+  d.lo[2] = global->lo[2] + hz * z_begin;
+  d.hi[2] = z_end == global->cells[2] ? global->hi[2] : global->lo[2] + hz * z_end;
+  if (z_begin > 0) d.dirichlet_mask &= ~16;
+  if (z_end < global->cells[2]) d.dirichlet_mask &= ~32;
+  if (!(global->perturb > 0.0)) return create_impl(&d, device, nullptr, out);
+  // the global mesh's vertex planes z_begin .. z_end
+  const std::vector<double> all = box_vertices(*global);
+  const int64_t plane = (int64_t)(global->cells[0] + 1) * (global->cells[1] + 1);
+  std::vector<double> verts(all.begin() + 3 * plane * z_begin,
+                            all.begin() + 3 * plane * (z_end + 1));
+  return create_impl(&d, device, &verts, out);
+}
+
 static int create_impl(const mpdg_mesh_desc *desc, int device, const std::vector<double> *verts,
                        mpdg_heat **out)
 {
@@ -2563,7 +2587,7 @@ extern "C" int mpdg_heat_inverse_diagonal_f32_picard(mpdg_heat *h, float *inv_di
   return MPDG_OK;
 }
 
-static int compute_diag(mpdg_heat *h, double *d)
+static int compute_diag(mpdg_heat *h, double *d, bool invert)
 {
   TRY(ensure_dt(h));
   TRY(ensure_lin(h));
@@ -2578,6 +2602,10 @@ static int compute_diag(mpdg_heat *h, double *d)
   CU(h->tab.diag(a, h->geo, klaw(h), h->stream, h->sm_count));
   ++h->launches;
   if (any_faces(h)) TRY(launch_faces<double>(h, 2, d, nullptr, h->T_lin, nullptr, nullptr));
+  if (!invert) {
+    CU(cudaGetLastError());
+    return MPDG_OK;
+  }
   k_invert_diag<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, d); ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;
@@ -2588,6 +2616,13 @@ extern "C" int mpdg_heat_compute_inverse_diagonal(mpdg_heat *h, double *inv_diag
   if (!h || !inv_diag) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   CU(cudaSetDevice(h->device));
   return compute_diag(h, inv_diag);
+}
+
+extern "C" int mpdg_heat_compute_diagonal(mpdg_heat *h, double *diag)
+{
+  if (!h || !diag) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  return compute_diag(h, diag, false);
 }
 
 static int create_rhs(mpdg_heat *h, double *dst, const double *src, const double *q)

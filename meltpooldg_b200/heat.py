@@ -182,12 +182,18 @@ def _ptr(t: torch.Tensor | None, dtype=torch.float64):
 class HeatDiffuseOperator:
     """Matrix-free heat tangent operator on one GPU (OperatorMatrixFree verbs)."""
 
-    def __init__(self, mesh: L.MeshDesc, device: int = 0):
+    def __init__(self, mesh: L.MeshDesc, device: int = 0, slab=None):
+        """slab=(z_begin, z_end): this rank's z-slab of cells of the global mesh `mesh`
+        (mpdg_heat_create_slab); the shared end planes are summed by the caller."""
         self._L = L.load()
         self.mesh = mesh
         self.device = torch.device("cuda", device)
         h = C.c_void_p()
-        check(self._L.mpdg_heat_create(C.byref(mesh), device, C.byref(h)))
+        if slab is None:
+            check(self._L.mpdg_heat_create(C.byref(mesh), device, C.byref(h)))
+        else:
+            check(self._L.mpdg_heat_create_slab(C.byref(mesh), int(slab[0]), int(slab[1]),
+                                                device, C.byref(h)))
         self.h = h
         n = C.c_int64()
         check(self._L.mpdg_heat_n_dofs(h, C.byref(n)))
@@ -277,6 +283,11 @@ class HeatDiffuseOperator:
 
     def compute_inverse_diagonal_from_matrixfree(self, diag):
         check(self._L.mpdg_heat_compute_inverse_diagonal(self.h, _ptr(diag)))
+        return diag
+
+    def compute_diagonal(self, diag):
+        """diag(J), not inverted (constrained rows 0)."""
+        check(self._L.mpdg_heat_compute_diagonal(self.h, _ptr(diag)))
         return diag
 
     def create_rhs(self, dst, src, heat_source=None):

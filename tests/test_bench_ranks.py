@@ -38,7 +38,7 @@ def _rank(rank, world, port, values, out):
 def test_two_gloo_ranks_take_the_slowest_time():
     world = 2
     values = [3.25, 7.5]
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of this process
         out = m.dict()
         mp.start_processes(_rank, args=(world, _free_port(), values, out), nprocs=world,
                            join=True, start_method="spawn")

@@ -725,6 +725,59 @@ __global__ void __launch_bounds__(block_threads(n)) k_coef_tangent(CellArgs<doub
 }
 
 // ---------------------------------------------------------------------------
+// Values of the heaviside field H and the velocity field v (component-major, 3 x N) at the
+// quadrature points, sum-factorised: cf[cell][0][q] = H (1 without a field),
+// cf[cell][2 + e][q] = v_e (0 without a field); the per-point coefficient set-up then reads
+// them in place.
+// ---------------------------------------------------------------------------
+template <int n>
+__global__ void __launch_bounds__(block_threads(n)) k_field_values(CellArgs<double> a,
+                                                                   const double *H,
+                                                                   const double *vel,
+                                                                   int64_t n_dofs, double *cf)
+{
+  using T = double;
+  constexpr int n2 = n * n, n3 = n2 * n, CPB = cells_per_block(n);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  const int cl = threadIdx.x / n2, line = threadIdx.x % n2;
+  T *u = sm + cl * 4 * n3, *t1 = u + n3, *t2 = u + 2 * n3, *vq = u + 3 * n3;
+  const MeshDims &d = a.d;
+  const int64_t n_batches = (a.n_cells + CPB - 1) / CPB;
+  for (int64_t batch = blockIdx.x; batch < n_batches; batch += gridDim.x) {
+    const int64_t cell = batch * CPB + cl;
+    const bool active = cell < a.n_cells;
+    const int64_t cc = active ? cell : 0;
+    const int cx = (int)(cc % d.m[0]);
+    const int cy = (int)((cc / d.m[0]) % d.m[1]);
+    const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
+    const int j = line % n, k = line / n;
+    const int I0 = d.p * cx, J = d.p * cy + j, K = d.p * cz + k;
+    const int64_t row = (int64_t)d.nd[0] * (J + (int64_t)d.nd[1] * K) + I0;
+    for (int f = 0; f < 4; ++f) {
+      const double *g = f == 0 ? H : (vel ? vel + (int64_t)(f - 1) * n_dofs : nullptr);
+      const int slot = f == 0 ? 0 : f + 1;
+      if (!g) {
+        if (active)
+#pragma unroll
+          for (int r = 0; r < n; ++r) cf[cc * 5 * n3 + slot * n3 + line + n2 * r] = f == 0 ? 1.0 : 0.0;
+        continue;
+      }
+      T x[n];
+      gather_xline<n>(d, row, I0, J, K, false, g, x, active);
+#pragma unroll
+      for (int i = 0; i < n; ++i) u[i + n * line] = x[i];
+      __syncthreads();
+      eval_values<n>(u, t1, t2, vq, line);
+      if (active)
+#pragma unroll
+        for (int r = 0; r < n; ++r) cf[cc * 5 * n3 + slot * n3 + line + n2 * r] = vq[line + n2 * r];
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // L2 norm: sum over cells and q of u(q)^2 JxW (u read plain)
 // ---------------------------------------------------------------------------
 template <int n, int GEO>

@@ -257,6 +257,16 @@ struct DegreeOps {
   {
     return geo == 0 ? coef_tangent_t<0>(a, out, s, sm) : coef_tangent_t<1>(a, out, s, sm);
   }
+  static cudaError_t field_values(const CellArgs<double> &a, const double *H, const double *vel,
+                                  int64_t n_dofs, double *cf, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_field_values<n>;
+    const size_t smem = smem_norm<n>();
+    const int g = persistent_grid(k, THREADS, smem, (a.n_cells + CPB - 1) / CPB, sm, &cache);
+    k<<<g, THREADS, smem, s>>>(a, H, vel, n_dofs, cf);
+    return cudaGetLastError();
+  }
   static cudaError_t conductivity_q(const CellArgs<double> &a, float *kq, int law, cudaStream_t s,
                                     int sm)
   {
@@ -276,6 +286,7 @@ struct DegreeOps {
     t.diag = &diag;
     t.norm = &norm;
     t.coef_tangent = &coef_tangent;
+    t.field_values = &field_values;
     t.v2_d = use_v2<double>();
     t.v2_f = use_v2<float>();
     if constexpr (use_v2<float>()) {

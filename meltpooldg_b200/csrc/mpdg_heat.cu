@@ -320,15 +320,16 @@ __global__ void k_geometry(int64_t n_cells, MeshDims d, int n, Q1D q1, const dou
 // the product of the mixed density and capacity or the mixed volume-specific capacity
 // (heat_diffuse_operator.cpp:1138-1162).  Without a heaviside field w = 1 (liquid
 // properties, the constant law).  J^-1 v turns v.grad(u) into a contraction with the
-// reference gradient.  One thread per (cell, point); the interpolation is a direct
-// n^3-term sum (a set-up pass, run when the fields or the material change).
+// reference gradient.  The field values at the points come from the sum-factorised
+// k_field_values, written into the slots of cf that this kernel then overwrites (each thread
+// reads and writes only its own point); one thread per (cell, point).
 struct FieldArgs {
   MeshDims d;
   int n, geo, mode;
   int64_t n_cells, n_dofs;
   double hc[3];
-  double xg[8], wg[8], S[8][8];
-  const double *vert, *H, *vel;
+  double xg[8], wg[8];
+  const double *vert, *H, *vel;  // H, vel: presence flags (their values come through cf)
   int mix, sharp, vs;
   double rho_l, cp_l, k_l, rho_g, cp_g, k_g;
   double *cf;
@@ -345,20 +346,9 @@ __global__ void k_coef_fields(FieldArgs a)
     const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
     const int cx = (int)(c % a.d.m[0]), cy = (int)((c / a.d.m[0]) % a.d.m[1]),
               cz = (int)(c / ((int64_t)a.d.m[0] * a.d.m[1]));
-    const int64_t base =
-      (int64_t)a.d.p * cx + (int64_t)a.d.nd[0] * ((int64_t)a.d.p * cy + (int64_t)a.d.nd[1] * a.d.p * cz);
-    double Hq = 0.0, v[3] = {0.0, 0.0, 0.0};
-    for (int k = 0; k < n; ++k)
-      for (int j = 0; j < n; ++j) {
-        const double wjk = a.S[qk][k] * a.S[qj][j];
-        const int64_t row = base + (int64_t)a.d.nd[0] * (j + (int64_t)a.d.nd[1] * k);
-        for (int i = 0; i < n; ++i) {
-          const double w = wjk * a.S[qi][i];
-          if (a.H) Hq += w * a.H[row + i];
-          if (a.vel)
-            for (int e = 0; e < 3; ++e) v[e] += w * a.vel[(int64_t)e * a.n_dofs + row + i];
-        }
-      }
+    double *o = a.cf + c * 5 * npt + q;
+    const double Hq = o[0];
+    const double v[3] = {o[2 * npt], o[3 * npt], o[4 * npt]};
     const double w = !a.mix ? 1.0 : (!a.H ? 1.0 : (a.sharp ? (Hq > 0.5 ? 1.0 : 0.0) : Hq));
     const double kk = (1.0 - w) * a.k_g + w * a.k_l;
     const double rhocp = a.vs ? (1.0 - w) * (a.rho_g * a.cp_g) + w * (a.rho_l * a.cp_l)
@@ -383,7 +373,6 @@ __global__ void k_coef_fields(FieldArgs a)
         }
     }
     const double jxw = det * a.wg[qi] * a.wg[qj] * a.wg[qk];
-    double *o = a.cf + c * 5 * npt + q;
     const double s = a.mode == 5 ? jxw : jxw * rhocp;
     o[0] = a.mode == 5 ? w : rhocp * jxw;
     o[npt] = a.mode == 5 ? 0.0 : kk;
@@ -1200,7 +1189,6 @@ static int ensure_fields(mpdg_heat *h)
   for (int q = 0; q < h->n; ++q) {
     a.xg[q] = t1.xg[q];
     a.wg[q] = t1.wg[q];
-    for (int i = 0; i < h->n; ++i) a.S[q][i] = t1.A[kS][q][i];
   }
   a.vert = h->vert;
   a.H = h->Hf;
@@ -1215,6 +1203,11 @@ static int ensure_fields(mpdg_heat *h)
   a.cp_g = h->mat.cp_g;
   a.k_g = h->mat.k_g;
   a.cf = h->cf;
+  {
+    CellArgs<double> ca = cell_args<double>(h);
+    CU(h->tab.field_values(ca, h->Hf, h->vel, h->n_dofs, h->cf, h->stream, h->sm_count));
+    ++h->launches;
+  }
   const int64_t total = h->n_cells * h->npt;
   k_coef_fields<<<vgrid(h, total), VT, 0, h->stream>>>(a); ++h->launches;
   CU(cudaGetLastError());

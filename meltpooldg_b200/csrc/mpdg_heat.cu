@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "../../include/mpdg_heat.h"
@@ -157,6 +158,11 @@ struct mpdg_heat {
   bool wait_source = false, record_commit = false;
   double *told_host = nullptr;  // host destination of the committed T_old (copy stream)
   double *res_T = nullptr, *res_To = nullptr;  // device-resident history (time_step_resident)
+  // one iteration of the mixed-precision CG as a CUDA graph (recorded on cap_stream, replayed
+  // on stream) and the kernel launches / operator applications one replay performs
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t body_exec = nullptr;
+  int64_t body_launches = 0, body_vm64 = 0, body_vm32 = 0;
 };
 
 static cudaEvent_t take_event(mpdg_heat *h)
@@ -1908,6 +1914,95 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
 }
 
 // ---------------------------------------------------------------------------
+// CUDA graph of one solver iteration
+//
+// An iteration of the mixed-precision CG issues ~250 launches (the FP64 operator, the vector
+// updates and the V-cycle's smoothing, transfer and coarse-level kernels, many of them a few
+// microseconds long), the same sequence with the same arguments in every iteration of a
+// solve. It is recorded once per solve into a graph and replayed. Recording runs on a
+// private stream (the handle's stream may be the legacy default stream, which cannot be
+// captured) with every level's kernels redirected to it; the replay goes to the handle's
+// stream. The executable graph is kept and updated in place by the next solve's recording
+// when the topology is unchanged. Kernels test the device-side `done` flag, so a replay
+// after convergence exits at once, as the direct launches do. MPDG_GRAPHS=0 launches directly.
+// ---------------------------------------------------------------------------
+static bool graphs_enabled()
+{
+  static const int on = [] {
+    const char *e = getenv("MPDG_GRAPHS");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return on != 0;
+}
+
+static void set_level_streams(mpdg_heat *h, cudaStream_t s)
+{
+  h->stream = s;
+  for (MGLevel &lv : h->mg)
+    if (lv.h) lv.h->stream = s;
+}
+
+// record `body` into h->body_exec; false (nothing recorded, nothing launched) on any failure
+template <typename F>
+static bool record_body(mpdg_heat *h, F &&body)
+{
+  if (!h->cap_stream &&
+      cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    h->cap_stream = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  const cudaStream_t orig = h->stream;
+  // counters of every level before recording (the coarse levels count their own launches)
+  std::vector<std::array<int64_t, 3>> before;
+  for (MGLevel &lv : h->mg)
+    if (lv.h && lv.h != h) before.push_back({lv.h->launches, lv.h->vm64, lv.h->vm32});
+  const int64_t l0 = h->launches, a0 = h->vm64, b0 = h->vm32;
+  set_level_streams(h, h->cap_stream);
+  cudaGraph_t graph = nullptr;
+  bool ok = cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    const int rc = body();
+    ok = cudaStreamEndCapture(h->cap_stream, &graph) == cudaSuccess && rc == MPDG_OK && graph;
+  }
+  set_level_streams(h, orig);
+  // a replay is accounted on this handle: what all levels recorded, which did not run
+  h->body_launches = h->launches - l0;
+  h->body_vm64 = h->vm64 - a0;
+  h->body_vm32 = h->vm32 - b0;
+  h->launches = l0;
+  h->vm64 = a0;
+  h->vm32 = b0;
+  size_t i = 0;
+  for (MGLevel &lv : h->mg)
+    if (lv.h && lv.h != h) {
+      h->body_launches += lv.h->launches - before[i][0];
+      h->body_vm64 += lv.h->vm64 - before[i][1];
+      h->body_vm32 += lv.h->vm32 - before[i][2];
+      lv.h->launches = before[i][0];
+      lv.h->vm64 = before[i][1];
+      lv.h->vm32 = before[i][2];
+      ++i;
+    }
+  if (ok && h->body_exec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(h->body_exec, graph, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(h->body_exec);
+      h->body_exec = nullptr;
+    }
+  }
+  if (ok && !h->body_exec &&
+      cudaGraphInstantiate(&h->body_exec, graph, 0) != cudaSuccess) {
+    h->body_exec = nullptr;
+    ok = false;
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();  // a failed recording leaves a non-sticky error behind
+  return ok;
+}
+
+// ---------------------------------------------------------------------------
 // FP64 flexible CG with the FP32 Chebyshev-Jacobi or p-multigrid preconditioner
 // ---------------------------------------------------------------------------
 static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
@@ -1964,6 +2059,9 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   const int g = vgrid(h, N);
   int total_it = 0, restarts = 0;
   double res0 = -1.0, true_res = 0.0;
+  int graph_state = 0;  // 0 not recorded yet, 1 replaying, -1 direct launches
+  set_level_streams(h, h->stream);
+  if (any_faces(h)) TRY(dvec(h, &h->face_dot, 1));
   for (;;) {
     CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
     if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
@@ -2002,14 +2100,28 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
       return MPDG_OK;
     };
     if (!h->st_host->done) TRY(precondition());
+    auto iteration = [&]() -> int {
+      TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
+      k_cgm_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, h->r32, h->x32, h->d32,
+                                               h->inv_diag_f, inv_theta, h->st, h->partials,
+                                               h->counter); ++h->launches;
+      TRY(precondition());
+      return MPDG_OK;
+    };
+    // the first preconditioner call above has made every allocation an iteration needs
+    if (graph_state == 0 && !h->st_host->done)
+      graph_state = (graphs_enabled() && !h->timing && record_body(h, iteration)) ? 1 : -1;
     int chunk = 2;
     while (!h->st_host->done) {
       for (int c = 0; c < chunk; ++c) {
-        TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
-        k_cgm_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, h->r32, h->x32, h->d32,
-                                                 h->inv_diag_f, inv_theta, h->st, h->partials,
-                                                 h->counter); ++h->launches;
-        TRY(precondition());
+        if (graph_state == 1) {
+          CU(cudaGraphLaunch(h->body_exec, h->stream));
+          h->launches += h->body_launches;
+          h->vm64 += h->body_vm64;
+          h->vm32 += h->body_vm32;
+        } else {
+          TRY(iteration());
+        }
       }
       TRY(poll(h));
       chunk = std::min(chunk * 2, 16);
@@ -2232,6 +2344,10 @@ static void release(mpdg_heat *h)
       delete lv.h;
     }
   h->mg.clear();
+  if (h->body_exec) cudaGraphExecDestroy(h->body_exec);
+  h->body_exec = nullptr;
+  if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+  h->cap_stream = nullptr;
   drain_events(h);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   h->ev_pool.clear();
@@ -3099,14 +3215,23 @@ extern "C" int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset)
   CU(cudaSetDevice(h->device));
   CU(cudaStreamSynchronize(h->stream));
   drain_events(h);
+  // this handle's launches and those of its multigrid levels
   c->launches = h->launches;
   c->vmult64_calls = h->vm64;
   c->vmult32_calls = h->vm32;
+  for (MGLevel &lv : h->mg)
+    if (lv.h && lv.h != h) {
+      c->launches += lv.h->launches;
+      c->vmult64_calls += lv.h->vm64;
+      c->vmult32_calls += lv.h->vm32;
+    }
   c->vmult64_ms = h->ms64;
   c->vmult32_ms = h->ms32;
   if (reset) {
     h->launches = h->vm64 = h->vm32 = 0;
     h->ms64 = h->ms32 = 0.0;
+    for (MGLevel &lv : h->mg)
+      if (lv.h && lv.h != h) lv.h->launches = lv.h->vm64 = lv.h->vm32 = 0;
   }
   return MPDG_OK;
 }

@@ -322,3 +322,51 @@ def test_unidirectional_solidification_with_transport_on_gpu(case):
         st = opn.solve(dt)
         assert st.converged == 1
         assert float(f"{op.l2_norm(opn.T):.5e}") == ref
+
+
+_GRAPH_CASE = r"""
+import json, sys, torch
+from meltpooldg_b200 import _lib as L
+from meltpooldg_b200 import heat as H
+op = H.HeatDiffuseOperator(H.box_mesh(3, (16, 16, 16)))
+op.set_material(H.material(law=L.LAW_LINEAR_K, k=1.0, k1=0.5))
+out = {}
+for name, pre in [("mg", L.PRECOND_MG_F32), ("cheb", L.PRECOND_CHEBYSHEV_JACOBI_F32)]:
+    lin = H.LinearSolverData(preconditioner_type=pre, rel_tolerance=1e-10, abs_tolerance=0.0,
+                             cheb_picard=True)
+    opn = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    q = op.new_vector()
+    opn.heat_source = q
+    its = []
+    for s in range(3):
+        op.gaussian_source(q, 300.0, (0.3 + 0.1 * s, 0.5, 0.9), 0.1)
+        its.append(opn.solve(5e-4).linear_iterations)
+    out[name] = {"its": its, "T": opn.T.cpu().tolist()}
+out["launches"] = op.counters()["launches"]
+json.dump(out, open(sys.argv[1], "w"))
+"""
+
+
+def test_graph_replay_matches_direct_launches(tmp_path):
+    """The mixed-precision solvers replay one recorded iteration as a CUDA graph; with
+    MPDG_GRAPHS=0 they launch directly. Both give the same iterations, fields (to the
+    solver tolerance: the atomic scatter's summation order varies) and launch counts.
+    Child processes, because the mode is read once per process."""
+    import json
+    import os
+    import subprocess
+    import sys
+    res = {}
+    for mode in ("1", "0"):
+        path = tmp_path / f"graphs_{mode}.json"
+        r = subprocess.run([sys.executable, "-c", _GRAPH_CASE, str(path)],
+                           env=dict(os.environ, MPDG_GRAPHS=mode), capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        res[mode] = json.load(open(path))
+    for name in ("mg", "cheb"):
+        a, b = res["1"][name], res["0"][name]
+        assert a["its"] == b["its"] and min(a["its"]) > 0
+        Ta, Tb = torch.tensor(a["T"]), torch.tensor(b["T"])
+        assert (Ta - Tb).abs().max() <= 1e-8 * Tb.abs().max()
+    assert res["1"]["launches"] == res["0"]["launches"] > 0

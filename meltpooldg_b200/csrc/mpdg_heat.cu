@@ -163,6 +163,9 @@ struct mpdg_heat {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t body_exec = nullptr;
   int64_t body_launches = 0, body_vm64 = 0, body_vm32 = 0;
+  // iterations of the last mixed-precision solve per preconditioner (0 multigrid, 1 Chebyshev):
+  // the next solve issues that many before its first convergence poll
+  int its_hint[2] = {0, 0};
 };
 
 static cudaEvent_t take_event(mpdg_heat *h)
@@ -2111,7 +2114,13 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     // the first preconditioner call above has made every allocation an iteration needs
     if (graph_state == 0 && !h->st_host->done)
       graph_state = (graphs_enabled() && !h->timing && record_body(h, iteration)) ? 1 : -1;
-    int chunk = 2;
+    // iterations are issued in chunks between host polls of the device-side state; the kernels
+    // of an iteration issued after convergence return at once, but each launch still costs a
+    // few microseconds (~0.3 ms for the ~130 launches of a multigrid iteration, more than a
+    // poll), so the first chunk is the previous solve's count (one less with multigrid) and
+    // the next ones single iterations (without a count yet: 2, 4, 8, 16)
+    int &hint = h->its_hint[use_mg ? 0 : 1];
+    int chunk = hint > 0 ? std::max(1, use_mg ? hint - 1 : hint) : 2;
     while (!h->st_host->done) {
       for (int c = 0; c < chunk; ++c) {
         if (graph_state == 1) {
@@ -2124,8 +2133,9 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
         }
       }
       TRY(poll(h));
-      chunk = std::min(chunk * 2, 16);
+      chunk = hint > 0 ? 1 : std::min(chunk * 2, 16);
     }
+    if (h->st_host->done == 1 && restarts == 0) hint = h->st_host->it;
     total_it += h->st_host->it;
     const int done = h->st_host->done, status = h->st_host->status;
     const double tol = h->st_host->tol;

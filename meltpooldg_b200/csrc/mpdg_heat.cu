@@ -163,6 +163,11 @@ struct mpdg_heat {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t body_exec = nullptr;
   int64_t body_launches = 0, body_vm64 = 0, body_vm32 = 0;
+  // flexible GMRES: the FP32 preconditioned directions (m vectors) and a solver state that
+  // stays "running" for the Chebyshev kernels
+  float *gZ = nullptr;
+  int gZ_m = 0;
+  SolverState *st_run = nullptr;
   // iterations of the last mixed-precision solve per preconditioner (0 multigrid, 1 Chebyshev):
   // the next solve issues that many before its first convergence poll
   int its_hint[2] = {0, 0};
@@ -1020,6 +1025,41 @@ __global__ void k_gmres_update(int64_t N, const double *__restrict__ V, int64_t 
   }
 }
 
+// ---- flexible GMRES with the FP32 Chebyshev-Jacobi preconditioner -----------
+// Chebyshev start from the FP64 direction v: r32 = v ; x32 = D32 r32 / theta ; d32 = x32
+__global__ void k_fgm_cheb_start(int64_t N, const double *__restrict__ v, float *r32, float *x32,
+                                 float *d32, float *Ax32, const float *__restrict__ D32,
+                                 float inv_theta)
+{
+  GRID_STRIDE(k, N)
+  {
+    const float rf = (float)v[k];
+    r32[k] = rf;
+    const float xf = D32[k] * rf * inv_theta;
+    x32[k] = xf;
+    d32[k] = xf;
+    Ax32[k] = 0.0f;
+  }
+}
+
+// z = x32 widened to FP64 (exact)
+__global__ void k_widen(int64_t N, const float *__restrict__ x32, double *z)
+{
+  GRID_STRIDE(k, N) z[k] = (double)x32[k];
+}
+
+// x += sum_i y_i Z_i with the FP32-stored preconditioned directions Z_i (widened exactly)
+__global__ void k_fgmres_update(int64_t N, const float *__restrict__ Z, int64_t ld, int nv,
+                                const double *__restrict__ y, double *x)
+{
+  GRID_STRIDE(k, N)
+  {
+    double s = 0.0;
+    for (int i = 0; i < nv; ++i) s += y[i] * (double)Z[(int64_t)i * ld + k];
+    x[k] += s;
+  }
+}
+
 // ---- boundary faces (Robin / Neumann) ----------------------------------------
 // heat_diffuse_operator.cpp:243-269 (tangent loop), :719-781 (rhs loop),
 // :1088-1129 (local face operation). Boundary vertices are never perturbed, so
@@ -1556,7 +1596,12 @@ static int estimate_eigenvalues(mpdg_heat *h, int n_it, double *lmin, double *lm
   prm.max_iterations = n_it;
   prm.rel_tolerance = 0.0;
   prm.abs_tolerance = 0.0;
-  TRY(cg_jacobi(h, &prm, h->z, h->w3, h->inv_diag, 1, nullptr));
+  // the Lanczos CG starts from z = 0; the caller's own zero-start hint is kept for its solve
+  const bool keep_x_zero = h->x_zero;
+  h->x_zero = true;
+  const int rc_cg = cg_jacobi(h, &prm, h->z, h->w3, h->inv_diag, 1, nullptr);
+  h->x_zero = keep_x_zero;
+  TRY(rc_cg);
   const SolverState &s = *h->st_host;
   const int m = std::min(s.it, 64);
   if (m < 1) {
@@ -2174,8 +2219,12 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
 // (one multi-dot and one multi-axpy pass per round); the small Hessenberg
 // problem is solved on the host.
 // ---------------------------------------------------------------------------
+// cheb: flexible GMRES whose preconditioner is the FP32 Chebyshev-Jacobi polynomial of the
+// FP32 operator (D unused); each preconditioned direction z_j is kept in FP32 and the FP64
+// operator is applied to its exact FP64 widening, so x += Z y uses exactly the vectors the
+// Arnoldi process saw
 static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
-                 const double *D, mpdg_solve_stats *stats)
+                 const double *D, mpdg_solve_stats *stats, bool cheb = false)
 {
   const int64_t N = h->n_dofs;
   const int m = std::max(1, std::min(prm->gmres_restart > 0 ? prm->gmres_restart : 28,
@@ -2185,6 +2234,55 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
     TRY(dvec(h, &h->gV, (int64_t)(m + 1) * N));
     h->gV_m = m;
   }
+  std::vector<float> c1, c2;
+  float inv_theta = 1.f;
+  const int kdeg = prm->cheb_degree;
+  if (cheb) {
+    if (kdeg < 1) return fail(MPDG_ERR_INVALID_ARGUMENT, "cheb_degree < 1");
+    if (h->gZ && h->gZ_m < m) return fail(MPDG_ERR_INVALID_ARGUMENT, "GMRES restart grew");
+    if (!h->gZ) {
+      TRY(dvec(h, &h->gZ, (int64_t)m * N));
+      h->gZ_m = m;
+    }
+    if (!h->st_run) {
+      TRY(dvec(h, &h->st_run, 1));
+      CU(cudaMemsetAsync(h->st_run, 0, sizeof(SolverState), h->stream));  // done = 0, forever
+    }
+    TRY(ensure_workspace_f32(h));
+    TRY(refresh_f32(h));
+    if (h->diag_f_dirty) {
+      k_cast_f<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->inv_diag, h->inv_diag_f); ++h->launches;
+      CU(cudaGetLastError());
+      h->diag_f_dirty = false;
+    }
+    if (!h->eig_valid || !prm->cheb_eig_reuse) {
+      TRY(estimate_eigenvalues(h, prm->cheb_eig_iterations, &h->eig_min, &h->eig_max));
+      h->eig_valid = true;
+    }
+    const double bmax = prm->cheb_max_factor * h->eig_max;
+    const double amin = std::max(h->eig_min, prm->cheb_min_fraction * bmax);
+    const double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin);
+    cheb_coefficients(theta, delta, kdeg, c1, c2);
+    inv_theta = (float)(1.0 / theta);
+  }
+  // z = P(v_j): Chebyshev steps of the FP32 operator from v_j, stored in Z_j, widened into z
+  auto precondition = [&](const double *vj, int j) -> int {
+    float *zj = h->gZ + (int64_t)j * N;
+    const int gg32 = vgrid(h, N);
+    k_fgm_cheb_start<<<gg32, VT, 0, h->stream>>>(N, vj, h->r32, zj, h->d32, h->Ax32,
+                                                 h->inv_diag_f, inv_theta);
+    ++h->launches;
+    for (int s = 1; s <= kdeg; ++s) {
+      TRY(op_apply_f(h, h->Ax32, zj, nullptr, false));
+      k_cheb_step<<<gg32, VT, 0, h->stream>>>(N, h->r32, zj, h->d32, h->Ax32, h->inv_diag_f,
+                                              c1[s], c2[s], h->st_run);
+      ++h->launches;
+    }
+    k_widen<<<gg32, VT, 0, h->stream>>>(N, zj, h->z);
+    ++h->launches;
+    CU(cudaGetLastError());
+    return MPDG_OK;
+  };
   TRY(dvec(h, &h->gsmall, 4 * kMaxBasis));
   TRY(ensure_workspace(h));
   TRY(dvec(h, &h->z, N));
@@ -2226,6 +2324,7 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
     if (it >= prm->max_iterations) break;
     k_scale_precond<<<g, VT, 0, h->stream>>>(N, V, 1.0 / beta, D, h->z);
     ++h->launches;
+    if (cheb) TRY(precondition(V, 0));
     std::fill(gg.begin(), gg.end(), 0.0);
     std::fill(H.begin(), H.end(), 0.0);
     gg[0] = beta;
@@ -2270,6 +2369,9 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
       if (res <= tol || it >= prm->max_iterations || hn == 0.0) break;
       k_scale_precond<<<g, VT, 0, h->stream>>>(N, w, 1.0 / hn, D, h->z);
       ++h->launches;
+      // the cycle's last direction is not preconditioned (Z holds m vectors; a restart
+      // begins from the new residual)
+      if (cheb && j + 1 < m) TRY(precondition(w, j + 1));
     }
     if (stop) break;
     // y = R^-1 g, x += M^-1 V y
@@ -2279,7 +2381,10 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
       y[i] = sacc / H[(size_t)i * m + i];
     }
     CU(cudaMemcpyAsync(ydev, y.data(), sizeof(double) * jj, cudaMemcpyHostToDevice, h->stream));
-    k_gmres_update<<<g, VT, 0, h->stream>>>(N, V, N, jj, ydev, D, x);
+    if (cheb)
+      k_fgmres_update<<<g, VT, 0, h->stream>>>(N, h->gZ, N, jj, ydev, x);
+    else
+      k_gmres_update<<<g, VT, 0, h->stream>>>(N, V, N, jj, ydev, D, x);
     ++h->launches;
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(h->stream));  // y lives on the host stack
@@ -2921,15 +3026,16 @@ static int linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   mpdg_solve_stats local;
   memset(&local, 0, sizeof(local));
   if (prm->solver == MPDG_SOLVER_GMRES) {
-    if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 ||
-        prm->preconditioner == MPDG_PRECOND_MG_F32)
-      return fail(MPDG_ERR_NOT_SUPPORTED, "GMRES supports identity or Jacobi preconditioning");
+    if (prm->preconditioner == MPDG_PRECOND_MG_F32)
+      return fail(MPDG_ERR_NOT_SUPPORTED,
+                  "GMRES supports identity, Jacobi or FP32 Chebyshev-Jacobi preconditioning");
+    const bool cheb = prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32;
     const double *D = nullptr;
-    if (prm->preconditioner == MPDG_PRECOND_JACOBI) {
+    if (prm->preconditioner == MPDG_PRECOND_JACOBI || cheb) {
       if (!h->diag_valid) return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
-      D = h->inv_diag;
+      if (!cheb) D = h->inv_diag;
     }
-    TRY(gmres(h, prm, x, b, D, &local));
+    TRY(gmres(h, prm, x, b, D, &local, cheb));
   } else if (prm->solver != MPDG_SOLVER_CG) {
     return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown solver type");
   } else if (prm->preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 ||

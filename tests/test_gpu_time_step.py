@@ -293,8 +293,10 @@ SOLIDIFICATION_TRANSPORT = {
 }
 
 
+@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_CHEBYSHEV_JACOBI_F32])
 @pytest.mark.parametrize("case", list(SOLIDIFICATION_TRANSPORT))
-def test_unidirectional_solidification_with_transport_on_gpu(case):
+def test_unidirectional_solidification_with_transport_on_gpu(case, precond):
+    """Also through GMRES with the FP32 Chebyshev-Jacobi preconditioner (flexible GMRES)."""
     dt, vel, two_phase, refs = SOLIDIFICATION_TRANSPORT[case]
     op = H.HeatDiffuseOperator(H.box_mesh(1, (32, 32, 1), (0, 0, 0), (0.1, 0.1, 1.0),
                                           dirichlet=()))
@@ -309,6 +311,7 @@ def test_unidirectional_solidification_with_transport_on_gpu(case):
     v = torch.zeros((3, op.n_dofs), dtype=torch.float64, device="cuda")
     v[0] = -vel
     opn = H.HeatDiffuseOperation(op, H.LinearSolverData(solver_type=L.SOLVER_GMRES,
+                                                        preconditioner_type=precond,
                                                         rel_tolerance=1e-12),
                                  H.NonlinearSolverData(residual_tolerance=1e-7))
     opn.set_initial_condition((1960.0 + 20.0 * x[:, 0] / 0.1).contiguous())

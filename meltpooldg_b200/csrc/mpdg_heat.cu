@@ -962,23 +962,58 @@ __global__ void k_cheb_init(int64_t N, const float *__restrict__ b, float *x, fl
 constexpr int kMaxBasis = 32;
 
 // out[i] = V_i . w for i < nv (V_i = V + i * ld)
-__global__ void k_multidot(int64_t N, const double *__restrict__ V, int64_t ld, int nv,
-                           const double *__restrict__ w, double *partials, unsigned *counter,
-                           double *out)
+// A CTA stages a chunk of w (kDotChunk values) in shared memory, then streams each V_i over
+// the chunk (coalesced), each warp accumulating into its own shared slot per vector (fixed
+// summation order: deterministic); the last CTA sums the nv per-CTA totals. Every vector and
+// w are read once from memory, and the work per element is one load and one FMA whatever nv
+// is (launch with VT = 256 threads).
+constexpr int kDotChunk = 2048;
+__global__ void __launch_bounds__(256) k_multidot(int64_t N, const double *__restrict__ V,
+                                                  int64_t ld, int nv,
+                                                  const double *__restrict__ w,
+                                                  double *partials, unsigned *counter,
+                                                  double *out)
 {
-  double v[kMaxBasis];
+  __shared__ double ws[kDotChunk];
+  __shared__ double acc[kMaxBasis][8];  // [vector][warp]
+  __shared__ int is_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int t = threadIdx.x; t < kMaxBasis * 8; t += blockDim.x) acc[t / 8][t % 8] = 0.0;
+  for (int64_t c0 = (int64_t)blockIdx.x * kDotChunk; c0 < N;
+       c0 += (int64_t)gridDim.x * kDotChunk) {
+    const int len = (int)min((int64_t)kDotChunk, N - c0);
+    __syncthreads();  // previous chunk's readers are done with ws
+    for (int t = threadIdx.x; t < len; t += blockDim.x) ws[t] = w[c0 + t];
+    __syncthreads();
+    for (int i = 0; i < nv; ++i) {
+      const double *vi = V + (int64_t)i * ld + c0;
+      double s = 0.0;
+      for (int t = threadIdx.x; t < len; t += blockDim.x) s += ws[t] * vi[t];
 #pragma unroll
-  for (int i = 0; i < kMaxBasis; ++i) v[i] = 0.0;
-  GRID_STRIDE(k, N)
-  {
-    const double wk = w[k];
-#pragma unroll
-    for (int i = 0; i < kMaxBasis; ++i)
-      if (i < nv) v[i] += wk * V[(int64_t)i * ld + k];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) acc[i][warp] += s;
+    }
   }
-  double tot[kMaxBasis];
-  if (grid_sum<kMaxBasis>(v, partials, counter, tot))
-    for (int i = 0; i < nv; ++i) out[i] = tot[i];
+  __syncthreads();
+  if (threadIdx.x < nv) {
+    double s = 0.0;
+    for (int q = 0; q < nwarp; ++q) s += acc[threadIdx.x][q];
+    partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  for (int i = warp; i < nv; i += nwarp) {
+    double s = 0.0;
+    for (unsigned b = lane; b < gridDim.x; b += 32) s += __ldcg(partials + (size_t)i * gridDim.x + b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[i] = s;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
 }
 
 // w -= sum_i c_i V_i (i < nv)

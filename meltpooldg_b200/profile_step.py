@@ -47,6 +47,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--transport", action="store_true")
+    ap.add_argument("--cheb-degree", type=int, default=6,
+                    help="degree of the FP32 Chebyshev preconditioner of the --transport solve")
     a = ap.parse_args()
     op = H.HeatDiffuseOperator(H.box_mesh(a.degree, (a.cells,) * 3, perturb=a.perturb, seed=1))
     q = op.new_vector()
@@ -63,7 +65,7 @@ def main():
         op.set_fields(hs, vel)
         solvers = {"mixed": H.LinearSolverData(solver_type=L.SOLVER_GMRES,
                                                preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32,
-                                               cheb_degree=6, rel_tolerance=1e-8,
+                                               cheb_degree=a.cheb_degree, rel_tolerance=1e-8,
                                                abs_tolerance=0.0, cheb_eig_reuse=True)}
         if not a.no_plain:
             solvers["plain"] = H.LinearSolverData(solver_type=L.SOLVER_GMRES, rel_tolerance=1e-8,
@@ -76,7 +78,8 @@ def main():
         if not a.no_plain:
             solvers["plain"] = H.LinearSolverData(rel_tolerance=1e-8, abs_tolerance=0.0)
     out = {"degree": a.degree, "cells": a.cells, "perturb": a.perturb, "n_dofs": op.n_dofs,
-           "steps": a.steps, "warmup": a.warmup, "transport": a.transport}
+           "steps": a.steps, "warmup": a.warmup, "transport": a.transport,
+           "cheb_degree": a.cheb_degree if a.transport else None}
     fields = {}
     for name, data in solvers.items():
         opn = H.HeatDiffuseOperation(op, data, predictor=L.PREDICTOR_LINEAR,

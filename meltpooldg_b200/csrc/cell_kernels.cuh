@@ -281,6 +281,41 @@ __device__ __forceinline__ void apply_G(const T G[6], T a, T b, T c, T &x, T &y,
   }
 }
 
+// L2 prefetch of the next batch of a line-per-thread kernel: this thread's x-line of each
+// given vector and, cooperatively over the block, the batch's contiguous per-cell blocks of
+// per-q data (nper values per q-point), so the next batch's gathers and q-point loads hit L2
+// instead of stalling on DRAM (the long-scoreboard stall of the q-point loop).
+template <int n, typename T>
+__device__ __forceinline__ void prefetch_next_batch(const MeshDims &d, int64_t n_cells,
+                                                    int64_t next_batch, int cl, int j, int k,
+                                                    const T *v0, const T *v1, const T *perq,
+                                                    int nper)
+{
+  constexpr int n3 = n * n * n, CPB = cells_per_block(n);
+  const int64_t first = next_batch * CPB;
+  if (first >= n_cells) return;
+  const int64_t ncell = first + cl;
+  if (ncell < n_cells) {
+    const int ncx = (int)(ncell % d.m[0]);
+    const int ncy = (int)((ncell / d.m[0]) % d.m[1]);
+    const int ncz = (int)(ncell / ((int64_t)d.m[0] * d.m[1]));
+    const int64_t nrow =
+      (int64_t)d.nd[0] * ((d.p * ncy + j) + (int64_t)d.nd[1] * (d.p * ncz + k)) + d.p * ncx;
+    for (const T *v : {v0, v1}) {
+      if (!v) continue;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(v + nrow));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(v + nrow + n - 1));
+    }
+  }
+  if (perq) {
+    const int64_t last = first + CPB < n_cells ? first + CPB : n_cells;
+    const char *g0 = reinterpret_cast<const char *>(perq + first * nper * n3);
+    const int64_t bytes = (last - first) * nper * n3 * (int64_t)sizeof(T);
+    for (int64_t off = (int64_t)threadIdx.x * 128; off < bytes; off += (int64_t)blockDim.x * 128)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(g0 + off));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // vmult: dst += J src (dst zeroed by the caller); optional src.dst dot
 // ---------------------------------------------------------------------------
@@ -310,6 +345,13 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
     const int j = line % n, k = line / n;
     const int I0 = d.p * cx, J = d.p * cy + j, K = d.p * cz + k;
     const int64_t row = (int64_t)d.nd[0] * (J + (int64_t)d.nd[1] * K) + I0;
+    // the geometry, or the coefficient fields of LAW 4/5, dominate a batch's q-point loads
+    if (GEO == 1)
+      prefetch_next_batch<n>(d, a.n_cells, batch + gridDim.x, cl, j, k, a.src,
+                             TDEP ? a.Tl : nullptr, a.g.q, 7);
+    else
+      prefetch_next_batch<n>(d, a.n_cells, batch + gridDim.x, cl, j, k, a.src,
+                             TDEP ? a.Tl : nullptr, (LAW == 4 || LAW == 5) ? a.cf : nullptr, 5);
     T xs[n];
     gather_xline<n>(d, row, I0, J, K, true, a.src, xs, active);
 #pragma unroll

@@ -767,6 +767,56 @@ __global__ void __launch_bounds__(block_threads(n)) k_coef_tangent(CellArgs<doub
 }
 
 // ---------------------------------------------------------------------------
+// Tangent fields of the linear-k law at the linearisation point, built once per
+// linearisation for the register-resident kernel's LAW 7: out[cell][4][n^3] =
+// {k_l + k1 T_lin, k1 grad_ref T_lin} (the 7 T_lin sweeps of every LAW 1 application).
+// ---------------------------------------------------------------------------
+template <int n, int GEO>
+__global__ void __launch_bounds__(block_threads(n)) k_coef_lineark(CellArgs<double> a, double *out)
+{
+  using T = double;
+  constexpr int n2 = n * n, n3 = n2 * n, CPB = cells_per_block(n);
+  constexpr int NF = 7;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  const int cl = threadIdx.x / n2, line = threadIdx.x % n2;
+  T *x = sm + cl * NF * n3, *t1 = x + n3, *t2 = x + 2 * n3, *Tq = x + 3 * n3, *Tx = x + 4 * n3,
+    *Ty = x + 5 * n3, *Tz = x + 6 * n3;
+  const MeshDims &d = a.d;
+  const int64_t n_batches = (a.n_cells + CPB - 1) / CPB;
+  for (int64_t batch = blockIdx.x; batch < n_batches; batch += gridDim.x) {
+    const int64_t cell = batch * CPB + cl;
+    const bool active = cell < a.n_cells;
+    const int64_t cc = active ? cell : 0;
+    const int cx = (int)(cc % d.m[0]);
+    const int cy = (int)((cc / d.m[0]) % d.m[1]);
+    const int cz = (int)(cc / ((int64_t)d.m[0] * d.m[1]));
+    const int j = line % n, k = line / n;
+    const int I0 = d.p * cx, J = d.p * cy + j, K = d.p * cz + k;
+    const int64_t row = (int64_t)d.nd[0] * (J + (int64_t)d.nd[1] * K) + I0;
+    T xv[n];
+    gather_xline<n>(d, row, I0, J, K, false, a.Tl, xv, active);
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i + n * line] = xv[i];
+    __syncthreads();
+    eval_values<n>(x, t1, t2, Tq, line);
+    eval_gradients<n>(Tq, Tx, Ty, Tz, line);
+    if (active) {
+#pragma unroll
+      for (int r = 0; r < n; ++r) {
+        const int q = line + n2 * r;
+        T *o = out + cc * 4 * n3 + q;
+        o[0] = a.m.k_l + a.m.k1 * Tq[q];
+        o[n3] = a.m.k1 * Tx[q];
+        o[2 * n3] = a.m.k1 * Ty[q];
+        o[3 * n3] = a.m.k1 * Tz[q];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Values of the heaviside field H and the velocity field v (component-major, 3 x N) at the
 // quadrature points, sum-factorised: cf[cell][0][q] = H (1 without a field),
 // cf[cell][2 + e][q] = v_e (0 without a field); the per-point coefficient set-up then reads
@@ -874,5 +924,6 @@ template <int n> constexpr size_t smem_rhs() { return sizeof(double) * cells_per
 template <int n> constexpr size_t smem_diag() { return sizeof(double) * cells_per_block(n) * 16 * n * n * n; }
 template <int n> constexpr size_t smem_norm() { return sizeof(double) * cells_per_block(n) * 4 * n * n * n; }
 template <int n> constexpr size_t smem_coef_tangent() { return sizeof(double) * cells_per_block(n) * 8 * n * n * n; }
+template <int n> constexpr size_t smem_coef_lineark() { return sizeof(double) * cells_per_block(n) * 7 * n * n * n; }
 
 }  // namespace mpdg

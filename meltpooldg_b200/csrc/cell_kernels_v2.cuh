@@ -294,8 +294,8 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           for (int off = t * 128; off < n * n * n * 4; off += n * 128)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(kq + off));
         }
-        if (LAW == 4 || LAW == 6) {
-          constexpr int nf = LAW == 4 ? 5 : 8;
+        if (LAW == 4 || LAW == 6 || LAW == 7) {
+          constexpr int nf = LAW == 4 ? 5 : (LAW == 6 ? 8 : 4);
           constexpr int bytes = nf * n * n * n * (int)sizeof(T);
           const char *cf = reinterpret_cast<const char *>(a.cf + ncell * nf * (n * n * n));
           for (int off = t * 128; off < bytes; off += n * 128)
@@ -389,6 +389,15 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
           f1 = kk * Uy[k][j];
           f2 = kk * Uz[k][j];
           cval = T(0);
+        } else if (LAW == 7) {
+          // linear-k tangent from its fields: flux k(T_lin) grad(u) + k1 grad(T_lin) u
+          constexpr int npt = n * n * n;
+          const T *cf = a.cf + cc * 4 * npt + t + n * (j + n * k);
+          kk = __ldg(cf);
+          f0 = kk * Ux[k][j] + __ldg(cf + npt) * uu;
+          f1 = kk * Uy[k][j] + __ldg(cf + 2 * npt) * uu;
+          f2 = kk * Uz[k][j] + __ldg(cf + 3 * npt) * uu;
+          cval = a.m.idt * (a.m.rho_l * a.m.cp_l);
         } else if (LAW == 6) {
           // c u + rho_cp b.grad(u), flux k grad(u) + dk grad(T_lin) u
           constexpr int npt = n * n * n;

@@ -117,8 +117,9 @@ struct DegreeOps {
     }
     if (law == 4) return geo == 0 ? vmult_t<T, 0, 4>(a, s, sm) : vmult_t<T, 1, 4>(a, s, sm);
     if (law == 5) return geo == 0 ? vmult_t<T, 0, 5>(a, s, sm) : vmult_t<T, 1, 5>(a, s, sm);
-    if (law == 6) {
+    if (law == 6 || law == 7) {
       if constexpr (use_v2<T>()) {
+        if (law == 7) return geo == 0 ? vmult_t<T, 0, 7>(a, s, sm) : vmult_t<T, 1, 7>(a, s, sm);
         return geo == 0 ? vmult_t<T, 0, 6>(a, s, sm) : vmult_t<T, 1, 6>(a, s, sm);
       } else {
         return cudaErrorNotSupported;
@@ -257,6 +258,21 @@ struct DegreeOps {
   {
     return geo == 0 ? coef_tangent_t<0>(a, out, s, sm) : coef_tangent_t<1>(a, out, s, sm);
   }
+  template <int GEO>
+  static cudaError_t coef_lineark_t(const CellArgs<double> &a, double *out, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_coef_lineark<n, GEO>;
+    const size_t smem = smem_coef_lineark<n>();
+    const int g = persistent_grid(k, THREADS, smem, (a.n_cells + CPB - 1) / CPB, sm, &cache);
+    k<<<g, THREADS, smem, s>>>(a, out);
+    return cudaGetLastError();
+  }
+  static cudaError_t coef_lineark(const CellArgs<double> &a, double *out, int geo, cudaStream_t s,
+                                  int sm)
+  {
+    return geo == 0 ? coef_lineark_t<0>(a, out, s, sm) : coef_lineark_t<1>(a, out, s, sm);
+  }
   static cudaError_t field_values(const CellArgs<double> &a, const double *H, const double *vel,
                                   int64_t n_dofs, double *cf, cudaStream_t s, int sm)
   {
@@ -286,6 +302,7 @@ struct DegreeOps {
     t.diag = &diag;
     t.norm = &norm;
     t.coef_tangent = &coef_tangent;
+    t.coef_lineark = &coef_lineark;
     t.field_values = &field_values;
     t.v2_d = use_v2<double>();
     t.v2_f = use_v2<float>();

@@ -25,6 +25,9 @@ struct DegreeTable {
   // slots 0 and 2..4 ([cell][5][npt])
   cudaError_t (*field_values)(const CellArgs<double> &, const double *H, const double *vel,
                               int64_t n_dofs, double *cf, cudaStream_t, int sm) = nullptr;
+  // linear-k tangent fields at a.Tl (4 per point, FP64)
+  cudaError_t (*coef_lineark)(const CellArgs<double> &, double *out, int geo, cudaStream_t,
+                              int sm) = nullptr;
   // the register-resident operator kernel exists for this degree (FP64 / FP32)
   bool v2_d = false, v2_f = false;
   // a.dst += diagonal of the FP32 Picard operator (conductivity field a.kq); same degrees

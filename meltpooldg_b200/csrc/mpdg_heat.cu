@@ -117,6 +117,9 @@ struct mpdg_heat {
   double *tf = nullptr;
   float *tf_f = nullptr;
   bool tf_dirty = true, tf_f_dirty = true;
+  // tangent fields of the linear-k law at the linearisation point (4 per point, LAW 7)
+  double *tk = nullptr;
+  bool tk_dirty = true;
   // GMRES basis (m + 1 vectors) and small device buffers
   double *gV = nullptr;
   int gV_m = 0;
@@ -1300,6 +1303,30 @@ static int ensure_fields(mpdg_heat *h)
   return MPDG_OK;
 }
 
+// The linear-k tangent from fields built once per linearisation (LAW 7) instead of
+// re-evaluating T_lin in every application; MPDG_TANGENT_FIELDS=0 keeps the evaluation.
+static bool tangent_fields_enabled()
+{
+  static const int on = [] {
+    const char *e = getenv("MPDG_TANGENT_FIELDS");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return on != 0;
+}
+
+static int ensure_lineark(mpdg_heat *h)
+{
+  if (!h->tk_dirty) return MPDG_OK;
+  TRY(dvec(h, &h->tk, h->n_cells * 4 * h->npt));
+  CellArgs<double> a = cell_args<double>(h);
+  a.g.q = h->geoq;
+  a.Tl = h->T_lin;
+  CU(h->tab.coef_lineark(a, h->tk, h->geo, h->stream, h->sm_count));
+  ++h->launches;
+  h->tk_dirty = false;
+  return MPDG_OK;
+}
+
 // (re)build the LAW 5 tangent coefficient fields at the current linearisation point
 static int ensure_tangent(mpdg_heat *h)
 {
@@ -1401,6 +1428,11 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
     TRY(ensure_tangent(h));
     a.cf = h->tf;
     law = 6;
+  } else if (law == MPDG_LAW_LINEAR_K && h->tab.v2_d && h->tab.coef_lineark &&
+             tangent_fields_enabled()) {
+    TRY(ensure_lineark(h));
+    a.cf = h->tk;
+    law = 7;
   }
   a.src = src;
   a.dst = dst;
@@ -1845,6 +1877,7 @@ static int mg_setup(mpdg_heat *h, const mpdg_solver_params *prm, bool picard)
       c->T_old = fTo ? v.To : nullptr;
       c->lin_f_dirty = true;
       c->tf_dirty = true;
+      c->tk_dirty = true;
       TRY(refresh_f32(c));
       if (picard) {
         TRY(dvec(c, &c->kq, c->n_cells * c->npt));
@@ -2733,6 +2766,7 @@ extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
   h->eig_valid = false;
   h->cf_dirty = true;
   h->tf_dirty = true;
+  h->tk_dirty = true;
   return MPDG_OK;
 }
 
@@ -2745,6 +2779,7 @@ extern "C" int mpdg_heat_set_fields(mpdg_heat *h, const double *heaviside, const
   h->vel = velocity;
   h->cf_dirty = true;
   h->tf_dirty = true;
+  h->tk_dirty = true;
   h->diag_valid = false;
   h->eig_valid = false;
   return MPDG_OK;
@@ -2771,6 +2806,7 @@ extern "C" int mpdg_heat_set_boundary(mpdg_heat *h, int face, int type, double h
   h->bqn[face] = q_n;
   h->lin_f_dirty = true;
   h->tf_dirty = true;
+  h->tk_dirty = true;
   h->diag_valid = false;
   h->eig_valid = false;
   return MPDG_OK;
@@ -2792,6 +2828,7 @@ extern "C" int mpdg_heat_set_linearization(mpdg_heat *h, const double *T, const 
   h->T_old = T_old;
   h->lin_f_dirty = true;
   h->tf_dirty = true;
+  h->tk_dirty = true;
   return MPDG_OK;
 }
 
@@ -3154,6 +3191,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     h->T_old = T_old;
     h->lin_f_dirty = true;
     h->tf_dirty = true;
+    h->tk_dirty = true;
     // JacobiPreconditioner::update; the multigrid preconditioner on the Picard operator
     // needs the FP64 diagonal only for a new Lanczos estimate
     const bool mg_picard = prm->linear.preconditioner == MPDG_PRECOND_MG_F32 &&
@@ -3219,6 +3257,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
         if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
         h->lin_f_dirty = true;
         h->tf_dirty = true;
+        h->tk_dirty = true;
         s.newton_iterations = i + 1;
       }
       if (rc == MPDG_OK && !s.converged)
@@ -3607,6 +3646,7 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
     h->T_old = T;
     h->lin_f_dirty = true;
     h->tf_dirty = true;
+    h->tk_dirty = true;
     CU(cudaMemsetAsync(h->w2, 0, sizeof(double) * N, h->stream));
     int rr = create_rhs(h, h->w2, T, heat_source);               // r = -R(LE)
     if (rr == MPDG_OK) {
@@ -3617,6 +3657,7 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
     h->T_old = keepTo;
     h->lin_f_dirty = true;
     h->tf_dirty = true;
+    h->tk_dirty = true;
     TRY(rr);
     double jj = 0.0, rj_plus = 0.0;
     TRY(norms(h, h->w3, nullptr, &jj, nullptr));

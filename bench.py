@@ -468,6 +468,11 @@ def run_mine(args):
                          "post steps over [upper/8, upper]; 8 steps on the coarsest level); "
                          "Picard operators (k(T_lin) at the q-points) on every level; Lanczos "
                          "intervals reused across steps", "predictor": "linear extrapolation",
+                         "outer_operator": "FP64 k(T) tangent from k(T_lin), k1 grad(T_lin) "
+                                           "fields built once per linearisation (their build "
+                                           "is inside the timed step)",
+                         "launches": "one CG iteration recorded per solve as a CUDA graph and "
+                                     "replayed",
                          "cheb": f"FP32 Chebyshev-Jacobi degree {CHEB_DEGREE}, Picard operator"},
         "mixed_vs_plain_error": err,
         "vmult_fp64_gdofs": N / (vm_ms / 1e3) / 1e9, "vmult_fp64_ms": vm_ms,

@@ -165,6 +165,48 @@ def max_over_ranks(value, device, world):
     return float(t.item())
 
 
+def gpu_local_cpus(dev_index):
+    """CPUs of the GPU's own NUMA node (NVML's CPU affinity of the device), or None when it
+    cannot be read. Pinned host buffers allocated while the process runs there are placed in
+    that node's memory, next to the GPU's PCIe root, so host<->device copies do not cross the
+    inter-socket link."""
+    try:
+        import pynvml
+        from cuda.bindings import runtime as cudart
+        err, bus = cudart.cudaDeviceGetPCIBusId(64, dev_index)
+        if int(err) != 0:
+            return None
+        bus = bus.split(b"\0", 1)[0].decode()
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            words = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
+        finally:
+            pynvml.nvmlShutdown()
+        cpus = {64 * w + b for w, m in enumerate(words) for b in range(64) if (m >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+    except Exception:
+        return None
+
+
+def pinned_near_gpu(dev_index, n, count):
+    """`count` pinned float64 host buffers of n values on the GPU's NUMA node (the process's
+    CPU affinity is restored afterwards); plain pinned buffers when the node is unknown."""
+    import torch
+    local = gpu_local_cpus(dev_index)
+    before = os.sched_getaffinity(0)
+    try:
+        if local:
+            os.sched_setaffinity(0, local)
+        bufs = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(count)]
+        for b in bufs:
+            b.zero_()  # first touch on this node
+    finally:
+        os.sched_setaffinity(0, before)
+    return bufs, sorted(local) if local else None
+
+
 def replica_throughput(world, n_dofs, steps, ms):
     """Whole-job DoFs advanced per second: every replica advances n_dofs per step."""
     return world * n_dofs * steps / (ms / 1e3)
@@ -320,9 +362,7 @@ def run_mine(args):
     e2e = None
     if not args.no_e2e:
         import ctypes as C
-        hT = torch.empty(N, dtype=torch.float64, pin_memory=True)
-        hTo = torch.empty(N, dtype=torch.float64, pin_memory=True)
-        hq = torch.empty(N, dtype=torch.float64, pin_memory=True)
+        (hT, hTo, hq), numa_cpus = pinned_near_gpu(dev.index if dev.index is not None else 0, N, 3)
         hT.copy_(T_W)  # the headline's steps W .. W+K-1 again, from the same state
         hTo.copy_(T_old_W)
         prm = mixed.params
@@ -368,6 +408,9 @@ def run_mine(args):
                "ms_per_step": ms_res / K,
                "api": "mpdg_heat_time_step_resident (history resident on the device, loaded "
                       "once; per step: host source in, new T out, pinned buffers)",
+               "host_buffers": ("pinned, allocated on the GPU's NUMA node (CPUs "
+                                f"{numa_cpus[0]}-{numa_cpus[-1]})" if numa_cpus else
+                                "pinned (GPU's NUMA node unknown)"),
                "stateless": {"value": replica_throughput(world, N, K, ms_e2e), "unit": "DoF/s",
                              "h2d_bytes_per_step": 3 * N * 8, "d2h_bytes_per_step": 2 * N * 8,
                              "ms_per_step": ms_e2e / K,

@@ -346,17 +346,12 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
     const int I0 = d.p * cx, J = d.p * cy + j, K = d.p * cz + k;
     const int64_t row = (int64_t)d.nd[0] * (J + (int64_t)d.nd[1] * K) + I0;
     // the geometry, or the coefficient fields of LAW 4/5, dominate a batch's q-point loads
-    constexpr int NCF = LAW == 7 ? 4 : 5;  // coefficient fields per point of LAW 4/5/7
-    const T *cfq = (LAW == 4 || LAW == 5 || LAW == 7) ? a.cf : nullptr;
-    if (GEO == 1) {
+    if (GEO == 1)
       prefetch_next_batch<n>(d, a.n_cells, batch + gridDim.x, cl, j, k, a.src,
                              TDEP ? a.Tl : nullptr, a.g.q, 7);
-      if (cfq) prefetch_next_batch<n>(d, a.n_cells, batch + gridDim.x, cl, j, k,
-                                      (const T *)nullptr, (const T *)nullptr, cfq, NCF);
-    } else {
+    else
       prefetch_next_batch<n>(d, a.n_cells, batch + gridDim.x, cl, j, k, a.src,
-                             TDEP ? a.Tl : nullptr, cfq, NCF);
-    }
+                             TDEP ? a.Tl : nullptr, (LAW == 4 || LAW == 5) ? a.cf : nullptr, 5);
     T xs[n];
     gather_xline<n>(d, row, I0, J, K, true, a.src, xs, active);
 #pragma unroll
@@ -393,21 +388,12 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
       T rhocp, kk, drhocp, dk;
       const T uu = u[q];
       T val, b0 = T(0), b1 = T(0), b2 = T(0);
-      T k7x = T(0), k7y = T(0), k7z = T(0);  // LAW 7: k1 grad_ref T_lin from the fields
       if (LAW == 5) {
         const T *cf = a.cf + cc * 5 * n3 + q;
         mat_eval_w(a.m, Tq[q], __ldg(cf), rhocp, kk, drhocp, dk);
         b0 = __ldg(cf + 2 * n3);
         b1 = __ldg(cf + 3 * n3);
         b2 = __ldg(cf + 4 * n3);
-      } else if (LAW == 7) {
-        const T *cf = a.cf + cc * 4 * n3 + q;
-        kk = __ldg(cf);
-        k7x = __ldg(cf + n3);
-        k7y = __ldg(cf + 2 * n3);
-        k7z = __ldg(cf + 3 * n3);
-        rhocp = a.m.rho_l * a.m.cp_l;
-        drhocp = dk = T(0);
       } else if (LAW == 4) {
         const T *cf = a.cf + cc * 5 * n3 + q;
         kk = __ldg(cf + n3);
@@ -424,11 +410,6 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
         f0 += dk * Tx[q] * uu;
         f1 += dk * Ty[q] * uu;
         f2 += dk * Tz[q] * uu;
-      }
-      if (LAW == 7) {
-        f0 += k7x * uu;
-        f1 += k7y * uu;
-        f2 += k7z * uu;
       }
       if (LAW == 5)  // rho_cp b.grad(u) + d(rho_cp)/dT (b.grad T) u, b = JxW J^-1 v
         val = cval * uu * jxw + rhocp * (b0 * gx[q] + b1 * gy[q] + b2 * gz[q]) +

@@ -1430,9 +1430,8 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
     law = 6;
   } else if (law == MPDG_LAW_LINEAR_K && h->tab.v2_d && h->tab.coef_lineark &&
              tangent_fields_enabled()) {
-    // register-resident degrees only: on the line-per-thread kernel (p >= 4) the 4 extra
-    // loads per point cost more than the T_lin sweeps and shared memory they save (p = 4
-    // deformed: 6.68 ms with the fields, 5.94 ms without)
+    // register-resident degrees only: on the line-per-thread kernel (p >= 4) 4 extra loads
+    // per point measured slower than the T_lin sweeps they replace
     TRY(ensure_lineark(h));
     a.cf = h->tk;
     law = 7;

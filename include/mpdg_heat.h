@@ -270,9 +270,13 @@ int mpdg_heat_preconditioner_update(mpdg_heat *h);
 /* JacobiPreconditioner::vmult: dst = src .* inv_diag. */
 int mpdg_heat_preconditioner_vmult(mpdg_heat *h, double *dst, const double *src);
 /* LinearSolver::solve(op, x, b, data, precond) (linear_solver.hpp:22-134): solve J x = b
- * from the initial guess in x, ReductionControl(max_it, abs_tol, rel_tol). CG or GMRES,
- * identity / Jacobi / FP32 Chebyshev-Jacobi preconditioning; the preconditioner must
- * have been updated. */
+ * from the initial guess in x, ReductionControl(max_it, abs_tol, rel_tol); the
+ * preconditioner must have been updated.
+ *   CG:    identity, Jacobi (FP64); FP32 Chebyshev-Jacobi or FP32 p-multigrid inside FP64
+ *          flexible CG
+ *   GMRES: identity, Jacobi (FP64, right preconditioning); FP32 Chebyshev-Jacobi as a
+ *          flexible GMRES (the preconditioned directions kept in FP32, the FP64 operator
+ *          applied to their exact widening); not the multigrid preconditioner */
 int mpdg_heat_linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x,
                            const double *b, mpdg_solve_stats *stats);
 

@@ -363,16 +363,20 @@ def run_mine(args):
     if not args.no_e2e:
         import ctypes as C
         (hT, hTo, hq), numa_cpus = pinned_near_gpu(dev.index if dev.index is not None else 0, N, 3)
-        hT.copy_(T_W)  # the headline's steps W .. W+K-1 again, from the same state
-        hTo.copy_(T_old_W)
         prm = mixed.params
         first = W
+
+        def host_source(step, dst):
+            op.gaussian_source(q, AMP, source_center((step + 1) * DT), RADIUS)
+            dst.copy_(q)
+
+        hT.copy_(T_W)  # the headline's steps W .. W+K-1 again, from the same state
+        hTo.copy_(T_old_W)
         H.check(op._L.mpdg_heat_load_history(op.h, C.c_void_p(hT.data_ptr()),
                                              C.c_void_p(hTo.data_ptr())))
         ms_res = 0.0
-        for s in range(first, first + K):
-            op.gaussian_source(q, AMP, source_center((s + 1) * DT), RADIUS)
-            hq.copy_(q)
+        for st in range(first, first + K):
+            host_source(st, hq)
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -388,9 +392,8 @@ def run_mine(args):
         hT.copy_(T_W)
         hTo.copy_(T_old_W)
         ms_e2e = 0.0
-        for s in range(first, first + K):
-            op.gaussian_source(q, AMP, source_center((s + 1) * DT), RADIUS)
-            hq.copy_(q)
+        for st in range(first, first + K):
+            host_source(st, hq)
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -415,6 +418,7 @@ def run_mine(args):
                              "h2d_bytes_per_step": 3 * N * 8, "d2h_bytes_per_step": 2 * N * 8,
                              "ms_per_step": ms_e2e / K,
                              "api": "mpdg_heat_time_step_host (T, T_old, source in; T, T_old out)"}}
+        del hT, hTo, hq
 
     # vmult throughput of the FP64 operator (MF vmult GDoF/s), CUDA events
     x = torch.rand(N, dtype=torch.float64, device=dev)

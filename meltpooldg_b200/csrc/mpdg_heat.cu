@@ -135,6 +135,11 @@ struct mpdg_heat {
   unsigned *counter = nullptr;
   SolverState *st = nullptr, *st_host = nullptr;
   double *scal = nullptr, *scal_host = nullptr;
+  // the page-locked st_host / scal_host / rd_host are mapped: st_map, scal_map and rd_map are
+  // their device addresses, written by k_read_words (small reads then never wait behind a
+  // bulk host copy on a copy engine)
+  SolverState *st_map = nullptr;
+  double *scal_map = nullptr, *rd_host = nullptr, *rd_map = nullptr;
   // Krylov / step workspace
   double *r = nullptr, *pv = nullptr, *Ap = nullptr, *z = nullptr, *w1 = nullptr, *w2 = nullptr,
          *w3 = nullptr;
@@ -161,6 +166,9 @@ struct mpdg_heat {
   bool wait_source = false, record_commit = false;
   double *told_host = nullptr;  // host destination of the committed T_old (copy stream)
   double *res_T = nullptr, *res_To = nullptr;  // device-resident history (time_step_resident)
+  // the resident step swaps the roles of its two history buffers instead of copying T into
+  // T_old (the predictor writes in place over T_{n-1}); rotated reports that the swap happened
+  bool rotate = false, rotated = false;
   // one iteration of the mixed-precision CG as a CUDA graph (recorded on cap_stream, replayed
   // on stream) and the kernel launches / operator applications one replay performs
   cudaStream_t cap_stream = nullptr;
@@ -570,6 +578,11 @@ __global__ void k_predict(int64_t N, const double *__restrict__ T, const double 
                           double *out, double f)
 {
   GRID_STRIDE(i, N) out[i] = (f + 1.0) * T[i] - f * To[i];
+}
+// the same extrapolation written over T_{n-1} (each entry is read before it is written)
+__global__ void k_predict_inplace(int64_t N, const double *__restrict__ T, double *To, double f)
+{
+  GRID_STRIDE(i, N) To[i] = (f + 1.0) * T[i] - f * To[i];
 }
 __global__ void k_axpy(int64_t N, double *y, double a, const double *__restrict__ x)
 {
@@ -1199,6 +1212,34 @@ static int vgrid(const mpdg_heat *h, int64_t N)
   return (int)std::max<int64_t>(g, 1);
 }
 
+__global__ void k_zero16(int64_t n, uint4 *p)
+{
+  GRID_STRIDE(i, n) p[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+__global__ void k_zero4(int64_t n, unsigned *p)
+{
+  GRID_STRIDE(i, n) p[i] = 0u;
+}
+
+// zero fill by a kernel: a cudaMemsetAsync is not a kernel launch and can queue on a copy
+// engine behind a bulk host copy in flight on another stream (the host step's T_old download)
+static cudaError_t zero_async(mpdg_heat *h, void *p, size_t bytes, cudaStream_t s)
+{
+  if (bytes == 0) return cudaSuccess;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p) | (uintptr_t)bytes;
+  if (a % 16 == 0) {
+    const int64_t n = (int64_t)(bytes / 16);
+    k_zero16<<<vgrid(h, n), VT, 0, s>>>(n, static_cast<uint4 *>(p));
+  } else if (a % 4 == 0) {
+    const int64_t n = (int64_t)(bytes / 4);
+    k_zero4<<<vgrid(h, n), VT, 0, s>>>(n, static_cast<unsigned *>(p));
+  } else {
+    return cudaMemsetAsync(p, 0, bytes, s);
+  }
+  ++h->launches;
+  return cudaGetLastError();
+}
+
 template <typename T>
 static CellArgs<T> cell_args(mpdg_heat *h)
 {
@@ -1451,7 +1492,7 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
   }
   if (any_faces(h)) {
     TRY(dvec(h, &h->face_dot, 1));
-    CU(cudaMemsetAsync(h->face_dot, 0, sizeof(double), h->stream));
+    CU(zero_async(h, h->face_dot, sizeof(double), h->stream));
     TRY(launch_faces<double>(h, 0, dst, src, h->T_lin, fin != FIN_NONE ? h->face_dot : nullptr, st));
     if (fin != FIN_NONE) a.extra_dot = h->face_dot;
   }
@@ -1545,20 +1586,33 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
   return MPDG_OK;
 }
 
-static int poll(mpdg_heat *h)
+// copies n 4-byte words into mapped page-locked host memory: the stores travel over the host
+// link from the SMs, so a read of a few words does not queue behind a bulk copy (the host
+// step's T_old download during the solve) on the device-to-host copy engine
+__global__ void k_read_words(const unsigned *__restrict__ src, unsigned *dst, int n)
 {
-  CU(cudaMemcpyAsync(h->st_host, h->st, sizeof(SolverState), cudaMemcpyDeviceToHost, h->stream));
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+static int read_to_host(mpdg_heat *h, void *mapped, const void *dev, size_t bytes)
+{
+  k_read_words<<<1, 256, 0, h->stream>>>((const unsigned *)dev, (unsigned *)mapped,
+                                         (int)(bytes / sizeof(unsigned)));
+  ++h->launches;
+  CU(cudaGetLastError());
   CU(cudaStreamSynchronize(h->stream));
   return MPDG_OK;
 }
+static_assert(sizeof(SolverState) % sizeof(unsigned) == 0, "SolverState is read in words");
+
+static int poll(mpdg_heat *h) { return read_to_host(h, h->st_map, h->st, sizeof(SolverState)); }
 
 static int norms(mpdg_heat *h, const double *a, const double *b, double *aa, double *ab)
 {
   const int64_t N = h->n_dofs;
   k_norms<<<vgrid(h, N), VT, 0, h->stream>>>(N, a, b, h->partials, h->counter, h->scal); ++h->launches;
   CU(cudaGetLastError());
-  CU(cudaMemcpyAsync(h->scal_host, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
+  TRY(read_to_host(h, h->scal_map, h->scal, 2 * sizeof(double)));
   if (aa) *aa = h->scal_host[0];
   if (ab) *ab = h->scal_host[1];
   return MPDG_OK;
@@ -1594,7 +1648,7 @@ static int cg_jacobi(mpdg_heat *h, const mpdg_solver_params *prm, double *x, con
   const int64_t N = h->n_dofs;
   TRY(ensure_workspace(h));
   const int g = vgrid(h, N);
-  CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+  CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
   if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
   h->x_zero = false;
   k_cg_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->pv, h->Ap, D, h->st, h->partials, h->counter,
@@ -1659,7 +1713,7 @@ static int estimate_eigenvalues(mpdg_heat *h, int n_it, double *lmin, double *lm
   TRY(dvec(h, &h->w3, N));
   TRY(dvec(h, &h->z, N));
   k_masked_random<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, h->w3); ++h->launches;
-  CU(cudaMemsetAsync(h->z, 0, sizeof(double) * N, h->stream));
+  CU(zero_async(h, h->z, sizeof(double) * N, h->stream));
   mpdg_solver_params prm;
   mpdg_solver_params_default(&prm);
   prm.max_iterations = n_it;
@@ -1732,7 +1786,7 @@ static int picard_inverse_diagonal(mpdg_heat *h)
   TRY(ensure_dt(h));
   TRY(ensure_workspace_f32(h));
   TRY(refresh_f32(h));
-  CU(cudaMemsetAsync(h->d32, 0, sizeof(float) * N, h->stream));
+  CU(zero_async(h, h->d32, sizeof(float) * N, h->stream));
   CellArgs<float> a = cell_args<float>(h);
   a.kq = h->kq;
   a.g.q = h->geoq_f;
@@ -1795,7 +1849,7 @@ static int mg_build(mpdg_heat *h, const mpdg_solver_params *prm)
     L.x = c->x32;
     L.d = c->d32;
     L.Ax = c->Ax32;
-    CU(cudaMemsetAsync(L.Ax, 0, sizeof(float) * c->n_dofs, h->stream));
+    CU(zero_async(h, L.Ax, sizeof(float) * c->n_dofs, h->stream));
     return MPDG_OK;
   };
   if (h->p > 1) {
@@ -2181,7 +2235,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   set_level_streams(h, h->stream);
   if (any_faces(h)) TRY(dvec(h, &h->face_dot, 1));
   for (;;) {
-    CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+    CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
     if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
     h->x_zero = false;
     k_cgm_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->Ap, h->r32, h->x32, h->d32, h->Ax32,
@@ -2255,7 +2309,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     const int done = h->st_host->done, status = h->st_host->status;
     const double tol = h->st_host->tol;
     // true residual recheck in FP64
-    CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+    CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
     TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
     TRY(dvec(h, &h->w3, N));
     CU(cudaMemcpyAsync(h->w3, b, sizeof(double) * N, cudaMemcpyDeviceToDevice, h->stream));
@@ -2316,7 +2370,7 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
     }
     if (!h->st_run) {
       TRY(dvec(h, &h->st_run, 1));
-      CU(cudaMemsetAsync(h->st_run, 0, sizeof(SolverState), h->stream));  // done = 0, forever
+      CU(zero_async(h, h->st_run, sizeof(SolverState), h->stream));  // done = 0, forever
     }
     TRY(ensure_workspace_f32(h));
     TRY(refresh_f32(h));
@@ -2364,12 +2418,12 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
   int it = 0, status = MPDG_ERR_NOT_CONVERGED;
   double tol = 0.0, res = 0.0, res0 = -1.0;
   auto host_read = [&](const double *dev, double *dst, int cnt) -> int {
-    CU(cudaMemcpyAsync(dst, dev, sizeof(double) * cnt, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
+    TRY(read_to_host(h, h->rd_map, dev, sizeof(double) * cnt));  // cnt <= m <= kMaxBasis
+    memcpy(dst, h->rd_host, sizeof(double) * cnt);
     return MPDG_OK;
   };
   for (;;) {
-    CU(cudaMemsetAsync(h->Ap, 0, sizeof(double) * N, h->stream));
+    CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
     if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
     h->x_zero = false;
     k_residual<<<g, VT, 0, h->stream>>>(N, b, h->Ap, V);
@@ -2402,7 +2456,7 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
     bool stop = false;
     for (int j = 0; j < m; ++j) {
       double *w = V + (int64_t)(j + 1) * N;
-      CU(cudaMemsetAsync(w, 0, sizeof(double) * N, h->stream));
+      CU(zero_async(h, w, sizeof(double) * N, h->stream));
       TRY(op_apply_d(h, w, h->z, FIN_NONE, nullptr, nullptr));
       for (int pass = 0; pass < 2; ++pass) {
         k_multidot<<<g, VT, 0, h->stream>>>(N, V, N, j + 1, w, h->partials, h->counter, hcol);
@@ -2540,8 +2594,10 @@ static void release(mpdg_heat *h)
   h->owned.clear();
   if (h->st_host) cudaFreeHost(h->st_host);
   if (h->scal_host) cudaFreeHost(h->scal_host);
+  if (h->rd_host) cudaFreeHost(h->rd_host);
   h->st_host = nullptr;
   h->scal_host = nullptr;
+  h->rd_host = nullptr;
 }
 
 // vertices of the box mesh: interior vertices perturbed by a counter hash of
@@ -2662,9 +2718,17 @@ static int create_impl(const mpdg_mesh_desc *desc, int device, const std::vector
   if ((rc = dalloc(h, (void **)&h->counter, sizeof(unsigned) * 4)) != MPDG_OK) return cleanup(rc);
   if ((rc = dalloc(h, (void **)&h->st, sizeof(SolverState))) != MPDG_OK) return cleanup(rc);
   if ((rc = dalloc(h, (void **)&h->scal, sizeof(double) * 8)) != MPDG_OK) return cleanup(rc);
-  if (cudaMallocHost((void **)&h->st_host, sizeof(SolverState)) != cudaSuccess ||
-      cudaMallocHost((void **)&h->scal_host, sizeof(double) * 8) != cudaSuccess)
-    return cleanup(fail(MPDG_ERR_OUT_OF_MEMORY, "cudaMallocHost"));
+  if (cudaHostAlloc((void **)&h->st_host, sizeof(SolverState), cudaHostAllocMapped) !=
+          cudaSuccess ||
+      cudaHostAlloc((void **)&h->scal_host, sizeof(double) * 8, cudaHostAllocMapped) !=
+          cudaSuccess ||
+      cudaHostAlloc((void **)&h->rd_host, sizeof(double) * kMaxBasis, cudaHostAllocMapped) !=
+          cudaSuccess)
+    return cleanup(fail(MPDG_ERR_OUT_OF_MEMORY, "cudaHostAlloc"));
+  if (cudaHostGetDevicePointer((void **)&h->st_map, h->st_host, 0) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&h->scal_map, h->scal_host, 0) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&h->rd_map, h->rd_host, 0) != cudaSuccess)
+    return cleanup(fail(MPDG_ERR_CUDA, "cudaHostGetDevicePointer"));
   cudaMemset(h->counter, 0, sizeof(unsigned) * 4);
   cudaMemset(h->st, 0, sizeof(SolverState));
   memset(h->st_host, 0, sizeof(SolverState));
@@ -2838,7 +2902,7 @@ extern "C" int mpdg_heat_vmult(mpdg_heat *h, double *dst, const double *src)
 {
   if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   CU(cudaSetDevice(h->device));
-  CU(cudaMemsetAsync(dst, 0, sizeof(double) * h->n_dofs, h->stream));
+  CU(zero_async(h, dst, sizeof(double) * h->n_dofs, h->stream));
   return op_apply_d(h, dst, src, FIN_NONE, nullptr, nullptr);
 }
 
@@ -2846,7 +2910,7 @@ extern "C" int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src)
 {
   if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   CU(cudaSetDevice(h->device));
-  CU(cudaMemsetAsync(dst, 0, sizeof(float) * h->n_dofs, h->stream));
+  CU(zero_async(h, dst, sizeof(float) * h->n_dofs, h->stream));
   return op_apply_f(h, dst, src, nullptr);
 }
 
@@ -2862,7 +2926,7 @@ extern "C" int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float 
   a.Tl = h->T_lin;
   CU(h->tab.conductivity_q(a, h->kq, h->law, h->stream, h->sm_count));
   ++h->launches;
-  CU(cudaMemsetAsync(dst, 0, sizeof(float) * h->n_dofs, h->stream));
+  CU(zero_async(h, dst, sizeof(float) * h->n_dofs, h->stream));
   return op_apply_f(h, dst, src, nullptr, true);
 }
 
@@ -2890,7 +2954,7 @@ static int compute_diag(mpdg_heat *h, double *d, bool invert)
   TRY(ensure_dt(h));
   TRY(ensure_lin(h));
   TRY(ensure_fields(h));
-  CU(cudaMemsetAsync(d, 0, sizeof(double) * h->n_dofs, h->stream));
+  CU(zero_async(h, d, sizeof(double) * h->n_dofs, h->stream));
   CellArgs<double> a = cell_args<double>(h);
   a.g.q = h->geoq;
   a.cf = h->cf;
@@ -2983,8 +3047,7 @@ extern "C" int mpdg_heat_l2_norm(mpdg_heat *h, const double *u, double *norm)
   a.out = h->scal;
   CU(h->tab.norm(a, h->geo, 0, h->stream, h->sm_count));
   ++h->launches;
-  CU(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
+  TRY(read_to_host(h, h->scal_map, h->scal, sizeof(double)));
   *norm = std::sqrt(h->scal_host[0]);
   return MPDG_OK;
 }
@@ -3171,7 +3234,20 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     if (h->dt != dt || !prm->linear.cheb_eig_reuse) h->eig_valid = false;
     h->dt = dt;
     // init_time_advance: predictor into w1, commit history, constraints
-    if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
+    if (h->rotate) {
+      // the predicted T replaces T_{n-1} in its buffer and the two buffers swap roles
+      if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
+        k_predict_inplace<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, dt / dt_old);
+        ++h->launches;
+      } else {
+        const double *from = prm->predictor == MPDG_PREDICTOR_GIVEN ? h->guess : T_cur;
+        if ((rc = (cudaMemcpyAsync(T_old, from, vb, cudaMemcpyDeviceToDevice, h->stream) ==
+                   cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, "predictor copy"))) != MPDG_OK)
+          break;
+      }
+      std::swap(T_cur, T_old);
+      h->rotated = true;
+    } else if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
       k_predict<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, h->w1, dt / dt_old); ++h->launches;
     } else if (prm->predictor == MPDG_PREDICTOR_GIVEN) {
       if ((rc = (cudaMemcpyAsync(h->w1, h->guess, vb, cudaMemcpyDeviceToDevice, h->stream) ==
@@ -3180,8 +3256,10 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
       if ((rc = (cudaMemcpyAsync(h->w1, T_cur, vb, cudaMemcpyDeviceToDevice, h->stream) ==
                  cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, "copy"))) != MPDG_OK) break;
     }
-    cudaMemcpyAsync(T_old, T_cur, vb, cudaMemcpyDeviceToDevice, h->stream);
-    cudaMemcpyAsync(T_cur, h->w1, vb, cudaMemcpyDeviceToDevice, h->stream);
+    if (!h->rotate) {
+      cudaMemcpyAsync(T_old, T_cur, vb, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(T_cur, h->w1, vb, cudaMemcpyDeviceToDevice, h->stream);
+    }
     if (h->record_commit) {
       // T_old is final here: its copy to the host runs on the copy stream during the step
       cudaEventRecord(h->ev_commit, h->stream);
@@ -3211,9 +3289,9 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     if (prm->single_linearization) {
       // b = J T_g - R(T_g); solve J delta = -R(T_g) to |b - J T| <= tol |b|
       // J T_g first: it does not need the source, whose upload may still be running
-      cudaMemsetAsync(h->z, 0, vb, h->stream);
+      zero_async(h, h->z, vb, h->stream);
       if ((rc = op_apply_d(h, h->z, T_cur, FIN_NONE, nullptr, nullptr)) != MPDG_OK) break;
-      cudaMemsetAsync(h->w2, 0, vb, h->stream);
+      zero_async(h, h->w2, vb, h->stream);
       if (h->wait_source) cudaStreamWaitEvent(h->stream, h->ev_source, 0);
       if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
       double rr = 0.0, bb = 0.0;
@@ -3221,7 +3299,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
       mpdg_solver_params lp = prm->linear;
       lp.tol_reference_norm = std::sqrt(bb);
       lp.abs_tolerance = std::max(lp.abs_tolerance, 0.0);
-      cudaMemsetAsync(h->w1, 0, vb, h->stream);
+      zero_async(h, h->w1, vb, h->stream);
       mpdg_solve_stats ls;
       memset(&ls, 0, sizeof(ls));
       h->x_zero = true;
@@ -3236,10 +3314,10 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
       s.initial_relative_residual = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
     } else {
       for (int i = 0; i < prm->newton_max_iterations; ++i) {
-        cudaMemsetAsync(h->w2, 0, vb, h->stream);
+        zero_async(h, h->w2, vb, h->stream);
         if (h->wait_source) cudaStreamWaitEvent(h->stream, h->ev_source, 0);
         if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
-        cudaMemsetAsync(h->w1, 0, vb, h->stream);
+        zero_async(h, h->w1, vb, h->stream);
         mpdg_solve_stats ls;
         memset(&ls, 0, sizeof(ls));
         h->x_zero = true;
@@ -3380,10 +3458,16 @@ extern "C" int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params
     CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->copy_stream));
     CU(cudaEventRecord(h->ev_source, h->copy_stream));
   }
+  // the two history buffers swap roles: the predictor overwrites T_{n-1} in place
   h->wait_source = heat_source != nullptr;
+  h->rotate = true;
+  h->rotated = false;
   const int rc = mpdg_heat_time_step(h, prm, dt, dt_old, h->res_T, h->res_To,
                                      heat_source ? h->host_q : nullptr, stats);
   h->wait_source = false;
+  h->rotate = false;
+  if (h->rotated) std::swap(h->res_T, h->res_To);
+  h->rotated = false;
   if (rc != MPDG_OK) {
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     return rc;
@@ -3635,7 +3719,7 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
   const int rc = mpdg_unet_forward(u, h->nn_buf, h->nn_buf + 3 * nc);
   if (rc != MPDG_OK) return fail(rc, "network forward failed");
   // d = a * P(y) (prolongated correction) into w1, zero at Dirichlet DoFs
-  CU(cudaMemsetAsync(h->w2, 0, sizeof(double) * N, h->stream));
+  CU(zero_async(h, h->w2, sizeof(double) * N, h->stream));
   k_learned_guess<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, stride, c[0], c[1], c[2], h->w2,
                                                      h->w2, h->nn_buf + 3 * nc, a, h->w1);
   ++h->launches;
@@ -3649,10 +3733,10 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
     h->lin_f_dirty = true;
     h->tf_dirty = true;
     h->tk_dirty = true;
-    CU(cudaMemsetAsync(h->w2, 0, sizeof(double) * N, h->stream));
+    CU(zero_async(h, h->w2, sizeof(double) * N, h->stream));
     int rr = create_rhs(h, h->w2, T, heat_source);               // r = -R(LE)
     if (rr == MPDG_OK) {
-      CU(cudaMemsetAsync(h->w3, 0, sizeof(double) * N, h->stream));
+      CU(zero_async(h, h->w3, sizeof(double) * N, h->stream));
       rr = op_apply_d(h, h->w3, h->w1, FIN_NONE, nullptr, nullptr);  // J d
     }
     h->T_lin = keepT;

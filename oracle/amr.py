@@ -1,0 +1,275 @@
+"""Heat operator on a two-level box mesh with hanging-node constraints (TEST INFRASTRUCTURE ONLY).
+
+A CPU restatement of what MeltPoolDG's heat path does on an adaptively refined mesh. The heat
+application refines its triangulation with ``refine_grid`` (``source/utilities/amr.cpp:18-41``,
+called from ``applications/mp-heat-transfer/heat_transfer_application.cpp:363-453``) and builds
+the heat DoFs' constraints with deal.II's ``DoFTools::make_hanging_node_constraints``, merged into
+the Dirichlet constraints (``include/meltpooldg/utilities/constraints.hpp:111-132``, ``:256-269``).
+deal.II is not vendored with the reference; its published rule is restated here: a node of a
+refined cell that lies on a face or an edge of an unrefined neighbour, and is not one of the
+neighbour's nodes, is constrained to the neighbour's FE_Q(p) interpolant at that point,
+``u_h = sum_c phi_c(x_h) u_c`` over the neighbour's nodes (the continuous FE space on a mesh with
+one level of refinement difference).
+
+The mesh is a structured box of ``cells`` coarse cells in which any set of coarse cells is
+refined once (each into 8 children). The operator is the heat tangent of the structured oracle
+(``mpdg_oracle.c``: ``rho_cp/dt M + K_k`` with ``k = k0 + k1 T_lin`` and the ``k1 grad(T_lin) u``
+term of the linear law, ``heat_diffuse_operator.cpp:1029-1078``), assembled from element
+matrices on the active cells and condensed as ``C^T A C`` with the hanging-node matrix ``C``.
+Dirichlet DoFs follow the deal.II conventions of the structured oracle: read as zero, zero rows.
+
+Only tests use this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+FACES = {"x-": (0, 0), "x+": (0, 1), "y-": (1, 0), "y+": (1, 1), "z-": (2, 0), "z+": (2, 1)}
+
+
+def gauss_lobatto(p: int) -> np.ndarray:
+    """The p+1 Gauss-Lobatto points on [0, 1]: the ends and the roots of P_p' (Newton-polished)."""
+    if p == 1:
+        return np.array([0.0, 1.0])
+    dP = np.polynomial.legendre.Legendre.basis(p).deriv()
+    x = np.sort(dP.roots().real)
+    d2P = dP.deriv()
+    for _ in range(3):
+        x = x - dP(x) / d2P(x)
+    return (np.concatenate([[-1.0], x, [1.0]]) + 1.0) / 2.0
+
+
+def gauss(n: int):
+    """n-point Gauss-Legendre rule on [0, 1]."""
+    x, w = np.polynomial.legendre.leggauss(n)
+    return (x + 1.0) / 2.0, w / 2.0
+
+
+def lagrange(nodes: np.ndarray, x: np.ndarray):
+    """Values V[q, i] = l_i(x_q) and derivatives D[q, i] of the Lagrange basis on `nodes`."""
+    x = np.atleast_1d(np.asarray(x, dtype=np.float64))
+    n = len(nodes)
+    V = np.ones((len(x), n))
+    D = np.zeros((len(x), n))
+    for i in range(n):
+        others = [j for j in range(n) if j != i]
+        den = np.prod([nodes[i] - nodes[j] for j in others])
+        for j in others:
+            V[:, i] *= (x - nodes[j])
+        for m in others:
+            term = np.ones(len(x))
+            for j in others:
+                if j != m:
+                    term *= (x - nodes[j])
+            D[:, i] += term
+        V[:, i] /= den
+        D[:, i] /= den
+    return V, D
+
+
+class TwoLevelBoxMesh:
+    """FE_Q(p) heat operator on a box of coarse cells, the cells in `refine` split once.
+
+    refine: iterable of coarse cell indices (ix, iy, iz), or a boolean array [mz][my][mx].
+    DoFs are the nodes that are not hanging, numbered by position (z, y, x lexicographic).
+    constrain_hanging=False leaves the hanging nodes free (a nonconforming space): a planted
+    mistake for the tests that check the constraints matter.
+    """
+
+    def __init__(self, degree, cells, refine=(), lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
+                 dirichlet=("x-", "x+", "y-", "y+", "z-", "z+"), constrain_hanging=True):
+        self.p = p = int(degree)
+        self.n = n = p + 1
+        self.m = m = tuple(int(c) for c in cells)
+        self.lo = np.asarray(lo, dtype=np.float64)
+        self.h = (np.asarray(hi, dtype=np.float64) - self.lo) / np.asarray(m)
+        ref = np.zeros((m[2], m[1], m[0]), dtype=bool)
+        if isinstance(refine, np.ndarray) and refine.dtype == bool:
+            ref[...] = refine
+        else:
+            for ix, iy, iz in refine:
+                ref[iz, iy, ix] = True
+        self.refined = ref
+        self.xi = gauss_lobatto(p)
+        # active cells: origin and size in coarse-cell units
+        origins, sizes, parents = [], [], []
+        for iz in range(m[2]):
+            for iy in range(m[1]):
+                for ix in range(m[0]):
+                    if ref[iz, iy, ix]:
+                        for sz in (0, 1):
+                            for sy in (0, 1):
+                                for sx in (0, 1):
+                                    origins.append((ix + 0.5 * sx, iy + 0.5 * sy, iz + 0.5 * sz))
+                                    sizes.append(0.5)
+                                    parents.append((ix, iy, iz))
+                    else:
+                        origins.append((ix, iy, iz))
+                        sizes.append(1.0)
+                        parents.append((ix, iy, iz))
+        self.origins = np.asarray(origins, dtype=np.float64)
+        self.sizes = np.asarray(sizes, dtype=np.float64)
+        self.n_cells = len(sizes)
+        # local node offsets in the unit cell, x fastest
+        lx = np.array([(self.xi[i], self.xi[j], self.xi[k])
+                       for k in range(n) for j in range(n) for i in range(n)])
+        self._local = lx
+        pos = self.origins[:, None, :] + self.sizes[:, None, None] * lx[None, :, :]
+        keys = np.round(pos.reshape(-1, 3) * (1 << 26)).astype(np.int64)
+        uniq, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+        self.cell_nodes = inv.reshape(self.n_cells, n ** 3)
+        self.node_pos = pos.reshape(-1, 3)[first]  # coarse-cell units (the key only matches)
+        n_nodes = len(uniq)
+        # hanging nodes: nodes of refined cells that lie on the closed box of an unrefined
+        # coarse cell without being one of its nodes; constrained to its interpolant there
+        coarse_cells = [c for c in range(self.n_cells) if self.sizes[c] == 1.0]
+        is_coarse_node = np.zeros(n_nodes, dtype=bool)
+        for c in coarse_cells:
+            is_coarse_node[self.cell_nodes[c]] = True
+        fine_nodes = np.unique(self.cell_nodes[self.sizes == 0.5]) if np.any(
+            self.sizes == 0.5) else np.zeros(0, dtype=np.int64)
+        candidates = [v for v in fine_nodes if not is_coarse_node[v]] if constrain_hanging else []
+        cons = {}
+        tol = 1e-9
+        coarse_origin = {tuple(self.origins[c].astype(int)): c for c in coarse_cells}
+        for v in candidates:
+            x = self.node_pos[v]
+            # unrefined coarse cells whose closed box holds x
+            base = np.floor(x + tol).astype(int)
+            owner = None
+            for dz in (0, -1):
+                for dy in (0, -1):
+                    for dx in (0, -1):
+                        c0 = (base[0] + dx, base[1] + dy, base[2] + dz)
+                        if c0 in coarse_origin:
+                            o = np.asarray(c0, dtype=np.float64)
+                            if np.all(x >= o - tol) and np.all(x <= o + 1.0 + tol):
+                                owner = coarse_origin[c0]
+                                break
+                    if owner is not None:
+                        break
+                if owner is not None:
+                    break
+            if owner is None:
+                continue  # interior of the refined region: a regular node
+            loc = np.clip(x - self.origins[owner], 0.0, 1.0)
+            w = self._tensor_basis(loc)
+            nz = np.abs(w) > 1e-14
+            cons[v] = (self.cell_nodes[owner][nz], w[nz])
+        self.hanging = np.zeros(n_nodes, dtype=bool)
+        self.hanging[list(cons)] = True
+        # DoFs: the regular nodes, in position order (z, y, x)
+        regular = np.flatnonzero(~self.hanging)
+        order = np.lexsort((self.node_pos[regular, 0], self.node_pos[regular, 1],
+                            self.node_pos[regular, 2]))
+        regular = regular[order]
+        self.dof_of_node = -np.ones(n_nodes, dtype=np.int64)
+        self.dof_of_node[regular] = np.arange(len(regular))
+        self.n_dofs = len(regular)
+        self.node_of_dof = regular
+        rows, cols, vals = [], [], []
+        for v in regular:
+            rows.append(v)
+            cols.append(self.dof_of_node[v])
+            vals.append(1.0)
+        for v, (cn, w) in cons.items():
+            for c, wc in zip(cn, w):
+                d = self.dof_of_node[c]
+                assert d >= 0, "a hanging node depends on another hanging node"
+                rows.append(v)
+                cols.append(d)
+                vals.append(wc)
+        self.C = sp.csr_matrix((vals, (rows, cols)), shape=(n_nodes, self.n_dofs))
+        # Dirichlet DoFs: regular nodes on the flagged faces of the box
+        mask = np.zeros(self.n_dofs, dtype=bool)
+        P = self.node_pos[regular]
+        for f in dirichlet:
+            d, side = FACES[f]
+            mask |= np.abs(P[:, d] - (m[d] if side else 0)) < 1e-9
+        self.mask = mask
+        # reference-cell tables: QGauss(p+1), FE_Q(p) on Gauss-Lobatto points
+        xq, wq = gauss(n)
+        V1, D1 = lagrange(self.xi, xq)
+        self._N = np.kron(V1, np.kron(V1, V1))
+        self._G = [np.kron(V1, np.kron(V1, D1)), np.kron(V1, np.kron(D1, V1)),
+                   np.kron(D1, np.kron(V1, V1))]
+        self._w = np.kron(wq, np.kron(wq, wq))
+        self._xq = np.array([(xq[i], xq[j], xq[k]) for k in range(n) for j in range(n)
+                             for i in range(n)])
+
+    def _tensor_basis(self, loc):
+        vx = lagrange(self.xi, [loc[0]])[0][0]
+        vy = lagrange(self.xi, [loc[1]])[0][0]
+        vz = lagrange(self.xi, [loc[2]])[0][0]
+        return np.kron(vz, np.kron(vy, vx))
+
+    # ------------------------------------------------------------------------------------
+    def support_points(self) -> np.ndarray:
+        """Physical coordinates of the DoFs, shape (n_dofs, 3)."""
+        return self.lo + self.node_pos[self.node_of_dof] * self.h
+
+    def quadrature_points(self, cell: int) -> np.ndarray:
+        return self.lo + (self.origins[cell] + self.sizes[cell] * self._xq) * self.h
+
+    def node_values(self, u_dofs: np.ndarray) -> np.ndarray:
+        """All nodal values (hanging nodes from their constraints)."""
+        return self.C @ u_dofs
+
+    def _cell_factors(self, cell):
+        hs = self.sizes[cell] * self.h
+        jxw = self._w * np.prod(hs)
+        G = [self._G[d] / hs[d] for d in range(3)]
+        return jxw, G
+
+    def assemble(self, rho_cp=1.0, dt=1.0, k0=1.0, k1=0.0, T_lin=None) -> sp.csr_matrix:
+        """C^T A C of the tangent rho_cp/dt M + K_k(T_lin) (+ k1 grad(T_lin) u), on all DoFs."""
+        n3 = self.n ** 3
+        Tn = None if T_lin is None or k1 == 0.0 else self.node_values(T_lin)
+        rows = np.repeat(self.cell_nodes, n3, axis=1).ravel()
+        cols = np.tile(self.cell_nodes, (1, n3)).ravel()
+        data = np.empty((self.n_cells, n3, n3))
+        N = self._N
+        for c in range(self.n_cells):
+            jxw, G = self._cell_factors(c)
+            A = (rho_cp / dt) * (N.T * jxw) @ N
+            if Tn is None:
+                kq = np.full(len(jxw), k0)
+                gT = None
+            else:
+                te = Tn[self.cell_nodes[c]]
+                kq = k0 + k1 * (N @ te)
+                gT = [Gd @ te for Gd in G]
+            for d in range(3):
+                A += (G[d].T * (jxw * kq)) @ G[d]
+                if gT is not None:
+                    A += (G[d].T * (jxw * k1 * gT[d])) @ N
+            data[c] = A
+        An = sp.csr_matrix((data.ravel(), (rows, cols)),
+                           shape=(len(self.node_pos), len(self.node_pos)))
+        return (self.C.T @ An @ self.C).tocsr()
+
+    def vmult(self, src, **coef) -> np.ndarray:
+        """dst = J src with Dirichlet DoFs read as zero and their rows zero."""
+        s = np.where(self.mask, 0.0, src)
+        y = self.assemble(**coef) @ s
+        y[self.mask] = 0.0
+        return y
+
+    def load_vector(self, f) -> np.ndarray:
+        """C^T of the element integrals of f(x) phi_i (f evaluated at the q-points)."""
+        b = np.zeros(len(self.node_pos))
+        for c in range(self.n_cells):
+            jxw, _ = self._cell_factors(c)
+            fq = f(self.quadrature_points(c))
+            np.add.at(b, self.cell_nodes[c], self._N.T @ (jxw * fq))
+        return self.C.T @ b
+
+    def solve(self, b, **coef) -> np.ndarray:
+        """Solve J x = b on the free DoFs (direct), x = 0 on the Dirichlet DoFs."""
+        A = self.assemble(**coef)
+        free = np.flatnonzero(~self.mask)
+        x = np.zeros(self.n_dofs)
+        x[free] = spla.spsolve(A[free][:, free].tocsc(), b[free])
+        return x

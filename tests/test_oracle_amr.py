@@ -1,0 +1,122 @@
+"""The two-level (hanging-node) restatement of the heat operator, oracle/amr.py, against the
+structured oracle where the two meshes coincide, and against solutions the constrained FE space
+holds exactly where they do not."""
+import numpy as np
+import pytest
+
+from oracle import amr as A
+from oracle import oracle as O
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("case", ["unrefined", "refined"])
+def test_matches_structured_oracle_without_hanging_nodes(p, case):
+    """No cell refined, or every cell refined: the same operator as the structured oracle on
+    the coarse or the twice finer box (constant law and the linear-k tangent)."""
+    if case == "unrefined":
+        mesh = A.TwoLevelBoxMesh(p, (3, 2, 2))
+        o = O.Oracle(p, (3, 2, 2))
+    else:
+        mesh = A.TwoLevelBoxMesh(p, (2, 2, 1), refine=np.ones((1, 2, 2), dtype=bool))
+        o = O.Oracle(p, (4, 4, 2))
+    assert not mesh.hanging.any()
+    assert mesh.n_dofs == o.n_dofs
+    assert np.abs(mesh.support_points() - o.support_points()).max() < 1e-13
+    assert np.array_equal(mesh.mask, o.mask().astype(bool))
+    rng = np.random.default_rng(10 + p)
+    src = rng.uniform(-1.0, 1.0, mesh.n_dofs)
+    dt = 1e-2
+    o.set_material(O.material(O.LAW_CONSTANT, rho=2.0, cp=1.5, k=0.7), dt)
+    assert _rel(mesh.vmult(src, rho_cp=3.0, dt=dt, k0=0.7), o.vmult(src)) < 1e-12
+    o.set_material(O.material(O.LAW_LINEAR_K, k=1.0, k1=0.5), dt)
+    T = o.distribute(rng.uniform(0.0, 1.0, mesh.n_dofs))
+    ref = o.vmult(src, T_lin=T)
+    assert _rel(mesh.vmult(src, dt=dt, k0=1.0, k1=0.5, T_lin=T), ref) < 1e-12
+
+
+REFINE = [(1, 1, 1), (2, 1, 1), (1, 2, 1), (1, 1, 2), (0, 0, 0)]  # a block, a corner cell
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_hanging_constraints_interpolate_the_coarse_space(p):
+    """Every hanging node's weights sum to one and reproduce any global Q_p function."""
+    mesh = A.TwoLevelBoxMesh(p, (4, 3, 3), refine=REFINE)
+    assert mesh.hanging.any()
+    rows = mesh.C[np.flatnonzero(mesh.hanging)]
+    assert np.abs(np.asarray(rows.sum(axis=1)).ravel() - 1.0).max() < 1e-13
+    rng = np.random.default_rng(p)
+    c = rng.uniform(-1.0, 1.0, (p + 1, p + 1, p + 1))
+
+    def f(x):
+        P = [np.stack([x[:, d] ** e for e in range(p + 1)], axis=1) for d in range(3)]
+        return np.einsum("ijk,ni,nj,nk->n", c, P[0], P[1], P[2])
+
+    nodes = mesh.lo + mesh.node_pos * mesh.h
+    u = f(mesh.support_points())
+    assert np.abs(mesh.node_values(u) - f(nodes)).max() < 1e-12 * np.abs(f(nodes)).max()
+
+
+S = 64.0  # u = S x(1-x) y(1-y) z(1-z) peaks at 1
+
+
+def _u(x):
+    return S * np.prod(x * (1.0 - x), axis=1)
+
+
+def _grad_u(x):
+    q = x * (1.0 - x)
+    return S * np.stack([(1.0 - 2.0 * x[:, d]) * np.prod(np.delete(q, d, axis=1), axis=1)
+                         for d in range(3)], axis=1)
+
+
+def _lap_u(x):
+    q = x * (1.0 - x)
+    return -2.0 * S * sum(np.prod(np.delete(q, d, axis=1), axis=1) for d in range(3))
+
+
+# (p, tangent): QGauss(p+1) integrates the constant-law forms exactly for p >= 2 and the
+# tangent's (k0 + 2 k1 u) grad(u).grad(v) for p >= 3
+@pytest.mark.parametrize("p,tangent", [(2, False), (3, False), (4, False), (3, True), (4, True)])
+def test_galerkin_solution_is_exact_for_representable_fields(p, tangent):
+    """u = 64 x(1-x) y(1-y) z(1-z) lies in the constrained space for p >= 2: the heat
+    operator's Galerkin solution with the matching load reproduces it at every DoF, and the
+    same mesh with its hanging nodes left free (a planted mistake) does not."""
+    refine = [(1, 1, 1), (2, 1, 1), (0, 2, 2)]
+    rho_cp, dt, k0, k1 = 2.0, 0.1, 1.0, (0.5 if tangent else 0.0)
+
+    def load(x):
+        # strong form of rho_cp/dt w - div((k0 + k1 T) grad(w) + k1 grad(T) w) at T = w = u
+        val = rho_cp / dt * _u(x)
+        if tangent:
+            return (val - (k0 + 2.0 * k1 * _u(x)) * _lap_u(x)
+                    - 2.0 * k1 * (_grad_u(x) ** 2).sum(axis=1))
+        return val - k0 * _lap_u(x)
+
+    errs = []
+    for constrained in (True, False):
+        mesh = A.TwoLevelBoxMesh(p, (3, 3, 3), refine=refine, constrain_hanging=constrained)
+        assert mesh.hanging.any() == constrained
+        T = _u(mesh.support_points())
+        x = mesh.solve(mesh.load_vector(load), rho_cp=rho_cp, dt=dt, k0=k0, k1=k1,
+                       T_lin=T if tangent else None)
+        exact = np.where(mesh.mask, 0.0, T)
+        errs.append(np.abs(x - exact).max() / np.abs(exact).max())
+    assert errs[0] < 1e-10
+    assert errs[1] > 1e-6
+
+
+def test_constrained_operator_is_symmetric_positive_definite():
+    mesh = A.TwoLevelBoxMesh(3, (3, 3, 2), refine=[(1, 1, 0), (0, 0, 1)])
+    Amat = mesh.assemble(rho_cp=1.0, dt=1e-3, k0=2.0)
+    free = np.flatnonzero(~mesh.mask)
+    Af = Amat[free][:, free].toarray()
+    assert np.abs(Af - Af.T).max() < 1e-12 * np.abs(Af).max()
+    assert np.linalg.eigvalsh(Af).min() > 0.0
+    # the mass part integrates the constant function to the volume
+    M = mesh.assemble(rho_cp=1.0, dt=1.0, k0=0.0)
+    one = np.ones(mesh.n_dofs)
+    assert abs(one @ (M @ one) - 1.0) < 1e-12

@@ -111,6 +111,9 @@ class TwoLevelBoxMesh:
                         parents.append((ix, iy, iz))
         self.origins = np.asarray(origins, dtype=np.float64)
         self.sizes = np.asarray(sizes, dtype=np.float64)
+        self.parents = np.asarray(parents, dtype=np.int64)
+        # child position (s_x, s_y, s_z) of a refined cell in its parent
+        self.child = np.rint((self.origins - self.parents) * 2.0).astype(np.int64)
         self.n_cells = len(sizes)
         # local node offsets in the unit cell, x fastest
         lx = np.array([(self.xi[i], self.xi[j], self.xi[k])
@@ -223,6 +226,23 @@ class TwoLevelBoxMesh:
         G = [self._G[d] / hs[d] for d in range(3)]
         return jxw, G
 
+    def _element_matrix(self, c, rho_cp, dt, k0, k1, te):
+        """Cell matrix of rho_cp/dt M + K_k (+ k1 grad(T_lin) u) with te the cell's T_lin."""
+        jxw, G = self._cell_factors(c)
+        N = self._N
+        A = (rho_cp / dt) * (N.T * jxw) @ N
+        if te is None:
+            kq = np.full(len(jxw), k0)
+            gT = None
+        else:
+            kq = k0 + k1 * (N @ te)
+            gT = [Gd @ te for Gd in G]
+        for d in range(3):
+            A += (G[d].T * (jxw * kq)) @ G[d]
+            if gT is not None:
+                A += (G[d].T * (jxw * k1 * gT[d])) @ N
+        return A
+
     def assemble(self, rho_cp=1.0, dt=1.0, k0=1.0, k1=0.0, T_lin=None) -> sp.csr_matrix:
         """C^T A C of the tangent rho_cp/dt M + K_k(T_lin) (+ k1 grad(T_lin) u), on all DoFs."""
         n3 = self.n ** 3
@@ -230,22 +250,9 @@ class TwoLevelBoxMesh:
         rows = np.repeat(self.cell_nodes, n3, axis=1).ravel()
         cols = np.tile(self.cell_nodes, (1, n3)).ravel()
         data = np.empty((self.n_cells, n3, n3))
-        N = self._N
         for c in range(self.n_cells):
-            jxw, G = self._cell_factors(c)
-            A = (rho_cp / dt) * (N.T * jxw) @ N
-            if Tn is None:
-                kq = np.full(len(jxw), k0)
-                gT = None
-            else:
-                te = Tn[self.cell_nodes[c]]
-                kq = k0 + k1 * (N @ te)
-                gT = [Gd @ te for Gd in G]
-            for d in range(3):
-                A += (G[d].T * (jxw * kq)) @ G[d]
-                if gT is not None:
-                    A += (G[d].T * (jxw * k1 * gT[d])) @ N
-            data[c] = A
+            te = None if Tn is None else Tn[self.cell_nodes[c]]
+            data[c] = self._element_matrix(c, rho_cp, dt, k0, k1, te)
         An = sp.csr_matrix((data.ravel(), (rows, cols)),
                            shape=(len(self.node_pos), len(self.node_pos)))
         return (self.C.T @ An @ self.C).tocsr()
@@ -273,3 +280,134 @@ class TwoLevelBoxMesh:
         x = np.zeros(self.n_dofs)
         x[free] = spla.spsolve(A[free][:, free].tocsc(), b[free])
         return x
+
+    # ------------------------------------------------------------------------------------
+    # second form: the constraints applied inside each cell, as a cell kernel applies them
+    def _coarse_unrefined(self, q):
+        m = self.m
+        if not all(0 <= q[d] < m[d] for d in range(3)):
+            return None
+        if self.refined[q[2], q[1], q[0]]:
+            return None
+        return q
+
+    def hanging_code(self, c) -> int:
+        """9-bit code of a cell's hanging faces and edges: bits 0-2 its child position
+        (s_x, s_y, s_z) in the parent, bit 3+d a hanging face normal to direction d (at side
+        s_d), bit 6+d a hanging edge parallel to d (at the sides s of the two other directions)
+        whose two adjacent faces do not hang. 0 for a cell without hanging nodes."""
+        if self.sizes[c] == 1.0 or not self.hanging.any():
+            return 0
+        par, sv = self.parents[c], self.child[c]
+        step = np.where(sv == 0, -1, 1)
+        face = [self._coarse_unrefined(par + step[d] * np.eye(3, dtype=np.int64)[d]) is not None
+                for d in range(3)]
+        edge = []
+        for d in range(3):
+            d1, d2 = [e for e in range(3) if e != d]
+            off = np.zeros(3, dtype=np.int64)
+            off[d1], off[d2] = step[d1], step[d2]
+            edge.append(self._coarse_unrefined(par + off) is not None and not face[d1]
+                        and not face[d2])
+        code = sum(int(face[d]) << (3 + d) for d in range(3)) + \
+            sum(int(edge[d]) << (6 + d) for d in range(3))
+        if code == 0:
+            return 0
+        return code | int(sv[0]) | (int(sv[1]) << 1) | (int(sv[2]) << 2)
+
+    def child_interpolation(self, s: int) -> np.ndarray:
+        """I[j, a] = l_a((s + xi_j) / 2): the coarse 1D basis at the nodes of child s."""
+        return lagrange(self.xi, (s + self.xi) / 2.0)[0]
+
+    def cell_map(self, c):
+        """Gathered DoF indices of cell c and the matrix F with local = F gathered: the nodes
+        of a hanging face or edge gather the coarse neighbour's face or edge DoFs of the same
+        indices, and F interpolates them with the 1D child matrices, one direction at a time."""
+        n, n3 = self.n, self.n ** 3
+        idx = self.dof_of_node[self.cell_nodes[c]].copy()
+        code = self.hanging_code(c)
+        if code == 0:
+            return idx, None
+        sv = [(code >> d) & 1 for d in range(3)]
+        par = self.parents[c]
+        step = [(-1 if sv[d] == 0 else 1) for d in range(3)]
+        own = [0 if sv[d] == 0 else n - 1 for d in range(3)]   # the cell's side
+        other = [n - 1 - own[d] for d in range(3)]             # the neighbour's side
+        lin = lambda i, j, k: i + n * (j + n * k)
+        lines = {0: [], 1: [], 2: []}  # lines along d to interpolate: fixed (index, index)
+        for d in range(3):
+            if not (code >> (3 + d)) & 1:
+                continue
+            q = par.copy()
+            q[d] += step[d]
+            nb = self._coarse_cell(q)
+            for a in range(n):
+                for b in range(n):
+                    i = [0, 0, 0]
+                    d1, d2 = [e for e in range(3) if e != d]
+                    i[d], i[d1], i[d2] = own[d], a, b
+                    jn = list(i)
+                    jn[d] = other[d]
+                    idx[lin(*i)] = self.dof_of_node[self.cell_nodes[nb][lin(*jn)]]
+            for e in range(3):
+                if e != d:
+                    lines[e].append((d, own[d]))
+        for d in range(3):
+            if not (code >> (6 + d)) & 1:
+                continue
+            d1, d2 = [e for e in range(3) if e != d]
+            q = par.copy()
+            q[d1] += step[d1]
+            q[d2] += step[d2]
+            nb = self._coarse_cell(q)
+            for a in range(n):
+                i = [0, 0, 0]
+                i[d], i[d1], i[d2] = a, own[d1], own[d2]
+                jn = list(i)
+                jn[d1], jn[d2] = other[d1], other[d2]
+                idx[lin(*i)] = self.dof_of_node[self.cell_nodes[nb][lin(*jn)]]
+            lines[d].append(((d1, own[d1]), (d2, own[d2])))
+        F = np.eye(n3)
+        for d in range(3):
+            I = self.child_interpolation(sv[d])
+            Fd = np.eye(n3)
+            done = set()
+            for spec in lines[d]:
+                fixed = [spec] if isinstance(spec[0], int) else list(spec)
+                d1, d2 = [e for e in range(3) if e != d]
+                for a in range(n):
+                    for b in range(n):
+                        i = [0, 0, 0]
+                        i[d1], i[d2] = a, b
+                        if any(i[fd] != fv for fd, fv in fixed) or (a, b) in done:
+                            continue
+                        done.add((a, b))
+                        nodes = []
+                        for t in range(n):
+                            i[d] = t
+                            nodes.append(lin(*i))
+                        Fd[np.ix_(nodes, nodes)] = I
+            F = Fd @ F
+        assert (idx >= 0).all(), "a hanging node left ungathered"
+        return idx, F
+
+    def _coarse_cell(self, q):
+        ox = np.asarray(q, dtype=np.float64)
+        hit = np.flatnonzero((self.sizes == 1.0) & np.all(self.origins == ox, axis=1))
+        return int(hit[0])
+
+    def vmult_cellwise(self, src, rho_cp=1.0, dt=1.0, k0=1.0, k1=0.0, T_lin=None) -> np.ndarray:
+        """The operator of vmult with the constraints applied per cell (gather, F, cell matrix,
+        F^T, scatter), as a matrix-free cell kernel applies them."""
+        s = np.where(self.mask, 0.0, src)
+        y = np.zeros(self.n_dofs)
+        for c in range(self.n_cells):
+            idx, F = self.cell_map(c)
+            ul = s[idx] if F is None else F @ s[idx]
+            te = None
+            if T_lin is not None and k1 != 0.0:
+                te = T_lin[idx] if F is None else F @ T_lin[idx]
+            yl = self._element_matrix(c, rho_cp, dt, k0, k1, te) @ ul
+            np.add.at(y, idx, yl if F is None else F.T @ yl)
+        y[self.mask] = 0.0
+        return y

@@ -120,3 +120,28 @@ def test_constrained_operator_is_symmetric_positive_definite():
     M = mesh.assemble(rho_cp=1.0, dt=1.0, k0=0.0)
     one = np.ones(mesh.n_dofs)
     assert abs(one @ (M @ one) - 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_cellwise_constraints_match_the_condensed_operator(p):
+    """The second form: each refined cell gathers its coarse neighbours' face and edge DoFs and
+    interpolates them with the 1D child matrices, one direction at a time (the cell kernel's
+    form); cell by cell it gives the constrained nodal values, and its operator equals
+    C^T A C. The refinement has cells with hanging faces, with two hanging faces and with
+    hanging edges only (the coarse cell (2, 2, 1) touches (1, 1, 1)'s children on one edge)."""
+    mesh = A.TwoLevelBoxMesh(p, (4, 3, 3), refine=REFINE)
+    codes = [mesh.hanging_code(c) for c in range(mesh.n_cells)]
+    assert any(c & 0o70 for c in codes) and any(c & 0o700 for c in codes)
+    assert any(bin(c & 0o70).count("1") >= 2 for c in codes)
+    rng = np.random.default_rng(20 + p)
+    u = rng.uniform(-1.0, 1.0, mesh.n_dofs)
+    nodal = mesh.node_values(u)
+    for c in range(mesh.n_cells):
+        idx, F = mesh.cell_map(c)
+        local = u[idx] if F is None else F @ u[idx]
+        assert np.abs(local - nodal[mesh.cell_nodes[c]]).max() < 1e-13
+    coef = dict(rho_cp=2.0, dt=0.05, k0=1.0)
+    assert _rel(mesh.vmult_cellwise(u, **coef), mesh.vmult(u, **coef)) < 1e-13
+    T = np.where(mesh.mask, 0.0, rng.uniform(0.0, 1.0, mesh.n_dofs))
+    coef = dict(rho_cp=1.0, dt=0.05, k0=1.0, k1=0.5, T_lin=T)
+    assert _rel(mesh.vmult_cellwise(u, **coef), mesh.vmult(u, **coef)) < 1e-13

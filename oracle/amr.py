@@ -411,3 +411,52 @@ class TwoLevelBoxMesh:
             np.add.at(y, idx, yl if F is None else F.T @ yl)
         y[self.mask] = 0.0
         return y
+
+    # ------------------------------------------------------------------------------------
+    # residual and implicit step (the rest of the path on the refined mesh)
+    def create_rhs(self, T, T_old, heat_source=None, dst=None, rho_cp=1.0, dt=1.0, k0=1.0,
+                   k1=0.0) -> np.ndarray:
+        """dst += -R(T) (create_rhs, heat_diffuse_operator.cpp:393-529): per q-point
+        -(rho_cp/dt (T - T_old) - q_h) against v and -k(T) grad(T) against grad(v), with q_h the
+        FE interpolant of the nodal source; T, T_old and the source are read plain, the
+        Dirichlet rows are left untouched."""
+        dst = np.zeros(self.n_dofs) if dst is None else dst
+        Tn, Ton = self.node_values(T), self.node_values(T_old)
+        qn = None if heat_source is None else self.node_values(heat_source)
+        b = np.zeros(len(self.node_pos))
+        N = self._N
+        for c in range(self.n_cells):
+            jxw, G = self._cell_factors(c)
+            nodes = self.cell_nodes[c]
+            Tq = N @ Tn[nodes]
+            val = rho_cp / dt * (Tq - N @ Ton[nodes])
+            if qn is not None:
+                val = val - N @ qn[nodes]
+            kq = k0 + k1 * Tq
+            r = N.T @ (jxw * val)
+            for d in range(3):
+                r += G[d].T @ (jxw * kq * (G[d] @ Tn[nodes]))
+            np.add.at(b, nodes, -r)
+        r = self.C.T @ b
+        dst[~self.mask] += r[~self.mask]
+        return dst
+
+    def time_step_newton(self, T_cur, T_old, dt, dt_old, heat_source=None, rho_cp=1.0, k0=1.0,
+                         k1=0.0, newton_max_it=10, res_tol=1e-9, corr_tol=1e-10):
+        """HeatDiffuseOperation::solve on the refined mesh, in place: linear predictor
+        (predictor_linear.cpp:74-96), history commit T_old <- T, Dirichlet values (zero), then
+        Newton (newton_raphson_solver.cpp:22-68) with exact linear solves; converged when
+        |rhs| < res_tol and |delta| < corr_tol (the converged update is not applied).
+        Returns the number of Newton iterations."""
+        r = dt / dt_old if abs(dt_old) >= 1e-12 else 0.0
+        pred = (1.0 + r) * T_cur - r * T_old
+        T_old[:] = T_cur
+        T_cur[:] = np.where(self.mask, 0.0, pred)
+        for it in range(newton_max_it):
+            rhs = self.create_rhs(T_cur, T_old, heat_source, rho_cp=rho_cp, dt=dt, k0=k0, k1=k1)
+            delta = self.solve(rhs, rho_cp=rho_cp, dt=dt, k0=k0, k1=k1,
+                               T_lin=T_cur if k1 != 0.0 else None)
+            if np.linalg.norm(rhs) < res_tol and np.linalg.norm(delta) < corr_tol:
+                return it + 1
+            T_cur += delta
+        raise RuntimeError("Newton-Raphson did not converge")

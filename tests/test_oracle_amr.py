@@ -145,3 +145,40 @@ def test_cellwise_constraints_match_the_condensed_operator(p):
     T = np.where(mesh.mask, 0.0, rng.uniform(0.0, 1.0, mesh.n_dofs))
     coef = dict(rho_cp=1.0, dt=0.05, k0=1.0, k1=0.5, T_lin=T)
     assert _rel(mesh.vmult_cellwise(u, **coef), mesh.vmult(u, **coef)) < 1e-13
+
+
+def test_rhs_and_newton_step_match_structured_oracle_without_hanging_nodes():
+    """create_rhs and two implicit k(T) = 1 + 0.5 T steps with a Gaussian source: the refined
+    mesh with every cell refined against the structured oracle on the twice finer box."""
+    p, dt = 2, 1e-2
+    mesh = A.TwoLevelBoxMesh(p, (2, 2, 2), refine=np.ones((2, 2, 2), dtype=bool))
+    o = O.Oracle(p, (4, 4, 4))
+    o.set_material(O.material(O.LAW_LINEAR_K, k=1.0, k1=0.5), dt)
+    rng = np.random.default_rng(3)
+    T = o.distribute(rng.uniform(0.0, 1.0, o.n_dofs))
+    To = rng.uniform(0.0, 1.0, o.n_dofs)
+    q = o.gaussian_source(50.0, (0.5, 0.5, 0.9), 0.2)
+    ref = o.create_rhs(T, To, q)
+    got = mesh.create_rhs(T, To, q, dt=dt, k0=1.0, k1=0.5)
+    assert _rel(got, ref) < 1e-12
+    Ta, Toa = T.copy(), T.copy()
+    Tb, Tob = T.copy(), T.copy()
+    for _ in range(2):
+        rc, _ = o.time_step_newton(Ta, Toa, dt, dt, q, res_tol=1e-9, corr_tol=1e-10,
+                                   solver="cg")
+        assert rc == 0
+        mesh.time_step_newton(Tb, Tob, dt, dt, q, k0=1.0, k1=0.5)
+    assert _rel(Tb, Ta) < 1e-9
+    assert _rel(Tob, Toa) < 1e-9
+
+
+def test_newton_step_with_hanging_nodes_converges_to_the_residual_tolerance():
+    mesh = A.TwoLevelBoxMesh(2, (3, 3, 3), refine=[(1, 1, 1), (2, 1, 1), (1, 2, 2)])
+    x = mesh.support_points()
+    q = 50.0 * np.exp(-((x - np.array([0.5, 0.5, 0.6])) ** 2).sum(axis=1) / 0.2 ** 2)
+    T = np.where(mesh.mask, 0.0, 0.5 * _u(x))
+    To = T.copy()
+    its = mesh.time_step_newton(T, To, 1e-2, 1e-2, q, k0=1.0, k1=0.5)
+    assert 1 < its <= 5
+    r = mesh.create_rhs(T, To, q, dt=1e-2, k0=1.0, k1=0.5)
+    assert np.linalg.norm(r) < 1e-9

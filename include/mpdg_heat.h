@@ -388,6 +388,41 @@ int mpdg_heat_set_timing(mpdg_heat *h, int enable);
 /* Read (synchronises the stream) and optionally reset the counters. */
 int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset);
 
+/* ---- meshes with hanging nodes (adaptive refinement) ---------------------------------
+ * A box of coarse cells in which the cells flagged in `refine` (mz*my*mx bytes, x fastest,
+ * nonzero = refined) are split once into 8 children: the mesh refine_grid produces with one
+ * level of refinement difference (source/utilities/amr.cpp:18-41). A node of a refined cell
+ * on a face or an edge of an unrefined neighbour that is not one of the neighbour's nodes
+ * hangs: it is constrained to the neighbour's interpolant (DoFTools::
+ * make_hanging_node_constraints merged into the Dirichlet constraints,
+ * include/meltpooldg/utilities/constraints.hpp:111-132). The DoFs are the other nodes,
+ * numbered by position (z, then y, then x). Affine boxes only (perturb = 0), degree 1..4.
+ * device < 0 builds the host description only (no CUDA call; vmult then fails). */
+typedef struct mpdg_amr mpdg_amr;
+int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine, int device,
+                    mpdg_amr **out);
+int mpdg_amr_destroy(mpdg_amr *h);
+int64_t mpdg_amr_n_dofs(const mpdg_amr *h);
+int64_t mpdg_amr_n_cells(const mpdg_amr *h);
+/* Host arrays: support points (n_dofs x 3), Dirichlet mask (n_dofs bytes). */
+int mpdg_amr_support_points(const mpdg_amr *h, double *xyz);
+int mpdg_amr_constraint_mask(const mpdg_amr *h, uint8_t *mask);
+/* Host arrays per active cell (coarse cells in z, y, x order, a refined one as its 8 children
+ * in the same order): the (p+1)^3 gathered DoF indices, where the nodes of a hanging face or
+ * edge name the unrefined neighbour's face or edge DoFs of the same local indices, and the
+ * hanging code: bits 0-2 the child position in the parent, bit 3+d a hanging face normal to
+ * direction d, bit 6+d a hanging edge parallel to d whose faces do not hang (bits 0-8 zero
+ * without hanging nodes), bit 9 a refined cell. */
+int mpdg_amr_cell_data(const mpdg_amr *h, int64_t *dofs, uint16_t *codes);
+/* Constant or LINEAR_K material and the time increment (mpdg_heat_set_material,
+ * mpdg_heat_reset_time_increment). */
+int mpdg_amr_set_material(mpdg_amr *h, const mpdg_material *m, double dt);
+/* dst = J src (HeatDiffuseMultiPhaseOperator::vmult, heat_diffuse_operator.cpp:179-197) on
+ * device vectors of n_dofs: Dirichlet DoFs read as zero, their rows zero; the hanging nodes
+ * interpolated inside each refined cell from its gathered coarse DoFs and the transpose
+ * applied in the scatter. T_lin: the linearisation point for LINEAR_K (NULL otherwise). */
+int mpdg_amr_vmult(mpdg_amr *h, double *dst, const double *src, const double *T_lin);
+
 /* Last error message of this thread (static storage). */
 const char *mpdg_last_error(void);
 

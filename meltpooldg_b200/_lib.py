@@ -141,6 +141,15 @@ _SIGS = {
     "mpdg_heat_time_step_resident": (C.c_int, [_H, C.POINTER(StepParams), C.c_double,
                                                C.c_double, _P, _P, C.POINTER(StepStats)]),
     "mpdg_heat_set_timing": (C.c_int, [_H, C.c_int]),
+    "mpdg_amr_create": (C.c_int, [C.POINTER(MeshDesc), _P, C.c_int, C.POINTER(_H)]),
+    "mpdg_amr_destroy": (C.c_int, [_H]),
+    "mpdg_amr_n_dofs": (C.c_int64, [_H]),
+    "mpdg_amr_n_cells": (C.c_int64, [_H]),
+    "mpdg_amr_support_points": (C.c_int, [_H, _P]),
+    "mpdg_amr_constraint_mask": (C.c_int, [_H, _P]),
+    "mpdg_amr_cell_data": (C.c_int, [_H, _P, _P]),
+    "mpdg_amr_set_material": (C.c_int, [_H, C.POINTER(Material), C.c_double]),
+    "mpdg_amr_vmult": (C.c_int, [_H, _D, _D, _D]),
     "mpdg_heat_get_counters": (C.c_int, [_H, C.POINTER(Counters), C.c_int]),
     "mpdg_unet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_H)]),
     "mpdg_unet_destroy": (C.c_int, [_H]),

@@ -1,0 +1,566 @@
+// Heat operator on a box mesh with one level of refinement and hanging-node constraints.
+//
+// The mesh: a box of coarse cells, some split once into 8 children (the meshes
+// refine_grid in source/utilities/amr.cpp:18-41 produces with one level of difference).
+// A node of a refined cell that lies on a face or an edge of an unrefined neighbour and is
+// not one of its nodes hangs; its value is the neighbour's FE_Q(p) interpolant there, the
+// rule of DoFTools::make_hanging_node_constraints that MeltPoolDG merges into its Dirichlet
+// constraints (include/meltpooldg/utilities/constraints.hpp:111-132).
+//
+// The cell kernel applies the constraints inside the cell, from a per-cell code: a refined
+// cell with a hanging face or edge gathers the unrefined neighbour's face or edge DoFs at the
+// same local indices and interpolates them in place with the 1D child matrices
+// I_s[j][a] = l_a((s + xi_j)/2), one direction at a time (lines along d on a hanging face
+// normal to another direction, or on a hanging edge parallel to d); the scatter applies the
+// transposes in the reverse order. One CTA of (p+1)^3 threads per cell, every sweep through
+// shared memory: the first GPU form of this path, written for parity.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mpdg_heat.h"
+#include "fe_tables.hpp"
+
+int mpdg_internal_fail(int code, const char *msg);
+
+namespace {
+
+constexpr int kAmrMaxN = 5;  // degree <= 4
+constexpr uint16_t kFineBit = 1u << 9;
+
+struct AmrArgs {
+  const int *idx;
+  const uint16_t *code;
+  const uint8_t *mask;
+  const double *src;
+  const double *Tl;
+  double *dst;
+  int64_t n_cells;
+  double h[3];
+  double cval, k0, k1;
+  int tangent;
+  double S[kAmrMaxN * kAmrMaxN];   // S[q][i] = l_i(x_q) at the Gauss points
+  double Sd[kAmrMaxN * kAmrMaxN];  // Sd[q][i] = l_i'(x_q)
+  double I[2][kAmrMaxN * kAmrMaxN];  // child interpolation I_s[j][a] = l_a((s + xi_j)/2)
+  double w[kAmrMaxN];
+};
+
+int fail(int code, const std::string &msg) { return mpdg_internal_fail(code, msg.c_str()); }
+
+// out[t] = sum_a M[o][a] in[line(a)], o = t's index along dir (M row-major n x n);
+// transpose: sum_a M[a][o] in[line(a)]
+template <int n>
+__device__ __forceinline__ double line_sum(const double *M, const double *in, int t, int dir,
+                                           bool transpose)
+{
+  const int st = dir == 0 ? 1 : (dir == 1 ? n : n * n);
+  const int o = (t / st) % n;
+  const int base = t - o * st;
+  double v = 0.0;
+#pragma unroll
+  for (int a = 0; a < n; ++a) v += (transpose ? M[a * n + o] : M[o * n + a]) * in[base + a * st];
+  return v;
+}
+
+// in-place hanging interpolation of u along direction d (or its transpose)
+template <int n>
+__device__ __forceinline__ void hang_dir(double *u, double *tmp, int code, int d, const double *I,
+                                         bool transpose, int t)
+{
+  const int ix[3] = {t % n, (t / n) % n, t / (n * n)};
+  const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+  const int own1 = ((code >> d1) & 1) ? n - 1 : 0, own2 = ((code >> d2) & 1) ? n - 1 : 0;
+  const bool f = (((code >> (3 + d1)) & 1) && ix[d1] == own1) ||
+                 (((code >> (3 + d2)) & 1) && ix[d2] == own2) ||
+                 (((code >> (6 + d)) & 1) && ix[d1] == own1 && ix[d2] == own2);
+  tmp[t] = f ? line_sum<n>(I, u, t, d, transpose) : u[t];
+  __syncthreads();
+  u[t] = tmp[t];
+  __syncthreads();
+}
+
+// values and reference gradients at the Gauss points of the nodal values u
+template <int n>
+__device__ __forceinline__ void evaluate(const AmrArgs &a, const double *u, double *val,
+                                         double *gx, double *gy, double *gz, double *t1,
+                                         double *t2, double *s1, double *s2, double *s3, int t)
+{
+  t1[t] = line_sum<n>(a.S, u, t, 0, false);
+  t2[t] = line_sum<n>(a.Sd, u, t, 0, false);
+  __syncthreads();
+  s1[t] = line_sum<n>(a.S, t1, t, 1, false);
+  s2[t] = line_sum<n>(a.Sd, t1, t, 1, false);
+  s3[t] = line_sum<n>(a.S, t2, t, 1, false);
+  __syncthreads();
+  val[t] = line_sum<n>(a.S, s1, t, 2, false);
+  gz[t] = line_sum<n>(a.Sd, s1, t, 2, false);
+  gy[t] = line_sum<n>(a.S, s2, t, 2, false);
+  gx[t] = line_sum<n>(a.S, s3, t, 2, false);
+  __syncthreads();
+}
+
+template <int n>
+__global__ void k_amr_vmult(const AmrArgs a)
+{
+  constexpr int n3 = n * n * n;
+  __shared__ double u[n3], T[n3], tmp[n3], t1[n3], t2[n3], s1[n3], s2[n3], s3[n3];
+  __shared__ double val[n3], gx[n3], gy[n3], gz[n3], Tv[n3], Tx[n3], Ty[n3], Tz[n3];
+  const int t = threadIdx.x;
+  for (int64_t c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
+    const int code = a.code[c];
+    const int dof = a.idx[c * n3 + t];
+    const bool hang = (code & 0x1F8) != 0;
+    const double size = (code & kFineBit) ? 0.5 : 1.0;
+    u[t] = a.mask[dof] ? 0.0 : a.src[dof];
+    if (a.tangent) T[t] = a.Tl[dof];
+    __syncthreads();
+    if (hang) {
+      for (int d = 0; d < 3; ++d) {
+        const double *I = a.I[(code >> d) & 1];
+        hang_dir<n>(u, tmp, code, d, I, false, t);
+        if (a.tangent) hang_dir<n>(T, tmp, code, d, I, false, t);
+      }
+    }
+    if (a.tangent) evaluate<n>(a, T, Tv, Tx, Ty, Tz, t1, t2, s1, s2, s3, t);
+    evaluate<n>(a, u, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
+    // quadrature point t: rho_cp/dt u and the flux k grad(u) (+ k1 grad(T_lin) u)
+    {
+      const int qx = t % n, qy = (t / n) % n, qz = t / (n * n);
+      const double hx = a.h[0] * size, hy = a.h[1] * size, hz = a.h[2] * size;
+      const double jxw = a.w[qx] * a.w[qy] * a.w[qz] * hx * hy * hz;
+      const double k = a.tangent ? a.k0 + a.k1 * Tv[t] : a.k0;
+      double fx = k * gx[t] / hx, fy = k * gy[t] / hy, fz = k * gz[t] / hz;
+      if (a.tangent) {
+        fx += a.k1 * Tx[t] / hx * val[t];
+        fy += a.k1 * Ty[t] / hy * val[t];
+        fz += a.k1 * Tz[t] / hz * val[t];
+      }
+      val[t] = a.cval * val[t] * jxw;
+      gx[t] = fx * jxw / hx;
+      gy[t] = fy * jxw / hy;
+      gz[t] = fz * jxw / hz;
+    }
+    __syncthreads();
+    // integration: S^T / Sd^T along z, then y, then x
+    s1[t] = line_sum<n>(a.S, val, t, 2, true) + line_sum<n>(a.Sd, gz, t, 2, true);
+    s2[t] = line_sum<n>(a.S, gx, t, 2, true);
+    s3[t] = line_sum<n>(a.S, gy, t, 2, true);
+    __syncthreads();
+    t1[t] = line_sum<n>(a.S, s1, t, 1, true) + line_sum<n>(a.Sd, s3, t, 1, true);
+    t2[t] = line_sum<n>(a.S, s2, t, 1, true);
+    __syncthreads();
+    u[t] = line_sum<n>(a.S, t1, t, 0, true) + line_sum<n>(a.Sd, t2, t, 0, true);
+    __syncthreads();
+    if (hang) {
+      for (int d = 2; d >= 0; --d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], true, t);
+    }
+    if (!a.mask[dof]) atomicAdd(a.dst + dof, u[t]);
+    __syncthreads();
+  }
+}
+
+__global__ void k_amr_zero(int64_t n, double *p)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = 0.0;
+}
+
+}  // namespace
+
+struct mpdg_amr {
+  int p = 1, n = 2, device = -1;
+  int m[3] = {0, 0, 0};
+  double lo[3] = {0, 0, 0}, h[3] = {0, 0, 0};
+  int64_t n_cells = 0, n_dofs = 0;
+  std::vector<int64_t> cell_dofs;  // n_cells x n^3
+  std::vector<uint16_t> codes;
+  std::vector<double> dof_pos;     // n_dofs x 3, physical
+  std::vector<uint8_t> mask;
+  mpdg_material mat{};
+  double dt = 0.0;
+  bool mat_set = false;
+  int *d_idx = nullptr;
+  uint16_t *d_code = nullptr;
+  uint8_t *d_mask = nullptr;
+};
+
+namespace {
+
+using Key = std::array<int64_t, 3>;
+
+Key key_of(const double *x)
+{
+  return {std::llround(x[0] * 67108864.0), std::llround(x[1] * 67108864.0),
+          std::llround(x[2] * 67108864.0)};
+}
+
+void release(mpdg_amr *h)
+{
+  if (h->d_idx) cudaFree(h->d_idx);
+  if (h->d_code) cudaFree(h->d_code);
+  if (h->d_mask) cudaFree(h->d_mask);
+  h->d_idx = nullptr;
+  h->d_code = nullptr;
+  h->d_mask = nullptr;
+}
+
+// the host description: active cells, node numbering, hanging nodes, DoFs, cell data
+int build_host(mpdg_amr *h, const mpdg_mesh_desc *desc, const uint8_t *refine)
+{
+  const int p = h->p, n = h->n, n3 = n * n * n;
+  const int mx = h->m[0], my = h->m[1], mz = h->m[2];
+  auto refined = [&](int ix, int iy, int iz) {
+    return refine[(size_t)ix + (size_t)mx * (iy + (size_t)my * iz)] != 0;
+  };
+  auto unrefined_at = [&](int ix, int iy, int iz) {
+    return ix >= 0 && iy >= 0 && iz >= 0 && ix < mx && iy < my && iz < mz && !refined(ix, iy, iz);
+  };
+  mpdg::Tables1D tb = mpdg::make_tables(n);
+  const double *xi = tb.xl;
+  // active cells
+  struct Cell {
+    double o[3];
+    double size;
+    int par[3];
+    int s[3];
+  };
+  std::vector<Cell> cells;
+  std::vector<int64_t> coarse_id((size_t)mx * my * mz, -1);
+  for (int iz = 0; iz < mz; ++iz)
+    for (int iy = 0; iy < my; ++iy)
+      for (int ix = 0; ix < mx; ++ix) {
+        if (refined(ix, iy, iz)) {
+          for (int sz = 0; sz < 2; ++sz)
+            for (int sy = 0; sy < 2; ++sy)
+              for (int sx = 0; sx < 2; ++sx)
+                cells.push_back({{ix + 0.5 * sx, iy + 0.5 * sy, iz + 0.5 * sz}, 0.5,
+                                 {ix, iy, iz}, {sx, sy, sz}});
+        } else {
+          coarse_id[(size_t)ix + (size_t)mx * (iy + (size_t)my * iz)] = (int64_t)cells.size();
+          cells.push_back({{(double)ix, (double)iy, (double)iz}, 1.0, {ix, iy, iz}, {0, 0, 0}});
+        }
+      }
+  const int64_t nc = (int64_t)cells.size();
+  // nodes by position key (coarse-cell units)
+  std::vector<std::pair<Key, int64_t>> ent((size_t)nc * n3);
+  std::vector<double> pos((size_t)nc * n3 * 3);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+          const int64_t e = c * n3 + i + n * (j + n * k);
+          double *x = &pos[(size_t)e * 3];
+          x[0] = cells[c].o[0] + cells[c].size * xi[i];
+          x[1] = cells[c].o[1] + cells[c].size * xi[j];
+          x[2] = cells[c].o[2] + cells[c].size * xi[k];
+          ent[(size_t)e] = {key_of(x), e};
+        }
+  std::sort(ent.begin(), ent.end());
+  std::vector<int64_t> node_of((size_t)nc * n3);
+  std::vector<int64_t> first;  // one entry per node: its first occurrence
+  std::vector<Key> node_key;
+  for (size_t a = 0; a < ent.size(); ++a) {
+    if (a == 0 || ent[a].first != ent[a - 1].first) {
+      first.push_back(ent[a].second);
+      node_key.push_back(ent[a].first);
+    }
+    node_of[(size_t)ent[a].second] = (int64_t)first.size() - 1;
+  }
+  const int64_t n_nodes = (int64_t)first.size();
+  // hanging nodes: nodes of refined cells on the closed box of an unrefined coarse cell
+  // that are not nodes of an unrefined cell
+  std::vector<uint8_t> coarse_node((size_t)n_nodes, 0), fine_node((size_t)n_nodes, 0);
+  for (int64_t c = 0; c < nc; ++c)
+    for (int l = 0; l < n3; ++l)
+      (cells[c].size == 1.0 ? coarse_node : fine_node)[(size_t)node_of[c * n3 + l]] = 1;
+  std::vector<uint8_t> hanging((size_t)n_nodes, 0);
+  const double tol = 1e-9;
+  for (int64_t v = 0; v < n_nodes; ++v) {
+    if (!fine_node[v] || coarse_node[v]) continue;
+    const double *x = &pos[(size_t)first[v] * 3];
+    const int bx = (int)std::floor(x[0] + tol), by = (int)std::floor(x[1] + tol),
+              bz = (int)std::floor(x[2] + tol);
+    bool found = false;
+    for (int dz = 0; dz >= -1 && !found; --dz)
+      for (int dy = 0; dy >= -1 && !found; --dy)
+        for (int dx = 0; dx >= -1 && !found; --dx) {
+          const int cx = bx + dx, cy = by + dy, cz = bz + dz;
+          if (!unrefined_at(cx, cy, cz)) continue;
+          if (x[0] >= cx - tol && x[0] <= cx + 1 + tol && x[1] >= cy - tol &&
+              x[1] <= cy + 1 + tol && x[2] >= cz - tol && x[2] <= cz + 1 + tol)
+            found = true;
+        }
+    hanging[v] = found;
+  }
+  // DoFs: the regular nodes ordered by (z, y, x)
+  std::vector<int64_t> regular;
+  for (int64_t v = 0; v < n_nodes; ++v)
+    if (!hanging[v]) regular.push_back(v);
+  std::sort(regular.begin(), regular.end(), [&](int64_t a, int64_t b) {
+    const Key &ka = node_key[a], &kb = node_key[b];
+    if (ka[2] != kb[2]) return ka[2] < kb[2];
+    if (ka[1] != kb[1]) return ka[1] < kb[1];
+    return ka[0] < kb[0];
+  });
+  std::vector<int64_t> dof_of((size_t)n_nodes, -1);
+  for (size_t r = 0; r < regular.size(); ++r) dof_of[(size_t)regular[r]] = (int64_t)r;
+  h->n_dofs = (int64_t)regular.size();
+  h->n_cells = nc;
+  h->dof_pos.resize((size_t)h->n_dofs * 3);
+  h->mask.assign((size_t)h->n_dofs, 0);
+  const int mm[3] = {mx, my, mz};
+  for (int64_t r = 0; r < h->n_dofs; ++r) {
+    const double *x = &pos[(size_t)first[(size_t)regular[r]] * 3];
+    for (int d = 0; d < 3; ++d) {
+      h->dof_pos[(size_t)r * 3 + d] = h->lo[d] + x[d] * h->h[d];
+      if (((desc->dirichlet_mask >> (2 * d)) & 1) && std::fabs(x[d]) < tol) h->mask[r] = 1;
+      if (((desc->dirichlet_mask >> (2 * d + 1)) & 1) && std::fabs(x[d] - mm[d]) < tol)
+        h->mask[r] = 1;
+    }
+  }
+  // per cell: gathered DoFs and the hanging code
+  h->cell_dofs.assign((size_t)nc * n3, -1);
+  h->codes.assign((size_t)nc, 0);
+  auto lin = [n](int i, int j, int k) { return i + n * (j + n * k); };
+  for (int64_t c = 0; c < nc; ++c) {
+    const Cell &cl = cells[c];
+    int64_t *idx = &h->cell_dofs[(size_t)c * n3];
+    for (int l = 0; l < n3; ++l) idx[l] = dof_of[(size_t)node_of[c * n3 + l]];
+    if (cl.size == 1.0) continue;
+    int code = kFineBit;
+    int step[3], own[3], other[3];
+    for (int d = 0; d < 3; ++d) {
+      step[d] = cl.s[d] ? 1 : -1;
+      own[d] = cl.s[d] ? n - 1 : 0;
+      other[d] = n - 1 - own[d];
+    }
+    bool face[3], edge[3];
+    for (int d = 0; d < 3; ++d) {
+      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
+      q[d] += step[d];
+      face[d] = unrefined_at(q[0], q[1], q[2]);
+    }
+    for (int d = 0; d < 3; ++d) {
+      const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
+      q[d1] += step[d1];
+      q[d2] += step[d2];
+      edge[d] = unrefined_at(q[0], q[1], q[2]) && !face[d1] && !face[d2];
+    }
+    int hb = 0;
+    for (int d = 0; d < 3; ++d) hb |= (face[d] ? 1 << (3 + d) : 0) | (edge[d] ? 1 << (6 + d) : 0);
+    if (hb) code |= hb | cl.s[0] | (cl.s[1] << 1) | (cl.s[2] << 2);
+    h->codes[(size_t)c] = (uint16_t)code;
+    // gather the neighbour's face / edge DoFs at the same local indices
+    for (int d = 0; d < 3; ++d) {
+      if (!face[d]) continue;
+      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
+      q[d] += step[d];
+      const int64_t nb = coarse_id[(size_t)q[0] + (size_t)mx * (q[1] + (size_t)my * q[2])];
+      const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+      for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b) {
+          int i[3], jn[3];
+          i[d] = own[d];
+          i[d1] = a;
+          i[d2] = b;
+          jn[d] = other[d];
+          jn[d1] = a;
+          jn[d2] = b;
+          idx[lin(i[0], i[1], i[2])] = dof_of[(size_t)node_of[nb * n3 + lin(jn[0], jn[1], jn[2])]];
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+      if (!edge[d]) continue;
+      const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
+      q[d1] += step[d1];
+      q[d2] += step[d2];
+      const int64_t nb = coarse_id[(size_t)q[0] + (size_t)mx * (q[1] + (size_t)my * q[2])];
+      for (int a = 0; a < n; ++a) {
+        int i[3], jn[3];
+        i[d] = a;
+        i[d1] = own[d1];
+        i[d2] = own[d2];
+        jn[d] = a;
+        jn[d1] = other[d1];
+        jn[d2] = other[d2];
+        idx[lin(i[0], i[1], i[2])] = dof_of[(size_t)node_of[nb * n3 + lin(jn[0], jn[1], jn[2])]];
+      }
+    }
+  }
+  for (int64_t v : h->cell_dofs)
+    if (v < 0 || v >= h->n_dofs)
+      return fail(MPDG_ERR_INVALID_ARGUMENT, "hanging node left ungathered (unsupported mesh)");
+  (void)p;
+  return MPDG_OK;
+}
+
+}  // namespace
+
+extern "C" int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine, int device,
+                               mpdg_amr **out)
+{
+  if (!desc || !refine || !out) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (desc->degree < 1 || desc->degree > kAmrMaxN - 1)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "hanging-node meshes: degree 1..4");
+  if (desc->perturb != 0.0)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "hanging-node meshes: affine boxes only");
+  for (int d = 0; d < 3; ++d)
+    if (desc->cells[d] < 1 || !(desc->hi[d] > desc->lo[d]))
+      return fail(MPDG_ERR_INVALID_ARGUMENT, "invalid box");
+  if ((int64_t)desc->cells[0] * desc->cells[1] * desc->cells[2] * 8 *
+          (int64_t)std::pow(desc->degree + 1, 3) > (int64_t)1 << 30)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "hanging-node mesh too large for 32-bit cell data");
+  mpdg_amr *h = new mpdg_amr();
+  h->p = desc->degree;
+  h->n = desc->degree + 1;
+  h->device = device;
+  for (int d = 0; d < 3; ++d) {
+    h->m[d] = desc->cells[d];
+    h->lo[d] = desc->lo[d];
+    h->h[d] = (desc->hi[d] - desc->lo[d]) / desc->cells[d];
+  }
+  int rc = build_host(h, desc, refine);
+  if (rc != MPDG_OK) {
+    delete h;
+    return rc;
+  }
+  if (device >= 0) {
+    const int n3 = h->n * h->n * h->n;
+    std::vector<int> idx32(h->cell_dofs.begin(), h->cell_dofs.end());
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_idx, sizeof(int) * idx32.size());
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_code, sizeof(uint16_t) * h->codes.size());
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_mask, h->mask.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->d_idx, idx32.data(), sizeof(int) * idx32.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->d_code, h->codes.data(), sizeof(uint16_t) * h->codes.size(),
+                     cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->d_mask, h->mask.data(), h->mask.size(), cudaMemcpyHostToDevice);
+    (void)n3;
+    if (e != cudaSuccess) {
+      release(h);
+      delete h;
+      return fail(e == cudaErrorMemoryAllocation ? MPDG_ERR_OUT_OF_MEMORY : MPDG_ERR_CUDA,
+                  std::string("hanging-node mesh: ") + cudaGetErrorString(e));
+    }
+  }
+  *out = h;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_amr_destroy(mpdg_amr *h)
+{
+  if (!h) return MPDG_OK;
+  if (h->device >= 0) {
+    cudaSetDevice(h->device);
+    release(h);
+  }
+  delete h;
+  return MPDG_OK;
+}
+
+extern "C" int64_t mpdg_amr_n_dofs(const mpdg_amr *h) { return h ? h->n_dofs : -1; }
+extern "C" int64_t mpdg_amr_n_cells(const mpdg_amr *h) { return h ? h->n_cells : -1; }
+
+extern "C" int mpdg_amr_support_points(const mpdg_amr *h, double *xyz)
+{
+  if (!h || !xyz) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  std::memcpy(xyz, h->dof_pos.data(), sizeof(double) * h->dof_pos.size());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_amr_constraint_mask(const mpdg_amr *h, uint8_t *mask)
+{
+  if (!h || !mask) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  std::memcpy(mask, h->mask.data(), h->mask.size());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_amr_cell_data(const mpdg_amr *h, int64_t *dofs, uint16_t *codes)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  if (dofs) std::memcpy(dofs, h->cell_dofs.data(), sizeof(int64_t) * h->cell_dofs.size());
+  if (codes) std::memcpy(codes, h->codes.data(), sizeof(uint16_t) * h->codes.size());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_amr_set_material(mpdg_amr *h, const mpdg_material *m, double dt)
+{
+  if (!h || !m) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (m->law != MPDG_LAW_CONSTANT && m->law != MPDG_LAW_LINEAR_K)
+    return fail(MPDG_ERR_NOT_SUPPORTED, "hanging-node meshes: constant or LINEAR_K law");
+  if (dt == 0.0) return fail(MPDG_ERR_ZERO_TIME_INCREMENT, "time increment is zero");
+  h->mat = *m;
+  h->dt = dt;
+  h->mat_set = true;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_amr_vmult(mpdg_amr *h, double *dst, const double *src, const double *T_lin)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (h->device < 0) return fail(MPDG_ERR_INVALID_ARGUMENT, "host-only hanging-node mesh");
+  if (!h->mat_set) return fail(MPDG_ERR_INVALID_ARGUMENT, "call mpdg_amr_set_material first");
+  const bool tangent = h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0;
+  if (tangent && !T_lin)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "LINEAR_K needs the linearisation point");
+  for (const void *ptr : {(const void *)dst, (const void *)src, (const void *)T_lin}) {
+    if (!ptr) continue;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || at.type != cudaMemoryTypeDevice)
+      return fail(MPDG_ERR_INVALID_ARGUMENT, "vectors must be device memory");
+  }
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+  AmrArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.idx = h->d_idx;
+  a.code = h->d_code;
+  a.mask = h->d_mask;
+  a.src = src;
+  a.Tl = tangent ? T_lin : src;
+  a.dst = dst;
+  a.n_cells = h->n_cells;
+  for (int d = 0; d < 3; ++d) a.h[d] = h->h[d];
+  a.cval = h->mat.rho_l * h->mat.cp_l / h->dt;
+  a.k0 = h->mat.k_l;
+  a.k1 = tangent ? h->mat.k1 : 0.0;
+  a.tangent = tangent;
+  const int n = h->n;
+  mpdg::Tables1D tb = mpdg::make_tables(n);
+  for (int q = 0; q < n; ++q) {
+    a.w[q] = tb.wg[q];
+    for (int i = 0; i < n; ++i) {
+      a.S[q * n + i] = mpdg::lagrange(tb.xl, n, i, tb.xg[q]);
+      a.Sd[q * n + i] = mpdg::lagrange_d(tb.xl, n, i, tb.xg[q]);
+    }
+  }
+  for (int s = 0; s < 2; ++s)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) a.I[s][j * n + i] = mpdg::lagrange(tb.xl, n, i, 0.5 * (s + tb.xl[j]));
+  k_amr_zero<<<256, 256>>>(h->n_dofs, dst);
+  const int grid = (int)std::min<int64_t>(h->n_cells, 148 * 16);
+  switch (n) {
+    case 2: k_amr_vmult<2><<<grid, 8>>>(a); break;
+    case 3: k_amr_vmult<3><<<grid, 27>>>(a); break;
+    case 4: k_amr_vmult<4><<<grid, 64>>>(a); break;
+    case 5: k_amr_vmult<5><<<grid, 125>>>(a); break;
+    default: return fail(MPDG_ERR_INVALID_ARGUMENT, "degree");
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+  return MPDG_OK;
+}

@@ -54,6 +54,9 @@ static int fail(int code, const std::string &msg)
 
 extern "C" const char *mpdg_last_error(void) { return g_err.c_str(); }
 
+// the library's other translation units report errors through the same thread-local message
+int mpdg_internal_fail(int code, const char *msg) { return fail(code, msg); }
+
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------

@@ -460,3 +460,53 @@ class TwoLevelBoxMesh:
                 return it + 1
             T_cur += delta
         raise RuntimeError("Newton-Raphson did not converge")
+
+    # ------------------------------------------------------------------------------------
+    # the inverse diagonal and the residual in the cell-wise form (what the GPU path needs
+    # next: a refined cell on an interface has no closed-form diagonal, F^T A F is applied to
+    # its unit vectors instead)
+    def inverse_diagonal(self, **coef) -> np.ndarray:
+        """1/diag(C^T A C) with the reference's rule |d| > 1e-10 ? 1/d : 1
+        (heat_diffuse_operator.cpp:282-283); Dirichlet DoFs 1."""
+        d = self.assemble(**coef).diagonal().copy()
+        d[self.mask] = 0.0
+        return np.where(np.abs(d) > 1e-10, 1.0 / np.where(d == 0.0, 1.0, d), 1.0)
+
+    def inverse_diagonal_cellwise(self, rho_cp=1.0, dt=1.0, k0=1.0, k1=0.0, T_lin=None):
+        """The same diagonal accumulated cell by cell: diag(F^T A_e F) at the gathered DoFs
+        (the gathered DoFs of a cell are distinct, so the local diagonal is the contribution)."""
+        d = np.zeros(self.n_dofs)
+        for c in range(self.n_cells):
+            idx, F = self.cell_map(c)
+            te = None
+            if T_lin is not None and k1 != 0.0:
+                te = T_lin[idx] if F is None else F @ T_lin[idx]
+            A = self._element_matrix(c, rho_cp, dt, k0, k1, te)
+            loc = np.diag(A) if F is None else np.einsum("il,ij,jl->l", F, A, F)
+            np.add.at(d, idx, loc)
+        d[self.mask] = 0.0
+        return np.where(np.abs(d) > 1e-10, 1.0 / np.where(d == 0.0, 1.0, d), 1.0)
+
+    def create_rhs_cellwise(self, T, T_old, heat_source=None, dst=None, rho_cp=1.0, dt=1.0,
+                            k0=1.0, k1=0.0) -> np.ndarray:
+        """create_rhs with the constraints applied per cell: T, T_old and the source gathered
+        and interpolated by F, the residual integrated, F^T in the scatter."""
+        dst = np.zeros(self.n_dofs) if dst is None else dst
+        N = self._N
+        y = np.zeros(self.n_dofs)
+        for c in range(self.n_cells):
+            idx, F = self.cell_map(c)
+            loc = (lambda v: v[idx]) if F is None else (lambda v: F @ v[idx])
+            te, to = loc(T), loc(T_old)
+            jxw, G = self._cell_factors(c)
+            Tq = N @ te
+            val = rho_cp / dt * (Tq - N @ to)
+            if heat_source is not None:
+                val = val - N @ loc(heat_source)
+            kq = k0 + k1 * Tq
+            r = N.T @ (jxw * val)
+            for d in range(3):
+                r += G[d].T @ (jxw * kq * (G[d] @ te))
+            np.add.at(y, idx, -(r if F is None else F.T @ r))
+        dst[~self.mask] += y[~self.mask]
+        return dst

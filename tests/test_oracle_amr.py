@@ -182,3 +182,25 @@ def test_newton_step_with_hanging_nodes_converges_to_the_residual_tolerance():
     assert 1 < its <= 5
     r = mesh.create_rhs(T, To, q, dt=1e-2, k0=1.0, k1=0.5)
     assert np.linalg.norm(r) < 1e-9
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_cellwise_diagonal_and_residual_match_the_condensed_forms(p):
+    """The inverse diagonal (the reference's |d| > 1e-10 rule) and create_rhs accumulated cell
+    by cell with the in-cell constraints equal those of C^T A C, with hanging faces and edges."""
+    mesh = A.TwoLevelBoxMesh(p, (4, 3, 3), refine=REFINE)
+    rng = np.random.default_rng(40 + p)
+    T = rng.uniform(0.0, 1.0, mesh.n_dofs)
+    To = rng.uniform(0.0, 1.0, mesh.n_dofs)
+    q = rng.uniform(0.0, 5.0, mesh.n_dofs)
+    for coef in (dict(rho_cp=2.0, dt=0.05, k0=1.0),
+                 dict(rho_cp=1.0, dt=0.05, k0=1.0, k1=0.5, T_lin=T)):
+        a = mesh.inverse_diagonal(**coef)
+        b = mesh.inverse_diagonal_cellwise(**coef)
+        assert _rel(b, a) < 1e-13
+        assert np.all(a[mesh.mask] == 1.0)
+    kw = dict(rho_cp=2.0, dt=0.05, k0=1.0, k1=0.5)
+    a = mesh.create_rhs(T, To, q, **kw)
+    b = mesh.create_rhs_cellwise(T, To, q, **kw)
+    assert _rel(b, a) < 1e-13
+    assert np.all(b[mesh.mask] == 0.0)

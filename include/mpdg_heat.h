@@ -420,7 +420,8 @@ int mpdg_amr_set_material(mpdg_amr *h, const mpdg_material *m, double dt);
 /* dst = J src (HeatDiffuseMultiPhaseOperator::vmult, heat_diffuse_operator.cpp:179-197) on
  * device vectors of n_dofs: Dirichlet DoFs read as zero, their rows zero; the hanging nodes
  * interpolated inside each refined cell from its gathered coarse DoFs and the transpose
- * applied in the scatter. T_lin: the linearisation point for LINEAR_K (NULL otherwise). */
+ * applied in the scatter. T_lin: the linearisation point for LINEAR_K (NULL otherwise).
+ * Runs on the legacy default stream and returns once the result is complete. */
 int mpdg_amr_vmult(mpdg_amr *h, double *dst, const double *src, const double *T_lin);
 
 /* Last error message of this thread (static storage). */

@@ -472,6 +472,9 @@ void orc_distribute(const orc_heat *h, double *u)
 int orc_set_material(orc_heat *h, const orc_material *m, double dt)
 {
   if (h->vel && m->law == ORC_LAW_LINEAR_K) return -1;
+  /* the reference throws for an apparent capacity with volume-specific rho*cp
+   * (material.templates.hpp:321-328) */
+  if (m->latent_heat > 0.0 && m->volume_specific) return -2;
   h->mat = *m;
   h->dt = dt;
   h->tdep = m->law == ORC_LAW_LINEAR_K || m->law == ORC_LAW_LIQUID_SOLID ||
@@ -482,7 +485,7 @@ int orc_set_material(orc_heat *h, const orc_material *m, double dt)
     if (m->volume_specific)
       h->need_told = (m->rho_l * m->cp_l != m->rho_s * m->cp_s);
     else
-      h->need_told = (m->rho_l != m->rho_s) || (m->cp_l != m->cp_s);
+      h->need_told = (m->rho_l != m->rho_s) || (m->cp_l != m->cp_s) || m->latent_heat > 0.0;
   }
   return 0;
 }
@@ -528,22 +531,71 @@ static void ref_direction(const orc_heat *h, int64_t c, int q, const double v[3]
  * fraction sf from the mushy zone (or sharp at T_solidus), cubic smoothstep
  * interpolate_cubic(sf, l, s) = l + (s - l) (3 sf^2 - 2 sf^3), derivative
  * -(s - l) 6 sf (1 - sf) / (T_liquidus - T_solidus), both exact at sf = 0 and 1 */
+static inline double solid_fraction(const orc_material *m, double T)
+{
+  if (m->sharp) return T < m->T_solidus ? 1.0 : 0.0;
+  const double inv_mushy = 1.0 / (m->T_liquidus - m->T_solidus);
+  const double sf = (m->T_liquidus - T) * inv_mushy;
+  return sf < 0.0 ? 0.0 : (sf > 1.0 ? 1.0 : sf);
+}
+
 static inline void ls_interp(const orc_material *m, double T, double l, double s, double *val,
                              double *dval)
 {
   const double inv_mushy = 1.0 / (m->T_liquidus - m->T_solidus);
-  double sf;
-  if (m->sharp)
-    sf = T < m->T_solidus ? 1.0 : 0.0;
-  else {
-    sf = (m->T_liquidus - T) * inv_mushy;
-    sf = sf < 0.0 ? 0.0 : (sf > 1.0 ? 1.0 : sf);
-  }
+  const double sf = solid_fraction(m, T);
   const double hs = -2.0 * sf * sf * sf + 3.0 * sf * sf; /* interpolate_cubic weight */
   const double dhs = -6.0 * sf * sf + 6.0 * sf;           /* its derivative */
   const int edge = (sf == 0.0 || sf == 1.0);
   *val = sf == 0.0 ? l : (sf == 1.0 ? s : l + (s - l) * hs);
   *dval = edge ? 0.0 : -1.0 * inv_mushy * ((s - l) * dhs);
+}
+
+/* ramp from (x1, y1) to (x2, y2) with zero slope at both ends: quadratic over the first and the
+ * last `delta`, linear in between with the slope s = (y2 - y1) / (x2 - x1 - delta) that makes the
+ * pieces meet with continuous slopes (qlq_zero_slope, source/heat/apparent_capacity.cpp:41-110);
+ * *dy its derivative */
+static inline double qlq_ramp(double x, double x1, double x2, double y1, double y2, double delta,
+                              double *dy)
+{
+  const double s = (y2 - y1) / (x2 - x1 - delta);
+  if (x < x1 + delta) {
+    *dy = s / delta * (x - x1);
+    return y1 + 0.5 * s / delta * (x - x1) * (x - x1);
+  }
+  if (x > x2 - delta) {
+    *dy = -s / delta * (x - x2);
+    return y2 - 0.5 * s / delta * (x - x2) * (x - x2);
+  }
+  *dy = s;
+  return y1 + s * (x - x1 - 0.5 * delta);
+}
+
+/* apparent heat capacity of the latent heat of fusion L in the mushy zone, added to the liquid-
+ * solid specific heat capacity when L > 0 (Heat::ApparentCapacity, apparent_capacity.cpp:
+ * 157-300; compute_solid_liquid_phases_specific_heat_capacity and its derivative,
+ * material.templates.hpp:562-616; material.hpp:655-656): zero unless 0 < sf < 1; with
+ * dT = T_l - T_s each profile integrates to L over [T_s, T_l]:
+ *   CONSTANT    L / dT
+ *   QLQ         qlq_ramp from (T_s, 0) to (T_mid, 2 L / dT) and back to (T_l, 0), delta = dT / 6,
+ *               at T = T_l - sf dT
+ *   POLY4_BELL  (2 L / dT) f(xi), f(x) = 15/16 (x^2 - 1)^2, xi = 1 - 2 sf
+ * *dA is the temperature derivative. */
+static inline double apparent_capacity(const orc_material *m, double sf, double *dA)
+{
+  *dA = 0.0;
+  if (!(m->latent_heat > 0.0) || sf <= 0.0 || sf >= 1.0) return 0.0;
+  const double L = m->latent_heat, dT = m->T_liquidus - m->T_solidus;
+  if (m->apparent_capacity == ORC_APPARENT_CONSTANT) return L / dT;
+  if (m->apparent_capacity == ORC_APPARENT_POLY4_BELL) {
+    const double r = 2.0 / dT, xi = 1.0 - 2.0 * sf, q = xi * xi - 1.0;
+    *dA = L * r * r * 3.75 * xi * q;
+    return L * r * 0.9375 * q * q;
+  }
+  const double T = m->T_liquidus - sf * dT, Tm = 0.5 * (m->T_solidus + m->T_liquidus);
+  const double peak = 2.0 * L / dT, delta = dT / 6.0;
+  return T <= Tm ? qlq_ramp(T, m->T_solidus, Tm, 0.0, peak, delta, dA)
+                 : qlq_ramp(T, Tm, m->T_liquidus, peak, 0.0, delta, dA);
 }
 
 /* Material::compute_parameters of the heat operator's material types at temperature T and
@@ -590,6 +642,9 @@ static inline void material_eval(const orc_material *m, double T, double H, doub
     } else {
       ls_interp(m, T, m->rho_l, m->rho_s, &rho, &drho);
       ls_interp(m, T, m->cp_l, m->cp_s, &cp, &dcp);
+      double dA;
+      cp += apparent_capacity(m, solid_fraction(m, T), &dA);
+      dcp += dA;
     }
   }
   if (law == ORC_LAW_LIQUID_SOLID) {

@@ -69,7 +69,12 @@ typedef struct {
   double k1;              /* linear law: k(T) = k_l + k1*T */
   int    sharp_gas_liquid;  /* gas-liquid transition: 0 smooth (w = H), 1 sharp (w = H > 0.5) */
   double rho_g, cp_g, k_g;  /* gas */
+  double latent_heat;       /* latent heat of fusion (> 0: apparent capacity in the mushy zone) */
+  int    apparent_capacity; /* ORC_APPARENT_* profile of that capacity */
 } orc_material;
+
+/* apparent-capacity profiles (ApparentCapacityType, material_data.hpp:43; qlq the default) */
+enum { ORC_APPARENT_QLQ = 0, ORC_APPARENT_CONSTANT = 1, ORC_APPARENT_POLY4_BELL = 2 };
 
 typedef struct orc_heat orc_heat;
 

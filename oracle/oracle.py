@@ -69,7 +69,11 @@ class Material(C.Structure):
                 ("rho_s", C.c_double), ("cp_s", C.c_double), ("k_s", C.c_double),
                 ("T_solidus", C.c_double), ("T_liquidus", C.c_double), ("k1", C.c_double),
                 ("sharp_gas_liquid", C.c_int),
-                ("rho_g", C.c_double), ("cp_g", C.c_double), ("k_g", C.c_double)]
+                ("rho_g", C.c_double), ("cp_g", C.c_double), ("k_g", C.c_double),
+                ("latent_heat", C.c_double), ("apparent_capacity", C.c_int)]
+
+
+APPARENT_QLQ, APPARENT_CONSTANT, APPARENT_POLY4_BELL = 0, 1, 2
 
 
 class SolverParams(C.Structure):
@@ -148,7 +152,8 @@ def _ptr(a):
 
 def material(law=LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_s=None, k_s=None,
              T_solidus=0.0, T_liquidus=1.0, sharp=False, volume_specific=False, rho_g=None,
-             cp_g=None, k_g=None, sharp_gas_liquid=False) -> Material:
+             cp_g=None, k_g=None, sharp_gas_liquid=False, latent_heat=0.0,
+             apparent_capacity=APPARENT_QLQ) -> Material:
     m = Material()
     m.law = law
     m.sharp = int(sharp)
@@ -162,6 +167,8 @@ def material(law=LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_s=
     m.rho_g = rho if rho_g is None else rho_g
     m.cp_g = cp if cp_g is None else cp_g
     m.k_g = k if k_g is None else k_g
+    m.latent_heat = float(latent_heat)
+    m.apparent_capacity = int(apparent_capacity)
     return m
 
 
@@ -224,8 +231,10 @@ class Oracle:
         return u
 
     def set_material(self, m: Material, dt: float):
-        if self.L.orc_set_material(self.h, C.byref(m), dt) != 0:
-            raise ValueError("velocity with the linear-k law")
+        rc = self.L.orc_set_material(self.h, C.byref(m), dt)
+        if rc != 0:
+            raise ValueError("velocity with the linear-k law" if rc == -1 else
+                             "apparent capacity with volume-specific rho*cp")
         self.dt = dt
         self._material = m
 

@@ -85,6 +85,10 @@ typedef struct {
   double rho_g, cp_g, k_g; /* gas (GAS_LIQUID, GAS_LIQUID_SOLID)                      */
 } mpdg_material;
 
+/* Apparent-capacity profiles of the latent heat of fusion (ApparentCapacityType,
+ * include/meltpooldg/core/material_data.hpp:43; qlq the reference's default). */
+enum { MPDG_APPARENT_QLQ = 0, MPDG_APPARENT_CONSTANT = 1, MPDG_APPARENT_POLY4_BELL = 2 };
+
 enum { MPDG_SOLVER_CG = 0, MPDG_SOLVER_GMRES = 1 };           /* LinearSolverType  */
 enum { MPDG_PRECOND_IDENTITY = 0, MPDG_PRECOND_JACOBI = 1,    /* PreconditionerType */
        MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 = 2,
@@ -173,6 +177,19 @@ int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m);
  * with either field.  A field that was interpolated from another finite element space is
  * passed after its interpolation to this one. */
 int mpdg_heat_set_fields(mpdg_heat *h, const double *heaviside, const double *velocity);
+/* Latent heat of fusion as an apparent heat capacity in the mushy zone: with latent_heat > 0
+ * the liquid-solid specific heat capacity (LIQUID_SOLID, GAS_LIQUID_SOLID) gains the profile's
+ * capacity and its temperature derivative enters the tangent (MaterialData::
+ * latent_heat_of_fusion and apparent_capacity_type, material.hpp:655-656,
+ * material.templates.hpp:562-616, source/heat/apparent_capacity.cpp). 0 switches it off.
+ * MPDG_ERR_NOT_SUPPORTED with volume_specific (the reference throws there). */
+int mpdg_heat_set_latent_heat(mpdg_heat *h, double latent_heat, int profile);
+/* Host evaluation of a law as the cell kernels evaluate it, at temperature T and heaviside H:
+ * out = {rho*cp, k, d(rho*cp)/dT, dk/dT} (Material::compute_parameters with the temperature
+ * derivatives of get_material_parameters_and_derivatives, heat_diffuse_operator.cpp:1167-1210).
+ * Laws CONSTANT, LINEAR_K, LIQUID_SOLID and GAS_LIQUID_SOLID; needs no GPU. */
+int mpdg_material_eval(const mpdg_material *m, double latent_heat, int profile, double T,
+                       double H, double out[4]);
 /* Boundary terms on one box face (0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+), replacing the
  * heat BoundaryConditionManager's "convection" / "radiation" / "neumann" entries
  * (heat_diffuse_operator.cpp:243-269 tangent, :690-781 rhs, :1088-1129 local op):

@@ -29,6 +29,7 @@ LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID, LAW_GAS_LIQUID_SOL
 SOLVER_CG, SOLVER_GMRES = 0, 1
 PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_CHEBYSHEV_JACOBI_F32, PRECOND_MG_F32 = 0, 1, 2, 3
 PREDICTOR_NONE, PREDICTOR_LINEAR, PREDICTOR_GIVEN = 0, 1, 2
+APPARENT_QLQ, APPARENT_CONSTANT, APPARENT_POLY4_BELL = 0, 1, 2
 
 
 class MeshDesc(C.Structure):
@@ -141,6 +142,9 @@ _SIGS = {
     "mpdg_heat_time_step_resident": (C.c_int, [_H, C.POINTER(StepParams), C.c_double,
                                                C.c_double, _P, _P, C.POINTER(StepStats)]),
     "mpdg_heat_set_timing": (C.c_int, [_H, C.c_int]),
+    "mpdg_heat_set_latent_heat": (C.c_int, [_H, C.c_double, C.c_int]),
+    "mpdg_material_eval": (C.c_int, [C.POINTER(Material), C.c_double, C.c_int, C.c_double,
+                                     C.c_double, _P]),
     "mpdg_amr_create": (C.c_int, [C.POINTER(MeshDesc), _P, C.c_int, C.POINTER(_H)]),
     "mpdg_amr_destroy": (C.c_int, [_H]),
     "mpdg_amr_n_dofs": (C.c_int64, [_H]),

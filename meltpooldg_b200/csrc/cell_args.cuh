@@ -21,6 +21,8 @@ struct MatParams {
   T T_liq, T_sol, inv_mushy, k1;
   T idt;
   int sharp, vs, need_told;
+  T latent;  // latent heat of fusion (> 0: apparent capacity of profile acap in the mushy zone)
+  int acap;
 };
 
 template <typename T>

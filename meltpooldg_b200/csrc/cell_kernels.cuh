@@ -31,6 +31,7 @@
 
 #include "cell_args.cuh"
 #include "fe_tables.hpp"
+#include "material_law.cuh"
 #include "reduce.cuh"
 
 namespace mpdg {
@@ -60,82 +61,6 @@ template <typename T> __device__ __forceinline__ void atomic_add(T *p, T v) { at
 template <int LAW> __host__ __device__ constexpr bool law_tdep() { return LAW == 1 || LAW == 2 || LAW == 5; }
 // laws that may need T_old (d(rho_cp)/dT (T_lin - T_old) / dt in the tangent)
 template <int LAW> __host__ __device__ constexpr bool law_told() { return LAW == 2 || LAW == 5; }
-
-// Material::compute_parameters for the three laws; LAW is a template constant.
-template <int LAW, typename T>
-__device__ __forceinline__ void mat_eval(const MatParams<T> &m, T temp, T &rhocp, T &k, T &drhocp,
-                                         T &dk)
-{
-  if (LAW == 0) {
-    rhocp = m.rho_l * m.cp_l;
-    k = m.k_l;
-    drhocp = T(0);
-    dk = T(0);
-  } else if (LAW == 1) {
-    rhocp = m.rho_l * m.cp_l;
-    k = m.k_l + m.k1 * temp;
-    drhocp = T(0);
-    dk = m.k1;
-  } else {
-    T sf;
-    if (m.sharp)
-      sf = temp < m.T_sol ? T(1) : T(0);
-    else {
-      sf = (m.T_liq - temp) * m.inv_mushy;
-      sf = sf < T(0) ? T(0) : (sf > T(1) ? T(1) : sf);
-    }
-    const T hs = T(-2) * sf * sf * sf + T(3) * sf * sf;
-    const T dhs = T(-6) * sf * sf + T(6) * sf;
-    const bool edge = (sf == T(0) || sf == T(1));
-    auto prop = [&](T l, T s) { return sf == T(0) ? l : (sf == T(1) ? s : l + (s - l) * hs); };
-    auto dprop = [&](T l, T s) { return edge ? T(0) : T(-1) * m.inv_mushy * ((s - l) * dhs); };
-    k = prop(m.k_l, m.k_s);
-    dk = dprop(m.k_l, m.k_s);
-    if (m.vs) {
-      rhocp = prop(m.rho_l * m.cp_l, m.rho_s * m.cp_s);
-      drhocp = dprop(m.rho_l * m.cp_l, m.rho_s * m.cp_s);
-    } else {
-      const T rho = prop(m.rho_l, m.rho_s), cp = prop(m.cp_l, m.cp_s);
-      const T drho = dprop(m.rho_l, m.rho_s), dcp = dprop(m.cp_l, m.cp_s);
-      rhocp = rho * cp;
-      drhocp = dcp * rho + drho * cp;
-    }
-  }
-}
-
-// Three-phase law (Material::compute_parameters, gas_liquid_solid,
-// material.templates.hpp:376-500, 620-740): every property is (1 - w) gas + w ls(T) with
-// ls the liquid-solid interpolation of mat_eval<2>, its T derivative w dls/dT; w = 1 gives
-// the liquid-solid law exactly.
-template <typename T>
-__device__ __forceinline__ void mat_eval_w(const MatParams<T> &m, T temp, T w, T &rhocp, T &k,
-                                           T &drhocp, T &dk)
-{
-  T sf;
-  if (m.sharp)
-    sf = temp < m.T_sol ? T(1) : T(0);
-  else {
-    sf = (m.T_liq - temp) * m.inv_mushy;
-    sf = sf < T(0) ? T(0) : (sf > T(1) ? T(1) : sf);
-  }
-  const T hs = T(-2) * sf * sf * sf + T(3) * sf * sf;
-  const T dhs = T(-6) * sf * sf + T(6) * sf;
-  const bool edge = (sf == T(0) || sf == T(1));
-  auto prop = [&](T l, T s) { return sf == T(0) ? l : (sf == T(1) ? s : l + (s - l) * hs); };
-  auto dprop = [&](T l, T s) { return edge ? T(0) : T(-1) * m.inv_mushy * ((s - l) * dhs); };
-  const T g = T(1) - w;
-  k = g * m.k_g + w * prop(m.k_l, m.k_s);
-  dk = w * dprop(m.k_l, m.k_s);
-  if (m.vs) {
-    rhocp = g * (m.rho_g * m.cp_g) + w * prop(m.rho_l * m.cp_l, m.rho_s * m.cp_s);
-    drhocp = w * dprop(m.rho_l * m.cp_l, m.rho_s * m.cp_s);
-  } else {
-    const T rho = g * m.rho_g + w * prop(m.rho_l, m.rho_s);
-    const T cp = g * m.cp_g + w * prop(m.cp_l, m.cp_s);
-    drhocp = (w * dprop(m.cp_l, m.cp_s)) * rho + (w * dprop(m.rho_l, m.rho_s)) * cp;
-    rhocp = rho * cp;
-  }
-}
 
 // One 1D sweep of matrix `kind` along `dir` for line `line` (0 <= line < n^2).
 template <int n, int kind, int dir, bool add, typename T>

@@ -23,6 +23,7 @@
 #include "cell_args.cuh"
 #include "degree_table.hpp"
 #include "fe_tables.hpp"
+#include "material_law.cuh"
 #include "reduce.cuh"
 
 using namespace mpdg;
@@ -98,6 +99,8 @@ struct mpdg_heat {
   // coefficients
   mpdg_material mat{};
   int law = 0, need_told = 0;
+  double latent = 0.0;  // latent heat of fusion (mpdg_heat_set_latent_heat)
+  int acap = MPDG_APPARENT_QLQ;
   double dt = 0.0;
   const double *T_lin = nullptr, *T_old = nullptr;
   float *T_lin_f = nullptr, *T_old_f = nullptr;
@@ -1272,6 +1275,8 @@ static CellArgs<T> cell_args(mpdg_heat *h)
   a.m.sharp = m.sharp;
   a.m.vs = m.volume_specific;
   a.m.need_told = h->need_told;
+  a.m.latent = (T)h->latent;
+  a.m.acap = h->acap;
   a.partials = h->partials;
   a.counter = h->counter;
   a.fin = FIN_NONE;
@@ -1835,6 +1840,8 @@ static int mg_build(mpdg_heat *h, const mpdg_solver_params *prm)
     h->mg.push_back(lv);
     MGLevel &L = h->mg.back();
     c->stream = h->stream;
+    c->latent = h->latent;
+    c->acap = h->acap;
     TRY(mpdg_heat_set_material(c, &h->mat));
     for (int f = 0; f < 6; ++f) {
       c->btype[f] = h->btype[f];
@@ -2816,6 +2823,17 @@ extern "C" int mpdg_heat_device_bytes(const mpdg_heat *h, int64_t *bytes)
   return MPDG_OK;
 }
 
+// d(rho_cp)/dT (T_lin - T_old) / dt enters the tangent when rho*cp depends on T
+static void set_need_told(mpdg_heat *h)
+{
+  const mpdg_material *m = &h->mat;
+  h->need_told = 0;
+  if (m->law == MPDG_LAW_LIQUID_SOLID || m->law == MPDG_LAW_GAS_LIQUID_SOLID)
+    h->need_told = m->volume_specific
+                     ? (m->rho_l * m->cp_l != m->rho_s * m->cp_s)
+                     : (m->rho_l != m->rho_s || m->cp_l != m->cp_s || h->latent > 0.0);
+}
+
 extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
 {
   if (!h || !m) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
@@ -2825,17 +2843,72 @@ extern "C" int mpdg_heat_set_material(mpdg_heat *h, const mpdg_material *m)
   if ((m->law == MPDG_LAW_LIQUID_SOLID || m->law == MPDG_LAW_GAS_LIQUID_SOLID) && !m->sharp &&
       !(m->T_liquidus > m->T_solidus))
     return fail(MPDG_ERR_INVALID_ARGUMENT, "liquidus must exceed solidus");
+  if (h->latent > 0.0 && m->volume_specific)
+    return fail(MPDG_ERR_NOT_SUPPORTED,
+                "the apparent capacity (latent heat) is not implemented for the volume specific "
+                "heat capacity");
   h->mat = *m;
   h->law = m->law;
-  h->need_told = 0;
-  if (m->law == MPDG_LAW_LIQUID_SOLID || m->law == MPDG_LAW_GAS_LIQUID_SOLID)
-    h->need_told = m->volume_specific ? (m->rho_l * m->cp_l != m->rho_s * m->cp_s)
-                                      : (m->rho_l != m->rho_s || m->cp_l != m->cp_s);
+  set_need_told(h);
   h->diag_valid = false;
   h->eig_valid = false;
   h->cf_dirty = true;
   h->tf_dirty = true;
   h->tk_dirty = true;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_latent_heat(mpdg_heat *h, double latent_heat, int profile)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  if (!(latent_heat >= 0.0) || !std::isfinite(latent_heat) || profile < MPDG_APPARENT_QLQ ||
+      profile > MPDG_APPARENT_POLY4_BELL)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "latent heat >= 0 and a known apparent-capacity profile");
+  if (latent_heat > 0.0 && h->mat.volume_specific)
+    return fail(MPDG_ERR_NOT_SUPPORTED,
+                "the apparent capacity (latent heat) is not implemented for the volume specific "
+                "heat capacity");
+  h->latent = latent_heat;
+  h->acap = profile;
+  set_need_told(h);
+  h->diag_valid = false;
+  h->eig_valid = false;
+  h->cf_dirty = true;
+  h->tf_dirty = true;
+  h->tk_dirty = true;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_material_eval(const mpdg_material *m, double latent_heat, int profile,
+                                  double T, double H, double out[4])
+{
+  if (!m || !out) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (profile < MPDG_APPARENT_QLQ || profile > MPDG_APPARENT_POLY4_BELL || !(latent_heat >= 0.0))
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "latent heat >= 0 and a known apparent-capacity profile");
+  MatParams<double> p;
+  memset(&p, 0, sizeof(p));
+  p.rho_l = m->rho_l, p.cp_l = m->cp_l, p.k_l = m->k_l;
+  p.rho_s = m->rho_s, p.cp_s = m->cp_s, p.k_s = m->k_s;
+  p.rho_g = m->rho_g, p.cp_g = m->cp_g, p.k_g = m->k_g;
+  p.T_liq = m->T_liquidus, p.T_sol = m->T_solidus, p.k1 = m->k1;
+  p.inv_mushy = m->T_liquidus != m->T_solidus ? 1.0 / (m->T_liquidus - m->T_solidus) : 0.0;
+  p.sharp = m->sharp;
+  p.vs = m->volume_specific;
+  p.latent = latent_heat;
+  p.acap = profile;
+  if (latent_heat > 0.0 && m->volume_specific)
+    return fail(MPDG_ERR_NOT_SUPPORTED, "apparent capacity with the volume specific capacity");
+  switch (m->law) {
+    case MPDG_LAW_CONSTANT: mat_eval<0>(p, T, out[0], out[1], out[2], out[3]); break;
+    case MPDG_LAW_LINEAR_K: mat_eval<1>(p, T, out[0], out[1], out[2], out[3]); break;
+    case MPDG_LAW_LIQUID_SOLID: mat_eval<2>(p, T, out[0], out[1], out[2], out[3]); break;
+    case MPDG_LAW_GAS_LIQUID_SOLID: {
+      const double w = m->sharp_gas_liquid ? (H > 0.5 ? 1.0 : 0.0) : H;
+      mat_eval_w(p, T, w, out[0], out[1], out[2], out[3]);
+      break;
+    }
+    default: return fail(MPDG_ERR_NOT_SUPPORTED, "host evaluation: laws 0, 1, 2 and 4");
+  }
   return MPDG_OK;
 }
 

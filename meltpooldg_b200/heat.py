@@ -125,6 +125,16 @@ def material(law=L.LAW_CONSTANT, rho=1.0, cp=1.0, k=1.0, k1=0.0, rho_s=None, cp_
     return m
 
 
+def material_eval(m: L.Material, T: float, H: float = 1.0, latent_heat: float = 0.0,
+                  profile: int = L.APPARENT_QLQ):
+    """(rho*cp, k, d(rho*cp)/dT, dk/dT) of the law at temperature T and heaviside H, evaluated
+    on the host by the code the cell kernels run (mpdg_material_eval; no GPU needed)."""
+    out = (C.c_double * 4)()
+    check(L.load().mpdg_material_eval(C.byref(m), float(latent_heat), int(profile), float(T),
+                                      float(H), out))
+    return tuple(out)
+
+
 @dataclass
 class LinearSolverData:
     """LinearSolverData (linear_solver_data.hpp:40-47) plus the Chebyshev and multigrid options."""
@@ -232,6 +242,11 @@ class HeatDiffuseOperator:
     # coefficients ---------------------------------------------------------
     def set_material(self, m: L.Material):
         check(self._L.mpdg_heat_set_material(self.h, C.byref(m)))
+
+    def set_latent_heat(self, latent_heat: float, profile: int = L.APPARENT_QLQ):
+        """Latent heat of fusion as an apparent heat capacity in the mushy zone
+        (MaterialData::latent_heat_of_fusion, apparent_capacity_type); 0 switches it off."""
+        check(self._L.mpdg_heat_set_latent_heat(self.h, float(latent_heat), int(profile)))
 
     def set_fields(self, heaviside=None, velocity=None):
         """Level-set heaviside (n_dofs) and velocity ((3, n_dofs), component-major) fields

@@ -84,3 +84,36 @@ def test_volume_specific_capacity_with_latent_heat_is_rejected():
     with pytest.raises(ValueError):
         o.set_material(O.material(O.LAW_LIQUID_SOLID, volume_specific=True, T_solidus=0.2,
                                   T_liquidus=0.8, latent_heat=1.0), 1e-2)
+
+
+# the product's law, evaluated on the host by the code the cell kernels run, against the oracle
+PRODUCT_CASES = [
+    ("liquid_solid", dict(law=2), False),
+    ("liquid_solid_sharp", dict(law=2, sharp=True), False),
+    ("three_phase", dict(law=4), True),
+    ("three_phase_sharp_gl", dict(law=4, sharp_gas_liquid=True), True),
+]
+
+
+@pytest.mark.parametrize("name,kw,uses_h", PRODUCT_CASES)
+@pytest.mark.parametrize("kind", list(TYPES) + ["none"])
+def test_product_material_law_matches_oracle(name, kw, uses_h, kind):
+    from meltpooldg_b200 import heat as H
+    props = dict(rho=7850.0, cp=460.0, k=55.563, rho_s=7000.0, cp_s=700.0, k_s=30.0,
+                 T_solidus=TS, T_liquidus=TL, rho_g=1.2, cp_g=1000.0, k_g=0.03)
+    latent, prof = (0.0, 0) if kind == "none" else (L, TYPES[kind][0])
+    om = O.material(latent_heat=latent, apparent_capacity=prof, **props, **kw)
+    pm = H.material(**props, **kw)
+    for T in np.linspace(265.0, 281.0, 41):
+        for Hv in ((0.0, 0.3, 0.6, 1.0) if uses_h else (1.0,)):
+            a = np.array(O.material_eval(om, T, Hv))
+            b = np.array(H.material_eval(pm, T, Hv, latent, prof))
+            assert np.allclose(b, a, rtol=1e-13, atol=1e-9), (T, Hv, a, b)
+
+
+def test_product_rejects_latent_heat_with_volume_specific_capacity():
+    from meltpooldg_b200 import heat as H
+    pm = H.material(law=2, T_solidus=TS, T_liquidus=TL, volume_specific=True)
+    with pytest.raises(H.ExcNotImplemented):
+        H.material_eval(pm, 273.0, 1.0, L, 0)
+    assert H.material_eval(pm, 273.0, 1.0, 0.0, 0)[0] > 0.0

@@ -161,6 +161,13 @@ class TwoLevelBoxMesh:
             w = self._tensor_basis(loc)
             nz = np.abs(w) > 1e-14
             cons[v] = (self.cell_nodes[owner][nz], w[nz])
+        self._finish(cons, dirichlet)
+
+    def _finish(self, cons, dirichlet):
+        """DoF numbering, the constraint matrix, the Dirichlet mask and the reference tables,
+        given the hanging nodes' constraints {node: (nodes, weights)}."""
+        n, m = self.n, self.m
+        n_nodes = len(self.node_pos)
         self.hanging = np.zeros(n_nodes, dtype=bool)
         self.hanging[list(cons)] = True
         # DoFs: the regular nodes, in position order (z, y, x)
@@ -340,7 +347,7 @@ class TwoLevelBoxMesh:
                 continue
             q = par.copy()
             q[d] += step[d]
-            nb = self._coarse_cell(q)
+            nb = self._neighbour(c, q)
             for a in range(n):
                 for b in range(n):
                     i = [0, 0, 0]
@@ -359,7 +366,7 @@ class TwoLevelBoxMesh:
             q = par.copy()
             q[d1] += step[d1]
             q[d2] += step[d2]
-            nb = self._coarse_cell(q)
+            nb = self._neighbour(c, q)
             for a in range(n):
                 i = [0, 0, 0]
                 i[d], i[d1], i[d2] = a, own[d1], own[d2]
@@ -390,6 +397,10 @@ class TwoLevelBoxMesh:
             F = Fd @ F
         assert (idx >= 0).all(), "a hanging node left ungathered"
         return idx, F
+
+    def _neighbour(self, c, q):
+        """The unrefined neighbour of cell c's parent at coarse index q."""
+        return self._coarse_cell(q)
 
     def _coarse_cell(self, q):
         ox = np.asarray(q, dtype=np.float64)
@@ -510,3 +521,127 @@ class TwoLevelBoxMesh:
             np.add.at(y, idx, -(r if F is None else F.T @ r))
         dst[~self.mask] += y[~self.mask]
         return dst
+
+
+class MultiLevelBoxMesh(TwoLevelBoxMesh):
+    """The box with each coarse cell refined uniformly `levels[iz][iy][ix]` times, neighbouring
+    coarse cells (across faces, edges and vertices) differing by one level at most: the 2:1
+    balance p4est keeps for MeltPoolDG's adaptive meshes. A node hangs when the coarsest cells
+    whose closed boxes hold it (level l_min) do not have it as a node; it is constrained to such
+    a cell's interpolant. Under the balance the constraining nodes never hang, so the rule of
+    the two-level mesh applies unchanged at every interface. The operator, the residual, the
+    solve and the cell-wise form are those of TwoLevelBoxMesh."""
+
+    def __init__(self, degree, cells, levels, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
+                 dirichlet=("x-", "x+", "y-", "y+", "z-", "z+")):
+        self.p = p = int(degree)
+        self.n = n = p + 1
+        self.m = m = tuple(int(c) for c in cells)
+        self.lo = np.asarray(lo, dtype=np.float64)
+        self.h = (np.asarray(hi, dtype=np.float64) - self.lo) / np.asarray(m)
+        lev = np.asarray(levels, dtype=np.int64).reshape(m[2], m[1], m[0])
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    a = lev[max(dz, 0):m[2] + min(dz, 0), max(dy, 0):m[1] + min(dy, 0),
+                            max(dx, 0):m[0] + min(dx, 0)]
+                    b = lev[max(-dz, 0):m[2] + min(-dz, 0), max(-dy, 0):m[1] + min(-dy, 0),
+                            max(-dx, 0):m[0] + min(-dx, 0)]
+                    if a.size and np.abs(a - b).max() > 1:
+                        raise ValueError("neighbouring coarse cells differ by more than one level")
+        self.levels = lev
+        self.refined = lev > 0
+        self.xi = gauss_lobatto(p)
+        origins, sizes, parents, lvl, gidx = [], [], [], [], []
+        for iz in range(m[2]):
+            for iy in range(m[1]):
+                for ix in range(m[0]):
+                    L = int(lev[iz, iy, ix])
+                    k = 1 << L
+                    for sz in range(k):
+                        for sy in range(k):
+                            for sx in range(k):
+                                origins.append((ix + sx / k, iy + sy / k, iz + sz / k))
+                                sizes.append(1.0 / k)
+                                lvl.append(L)
+                                g = (ix * k + sx, iy * k + sy, iz * k + sz)
+                                gidx.append(g)
+                                parents.append(tuple(v // 2 for v in g))
+        self.origins = np.asarray(origins, dtype=np.float64)
+        self.sizes = np.asarray(sizes, dtype=np.float64)
+        self.cell_level = np.asarray(lvl, dtype=np.int64)
+        self.gidx = np.asarray(gidx, dtype=np.int64)        # index on its level's lattice
+        self.parents = np.asarray(parents, dtype=np.int64)  # index on the level below
+        self.child = self.gidx % 2
+        self.n_cells = len(sizes)
+        self._cell_at = {(int(lvl[c]),) + tuple(int(v) for v in gidx[c]): c
+                         for c in range(self.n_cells)}
+        lx = np.array([(self.xi[i], self.xi[j], self.xi[k])
+                       for k in range(n) for j in range(n) for i in range(n)])
+        self._local = lx
+        pos = self.origins[:, None, :] + self.sizes[:, None, None] * lx[None, :, :]
+        keys = np.round(pos.reshape(-1, 3) * (1 << 26)).astype(np.int64)
+        uniq, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+        self.cell_nodes = inv.reshape(self.n_cells, n ** 3)
+        self.node_pos = pos.reshape(-1, 3)[first]
+        n_nodes = len(uniq)
+        node_of_level = {}
+        for L in np.unique(self.cell_level):
+            f = np.zeros(n_nodes, dtype=bool)
+            f[self.cell_nodes[self.cell_level == L].ravel()] = True
+            node_of_level[int(L)] = f
+        tol = 1e-9
+        cons = {}
+        for v in range(n_nodes):
+            x = self.node_pos[v]
+            base = np.floor(x + tol).astype(int)
+            holders = []
+            for dz in (0, -1):
+                for dy in (0, -1):
+                    for dx in (0, -1):
+                        c0 = (base[0] + dx, base[1] + dy, base[2] + dz)
+                        if all(0 <= c0[d] < m[d] for d in range(3)):
+                            o = np.asarray(c0, dtype=np.float64)
+                            if np.all(x >= o - tol) and np.all(x <= o + 1.0 + tol):
+                                holders.append(c0)
+            lmin = min(int(lev[c[2], c[1], c[0]]) for c in holders)
+            if node_of_level[lmin][v]:
+                continue
+            c0 = next(c for c in holders if lev[c[2], c[1], c[0]] == lmin)
+            k = 1 << lmin
+            sub = np.clip(np.floor((x - np.asarray(c0)) * k + tol).astype(int), 0, k - 1)
+            g = tuple(int(c0[d] * k + sub[d]) for d in range(3))
+            owner = self._cell_at[(lmin,) + g]
+            loc = np.clip((x - self.origins[owner]) / self.sizes[owner], 0.0, 1.0)
+            w = self._tensor_basis(loc)
+            nz = np.abs(w) > 1e-14
+            cons[v] = (self.cell_nodes[owner][nz], w[nz])
+        self._finish(cons, dirichlet)
+
+    def _neighbour(self, c, q):
+        return self._coarse_unrefined_at(c, q)
+
+    # neighbour lookups on the level below the cell: the coarse cell of the two-level mesh
+    def _coarse_unrefined_at(self, c, q):
+        L = int(self.cell_level[c]) - 1
+        return self._cell_at.get((L,) + tuple(int(v) for v in q))
+
+    def hanging_code(self, c) -> int:
+        if self.cell_level[c] == 0 or not self.hanging.any():
+            return 0
+        par, sv = self.parents[c], self.child[c]
+        step = np.where(sv == 0, -1, 1)
+        e = np.eye(3, dtype=np.int64)
+        face = [self._coarse_unrefined_at(c, par + step[d] * e[d]) is not None for d in range(3)]
+        edge = []
+        for d in range(3):
+            d1, d2 = [x for x in range(3) if x != d]
+            off = np.zeros(3, dtype=np.int64)
+            off[d1], off[d2] = step[d1], step[d2]
+            edge.append(self._coarse_unrefined_at(c, par + off) is not None and not face[d1]
+                        and not face[d2])
+        code = sum(int(face[d]) << (3 + d) for d in range(3)) + \
+            sum(int(edge[d]) << (6 + d) for d in range(3))
+        if code == 0:
+            return 0
+        return code | int(sv[0]) | (int(sv[1]) << 1) | (int(sv[2]) << 2)

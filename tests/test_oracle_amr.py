@@ -204,3 +204,68 @@ def test_cellwise_diagonal_and_residual_match_the_condensed_forms(p):
     b = mesh.create_rhs_cellwise(T, To, q, **kw)
     assert _rel(b, a) < 1e-13
     assert np.all(b[mesh.mask] == 0.0)
+
+
+def _three_levels():
+    lev = np.zeros((5, 5, 5), dtype=np.int64)
+    lev[1:4, 1:4, 1:4] = 1
+    lev[2, 2, 2] = 2
+    return lev
+
+
+def test_multilevel_mesh_reduces_to_the_two_level_and_structured_meshes():
+    rng = np.random.default_rng(50)
+    lev = np.zeros((3, 3, 4), dtype=np.int64)
+    for ix, iy, iz in REFINE:
+        lev[iz, iy, ix] = 1
+    a = A.MultiLevelBoxMesh(2, (4, 3, 3), lev)
+    b = A.TwoLevelBoxMesh(2, (4, 3, 3), refine=REFINE)
+    assert a.n_dofs == b.n_dofs and a.hanging.sum() == b.hanging.sum()
+    assert np.abs(a.support_points() - b.support_points()).max() < 1e-14
+    u = rng.uniform(-1.0, 1.0, a.n_dofs)
+    assert np.abs(a.node_values(u) - b.node_values(u)).max() < 1e-14
+    coef = dict(rho_cp=2.0, dt=0.05, k0=1.0)
+    assert _rel(a.vmult(u, **coef), b.vmult(u, **coef)) < 1e-13
+    assert [a.hanging_code(c) for c in range(a.n_cells)] == \
+        [b.hanging_code(c) for c in range(b.n_cells)]
+    # every cell twice refined: the structured oracle on the four times finer box
+    c = A.MultiLevelBoxMesh(2, (2, 1, 1), np.full((1, 1, 2), 2))
+    o = O.Oracle(2, (8, 4, 4))
+    o.set_material(O.material(O.LAW_CONSTANT, rho=2.0, cp=1.0, k=1.0), 0.05)
+    v = rng.uniform(-1.0, 1.0, c.n_dofs)
+    assert c.n_dofs == o.n_dofs and not c.hanging.any()
+    assert _rel(c.vmult(v, **coef), o.vmult(v)) < 1e-12
+
+
+def test_unbalanced_levels_are_rejected():
+    lev = np.zeros((1, 1, 2), dtype=np.int64)
+    lev[0, 0, 1] = 2
+    with pytest.raises(ValueError):
+        A.MultiLevelBoxMesh(2, (2, 1, 1), lev)
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_three_level_mesh_constraints_and_galerkin_exactness(p):
+    """Levels 0, 1 and 2 (2:1 balanced): constraint weights reproduce Q_p, the cell-wise form
+    equals C^T A C, and the Galerkin solution reproduces u = 64 x(1-x) y(1-y) z(1-z)."""
+    mesh = A.MultiLevelBoxMesh(p, (5, 5, 5), _three_levels())
+    lv = mesh.cell_level
+    assert set(np.unique(lv)) == {0, 1, 2}
+    codes = [mesh.hanging_code(c) for c in range(mesh.n_cells)]
+    assert any(codes[c] for c in np.flatnonzero(lv == 2))  # level-2 cells hang on level 1
+    rng = np.random.default_rng(60 + p)
+    u = rng.uniform(-1.0, 1.0, mesh.n_dofs)
+    nodal = mesh.node_values(u)
+    for c in range(mesh.n_cells):
+        idx, F = mesh.cell_map(c)
+        local = u[idx] if F is None else F @ u[idx]
+        assert np.abs(local - nodal[mesh.cell_nodes[c]]).max() < 1e-13
+    coef = dict(rho_cp=2.0, dt=0.1, k0=1.0)
+    assert _rel(mesh.vmult_cellwise(u, **coef), mesh.vmult(u, **coef)) < 1e-13
+
+    def load(x):
+        return 2.0 / 0.1 * _u(x) - _lap_u(x)
+
+    x = mesh.solve(mesh.load_vector(load), **coef)
+    exact = np.where(mesh.mask, 0.0, _u(mesh.support_points()))
+    assert np.abs(x - exact).max() < 1e-10 * np.abs(exact).max()

@@ -406,15 +406,16 @@ int mpdg_heat_set_timing(mpdg_heat *h, int enable);
 int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset);
 
 /* ---- meshes with hanging nodes (adaptive refinement) ---------------------------------
- * A box of coarse cells in which the cells flagged in `refine` (mz*my*mx bytes, x fastest,
- * nonzero = refined) are split once into 8 children: the mesh refine_grid produces with one
- * level of refinement difference (source/utilities/amr.cpp:18-41). A node of a refined cell
- * on a face or an edge of an unrefined neighbour that is not one of the neighbour's nodes
- * hangs: it is constrained to the neighbour's interpolant (DoFTools::
+ * A box of coarse cells, each refined uniformly `refine[c]` times (mz*my*mx bytes, x fastest;
+ * 0 = unrefined, 1 = split into 8 children, up to 6), neighbouring coarse cells across faces,
+ * edges and vertices differing by one level at most: the 2:1-balanced meshes refine_grid
+ * produces (source/utilities/amr.cpp:18-41). A node hangs when the coarsest cells holding it do
+ * not have it as a node: it is constrained to such a cell's interpolant (DoFTools::
  * make_hanging_node_constraints merged into the Dirichlet constraints,
  * include/meltpooldg/utilities/constraints.hpp:111-132). The DoFs are the other nodes,
  * numbered by position (z, then y, then x). Affine boxes only (perturb = 0), degree 1..4.
- * device < 0 builds the host description only (no CUDA call; vmult then fails). */
+ * device < 0 builds the host description only (no CUDA call; vmult then fails); on a device
+ * the levels are 0 and 1 (MPDG_ERR_NOT_SUPPORTED otherwise). */
 typedef struct mpdg_amr mpdg_amr;
 int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine, int device,
                     mpdg_amr **out);
@@ -429,7 +430,8 @@ int mpdg_amr_constraint_mask(const mpdg_amr *h, uint8_t *mask);
  * edge name the unrefined neighbour's face or edge DoFs of the same local indices, and the
  * hanging code: bits 0-2 the child position in the parent, bit 3+d a hanging face normal to
  * direction d, bit 6+d a hanging edge parallel to d whose faces do not hang (bits 0-8 zero
- * without hanging nodes), bit 9 a refined cell. */
+ * without hanging nodes), bit 9 a refined cell, bits 10-12 its level. Coarse cells are
+ * listed in z, y, x order, each as its 8^level cells in z, y, x order of its own lattice. */
 int mpdg_amr_cell_data(const mpdg_amr *h, int64_t *dofs, uint16_t *codes);
 /* Constant or LINEAR_K material and the time increment (mpdg_heat_set_material,
  * mpdg_heat_reset_time_increment). */

@@ -14,15 +14,16 @@ from .heat import ExcInvalidArgument, check
 
 
 class AmrHeatOperator:
-    """refine: coarse cell indices (ix, iy, iz) to split once, or a bool array [mz][my][mx].
+    """refine: coarse cell indices (ix, iy, iz) to split once, a bool array [mz][my][mx], or an
+    integer array [mz][my][mx] of refinement levels (2:1 balanced; one level on a device).
     device=None builds the host description only (DoFs, support points, cell data)."""
 
     def __init__(self, mesh: L.MeshDesc, refine=(), device: int | None = 0):
         self._L = L.load()
         m = tuple(mesh.cells)
         ref = np.zeros((m[2], m[1], m[0]), dtype=np.uint8)
-        if isinstance(refine, np.ndarray) and refine.dtype == bool:
-            ref[...] = refine
+        if isinstance(refine, np.ndarray) and refine.dtype.kind in "biu":
+            ref[...] = refine.astype(np.uint8)
         else:
             for ix, iy, iz in refine:
                 ref[iz, iy, ix] = 1

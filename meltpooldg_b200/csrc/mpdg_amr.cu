@@ -1,7 +1,8 @@
-// Heat operator on a box mesh with one level of refinement and hanging-node constraints.
+// Heat operator on a box mesh with refined cells and hanging-node constraints.
 //
-// The mesh: a box of coarse cells, some split once into 8 children (the meshes
-// refine_grid in source/utilities/amr.cpp:18-41 produces with one level of difference).
+// The mesh: a box of coarse cells, each refined uniformly to its level, neighbouring coarse
+// cells differing by one level at most (the 2:1 balance of the meshes refine_grid in
+// source/utilities/amr.cpp:18-41 produces); the GPU operator takes one level for now.
 // A node of a refined cell that lies on a face or an edge of an unrefined neighbour and is
 // not one of its nodes hangs; its value is the neighbour's FE_Q(p) interpolant there, the
 // rule of DoFTools::make_hanging_node_constraints that MeltPoolDG merges into its Dirichlet
@@ -22,6 +23,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/mpdg_heat.h"
@@ -33,6 +35,8 @@ namespace {
 
 constexpr int kAmrMaxN = 5;  // degree <= 4
 constexpr uint16_t kFineBit = 1u << 9;
+constexpr int kLevelShift = 10;  // bits 10-12: the cell's refinement level
+constexpr int kAmrMaxLevel = 6;
 
 struct AmrArgs {
   const int *idx;
@@ -179,6 +183,7 @@ struct mpdg_amr {
   int m[3] = {0, 0, 0};
   double lo[3] = {0, 0, 0}, h[3] = {0, 0, 0};
   int64_t n_cells = 0, n_dofs = 0;
+  int max_level = 0;
   std::vector<int64_t> cell_dofs;  // n_cells x n^3
   std::vector<uint16_t> codes;
   std::vector<double> dof_pos;     // n_dofs x 3, physical
@@ -214,39 +219,60 @@ void release(mpdg_amr *h)
 // the host description: active cells, node numbering, hanging nodes, DoFs, cell data
 int build_host(mpdg_amr *h, const mpdg_mesh_desc *desc, const uint8_t *refine)
 {
-  const int p = h->p, n = h->n, n3 = n * n * n;
+  const int n = h->n, n3 = n * n * n;
   const int mx = h->m[0], my = h->m[1], mz = h->m[2];
-  auto refined = [&](int ix, int iy, int iz) {
-    return refine[(size_t)ix + (size_t)mx * (iy + (size_t)my * iz)] != 0;
+  auto level = [&](int ix, int iy, int iz) {
+    return (int)refine[(size_t)ix + (size_t)mx * (iy + (size_t)my * iz)];
   };
-  auto unrefined_at = [&](int ix, int iy, int iz) {
-    return ix >= 0 && iy >= 0 && iz >= 0 && ix < mx && iy < my && iz < mz && !refined(ix, iy, iz);
+  auto inside = [&](int ix, int iy, int iz) {
+    return ix >= 0 && iy >= 0 && iz >= 0 && ix < mx && iy < my && iz < mz;
   };
-  mpdg::Tables1D tb = mpdg::make_tables(n);
-  const double *xi = tb.xl;
-  // active cells
-  struct Cell {
-    double o[3];
-    double size;
-    int par[3];
-    int s[3];
-  };
-  std::vector<Cell> cells;
-  std::vector<int64_t> coarse_id((size_t)mx * my * mz, -1);
+  // 2:1 balance across faces, edges and vertices
   for (int iz = 0; iz < mz; ++iz)
     for (int iy = 0; iy < my; ++iy)
       for (int ix = 0; ix < mx; ++ix) {
-        if (refined(ix, iy, iz)) {
-          for (int sz = 0; sz < 2; ++sz)
-            for (int sy = 0; sy < 2; ++sy)
-              for (int sx = 0; sx < 2; ++sx)
-                cells.push_back({{ix + 0.5 * sx, iy + 0.5 * sy, iz + 0.5 * sz}, 0.5,
-                                 {ix, iy, iz}, {sx, sy, sz}});
-        } else {
-          coarse_id[(size_t)ix + (size_t)mx * (iy + (size_t)my * iz)] = (int64_t)cells.size();
-          cells.push_back({{(double)ix, (double)iy, (double)iz}, 1.0, {ix, iy, iz}, {0, 0, 0}});
-        }
+        if (level(ix, iy, iz) > kAmrMaxLevel)
+          return fail(MPDG_ERR_INVALID_ARGUMENT, "refinement level above the maximum");
+        for (int dz = -1; dz <= 1; ++dz)
+          for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+              if (inside(ix + dx, iy + dy, iz + dz) &&
+                  std::abs(level(ix + dx, iy + dy, iz + dz) - level(ix, iy, iz)) > 1)
+                return fail(MPDG_ERR_INVALID_ARGUMENT,
+                            "neighbouring coarse cells differ by more than one level");
       }
+  mpdg::Tables1D tb = mpdg::make_tables(n);
+  const double *xi = tb.xl;
+  // active cells: every coarse cell refined uniformly to its level
+  struct Cell {
+    double o[3];
+    double size;
+    int level;
+    int64_t g[3];  // index on its level's lattice
+  };
+  std::vector<Cell> cells;
+  std::unordered_map<int64_t, int64_t> cell_at;  // (level, lattice index) -> cell
+  auto lattice_key = [](int L, int64_t gx, int64_t gy, int64_t gz) {
+    return (((int64_t)L * 1048576 + gz) * 1048576 + gy) * 1048576 + gx;
+  };
+  for (int iz = 0; iz < mz; ++iz)
+    for (int iy = 0; iy < my; ++iy)
+      for (int ix = 0; ix < mx; ++ix) {
+        const int L = level(ix, iy, iz), k = 1 << L;
+        for (int sz = 0; sz < k; ++sz)
+          for (int sy = 0; sy < k; ++sy)
+            for (int sx = 0; sx < k; ++sx) {
+              Cell cl{{ix + (double)sx / k, iy + (double)sy / k, iz + (double)sz / k}, 1.0 / k, L,
+                      {(int64_t)ix * k + sx, (int64_t)iy * k + sy, (int64_t)iz * k + sz}};
+              cell_at[lattice_key(L, cl.g[0], cl.g[1], cl.g[2])] = (int64_t)cells.size();
+              cells.push_back(cl);
+            }
+      }
+  auto find_cell = [&](int L, int64_t gx, int64_t gy, int64_t gz) -> int64_t {
+    if (L < 0 || gx < 0 || gy < 0 || gz < 0) return -1;
+    auto it = cell_at.find(lattice_key(L, gx, gy, gz));
+    return it == cell_at.end() ? -1 : it->second;
+  };
   const int64_t nc = (int64_t)cells.size();
   // nodes by position key (coarse-cell units)
   std::vector<std::pair<Key, int64_t>> ent((size_t)nc * n3);
@@ -274,30 +300,28 @@ int build_host(mpdg_amr *h, const mpdg_mesh_desc *desc, const uint8_t *refine)
     node_of[(size_t)ent[a].second] = (int64_t)first.size() - 1;
   }
   const int64_t n_nodes = (int64_t)first.size();
-  // hanging nodes: nodes of refined cells on the closed box of an unrefined coarse cell
-  // that are not nodes of an unrefined cell
-  std::vector<uint8_t> coarse_node((size_t)n_nodes, 0), fine_node((size_t)n_nodes, 0);
+  // a node hangs when the coarsest cells whose closed boxes hold it (level l_min) do not have
+  // it as a node; under the 2:1 balance its constraining nodes never hang
+  std::vector<uint32_t> level_bits((size_t)n_nodes, 0);  // levels of the cells that have it
   for (int64_t c = 0; c < nc; ++c)
-    for (int l = 0; l < n3; ++l)
-      (cells[c].size == 1.0 ? coarse_node : fine_node)[(size_t)node_of[c * n3 + l]] = 1;
+    for (int l = 0; l < n3; ++l) level_bits[(size_t)node_of[c * n3 + l]] |= 1u << cells[c].level;
   std::vector<uint8_t> hanging((size_t)n_nodes, 0);
   const double tol = 1e-9;
   for (int64_t v = 0; v < n_nodes; ++v) {
-    if (!fine_node[v] || coarse_node[v]) continue;
     const double *x = &pos[(size_t)first[v] * 3];
     const int bx = (int)std::floor(x[0] + tol), by = (int)std::floor(x[1] + tol),
               bz = (int)std::floor(x[2] + tol);
-    bool found = false;
-    for (int dz = 0; dz >= -1 && !found; --dz)
-      for (int dy = 0; dy >= -1 && !found; --dy)
-        for (int dx = 0; dx >= -1 && !found; --dx) {
+    int lmin = 1 << 30;
+    for (int dz = 0; dz >= -1; --dz)
+      for (int dy = 0; dy >= -1; --dy)
+        for (int dx = 0; dx >= -1; --dx) {
           const int cx = bx + dx, cy = by + dy, cz = bz + dz;
-          if (!unrefined_at(cx, cy, cz)) continue;
+          if (!inside(cx, cy, cz)) continue;
           if (x[0] >= cx - tol && x[0] <= cx + 1 + tol && x[1] >= cy - tol &&
               x[1] <= cy + 1 + tol && x[2] >= cz - tol && x[2] <= cz + 1 + tol)
-            found = true;
+            lmin = std::min(lmin, level(cx, cy, cz));
         }
-    hanging[v] = found;
+    hanging[v] = !((level_bits[v] >> lmin) & 1u);
   }
   // DoFs: the regular nodes ordered by (z, y, x)
   std::vector<int64_t> regular;
@@ -325,45 +349,55 @@ int build_host(mpdg_amr *h, const mpdg_mesh_desc *desc, const uint8_t *refine)
         h->mask[r] = 1;
     }
   }
-  // per cell: gathered DoFs and the hanging code
+  // per cell: gathered DoFs and the hanging code (the neighbours of its parent one level down)
   h->cell_dofs.assign((size_t)nc * n3, -1);
   h->codes.assign((size_t)nc, 0);
+  h->max_level = 0;
   auto lin = [n](int i, int j, int k) { return i + n * (j + n * k); };
   for (int64_t c = 0; c < nc; ++c) {
     const Cell &cl = cells[c];
     int64_t *idx = &h->cell_dofs[(size_t)c * n3];
     for (int l = 0; l < n3; ++l) idx[l] = dof_of[(size_t)node_of[c * n3 + l]];
-    if (cl.size == 1.0) continue;
-    int code = kFineBit;
+    h->max_level = std::max(h->max_level, cl.level);
+    if (cl.level == 0) continue;
+    int s[3];
+    int64_t par[3];
+    for (int d = 0; d < 3; ++d) {
+      s[d] = (int)(cl.g[d] & 1);
+      par[d] = cl.g[d] >> 1;
+    }
+    const int L = cl.level - 1;
+    int code = kFineBit | (cl.level << kLevelShift);
     int step[3], own[3], other[3];
     for (int d = 0; d < 3; ++d) {
-      step[d] = cl.s[d] ? 1 : -1;
-      own[d] = cl.s[d] ? n - 1 : 0;
+      step[d] = s[d] ? 1 : -1;
+      own[d] = s[d] ? n - 1 : 0;
       other[d] = n - 1 - own[d];
     }
+    int64_t face_nb[3], edge_nb[3];
     bool face[3], edge[3];
     for (int d = 0; d < 3; ++d) {
-      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
+      int64_t q[3] = {par[0], par[1], par[2]};
       q[d] += step[d];
-      face[d] = unrefined_at(q[0], q[1], q[2]);
+      face_nb[d] = find_cell(L, q[0], q[1], q[2]);
+      face[d] = face_nb[d] >= 0;
     }
     for (int d = 0; d < 3; ++d) {
       const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
-      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
+      int64_t q[3] = {par[0], par[1], par[2]};
       q[d1] += step[d1];
       q[d2] += step[d2];
-      edge[d] = unrefined_at(q[0], q[1], q[2]) && !face[d1] && !face[d2];
+      edge_nb[d] = find_cell(L, q[0], q[1], q[2]);
+      edge[d] = edge_nb[d] >= 0 && !face[d1] && !face[d2];
     }
     int hb = 0;
     for (int d = 0; d < 3; ++d) hb |= (face[d] ? 1 << (3 + d) : 0) | (edge[d] ? 1 << (6 + d) : 0);
-    if (hb) code |= hb | cl.s[0] | (cl.s[1] << 1) | (cl.s[2] << 2);
+    if (hb) code |= hb | s[0] | (s[1] << 1) | (s[2] << 2);
     h->codes[(size_t)c] = (uint16_t)code;
     // gather the neighbour's face / edge DoFs at the same local indices
     for (int d = 0; d < 3; ++d) {
       if (!face[d]) continue;
-      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
-      q[d] += step[d];
-      const int64_t nb = coarse_id[(size_t)q[0] + (size_t)mx * (q[1] + (size_t)my * q[2])];
+      const int64_t nb = face_nb[d];
       const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
       for (int a = 0; a < n; ++a)
         for (int b = 0; b < n; ++b) {
@@ -380,10 +414,7 @@ int build_host(mpdg_amr *h, const mpdg_mesh_desc *desc, const uint8_t *refine)
     for (int d = 0; d < 3; ++d) {
       if (!edge[d]) continue;
       const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
-      int q[3] = {cl.par[0], cl.par[1], cl.par[2]};
-      q[d1] += step[d1];
-      q[d2] += step[d2];
-      const int64_t nb = coarse_id[(size_t)q[0] + (size_t)mx * (q[1] + (size_t)my * q[2])];
+      const int64_t nb = edge_nb[d];
       for (int a = 0; a < n; ++a) {
         int i[3], jn[3];
         i[d] = a;
@@ -399,7 +430,6 @@ int build_host(mpdg_amr *h, const mpdg_mesh_desc *desc, const uint8_t *refine)
   for (int64_t v : h->cell_dofs)
     if (v < 0 || v >= h->n_dofs)
       return fail(MPDG_ERR_INVALID_ARGUMENT, "hanging node left ungathered (unsupported mesh)");
-  (void)p;
   return MPDG_OK;
 }
 
@@ -417,9 +447,6 @@ extern "C" int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine
   for (int d = 0; d < 3; ++d)
     if (desc->cells[d] < 1 || !(desc->hi[d] > desc->lo[d]))
       return fail(MPDG_ERR_INVALID_ARGUMENT, "invalid box");
-  if ((int64_t)desc->cells[0] * desc->cells[1] * desc->cells[2] * 8 *
-          (int64_t)std::pow(desc->degree + 1, 3) > (int64_t)1 << 30)
-    return fail(MPDG_ERR_INVALID_ARGUMENT, "hanging-node mesh too large for 32-bit cell data");
   mpdg_amr *h = new mpdg_amr();
   h->p = desc->degree;
   h->n = desc->degree + 1;
@@ -433,6 +460,15 @@ extern "C" int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine
   if (rc != MPDG_OK) {
     delete h;
     return rc;
+  }
+  if (device >= 0 && h->max_level > 1) {
+    delete h;
+    return fail(MPDG_ERR_NOT_SUPPORTED,
+                "hanging-node meshes on the GPU: one refinement level (several on the host only)");
+  }
+  if (device >= 0 && h->n_cells * (int64_t)h->n * h->n * h->n >= ((int64_t)1 << 31)) {
+    delete h;
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "hanging-node mesh too large for 32-bit cell data");
   }
   if (device >= 0) {
     const int n3 = h->n * h->n * h->n;

@@ -46,3 +46,31 @@ def test_invalid_meshes_rejected_without_gpu():
     op = AmrHeatOperator(H.box_mesh(2, (2, 2, 2)), [(0, 0, 0)], device=None)
     with pytest.raises(H.ExcNotImplemented):
         op.set_material(H.material(law=L.LAW_LIQUID_SOLID), 1e-3)
+
+
+def test_multilevel_host_description_matches_oracle():
+    """Levels 0, 1 and 2 (2:1 balanced) on the host: DoFs, support points, mask, gathered DoFs
+    and codes (bits 10-12 the level) equal the oracle's multi-level mesh; a device handle is
+    refused before any CUDA call."""
+    p = 2
+    lev = np.zeros((5, 5, 5), dtype=np.int64)
+    lev[1:4, 1:4, 1:4] = 1
+    lev[2, 2, 2] = 2
+    mesh = H.box_mesh(p, (5, 5, 5), dirichlet=("x-", "x+", "z-"))
+    op = AmrHeatOperator(mesh, lev, device=None)
+    o = A.MultiLevelBoxMesh(p, (5, 5, 5), lev, dirichlet=("x-", "x+", "z-"))
+    assert op.n_dofs == o.n_dofs and op.n_cells == o.n_cells
+    assert np.abs(op.support_points() - o.support_points()).max() < 1e-14
+    assert np.array_equal(op.constraint_mask().astype(bool), o.mask)
+    dofs, codes = op.cell_data()
+    for c in range(o.n_cells):
+        idx, _ = o.cell_map(c)
+        assert np.array_equal(dofs[c], idx), c
+        assert int(codes[c]) & 0x1FF == o.hanging_code(c), c
+        assert (int(codes[c]) >> 10) & 7 == o.cell_level[c]
+    with pytest.raises(H.ExcNotImplemented):
+        AmrHeatOperator(mesh, lev, device=0)
+    bad = lev.copy()
+    bad[0, 0, 0] = 2
+    with pytest.raises(H.ExcInvalidArgument):
+        AmrHeatOperator(mesh, bad, device=None)

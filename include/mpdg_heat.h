@@ -184,6 +184,12 @@ int mpdg_heat_set_fields(mpdg_heat *h, const double *heaviside, const double *ve
  * material.templates.hpp:562-616, source/heat/apparent_capacity.cpp). 0 switches it off.
  * MPDG_ERR_NOT_SUPPORTED with volume_specific (the reference throws there). */
 int mpdg_heat_set_latent_heat(mpdg_heat *h, double latent_heat, int profile);
+/* Dirichlet values per face (x-, x+, y-, y+, z-, z+; the faces of the mesh description's mask)
+ * for the following steps and distribute calls: boundary data that change in time
+ * (HeatData::enable_time_dependent_bc, whose constraints init_time_advance rebuilds every step,
+ * heat_diffuse_operation.cpp:219-226), constant per face. The first flagged face in that order
+ * owns an edge or corner DoF. */
+int mpdg_heat_set_dirichlet_values(mpdg_heat *h, const double values[6]);
 /* Host evaluation of a law as the cell kernels evaluate it, at temperature T and heaviside H:
  * out = {rho*cp, k, d(rho*cp)/dT, dk/dT} (Material::compute_parameters with the temperature
  * derivatives of get_material_parameters_and_derivatives, heat_diffuse_operator.cpp:1167-1210).

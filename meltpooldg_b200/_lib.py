@@ -143,6 +143,7 @@ _SIGS = {
                                                C.c_double, _P, _P, C.POINTER(StepStats)]),
     "mpdg_heat_set_timing": (C.c_int, [_H, C.c_int]),
     "mpdg_heat_set_latent_heat": (C.c_int, [_H, C.c_double, C.c_int]),
+    "mpdg_heat_set_dirichlet_values": (C.c_int, [_H, _P]),
     "mpdg_material_eval": (C.c_int, [C.POINTER(Material), C.c_double, C.c_int, C.c_double,
                                      C.c_double, _P]),
     "mpdg_amr_create": (C.c_int, [C.POINTER(MeshDesc), _P, C.c_int, C.POINTER(_H)]),

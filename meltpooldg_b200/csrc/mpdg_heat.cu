@@ -2879,6 +2879,15 @@ extern "C" int mpdg_heat_set_latent_heat(mpdg_heat *h, double latent_heat, int p
   return MPDG_OK;
 }
 
+extern "C" int mpdg_heat_set_dirichlet_values(mpdg_heat *h, const double values[6])
+{
+  if (!h || !values) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  for (int f = 0; f < 6; ++f)
+    if (!std::isfinite(values[f])) return fail(MPDG_ERR_INVALID_ARGUMENT, "Dirichlet value not finite");
+  for (int f = 0; f < 6; ++f) h->desc.dirichlet_value[f] = values[f];
+  return MPDG_OK;
+}
+
 extern "C" int mpdg_material_eval(const mpdg_material *m, double latent_heat, int profile,
                                   double T, double H, double out[4])
 {

@@ -248,6 +248,21 @@ class HeatDiffuseOperator:
         (MaterialData::latent_heat_of_fusion, apparent_capacity_type); 0 switches it off."""
         check(self._L.mpdg_heat_set_latent_heat(self.h, float(latent_heat), int(profile)))
 
+    def set_dirichlet_values(self, values):
+        """Dirichlet values per face for the following steps (a dict {"x-": v, ...} over the
+        Dirichlet faces, or six values in the order x-, x+, y-, y+, z-, z+)."""
+        v = (C.c_double * 6)()
+        if isinstance(values, dict):
+            cur = list(self.mesh.dirichlet_value)
+            for f, val in values.items():
+                cur[FACES[f]] = float(val)
+            values = cur
+        for i, val in enumerate(values):
+            v[i] = float(val)
+        check(self._L.mpdg_heat_set_dirichlet_values(self.h, v))
+        for i in range(6):
+            self.mesh.dirichlet_value[i] = v[i]
+
     def set_fields(self, heaviside=None, velocity=None):
         """Level-set heaviside (n_dofs) and velocity ((3, n_dofs), component-major) fields
         of the two-phase operator, torch CUDA float64 tensors on this operator's DoFs; None

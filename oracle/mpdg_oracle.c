@@ -146,6 +146,7 @@ struct orc_heat {
   double  *geo;   /* affine: n_cells x 7 ; else n_cells x npt x 7 */
   uint8_t *mask;  /* constrained DoFs */
   double  *dvalue; /* Dirichlet value per DoF (valid where mask) */
+  int      dirichlet_mask;
   /* 1D data */
   double xg[NMAX], wg[NMAX], xl[NMAX];
   double S[NMAX][NMAX], Sd[NMAX][NMAX], D[NMAX][NMAX];
@@ -360,21 +361,8 @@ orc_heat *orc_create(const orc_mesh_desc *desc)
   /* constraints */
   h->mask = (uint8_t *)calloc((size_t)h->n_dofs, 1);
   h->dvalue = (double *)calloc((size_t)h->n_dofs, sizeof(double));
-  for (int64_t K = 0; K < h->nd[2]; ++K)
-    for (int64_t J = 0; J < h->nd[1]; ++J)
-      for (int64_t I = 0; I < h->nd[0]; ++I) {
-        const int64_t idx = I + h->nd[0] * (J + (int64_t)h->nd[1] * K);
-        const int64_t pos[3] = {I, J, K};
-        for (int f = 0; f < 6; ++f) {
-          if (!(desc->dirichlet_mask & (1 << f))) continue;
-          const int d = f / 2;
-          const int64_t at = (f & 1) ? h->nd[d] - 1 : 0;
-          if (pos[d] == at) {
-            if (!h->mask[idx]) h->dvalue[idx] = desc->dirichlet_value[f];
-            h->mask[idx] = 1;
-          }
-        }
-      }
+  h->dirichlet_mask = desc->dirichlet_mask;
+  orc_set_dirichlet_values(h, desc->dirichlet_value);
 
   /* colouring */
   for (int col = 0; col < 8; ++col) h->color_n[col] = 0;
@@ -459,6 +447,31 @@ void orc_support_points(const orc_heat *h, double *xyz)
         cell_map(h, c, xi, x, Jm);
         const int64_t idx = I + h->nd[0] * (J + (int64_t)h->nd[1] * K);
         for (int d = 0; d < 3; ++d) xyz[3 * idx + d] = x[d];
+      }
+}
+
+/* Dirichlet values per face (the first flagged face in the order x-, x+, y-, y+, z-, z+ owns
+ * an edge or corner DoF); called again for boundary data that change in time
+ * (HeatData::enable_time_dependent_bc: init_time_advance rebuilds the constraints every step,
+ * heat_diffuse_operation.cpp:219-226) */
+void orc_set_dirichlet_values(orc_heat *h, const double values[6])
+{
+  for (int64_t K = 0; K < h->nd[2]; ++K)
+    for (int64_t J = 0; J < h->nd[1]; ++J)
+      for (int64_t I = 0; I < h->nd[0]; ++I) {
+        const int64_t idx = I + h->nd[0] * (J + (int64_t)h->nd[1] * K);
+        const int64_t pos[3] = {I, J, K};
+        int owned = 0;
+        for (int f = 0; f < 6; ++f) {
+          if (!(h->dirichlet_mask & (1 << f))) continue;
+          const int d = f / 2;
+          const int64_t at = (f & 1) ? h->nd[d] - 1 : 0;
+          if (pos[d] == at) {
+            if (!owned) h->dvalue[idx] = values[f];
+            owned = 1;
+            h->mask[idx] = 1;
+          }
+        }
       }
 }
 

@@ -112,6 +112,8 @@ int orc_set_material(orc_heat *h, const orc_material *m, double dt);
  * (:1044-1049).  Either may be NULL (no heaviside: weight 1, the liquid or liquid-solid
  * properties).  Returns -1 if a velocity is combined with the linear-k law. */
 int orc_set_fields(orc_heat *h, const double *heaviside, const double *velocity);
+/* Dirichlet values per face from now on (time-dependent boundary data) */
+void orc_set_dirichlet_values(orc_heat *h, const double values[6]);
 
 /* dst = J(T_lin, T_old) src.  form 0: sum-factorised, 1: direct quadrature,
  * 2: sum-factorised Picard operator (the tangent without its dk/dT grad(T_lin) u

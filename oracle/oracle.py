@@ -117,6 +117,8 @@ def lib():
             L.orc_set_fields.argtypes = [_P, _D, _D]
             L.orc_material_eval.argtypes = [C.POINTER(Material), C.c_double, C.c_double, _D]
             L.orc_material_eval.restype = None
+            L.orc_set_dirichlet_values.argtypes = [_P, _D]
+            L.orc_set_dirichlet_values.restype = None
             L.orc_vmult.argtypes = [_P, _D, _D, _D, _D, C.c_int]
             L.orc_inverse_diagonal.argtypes = [_P, _D, _D, _D, C.c_int]
             L.orc_create_rhs.argtypes = [_P, _D, _D, _D, _D]
@@ -237,6 +239,11 @@ class Oracle:
                              "apparent capacity with volume-specific rho*cp")
         self.dt = dt
         self._material = m
+
+    def set_dirichlet_values(self, values):
+        """Dirichlet values per face (x-, x+, y-, y+, z-, z+) from now on."""
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(6)
+        self.L.orc_set_dirichlet_values(self.h, _ptr(v))
 
     def set_fields(self, heaviside=None, velocity=None):
         """Nodal heaviside (n_dofs) and velocity ((3, n_dofs)) fields; None clears one."""

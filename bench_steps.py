@@ -2,7 +2,7 @@
 iterations of the mixed-precision solver (FP64 flexible CG + FP32 p-multigrid) and
 of plain FP64 Jacobi-CG on the same steps, and the difference of their fields.
 
-  python -m meltpooldg_b200.profile_step --degree 4 --cells 96 --perturb 0.2 \\
+  python bench_steps.py --degree 4 --cells 96 --perturb 0.2 \\
       --steps 6 --warmup 2
 
 Problem: unit cube, k(T) = 1 + 0.5 T, rho cp = 1, dt = 5e-4, Dirichlet 0, T0 = 0, a
@@ -23,8 +23,8 @@ import json
 
 import torch
 
-from . import _lib as L
-from . import heat as H
+from meltpooldg_b200 import _lib as L
+from meltpooldg_b200 import heat as H
 
 DT, AMP, RADIUS, Z0, SPEED = 5e-4, 500.0, 0.05, 0.95, 1.0
 

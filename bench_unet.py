@@ -1,6 +1,6 @@
 """Forward time of the learned-guess network on an (nx, ny, nz) grid.
 
-    python -m meltpooldg_b200.profile_unet --dims 97 97 97 [--reps 10]
+    python bench_unet.py --dims 97 97 97 [--reps 10]
 
 prints one JSON line with the CUDA-event time per forward (tensor-core
 convolutions, or the CUDA-core ones with MPDG_UNET_TC=0) and the nominal FLOPs
@@ -11,7 +11,7 @@ import os
 
 import torch
 
-from . import learned as LG
+from meltpooldg_b200 import learned as LG
 
 
 def conv_flops(dims):

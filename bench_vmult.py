@@ -1,6 +1,6 @@
 """Time (and give ncu a target for) the operator application on one mesh.
 
-  python -m meltpooldg_b200.profile_vmult --degree 3 --cells 96 --law 1 --reps 3
+  python bench_vmult.py --degree 3 --cells 96 --law 1 --reps 3
 prints one JSON line per precision with the CUDA-event time per application,
 DoFs/s and algorithmic GB/s (src + dst + linearisation point [+ per-q geometry]).
 With --solve it instead runs a few outer iterations of FP64 CG with the FP32
@@ -22,7 +22,7 @@ import json
 
 import torch
 
-from . import heat as H
+from meltpooldg_b200 import heat as H
 
 
 def main():
@@ -55,7 +55,7 @@ def main():
         vel = torch.stack([torch.sin(3 * x[:, 1]), 0.5 + x[:, 2], -x[:, 0] * x[:, 1]]).contiguous()
         op.set_fields(hs, vel)
     if a.solve:
-        from . import _lib as L
+        from meltpooldg_b200 import _lib as L
         op.distribute_constraints(T)
         H.JacobiPreconditioner(op).update()
         b = op.vmult(op.new_vector(), torch.rand(N, dtype=torch.float64, device="cuda",

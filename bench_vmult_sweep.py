@@ -2,11 +2,11 @@
 deformed (interior vertices perturbed by up to 0.2 h), FP64 and FP32, constant
 coefficients: the vmult throughput table.
 
-  python -m meltpooldg_b200.sweep_vmult [--size large|small] [--reps 10]
+  python bench_vmult_sweep.py [--size large|small] [--reps 10]
 
 Meshes hold ~64 M (large) or ~2 M (small) DoFs: 399/125 cells per direction at
 p = 1, 199/62 (p = 2), 133/42 (3), 100/31 (4), 80/25 (5), 66/21 (6). Each case runs
-in its own process (profile_vmult); prints one JSON line per case and a markdown
+in its own process (bench_vmult.py); prints one JSON line per case and a markdown
 table with GDoF/s, algorithmic GB/s (src + dst [+ 7 per-q geometry factors]) and
 its fraction of the measured HBM bandwidth.
 """
@@ -18,14 +18,15 @@ import os
 import subprocess
 import sys
 
+HERE = os.path.dirname(os.path.abspath(__file__))
+
 CELLS = {"large": {1: 399, 2: 199, 3: 133, 4: 100, 5: 80, 6: 66},
          "small": {1: 125, 2: 62, 3: 42, 4: 31, 5: 25, 6: 21}}
 
 
 def hbm_peak():
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     try:
-        return float(json.load(open(os.path.join(root, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return float(json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))["hbm_gbs"])
     except Exception:
         return 6650.0
 
@@ -39,7 +40,7 @@ def main():
     rows = []
     for p, m in CELLS[a.size].items():
         for perturb in (0.0, 0.2):
-            r = subprocess.run([sys.executable, "-m", "meltpooldg_b200.profile_vmult", "--degree",
+            r = subprocess.run([sys.executable, os.path.join(HERE, "bench_vmult.py"), "--degree",
                                 str(p), "--cells", str(m), "--perturb", str(perturb), "--law", "0",
                                 "--reps", str(a.reps), "--dtype", "both"],
                                capture_output=True, text=True)

@@ -245,14 +245,16 @@ int mpdg_heat_create_rhs(mpdg_heat *h, double *dst, const double *src,
 int mpdg_heat_distribute_constraints(mpdg_heat *h, double *u);
 /* VectorTools::compute_norm(u, L2) with QGauss(p+1) (vector_tools.cpp:188-200). */
 int mpdg_heat_l2_norm(mpdg_heat *h, const double *u, double *norm);
-/* FE L2 norm for callers that cannot allocate device memory (CUDA-graph capture,
- * a foreign memory pool, loops that must not synchronise on a first-use allocation).
- * No counterpart in the reference. Writes |u|_L2 to the caller's device scalar
- * `norm` on the handle's stream; the reduction scratch is a fixed 128 KiB array
- * in the library (at most 16384 partial sums; larger reductions are rejected with
- * MPDG_ERR_INVALID_ARGUMENT), so the call calls no cudaMalloc/cudaFree. The
- * first call on a device looks up that array's device address (do it before any
- * stream capture). Calls share the array: calls that overlap on the GPU race. */
+/* FE L2 norm for callers that cannot allocate device memory (code inside a foreign
+ * memory pool whose accounting a raw allocation would break, loops that must not
+ * synchronise on a first-use allocation). No counterpart in the reference. Writes
+ * |u|_L2 to the caller's device scalar `norm` on the handle's stream; the reduction
+ * scratch is a fixed 128 KiB array in the library (at most 16384 partial sums;
+ * larger reductions are rejected with MPDG_ERR_INVALID_ARGUMENT), so the call calls
+ * no cudaMalloc/cudaFree. The first call on a device looks up that array's device
+ * address and caches it (make it before any stream capture; the cached address is
+ * not valid after cudaDeviceReset). Calls share the array: calls that overlap on
+ * the GPU race. */
 int mpdg_heat_l2_norm_noalloc(mpdg_heat *h, const double *u, double *norm);
 /* DoF support point coordinates, xyz[3*i + d] (device pointer, 3*n_dofs doubles). */
 int mpdg_heat_support_points(mpdg_heat *h, double *xyz);

@@ -22,6 +22,8 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -447,7 +449,34 @@ extern "C" int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine
   for (int d = 0; d < 3; ++d)
     if (desc->cells[d] < 1 || !(desc->hi[d] > desc->lo[d]))
       return fail(MPDG_ERR_INVALID_ARGUMENT, "invalid box");
-  mpdg_amr *h = new mpdg_amr();
+  // Bound the host description before building it: active cells x (p+1)^3 gathered entries
+  // (32-bit device indices), and lattice coordinates below 2^20 (the cell map's key packs
+  // each of them into 20 bits).
+  {
+    const int64_t n3 = (int64_t)(desc->degree + 1) * (desc->degree + 1) * (desc->degree + 1);
+    const int64_t n_coarse = (int64_t)desc->cells[0] * desc->cells[1] * desc->cells[2];
+    int max_level = 0;
+    int64_t entries = 0;
+    for (int64_t c = 0; c < n_coarse; ++c) {
+      const int L = refine[c];
+      if (L > kAmrMaxLevel)
+        return fail(MPDG_ERR_INVALID_ARGUMENT, "refinement level above the maximum");
+      max_level = std::max(max_level, L);
+      entries += ((int64_t)1 << (3 * L)) * n3;
+      if (entries >= ((int64_t)1 << 31))
+        return fail(MPDG_ERR_INVALID_ARGUMENT,
+                    "hanging-node mesh too large (cells x (p+1)^3 must stay below 2^31)");
+    }
+    for (int d = 0; d < 3; ++d)
+      if (((int64_t)desc->cells[d] << max_level) >= ((int64_t)1 << 20))
+        return fail(MPDG_ERR_INVALID_ARGUMENT,
+                    "hanging-node mesh: cells per direction x 2^level must stay below 2^20");
+    if (device >= 0 && max_level > 1)
+      return fail(MPDG_ERR_NOT_SUPPORTED,
+                  "hanging-node meshes on the GPU: one refinement level (several on the host only)");
+  }
+  mpdg_amr *h = new (std::nothrow) mpdg_amr();
+  if (!h) return fail(MPDG_ERR_OUT_OF_MEMORY, "hanging-node mesh: host allocation failed");
   h->p = desc->degree;
   h->n = desc->degree + 1;
   h->device = device;
@@ -456,7 +485,14 @@ extern "C" int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine
     h->lo[d] = desc->lo[d];
     h->h[d] = (desc->hi[d] - desc->lo[d]) / desc->cells[d];
   }
-  int rc = build_host(h, desc, refine);
+  int rc;
+  try {
+    rc = build_host(h, desc, refine);
+  } catch (const std::bad_alloc &) {
+    rc = fail(MPDG_ERR_OUT_OF_MEMORY, "hanging-node mesh: host allocation failed");
+  } catch (const std::exception &e) {
+    rc = fail(MPDG_ERR_INVALID_ARGUMENT, std::string("hanging-node mesh: ") + e.what());
+  }
   if (rc != MPDG_OK) {
     delete h;
     return rc;

@@ -3600,9 +3600,8 @@ extern "C" int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset)
 // ---------------------------------------------------------------------------
 // FE L2 norm that allocates nothing
 //
-// Some callers cannot call cudaMalloc: code being captured into a CUDA graph
-// (allocation is not a capturable operation), code that runs inside another
-// framework's memory pool where raw driver allocations are forbidden or would
+// Some callers cannot call cudaMalloc: code that runs inside another
+// framework's memory pool, where raw driver allocations are forbidden or would
 // break its accounting, and loops that must not pay the implicit device
 // synchronisation of a first-use allocation. For them this variant of the L2
 // norm keeps its reduction scratch (one partial sum per CTA plus the last-CTA
@@ -3616,7 +3615,10 @@ extern "C" int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset)
 // array until the process exits. All calls on a device share it and it keeps
 // the last call's contents; the counter is cleared at the start of each call,
 // so calls that overlap on the GPU (different streams, or different host
-// threads on one device) race and must be serialised by the caller.
+// threads on one device) race and must be serialised by the caller. The first
+// call on a device looks up the array's device address (cudaGetSymbolAddress)
+// and caches it per device; make that first call before any stream capture.
+// The cached address is not valid after cudaDeviceReset on that device.
 // ---------------------------------------------------------------------------
 static constexpr int kNoAllocSlots = 16384;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlots + 32];

@@ -196,7 +196,10 @@ class HeatDiffuseOperator:
         """slab=(z_begin, z_end): this rank's z-slab of cells of the global mesh `mesh`
         (mpdg_heat_create_slab); the shared end planes are summed by the caller."""
         self._L = L.load()
-        self.mesh = mesh
+        # a private copy: set_dirichlet_values changes this operator's values only, not the
+        # caller's descriptor (which may also describe an oracle, a slab or another operator)
+        self.mesh = L.MeshDesc.from_buffer_copy(mesh)
+        mesh = self.mesh
         self.device = torch.device("cuda", device)
         h = C.c_void_p()
         if slab is None:

@@ -1,7 +1,7 @@
 """The allocation-free L2 norm (mpdg_heat_l2_norm_noalloc) through the C ABI.
 
-Callers that cannot allocate device memory (CUDA-graph capture, a foreign memory
-pool) use this entry point; it must agree with the ordinary mpdg_heat_l2_norm and
+Callers that cannot allocate device memory (code inside a foreign memory pool whose
+accounting a raw allocation would break) use this entry point; it must agree with the ordinary mpdg_heat_l2_norm and
 must not change the device's free memory. Two calls in a row check that the shared
 static scratch is reset between calls. Collected last on purpose.
 """

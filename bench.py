@@ -9,9 +9,12 @@ per step solved to |b - J T| <= 1e-8 |b|. The solvers run the same steps:
   mixed    FP64 flexible CG with the FP32 p-multigrid V-cycle preconditioner
   cheb     FP64 flexible CG with the FP32 degree-6 Chebyshev-Jacobi preconditioner
   learned  the mixed solver started from the learned guess
-`value` is the step throughput of the fastest one in DoFs advanced per second
-(whole job: summed over replicas when run with --gpus N > 1, which runs
-independent replicas: the path has no data-parallel exchange on one mesh).
+`value` is the step throughput of the fastest one (named in "variant") in DoFs
+advanced per second (whole job: summed over replicas when run with --gpus N > 1,
+which runs independent replicas: the path has no data-parallel exchange on one
+mesh). The CPU baseline and the reference arm run the oracle port (the reference's
+plain FP64 Jacobi-CG step) on the same 128^3 workload, bounded to a few steps; the
+first step's CPU solution is the FP64 reference of "error_vs_cpu_fp64".
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -34,6 +37,7 @@ DEGREE, CELLS, DT, K1 = 3, 128, 5e-4, 0.5
 AMP, RADIUS, Z0, SPEED, X0 = 500.0, 0.05, 0.95, 1.0, 0.1
 REL_TOL = 1e-8
 CHEB_DEGREE = 6
+REF_WARMUP, REF_STEPS = 1, 2  # CPU reference arm: bounded sample of the requested steps
 
 
 def source_center(t):
@@ -100,9 +104,11 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # CPU legs (oracle port: the reference's algorithm restated in C, OpenMP)
 # ---------------------------------------------------------------------------
-def cpu_step_sample(cells, steps):
-    """Implicit steps of the same problem on a smaller mesh with the oracle; returns
-    (DoFs/s, seconds, n_dofs, cores)."""
+def cpu_step_sample(cells, steps, first=0, keep=None):
+    """Implicit steps `first` .. `first + steps - 1` of the same problem with the oracle
+    (plain FP64 Jacobi-CG, the reference's algorithm), from T0 = 0; the steps before
+    `first` run untimed. Returns (DoFs/s, seconds, n_dofs, cores); with a dict `keep`, the
+    solution after the first step is stored in keep["T1"]."""
     import numpy as np
     from oracle import oracle as O
     o = O.Oracle(DEGREE, (cells,) * 3)
@@ -111,7 +117,9 @@ def cpu_step_sample(cells, steps):
     T_old = np.zeros(o.n_dofs)
     dt_old = 0.0
     t0 = time.perf_counter()
-    for s in range(steps):
+    for s in range(first + steps):
+        if s == first:
+            t0 = time.perf_counter()
         t = (s + 1) * DT
         q = o.gaussian_source(AMP, source_center(t), RADIUS)
         Tg = o.linear_predictor(T, T_old, DT, dt_old)
@@ -122,26 +130,33 @@ def cpu_step_sample(cells, steps):
         if rn > 0.0:
             d, _, _ = o.cg(r, T_lin=T, T_old=T_old, rel_tol=REL_TOL * bn / rn, abs_tol=0.0)
             T = T + d
+        if keep is not None and s == 0:
+            keep["T1"] = T.copy()
         dt_old = DT
     sec = time.perf_counter() - t0
     return o.n_dofs * steps / sec, sec, o.n_dofs, os.cpu_count()
 
 
 def run_reference(args):
+    """The reference's algorithm (plain FP64 Jacobi-CG steps, the oracle port on all host
+    cores) on the benchmark's own workload. A CPU step of the 128^3 mesh takes tens of
+    seconds, so the run is a bounded sample: at most REF_WARMUP untimed and REF_STEPS timed
+    steps of the requested W and K (stated in the line)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     cells = args.cpu_cells
-    for _ in range(args.warmup):
-        cpu_step_sample(cells, 1)
-    rate, sec, n, cores = cpu_step_sample(cells, args.steps)
-    sample = (f"{args.steps} implicit steps of the same problem on {cells}^3 cells ({n} DoFs) "
-              f"with the oracle port (OpenMP, {cores} threads)")
+    warm, steps = min(args.warmup, REF_WARMUP), min(args.steps, REF_STEPS)
+    rate, sec, n, cores = cpu_step_sample(cells, steps, first=warm)
+    sample = (f"steps {warm}..{warm + steps - 1} of the workload on {cells}^3 cells ({n} DoFs) "
+              f"after {warm} untimed, oracle port (OpenMP, {cores} threads); a bounded sample "
+              f"of the requested --warmup {args.warmup} --steps {args.steps}")
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "DoF/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True, "scaling": "weak",
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "steps_requested": args.steps, "warmup_requested": args.warmup,
+            "ms_per_step": 1e3 * sec / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(CELLS),
+            "config": workload_config(cells), "parallelism": "CPU, rank 0 only",
             "cpu_baseline": {"value": rate, "unit": "DoF/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": rate, "unit": "DoF/s", "h2d_bytes_per_step": 0,
@@ -321,7 +336,9 @@ def run_mine(args):
     W, K = args.warmup, args.steps
     # mixed precision first: the headline timed region (clock sampling, launch count),
     # then K more steps with per-operator CUDA-event timing for the kernel shares
-    march(mixed, 0, W)
+    march(mixed, 0, 1)
+    first_step = {"mixed": mixed.T.clone()}  # compared with the CPU FP64 solution below
+    march(mixed, 1, W - 1)
     T_W, T_old_W = mixed.T.clone(), mixed.T_old.clone()  # state before the timed steps
     clocks = Clocks(local) if rank == 0 else None
     op.counters(reset=True)
@@ -345,7 +362,9 @@ def run_mine(args):
     # plain FP64 Jacobi-CG on the same steps
     ms_plain = its_plain = None
     if not args.no_plain:
-        march(plain, 0, W)
+        march(plain, 0, 1)
+        first_step["plain"] = plain.T.clone()
+        march(plain, 1, W - 1)
         ms_plain, its_plain, _ = timed(plain, W, K)
     err = None
     if not args.no_plain:
@@ -484,20 +503,46 @@ def run_mine(args):
                 "note": "share from CUDA events around every operator launch of K further "
                         "steps; duration from back-to-back launches"}
 
-    cpu = None
-    if not args.no_cpu:
-        rate, sec, n, cores = cpu_step_sample(args.cpu_cells, args.cpu_steps)
+    # CPU baseline (rank 0, one GPU): the oracle port's first step of the same workload; its
+    # solution is the FP64 CPU solution the GPU solvers' first step is compared with
+    cpu = cpu_err = None
+    if not args.no_cpu and world == 1:
+        keep = {}
+        rate, sec, n, cores = cpu_step_sample(args.cpu_cells, args.cpu_steps, keep=keep)
         cpu = {"value": rate, "unit": "DoF/s", "cores": cores, "kind": "port",
-               "sample": f"{args.cpu_steps} implicit steps of the same problem on "
-                         f"{args.cpu_cells}^3 cells ({n} DoFs), oracle port, {sec:.1f} s"}
+               "sample": f"the first {args.cpu_steps} implicit step(s) of the workload on "
+                         f"{args.cpu_cells}^3 cells ({n} DoFs), oracle port (plain FP64 "
+                         f"Jacobi-CG, OpenMP), {sec:.1f} s"}
+        if args.cpu_cells == cells:
+            ref = torch.from_numpy(keep["T1"]).to(dev)
+            rn, rm = torch.linalg.vector_norm(ref).item(), ref.abs().max().item()
+            cpu_err = {"step": 1, "reference": "oracle FP64 Jacobi-CG on the host, |b-JT|<=1e-8|b|"}
+            for name, T1 in first_step.items():
+                cpu_err[name] = {"rel_l2": torch.linalg.vector_norm(T1 - ref).item() / rn,
+                                 "rel_max": (T1 - ref).abs().max().item() / rm}
+            del ref
+    del first_step
 
-    best_ms = min(x for x in (ms_mixed, ms_cheb, ms_plain, ms_learned) if x)
+    # headline: the fastest solver on these steps (named in "variant"); every variant's
+    # time is reported beside it
+    variants = {"mixed": ms_mixed, "cheb": ms_cheb, "plain": ms_plain,
+                "learned+mixed": ms_learned}
+    best = min((v, k) for k, v in variants.items() if v)
+    best_ms, best_name = best
     line = {
         "metric": METRIC, "value": replica_throughput(world, N, K, best_ms), "unit": "DoF/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": best_ms / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 (outer CG) + f32 (Chebyshev preconditioner)", "data": "synthetic",
-        "config": {**workload_config(cells), "parallelism": f"replicas x{world}"},
+        "variant": best_name,
+        "variant_note": {
+            "mixed": "FP64 flexible CG + FP32 p-multigrid, linear-extrapolation predictor",
+            "learned+mixed": "the mixed solver started from the learned guess",
+            "cheb": "FP64 flexible CG + FP32 Chebyshev(6)",
+            "plain": "FP64 Jacobi-CG"}[best_name],
+        "dtype": "f64 (outer flexible CG, k(T) tangent, residual) + f32 (p-multigrid "
+                 "preconditioner)" if best_name != "plain" else "f64",
+        "data": "synthetic",
+        "config": workload_config(cells), "parallelism": f"replicas x{world}",
         "mixed_ms_per_step": ms_mixed / K,
         "plain_fp64_ms_per_step": ms_plain / K if ms_plain else None,
         "speedup_mixed_vs_plain": (ms_plain / ms_mixed) if ms_plain else None,
@@ -522,6 +567,7 @@ def run_mine(args):
                                      "replayed",
                          "cheb": f"FP32 Chebyshev-Jacobi degree {CHEB_DEGREE}, Picard operator"},
         "mixed_vs_plain_error": err,
+        "error_vs_cpu_fp64": cpu_err,
         "vmult_fp64_gdofs": N / (vm_ms / 1e3) / 1e9, "vmult_fp64_ms": vm_ms,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": launches, "clocks": clk,
@@ -539,8 +585,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
-    ap.add_argument("--cpu-cells", type=int, default=48)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-cells", type=int, default=CELLS)
+    ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cheb", action="store_true")

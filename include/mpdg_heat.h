@@ -241,6 +241,31 @@ int mpdg_heat_compute_diagonal(mpdg_heat *h, double *diag);
  * (may be NULL for zero); dst is not zeroed. */
 int mpdg_heat_create_rhs(mpdg_heat *h, double *dst, const double *src,
                          const double *heat_source);
+/* ---- OperatorMatrixFree verbs on HOST vectors ------------------------------------------
+ * OperatorMatrixFree<dim, double>::VectorType is the host vector
+ * dealii::LinearAlgebra::distributed::Vector<double> (operator_base.hpp:192); on one rank its
+ * local array holds every DoF. These verbs take such arrays (length n_dofs, host memory, in
+ * the caller's DoF numbering), copy them into device mirrors the handle keeps, run the device
+ * verb and copy the result back before returning (the stream is synchronised).
+ * set_dof_permutation gives the caller's numbering: lex_of_dof[i] is the lexicographic index
+ * (I + nx (J + ny K) on the nodal grid) of the caller's DoF i; it must be a permutation of
+ * 0 .. n_dofs-1 (MPDG_ERR_INVALID_ARGUMENT otherwise); NULL restores the identity. deal.II
+ * numbers DoFs cell by cell, so a MeltPoolDG adapter passes the map built from its
+ * DoFHandler. The device verbs above keep taking lexicographic vectors. */
+int mpdg_heat_set_dof_permutation(mpdg_heat *h, const int64_t *lex_of_dof);
+/* HeatDiffuseMultiPhaseOperator::pre() with the operator's references to temperature and
+ * temperature_old (heat_diffuse_operator.hpp:128-135): copies both to the device mirrors and
+ * linearises there (T_old may be NULL). */
+int mpdg_heat_set_linearization_host(mpdg_heat *h, const double *T, const double *T_old);
+/* vmult(dst, src) (heat_diffuse_operator.cpp:179-197) on host vectors. */
+int mpdg_heat_vmult_host(mpdg_heat *h, double *dst, const double *src);
+/* compute_inverse_diagonal_from_matrixfree(diag) (heat_diffuse_operator.cpp:271-284). */
+int mpdg_heat_compute_inverse_diagonal_host(mpdg_heat *h, double *inv_diag);
+/* create_rhs(dst, src) (heat_diffuse_operator.cpp:783-806): dst += -R(T), src = T_old,
+ * heat_source the nodal source (may be NULL). */
+int mpdg_heat_create_rhs_host(mpdg_heat *h, double *dst, const double *src,
+                              const double *heat_source);
+
 /* AffineConstraints::distribute: set Dirichlet DoFs of u to their values. */
 int mpdg_heat_distribute_constraints(mpdg_heat *h, double *u);
 /* VectorTools::compute_norm(u, L2) with QGauss(p+1) (vector_tools.cpp:188-200). */
@@ -285,6 +310,9 @@ typedef struct {
   double reflectivity;            /* Gusarov: rho                                        */
   double extinction_coefficient;  /* Gusarov: beta                                       */
   double layer_thickness;         /* Gusarov: L                                          */
+  int    planar;                  /* 1: the profile of a 2D problem (laser_intensity_profiles
+                                     with dim = 2) on a mesh one cell thick in y: distances
+                                     in the x-z plane, z the depth direction; 0: 3D         */
 } mpdg_laser;
 int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser *laser);
 
@@ -342,7 +370,10 @@ int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, double dt, do
                         mpdg_step_stats *stats);
 
 /* Same with HOST vectors: copies T_cur, T_old, heat_source to the device, runs the
- * step, copies T_cur and T_old back (the reference operation's own data location). */
+ * step, copies T_cur and T_old back (the reference operation's own data location). The
+ * host vectors of the time-step entry points (here and in the resident ones below) are in
+ * the lexicographic numbering; mpdg_heat_set_dof_permutation applies to the *_host verbs
+ * above only. */
 int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *prm, double dt,
                              double dt_old, double *T_cur, double *T_old,
                              const double *heat_source, mpdg_step_stats *stats);

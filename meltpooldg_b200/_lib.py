@@ -84,7 +84,7 @@ class Laser(C.Structure):
     _fields_ = [("profile", C.c_int), ("power", C.c_double), ("position", C.c_double * 3),
                 ("direction", C.c_double * 3), ("radius", C.c_double),
                 ("reflectivity", C.c_double), ("extinction_coefficient", C.c_double),
-                ("layer_thickness", C.c_double)]
+                ("layer_thickness", C.c_double), ("planar", C.c_int)]
 
 
 class Counters(C.Structure):
@@ -121,6 +121,11 @@ _SIGS = {
     "mpdg_heat_compute_inverse_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_compute_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),
+    "mpdg_heat_set_dof_permutation": (C.c_int, [_H, _P]),
+    "mpdg_heat_set_linearization_host": (C.c_int, [_H, _D, _D]),
+    "mpdg_heat_vmult_host": (C.c_int, [_H, _D, _D]),
+    "mpdg_heat_compute_inverse_diagonal_host": (C.c_int, [_H, _D]),
+    "mpdg_heat_create_rhs_host": (C.c_int, [_H, _D, _D, _D]),
     "mpdg_heat_distribute_constraints": (C.c_int, [_H, _D]),
     "mpdg_heat_l2_norm": (C.c_int, [_H, _D, C.POINTER(C.c_double)]),
     "mpdg_heat_l2_norm_noalloc": (C.c_int, [_H, _D, _D]),

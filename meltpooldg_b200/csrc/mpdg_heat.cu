@@ -151,6 +151,10 @@ struct mpdg_heat {
          *w3 = nullptr;
   float *r32 = nullptr, *x32 = nullptr, *d32 = nullptr, *Ax32 = nullptr;
   double *host_T = nullptr, *host_To = nullptr, *host_q = nullptr;  // device buffers for *_host
+  // host-vector verbs: device mirrors of the linearisation point and of the verb's vectors,
+  // and the caller's DoF numbering (lex[i] = lexicographic index of the caller's DoF i)
+  double *hv_T = nullptr, *hv_To = nullptr, *hv_a = nullptr, *hv_b = nullptr, *hv_c = nullptr;
+  int64_t *perm = nullptr, *perm_buf = nullptr;  // perm: perm_buf while a permutation is set
   const double *guess = nullptr;
   int64_t bytes = 0;
   std::vector<void *> owned;
@@ -468,7 +472,7 @@ __global__ void k_gaussian(int64_t N, PosArgs a, double *q, double amp, double c
 // volumetric laser intensity at x (laser_intensity_profiles.hpp), parameters precomputed
 // on the host
 struct LaserArgs {
-  int profile;
+  int profile, planar;  // planar: the y coordinate is ignored (2D profile in the x-z plane)
   double power, c[3], dir[3], radius, peak;
   double rho, beta, L, lambda, a, D;  // Gusarov
 };
@@ -484,7 +488,7 @@ __device__ __forceinline__ double gusarov_dq_dxi(const LaserArgs &g, double xi)
 }
 __device__ __forceinline__ double laser_intensity(const LaserArgs &g, const double x[3])
 {
-  const double v0 = x[0] - g.c[0], v1 = x[1] - g.c[1], v2 = x[2] - g.c[2];
+  const double v0 = x[0] - g.c[0], v1 = g.planar ? 0.0 : x[1] - g.c[1], v2 = x[2] - g.c[2];
   if (g.profile == MPDG_LASER_UNIFORM) return g.power;
   if (g.profile == MPDG_LASER_GAUSS_VOLUMETRIC) {
     const double s2 = (v0 * v0 + v1 * v1 + v2 * v2) / (g.radius * g.radius);
@@ -3099,6 +3103,139 @@ extern "C" int mpdg_heat_create_rhs(mpdg_heat *h, double *dst, const double *src
   return create_rhs(h, dst, src, heat_source);
 }
 
+// ---------------------------------------------------------------------------
+// host-vector verbs (OperatorMatrixFree's VectorType is the host vector
+// LinearAlgebra::distributed::Vector<number>, operator_base.hpp:192): the vectors are
+// copied into device mirrors the handle keeps, renumbered from the caller's DoF order to
+// the lexicographic one on the device, and the results copied back
+// ---------------------------------------------------------------------------
+__global__ void k_perm_in(int64_t N, const int64_t *__restrict__ lex, const double *__restrict__ x,
+                          double *__restrict__ y)
+{
+  GRID_STRIDE(i, N) y[lex[i]] = x[i];
+}
+
+__global__ void k_perm_out(int64_t N, const int64_t *__restrict__ lex, const double *__restrict__ y,
+                           double *__restrict__ x)
+{
+  GRID_STRIDE(i, N) x[i] = y[lex[i]];
+}
+
+static int host_mirrors(mpdg_heat *h)
+{
+  TRY(dvec(h, &h->hv_a, h->n_dofs));
+  TRY(dvec(h, &h->hv_b, h->n_dofs));
+  TRY(dvec(h, &h->hv_c, h->n_dofs));
+  return MPDG_OK;
+}
+
+// host vector in caller numbering -> device vector in lexicographic numbering
+static int upload_host(mpdg_heat *h, double *dev, const double *host)
+{
+  const int64_t N = h->n_dofs;
+  if (!h->perm) {
+    CU(cudaMemcpyAsync(dev, host, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream));
+    return MPDG_OK;
+  }
+  CU(cudaMemcpyAsync(h->hv_c, host, sizeof(double) * N, cudaMemcpyHostToDevice, h->stream));
+  k_perm_in<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->perm, h->hv_c, dev);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+// device vector in lexicographic numbering -> host vector in caller numbering; synchronises
+static int download_host(mpdg_heat *h, double *host, const double *dev)
+{
+  const int64_t N = h->n_dofs;
+  const double *from = dev;
+  if (h->perm) {
+    k_perm_out<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->perm, dev, h->hv_c);
+    ++h->launches;
+    CU(cudaGetLastError());
+    from = h->hv_c;
+  }
+  CU(cudaMemcpyAsync(host, from, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_dof_permutation(mpdg_heat *h, const int64_t *lex_of_dof)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  CU(cudaSetDevice(h->device));
+  if (!lex_of_dof) {
+    h->perm = nullptr;  // identity (the buffer stays owned by the handle)
+    return MPDG_OK;
+  }
+  const int64_t N = h->n_dofs;
+  std::vector<unsigned char> seen((size_t)N, 0);
+  for (int64_t i = 0; i < N; ++i) {
+    const int64_t v = lex_of_dof[i];
+    if (v < 0 || v >= N || seen[(size_t)v])
+      return fail(MPDG_ERR_INVALID_ARGUMENT,
+                  "DoF permutation: entry " + std::to_string(i) + " is out of range or repeated");
+    seen[(size_t)v] = 1;
+  }
+  TRY(dvec(h, &h->perm_buf, N));
+  CU(cudaMemcpyAsync(h->perm_buf, lex_of_dof, sizeof(int64_t) * N, cudaMemcpyHostToDevice,
+                     h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  h->perm = h->perm_buf;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_linearization_host(mpdg_heat *h, const double *T, const double *T_old)
+{
+  if (!h || !T) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  TRY(host_mirrors(h));
+  TRY(dvec(h, &h->hv_T, h->n_dofs));
+  TRY(upload_host(h, h->hv_T, T));
+  if (T_old) {
+    TRY(dvec(h, &h->hv_To, h->n_dofs));
+    TRY(upload_host(h, h->hv_To, T_old));
+  }
+  return mpdg_heat_set_linearization(h, h->hv_T, T_old ? h->hv_To : nullptr);
+}
+
+extern "C" int mpdg_heat_vmult_host(mpdg_heat *h, double *dst, const double *src)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  TRY(host_mirrors(h));
+  TRY(upload_host(h, h->hv_a, src));
+  TRY(mpdg_heat_vmult(h, h->hv_b, h->hv_a));
+  return download_host(h, dst, h->hv_b);
+}
+
+extern "C" int mpdg_heat_compute_inverse_diagonal_host(mpdg_heat *h, double *inv_diag)
+{
+  if (!h || !inv_diag) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  TRY(host_mirrors(h));
+  TRY(compute_diag(h, h->hv_b));
+  return download_host(h, inv_diag, h->hv_b);
+}
+
+extern "C" int mpdg_heat_create_rhs_host(mpdg_heat *h, double *dst, const double *src,
+                                         const double *heat_source)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  TRY(host_mirrors(h));
+  TRY(upload_host(h, h->hv_b, dst));
+  TRY(upload_host(h, h->hv_a, src));
+  double *q = nullptr;
+  if (heat_source) {
+    TRY(dvec(h, &h->host_q, h->n_dofs));
+    TRY(upload_host(h, h->host_q, heat_source));
+    q = h->host_q;
+  }
+  TRY(create_rhs(h, h->hv_b, h->hv_a, q));
+  return download_host(h, dst, h->hv_b);
+}
+
 static int distribute(mpdg_heat *h, double *u)
 {
   DirArgs a;
@@ -3174,6 +3311,7 @@ extern "C" int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser 
   LaserArgs g;
   memset(&g, 0, sizeof(g));
   g.profile = pr;
+  g.planar = laser->planar != 0;
   g.power = laser->power;
   for (int e = 0; e < 3; ++e) {
     g.c[e] = laser->position[e];

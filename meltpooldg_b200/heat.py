@@ -186,6 +186,25 @@ def _ptr(t: torch.Tensor | None, dtype=torch.float64):
     return t.data_ptr()
 
 
+def _host_ptr(a, n=None, dtype=None):
+    """Data pointer of a contiguous host array (numpy or CPU torch) of n float64 values."""
+    if a is None:
+        return None
+    import numpy as np
+    if isinstance(a, torch.Tensor):
+        if a.is_cuda or not a.is_contiguous() or a.dtype != (dtype or torch.float64):
+            raise ExcInvalidArgument("expected a contiguous host tensor")
+        size, ptr = a.numel(), a.data_ptr()
+    else:
+        want = np.int64 if dtype is torch.int64 else np.float64
+        if not isinstance(a, np.ndarray) or a.dtype != want or not a.flags.c_contiguous:
+            raise ExcInvalidArgument(f"expected a contiguous {want.__name__} numpy array")
+        size, ptr = a.size, a.ctypes.data
+    if n is not None and size != n:
+        raise ExcInvalidArgument(f"expected {n} values, got {size}")
+    return C.c_void_p(ptr)
+
+
 # ---------------------------------------------------------------------------
 # operator
 # ---------------------------------------------------------------------------
@@ -331,6 +350,33 @@ class HeatDiffuseOperator:
         check(self._L.mpdg_heat_distribute_constraints(self.h, _ptr(u)))
         return u
 
+    # verbs on host vectors (OperatorMatrixFree's VectorType lives in host memory) --------
+    def set_dof_permutation(self, lex_of_dof):
+        """The caller's DoF numbering: lex_of_dof[i] is the lexicographic index of the
+        caller's DoF i (int64 host array); None restores the identity."""
+        self._perm = lex_of_dof
+        check(self._L.mpdg_heat_set_dof_permutation(
+            self.h, _host_ptr(lex_of_dof, self.n_dofs, torch.int64)))
+
+    def set_linearization_host(self, temperature, temperature_old=None):
+        check(self._L.mpdg_heat_set_linearization_host(
+            self.h, _host_ptr(temperature, self.n_dofs), _host_ptr(temperature_old, self.n_dofs)))
+
+    def vmult_host(self, dst, src):
+        check(self._L.mpdg_heat_vmult_host(self.h, _host_ptr(dst, self.n_dofs),
+                                           _host_ptr(src, self.n_dofs)))
+        return dst
+
+    def compute_inverse_diagonal_host(self, diag):
+        check(self._L.mpdg_heat_compute_inverse_diagonal_host(self.h, _host_ptr(diag, self.n_dofs)))
+        return diag
+
+    def create_rhs_host(self, dst, src, heat_source=None):
+        check(self._L.mpdg_heat_create_rhs_host(self.h, _host_ptr(dst, self.n_dofs),
+                                                _host_ptr(src, self.n_dofs),
+                                                _host_ptr(heat_source, self.n_dofs)))
+        return dst
+
     def l2_norm(self, u) -> float:
         v = C.c_double()
         check(self._L.mpdg_heat_l2_norm(self.h, _ptr(u), C.byref(v)))
@@ -350,13 +396,14 @@ class HeatDiffuseOperator:
         return x
 
     def laser_source(self, q, profile, power, position, radius=1.0, direction=(0.0, 0.0, -1.0),
-                     gusarov=(0.0, 0.0, 0.0)):
+                     gusarov=(0.0, 0.0, 0.0), planar=False):
         """LaserHeatSourceVolumetric::compute_volumetric_heat_source: q = I(x) at the
         support points for profile L.LASER_UNIFORM / _GAUSS_VOLUMETRIC / _GAUSS_PROJECTION /
-        _GUSAROV (gusarov = (reflectivity, extinction coefficient, layer thickness))."""
+        _GUSAROV (gusarov = (reflectivity, extinction coefficient, layer thickness));
+        planar: the 2D profile in the x-z plane of a mesh one cell thick in y."""
         las = L.Laser(int(profile), float(power), (C.c_double * 3)(*map(float, position)),
                       (C.c_double * 3)(*map(float, direction)), float(radius),
-                      *[float(v) for v in gusarov])
+                      *[float(v) for v in gusarov], int(bool(planar)))
         check(self._L.mpdg_heat_laser_source(self.h, _ptr(q), C.byref(las)))
         return q
 

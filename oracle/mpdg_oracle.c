@@ -1330,7 +1330,8 @@ static double orc_gusarov_dq_dxi(double rho, double lambda, double a, double D, 
 }
 
 void orc_laser_source(const orc_heat *h, double *q, int profile, double power, const double c[3],
-                      const double dir[3], double radius, double rho, double beta, double L)
+                      const double dir[3], double radius, double rho, double beta, double L,
+                      int planar)
 {
   double *xyz = (double *)malloc(sizeof(double) * 3 * h->n_dofs);
   orc_support_points(h, xyz);
@@ -1344,7 +1345,7 @@ void orc_laser_source(const orc_heat *h, double *q, int profile, double power, c
 #pragma omp parallel for num_threads(nthreads())
   for (int64_t i = 0; i < h->n_dofs; ++i) {
     const double *x = xyz + 3 * i;
-    const double v[3] = {x[0] - c[0], x[1] - c[1], x[2] - c[2]};
+    const double v[3] = {x[0] - c[0], planar ? 0.0 : x[1] - c[1], x[2] - c[2]};
     double val = 0.0;
     if (profile == 0) {
       val = power;

@@ -189,9 +189,12 @@ int orc_time_step_newton(orc_heat *h, double *T_cur, double *T_old, const double
  * q(x) = amp * exp(-|x - c|^2 / r^2) at the DoF support points. */
 void orc_gaussian_source(const orc_heat *h, double *q, double amp, const double c[3], double r);
 /* volumetric laser intensity at the support points; profile 0 uniform, 1 Gauss
- * volumetric, 2 Gauss projection (unit dir), 3 Gusarov (rho, beta, L) */
+ * volumetric, 2 Gauss projection (unit dir), 3 Gusarov (rho, beta, L); planar != 0: the
+ * two-dimensional profile of a 2D problem (points (x, z), the y coordinate of a one-cell-
+ * thick mesh ignored; laser_intensity_profiles.hpp with dim = 2) */
 void orc_laser_source(const orc_heat *h, double *q, int profile, double power, const double c[3],
-                      const double dir[3], double radius, double rho, double beta, double L);
+                      const double dir[3], double radius, double rho, double beta, double L,
+                      int planar);
 
 #ifdef __cplusplus
 }

@@ -140,7 +140,7 @@ def lib():
                                            C.c_double, C.c_double, C.c_double]
             L.orc_gaussian_source.argtypes = [_P, _D, C.c_double, _D, C.c_double]
             L.orc_laser_source.argtypes = [_P, _D, C.c_int, C.c_double, _D, _D, C.c_double,
-                                           C.c_double, C.c_double, C.c_double]
+                                           C.c_double, C.c_double, C.c_double, C.c_int]
             _lib = L
     return _lib
 
@@ -350,14 +350,15 @@ class Oracle:
         return rc, st
 
     def laser_source(self, profile, power, position, radius=1.0, direction=(0.0, 0.0, -1.0),
-                     gusarov=(0.0, 0.0, 0.0)):
+                     gusarov=(0.0, 0.0, 0.0), planar=False):
         """Volumetric laser intensity at the support points (profile 0 uniform, 1 Gauss
-        volumetric, 2 Gauss projection, 3 Gusarov with (reflectivity, extinction, layer))."""
+        volumetric, 2 Gauss projection, 3 Gusarov with (reflectivity, extinction, layer));
+        planar: the 2D profile in the x-z plane of a one-cell-thick mesh (y ignored)."""
         q = np.empty(self.n_dofs)
         c = np.ascontiguousarray(position, dtype=np.float64)
         d = np.ascontiguousarray(direction, dtype=np.float64)
         self.L.orc_laser_source(self.h, _ptr(q), int(profile), float(power), _ptr(c), _ptr(d),
-                                float(radius), *[float(v) for v in gusarov])
+                                float(radius), *[float(v) for v in gusarov], int(bool(planar)))
         return q
 
     def gaussian_source(self, amp, center, radius):

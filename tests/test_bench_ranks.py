@@ -58,3 +58,28 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
         cpu_cells, warmup, steps, gpus = 8, 3, 1, 2
     assert bench.run_reference(Args()) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_bounds_its_sample_and_keeps_the_config(monkeypatch, capsys):
+    """The CPU reference arm on rank 0 times at most REF_STEPS steps after at most REF_WARMUP,
+    says so, and prints the GPU arm's config for the same mesh."""
+    import json
+    monkeypatch.setenv("RANK", "0")
+
+    class Args:
+        cpu_cells, warmup, steps, gpus = 6, 5, 20, 1
+    assert bench.run_reference(Args()) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["steps"] == bench.REF_STEPS and line["warmup"] == bench.REF_WARMUP
+    assert line["steps_requested"] == 20 and line["warmup_requested"] == 5
+    assert line["config"] == bench.workload_config(6)
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert line["cpu_baseline"]["kind"] == "port"
+
+
+def test_cpu_sample_keeps_the_first_step():
+    keep = {}
+    rate, sec, n, cores = bench.cpu_step_sample(4, 1, keep=keep)
+    assert keep["T1"].shape == (n,) and rate > 0
+    assert keep["T1"].max() > 0.0  # the source heated the first step

@@ -1,0 +1,123 @@
+"""The latent heat of fusion (apparent heat capacity in the mushy zone) in the GPU operator,
+against the oracle: the liquid-solid law (mushy zone) and the gas-liquid-solid law with every
+apparent-capacity profile, FP64 vmult, inverse diagonal and residual to 1e-12 relative, the FP32
+operator to 2e-5; and one implicit Newton step through the GPU time step.
+
+Material and temperatures follow the reference's apparent-capacity unit test
+(unit_tests/heat/apparent_capacity.cpp: solidus 271, liquidus 275), with temperatures sampled
+across the mushy zone so that the capacity profile and its derivative are exercised."""
+import numpy as np
+import pytest
+import torch
+
+from meltpooldg_b200 import _lib as L
+from meltpooldg_b200 import heat as H
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL64, TOL32 = 1e-12, 2e-5
+PROFILES = {"qlq": L.APPARENT_QLQ, "constant": L.APPARENT_CONSTANT,
+            "poly4_bell": L.APPARENT_POLY4_BELL}
+LAWS = {
+    "liquid_solid": dict(law=L.LAW_LIQUID_SOLID, rho=1000.0, cp=4226.0, k=0.556, rho_s=900.0,
+                         cp_s=1762.0, k_s=2.22, T_solidus=271.0, T_liquidus=275.0),
+    "three_phase": dict(law=L.LAW_GAS_LIQUID_SOLID, rho=1000.0, cp=4226.0, k=0.556, rho_s=900.0,
+                        cp_s=1762.0, k_s=2.22, T_solidus=271.0, T_liquidus=275.0, rho_g=1.2,
+                        cp_g=1005.0, k_g=0.026),
+}
+LATENT = 338e3
+
+
+def cuda(a, dtype=torch.float64):
+    return torch.tensor(a, dtype=dtype, device="cuda")
+
+
+def rel(a, b):
+    a = a.detach().cpu().double().numpy() if isinstance(a, torch.Tensor) else a
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def pair(degree, cells, perturb, law, profile, dt=0.5):
+    hi = (1.0, 1.2, 0.9)
+    o = O.Oracle(degree, cells, hi=hi, perturb=perturb, seed=4)
+    o.set_material(O.material(**LAWS[law], latent_heat=LATENT,
+                              apparent_capacity=PROFILES[profile]), dt)
+    g = H.HeatDiffuseOperator(H.box_mesh(degree, cells, (0, 0, 0), hi, perturb, 4))
+    g.set_material(H.material(**LAWS[law]))
+    g.set_latent_heat(LATENT, PROFILES[profile])
+    g.reset_time_increment(dt)
+    if LAWS[law]["law"] == L.LAW_GAS_LIQUID_SOLID:
+        x = o.support_points()
+        Hf = 0.5 + 0.5 * np.tanh((0.6 - x[:, 2]) / 0.1)
+        o.set_fields(Hf, None)
+        g.set_fields(cuda(Hf), None)
+    return o, g
+
+
+@pytest.mark.parametrize("degree,perturb", [(2, 0.0), (3, 0.2), (4, 0.1)])
+@pytest.mark.parametrize("law", list(LAWS))
+@pytest.mark.parametrize("profile", list(PROFILES))
+def test_latent_heat_operator_matches_oracle(degree, perturb, law, profile):
+    o, g = pair(degree, (4, 3, 3), perturb, law, profile)
+    rng = np.random.default_rng(3 * degree + len(profile))
+    N = o.n_dofs
+    src = rng.uniform(-1, 1, N)
+    Tl = rng.uniform(268.0, 278.0, N)  # across the mushy zone 271 .. 275
+    To = Tl - rng.uniform(0.0, 1.5, N)
+    q = rng.uniform(0, 1e4, N)
+    g.set_linearization(cuda(Tl), cuda(To))
+    ref = o.vmult(src, Tl, To)
+    assert rel(g.vmult(g.new_vector(), cuda(src)), ref) <= TOL64
+    assert rel(g.vmult(g.new_vector(torch.float32), cuda(src, torch.float32)), ref) <= TOL32
+    dref = o.inverse_diagonal(Tl, To)
+    dg = g.compute_inverse_diagonal_from_matrixfree(g.new_vector())
+    assert rel(1.0 / dg.cpu().numpy(), 1.0 / dref) <= TOL64
+    base = rng.uniform(-1, 1, N)
+    rref = o.create_rhs(Tl, To, q, dst=base.copy())
+    rg = cuda(base)
+    g.create_rhs(rg, cuda(To), cuda(q))
+    assert rel(rg, rref) <= TOL64
+
+
+def test_latent_heat_changes_the_operator_and_zero_switches_it_off():
+    o, g = pair(2, (3, 3, 3), 0.0, "liquid_solid", "qlq")
+    rng = np.random.default_rng(9)
+    N = o.n_dofs
+    src, Tl = rng.uniform(-1, 1, N), rng.uniform(271.5, 274.5, N)
+    g.set_linearization(cuda(Tl), cuda(Tl))
+    with_l = g.vmult(g.new_vector(), cuda(src)).cpu().numpy()
+    g.set_latent_heat(0.0)
+    without = g.vmult(g.new_vector(), cuda(src)).cpu().numpy()
+    o.set_material(O.material(**LAWS["liquid_solid"]), 0.5)
+    assert rel(without, o.vmult(src, Tl, Tl)) <= TOL64
+    assert rel(with_l, without) > 1e-3
+
+
+@pytest.mark.parametrize("profile", list(PROFILES))
+def test_newton_step_with_latent_heat_matches_oracle(profile):
+    """One implicit Newton step (GMRES, the reference's heat default) of a slab cooling through
+    the mushy zone, with the latent heat, on the GPU against the oracle's Newton step (3 to 5
+    Newton iterations in the oracle)."""
+    dt = 1.0
+    o = O.Oracle(2, (12, 2, 2), hi=(0.05, 0.01, 0.01), dirichlet_mask=0b1,
+                 dirichlet_value=(253.0, 0, 0, 0, 0, 0))
+    o.set_material(O.material(**LAWS["liquid_solid"], latent_heat=LATENT,
+                              apparent_capacity=PROFILES[profile]), dt)
+    g = H.HeatDiffuseOperator(H.box_mesh(2, (12, 2, 2), (0, 0, 0), (0.05, 0.01, 0.01),
+                                         dirichlet=("x-",), dirichlet_values={"x-": 253.0}))
+    g.set_material(H.material(**LAWS["liquid_solid"]))
+    g.set_latent_heat(LATENT, PROFILES[profile])
+    x = o.support_points()
+    T0 = o.distribute(272.0 + 2.0 * x[:, 0] / 0.05)
+    T, To = T0.copy(), T0.copy()
+    rc, _ = o.time_step_newton(T, To, dt, 0.0, predictor=0, rel_tol=1e-13, res_tol=1e-9,
+                               corr_tol=1e-10, solver="gmres")
+    assert rc == 0
+    lin = H.LinearSolverData(solver_type=L.SOLVER_GMRES, rel_tolerance=1e-13)
+    opn = H.HeatDiffuseOperation(g, lin, H.NonlinearSolverData(residual_tolerance=1e-9),
+                                 predictor=L.PREDICTOR_NONE)
+    opn.set_initial_condition(cuda(T0))
+    st = opn.solve(dt)
+    assert st.converged == 1 and st.newton_iterations >= 2
+    assert rel(opn.T, T) <= 1e-9

@@ -128,15 +128,16 @@ def test_picard_operator_rejects_other_laws():
         g.vmult_picard_f32(g.new_vector(torch.float32), x)
 
 
+@pytest.mark.parametrize("planar", [False, True])
 @pytest.mark.parametrize("profile", [0, 1, 2, 3])
 @pytest.mark.parametrize("degree,perturb", [(2, 0.15), (3, 0.0)])
-def test_laser_source_matches_oracle(profile, degree, perturb):
+def test_laser_source_matches_oracle(profile, degree, perturb, planar):
     """The four volumetric laser intensity profiles at the support points against the
     oracle, on a box with the powder surface at z = 0 (Gusarov's convention)."""
     lo, hi, cells = (0, 0, -1), (1, 1, 0), (5, 4, 6)
     o = O.Oracle(degree, cells, lo=lo, hi=hi, perturb=perturb, seed=2)
     g = H.HeatDiffuseOperator(H.box_mesh(degree, cells, lo, hi, perturb, 2))
-    kw = dict(radius=0.4, direction=(0.0, 0.6, -0.8), gusarov=(0.55, 15.0, 0.4))
+    kw = dict(radius=0.4, direction=(0.0, 0.6, -0.8), gusarov=(0.55, 15.0, 0.4), planar=planar)
     ref = o.laser_source(profile, 25.0, (0.45, 0.5, 0.0), **kw)
     q = g.laser_source(g.new_vector(), profile, 25.0, (0.45, 0.5, 0.0), **kw)
     assert rel(q, ref) <= 1e-13

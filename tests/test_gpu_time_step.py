@@ -373,3 +373,30 @@ def test_graph_replay_matches_direct_launches(tmp_path):
         Ta, Tb = torch.tensor(a["T"]), torch.tensor(b["T"])
         assert (Ta - Tb).abs().max() <= 1e-8 * Tb.abs().max()
     assert res["1"]["launches"] == res["0"]["launches"] > 0
+
+
+# applications/mp-heat-transfer/cases/melt_front_propagation/tests/
+#   melt_front_propagation_static_gusarov.mpirun=4.output
+GUSAROV = [3.46470e-01, 3.46530e-01, 3.46591e-01, 3.46653e-01, 3.46715e-01]
+
+
+def test_melt_front_propagation_static_gusarov_on_gpu():
+    """The reference's Gusarov laser case (2D Q1 96 x 32 on [0, 6e-4] x [-2e-4, 0], liquid-solid
+    steel, Dirichlet 1000 at x_max, dt 5e-6) through the GPU Newton path (GMRES, the heat
+    default), the source computed on the device with the planar Gusarov profile."""
+    op = H.HeatDiffuseOperator(H.box_mesh(1, (96, 1, 32), (0, 0, -2e-4), (6e-4, 1.0, 0.0),
+                                          dirichlet=("x+",), dirichlet_values={"x+": 1000.0}))
+    op.set_material(H.material(law=L.LAW_LIQUID_SOLID, rho=7850.0, cp=460.0, k=55.563,
+                               rho_s=7850.0, cp_s=700.0, k_s=17.0, T_solidus=1966.0,
+                               T_liquidus=1974.0))
+    q = op.laser_source(op.new_vector(), L.LASER_GUSAROV, 5.0, (0.0, 0.5, 0.0), radius=6e-5,
+                        gusarov=(0.7, 6e4, 5e-5), planar=True)
+    lin = H.LinearSolverData(solver_type=L.SOLVER_GMRES, rel_tolerance=1e-12)
+    opn = H.HeatDiffuseOperation(op, lin, H.NonlinearSolverData(residual_tolerance=1e-8))
+    opn.set_initial_condition(torch.full((op.n_dofs,), 1000.0, dtype=torch.float64,
+                                         device="cuda"))
+    opn.heat_source = q
+    for ref in GUSAROV:
+        st = opn.solve(5e-6)
+        assert st.converged == 1
+        assert float(f"{op.l2_norm(opn.T):.5e}") == ref

@@ -222,3 +222,39 @@ def test_material_law_values(kind):
         rhocp, kk, drhocp, dkk = O.material_eval(laws[kind], T, H)
         for got, want in [(kk, k), (dkk, dk), (rhocp, cp * rho), (drhocp, dcp * rho + drho * cp)]:
             assert abs(got - want) <= 5e-6 * max(abs(want), 1e-300) or got == want, (got, want)
+
+
+# applications/mp-heat-transfer/cases/melt_front_propagation/tests/
+#   melt_front_propagation_static_gusarov.mpirun=4.output
+GUSAROV = [3.46470e-01, 3.46530e-01, 3.46591e-01, 3.46653e-01, 3.46715e-01]
+
+
+def gusarov_case():
+    """melt_front_propagation_static_gusarov.json: 2D, Q1, [0, 6e-4] x [-2e-4, 0] as 3 x 1
+    cells refined 5 times (96 x 32, melt_front_propagation.templates.hpp:145-156), Dirichlet
+    T0 = 1000 on x = x_max (:247-264), T0 = 1000, liquid-solid mushy zone (steel: liquid k 55.563,
+    cp 460; solid k 17, cp 700; rho 7850; 1966..1974 K), dt = 5e-6, 5 steps, the volumetric
+    Gusarov laser (power 5, radius 6e-5 at (0, 0), reflectivity 0.7, extinction 6e4, layer 5e-5)
+    interpolated at the nodes, Newton residual tolerance 1e-8. The 2D vertical axis is z here;
+    the mesh is one cell (extent 1) thick in y and the profile is evaluated in the x-z plane."""
+    o = O.Oracle(1, (96, 1, 32), lo=(0, 0, -2e-4), hi=(6e-4, 1.0, 0.0), dirichlet_mask=0b10,
+                 dirichlet_value=(0, 1000.0, 0, 0, 0, 0))
+    m = O.material(O.LAW_LIQUID_SOLID, rho=7850.0, cp=460.0, k=55.563, rho_s=7850.0, cp_s=700.0,
+                   k_s=17.0, T_solidus=1966.0, T_liquidus=1974.0)
+    o.set_material(m, 5e-6)
+    q = o.laser_source(3, 5.0, (0.0, 0.5, 0.0), radius=6e-5, gusarov=(0.7, 6e4, 5e-5), planar=True)
+    return o, q
+
+
+def test_melt_front_propagation_static_gusarov():
+    o, q = gusarov_case()
+    assert np.count_nonzero(q) > 0 and np.all(q >= 0.0)
+    T = o.distribute(np.full(o.n_dofs, 1000.0))
+    T_old = np.zeros_like(T)
+    dt_old = 0.0
+    for ref in GUSAROV:
+        rc, st = o.time_step_newton(T, T_old, 5e-6, dt_old, heat_source=q, res_tol=1e-8,
+                                    solver="gmres")
+        dt_old = 5e-6
+        assert rc == 0 and st.converged
+        assert _six_digits(o.l2_norm(T), ref), (o.l2_norm(T), ref)

@@ -278,7 +278,8 @@ def run_mine(args):
         abs_tolerance=0.0, cheb_degree=CHEB_DEGREE, cheb_picard=True, cheb_eig_reuse=True),
         predictor=L.PREDICTOR_LINEAR, single_linearization=True)
     learned = H.HeatDiffuseOperation(op, H.LinearSolverData(**mg_data),
-                                     predictor=L.PREDICTOR_GIVEN, single_linearization=True)
+                                     predictor=L.PREDICTOR_LINEAR_DIRECTION,
+                                     single_linearization=True)
     q = op.new_vector()
     mixed.heat_source = q
     cheb.heat_source = q
@@ -308,9 +309,11 @@ def run_mine(args):
                 if s == 0:
                     opn.params.predictor = L.PREDICTOR_LINEAR
                 else:
-                    model.guess(op, opn.T, opn.T_old, q, DT, out=guess_buf)
-                    opn.set_guess(guess_buf)
-                    opn.params.predictor = L.PREDICTOR_GIVEN
+                    # the network's increment direction; the step starts its increment solve
+                    # from the residual-minimising multiple of it
+                    model.direction(op, opn.T, opn.T_old, q, DT, out=guess_buf)
+                    opn.set_direction(guess_buf)
+                    opn.params.predictor = L.PREDICTOR_LINEAR_DIRECTION
             st = opn.solve(DT)
             its.append(st.linear_iterations)
         return its
@@ -475,7 +478,7 @@ def run_mine(args):
         ys = torch.empty_like(xs)
         run = lambda: op.vmult_picard_f32(ys, xs)
     else:
-        kname = "k_vmult2<4,double,affine,linear_k>"
+        kname = "k_vmult2<4,double,affine,linear_k_tangent_fields>"
         kms = cnt["vmult64_ms"]
         alg_bytes = 3 * 8 * N  # src + dst + linearisation point
         xs = torch.rand(N, dtype=torch.float64, device=dev)
@@ -559,7 +562,8 @@ def run_mine(args):
                          "on 64^3, 32^3, 16^3, 8^3, 4^3; Chebyshev-Jacobi smoothing (2 pre, 2+1 "
                          "post steps over [upper/8, upper]; 8 steps on the coarsest level); "
                          "Picard operators (k(T_lin) at the q-points) on every level; Lanczos "
-                         "intervals reused across steps", "predictor": "linear extrapolation",
+                         "intervals reused across steps", "predictor": "linear extrapolation (learned: plus the network's increment direction, "
+                                      "scaled to minimise the initial residual)",
                          "outer_operator": "FP64 k(T) tangent from k(T_lin), k1 grad(T_lin) "
                                            "fields built once per linearisation (their build "
                                            "is inside the timed step)",

@@ -334,7 +334,13 @@ int mpdg_heat_linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *
                            const double *b, mpdg_solve_stats *stats);
 
 /* ---- time step --------------------------------------------------------- */
-enum { MPDG_PREDICTOR_NONE = 0, MPDG_PREDICTOR_LINEAR = 1, MPDG_PREDICTOR_GIVEN = 2 };
+/* LINEAR_DIRECTION (no reference counterpart; single_linearization only): the linear
+ * extrapolation is the linearisation point, and the increment solve starts from alpha d instead
+ * of 0, d the direction of mpdg_heat_set_direction (e.g. mpdg_heat_learned_direction) and
+ * alpha = argmin |r - alpha J d| (one operator application, handed to the solver as its
+ * initial A x); the converged T is that of LINEAR to the solver tolerance. */
+enum { MPDG_PREDICTOR_NONE = 0, MPDG_PREDICTOR_LINEAR = 1, MPDG_PREDICTOR_GIVEN = 2,
+       MPDG_PREDICTOR_LINEAR_DIRECTION = 3 };
 
 typedef struct {
   int    newton_max_iterations;   /* nonlinear_solver_data.hpp:13 default 10 */
@@ -359,6 +365,9 @@ void mpdg_step_params_default(mpdg_step_params *prm);
 /* Initial guess used by MPDG_PREDICTOR_GIVEN (e.g. a learned predictor's output);
  * a device pointer that must stay valid until the step has run. */
 int mpdg_heat_set_guess(mpdg_heat *h, const double *guess);
+/* Increment direction used by MPDG_PREDICTOR_LINEAR_DIRECTION (zero at Dirichlet DoFs); a
+ * device pointer that must stay valid until the step has run. */
+int mpdg_heat_set_direction(mpdg_heat *h, const double *direction);
 
 /* HeatDiffuseOperation::solve (heat_diffuse_operation.cpp:213-289) on device vectors:
  * predictor (none / linear extrapolation / the guess already in T_cur), history
@@ -429,6 +438,14 @@ int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T, const dou
 int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, const double *T,
                             const double *T_old, const double *heat_source, double dt,
                             double T_scale, int line_search, double *guess, double *alpha_out);
+
+/* The network's correction as an increment direction for MPDG_PREDICTOR_LINEAR_DIRECTION:
+ * direction = a P(y) with the inputs and the scale a of mpdg_heat_learned_guess, zero at the
+ * Dirichlet DoFs (and everywhere when T == T_old). Unlike learned_guess it linearises nothing:
+ * the step applies J to the direction once, at the point it linearises at anyway. */
+int mpdg_heat_learned_direction(mpdg_heat *h, mpdg_unet *u, int stride, const double *T,
+                                const double *T_old, const double *heat_source, double dt,
+                                double T_scale, double *direction);
 
 /* ---- instrumentation -------------------------------------------------- */
 typedef struct {

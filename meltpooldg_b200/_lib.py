@@ -28,7 +28,7 @@ ERR_NOT_SUPPORTED = 9
 LAW_CONSTANT, LAW_LINEAR_K, LAW_LIQUID_SOLID, LAW_GAS_LIQUID, LAW_GAS_LIQUID_SOLID = 0, 1, 2, 3, 4
 SOLVER_CG, SOLVER_GMRES = 0, 1
 PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_CHEBYSHEV_JACOBI_F32, PRECOND_MG_F32 = 0, 1, 2, 3
-PREDICTOR_NONE, PREDICTOR_LINEAR, PREDICTOR_GIVEN = 0, 1, 2
+PREDICTOR_NONE, PREDICTOR_LINEAR, PREDICTOR_GIVEN, PREDICTOR_LINEAR_DIRECTION = 0, 1, 2, 3
 APPARENT_QLQ, APPARENT_CONSTANT, APPARENT_POLY4_BELL = 0, 1, 2
 
 
@@ -177,6 +177,9 @@ _SIGS = {
                                           C.POINTER(C.c_double), _D]),
     "mpdg_heat_learned_guess": (C.c_int, [_H, _H, C.c_int, _D, _D, _D, C.c_double,
                                           C.c_double, C.c_int, _D, C.POINTER(C.c_double)]),
+    "mpdg_heat_learned_direction": (C.c_int, [_H, _H, C.c_int, _D, _D, _D, C.c_double,
+                                              C.c_double, _D]),
+    "mpdg_heat_set_direction": (C.c_int, [_H, _D]),
     "mpdg_last_error": (C.c_char_p, []),
 }
 

@@ -156,6 +156,11 @@ struct mpdg_heat {
   double *hv_T = nullptr, *hv_To = nullptr, *hv_a = nullptr, *hv_b = nullptr, *hv_c = nullptr;
   int64_t *perm = nullptr, *perm_buf = nullptr;  // perm: perm_buf while a permutation is set
   const double *guess = nullptr;
+  // MPDG_PREDICTOR_LINEAR_DIRECTION: the increment direction d, and for the next solve the
+  // operator applied to its initial guess (x_Ax_scale * x_Ax = A x, computed by the step)
+  const double *direction = nullptr;
+  const double *x_Ax = nullptr;
+  double x_Ax_scale = 0.0;
   int64_t bytes = 0;
   std::vector<void *> owned;
   // instrumentation
@@ -1651,6 +1656,29 @@ static int ensure_workspace_f32(mpdg_heat *h)
   return MPDG_OK;
 }
 
+__global__ void k_scale_copy(int64_t N, double *dst, const double *__restrict__ src, double a)
+{
+  GRID_STRIDE(i, N) dst[i] = a * src[i];
+}
+
+// Ap = A x at the start of a solve: zero when the solve starts from x = 0 (x_zero), the
+// step's precomputed A x when it gave one (x_Ax, used once), else one operator application
+static int initial_Ax(mpdg_heat *h, const double *x)
+{
+  const int64_t N = h->n_dofs;
+  if (h->x_Ax) {
+    k_scale_copy<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->Ap, h->x_Ax, h->x_Ax_scale);
+    ++h->launches;
+    CU(cudaGetLastError());
+  } else {
+    CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
+    if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
+  }
+  h->x_Ax = nullptr;
+  h->x_zero = false;
+  return MPDG_OK;
+}
+
 // ---------------------------------------------------------------------------
 // CG (FP64, identity or Jacobi); record = Lanczos history for eigenvalues
 // ---------------------------------------------------------------------------
@@ -1660,9 +1688,7 @@ static int cg_jacobi(mpdg_heat *h, const mpdg_solver_params *prm, double *x, con
   const int64_t N = h->n_dofs;
   TRY(ensure_workspace(h));
   const int g = vgrid(h, N);
-  CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
-  if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
-  h->x_zero = false;
+  TRY(initial_Ax(h, x));
   k_cg_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->pv, h->Ap, D, h->st, h->partials, h->counter,
                                       prm->rel_tolerance, prm->abs_tolerance,
                                       prm->tol_reference_norm, prm->max_iterations, record); ++h->launches;
@@ -2249,9 +2275,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   set_level_streams(h, h->stream);
   if (any_faces(h)) TRY(dvec(h, &h->face_dot, 1));
   for (;;) {
-    CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
-    if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
-    h->x_zero = false;
+    TRY(initial_Ax(h, x));
     k_cgm_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->Ap, h->r32, h->x32, h->d32, h->Ax32,
                                         h->inv_diag_f, inv_theta, h->st, h->partials, h->counter,
                                         prm->rel_tolerance, prm->abs_tolerance,
@@ -2437,9 +2461,7 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
     return MPDG_OK;
   };
   for (;;) {
-    CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
-    if (!h->x_zero) TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
-    h->x_zero = false;
+    TRY(initial_Ax(h, x));
     k_residual<<<g, VT, 0, h->stream>>>(N, b, h->Ap, V);
     ++h->launches;
     double rr = 0.0;
@@ -3426,6 +3448,13 @@ extern "C" int mpdg_heat_linear_solve(mpdg_heat *h, const mpdg_solver_params *pr
   return linear_solve(h, prm, x, b, stats);
 }
 
+extern "C" int mpdg_heat_set_direction(mpdg_heat *h, const double *direction)
+{
+  if (!h || !direction) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  h->direction = direction;
+  return MPDG_OK;
+}
+
 extern "C" int mpdg_heat_set_guess(mpdg_heat *h, const double *guess)
 {
   if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
@@ -3440,6 +3469,11 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
   if (!h || !prm || !T_cur || !T_old) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   if (prm->predictor == MPDG_PREDICTOR_GIVEN && !h->guess)
     return fail(MPDG_ERR_INVALID_ARGUMENT, "predictor GIVEN needs mpdg_heat_set_guess");
+  const bool with_direction = prm->predictor == MPDG_PREDICTOR_LINEAR_DIRECTION;
+  if (with_direction && (!h->direction || !prm->single_linearization))
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "predictor LINEAR_DIRECTION needs mpdg_heat_set_direction and single_linearization");
+  const int predictor = with_direction ? MPDG_PREDICTOR_LINEAR : prm->predictor;
   CU(cudaSetDevice(h->device));
   const int64_t N = h->n_dofs;
   const size_t vb = sizeof(double) * N;
@@ -3459,20 +3493,20 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
     // init_time_advance: predictor into w1, commit history, constraints
     if (h->rotate) {
       // the predicted T replaces T_{n-1} in its buffer and the two buffers swap roles
-      if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
+      if (predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
         k_predict_inplace<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, dt / dt_old);
         ++h->launches;
       } else {
-        const double *from = prm->predictor == MPDG_PREDICTOR_GIVEN ? h->guess : T_cur;
+        const double *from = predictor == MPDG_PREDICTOR_GIVEN ? h->guess : T_cur;
         if ((rc = (cudaMemcpyAsync(T_old, from, vb, cudaMemcpyDeviceToDevice, h->stream) ==
                    cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, "predictor copy"))) != MPDG_OK)
           break;
       }
       std::swap(T_cur, T_old);
       h->rotated = true;
-    } else if (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
+    } else if (predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12) {
       k_predict<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, T_old, h->w1, dt / dt_old); ++h->launches;
-    } else if (prm->predictor == MPDG_PREDICTOR_GIVEN) {
+    } else if (predictor == MPDG_PREDICTOR_GIVEN) {
       if ((rc = (cudaMemcpyAsync(h->w1, h->guess, vb, cudaMemcpyDeviceToDevice, h->stream) ==
                  cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, "guess copy"))) != MPDG_OK) break;
     } else {
@@ -3522,12 +3556,30 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
       mpdg_solver_params lp = prm->linear;
       lp.tol_reference_norm = std::sqrt(bb);
       lp.abs_tolerance = std::max(lp.abs_tolerance, 0.0);
-      zero_async(h, h->w1, vb, h->stream);
       mpdg_solve_stats ls;
       memset(&ls, 0, sizeof(ls));
-      h->x_zero = true;
+      if (with_direction) {
+        // the increment solve starts from alpha d, alpha = argmin |r - alpha J d| (never a
+        // larger initial residual than from 0); J d is computed once and handed to the solver
+        if ((rc = dvec(h, &h->w3, N)) != MPDG_OK) break;
+        zero_async(h, h->w3, vb, h->stream);
+        if ((rc = op_apply_d(h, h->w3, h->direction, FIN_NONE, nullptr, nullptr)) != MPDG_OK) break;
+        double jj = 0.0, jr = 0.0;
+        if ((rc = norms(h, h->w3, h->w2, &jj, &jr)) != MPDG_OK) break;
+        const double rj = 0.5 * (jr - jj - rr);
+        const double alpha = jj > 0.0 ? rj / jj : 0.0;
+        k_scale_copy<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->w1, h->direction, alpha);
+        ++h->launches;
+        h->x_Ax = h->w3;
+        h->x_Ax_scale = alpha;
+        rr = std::max(rr - alpha * rj, 0.0);
+      } else {
+        zero_async(h, h->w1, vb, h->stream);
+        h->x_zero = true;
+      }
       rc = linear_solve(h, &lp, h->w1, h->w2, &ls);
       h->x_zero = false;
+      h->x_Ax = nullptr;
       if (rc != MPDG_OK) break;
       k_axpy<<<vgrid(h, N), VT, 0, h->stream>>>(N, T_cur, 1.0, h->w1); ++h->launches;
       if ((rc = distribute(h, T_cur)) != MPDG_OK) break;
@@ -3832,33 +3884,63 @@ __global__ void k_learned_input(MeshDims d, int stride, int cx, int cy, int cz,
   }
 }
 
+// trilinear prolongation of the sampled-grid field y to nodal DoF i
+__device__ __forceinline__ double prolong_at(int64_t i, const MeshDims &d, int stride, int cx, int cy,
+                                             int cz, const float *__restrict__ y)
+{
+  const int64_t I = i % d.nd[0], J = (i / d.nd[0]) % d.nd[1], K = i / ((int64_t)d.nd[0] * d.nd[1]);
+  const int64_t pos[3] = {I, J, K};
+  const int cdim[3] = {cx, cy, cz};
+  int lo[3], hi[3];
+  double w[3];
+  for (int e = 0; e < 3; ++e) {
+    lo[e] = (int)(pos[e] / stride);
+    const int r = (int)(pos[e] - (int64_t)lo[e] * stride);
+    hi[e] = lo[e] + (r > 0 ? 1 : 0);
+    if (hi[e] >= cdim[e]) hi[e] = cdim[e] - 1;
+    w[e] = (double)r / stride;
+  }
+  double s = 0.0;
+  for (int c = 0; c < 8; ++c) {
+    const int ix = (c & 1) ? hi[0] : lo[0], iy = (c & 2) ? hi[1] : lo[1], iz = (c & 4) ? hi[2] : lo[2];
+    const double wt = ((c & 1) ? w[0] : 1.0 - w[0]) * ((c & 2) ? w[1] : 1.0 - w[1]) *
+                      ((c & 4) ? w[2] : 1.0 - w[2]);
+    if (wt != 0.0) s += wt * (double)y[ix + (int64_t)cx * (iy + (int64_t)cy * iz)];
+  }
+  return s;
+}
+
 __global__ void k_learned_guess(int64_t N, MeshDims d, int stride, int cx, int cy, int cz,
                                 const double *__restrict__ T, const double *__restrict__ To,
                                 const float *__restrict__ y, double s3, double *g)
 {
+  GRID_STRIDE(i, N) g[i] = 2.0 * T[i] - To[i] + s3 * prolong_at(i, d, stride, cx, cy, cz, y);
+}
+
+// the network's increment direction s3 P(y), zero at the Dirichlet DoFs
+__global__ void k_learned_direction(int64_t N, MeshDims d, int stride, int cx, int cy, int cz,
+                                    const float *__restrict__ y, double s3, double *g)
+{
   GRID_STRIDE(i, N)
   {
-    const int64_t I = i % d.nd[0], J = (i / d.nd[0]) % d.nd[1], K = i / ((int64_t)d.nd[0] * d.nd[1]);
-    const int64_t pos[3] = {I, J, K};
-    const int cdim[3] = {cx, cy, cz};
-    int lo[3], hi[3];
-    double w[3];
-    for (int e = 0; e < 3; ++e) {
-      lo[e] = (int)(pos[e] / stride);
-      const int r = (int)(pos[e] - (int64_t)lo[e] * stride);
-      hi[e] = lo[e] + (r > 0 ? 1 : 0);
-      if (hi[e] >= cdim[e]) hi[e] = cdim[e] - 1;
-      w[e] = (double)r / stride;
-    }
-    double s = 0.0;
-    for (int c = 0; c < 8; ++c) {
-      const int ix = (c & 1) ? hi[0] : lo[0], iy = (c & 2) ? hi[1] : lo[1], iz = (c & 4) ? hi[2] : lo[2];
-      const double wt = ((c & 1) ? w[0] : 1.0 - w[0]) * ((c & 2) ? w[1] : 1.0 - w[1]) *
-                        ((c & 4) ? w[2] : 1.0 - w[2]);
-      if (wt != 0.0) s += wt * (double)y[ix + (int64_t)cx * (iy + (int64_t)cy * iz)];
-    }
-    g[i] = 2.0 * T[i] - To[i] + s3 * s;
+    const int I = (int)(i % d.nd[0]), J = (int)((i / d.nd[0]) % d.nd[1]),
+              K = (int)(i / ((int64_t)d.nd[0] * d.nd[1]));
+    g[i] = constrained(d, I, J, K) ? 0.0 : s3 * prolong_at(i, d, stride, cx, cy, cz, y);
   }
+}
+
+// sum of (a - b)^2 into out[0] (last-CTA reduction)
+__global__ void k_diff_sq(int64_t N, const double *__restrict__ a, const double *__restrict__ b,
+                          double *partials, unsigned *counter, double *out)
+{
+  double v[1] = {0.0};
+  GRID_STRIDE(i, N)
+  {
+    const double x = a[i] - b[i];
+    v[0] += x * x;
+  }
+  double tot[1];
+  if (grid_sum<1>(v, partials, counter, tot)) out[0] = tot[0];
 }
 
 static int learned_dims(mpdg_heat *h, int stride, int c[3])
@@ -3983,4 +4065,44 @@ extern "C" int mpdg_heat_learned_guess(mpdg_heat *h, mpdg_unet *u, int stride, c
   CU(cudaGetLastError());
   if (alpha_out) *alpha_out = alpha;
   return distribute(h, guess);
+}
+
+extern "C" int mpdg_heat_learned_direction(mpdg_heat *h, mpdg_unet *u, int stride,
+                                           const double *T, const double *T_old,
+                                           const double *heat_source, double dt, double T_scale,
+                                           double *direction)
+{
+  if (!h || !u || !T || !T_old || !direction)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (!(dt > 0.0) || !(T_scale > 0.0)) return fail(MPDG_ERR_INVALID_ARGUMENT, "dt and T_scale must be > 0");
+  int c[3];
+  TRY(learned_dims(h, stride, c));
+  int ud[3];
+  TRY(mpdg_unet_dims(u, ud));
+  if (ud[0] != c[0] || ud[1] != c[1] || ud[2] != c[2])
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "network grid does not match the sampled mesh grid");
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  const int64_t nc = (int64_t)c[0] * c[1] * c[2];
+  TRY(dalloc(h, reinterpret_cast<void **>(&h->nn_buf), sizeof(float) * 4 * nc));
+  if (h->nn_buf_n == 0) h->nn_buf_n = nc;
+  if (h->nn_buf_n != nc) return fail(MPDG_ERR_INVALID_ARGUMENT, "network grid changed");
+  // per-sample scale: RMS of the time increment
+  k_diff_sq<<<vgrid(h, N), VT, 0, h->stream>>>(N, T, T_old, h->partials, h->counter, h->scal);
+  ++h->launches;
+  CU(cudaGetLastError());
+  TRY(read_to_host(h, h->scal_map, h->scal, sizeof(double)));
+  const double a = std::sqrt(h->scal_host[0] / (double)N);
+  if (!(a > 0.0)) return zero_async(h, direction, sizeof(double) * N, h->stream) == cudaSuccess
+                           ? MPDG_OK : fail(MPDG_ERR_CUDA, "zero fill");
+  const double scales[3] = {a, a, T_scale};
+  TRY(mpdg_heat_learned_input(h, stride, T, T_old, heat_source, dt, scales, h->nn_buf));
+  mpdg_unet_set_stream(u, h->stream);
+  const int rc = mpdg_unet_forward(u, h->nn_buf, h->nn_buf + 3 * nc);
+  if (rc != MPDG_OK) return fail(rc, "network forward failed");
+  k_learned_direction<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, stride, c[0], c[1], c[2],
+                                                         h->nn_buf + 3 * nc, a, direction);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
 }

@@ -491,6 +491,11 @@ class HeatDiffuseOperation:
         check(self.op._L.mpdg_heat_set_guess(self.op.h, _ptr(guess)))
         self._guess = guess
 
+    def set_direction(self, direction):
+        """Increment direction for PREDICTOR_LINEAR_DIRECTION (zero at Dirichlet DoFs)."""
+        check(self.op._L.mpdg_heat_set_direction(self.op.h, _ptr(direction)))
+        self._direction = direction
+
     # host-buffer steps with the history resident on the device --------------------------
     @staticmethod
     def _host_ptr(t):

@@ -129,6 +129,18 @@ class GuessModel:
                                                out.data_ptr(), C.byref(alpha)))
         return out, float(alpha.value)
 
+    def direction(self, op: H.HeatDiffuseOperator, T, T_old, q, dt, out=None):
+        """The network's increment direction a P(y) for PREDICTOR_LINEAR_DIRECTION (the step
+        starts its increment solve from alpha times it, alpha minimising the residual)."""
+        out = op.new_vector() if out is None else out
+        self.net.sync_stream()
+        H.check(op._L.mpdg_heat_learned_direction(op.h, self.net.h, self.stride, T.data_ptr(),
+                                                   T_old.data_ptr(),
+                                                   None if q is None else q.data_ptr(),
+                                                   float(dt), float(self.T_scale),
+                                                   out.data_ptr()))
+        return out
+
     def save(self, path):
         p = self.net.get_params().cpu()
         torch.save({"params": p, "dims": self.net.dims, "T_scale": self.T_scale}, path + ".pt")

@@ -1,7 +1,7 @@
 """The latent heat of fusion (apparent heat capacity in the mushy zone) in the GPU operator,
 against the oracle: the liquid-solid law (mushy zone) and the gas-liquid-solid law with every
 apparent-capacity profile, FP64 vmult, inverse diagonal and residual to 1e-12 relative, the FP32
-operator to 2e-5; and one implicit Newton step through the GPU time step.
+operator to 2e-4 (see TOL32); and one implicit Newton step through the GPU time step.
 
 Material and temperatures follow the reference's apparent-capacity unit test
 (unit_tests/heat/apparent_capacity.cpp: solidus 271, liquidus 275), with temperatures sampled
@@ -16,7 +16,10 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-TOL64, TOL32 = 1e-12, 2e-5
+# FP32: the FP32 operator evaluates the law at T_lin rounded to FP32 (ulp(278) = 3e-5 K) inside
+# a 4 K mushy zone where the apparent capacity is ~20x the sensible one, so its relative error is
+# set by that rounding (measured up to 9e-5), not by the 2e-5 of the other FP32 tests
+TOL64, TOL32 = 1e-12, 2e-4
 PROFILES = {"qlq": L.APPARENT_QLQ, "constant": L.APPARENT_CONSTANT,
             "poly4_bell": L.APPARENT_POLY4_BELL}
 LAWS = {

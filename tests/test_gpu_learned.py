@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 MODEL = os.path.join(os.path.dirname(LG.__file__), "models", "heat_guess_p3_h96")
 
 
-def run(op, model, seed, n_steps=14):
+def run(op, model, seed, n_steps=14, direction=False):
     path = LG.scan_path(torch.Generator().manual_seed(seed))
     lin = H.LinearSolverData(preconditioner_type=L.PRECOND_CHEBYSHEV_JACOBI_F32,
                              rel_tolerance=1e-8, abs_tolerance=0.0, cheb_degree=6,
@@ -29,7 +29,10 @@ def run(op, model, seed, n_steps=14):
     its, res = [], []
     for s in range(n_steps):
         op.gaussian_source(q, LG.AMP, path((s + 1) * LG.DT), LG.RADIUS)
-        if model is not None and s > 0:
+        if model is not None and s > 0 and direction:
+            opn.set_direction(model.direction(op, opn.T, opn.T_old, q, LG.DT))
+            opn.params.predictor = L.PREDICTOR_LINEAR_DIRECTION
+        elif model is not None and s > 0:
             g, _ = model.guess(op, opn.T, opn.T_old, q, LG.DT)
             opn.set_guess(g)
             opn.params.predictor = L.PREDICTOR_GIVEN
@@ -67,3 +70,35 @@ def test_guess_rejects_a_network_of_another_grid():
     T = op.new_vector()
     with pytest.raises(H.ExcInvalidArgument):
         model.guess(op, T, T, None, LG.DT)
+
+
+def test_learned_direction_starts_the_increment_solve_closer():
+    """PREDICTOR_LINEAR_DIRECTION: linearised at the extrapolation (as PREDICTOR_LINEAR), the
+    increment solve starts from alpha d with alpha minimising the residual, so the initial
+    residual never exceeds the extrapolation's and the converged fields are the same to the
+    solver tolerance (the linearisation point is the same; only the start differs)."""
+    op = LG.make_operator(32)
+    model = LG.GuessModel.load(MODEL, stride=1)
+    its0, res0, T0 = run(op, None, seed=77, n_steps=8)
+    its1, res1, T1 = run(op, model, seed=77, n_steps=8, direction=True)
+    print("initial residual", [f"{a:.2e}->{b:.2e}" for a, b in zip(res0, res1)],
+          "iterations", sum(its0), "->", sum(its1))
+    assert all(r1 <= r0 * (1 + 1e-9) for r0, r1 in zip(res0, res1))
+    assert any(r1 < 0.9 * r0 for r0, r1 in zip(res0[1:], res1[1:]))
+    # same linearisation points, different starts: the fields differ by the solver tolerance
+    assert torch.linalg.vector_norm(T1 - T0) <= 2e-5 * torch.linalg.vector_norm(T0)
+
+
+def test_direction_predictor_needs_a_direction_and_one_linearisation():
+    op = LG.make_operator(4)
+    opn = H.HeatDiffuseOperation(op, H.LinearSolverData(), predictor=L.PREDICTOR_LINEAR_DIRECTION,
+                                 single_linearization=True)
+    with pytest.raises(H.ExcInvalidArgument):
+        opn.solve(LG.DT)
+    opn.set_direction(op.new_vector())
+    opn.params.single_linearization = 0
+    with pytest.raises(H.ExcInvalidArgument):
+        opn.solve(LG.DT)
+    opn.params.single_linearization = 1
+    st = opn.solve(LG.DT)  # a zero direction: the plain linear-predictor step
+    assert st.converged == 1

@@ -333,6 +333,32 @@ int mpdg_heat_preconditioner_vmult(mpdg_heat *h, double *dst, const double *src)
 int mpdg_heat_linear_solve(mpdg_heat *h, const mpdg_solver_params *prm, double *x,
                            const double *b, mpdg_solve_stats *stats);
 
+/* ---- Jacobi-CG across ranks (z-slab decomposition; no reference counterpart beyond the
+ *      MPI_Allreduce'd dot products of SolverCG and the ghost exchange of MatrixFree::loop,
+ *      scratch_data.cpp:149-188) ----------------------------------------------------------
+ * The caller owns the collectives. Each stage reduces over this rank's owned DoFs (the first
+ * n_owned entries of the slab vector; a shared plane is owned by the upper slab) into
+ * `partial` (device doubles), which the caller all-reduces before the next stage; alpha and
+ * beta are device scalars, so an iteration needs no host round trip except the convergence
+ * test. One iteration: Ap = J p (mpdg_heat_vmult, shared planes summed by the caller),
+ * dcg_dot(p, Ap) -> all-reduce -> alpha = rz / pAp, dcg_update -> all-reduce ->
+ * (rz', rr) -> beta = rz' / rz, dcg_direction.
+ *   dcg_start      r = b - Ax (Ax may be NULL: x = 0), z = D r, p = z; partial = (r.z, r.r)
+ *   dcg_dot        partial[0] = a.b
+ *   dcg_update     x += alpha p, r -= alpha Ap, z = D r; partial = (r.z, r.r)
+ *   dcg_direction  p = z + beta p
+ *   invert_diagonal  d <- |d| > 1e-10 ? 1/d : 1 (after the shared planes of the diagonal
+ *                  of mpdg_heat_compute_diagonal were summed) */
+int mpdg_heat_dcg_start(mpdg_heat *h, int64_t n_owned, const double *b, const double *Ax,
+                        const double *inv_diag, double *r, double *z, double *p, double *partial);
+int mpdg_heat_dcg_dot(mpdg_heat *h, int64_t n_owned, const double *a, const double *b,
+                      double *partial);
+int mpdg_heat_dcg_update(mpdg_heat *h, int64_t n_owned, double *x, double *r, double *z,
+                         const double *p, const double *Ap, const double *inv_diag,
+                         const double *alpha, double *partial);
+int mpdg_heat_dcg_direction(mpdg_heat *h, double *p, const double *z, const double *beta);
+int mpdg_heat_invert_diagonal(mpdg_heat *h, double *d);
+
 /* ---- time step --------------------------------------------------------- */
 /* LINEAR_DIRECTION (no reference counterpart; single_linearization only): the linear
  * extrapolation is the linearisation point, and the increment solve starts from alpha d instead

@@ -122,6 +122,11 @@ _SIGS = {
     "mpdg_heat_compute_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),
     "mpdg_heat_set_dof_permutation": (C.c_int, [_H, _P]),
+    "mpdg_heat_dcg_start": (C.c_int, [_H, C.c_int64, _D, _D, _D, _D, _D, _D, _D]),
+    "mpdg_heat_dcg_dot": (C.c_int, [_H, C.c_int64, _D, _D, _D]),
+    "mpdg_heat_dcg_update": (C.c_int, [_H, C.c_int64, _D, _D, _D, _D, _D, _D, _D, _D]),
+    "mpdg_heat_dcg_direction": (C.c_int, [_H, _D, _D, _D]),
+    "mpdg_heat_invert_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_set_linearization_host": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult_host": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_compute_inverse_diagonal_host": (C.c_int, [_H, _D]),

@@ -3788,6 +3788,157 @@ extern "C" int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset)
 }
 
 // ---------------------------------------------------------------------------
+// stages of a Jacobi-CG iteration split across ranks (z-slab decomposition)
+//
+// The caller owns the collectives: each stage reduces over this rank's owned DoFs (the first
+// n_owned entries; a shared plane is owned by the upper slab) into device doubles, which the
+// caller all-reduces (NCCL on device buffers) before the next stage; the step lengths alpha
+// and beta are device scalars too, so an iteration needs no host round trip except the
+// convergence test.
+// ---------------------------------------------------------------------------
+__global__ void k_dcg_start(int64_t N, int64_t n_owned, const double *__restrict__ b,
+                            const double *__restrict__ Ax, const double *__restrict__ D,
+                            double *r, double *z, double *p, double *partials,
+                            unsigned *counter, double *out)
+{
+  double v[2] = {0.0, 0.0};
+  GRID_STRIDE(i, N)
+  {
+    const double ri = b[i] - (Ax ? Ax[i] : 0.0);
+    const double zi = D[i] * ri;
+    r[i] = ri;
+    z[i] = zi;
+    p[i] = zi;
+    if (i < n_owned) {
+      v[0] += ri * zi;
+      v[1] += ri * ri;
+    }
+  }
+  double tot[2];
+  if (grid_sum<2>(v, partials, counter, tot)) {
+    out[0] = tot[0];
+    out[1] = tot[1];
+  }
+}
+
+__global__ void k_dcg_dot(int64_t n_owned, const double *__restrict__ a,
+                          const double *__restrict__ b, double *partials, unsigned *counter,
+                          double *out)
+{
+  double v[1] = {0.0};
+  GRID_STRIDE(i, n_owned) v[0] += a[i] * b[i];
+  double tot[1];
+  if (grid_sum<1>(v, partials, counter, tot)) out[0] = tot[0];
+}
+
+// x += alpha p, r -= alpha Ap, z = D r; out = (r.z, r.r) over the owned DoFs
+__global__ void k_dcg_update(int64_t N, int64_t n_owned, double *x, double *r, double *z,
+                             const double *__restrict__ p, const double *__restrict__ Ap,
+                             const double *__restrict__ D, const double *__restrict__ alpha,
+                             double *partials, unsigned *counter, double *out)
+{
+  const double al = *alpha;
+  double v[2] = {0.0, 0.0};
+  GRID_STRIDE(i, N)
+  {
+    x[i] += al * p[i];
+    const double ri = r[i] - al * Ap[i];
+    const double zi = D[i] * ri;
+    r[i] = ri;
+    z[i] = zi;
+    if (i < n_owned) {
+      v[0] += ri * zi;
+      v[1] += ri * ri;
+    }
+  }
+  double tot[2];
+  if (grid_sum<2>(v, partials, counter, tot)) {
+    out[0] = tot[0];
+    out[1] = tot[1];
+  }
+}
+
+__global__ void k_dcg_direction(int64_t N, double *p, const double *__restrict__ z,
+                                const double *__restrict__ beta)
+{
+  const double be = *beta;
+  GRID_STRIDE(i, N) p[i] = z[i] + be * p[i];
+}
+
+static int dcg_check(mpdg_heat *h, int64_t n_owned)
+{
+  if (n_owned < 0 || n_owned > h->n_dofs)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "n_owned must be in [0, n_dofs]");
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_dcg_start(mpdg_heat *h, int64_t n_owned, const double *b, const double *Ax,
+                                   const double *inv_diag, double *r, double *z, double *p,
+                                   double *partial)
+{
+  if (!h || !b || !inv_diag || !r || !z || !p || !partial)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY(dcg_check(h, n_owned));
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  k_dcg_start<<<vgrid(h, N), VT, 0, h->stream>>>(N, n_owned, b, Ax, inv_diag, r, z, p,
+                                                 h->partials, h->counter, partial);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_dcg_dot(mpdg_heat *h, int64_t n_owned, const double *a, const double *b,
+                                 double *partial)
+{
+  if (!h || !a || !b || !partial) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY(dcg_check(h, n_owned));
+  CU(cudaSetDevice(h->device));
+  k_dcg_dot<<<vgrid(h, std::max<int64_t>(n_owned, 1)), VT, 0, h->stream>>>(
+    n_owned, a, b, h->partials, h->counter, partial);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_dcg_update(mpdg_heat *h, int64_t n_owned, double *x, double *r,
+                                    double *z, const double *p, const double *Ap,
+                                    const double *inv_diag, const double *alpha, double *partial)
+{
+  if (!h || !x || !r || !z || !p || !Ap || !inv_diag || !alpha || !partial)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY(dcg_check(h, n_owned));
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  k_dcg_update<<<vgrid(h, N), VT, 0, h->stream>>>(N, n_owned, x, r, z, p, Ap, inv_diag, alpha,
+                                                  h->partials, h->counter, partial);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_dcg_direction(mpdg_heat *h, double *p, const double *z, const double *beta)
+{
+  if (!h || !p || !z || !beta) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  const int64_t N = h->n_dofs;
+  k_dcg_direction<<<vgrid(h, N), VT, 0, h->stream>>>(N, p, z, beta);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_invert_diagonal(mpdg_heat *h, double *d)
+{
+  if (!h || !d) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  CU(cudaSetDevice(h->device));
+  k_invert_diag<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, d);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+// ---------------------------------------------------------------------------
 // FE L2 norm that allocates nothing
 //
 // Some callers cannot call cudaMalloc: code that runs inside another

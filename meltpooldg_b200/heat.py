@@ -350,6 +350,28 @@ class HeatDiffuseOperator:
         check(self._L.mpdg_heat_distribute_constraints(self.h, _ptr(u)))
         return u
 
+    # stages of a Jacobi-CG iteration split across ranks (the caller all-reduces `partial`
+    # between stages; alpha, beta and the partial sums are device tensors) ------------------
+    def dcg_start(self, n_owned, b, Ax, inv_diag, r, z, p, partial):
+        check(self._L.mpdg_heat_dcg_start(self.h, int(n_owned), _ptr(b), _ptr(Ax), _ptr(inv_diag),
+                                          _ptr(r), _ptr(z), _ptr(p), _ptr(partial)))
+
+    def dcg_dot(self, n_owned, a, b, partial):
+        check(self._L.mpdg_heat_dcg_dot(self.h, int(n_owned), _ptr(a), _ptr(b), _ptr(partial)))
+
+    def dcg_update(self, n_owned, x, r, z, p, Ap, inv_diag, alpha, partial):
+        check(self._L.mpdg_heat_dcg_update(self.h, int(n_owned), _ptr(x), _ptr(r), _ptr(z),
+                                           _ptr(p), _ptr(Ap), _ptr(inv_diag), _ptr(alpha),
+                                           _ptr(partial)))
+
+    def dcg_direction(self, p, z, beta):
+        check(self._L.mpdg_heat_dcg_direction(self.h, _ptr(p), _ptr(z), _ptr(beta)))
+
+    def invert_diagonal(self, d):
+        """d <- |d| > 1e-10 ? 1/d : 1 (compute_inverse_diagonal_from_matrixfree's rule)."""
+        check(self._L.mpdg_heat_invert_diagonal(self.h, _ptr(d)))
+        return d
+
     # verbs on host vectors (OperatorMatrixFree's VectorType lives in host memory) --------
     def set_dof_permutation(self, lex_of_dof):
         """The caller's DoF numbering: lex_of_dof[i] is the lexicographic index of the

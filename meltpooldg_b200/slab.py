@@ -18,11 +18,16 @@ norm are disjoint and need no weighting.
 
 The solvers are Jacobi-preconditioned CG (deal.II SolverCG with ReductionControl, as
 `LinearSolver::solve`) and the implicit step of HeatDiffuseOperation (predictor, history
-commit, Jacobi update at the predicted state, Newton-Raphson), driven from the host with one
-operator application, one plane exchange and two all-reduces per CG iteration. Every branch
-that involves a collective is taken on a globally reduced value, so all ranks take it.
+commit, Jacobi update at the predicted state, Newton-Raphson). A CG iteration is one operator
+application, one plane exchange and the library's fused stage kernels (`mpdg_heat_dcg_*`: the
+vector updates with their partial dot products over the owned DoFs), with two all-reduces of
+device buffers; the step lengths stay on the device, so the only host read per iteration is the
+convergence test. Every branch that involves a collective is taken on a globally reduced value,
+so all ranks take it.
 """
 from __future__ import annotations
+
+import math
 
 import torch
 import torch.distributed as dist
@@ -80,6 +85,19 @@ class SlabExchange:
         for r, t in recvs:
             (lo if r < self.rank else hi).add_(t.to(v.device))
         return v
+
+    def all_reduce_(self, t: torch.Tensor) -> torch.Tensor:
+        """In-place sum over the ranks of a small tensor: on the device over NCCL, staged
+        through host memory with a host backend (gloo)."""
+        if self.world == 1:
+            return t
+        if self.staged and t.is_cuda:
+            h = t.cpu()
+            dist.all_reduce(h, group=self.group)
+            t.copy_(h)
+        else:
+            dist.all_reduce(t, group=self.group)
+        return t
 
     def sum(self, x: float) -> float:
         if self.world == 1:
@@ -147,10 +165,7 @@ class SlabHeatOperator:
         """diag(J) summed over the slabs, inverted with |d| > 1e-10 ? 1/d : 1."""
         self.op.compute_diagonal(inv)
         self.x.add_shared_planes(inv, self.plane)
-        ok = inv.abs() > 1e-10
-        inv.copy_(torch.where(ok, 1.0 / torch.where(ok, inv, torch.ones_like(inv)),
-                              torch.ones_like(inv)))
-        return inv
+        return self.op.invert_diagonal(inv)
 
     def create_rhs(self, dst, T_old, heat_source=None):
         """dst += -R(T_lin) summed over the slabs."""
@@ -163,34 +178,45 @@ class SlabHeatOperator:
 
 def slab_cg(A: SlabHeatOperator, x, b, inv_diag, data: LinearSolverData) -> int:
     """Jacobi-preconditioned CG across the slabs (deal.II SolverCG, ReductionControl:
-    |r| <= max(abs_tol, rel_tol |r_0|)). Returns the iteration count."""
-    r = b.clone()
-    ax = A.new_vector()
-    if A.x.sum(float(x.abs().max().item())) > 0:  # the same branch on every rank
+    |r| <= max(abs_tol, rel_tol |r_0|)). Returns the iteration count.
+
+    Each iteration: Ap = J p with the shared planes summed; the fused stage kernels of the
+    operator (dcg_dot, dcg_update, dcg_direction) with their partial sums all-reduced as
+    device tensors; alpha = rz / pAp and beta = rz' / rz computed on the device. The host reads
+    (r.r, p.Ap) once per iteration for the convergence and breakdown tests."""
+    op, X, n = A.op, A.x, A.n_owned
+    r, z, p, ax = A.new_vector(), A.new_vector(), A.new_vector(), A.new_vector()
+    dev = b.device
+    part = torch.zeros(2, dtype=torch.float64, device=dev)
+    pap = torch.zeros(1, dtype=torch.float64, device=dev)
+    alpha = torch.zeros(1, dtype=torch.float64, device=dev)
+    beta = torch.zeros(1, dtype=torch.float64, device=dev)
+    nonzero_x = X.sum(float(x.abs().max().item())) > 0  # the same branch on every rank
+    if nonzero_x:
         A.vmult(ax, x)
-        r.sub_(ax)
-    res = A.norm(r)
+    op.dcg_start(n, b, ax if nonzero_x else None, inv_diag, r, z, p, part)
+    X.all_reduce_(part)
+    rz = part[:1].clone()
+    res = math.sqrt(max(float(part[1]), 0.0))
     tol = max(data.abs_tolerance, data.rel_tolerance * res)
     if res <= tol:
         return 0
-    z = r * inv_diag
-    p = z.clone()
-    rz = A.dot(r, z)
     for it in range(1, data.max_iterations + 1):
         A.vmult(ax, p)
-        pap = A.dot(p, ax)
-        if not pap > 0.0:
+        op.dcg_dot(n, p, ax, pap)
+        X.all_reduce_(pap)
+        torch.div(rz, pap, out=alpha)
+        op.dcg_update(n, x, r, z, p, ax, inv_diag, alpha, part)
+        X.all_reduce_(part)
+        rr, pAp = torch.cat([part[1:], pap]).tolist()  # the iteration's one host read
+        if not pAp > 0.0:
             raise ExcNoConvergence("CG breakdown: p.Ap <= 0")
-        alpha = rz / pap
-        x.add_(p, alpha=alpha)
-        r.sub_(ax, alpha=alpha)
-        res = A.norm(r)
+        res = math.sqrt(max(rr, 0.0))
         if res <= tol:
             return it
-        torch.mul(r, inv_diag, out=z)
-        rz_new = A.dot(r, z)
-        p.mul_(rz_new / rz).add_(z)
-        rz = rz_new
+        torch.div(part[:1], rz, out=beta)
+        rz.copy_(part[:1])
+        op.dcg_direction(p, z, beta)
     raise ExcNoConvergence(f"CG: {data.max_iterations} iterations, residual {res:.3e}")
 
 

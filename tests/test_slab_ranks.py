@@ -99,6 +99,32 @@ class BoxQ1:
     def set_material(self, m):
         pass
 
+    # the CG stage kernels of the library (mpdg_heat_dcg_*), same semantics
+    def invert_diagonal(self, d):
+        ok = d.abs() > 1e-10
+        d.copy_(torch.where(ok, 1.0 / torch.where(ok, d, torch.ones_like(d)), torch.ones_like(d)))
+        return d
+
+    def dcg_start(self, n_owned, b, Ax, D, r, z, p, partial):
+        r.copy_(b if Ax is None else b - Ax)
+        torch.mul(D, r, out=z)
+        p.copy_(z)
+        partial[0] = r[:n_owned] @ z[:n_owned]
+        partial[1] = r[:n_owned] @ r[:n_owned]
+
+    def dcg_dot(self, n_owned, a, b, partial):
+        partial[0] = a[:n_owned] @ b[:n_owned]
+
+    def dcg_update(self, n_owned, x, r, z, p, Ap, D, alpha, partial):
+        x.add_(alpha * p)
+        r.sub_(alpha * Ap)
+        torch.mul(D, r, out=z)
+        partial[0] = r[:n_owned] @ z[:n_owned]
+        partial[1] = r[:n_owned] @ r[:n_owned]
+
+    def dcg_direction(self, p, z, beta):
+        p.mul_(beta).add_(z)
+
     def reset_time_increment(self, dt):
         self.dt = dt
 
@@ -122,6 +148,9 @@ class _OneRank:
 
     def sum(self, x):
         return float(x)
+
+    def all_reduce_(self, t):
+        return t
 
 
 def _rank(rank, world, port, out):

@@ -495,9 +495,9 @@ int mpdg_heat_get_counters(mpdg_heat *h, mpdg_counters *c, int reset);
  * not have it as a node: it is constrained to such a cell's interpolant (DoFTools::
  * make_hanging_node_constraints merged into the Dirichlet constraints,
  * include/meltpooldg/utilities/constraints.hpp:111-132). The DoFs are the other nodes,
- * numbered by position (z, then y, then x). Affine boxes only (perturb = 0), degree 1..4.
- * device < 0 builds the host description only (no CUDA call; vmult then fails); on a device
- * the levels are 0 and 1 (MPDG_ERR_NOT_SUPPORTED otherwise). */
+ * numbered by position (z, then y, then x). Affine boxes only (perturb = 0), degree 1..4,
+ * levels 0..6 (each coarse cell's 8^level cells), Dirichlet values zero. device < 0 builds the
+ * host description only (no CUDA call; the operator verbs then fail). */
 typedef struct mpdg_amr mpdg_amr;
 int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine, int device,
                     mpdg_amr **out);
@@ -522,8 +522,30 @@ int mpdg_amr_set_material(mpdg_amr *h, const mpdg_material *m, double dt);
  * device vectors of n_dofs: Dirichlet DoFs read as zero, their rows zero; the hanging nodes
  * interpolated inside each refined cell from its gathered coarse DoFs and the transpose
  * applied in the scatter. T_lin: the linearisation point for LINEAR_K (NULL otherwise).
- * Runs on the legacy default stream and returns once the result is complete. */
+ * The mpdg_amr_* verbs run on the legacy default stream and return once the result is
+ * complete. */
 int mpdg_amr_vmult(mpdg_amr *h, double *dst, const double *src, const double *T_lin);
+/* compute_inverse_diagonal_from_matrixfree (heat_diffuse_operator.cpp:271-284) on the refined
+ * mesh: diag(F^T A_e F) accumulated cell by cell (F the cell's hanging-node interpolation),
+ * inverted with |d| > 1e-10 ? 1/d : 1. */
+int mpdg_amr_inverse_diagonal(mpdg_amr *h, double *inv_diag, const double *T_lin);
+/* create_rhs (heat_diffuse_operator.cpp:783-806): dst += -R(T) with T, T_old and the nodal
+ * source (nullable) interpolated by the hanging rule inside each cell; Dirichlet rows
+ * untouched. */
+int mpdg_amr_create_rhs(mpdg_amr *h, double *dst, const double *T, const double *T_old,
+                        const double *heat_source);
+/* LinearSolver::solve with CG and Jacobi (linear_solver.hpp:22-134) from x = 0:
+ * |r| <= max(abs_tol, rel_tol |b|); MPDG_ERR_NOT_CONVERGED after max_iterations. */
+int mpdg_amr_linear_solve(mpdg_amr *h, double *x, const double *b, const double *T_lin,
+                          double rel_tolerance, double abs_tolerance, int max_iterations,
+                          int *iterations);
+/* HeatDiffuseOperation::solve (heat_diffuse_operation.cpp:213-289) on the refined mesh:
+ * linear predictor (or a copy, prm->predictor), history commit, Dirichlet DoFs zero, Jacobi at
+ * the predicted state, Newton-Raphson with Jacobi-CG increment solves (prm->linear's
+ * tolerances) and the reference's convergence test. T_cur and T_old are updated in place. */
+int mpdg_amr_time_step(mpdg_amr *h, double dt, double dt_old, double *T_cur, double *T_old,
+                       const double *heat_source, const mpdg_step_params *prm,
+                       mpdg_step_stats *stats);
 
 /* Last error message of this thread (static storage). */
 const char *mpdg_last_error(void);

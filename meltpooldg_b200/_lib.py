@@ -165,6 +165,12 @@ _SIGS = {
     "mpdg_amr_cell_data": (C.c_int, [_H, _P, _P]),
     "mpdg_amr_set_material": (C.c_int, [_H, C.POINTER(Material), C.c_double]),
     "mpdg_amr_vmult": (C.c_int, [_H, _D, _D, _D]),
+    "mpdg_amr_inverse_diagonal": (C.c_int, [_H, _D, _D]),
+    "mpdg_amr_create_rhs": (C.c_int, [_H, _D, _D, _D, _D]),
+    "mpdg_amr_linear_solve": (C.c_int, [_H, _D, _D, _D, C.c_double, C.c_double, C.c_int,
+                                         C.POINTER(C.c_int)]),
+    "mpdg_amr_time_step": (C.c_int, [_H, C.c_double, C.c_double, _D, _D, _D,
+                                      C.POINTER(StepParams), C.POINTER(StepStats)]),
     "mpdg_heat_get_counters": (C.c_int, [_H, C.POINTER(Counters), C.c_int]),
     "mpdg_unet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_H)]),
     "mpdg_unet_destroy": (C.c_int, [_H]),

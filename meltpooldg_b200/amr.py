@@ -74,3 +74,42 @@ class AmrHeatOperator:
         torch.cuda.current_stream().synchronize()  # the kernel runs on the legacy stream
         check(self._L.mpdg_amr_vmult(self.h, dst.data_ptr(), src.data_ptr(),
                                      None if T_lin is None else T_lin.data_ptr()))
+
+    def _vec(self, *ts):
+        for t in ts:
+            if t is None:
+                continue
+            if not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous() or \
+                    t.numel() != self.n_dofs:
+                raise ExcInvalidArgument("expected contiguous CUDA float64 vectors of n_dofs")
+        torch.cuda.current_stream().synchronize()  # the kernels run on the legacy stream
+        return [None if t is None else t.data_ptr() for t in ts]
+
+    def inverse_diagonal(self, inv_diag: torch.Tensor, T_lin: torch.Tensor | None = None):
+        """compute_inverse_diagonal_from_matrixfree on the refined mesh."""
+        check(self._L.mpdg_amr_inverse_diagonal(self.h, *self._vec(inv_diag, T_lin)))
+        return inv_diag
+
+    def create_rhs(self, dst, T, T_old, heat_source=None):
+        """dst += -R(T) (T the linearisation point, T_old the previous step)."""
+        check(self._L.mpdg_amr_create_rhs(self.h, *self._vec(dst, T, T_old, heat_source)))
+        return dst
+
+    def linear_solve(self, x, b, T_lin=None, rel_tolerance=1e-12, abs_tolerance=1e-20,
+                     max_iterations=10000) -> int:
+        """Jacobi-CG from x = 0; returns the iteration count."""
+        its = C.c_int()
+        check(self._L.mpdg_amr_linear_solve(self.h, *self._vec(x, b, T_lin), float(rel_tolerance),
+                                            float(abs_tolerance), int(max_iterations),
+                                            C.byref(its)))
+        return int(its.value)
+
+    def time_step(self, T_cur, T_old, dt, dt_old, heat_source=None, params=None) -> L.StepStats:
+        """HeatDiffuseOperation::solve on the refined mesh (T_cur, T_old updated in place)."""
+        from .heat import step_params
+        prm = params if params is not None else step_params()
+        st = L.StepStats()
+        a, b, q = self._vec(T_cur, T_old, heat_source)
+        check(self._L.mpdg_amr_time_step(self.h, float(dt), float(dt_old), a, b, q,
+                                         C.byref(prm), C.byref(st)))
+        return st

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <initializer_list>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -46,6 +47,7 @@ struct AmrArgs {
   const uint8_t *mask;
   const double *src;
   const double *Tl;
+  const double *q;  // create_rhs: the nodal heat source (nullable)
   double *dst;
   int64_t n_cells;
   double h[3];
@@ -58,6 +60,12 @@ struct AmrArgs {
 };
 
 int fail(int code, const std::string &msg) { return mpdg_internal_fail(code, msg.c_str()); }
+
+#define TRY_AMR(call)              \
+  do {                             \
+    const int rc_ = (call);        \
+    if (rc_ != MPDG_OK) return rc_; \
+  } while (0)
 
 // out[t] = sum_a M[o][a] in[line(a)], o = t's index along dir (M row-major n x n);
 // transpose: sum_a M[a][o] in[line(a)]
@@ -111,6 +119,62 @@ __device__ __forceinline__ void evaluate(const AmrArgs &a, const double *u, doub
   __syncthreads();
 }
 
+// integration: u = S^T/Sd^T of (val, gx, gy, gz) along z, then y, then x
+template <int n>
+__device__ __forceinline__ void integrate_cell(const AmrArgs &a, double *u, const double *val,
+                                               const double *gx, const double *gy,
+                                               const double *gz, double *t1, double *t2,
+                                               double *s1, double *s2, double *s3, int t)
+{
+  s1[t] = line_sum<n>(a.S, val, t, 2, true) + line_sum<n>(a.Sd, gz, t, 2, true);
+  s2[t] = line_sum<n>(a.S, gx, t, 2, true);
+  s3[t] = line_sum<n>(a.S, gy, t, 2, true);
+  __syncthreads();
+  t1[t] = line_sum<n>(a.S, s1, t, 1, true) + line_sum<n>(a.Sd, s3, t, 1, true);
+  t2[t] = line_sum<n>(a.S, s2, t, 1, true);
+  __syncthreads();
+  u[t] = line_sum<n>(a.S, t1, t, 0, true) + line_sum<n>(a.Sd, t2, t, 0, true);
+  __syncthreads();
+}
+
+// the cell's edge length factor 2^-level (bits 10-12 of the code; 0 for a coarse cell)
+__device__ __forceinline__ double cell_size(int code)
+{
+  return ldexp(1.0, -((code >> kLevelShift) & 7));
+}
+
+// Apply the cell operator to the node values u (shared, overwritten with the integrated
+// result, before the transposed hanging interpolation); Tv, Tx, Ty, Tz hold the linearisation
+// point's values and reference gradients at the q-points when a.tangent.
+template <int n>
+__device__ __forceinline__ void apply_cell(const AmrArgs &a, double size, double *u,
+                                           const double *Tv, const double *Tx, const double *Ty,
+                                           const double *Tz, double *val, double *gx, double *gy,
+                                           double *gz, double *t1, double *t2, double *s1,
+                                           double *s2, double *s3, int t)
+{
+  evaluate<n>(a, u, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
+  // quadrature point t: rho_cp/dt u and the flux k grad(u) (+ k1 grad(T_lin) u)
+  {
+    const int qx = t % n, qy = (t / n) % n, qz = t / (n * n);
+    const double hx = a.h[0] * size, hy = a.h[1] * size, hz = a.h[2] * size;
+    const double jxw = a.w[qx] * a.w[qy] * a.w[qz] * hx * hy * hz;
+    const double k = a.tangent ? a.k0 + a.k1 * Tv[t] : a.k0;
+    double fx = k * gx[t] / hx, fy = k * gy[t] / hy, fz = k * gz[t] / hz;
+    if (a.tangent) {
+      fx += a.k1 * Tx[t] / hx * val[t];
+      fy += a.k1 * Ty[t] / hy * val[t];
+      fz += a.k1 * Tz[t] / hz * val[t];
+    }
+    val[t] = a.cval * val[t] * jxw;
+    gx[t] = fx * jxw / hx;
+    gy[t] = fy * jxw / hy;
+    gz[t] = fz * jxw / hz;
+  }
+  __syncthreads();
+  integrate_cell<n>(a, u, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
+}
+
 template <int n>
 __global__ void k_amr_vmult(const AmrArgs a)
 {
@@ -122,7 +186,7 @@ __global__ void k_amr_vmult(const AmrArgs a)
     const int code = a.code[c];
     const int dof = a.idx[c * n3 + t];
     const bool hang = (code & 0x1F8) != 0;
-    const double size = (code & kFineBit) ? 0.5 : 1.0;
+    const double size = cell_size(code);
     u[t] = a.mask[dof] ? 0.0 : a.src[dof];
     if (a.tangent) T[t] = a.Tl[dof];
     __syncthreads();
@@ -134,40 +198,159 @@ __global__ void k_amr_vmult(const AmrArgs a)
       }
     }
     if (a.tangent) evaluate<n>(a, T, Tv, Tx, Ty, Tz, t1, t2, s1, s2, s3, t);
-    evaluate<n>(a, u, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
-    // quadrature point t: rho_cp/dt u and the flux k grad(u) (+ k1 grad(T_lin) u)
-    {
-      const int qx = t % n, qy = (t / n) % n, qz = t / (n * n);
-      const double hx = a.h[0] * size, hy = a.h[1] * size, hz = a.h[2] * size;
-      const double jxw = a.w[qx] * a.w[qy] * a.w[qz] * hx * hy * hz;
-      const double k = a.tangent ? a.k0 + a.k1 * Tv[t] : a.k0;
-      double fx = k * gx[t] / hx, fy = k * gy[t] / hy, fz = k * gz[t] / hz;
-      if (a.tangent) {
-        fx += a.k1 * Tx[t] / hx * val[t];
-        fy += a.k1 * Ty[t] / hy * val[t];
-        fz += a.k1 * Tz[t] / hz * val[t];
-      }
-      val[t] = a.cval * val[t] * jxw;
-      gx[t] = fx * jxw / hx;
-      gy[t] = fy * jxw / hy;
-      gz[t] = fz * jxw / hz;
-    }
-    __syncthreads();
-    // integration: S^T / Sd^T along z, then y, then x
-    s1[t] = line_sum<n>(a.S, val, t, 2, true) + line_sum<n>(a.Sd, gz, t, 2, true);
-    s2[t] = line_sum<n>(a.S, gx, t, 2, true);
-    s3[t] = line_sum<n>(a.S, gy, t, 2, true);
-    __syncthreads();
-    t1[t] = line_sum<n>(a.S, s1, t, 1, true) + line_sum<n>(a.Sd, s3, t, 1, true);
-    t2[t] = line_sum<n>(a.S, s2, t, 1, true);
-    __syncthreads();
-    u[t] = line_sum<n>(a.S, t1, t, 0, true) + line_sum<n>(a.Sd, t2, t, 0, true);
-    __syncthreads();
+    apply_cell<n>(a, size, u, Tv, Tx, Ty, Tz, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
     if (hang) {
       for (int d = 2; d >= 0; --d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], true, t);
     }
     if (!a.mask[dof]) atomicAdd(a.dst + dof, u[t]);
     __syncthreads();
+  }
+}
+
+// diag(F^T A_e F) per cell at its gathered DoFs (distinct within a cell), by applying the
+// cell operator to the cell's unit vectors (a cell on a hanging interface has no closed form)
+template <int n>
+__global__ void k_amr_diag(const AmrArgs a)
+{
+  constexpr int n3 = n * n * n;
+  __shared__ double u[n3], T[n3], tmp[n3], t1[n3], t2[n3], s1[n3], s2[n3], s3[n3];
+  __shared__ double val[n3], gx[n3], gy[n3], gz[n3], Tv[n3], Tx[n3], Ty[n3], Tz[n3];
+  const int t = threadIdx.x;
+  for (int64_t c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
+    const int code = a.code[c];
+    const int dof = a.idx[c * n3 + t];
+    const bool hang = (code & 0x1F8) != 0;
+    const double size = cell_size(code);
+    if (a.tangent) {
+      T[t] = a.Tl[dof];
+      __syncthreads();
+      if (hang)
+        for (int d = 0; d < 3; ++d) hang_dir<n>(T, tmp, code, d, a.I[(code >> d) & 1], false, t);
+      evaluate<n>(a, T, Tv, Tx, Ty, Tz, t1, t2, s1, s2, s3, t);
+    }
+    double mine = 0.0;
+    for (int j = 0; j < n3; ++j) {
+      u[t] = t == j ? 1.0 : 0.0;
+      __syncthreads();
+      if (hang)
+        for (int d = 0; d < 3; ++d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], false, t);
+      apply_cell<n>(a, size, u, Tv, Tx, Ty, Tz, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
+      if (hang)
+        for (int d = 2; d >= 0; --d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], true, t);
+      if (t == j) mine = u[t];
+      __syncthreads();
+    }
+    if (!a.mask[dof]) atomicAdd(a.dst + dof, mine);
+    __syncthreads();
+  }
+}
+
+// dst += -R(T) (create_rhs): T = a.Tl, T_old = a.src, the nodal source a.q (nullable), all
+// read plain and interpolated by the hanging rule; Dirichlet rows untouched
+template <int n>
+__global__ void k_amr_rhs(const AmrArgs a)
+{
+  constexpr int n3 = n * n * n;
+  __shared__ double u[n3], T[n3], tmp[n3], t1[n3], t2[n3], s1[n3], s2[n3], s3[n3];
+  __shared__ double val[n3], gx[n3], gy[n3], gz[n3], To[n3], Q[n3], Tov[n3], Qv[n3];
+  const int t = threadIdx.x;
+  for (int64_t c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
+    const int code = a.code[c];
+    const int dof = a.idx[c * n3 + t];
+    const bool hang = (code & 0x1F8) != 0;
+    const double size = cell_size(code);
+    T[t] = a.Tl[dof];
+    To[t] = a.src[dof];
+    Q[t] = a.q ? a.q[dof] : 0.0;
+    __syncthreads();
+    if (hang) {
+      for (int d = 0; d < 3; ++d) {
+        const double *I = a.I[(code >> d) & 1];
+        hang_dir<n>(T, tmp, code, d, I, false, t);
+        hang_dir<n>(To, tmp, code, d, I, false, t);
+        hang_dir<n>(Q, tmp, code, d, I, false, t);
+      }
+    }
+    // values of T_old and the source at the q-points (gx.. as scratch), then T's values and
+    // gradients
+    evaluate<n>(a, To, Tov, gx, gy, gz, t1, t2, s1, s2, s3, t);
+    evaluate<n>(a, Q, Qv, gx, gy, gz, t1, t2, s1, s2, s3, t);
+    evaluate<n>(a, T, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
+    {
+      const int qx = t % n, qy = (t / n) % n, qz = t / (n * n);
+      const double hx = a.h[0] * size, hy = a.h[1] * size, hz = a.h[2] * size;
+      const double jxw = a.w[qx] * a.w[qy] * a.w[qz] * hx * hy * hz;
+      const double k = a.k0 + a.k1 * val[t];
+      const double v = a.cval * (val[t] - Tov[t]) - Qv[t];
+      val[t] = -v * jxw;
+      gx[t] = -k * gx[t] / (hx * hx) * jxw;
+      gy[t] = -k * gy[t] / (hy * hy) * jxw;
+      gz[t] = -k * gz[t] / (hz * hz) * jxw;
+    }
+    __syncthreads();
+    integrate_cell<n>(a, u, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
+    if (hang) {
+      for (int d = 2; d >= 0; --d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], true, t);
+    }
+    if (!a.mask[dof]) atomicAdd(a.dst + dof, u[t]);
+    __syncthreads();
+  }
+}
+
+// vector kernels of the Krylov solve on the refined mesh (sums by block reduction and one
+// atomic add per block into a device scalar)
+__global__ void k_amr_dot(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
+                          double *out)
+{
+  __shared__ double red[32];
+  double v = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v += a[i] * b[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) atomicAdd(out, v);
+  }
+}
+
+// y = a x + b y (x, y may alias nothing else)
+__global__ void k_amr_axpby(int64_t n, double a, const double *__restrict__ x, double b, double *y)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = a * x[i] + b * y[i];
+}
+
+// z = D r
+__global__ void k_amr_mul(int64_t n, const double *__restrict__ D, const double *__restrict__ r,
+                          double *z)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = D[i] * r[i];
+}
+
+// d <- |d| > 1e-10 ? 1/d : 1 (Dirichlet DoFs, left zero, become 1)
+__global__ void k_amr_invert(int64_t n, double *d)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = fabs(d[i]) > 1e-10 ? 1.0 / d[i] : 1.0;
+}
+
+// linear predictor (1 + r) T - r T_old, history commit T_old <- T, Dirichlet DoFs zero
+__global__ void k_amr_predict(int64_t n, double r, double *T, double *To,
+                              const uint8_t *__restrict__ mask)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double t = T[i], pred = (1.0 + r) * t - r * To[i];
+    To[i] = t;
+    T[i] = mask[i] ? 0.0 : pred;
   }
 }
 
@@ -196,6 +379,9 @@ struct mpdg_amr {
   int *d_idx = nullptr;
   uint16_t *d_code = nullptr;
   uint8_t *d_mask = nullptr;
+  // Krylov / step workspace (n_dofs each) and a device scalar for the sums
+  double *w[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  double *d_sum = nullptr;
 };
 
 namespace {
@@ -216,6 +402,12 @@ void release(mpdg_amr *h)
   h->d_idx = nullptr;
   h->d_code = nullptr;
   h->d_mask = nullptr;
+  for (double *&v : h->w) {
+    if (v) cudaFree(v);
+    v = nullptr;
+  }
+  if (h->d_sum) cudaFree(h->d_sum);
+  h->d_sum = nullptr;
 }
 
 // the host description: active cells, node numbering, hanging nodes, DoFs, cell data
@@ -471,9 +663,6 @@ extern "C" int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine
       if (((int64_t)desc->cells[d] << max_level) >= ((int64_t)1 << 20))
         return fail(MPDG_ERR_INVALID_ARGUMENT,
                     "hanging-node mesh: cells per direction x 2^level must stay below 2^20");
-    if (device >= 0 && max_level > 1)
-      return fail(MPDG_ERR_NOT_SUPPORTED,
-                  "hanging-node meshes on the GPU: one refinement level (several on the host only)");
   }
   mpdg_amr *h = new (std::nothrow) mpdg_amr();
   if (!h) return fail(MPDG_ERR_OUT_OF_MEMORY, "hanging-node mesh: host allocation failed");
@@ -496,11 +685,6 @@ extern "C" int mpdg_amr_create(const mpdg_mesh_desc *desc, const uint8_t *refine
   if (rc != MPDG_OK) {
     delete h;
     return rc;
-  }
-  if (device >= 0 && h->max_level > 1) {
-    delete h;
-    return fail(MPDG_ERR_NOT_SUPPORTED,
-                "hanging-node meshes on the GPU: one refinement level (several on the host only)");
   }
   if (device >= 0 && h->n_cells * (int64_t)h->n * h->n * h->n >= ((int64_t)1 << 31)) {
     delete h;
@@ -580,35 +764,34 @@ extern "C" int mpdg_amr_set_material(mpdg_amr *h, const mpdg_material *m, double
   return MPDG_OK;
 }
 
-extern "C" int mpdg_amr_vmult(mpdg_amr *h, double *dst, const double *src, const double *T_lin)
+namespace {
+
+int check_device_vectors(std::initializer_list<const void *> ptrs)
 {
-  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
-  if (h->device < 0) return fail(MPDG_ERR_INVALID_ARGUMENT, "host-only hanging-node mesh");
-  if (!h->mat_set) return fail(MPDG_ERR_INVALID_ARGUMENT, "call mpdg_amr_set_material first");
-  const bool tangent = h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0;
-  if (tangent && !T_lin)
-    return fail(MPDG_ERR_INVALID_ARGUMENT, "LINEAR_K needs the linearisation point");
-  for (const void *ptr : {(const void *)dst, (const void *)src, (const void *)T_lin}) {
+  for (const void *ptr : ptrs) {
     if (!ptr) continue;
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || at.type != cudaMemoryTypeDevice)
       return fail(MPDG_ERR_INVALID_ARGUMENT, "vectors must be device memory");
   }
-  cudaError_t e = cudaSetDevice(h->device);
-  if (e != cudaSuccess) return fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+  return MPDG_OK;
+}
+
+// kernel arguments of the handle's operator at the linearisation point T_lin (LINEAR_K)
+AmrArgs make_args(const mpdg_amr *h, const double *T_lin)
+{
+  const bool tangent = h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0;
   AmrArgs a;
   std::memset(&a, 0, sizeof(a));
   a.idx = h->d_idx;
   a.code = h->d_code;
   a.mask = h->d_mask;
-  a.src = src;
-  a.Tl = tangent ? T_lin : src;
-  a.dst = dst;
+  a.Tl = T_lin;
   a.n_cells = h->n_cells;
   for (int d = 0; d < 3; ++d) a.h[d] = h->h[d];
   a.cval = h->mat.rho_l * h->mat.cp_l / h->dt;
   a.k0 = h->mat.k_l;
-  a.k1 = tangent ? h->mat.k1 : 0.0;
+  a.k1 = h->mat.law == MPDG_LAW_LINEAR_K ? h->mat.k1 : 0.0;
   a.tangent = tangent;
   const int n = h->n;
   mpdg::Tables1D tb = mpdg::make_tables(n);
@@ -619,20 +802,253 @@ extern "C" int mpdg_amr_vmult(mpdg_amr *h, double *dst, const double *src, const
       a.Sd[q * n + i] = mpdg::lagrange_d(tb.xl, n, i, tb.xg[q]);
     }
   }
-  for (int s = 0; s < 2; ++s)
+  for (int s2 = 0; s2 < 2; ++s2)
     for (int j = 0; j < n; ++j)
-      for (int i = 0; i < n; ++i) a.I[s][j * n + i] = mpdg::lagrange(tb.xl, n, i, 0.5 * (s + tb.xl[j]));
-  k_amr_zero<<<256, 256>>>(h->n_dofs, dst);
+      for (int i = 0; i < n; ++i)
+        a.I[s2][j * n + i] = mpdg::lagrange(tb.xl, n, i, 0.5 * (s2 + tb.xl[j]));
+  return a;
+}
+
+enum { CELL_VMULT = 0, CELL_DIAG = 1, CELL_RHS = 2 };
+
+template <int n>
+void launch_n(int kind, const AmrArgs &a, int grid)
+{
+  constexpr int n3 = n * n * n;
+  if (kind == CELL_VMULT) k_amr_vmult<n><<<grid, n3>>>(a);
+  else if (kind == CELL_DIAG) k_amr_diag<n><<<grid, n3>>>(a);
+  else k_amr_rhs<n><<<grid, n3>>>(a);
+}
+
+int launch_cells(const mpdg_amr *h, int kind, const AmrArgs &a)
+{
   const int grid = (int)std::min<int64_t>(h->n_cells, 148 * 16);
-  switch (n) {
-    case 2: k_amr_vmult<2><<<grid, 8>>>(a); break;
-    case 3: k_amr_vmult<3><<<grid, 27>>>(a); break;
-    case 4: k_amr_vmult<4><<<grid, 64>>>(a); break;
-    case 5: k_amr_vmult<5><<<grid, 125>>>(a); break;
+  switch (h->n) {
+    case 2: launch_n<2>(kind, a, grid); break;
+    case 3: launch_n<3>(kind, a, grid); break;
+    case 4: launch_n<4>(kind, a, grid); break;
+    case 5: launch_n<5>(kind, a, grid); break;
     default: return fail(MPDG_ERR_INVALID_ARGUMENT, "degree");
   }
-  e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaDeviceSynchronize();
-  if (e != cudaSuccess) return fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int ready(const mpdg_amr *h)
+{
+  if (h->device < 0) return fail(MPDG_ERR_INVALID_ARGUMENT, "host-only hanging-node mesh");
+  if (!h->mat_set) return fail(MPDG_ERR_INVALID_ARGUMENT, "call mpdg_amr_set_material first");
+  const cudaError_t e = cudaSetDevice(h->device);
+  return e == cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int sync_status()
+{
+  const cudaError_t e = cudaDeviceSynchronize();
+  return e == cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int vgrid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
+
+int vmult_impl(mpdg_amr *h, double *dst, const double *src, const double *T_lin)
+{
+  AmrArgs a = make_args(h, T_lin);
+  a.src = src;
+  a.dst = dst;
+  if (!a.tangent) a.Tl = src;
+  k_amr_zero<<<vgrid(h->n_dofs), 256>>>(h->n_dofs, dst);
+  return launch_cells(h, CELL_VMULT, a);
+}
+
+int diag_impl(mpdg_amr *h, double *inv, const double *T_lin)
+{
+  AmrArgs a = make_args(h, T_lin);
+  a.dst = inv;
+  k_amr_zero<<<vgrid(h->n_dofs), 256>>>(h->n_dofs, inv);
+  TRY_AMR(launch_cells(h, CELL_DIAG, a));
+  k_amr_invert<<<vgrid(h->n_dofs), 256>>>(h->n_dofs, inv);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int rhs_impl(mpdg_amr *h, double *dst, const double *T, const double *T_old, const double *q)
+{
+  AmrArgs a = make_args(h, T);
+  a.Tl = T;
+  a.src = T_old;
+  a.q = q;
+  a.dst = dst;
+  return launch_cells(h, CELL_RHS, a);
+}
+
+int ensure_workspace(mpdg_amr *h)
+{
+  for (double *&v : h->w)
+    if (!v) {
+      const cudaError_t e = cudaMalloc(&v, sizeof(double) * (size_t)h->n_dofs);
+      if (e != cudaSuccess) {
+        v = nullptr;
+        return fail(MPDG_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      }
+    }
+  if (!h->d_sum) {
+    const cudaError_t e = cudaMalloc(&h->d_sum, sizeof(double));
+    if (e != cudaSuccess) {
+      h->d_sum = nullptr;
+      return fail(MPDG_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+  }
+  return MPDG_OK;
+}
+
+int dot(mpdg_amr *h, const double *a, const double *b, double *out)
+{
+  cudaMemset(h->d_sum, 0, sizeof(double));
+  k_amr_dot<<<vgrid(h->n_dofs), 256>>>(h->n_dofs, a, b, h->d_sum);
+  const cudaError_t e = cudaMemcpy(out, h->d_sum, sizeof(double), cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// Jacobi-CG (deal.II SolverCG semantics, ReductionControl) on the refined mesh: x from 0
+int cg_impl(mpdg_amr *h, double *x, const double *b, const double *inv, const double *T_lin,
+            double rel_tol, double abs_tol, int max_it, int *iterations)
+{
+  TRY_AMR(ensure_workspace(h));
+  const int64_t N = h->n_dofs;
+  const int g = vgrid(N);
+  double *r = h->w[0], *z = h->w[1], *p = h->w[2], *Ap = h->w[3];
+  k_amr_zero<<<g, 256>>>(N, x);
+  k_amr_axpby<<<g, 256>>>(N, 1.0, b, 0.0, r);
+  k_amr_mul<<<g, 256>>>(N, inv, r, z);
+  k_amr_axpby<<<g, 256>>>(N, 1.0, z, 0.0, p);
+  double rr = 0.0, rz = 0.0;
+  TRY_AMR(dot(h, r, r, &rr));
+  TRY_AMR(dot(h, r, z, &rz));
+  const double tol = std::max(abs_tol, rel_tol * std::sqrt(rr));
+  *iterations = 0;
+  if (std::sqrt(rr) <= tol) return MPDG_OK;
+  for (int it = 1; it <= max_it; ++it) {
+    TRY_AMR(vmult_impl(h, Ap, p, T_lin));
+    double pap = 0.0;
+    TRY_AMR(dot(h, p, Ap, &pap));
+    if (!(pap > 0.0)) return fail(MPDG_ERR_BREAKDOWN, "CG breakdown: p.Ap <= 0");
+    const double alpha = rz / pap;
+    k_amr_axpby<<<g, 256>>>(N, alpha, p, 1.0, x);
+    k_amr_axpby<<<g, 256>>>(N, -alpha, Ap, 1.0, r);
+    TRY_AMR(dot(h, r, r, &rr));
+    if (!std::isfinite(rr)) return fail(MPDG_ERR_NAN, "CG residual is not finite");
+    *iterations = it;
+    if (std::sqrt(rr) <= tol) return MPDG_OK;
+    k_amr_mul<<<g, 256>>>(N, inv, r, z);
+    double rz_new = 0.0;
+    TRY_AMR(dot(h, r, z, &rz_new));
+    k_amr_axpby<<<g, 256>>>(N, 1.0, z, rz_new / rz, p);
+    rz = rz_new;
+  }
+  return fail(MPDG_ERR_NOT_CONVERGED, "CG on the hanging-node mesh did not converge");
+}
+
+}  // namespace
+
+extern "C" int mpdg_amr_vmult(mpdg_amr *h, double *dst, const double *src, const double *T_lin)
+{
+  if (!h || !dst || !src) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY_AMR(ready(h));
+  const bool tangent = h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0;
+  if (tangent && !T_lin)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "LINEAR_K needs the linearisation point");
+  TRY_AMR(check_device_vectors({dst, src, T_lin}));
+  TRY_AMR(vmult_impl(h, dst, src, T_lin));
+  return sync_status();
+}
+
+extern "C" int mpdg_amr_inverse_diagonal(mpdg_amr *h, double *inv_diag, const double *T_lin)
+{
+  if (!h || !inv_diag) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY_AMR(ready(h));
+  const bool tangent = h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0;
+  if (tangent && !T_lin)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "LINEAR_K needs the linearisation point");
+  TRY_AMR(check_device_vectors({inv_diag, T_lin}));
+  TRY_AMR(diag_impl(h, inv_diag, T_lin));
+  return sync_status();
+}
+
+extern "C" int mpdg_amr_create_rhs(mpdg_amr *h, double *dst, const double *T, const double *T_old,
+                                   const double *heat_source)
+{
+  if (!h || !dst || !T || !T_old) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY_AMR(ready(h));
+  TRY_AMR(check_device_vectors({dst, T, T_old, heat_source}));
+  TRY_AMR(rhs_impl(h, dst, T, T_old, heat_source));
+  return sync_status();
+}
+
+extern "C" int mpdg_amr_linear_solve(mpdg_amr *h, double *x, const double *b, const double *T_lin,
+                                     double rel_tolerance, double abs_tolerance,
+                                     int max_iterations, int *iterations)
+{
+  if (!h || !x || !b) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY_AMR(ready(h));
+  const bool tangent = h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0;
+  if (tangent && !T_lin)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "LINEAR_K needs the linearisation point");
+  TRY_AMR(check_device_vectors({x, b, T_lin}));
+  TRY_AMR(ensure_workspace(h));
+  int its = 0;
+  double *inv = h->w[4];
+  TRY_AMR(diag_impl(h, inv, T_lin));
+  const int rc = cg_impl(h, x, b, inv, T_lin, rel_tolerance, abs_tolerance, max_iterations, &its);
+  if (iterations) *iterations = its;
+  if (rc != MPDG_OK) return rc;
+  return sync_status();
+}
+
+extern "C" int mpdg_amr_time_step(mpdg_amr *h, double dt, double dt_old, double *T_cur,
+                                  double *T_old, const double *heat_source,
+                                  const mpdg_step_params *prm, mpdg_step_stats *stats)
+{
+  if (!h || !T_cur || !T_old || !prm) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  TRY_AMR(ready(h));
+  if (dt == 0.0) return fail(MPDG_ERR_ZERO_TIME_INCREMENT, "time increment is zero");
+  TRY_AMR(check_device_vectors({T_cur, T_old, heat_source}));
+  TRY_AMR(ensure_workspace(h));
+  h->dt = dt;
+  const int64_t N = h->n_dofs;
+  const int g = vgrid(N);
+  mpdg_step_stats s;
+  std::memset(&s, 0, sizeof(s));
+  // init_time_advance: linear predictor (predictor_linear.cpp:74-96) or a copy, history commit,
+  // Dirichlet values (zero on these meshes); Jacobi at the predicted state
+  const double r = (prm->predictor == MPDG_PREDICTOR_LINEAR && std::fabs(dt_old) >= 1e-12)
+                     ? dt / dt_old : 0.0;
+  k_amr_predict<<<g, 256>>>(N, r, T_cur, T_old, h->d_mask);
+  const bool tangent = h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0;
+  double *rhs = h->w[5], *delta = h->w[6], *inv = h->w[4];
+  TRY_AMR(diag_impl(h, inv, tangent ? T_cur : nullptr));
+  // Newton-Raphson (newton_raphson_solver.cpp:22-68): rhs = -R(T); J delta = rhs; converged
+  // when |rhs| < tol_res and |delta| < tol_corr (the converged update is not applied)
+  for (int it = 0; it < prm->newton_max_iterations; ++it) {
+    k_amr_zero<<<g, 256>>>(N, rhs);
+    TRY_AMR(rhs_impl(h, rhs, T_cur, T_old, heat_source));
+    int its = 0;
+    TRY_AMR(cg_impl(h, delta, rhs, inv, tangent ? T_cur : nullptr, prm->linear.rel_tolerance,
+                    prm->linear.abs_tolerance, prm->linear.max_iterations, &its));
+    s.linear_iterations += its;
+    double rr = 0.0, dd = 0.0;
+    TRY_AMR(dot(h, rhs, rhs, &rr));
+    TRY_AMR(dot(h, delta, delta, &dd));
+    if (std::sqrt(rr) < prm->newton_residual_tolerance &&
+        std::sqrt(dd) < prm->newton_correction_tolerance) {
+      s.converged = 1;
+      s.newton_iterations = it + 1;
+      break;
+    }
+    k_amr_axpby<<<g, 256>>>(N, 1.0, delta, 1.0, T_cur);
+    s.newton_iterations = it + 1;
+  }
+  if (stats) *stats = s;
+  TRY_AMR(sync_status());
+  if (!s.converged) return fail(MPDG_ERR_NEWTON_NOT_CONVERGED, "Newton-Raphson did not converge");
   return MPDG_OK;
 }

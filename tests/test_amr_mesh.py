@@ -50,8 +50,8 @@ def test_invalid_meshes_rejected_without_gpu():
 
 def test_multilevel_host_description_matches_oracle():
     """Levels 0, 1 and 2 (2:1 balanced) on the host: DoFs, support points, mask, gathered DoFs
-    and codes (bits 10-12 the level) equal the oracle's multi-level mesh; a device handle is
-    refused before any CUDA call."""
+    and codes (bits 10-12 the level) equal the oracle's multi-level mesh; a level above the
+    maximum or an unbalanced mesh is refused before any CUDA call, on a device too."""
     p = 2
     lev = np.zeros((5, 5, 5), dtype=np.int64)
     lev[1:4, 1:4, 1:4] = 1
@@ -68,8 +68,10 @@ def test_multilevel_host_description_matches_oracle():
         assert np.array_equal(dofs[c], idx), c
         assert int(codes[c]) & 0x1FF == o.hanging_code(c), c
         assert (int(codes[c]) >> 10) & 7 == o.cell_level[c]
-    with pytest.raises(H.ExcNotImplemented):
-        AmrHeatOperator(mesh, lev, device=0)
+    too_deep = lev.copy()
+    too_deep[2, 2, 2] = 7
+    with pytest.raises(H.ExcInvalidArgument):
+        AmrHeatOperator(mesh, too_deep, device=0)
     bad = lev.copy()
     bad[0, 0, 0] = 2
     with pytest.raises(H.ExcInvalidArgument):

@@ -315,6 +315,13 @@ typedef struct {
                                      in the x-z plane, z the depth direction; 0: 3D         */
 } mpdg_laser;
 int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser *laser);
+/* The same laser as the source of the residual, evaluated at the support points inside the
+ * create_rhs cell kernels (no nodal source vector is written or read): create_rhs and the time
+ * steps use it wherever their heat_source is NULL, with the same values as
+ * mpdg_heat_laser_source followed by create_rhs on that vector (the reference integrates the
+ * nodal interpolant, heat_diffuse_operator.cpp:445-447). NULL switches it off; call again when
+ * the power or the position change (every step of a moving laser). */
+int mpdg_heat_set_laser(mpdg_heat *h, const mpdg_laser *laser);
 
 /* ---- preconditioner + linear solver ---------------------------------- */
 /* JacobiPreconditioner::update (preconditioner_jacobi.hpp:65-69): stores the inverse

@@ -122,6 +122,7 @@ _SIGS = {
     "mpdg_heat_compute_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),
     "mpdg_heat_set_dof_permutation": (C.c_int, [_H, _P]),
+    "mpdg_heat_set_laser": (C.c_int, [_H, _P]),
     "mpdg_heat_dcg_start": (C.c_int, [_H, C.c_int64, _D, _D, _D, _D, _D, _D, _D]),
     "mpdg_heat_dcg_dot": (C.c_int, [_H, C.c_int64, _D, _D, _D]),
     "mpdg_heat_dcg_update": (C.c_int, [_H, C.c_int64, _D, _D, _D, _D, _D, _D, _D, _D]),

@@ -3,6 +3,8 @@
 
 #include <stdint.h>
 
+#include "fe_tables.hpp"
+
 namespace mpdg {
 
 // ---------------------------------------------------------------------------
@@ -42,6 +44,35 @@ struct SolverState {
   double hist_alpha[64], hist_beta[64];
 };
 
+// ---------------------------------------------------------------------------
+// the support points of the DoFs and a volumetric laser source evaluated there
+// ---------------------------------------------------------------------------
+struct Q1D {
+  double xg[kMaxN], wg[kMaxN], xl[kMaxN];
+};
+
+struct PosArgs {
+  MeshDims d;
+  int geo;
+  double lo[3], hc[3];
+  Q1D q1;
+  const double *vert;
+};
+
+struct LaserArgs {
+  int profile, planar;  // planar: the y coordinate is ignored (2D profile in the x-z plane)
+  double power, c[3], dir[3], radius, peak;
+  double rho, beta, L, lambda, a, D;  // Gusarov
+};
+
+// a residual kernel's nodal heat source evaluated in place: the laser intensity at the
+// support points (on = 1) instead of a nodal source vector
+struct SourceEval {
+  int on;
+  LaserArgs laser;
+  PosArgs pos;
+};
+
 enum FinMode { FIN_NONE = 0, FIN_STORE = 1, FIN_CG_ALPHA = 2 };
 
 template <typename T>
@@ -66,6 +97,7 @@ struct CellArgs {
   double *out;         // FIN_STORE destination
   const double *extra_dot;  // boundary-face part of src.dst, added at finalisation (nullable)
   int fin;
+  SourceEval source;  // create_rhs: the laser source at the support points (source.on)
 };
 
 // ---------------------------------------------------------------------------

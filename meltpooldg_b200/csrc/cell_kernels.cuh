@@ -33,6 +33,7 @@
 #include "fe_tables.hpp"
 #include "material_law.cuh"
 #include "reduce.cuh"
+#include "source_eval.cuh"
 
 namespace mpdg {
 
@@ -244,11 +245,15 @@ __device__ __forceinline__ void prefetch_next_batch(const MeshDims &d, int64_t n
 // ---------------------------------------------------------------------------
 // vmult: dst += J src (dst zeroed by the caller); optional src.dst dot
 // ---------------------------------------------------------------------------
-template <int n, typename T, int GEO, int LAW>
+// PRE (deformed meshes): this batch's per-point geometry (7 values at each of the thread's n
+// points) is loaded into registers when the batch starts, so those loads are in flight during
+// the gather and the evaluation sweeps instead of stalling the quadrature-point loop.
+template <int n, typename T, int GEO, int LAW, bool PRE = false>
 __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
 {
   constexpr int n2 = n * n, n3 = n2 * n, CPB = cells_per_block(n);
   constexpr bool TDEP = law_tdep<LAW>();
+  static_assert(!PRE || GEO == 1, "the geometry preload is for per-point geometry");
   constexpr int NF = TDEP ? 11 : 6;
   if (a.st && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -270,6 +275,14 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
     const int j = line % n, k = line / n;
     const int I0 = d.p * cx, J = d.p * cy + j, K = d.p * cz + k;
     const int64_t row = (int64_t)d.nd[0] * (J + (int64_t)d.nd[1] * K) + I0;
+    T gpre[PRE ? n : 1][7];
+    if (PRE) {
+      const T *gb = a.g.q + cc * 7 * n3 + line;
+#pragma unroll
+      for (int r = 0; r < n; ++r)
+#pragma unroll
+        for (int c = 0; c < 7; ++c) gpre[r][c] = __ldg(gb + c * n3 + n2 * r);
+    }
     // the geometry, or the coefficient fields of LAW 4/5, dominate a batch's q-point loads
     if (GEO == 1)
       prefetch_next_batch<n>(d, a.n_cells, batch + gridDim.x, cl, j, k, a.src,
@@ -309,7 +322,13 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
       const int q = line + n2 * r;
       const int qi = q % n, qj = (q / n) % n, qk = q / n2;
       T jxw, G[6];
-      geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
+      if (PRE) {
+        jxw = gpre[r][0];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) G[c] = gpre[r][1 + c];
+      } else {
+        geo_at<n, GEO>(a.g, cc, qi, qj, qk, jxw, G);
+      }
       T rhocp, kk, drhocp, dk;
       const T uu = u[q];
       T val, b0 = T(0), b1 = T(0), b2 = T(0);
@@ -412,7 +431,10 @@ __global__ void __launch_bounds__(block_threads(n)) k_rhs(CellArgs<double> a)
     gather_xline<n>(d, row, I0, J, K, false, a.To, x, active);
 #pragma unroll
     for (int i = 0; i < n; ++i) Toq[i + n * line] = x[i];
-    if (a.qs) {
+    if (a.source.on) {
+#pragma unroll
+      for (int i = 0; i < n; ++i) x[i] = active ? source_at(a.source, row + i) : T(0);
+    } else if (a.qs) {
       gather_xline<n>(d, row, I0, J, K, false, a.qs, x, active);
     } else {
 #pragma unroll

@@ -674,7 +674,9 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_rhs2(CellArgs<double> a)
         T tv = T(0), w = T(0);
         if (active) {
           tv = __ldg(a.Tl + row + i);
-          w = c * (tv - __ldg(a.To + row + i)) - (a.qs ? __ldg(a.qs + row + i) : T(0));
+          const T qv = a.source.on ? (T)source_at(a.source, row + i)
+                                   : (a.qs ? __ldg(a.qs + row + i) : T(0));
+          w = c * (tv - __ldg(a.To + row + i)) - qv;
         }
         Pt[j][i] = tv;
         Pw[j][i] = w;

@@ -45,6 +45,18 @@ static inline bool fp32_packed()
   return on != 0;
 }
 
+// Line-per-thread operator on deformed meshes: the batch's per-point geometry
+// preloaded into registers (default) or loaded in the quadrature-point loop
+// (MPDG_GEO_PRELOAD=0); both compute the same operator.
+static inline bool geo_preload()
+{
+  static const int on = [] {
+    const char *e = getenv("MPDG_GEO_PRELOAD");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return on != 0;
+}
+
 template <int n>
 struct DegreeOps {
   static constexpr int CPB = cells_per_block(n);
@@ -96,10 +108,19 @@ struct DegreeOps {
       k2<<<g2, 32 * kV2Warps, smem2, s>>>(a);
       return cudaGetLastError();
     } else {
-      static int cache = 0;
-      auto k = k_vmult<n, T, GEO, LAW>;
       const size_t smem = smem_vmult<n, T>(law_tdep<LAW>());
       const int64_t nb = (a.n_cells + CPB - 1) / CPB;
+      if constexpr (GEO == 1) {
+        if (geo_preload()) {
+          static int cachep = 0;
+          auto kp = k_vmult<n, T, GEO, LAW, true>;
+          const int g = persistent_grid(kp, THREADS, smem, nb, sm, &cachep);
+          kp<<<g, THREADS, smem, s>>>(a);
+          return cudaGetLastError();
+        }
+      }
+      static int cache = 0;
+      auto k = k_vmult<n, T, GEO, LAW>;
       const int g = persistent_grid(k, THREADS, smem, nb, sm, &cache);
       k<<<g, THREADS, smem, s>>>(a);
       return cudaGetLastError();

@@ -25,6 +25,7 @@
 #include "fe_tables.hpp"
 #include "material_law.cuh"
 #include "reduce.cuh"
+#include "source_eval.cuh"
 
 using namespace mpdg;
 
@@ -155,6 +156,9 @@ struct mpdg_heat {
   // and the caller's DoF numbering (lex[i] = lexicographic index of the caller's DoF i)
   double *hv_T = nullptr, *hv_To = nullptr, *hv_a = nullptr, *hv_b = nullptr, *hv_c = nullptr;
   int64_t *perm = nullptr, *perm_buf = nullptr;  // perm: perm_buf while a permutation is set
+  // mpdg_heat_set_laser: the residual evaluates this laser at the support points in place of a
+  // NULL heat_source
+  SourceEval source{};
   const double *guess = nullptr;
   // MPDG_PREDICTOR_LINEAR_DIRECTION: the increment direction d, and for the next solve the
   // operator applied to its initial guess (x_Ax_scale * x_Ax = A x, computed by the step)
@@ -278,35 +282,6 @@ static int upload_tables(int device, int n)
 // ---------------------------------------------------------------------------
 // setup kernels
 // ---------------------------------------------------------------------------
-struct Q1D {
-  double xg[kMaxN], wg[kMaxN], xl[kMaxN];
-};
-
-__device__ __forceinline__ void trilinear(const double *__restrict__ vert, const MeshDims &d, int cx,
-                                          int cy, int cz, const double xi[3], double x[3],
-                                          double J[3][3])
-{
-  for (int a = 0; a < 3; ++a) {
-    x[a] = 0.0;
-    for (int b = 0; b < 3; ++b) J[a][b] = 0.0;
-  }
-  for (int v = 0; v < 8; ++v) {
-    const int a = v & 1, b = (v >> 1) & 1, c = (v >> 2) & 1;
-    const int64_t vid =
-      (int64_t)(cx + a) + (int64_t)(d.m[0] + 1) * ((cy + b) + (int64_t)(d.m[1] + 1) * (cz + c));
-    const double *X = vert + 3 * vid;
-    const double na = a ? xi[0] : 1.0 - xi[0], da = a ? 1.0 : -1.0;
-    const double nb = b ? xi[1] : 1.0 - xi[1], db = b ? 1.0 : -1.0;
-    const double nc = c ? xi[2] : 1.0 - xi[2], dc = c ? 1.0 : -1.0;
-    const double N = na * nb * nc;
-    const double dN[3] = {da * nb * nc, na * db * nc, na * nb * dc};
-    for (int e = 0; e < 3; ++e) {
-      x[e] += X[e] * N;
-      for (int f = 0; f < 3; ++f) J[e][f] += X[e] * dN[f];
-    }
-  }
-}
-
 // per-quadrature-point JxW and G = JxW J^-1 J^-T of the trilinear map
 __global__ void k_geometry(int64_t n_cells, MeshDims d, int n, Q1D q1, const double *vert,
                            double *geo)
@@ -421,35 +396,6 @@ __global__ void k_coef_fields(FieldArgs a)
   }
 }
 
-struct PosArgs {
-  MeshDims d;
-  int geo;
-  double lo[3], hc[3];
-  Q1D q1;
-  const double *vert;
-};
-
-__device__ __forceinline__ void dof_position(const PosArgs &a, int64_t idx, double x[3])
-{
-  const int64_t I = idx % a.d.nd[0];
-  const int64_t J = (idx / a.d.nd[0]) % a.d.nd[1];
-  const int64_t K = idx / ((int64_t)a.d.nd[0] * a.d.nd[1]);
-  const int64_t pos[3] = {I, J, K};
-  int cc[3];
-  double xi[3];
-  for (int e = 0; e < 3; ++e) {
-    cc[e] = (int)(pos[e] / a.d.p);
-    if (cc[e] >= a.d.m[e]) cc[e] = a.d.m[e] - 1;
-    xi[e] = a.q1.xl[pos[e] - (int64_t)cc[e] * a.d.p];
-  }
-  if (a.geo == 0) {
-    for (int e = 0; e < 3; ++e) x[e] = a.lo[e] + a.hc[e] * (cc[e] + xi[e]);
-  } else {
-    double J3[3][3];
-    trilinear(a.vert, a.d, cc[0], cc[1], cc[2], xi, x, J3);
-  }
-}
-
 __global__ void k_support_points(int64_t N, PosArgs a, double *xyz)
 {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
@@ -474,48 +420,6 @@ __global__ void k_gaussian(int64_t N, PosArgs a, double *q, double amp, double c
   }
 }
 
-// volumetric laser intensity at x (laser_intensity_profiles.hpp), parameters precomputed
-// on the host
-struct LaserArgs {
-  int profile, planar;  // planar: the y coordinate is ignored (2D profile in the x-z plane)
-  double power, c[3], dir[3], radius, peak;
-  double rho, beta, L, lambda, a, D;  // Gusarov
-};
-__device__ __forceinline__ double gusarov_dq_dxi(const LaserArgs &g, double xi)
-{
-  const double rho = g.rho, a = g.a, lambda = g.lambda;
-  if (!(xi < lambda)) return 0.0;
-  return (3 - 3 * rho) * (exp(-xi) + rho * exp(xi - 2 * lambda)) / (4 * rho - 3) +
-         2 * a * a * rho / (g.D * (4 * rho - 3)) *
-           (exp(-lambda) * (1 - rho * rho) * (exp(-2 * a * xi) * (a - 1) + exp(2 * a * xi) * (a + 1)) -
-            (rho * exp(-2 * lambda) + 3) * (exp(2 * a * (xi - lambda)) * (1 - a - rho * (a + 1)) -
-                                            exp(2 * a * (lambda - xi)) * (a + rho * (a - 1) + 1)));
-}
-__device__ __forceinline__ double laser_intensity(const LaserArgs &g, const double x[3])
-{
-  const double v0 = x[0] - g.c[0], v1 = g.planar ? 0.0 : x[1] - g.c[1], v2 = x[2] - g.c[2];
-  if (g.profile == MPDG_LASER_UNIFORM) return g.power;
-  if (g.profile == MPDG_LASER_GAUSS_VOLUMETRIC) {
-    const double s2 = (v0 * v0 + v1 * v1 + v2 * v2) / (g.radius * g.radius);
-    return g.peak * exp(-2.0 * s2);
-  }
-  if (g.profile == MPDG_LASER_GAUSS_PROJECTION) {
-    const double w0 = v1 * g.dir[2] - v2 * g.dir[1], w1 = v2 * g.dir[0] - v0 * g.dir[2],
-                 w2 = v0 * g.dir[1] - v1 * g.dir[0];
-    const double s2 = (w0 * w0 + w1 * w1 + w2 * w2) / (g.radius * g.radius);
-    return g.peak * exp(-2.0 * s2);
-  }
-  // Gusarov: z measured downwards from the beam centre; zero outside the layer
-  const double dist = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-  const double z = -(x[2] - g.c[2]);
-  if (z >= g.L || z < g.c[2]) return 0.0;
-  double pd = 0.0;
-  if (dist <= g.radius) {
-    const double m = 1.0 - dist / g.radius, p = 1.0 + dist / g.radius;
-    pd = 3.0 * g.power / (M_PI * g.radius * g.radius) * (m * m) * (p * p);
-  }
-  return -g.beta * pd * gusarov_dq_dxi(g, z * g.beta);
-}
 __global__ void k_laser(int64_t N, PosArgs a, LaserArgs g, double *q)
 {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
@@ -3111,6 +3015,7 @@ static int create_rhs(mpdg_heat *h, double *dst, const double *src, const double
   a.Tl = h->T_lin;
   a.To = src;
   a.qs = q;
+  if (!q && h->source.on) a.source = h->source;
   CU(h->tab.rhs(a, h->geo, klaw(h), h->stream, h->sm_count));
   ++h->launches;
   if (any_faces(h)) TRY(launch_faces<double>(h, 1, dst, nullptr, h->T_lin, nullptr, nullptr));
@@ -3324,13 +3229,11 @@ extern "C" int mpdg_heat_support_points(mpdg_heat *h, double *xyz)
   return MPDG_OK;
 }
 
-extern "C" int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser *laser)
+static int laser_args(const mpdg_laser *laser, LaserArgs &g)
 {
-  if (!h || !q || !laser) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
   const int pr = laser->profile;
   if (pr < MPDG_LASER_UNIFORM || pr > MPDG_LASER_GUSAROV)
     return fail(MPDG_ERR_INVALID_ARGUMENT, "unknown laser intensity profile");
-  LaserArgs g;
   memset(&g, 0, sizeof(g));
   g.profile = pr;
   g.planar = laser->planar != 0;
@@ -3361,10 +3264,33 @@ extern "C" int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser 
     g.D = (1.0 - g.a) * (1.0 - g.a - g.rho * (1.0 + g.a)) * std::exp(-2.0 * g.a * g.lambda) -
           (1.0 + g.a) * (1.0 + g.a - g.rho * (1.0 - g.a)) * std::exp(2.0 * g.a * g.lambda);
   }
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_laser_source(mpdg_heat *h, double *q, const mpdg_laser *laser)
+{
+  if (!h || !q || !laser) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  LaserArgs g;
+  TRY(laser_args(laser, g));
   CU(cudaSetDevice(h->device));
   k_laser<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, pos_args(h), g, q);
   ++h->launches;
   CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_set_laser(mpdg_heat *h, const mpdg_laser *laser)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  if (!laser) {
+    h->source.on = 0;
+    return MPDG_OK;
+  }
+  LaserArgs g;
+  TRY(laser_args(laser, g));
+  h->source.laser = g;
+  h->source.pos = pos_args(h);
+  h->source.on = 1;
   return MPDG_OK;
 }
 

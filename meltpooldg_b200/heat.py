@@ -429,6 +429,18 @@ class HeatDiffuseOperator:
         check(self._L.mpdg_heat_laser_source(self.h, _ptr(q), C.byref(las)))
         return q
 
+    def set_laser(self, profile=None, power=0.0, position=(0.0, 0.0, 0.0), radius=1.0,
+                  direction=(0.0, 0.0, -1.0), gusarov=(0.0, 0.0, 0.0), planar=False):
+        """The laser as the residual's source, evaluated inside the create_rhs kernels wherever
+        the heat source is None (profile None switches it off)."""
+        if profile is None:
+            check(self._L.mpdg_heat_set_laser(self.h, None))
+            return
+        las = L.Laser(int(profile), float(power), (C.c_double * 3)(*map(float, position)),
+                      (C.c_double * 3)(*map(float, direction)), float(radius),
+                      *[float(v) for v in gusarov], int(bool(planar)))
+        check(self._L.mpdg_heat_set_laser(self.h, C.byref(las)))
+
     def gaussian_source(self, q, amplitude, center, radius):
         c = (C.c_double * 3)(*[float(v) for v in center])
         check(self._L.mpdg_heat_gaussian_source(self.h, _ptr(q), float(amplitude), c,

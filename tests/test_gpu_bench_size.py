@@ -51,10 +51,10 @@ def smooth_state(o, scale=1.0):
     return o.distribute(T)
 
 
-def pair(cells, perturb=0.0, seed=3):
-    o = O.Oracle(3, cells, perturb=perturb, seed=seed)
+def pair(cells, perturb=0.0, seed=3, degree=3):
+    o = O.Oracle(degree, cells, perturb=perturb, seed=seed)
     o.set_material(O.material(O.LAW_LINEAR_K, k=1.0, k1=0.5), DT)
-    g = H.HeatDiffuseOperator(H.box_mesh(3, cells, perturb=perturb, seed=seed))
+    g = H.HeatDiffuseOperator(H.box_mesh(degree, cells, perturb=perturb, seed=seed))
     g.set_material(H.material(**LAW))
     g.reset_time_increment(DT)
     return o, g
@@ -105,6 +105,14 @@ def test_bench_kernels_multi_batch_affine_48cubed():
 
 def test_bench_kernels_multi_batch_deformed_40cubed():
     o, g = pair((40, 40, 40), perturb=0.2, seed=8)
+    check_bench_kernels(o, g)
+
+
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+def test_production_degree_kernels_multi_batch_40cubed(perturb):
+    """FE_Q(4), the production run's degree (deformed +-0.2 h there): the line-per-thread FP64
+    tangent, the register-resident FP32 operators and the diagonals, 4,173,281 DoFs."""
+    o, g = pair((40, 40, 40), perturb=perturb, seed=8, degree=4)
     check_bench_kernels(o, g)
 
 

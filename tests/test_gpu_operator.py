@@ -144,6 +144,38 @@ def test_laser_source_matches_oracle(profile, degree, perturb, planar):
     assert np.abs(ref).max() > 0.0
 
 
+@pytest.mark.parametrize("profile", [1, 3])
+@pytest.mark.parametrize("degree,perturb,law", [(3, 0.0, "linear_k"), (2, 0.15, "constant"),
+                                                (4, 0.1, "liquid_solid")])
+def test_fused_laser_residual_equals_the_nodal_source_path(profile, degree, perturb, law):
+    """create_rhs with the laser evaluated at the support points inside the residual kernel
+    (mpdg_heat_set_laser, heat_source NULL) against create_rhs on the nodal source vector of
+    mpdg_heat_laser_source, and against the oracle: the register-plane kernel (p <= 3,
+    constant and linear-k laws) and the line-per-thread one (the rest)."""
+    lo, hi, cells = (0, 0, -1), (1, 1, 0), (5, 4, 6)
+    o = O.Oracle(degree, cells, lo=lo, hi=hi, perturb=perturb, seed=2)
+    o.set_material(O.material(**LAWS[law]), 1e-3)
+    g = H.HeatDiffuseOperator(H.box_mesh(degree, cells, lo, hi, perturb, 2))
+    g.set_material(H.material(**LAWS[law]))
+    g.reset_time_increment(1e-3)
+    kw = dict(radius=0.4, gusarov=(0.55, 15.0, 0.4))
+    c = (0.45, 0.5, 0.0)
+    rng = np.random.default_rng(degree)
+    N = o.n_dofs
+    T, To = rng.uniform(0, 1, N), rng.uniform(0, 1, N)
+    g.set_linearization(cuda(T), cuda(To))
+    q = g.laser_source(g.new_vector(), profile, 25.0, c, **kw)
+    nodal = g.create_rhs(g.new_vector(), cuda(To), q)
+    g.set_laser(profile, 25.0, c, **kw)
+    fused = g.create_rhs(g.new_vector(), cuda(To), None)
+    assert rel(fused, nodal.cpu().numpy()) <= 1e-14
+    ref = o.create_rhs(T, To, o.laser_source(profile, 25.0, c, **kw))
+    assert rel(fused, ref) <= TOL64
+    g.set_laser(None)
+    plain = g.create_rhs(g.new_vector(), cuda(To), None)
+    assert rel(plain, o.create_rhs(T, To, None)) <= TOL64
+
+
 def test_laser_source_rejects_bad_parameters():
     g = H.HeatDiffuseOperator(H.box_mesh(1, (2, 2, 2)))
     with pytest.raises(H.ExcInvalidArgument):

@@ -380,7 +380,8 @@ def test_graph_replay_matches_direct_launches(tmp_path):
 GUSAROV = [3.46470e-01, 3.46530e-01, 3.46591e-01, 3.46653e-01, 3.46715e-01]
 
 
-def test_melt_front_propagation_static_gusarov_on_gpu():
+@pytest.mark.parametrize("fused", [False, True])
+def test_melt_front_propagation_static_gusarov_on_gpu(fused):
     """The reference's Gusarov laser case (2D Q1 96 x 32 on [0, 6e-4] x [-2e-4, 0], liquid-solid
     steel, Dirichlet 1000 at x_max, dt 5e-6) through the GPU Newton path (GMRES, the heat
     default), the source computed on the device with the planar Gusarov profile."""
@@ -389,13 +390,16 @@ def test_melt_front_propagation_static_gusarov_on_gpu():
     op.set_material(H.material(law=L.LAW_LIQUID_SOLID, rho=7850.0, cp=460.0, k=55.563,
                                rho_s=7850.0, cp_s=700.0, k_s=17.0, T_solidus=1966.0,
                                T_liquidus=1974.0))
-    q = op.laser_source(op.new_vector(), L.LASER_GUSAROV, 5.0, (0.0, 0.5, 0.0), radius=6e-5,
-                        gusarov=(0.7, 6e4, 5e-5), planar=True)
+    laser = dict(radius=6e-5, gusarov=(0.7, 6e4, 5e-5), planar=True)
     lin = H.LinearSolverData(solver_type=L.SOLVER_GMRES, rel_tolerance=1e-12)
     opn = H.HeatDiffuseOperation(op, lin, H.NonlinearSolverData(residual_tolerance=1e-8))
     opn.set_initial_condition(torch.full((op.n_dofs,), 1000.0, dtype=torch.float64,
                                          device="cuda"))
-    opn.heat_source = q
+    if fused:  # the source evaluated inside the residual kernel
+        op.set_laser(L.LASER_GUSAROV, 5.0, (0.0, 0.5, 0.0), **laser)
+    else:      # the nodal source vector, as LaserHeatSourceVolumetric fills it
+        opn.heat_source = op.laser_source(op.new_vector(), L.LASER_GUSAROV, 5.0, (0.0, 0.5, 0.0),
+                                          **laser)
     for ref in GUSAROV:
         st = opn.solve(5e-6)
         assert st.converged == 1

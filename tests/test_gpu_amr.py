@@ -103,14 +103,14 @@ def test_diagonal_and_residual_with_hanging_nodes_match_oracle(p, law):
     assert _relmax(d, rref) <= 1e-12
 
 
-MULTI = np.zeros((4, 4, 4), dtype=np.uint8)
-MULTI[1:3, 1:3, 1:3] = 1
+MULTI = np.zeros((5, 5, 5), dtype=np.uint8)
+MULTI[1:4, 1:4, 1:4] = 1
 MULTI[2, 2, 2] = 2  # levels 0, 1 and 2 under the 2:1 balance
 
 
 @pytest.mark.parametrize("p", [2, 3])
 def test_multilevel_operator_matches_oracle(p):
-    cells = (4, 4, 4)
+    cells = (5, 5, 5)
     op = AmrHeatOperator(H.box_mesh(p, cells, **BOX), MULTI, device=0)
     o = A.MultiLevelBoxMesh(p, cells, MULTI, **BOX)
     assert op.n_dofs == o.n_dofs and o.hanging.any()
@@ -152,7 +152,7 @@ def test_implicit_steps_on_refined_mesh_match_oracle(mesh):
         cells, ref_arg = (4, 3, 3), REFINE
         o = A.TwoLevelBoxMesh(p, cells, refine=REFINE, **BOX)
     else:
-        cells, ref_arg = (4, 4, 4), MULTI
+        cells, ref_arg = (5, 5, 5), MULTI
         o = A.MultiLevelBoxMesh(p, cells, MULTI, **BOX)
     op = AmrHeatOperator(H.box_mesh(p, cells, **BOX), ref_arg, device=0)
     m, coef = _coef("linear_k")

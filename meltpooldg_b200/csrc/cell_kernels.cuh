@@ -62,6 +62,12 @@ template <typename T> __device__ __forceinline__ void atomic_add(T *p, T v) { at
 template <int LAW> __host__ __device__ constexpr bool law_tdep() { return LAW == 1 || LAW == 2 || LAW == 5; }
 // laws that may need T_old (d(rho_cp)/dT (T_lin - T_old) / dt in the tangent)
 template <int LAW> __host__ __device__ constexpr bool law_told() { return LAW == 2 || LAW == 5; }
+// shared arrays per cell of the line-per-thread operator: u and its gradients, a temporary (Tq
+// doubles as it with T_lin), T_lin's values and gradients, T_old's values
+template <int LAW> __host__ __device__ constexpr int vmult_arrays()
+{
+  return law_tdep<LAW>() ? (law_told<LAW>() ? 9 : 8) : 5;
+}
 
 // One 1D sweep of matrix `kind` along `dir` for line `line` (0 <= line < n^2).
 template <int n, int kind, int dir, bool add, typename T>
@@ -254,14 +260,16 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
   constexpr int n2 = n * n, n3 = n2 * n, CPB = cells_per_block(n);
   constexpr bool TDEP = law_tdep<LAW>();
   static_assert(!PRE || GEO == 1, "the geometry preload is for per-point geometry");
-  constexpr int NF = TDEP ? 11 : 6;
+  // shared arrays per cell: the sweeps' temporaries alias arrays that are free at that time
+  // (gx, gy while values are interpolated, the gathered T_lin in gz, Tq after the q-point loop)
+  constexpr int NF = vmult_arrays<LAW>();
   if (a.st && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   const int cl = threadIdx.x / n2, line = threadIdx.x % n2;
-  T *u = sm + cl * NF * n3, *t1 = u + n3, *t2 = u + 2 * n3, *gx = u + 3 * n3, *gy = u + 4 * n3,
-    *gz = u + 5 * n3;
-  T *Tq = u + 6 * n3, *Tx = u + 7 * n3, *Ty = u + 8 * n3, *Tz = u + 9 * n3, *Toq = u + 10 * n3;
+  T *u = sm + cl * NF * n3, *gx = u + n3, *gy = u + 2 * n3, *gz = u + 3 * n3;
+  T *t1 = u + 4 * n3;  // integration temporary without the T_lin arrays
+  T *Tq = u + 4 * n3, *Tx = u + 5 * n3, *Ty = u + 6 * n3, *Tz = u + 7 * n3, *Toq = u + 8 * n3;
   const MeshDims &d = a.d;
   double dot = 0.0;
   const int64_t n_batches = (a.n_cells + CPB - 1) / CPB;
@@ -303,18 +311,18 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
       }
       gather_xline<n>(d, row, I0, J, K, false, a.Tl, xt, active);
 #pragma unroll
-      for (int i = 0; i < n; ++i) t1[i + n * line] = xt[i];
+      for (int i = 0; i < n; ++i) gz[i + n * line] = xt[i];
     }
     __syncthreads();
     if (TDEP) {
-      // T_lin values + gradients: t1 -> (S) -> Tq; old values first if needed
+      // T_lin values + gradients: gz -> (S) -> Tq; old values first if needed
       if (law_told<LAW>() && a.m.need_told) {
         eval_values<n>(Tq, gx, gy, Toq, line);
       }
-      eval_values<n>(t1, gx, gy, Tq, line);
+      eval_values<n>(gz, gx, gy, Tq, line);
       eval_gradients<n>(Tq, Tx, Ty, Tz, line);
     }
-    eval_values<n>(u, t1, t2, u, line);  // values overwrite the gathered nodal values
+    eval_values<n>(u, gx, gy, u, line);  // values overwrite the gathered nodal values
     eval_gradients<n>(u, gx, gy, gz, line);
     // quadrature-point operation (tangent_local_cell_operation)
 #pragma unroll
@@ -863,9 +871,9 @@ __global__ void __launch_bounds__(block_threads(n)) k_norm(CellArgs<double> a)
 }
 
 // shared-memory bytes of each kernel
-template <int n, typename T> constexpr size_t smem_vmult(bool tdep)
+template <int n, typename T, int LAW> constexpr size_t smem_vmult()
 {
-  return sizeof(T) * cells_per_block(n) * (tdep ? 11 : 6) * n * n * n;
+  return sizeof(T) * cells_per_block(n) * vmult_arrays<LAW>() * n * n * n;
 }
 template <int n> constexpr size_t smem_rhs() { return sizeof(double) * cells_per_block(n) * 9 * n * n * n; }
 template <int n> constexpr size_t smem_diag() { return sizeof(double) * cells_per_block(n) * 16 * n * n * n; }

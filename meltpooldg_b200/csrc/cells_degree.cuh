@@ -108,7 +108,7 @@ struct DegreeOps {
       k2<<<g2, 32 * kV2Warps, smem2, s>>>(a);
       return cudaGetLastError();
     } else {
-      const size_t smem = smem_vmult<n, T>(law_tdep<LAW>());
+      const size_t smem = smem_vmult<n, T, LAW>();
       const int64_t nb = (a.n_cells + CPB - 1) / CPB;
       if constexpr (GEO == 1) {
         if (geo_preload()) {

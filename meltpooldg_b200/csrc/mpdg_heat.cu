@@ -3414,7 +3414,11 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
   memset(&s, 0, sizeof(s));
   int rc = MPDG_OK;
   do {
-    if (h->dt != dt || !prm->linear.cheb_eig_reuse) h->eig_valid = false;
+    // the Chebyshev / multigrid interval: kept across steps with cheb_eig_reuse until dt (or
+    // the material or the mesh) changes; a solve that does not use it leaves it alone
+    const bool uses_interval = prm->linear.preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 ||
+                               prm->linear.preconditioner == MPDG_PRECOND_MG_F32;
+    if (h->dt != dt || (uses_interval && !prm->linear.cheb_eig_reuse)) h->eig_valid = false;
     h->dt = dt;
     // init_time_advance: predictor into w1, commit history, constraints
     if (h->rotate) {

@@ -149,3 +149,28 @@ def test_benchmark_step_at_48cubed_matches_oracle(precond):
           f"rel L2 {e_l2:.2e}, rel max {e_max:.2e}")
     assert e_l2 <= TOL_STEP and e_max <= TOL_STEP
     assert 0 < st.linear_iterations < its_ref
+
+
+# the vmult sweep's small meshes (bench_vmult_sweep.py --size small, ~2 M DoFs each)
+SWEEP_SMALL = {1: 125, 2: 62, 3: 42, 4: 31, 5: 25, 6: 21}
+
+
+@pytest.mark.parametrize("degree", sorted(SWEEP_SMALL))
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+def test_vmult_sweep_meshes_match_oracle(degree, perturb):
+    """The operator of the cfg2 sweep (M/dt + K, rho cp = k = 1, dt = 1e-3, seeded U[-1, 1]
+    input) on its ~2 M-DoF meshes, where every CTA of the persistent grids loops: FP64 to 1e-12,
+    FP32 to 2e-5 (2e-4 for p >= 5, as the small-mesh tests)."""
+    m = SWEEP_SMALL[degree]
+    o = O.Oracle(degree, (m,) * 3, perturb=perturb, seed=1)
+    o.set_material(O.material(O.LAW_CONSTANT, k=1.0), 1e-3)
+    g = H.HeatDiffuseOperator(H.box_mesh(degree, (m,) * 3, perturb=perturb, seed=1))
+    g.set_material(H.material(law=L.LAW_CONSTANT, k=1.0))
+    g.reset_time_increment(1e-3)
+    z = g.new_vector()
+    g.set_linearization(z, z)
+    src = np.random.default_rng(degree).uniform(-1, 1, o.n_dofs)
+    ref = o.vmult(src)
+    assert rel(g.vmult(g.new_vector(), cuda(src)), ref) <= TOL64
+    tol32 = TOL32 * (10 if degree >= 5 else 1)
+    assert rel(g.vmult(g.new_vector(torch.float32), cuda(src, torch.float32)), ref) <= tol32

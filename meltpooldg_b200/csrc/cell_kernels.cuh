@@ -284,12 +284,20 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
     const int I0 = d.p * cx, J = d.p * cy + j, K = d.p * cz + k;
     const int64_t row = (int64_t)d.nd[0] * (J + (int64_t)d.nd[1] * K) + I0;
     T gpre[PRE ? n : 1][7];
+    T fpre[(PRE && LAW == 7) ? n : 1][4];
     if (PRE) {
       const T *gb = a.g.q + cc * 7 * n3 + line;
 #pragma unroll
       for (int r = 0; r < n; ++r)
 #pragma unroll
         for (int c = 0; c < 7; ++c) gpre[r][c] = __ldg(gb + c * n3 + n2 * r);
+      if (LAW == 7) {
+        const T *fb = a.cf + cc * 4 * n3 + line;
+#pragma unroll
+        for (int r = 0; r < n; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) fpre[r][c] = __ldg(fb + c * n3 + n2 * r);
+      }
     }
     // the geometry, or the coefficient fields of LAW 4/5, dominate a batch's q-point loads
     if (GEO == 1)
@@ -352,11 +360,35 @@ __global__ void __launch_bounds__(block_threads(n)) k_vmult(CellArgs<T> a)
         rhocp = drhocp = dk = T(0);
         val = a.m.idt * __ldg(cf) * uu + __ldg(cf + 2 * n3) * gx[q] + __ldg(cf + 3 * n3) * gy[q] +
               __ldg(cf + 4 * n3) * gz[q];
+      } else if (LAW == 7) {
+        // linear-k tangent from its fields: k(T_lin) and k1 dT_lin/dxi_d at the point
+        T fk, fd[3];
+        if (PRE) {
+          fk = fpre[r][0];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) fd[c] = fpre[r][1 + c];
+        } else {
+          const T *cf = a.cf + cc * 4 * n3 + q;
+          fk = __ldg(cf);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) fd[c] = __ldg(cf + (1 + c) * n3);
+        }
+        kk = fk;
+        rhocp = a.m.rho_l * a.m.cp_l;
+        drhocp = dk = T(0);
+        b0 = fd[0];
+        b1 = fd[1];
+        b2 = fd[2];
       } else {
         mat_eval<LAW>(a.m, TDEP ? Tq[q] : T(0), rhocp, kk, drhocp, dk);
       }
       T cval = a.m.idt * rhocp;
       T f0 = kk * gx[q], f1 = kk * gy[q], f2 = kk * gz[q];
+      if (LAW == 7) {
+        f0 += b0 * uu;
+        f1 += b1 * uu;
+        f2 += b2 * uu;
+      }
       if (TDEP) {
         if (law_told<LAW>() && a.m.need_told) cval += a.m.idt * drhocp * (Tq[q] - Toq[q]);
         f0 += dk * Tx[q] * uu;

@@ -138,9 +138,9 @@ struct DegreeOps {
     }
     if (law == 4) return geo == 0 ? vmult_t<T, 0, 4>(a, s, sm) : vmult_t<T, 1, 4>(a, s, sm);
     if (law == 5) return geo == 0 ? vmult_t<T, 0, 5>(a, s, sm) : vmult_t<T, 1, 5>(a, s, sm);
-    if (law == 6 || law == 7) {  // register-resident kernel only
+    if (law == 7) return geo == 0 ? vmult_t<T, 0, 7>(a, s, sm) : vmult_t<T, 1, 7>(a, s, sm);
+    if (law == 6) {  // register-resident kernel only
       if constexpr (use_v2<T>()) {
-        if (law == 7) return geo == 0 ? vmult_t<T, 0, 7>(a, s, sm) : vmult_t<T, 1, 7>(a, s, sm);
         return geo == 0 ? vmult_t<T, 0, 6>(a, s, sm) : vmult_t<T, 1, 6>(a, s, sm);
       } else {
         return cudaErrorNotSupported;

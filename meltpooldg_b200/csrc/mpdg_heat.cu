@@ -1276,6 +1276,17 @@ static bool tangent_fields_enabled()
   return on != 0;
 }
 
+// line-per-thread kernel (FP64, p >= 4) on deformed meshes: the linear-k tangent from the
+// fields (preloaded with the geometry) instead of evaluating T_lin
+static bool tangent_fields_lpt()
+{
+  static const int on = [] {
+    const char *e = getenv("MPDG_TANGENT_FIELDS_LPT");
+    return (e && e[0] == '1') ? 1 : 0;
+  }();
+  return on != 0;
+}
+
 static int ensure_lineark(mpdg_heat *h)
 {
   if (!h->tk_dirty) return MPDG_OK;
@@ -1390,10 +1401,10 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
     TRY(ensure_tangent(h));
     a.cf = h->tf;
     law = 6;
-  } else if (law == MPDG_LAW_LINEAR_K && h->tab.v2_d && h->tab.coef_lineark &&
-             tangent_fields_enabled()) {
-    // register-resident degrees only: on the line-per-thread kernel (p >= 4) 4 extra loads
-    // per point measured slower than the T_lin sweeps they replace
+  } else if (law == MPDG_LAW_LINEAR_K && h->tab.coef_lineark && tangent_fields_enabled() &&
+             (h->tab.v2_d || (h->geo == 1 && tangent_fields_lpt()))) {
+    // the line-per-thread kernel (p >= 4) takes them on deformed meshes only with
+    // MPDG_TANGENT_FIELDS_LPT=1: 4 more loads per point against the 6 T_lin sweeps
     TRY(ensure_lineark(h));
     a.cf = h->tk;
     law = 7;

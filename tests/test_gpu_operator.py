@@ -120,6 +120,22 @@ def test_fp32_packed_kernel_matches_oracle():
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
 
 
+def test_line_per_thread_tangent_fields_match_oracle():
+    """The line-per-thread FP64 k(T) tangent from the fields built once per linearisation
+    (MPDG_TANGENT_FIELDS_LPT=1, deformed meshes at p >= 4) on the same cases, in a child process
+    because the choice is read once per process."""
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ, MPDG_TANGENT_FIELDS_LPT="1")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p",
+                        "no:cacheprovider", __file__, "-k",
+                        "vmult_diag_rhs_match_oracle and linear_k and 0.2 and (4 or 5 or 6)"],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert " passed" in r.stdout
+
+
 def test_picard_operator_rejects_other_laws():
     _, g = pair(2, (2, 2, 2), 0.0, "constant")
     g.set_linearization(g.new_vector(), g.new_vector())

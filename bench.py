@@ -471,7 +471,8 @@ def run_mine(args):
     picard_dominant = cnt["vmult32_ms"] >= cnt["vmult64_ms"]
     if picard_dominant:
         # FP32 Picard operator of the preconditioner: src + dst + conductivity per q-point
-        kname = "k_vmult2<4,float,affine,conductivity_field>"
+        kname = ("k_vmult_picard_tc<4>" if op.picard_tensor_cores
+                 else "k_vmult2<4,float,affine,conductivity_field>")
         kms = cnt["vmult32_ms"]
         alg_bytes = 2 * 4 * N + 4 * nq
         xs = torch.rand(N, dtype=torch.float32, device=dev)
@@ -542,8 +543,10 @@ def run_mine(args):
             "learned+mixed": "the mixed solver started from the learned guess",
             "cheb": "FP64 flexible CG + FP32 Chebyshev(6)",
             "plain": "FP64 Jacobi-CG"}[best_name],
-        "dtype": "f64 (outer flexible CG, k(T) tangent, residual) + f32 (p-multigrid "
-                 "preconditioner)" if best_name != "plain" else "f64",
+        "dtype": ("f64 (outer flexible CG, k(T) tangent, residual) + f32 (p-multigrid "
+                  "preconditioner" + ("; fine-level operator TF32 on the tensor cores, FP32 "
+                                      "accumulation)" if op.picard_tensor_cores else ")"))
+                 if best_name != "plain" else "f64",
         "data": "synthetic",
         "config": workload_config(cells), "parallelism": f"replicas x{world}",
         "mixed_ms_per_step": ms_mixed / K,

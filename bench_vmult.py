@@ -5,6 +5,9 @@ prints one JSON line per precision with the CUDA-event time per application,
 DoFs/s and algorithmic GB/s (src + dst + linearisation point [+ per-q geometry]).
 With --solve it instead runs a few outer iterations of FP64 CG with the FP32
 Chebyshev preconditioner on the Picard operator, so that kernel can be captured.
+With --picard it times the FP32 Picard operator of the multigrid fine level (conductivity
+frozen at the quadrature points; src + dst + the conductivity per point in the traffic), on
+the tensor cores where that kernel exists and on the CUDA cores, one line each.
 With --transport the operator is the two-phase one (gas-liquid law on a heaviside
 field plus the convective term of a velocity field), whose per-point coefficients
 (5 per quadrature point) replace the linearisation point in the traffic;
@@ -35,6 +38,7 @@ def main():
     ap.add_argument("--dtype", default="both", choices=["f64", "f32", "both"])
     ap.add_argument("--solve", action="store_true")
     ap.add_argument("--transport", action="store_true")
+    ap.add_argument("--picard", action="store_true")
     a = ap.parse_args()
     op = H.HeatDiffuseOperator(H.box_mesh(a.degree, (a.cells,) * 3, perturb=a.perturb))
     if a.transport:
@@ -54,6 +58,31 @@ def main():
         hs = (0.5 + 0.5 * torch.tanh((x[:, 2] - 0.5) / 0.05)).contiguous()
         vel = torch.stack([torch.sin(3 * x[:, 1]), 0.5 + x[:, 2], -x[:, 0] * x[:, 1]]).contiguous()
         op.set_fields(hs, vel)
+    if a.picard:
+        x = torch.rand(N, dtype=torch.float32, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        op.set_picard_tensor_cores(True)  # opt-in; exists for uniform boxes at FE_Q(3)
+        for tc in ([True, False] if op.picard_tensor_cores else [False]):
+            op.set_picard_tensor_cores(tc)
+            for _ in range(3):
+                op.vmult_picard_f32(y, x)
+            torch.cuda.synchronize()
+            # the verb also rebuilds the conductivity field and zeroes dst: time the operator
+            # kernel alone with the library's own events around it
+            op.set_timing(True)
+            op.counters(reset=True)
+            for _ in range(a.reps):
+                op.vmult_picard_f32(y, x)
+            torch.cuda.synchronize()
+            c = op.counters(reset=True)
+            op.set_timing(False)
+            ms = c["vmult32_ms"] / max(c["vmult32_calls"], 1)
+            alg = 2 * 4 * N + 4 * nq
+            print(json.dumps({"degree": a.degree, "cells": a.cells, "operator": "picard_f32",
+                              "kernel": "tensor-core" if tc else "cuda-core", "n_dofs": N,
+                              "ms": ms, "gdofs": N / ms / 1e6, "alg_bytes": alg,
+                              "alg_gbs": alg / ms / 1e6}), flush=True)
+        return
     if a.solve:
         from meltpooldg_b200 import _lib as L
         op.distribute_constraints(T)

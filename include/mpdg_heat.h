@@ -227,6 +227,14 @@ int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src);
  * k(T_lin) frozen at the quadrature points. Boundary-face terms as in
  * mpdg_heat_vmult_f32. MPDG_ERR_INVALID_ARGUMENT for the other laws. */
 int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float *src);
+/* The FP32 Picard operator (mpdg_heat_vmult_f32_picard and the multigrid fine level) on the
+ * tensor cores: tcgen05 TF32 GEMMs over bricks of 128 cells, operands rounded to TF32
+ * (relative error ~5e-4 against the oracle), FP32 accumulation. Exists for uniform box meshes
+ * and FE_Q(3); on = 1 uses it where it exists, on = 0 keeps the CUDA-core kernel (the default
+ * unless the environment sets MPDG_PICARD_TC=1: the CUDA-core kernel measured faster). The
+ * second call returns 1 when the handle applies the operator on the tensor cores. */
+int mpdg_heat_set_picard_tensor_cores(mpdg_heat *h, int on);
+int mpdg_heat_picard_tensor_cores(const mpdg_heat *h);
 /* Inverse diagonal of that FP32 Picard operator (|d| > 1e-10 ? 1/d : 1), the Jacobi
  * scaling of the multigrid smoothers. Same restrictions. */
 int mpdg_heat_inverse_diagonal_f32_picard(mpdg_heat *h, float *inv_diag);

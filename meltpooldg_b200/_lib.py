@@ -118,6 +118,8 @@ _SIGS = {
     "mpdg_heat_vmult_f32": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult_f32_picard": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_inverse_diagonal_f32_picard": (C.c_int, [_H, _D]),
+    "mpdg_heat_set_picard_tensor_cores": (C.c_int, [_H, C.c_int]),
+    "mpdg_heat_picard_tensor_cores": (C.c_int, [_H]),
     "mpdg_heat_compute_inverse_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_compute_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),

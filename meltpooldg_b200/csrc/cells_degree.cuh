@@ -7,9 +7,11 @@
 #include "cell_kernels.cuh"
 #include "cell_kernels_v2.cuh"
 #include "cell_kernels_f2.cuh"
+#include "cell_kernels_tc.cuh"
 #include "degree_table.hpp"
 
 #include <stdlib.h>
+#include <algorithm>
 #include <type_traits>
 
 namespace mpdg {
@@ -264,6 +266,31 @@ struct DegreeOps {
   {
     return geo == 0 ? diag_picard_t<0>(a, s, sm) : diag_picard_t<1>(a, s, sm);
   }
+  static cudaError_t vmult_picard_tc(const CellArgs<float> &a, const float *gmat, int *err,
+                                     cudaStream_t s, int sm)
+  {
+    if constexpr (n == 4) {
+      static bool attr = false;
+      auto k = k_vmult_picard_tc<n>;
+      if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)optc::kSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+      }
+      const int64_t nb = (int64_t)((a.d.m[0] + optc::kBX - 1) / optc::kBX) *
+                         ((a.d.m[1] + optc::kBY - 1) / optc::kBY) *
+                         ((a.d.m[2] + optc::kBZ - 1) / optc::kBZ);
+      // one CTA per SM (two brick pipelines, 512 tensor-memory columns, ~161 KB shared)
+      const int64_t nc = (nb + optc::kGroups - 1) / optc::kGroups;
+      const int g = (int)std::min<int64_t>(nc, (int64_t)sm);
+      k<<<g, optc::kThreads, optc::kSmem, s>>>(a, reinterpret_cast<const float4 *>(gmat), err);
+      return cudaGetLastError();
+    } else {
+      (void)a, (void)gmat, (void)err, (void)s, (void)sm;
+      return cudaErrorNotSupported;
+    }
+  }
   template <int GEO>
   static cudaError_t coef_tangent_t(const CellArgs<double> &a, double *out, cudaStream_t s, int sm)
   {
@@ -331,6 +358,7 @@ struct DegreeOps {
       t.conductivity_q = &conductivity_q;
       t.diag_picard = &diag_picard;
     }
+    if constexpr (n == 4) t.vmult_picard_tc = &vmult_picard_tc;
     return t;
   }
 };

@@ -32,6 +32,10 @@ struct DegreeTable {
   bool v2_d = false, v2_f = false;
   // a.dst += diagonal of the FP32 Picard operator (conductivity field a.kq); same degrees
   cudaError_t (*diag_picard)(const CellArgs<float> &, int geo, cudaStream_t, int sm) = nullptr;
+  // a.dst += the FP32 Picard operator on the tensor cores (uniform box, FE_Q(3) only; gmat:
+  // the 128 KB of optc::build_gmat in device memory, err: raised on a timed-out wait)
+  cudaError_t (*vmult_picard_tc)(const CellArgs<float> &, const float *gmat, int *err,
+                                 cudaStream_t, int sm) = nullptr;
 };
 
 DegreeTable degree_table_2();

@@ -24,6 +24,7 @@
 #include "degree_table.hpp"
 #include "fe_tables.hpp"
 #include "material_law.cuh"
+#include "picard_tc_layout.hpp"
 #include "reduce.cuh"
 #include "source_eval.cuh"
 
@@ -201,6 +202,12 @@ struct mpdg_heat {
   // iterations of the last mixed-precision solve per preconditioner (0 multigrid, 1 Chebyshev):
   // the next solve issues that many before its first convergence poll
   int its_hint[2] = {0, 0};
+  // FP32 Picard operator on the tensor cores (uniform box, FE_Q(3)): on/off (-1: the
+  // MPDG_PICARD_TC setting, off unless it is 1), its G matrices (device, 2 x 64 KB), and a page-locked mapped flag the
+  // kernel raises when a wait times out (tc_err_map: its device address)
+  int picard_tc = -1;
+  float *gmat_tc = nullptr;
+  int *tc_err_host = nullptr, *tc_err_map = nullptr;
 };
 
 static cudaEvent_t take_event(mpdg_heat *h)
@@ -1472,6 +1479,39 @@ static int refresh_f32(mpdg_heat *h)
   return MPDG_OK;
 }
 
+// The FP32 Picard operator on the tensor cores (TF32 operands, FP32 accumulation) where the
+// kernel exists (uniform box, FE_Q(3)), when MPDG_PICARD_TC=1 or mpdg_heat_set_picard_tensor_cores
+// asks for it; the default is the CUDA-core kernel, which measured faster (the operator is bound
+// by its gather/scatter path, not by the contractions the tensor cores take over)
+static bool picard_tc_on(const mpdg_heat *h)
+{
+  static const int env_on = [] {
+    const char *e = getenv("MPDG_PICARD_TC");
+    return (e && e[0] == '1') ? 1 : 0;
+  }();
+  const int on = h->picard_tc >= 0 ? h->picard_tc : env_on;
+  return on && h->geo == 0 && h->p == 3 && h->tab.vmult_picard_tc != nullptr;
+}
+
+static int ensure_picard_tc(mpdg_heat *h)
+{
+  if (!h->gmat_tc) {
+    std::vector<float> g(2 * optc::kGFloats);
+    optc::build_gmat(g.data());
+    TRY(dalloc(h, (void **)&h->gmat_tc, 2 * optc::kGBytes));
+    CU(cudaMemcpy(h->gmat_tc, g.data(), 2 * optc::kGBytes, cudaMemcpyHostToDevice));
+  }
+  if (!h->tc_err_host) {
+    if (cudaHostAlloc((void **)&h->tc_err_host, sizeof(int), cudaHostAllocMapped) != cudaSuccess)
+      return fail(MPDG_ERR_OUT_OF_MEMORY, "cudaHostAlloc");
+    *h->tc_err_host = 0;
+    CU(cudaHostGetDevicePointer((void **)&h->tc_err_map, h->tc_err_host, 0));
+  }
+  if (*(volatile int *)h->tc_err_host)
+    return fail(MPDG_ERR_CUDA, "tensor-core Picard operator: an MMA wait timed out");
+  return MPDG_OK;
+}
+
 static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *st,
                       bool picard = false)
 {
@@ -1507,8 +1547,13 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
     e1 = take_event(h);
     cudaEventRecord(e0, h->stream);
   }
+  const bool tc = law == 3 && picard_tc_on(h);
+  if (tc) TRY(ensure_picard_tc(h));
   if (any_faces(h)) TRY(launch_faces<float>(h, 0, dst, src, h->T_lin_f, nullptr, st));
-  CU(h->tab.vmult_f(a, h->geo, law, h->stream, h->sm_count));
+  if (tc)
+    CU(h->tab.vmult_picard_tc(a, h->gmat_tc, h->tc_err_map, h->stream, h->sm_count));
+  else
+    CU(h->tab.vmult_f(a, h->geo, law, h->stream, h->sm_count));
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
     h->ev32.push_back({e0, e1});
@@ -2546,6 +2591,8 @@ static void release(mpdg_heat *h)
   if (h->st_host) cudaFreeHost(h->st_host);
   if (h->scal_host) cudaFreeHost(h->scal_host);
   if (h->rd_host) cudaFreeHost(h->rd_host);
+  if (h->tc_err_host) cudaFreeHost(h->tc_err_host);
+  h->tc_err_host = nullptr;
   h->st_host = nullptr;
   h->scal_host = nullptr;
   h->rd_host = nullptr;
@@ -2954,6 +3001,19 @@ extern "C" int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float 
   ++h->launches;
   CU(zero_async(h, dst, sizeof(float) * h->n_dofs, h->stream));
   return op_apply_f(h, dst, src, nullptr, true);
+}
+
+extern "C" int mpdg_heat_set_picard_tensor_cores(mpdg_heat *h, int on)
+{
+  if (!h) return fail(MPDG_ERR_INVALID_ARGUMENT, "null handle");
+  h->picard_tc = on ? 1 : 0;
+  h->eig_valid = false;
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_picard_tensor_cores(const mpdg_heat *h)
+{
+  return h && picard_tc_on(h) ? 1 : 0;
 }
 
 extern "C" int mpdg_heat_inverse_diagonal_f32_picard(mpdg_heat *h, float *inv_diag)

@@ -328,6 +328,15 @@ class HeatDiffuseOperator:
                                                   _ptr(src, torch.float32)))
         return dst
 
+    def set_picard_tensor_cores(self, on: bool):
+        """Apply the FP32 Picard operator on the tensor cores (TF32 operands) where the kernel
+        exists (uniform box, FE_Q(3)); off (the default) keeps the CUDA-core kernel."""
+        check(self._L.mpdg_heat_set_picard_tensor_cores(self.h, int(bool(on))))
+
+    @property
+    def picard_tensor_cores(self) -> bool:
+        return bool(self._L.mpdg_heat_picard_tensor_cores(self.h))
+
     def inverse_diagonal_picard_f32(self, inv_diag):
         """Inverse diagonal of the FP32 Picard operator (the multigrid smoothers' scaling)."""
         check(self._L.mpdg_heat_inverse_diagonal_f32_picard(self.h, _ptr(inv_diag, torch.float32)))

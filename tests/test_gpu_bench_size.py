@@ -6,11 +6,13 @@ each CTA handles at most one batch. Here every CTA loops: 48^3 cells (110,592 ce
 ten batches per CTA at p = 3), 40^3 cells on a deformed mesh, and the benchmark mesh itself,
 FE_Q(3) on 128^3 cells (57,066,625 DoFs). The kernels checked are the ones the benchmark step
 launches: the FP64 k(T) tangent from its per-point fields (k_vmult2 LAW 7), the FP32 Picard
-operator of the multigrid smoothers (k_vmult2 LAW 3) and its diagonal (k_diag_picard), the
+operator of the multigrid smoothers (k_vmult_picard_tc on the tensor cores, and the CUDA-core
+k_vmult2 LAW 3) and its diagonal (k_diag_picard), the
 FP64 inverse diagonal (k_diag) and the residual (k_rhs2) with the Gaussian source of the
 benchmark, and the FE L2 norm (its multi-batch reduction).
 
-Tolerances: FP64 1e-12 relative (max norm against max |oracle|), FP32 2e-5 relative; the
+Tolerances: FP64 1e-12 relative (max norm against max |oracle|), FP32 2e-5 relative, the
+TF32 tensor-core operator 5e-3; the
 implicit step 1e-6 relative (L2 and max) against the oracle's FP64 Jacobi-CG solution, the
 accuracy the mixed-precision solver is specified to.
 """
@@ -25,6 +27,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 TOL64, TOL32, TOL_STEP = 1e-12, 2e-5, 1e-6
+TOL_TF32 = 5e-3  # the tensor-core Picard operator: TF32 operands
 DT = 5e-4
 LAW = dict(law=L.LAW_LINEAR_K, rho=1.0, cp=1.0, k=1.0, k1=0.5)  # k(T) = 1 + 0.5 T
 
@@ -87,7 +90,13 @@ def check_bench_kernels(o, g, tol64=TOL64):
     # FP32 Picard operator and its inverse diagonal (the multigrid fine level)
     s32 = cuda(src, torch.float32)
     pref = o.vmult(src, Tl, To, form=2)
+    g.set_picard_tensor_cores(True)  # the opt-in tensor-core kernel, where it exists
+    tc = g.picard_tensor_cores
+    g.set_picard_tensor_cores(False)
     assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), pref) <= TOL32
+    if tc:  # the tensor-core kernel (opt-in) on the benchmark's mesh
+        g.set_picard_tensor_cores(True)
+        assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), pref) <= TOL_TF32
     del pref
     dpref = o.inverse_diagonal(Tl, To, form=2)
     dp = g.inverse_diagonal_picard_f32(g.new_vector(torch.float32))

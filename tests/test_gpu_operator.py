@@ -21,6 +21,7 @@ LAWS = {
 }
 TOL64 = 1e-12
 TOL32 = 2e-5
+TOL_TF32 = 5e-3  # the tensor-core Picard operator: TF32 operands (10-bit mantissa)
 
 
 def pair(degree, cells, perturb=0.0, law="constant", dt=1e-3, dirichlet=0x3F, lo=(0, 0, 0),
@@ -101,7 +102,13 @@ def test_fp32_operator_cell_pairs(degree, cells, perturb):
     s32 = cuda(src, torch.float32)
     assert rel(g.vmult(g.new_vector(torch.float32), s32), o.vmult(src, Tl, To)) <= TOL32
     ref = o.vmult(src, Tl, To, form=2)
+    g.set_picard_tensor_cores(True)  # uniform box, FE_Q(3): the opt-in tensor-core kernel
+    tc = g.picard_tensor_cores
+    g.set_picard_tensor_cores(False)
     assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), ref) <= TOL32
+    if tc:
+        g.set_picard_tensor_cores(True)
+        assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), ref) <= TOL_TF32
     dref = o.inverse_diagonal(Tl, To, form=2)
     dg = g.inverse_diagonal_picard_f32(g.new_vector(torch.float32))
     assert rel(1.0 / dg.cpu().double().numpy(), 1.0 / dref) <= TOL32

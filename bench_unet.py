@@ -1,10 +1,12 @@
-"""Forward time of the learned-guess network on an (nx, ny, nz) grid.
+"""Forward, backward and training-step times of the learned-guess network on an (nx, ny, nz)
+grid.
 
     python bench_unet.py --dims 97 97 97 [--reps 10]
 
-prints one JSON line with the CUDA-event time per forward (tensor-core
-convolutions, or the CUDA-core ones with MPDG_UNET_TC=0) and the nominal FLOPs
-of the convolutions."""
+prints one JSON line with the CUDA-event time per forward (tensor-core convolutions, or the
+CUDA-core ones with MPDG_UNET_TC=0), per backward (data gradients on the tensor cores, or on
+the CUDA cores with MPDG_UNET_TC_BWD=0; weight gradients on the CUDA cores), per training step
+(forward + backward + Adam) and the nominal FLOPs of the convolutions."""
 import argparse
 import json
 import os
@@ -43,10 +45,34 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
+    gy = torch.randn(n, device="cuda", generator=g)
+    for _ in range(2):
+        net.backward(gy)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(a.reps):
+        gp = net.backward(gy)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_bwd = e0.elapsed_time(e1) / a.reps
+    t = torch.randn(n, device="cuda", generator=g)
+    for _ in range(2):
+        net.train_step(x, t, 1e-4)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(a.reps):
+        net.train_step(x, t, 1e-4)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_train = e0.elapsed_time(e1) / a.reps
     fl = conv_flops(a.dims)
+    tc_bwd = os.environ.get("MPDG_UNET_TC") != "0" and os.environ.get("MPDG_UNET_TC_BWD") != "0"
     print(json.dumps({"dims": a.dims, "path": "cuda-core" if os.environ.get("MPDG_UNET_TC") == "0"
-                      else "tensor-core", "forward_ms": ms, "conv_gflop": fl / 1e9,
-                      "conv_tflops": fl / ms / 1e9, "out_norm": float(y.norm())}), flush=True)
+                      else "tensor-core",
+                      "data_gradient": "tensor-core" if tc_bwd else "cuda-core",
+                      "forward_ms": ms, "backward_ms": ms_bwd, "train_step_ms": ms_train,
+                      "conv_gflop": fl / 1e9, "conv_tflops": fl / ms / 1e9,
+                      "out_norm": float(y.norm()), "grad_norm": float(gp.norm())}), flush=True)
 
 
 if __name__ == "__main__":

@@ -271,4 +271,31 @@ __global__ void k_pack_weights(int ci, int co, int cg, int npad, const __nv_bflo
   }
 }
 
+// The data gradient of a convolution is the convolution of the output gradient with the
+// flipped, channel-transposed weights: gin[c] = sum_o sum_tap w[o][c][tap] gout[o](x - shift(tap))
+// = conv(gout, w')[c] with w'[c][o][26 - tap] = w[o][c][tap]. Packs w' (ci' = co, co' = ci) in the
+// layout of k_pack_weights.
+__global__ void k_pack_weights_t(int ci, int co, int cg, int npad, const __nv_bfloat16 *__restrict__ w,
+                                 uint4 *wp)
+{
+  // cg = 16-channel groups of co (the transposed input), npad = ci padded (its output)
+  const int64_t n = (int64_t)27 * cg * 2 * npad;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % npad);  // output channel of the transposed convolution
+    const int half = (int)((i / npad) % 2);
+    const int g = (int)((i / (2 * npad)) % cg);
+    const int tap = (int)(i / ((int64_t)2 * npad * cg));
+    const unsigned short *ws = reinterpret_cast<const unsigned short *>(w);
+    uint32_t v4[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int o = 16 * g + 8 * half + e;  // input channel of the transposed convolution
+      const uint32_t v = (c < ci && o < co) ? (uint32_t)ws[((int64_t)o * ci + c) * 27 + (26 - tap)] : 0u;
+      v4[e >> 1] |= v << (16 * (e & 1));
+    }
+    wp[i] = make_uint4(v4[0], v4[1], v4[2], v4[3]);
+  }
+}
+
 }  // namespace nn_tc

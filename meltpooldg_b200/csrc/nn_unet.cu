@@ -16,11 +16,14 @@
 // Tensors are planar [C][z][y][x]; activations BF16, activation gradients FP32,
 // weights [Cout][Cin][27] as FP32 masters plus a BF16 copy used by the kernels.
 // The forward convolutions run on the tensor cores (tcgen05 implicit GEMM,
-// nn_conv_tc.cuh). The backward convolutions (FP32 gradients) and the
-// CUDA-core forward (MPDG_UNET_TC=0) use k_conv3d: a CTA holds an 8x8x4 output
-// tile and 16 output channels, stages one input channel's tile plus halo and
-// its 16 x 27 weights in shared memory at a time and accumulates in FP32
-// registers.
+// nn_conv_tc.cuh), and so do the data gradients of the backward pass: the
+// output gradient, rounded to BF16, convolved with the flipped, channel-
+// transposed weights (packed beside the forward ones), FP32 out
+// (MPDG_UNET_TC_BWD=0 keeps them on the CUDA cores in FP32). The weight
+// gradients and the CUDA-core forward (MPDG_UNET_TC=0) use k_conv3d: a CTA
+// holds an 8x8x4 output tile and 16 output channels, stages one input
+// channel's tile plus halo and its 16 x 27 weights in shared memory at a time
+// and accumulates in FP32 registers.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -355,6 +358,11 @@ struct mpdg_unet {
   __nv_bfloat16 *pb = nullptr;
   uint4 *wpk = nullptr;       // weights packed for the tensor-core convolution
   int64_t wpk_off[15] = {};   // per layer, in uint4
+  uint4 *wpkt = nullptr;      // flipped, channel-transposed packs (the data gradient)
+  int64_t wpkt_off[15] = {};
+  bool use_tc_bwd = true;     // data gradients on the tensor cores
+  __nv_bfloat16 *gbf = nullptr;  // an output gradient in BF16 (the tensor cores' input)
+  float *zero_bias = nullptr;    // 64 zeros
   bool wpk_dirty = true;      // pb changed since the last packing
   bool use_tc = true;         // forward convolutions on the tensor cores
   bool training = false;      // forward keeps what the backward pass reads
@@ -377,6 +385,7 @@ namespace {
 enum { E0A, E0B, E1A, E1B, E2A, E2B, E3A, E3B, D2A, D2B, D1A, D1B, D0A, D0B, OUT };
 const int kCi[15] = {3, 16, 16, 32, 32, 48, 48, 64, 64, 48, 48, 32, 32, 16, 16};
 const int kCo[15] = {16, 16, 32, 32, 48, 48, 64, 64, 48, 48, 32, 32, 16, 16, 1};
+const int kLevel[15] = {0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0, 0};  // the grid of each layer
 
 uint64_t mix(uint64_t x)
 {
@@ -421,6 +430,9 @@ int pack_weights(mpdg_unet *u)
     const int ci = u->L[l].ci, co = u->L[l].co;
     nn_tc::k_pack_weights<<<64, 256, 0, u->stream>>>(ci, co, cg_of(ci), npad_of(co), W(u, l),
                                                      u->wpk + u->wpk_off[l]);
+    if (u->wpkt)
+      nn_tc::k_pack_weights_t<<<64, 256, 0, u->stream>>>(ci, co, cg_of(co), npad_of(ci), W(u, l),
+                                                         u->wpkt + u->wpkt_off[l]);
   }
   NNCU(cudaGetLastError());
   u->wpk_dirty = false;
@@ -428,8 +440,8 @@ int pack_weights(mpdg_unet *u)
 }
 
 template <int NPAD, bool RELU, bool ADD, typename TO>
-int conv_tc_t(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_bfloat16 *add,
-              TO *out, const Grid3 *up_from)
+int tc_launch(mpdg_unet *u, Grid3 g, int ci, int co, const uint4 *wp, const float *bias,
+              const __nv_bfloat16 *in, const __nv_bfloat16 *add, TO *out, const Grid3 *up_from)
 {
   auto k = nn_tc::k_conv3d_tc<NPAD, RELU, ADD, TO>;
   static size_t attr_smem = 0;  // the attribute is kept at the request of the launch, so
@@ -438,8 +450,8 @@ int conv_tc_t(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_
   a.nx = g.nx;
   a.ny = g.ny;
   a.nz = g.nz;
-  a.ci = u->L[l].ci;
-  a.co = u->L[l].co;
+  a.ci = ci;
+  a.co = co;
   a.cg = cg_of(a.ci);
   a.taps_per_stage = nn_tc::smem_bytes(a.cg, NPAD, 27) <= 200 * 1024 ? 27 : 9;
   a.up = up_from != nullptr;
@@ -447,8 +459,8 @@ int conv_tc_t(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_
   a.sy = up_from ? up_from->ny : g.ny;
   a.sz = up_from ? up_from->nz : g.nz;
   a.in = in;
-  a.wp = u->wpk + u->wpk_off[l];
-  a.bias = B(u, l);
+  a.wp = wp;
+  a.bias = bias;
   a.add = add;
   a.out = out;
   a.err = u->tc_err;
@@ -480,6 +492,14 @@ int conv_tc_t(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_
   return MPDG_OK;
 }
 
+template <int NPAD, bool RELU, bool ADD, typename TO>
+int conv_tc_t(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_bfloat16 *add,
+              TO *out, const Grid3 *up_from)
+{
+  return tc_launch<NPAD, RELU, ADD, TO>(u, g, u->L[l].ci, u->L[l].co, u->wpk + u->wpk_off[l],
+                                        B(u, l), in, add, out, up_from);
+}
+
 template <bool RELU, bool ADD, typename TO>
 int conv_tc(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, const __nv_bfloat16 *add,
             TO *out, const Grid3 *up_from = nullptr)
@@ -506,9 +526,37 @@ int conv_relu(mpdg_unet *u, int l, Grid3 g, const __nv_bfloat16 *in, __nv_bfloat
   return conv<__nv_bfloat16, __nv_bfloat16, true, false, false, false>(u, g, u->L[l].ci, u->L[l].co, in, W(u, l), B(u, l), nullptr, nullptr, out);
 }
 
+// gin = (W^T * gout) [* (mask > 0)] on the tensor cores: gout rounded to BF16, convolved with
+// the flipped, channel-transposed weights (FP32 accumulation and output), then masked
+int dgrad_tc(mpdg_unet *u, int l, Grid3 g, const float *gout, float *gin,
+             const __nv_bfloat16 *mask)
+{
+  if (u->wpk_dirty) NNTRY(pack_weights(u));
+  const int ci = u->L[l].ci, co = u->L[l].co;
+  const int64_t n = g.n();
+  k_f32_to_bf16<<<grid1d((int64_t)co * n), 256, 0, u->stream>>>((int64_t)co * n, gout, u->gbf);
+  NNCU(cudaGetLastError());
+  const uint4 *wp = u->wpkt + u->wpkt_off[l];
+  int rc;
+  switch (npad_of(ci)) {
+  case 16: rc = tc_launch<16, false, false, float>(u, g, co, ci, wp, u->zero_bias, u->gbf, nullptr, gin, nullptr); break;
+  case 32: rc = tc_launch<32, false, false, float>(u, g, co, ci, wp, u->zero_bias, u->gbf, nullptr, gin, nullptr); break;
+  case 48: rc = tc_launch<48, false, false, float>(u, g, co, ci, wp, u->zero_bias, u->gbf, nullptr, gin, nullptr); break;
+  case 64: rc = tc_launch<64, false, false, float>(u, g, co, ci, wp, u->zero_bias, u->gbf, nullptr, gin, nullptr); break;
+  default: return nn_fail(MPDG_ERR_INVALID_ARGUMENT, "tensor-core data gradient: Cin > 64");
+  }
+  NNTRY(rc);
+  if (mask) {
+    k_relu_mask<<<grid1d((int64_t)ci * n), 256, 0, u->stream>>>((int64_t)ci * n, mask, gin);
+    NNCU(cudaGetLastError());
+  }
+  return MPDG_OK;
+}
+
 // gin = (W^T * gout) [* (mask > 0)]
 int dgrad(mpdg_unet *u, int l, Grid3 g, const float *gout, float *gin, const __nv_bfloat16 *mask)
 {
+  if (u->use_tc && u->use_tc_bwd) return dgrad_tc(u, l, g, gout, gin, mask);
   if (mask)
     return conv<float, float, false, false, true, true>(u, g, u->L[l].co, u->L[l].ci, gout, W(u, l), nullptr, nullptr, mask, gin);
   return conv<float, float, false, false, false, true>(u, g, u->L[l].co, u->L[l].ci, gout, W(u, l), nullptr, nullptr, nullptr, gin);
@@ -714,10 +762,23 @@ extern "C" int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet
     wtot += (int64_t)27 * cg_of(kCi[l]) * 2 * npad_of(kCo[l]);
   }
   if ((rc = ualloc(u, (void **)&u->wpk, sizeof(uint4) * wtot)) != MPDG_OK) return fail_free(rc);
+  int64_t wtot_t = 0, gbf_n = 0;
+  for (int l = 0; l < 15; ++l) {
+    u->wpkt_off[l] = wtot_t;
+    wtot_t += (int64_t)27 * cg_of(kCo[l]) * 2 * npad_of(kCi[l]);
+    gbf_n = std::max(gbf_n, (int64_t)kCo[l] * u->g[kLevel[l]].n());  // an output gradient
+  }
+  if ((rc = ualloc(u, (void **)&u->wpkt, sizeof(uint4) * wtot_t)) != MPDG_OK ||
+      (rc = ualloc(u, (void **)&u->gbf, sizeof(__nv_bfloat16) * gbf_n)) != MPDG_OK ||
+      (rc = ualloc(u, (void **)&u->zero_bias, sizeof(float) * 64)) != MPDG_OK)
+    return fail_free(rc);
+  cudaMemset(u->zero_bias, 0, sizeof(float) * 64);
   cudaMemset(u->tc_err, 0, sizeof(int));
   {
     const char *e = getenv("MPDG_UNET_TC");
     u->use_tc = !(e && e[0] == '0');
+    const char *eb = getenv("MPDG_UNET_TC_BWD");
+    u->use_tc_bwd = !(eb && eb[0] == '0');
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&u->sm_count, cudaDevAttrMultiProcessorCount, dev);

@@ -28,13 +28,33 @@ def up(t, shape):
     return t
 
 
-def reference(params, x, dims):
+class ConvBF16Backward(torch.autograd.Function):
+    """conv3d whose input gradient is formed from the output gradient rounded to BF16 (as the
+    tensor-core data gradient does) and whose weight and bias gradients from the FP32 one."""
+
+    @staticmethod
+    def forward(ctx, t, w, b):
+        ctx.save_for_backward(t, w)
+        return F.conv3d(t, w, b, padding=1)
+
+    @staticmethod
+    def backward(ctx, g):
+        t, w = ctx.saved_tensors
+        gi = torch.nn.grad.conv3d_input(t.shape, w, g.to(torch.bfloat16).float(), padding=1)
+        gw = torch.nn.grad.conv3d_weight(t, w.shape, g, padding=1)
+        return gi, gw, g.sum(dim=(0, 2, 3, 4))
+
+
+def reference(params, x, dims, bf16_dgrad=True):
     nx, ny, nz = dims
     layers = LG.unpack(params)
 
     def conv(t, l, relu=True, add=None):
         w, b = layers[l]
-        r = F.conv3d(t, bf(w), b, padding=1)
+        if bf16_dgrad:
+            r = ConvBF16Backward.apply(t, bf(w), b)
+        else:
+            r = F.conv3d(t, bf(w), b, padding=1)
         if add is not None:
             r = r + add
         return bf(torch.relu(r)) if relu else r
@@ -50,7 +70,12 @@ def reference(params, x, dims):
     return conv(d0, 14, relu=False).reshape(-1)
 
 
-def test_forward_and_parameter_gradients_match_torch_reference():
+@pytest.mark.parametrize("tc_bwd", [True, False])
+def test_forward_and_parameter_gradients_match_torch_reference(tc_bwd, monkeypatch):
+    """Default: the data gradients on the tensor cores (the output gradient rounded to BF16
+    before each one, as the reference here does too); MPDG_UNET_TC_BWD=0: on the CUDA cores in
+    FP32."""
+    monkeypatch.setenv("MPDG_UNET_TC_BWD", "1" if tc_bwd else "0")
     dims = (19, 14, 11)  # odd/even mixes: 19->10->5->3, 14->7->4->2, 11->6->3->2
     net = LG.UNet(dims, seed=3)
     g = torch.Generator().manual_seed(0)
@@ -58,7 +83,7 @@ def test_forward_and_parameter_gradients_match_torch_reference():
     x = torch.randn(3 * n, generator=g)
     y = net.forward(x.cuda()).cpu()
     p = net.get_params().cpu().requires_grad_(True)
-    y_ref = reference(p, x, dims)
+    y_ref = reference(p, x, dims, bf16_dgrad=tc_bwd)
     err = (y - y_ref.detach()).norm() / y_ref.detach().norm()
     assert err < 2e-2, err
     gy = torch.randn(n, generator=g)
@@ -107,3 +132,23 @@ def test_tensor_core_forward_matches_cuda_core_forward(monkeypatch):
         p.add_(0.01 * torch.randn(p.numel(), generator=g).cuda())
         net_tc.set_params(p)
         net_cc.set_params(p)
+
+
+def test_tensor_core_backward_matches_cuda_core_backward(monkeypatch):
+    """Parameter gradients with the data gradients on the tensor cores against the FP32
+    CUDA-core ones, same forward, on a grid with partial tiles at every level."""
+    dims = (40, 33, 9)
+    n = dims[0] * dims[1] * dims[2]
+    monkeypatch.setenv("MPDG_UNET_TC_BWD", "1")
+    net_tc = LG.UNet(dims, seed=11)
+    monkeypatch.setenv("MPDG_UNET_TC_BWD", "0")
+    net_cc = LG.UNet(dims, seed=11)
+    g = torch.Generator().manual_seed(4)
+    x = torch.randn(3 * n, generator=g).cuda()
+    gy = torch.randn(n, generator=g).cuda()
+    net_tc.forward(x)
+    net_cc.forward(x)
+    a, b = net_tc.backward(gy), net_cc.backward(gy)
+    cos = torch.dot(a, b) / (a.norm() * b.norm())
+    assert cos > 0.9999, cos
+    assert (a - b).norm() / b.norm() < 2e-2

@@ -235,6 +235,13 @@ int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float *src);
  * second call returns 1 when the handle applies the operator on the tensor cores. */
 int mpdg_heat_set_picard_tensor_cores(mpdg_heat *h, int on);
 int mpdg_heat_picard_tensor_cores(const mpdg_heat *h);
+/* The two 256 x 64 matrices that kernel keeps in shared memory (2 x 16384 floats, host memory,
+ * no device needed): G^T then G, rows j = c * 64 + q (c = 0..2 the reference-gradient
+ * components, 3 the values, q = qx + 4 (qy + 4 qz) the Gauss point), columns i = ix + 4 (iy +
+ * 4 iz) the cell's DoF, entries rounded to TF32, in the no-swizzle K-major UMMA layout:
+ * G^T (j, i) at (j / 8) * 512 + (i / 4) * 32 + (j % 8) * 4 + i % 4, G (i, j) at 16384 +
+ * (i / 8) * 2048 + (j / 4) * 32 + (i % 8) * 4 + j % 4. */
+int mpdg_picard_tc_matrices(float *out);
 /* Inverse diagonal of that FP32 Picard operator (|d| > 1e-10 ? 1/d : 1), the Jacobi
  * scaling of the multigrid smoothers. Same restrictions. */
 int mpdg_heat_inverse_diagonal_f32_picard(mpdg_heat *h, float *inv_diag);

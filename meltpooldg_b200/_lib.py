@@ -120,6 +120,7 @@ _SIGS = {
     "mpdg_heat_inverse_diagonal_f32_picard": (C.c_int, [_H, _D]),
     "mpdg_heat_set_picard_tensor_cores": (C.c_int, [_H, C.c_int]),
     "mpdg_heat_picard_tensor_cores": (C.c_int, [_H]),
+    "mpdg_picard_tc_matrices": (C.c_int, [_P]),
     "mpdg_heat_compute_inverse_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_compute_diagonal": (C.c_int, [_H, _D]),
     "mpdg_heat_create_rhs": (C.c_int, [_H, _D, _D, _D]),

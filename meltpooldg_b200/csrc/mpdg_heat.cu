@@ -3011,6 +3011,13 @@ extern "C" int mpdg_heat_set_picard_tensor_cores(mpdg_heat *h, int on)
   return MPDG_OK;
 }
 
+extern "C" int mpdg_picard_tc_matrices(float *out)
+{
+  if (!out) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  optc::build_gmat(out);
+  return MPDG_OK;
+}
+
 extern "C" int mpdg_heat_picard_tensor_cores(const mpdg_heat *h)
 {
   return h && picard_tc_on(h) ? 1 : 0;

@@ -404,3 +404,45 @@ def test_melt_front_propagation_static_gusarov_on_gpu(fused):
         st = opn.solve(5e-6)
         assert st.converged == 1
         assert float(f"{op.l2_norm(opn.T):.5e}") == ref
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_moving_ramped_laser_steps_match_oracle(fused):
+    """A Gauss volumetric laser moving along x (LaserOperation: scan speed 2, power ramped over
+    the first two steps), 4 single-linearisation steps of the constant-k problem on a deformed
+    FE_Q(2) mesh: the source as a nodal vector (compute_heat_source) or evaluated inside the
+    residual kernel (attach), against the oracle's steps with its own laser source at the same
+    positions and powers."""
+    from meltpooldg_b200.laser import LaserData, LaserOperation
+    deg, cells, dt = 2, (6, 5, 4), 0.05
+    o = O.Oracle(deg, cells, perturb=0.15, seed=2)
+    o.set_material(O.material(O.LAW_CONSTANT, k=0.3), dt)
+    op = H.HeatDiffuseOperator(H.box_mesh(deg, cells, perturb=0.15, seed=2))
+    op.set_material(H.material(law=0, k=0.3))
+    data = LaserData(intensity_profile=L.LASER_GAUSS_VOLUMETRIC, power=20.0, radius=0.2,
+                     power_over_time="ramp", power_start_time=0.0, power_end_time=0.1,
+                     scan_speed=2.0, starting_position=(0.2, 0.5, 0.8))
+    las = LaserOperation(data, op)
+    las.reset(0.0)
+    lin = H.LinearSolverData(rel_tolerance=1e-12)
+    opn = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_NONE, single_linearization=True)
+    T = np.zeros(o.n_dofs)
+    opn.set_initial_condition(torch.tensor(T, device="cuda"))
+    q = op.new_vector()
+    for _ in range(4):
+        las.move_laser(dt)
+        if fused:
+            opn.heat_source = None
+            las.attach()
+        else:
+            opn.heat_source = las.compute_heat_source(q)
+        opn.solve(dt)
+        qo = o.laser_source(L.LASER_GAUSS_VOLUMETRIC, las.get_laser_power(),
+                            las.get_laser_position(), radius=0.2)
+        r = o.create_rhs(T, T, qo)
+        d, _, _ = o.cg(r, T_lin=T, T_old=T, rel_tol=1e-13)
+        T = T + d
+    assert las.get_laser_position()[0] == pytest.approx(0.2 + 2.0 * 4 * dt)
+    Tg = opn.T.cpu().numpy()
+    assert np.abs(T).max() > 0.0
+    assert np.abs(Tg - T).max() <= 1e-9 * np.abs(T).max()

@@ -451,7 +451,8 @@ int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params *prm, doub
  *      Predictor's type switch, predictor.hpp:122-154) ---------------------- */
 /* A 3D U-Net (4 levels, 16/32/48/64 channels, 3x3x3 convolutions, BF16 weights and
  * activations, FP32 accumulation) on an nx x ny x nz nodal grid; input 3 channels,
- * output 1 channel, all tensors planar [C][z][y][x] FP32 on the device. */
+ * output 1 channel, the tensors of these calls planar [C][z][y][x] FP32 on the device (the
+ * activations inside are BF16 and channel-chunked). */
 typedef struct mpdg_unet mpdg_unet;
 int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet **out);
 int mpdg_unet_destroy(mpdg_unet *u);
@@ -461,6 +462,9 @@ int mpdg_unet_dims(const mpdg_unet *u, int dims[3]);
 /* FP32 master parameters (device, n_params): get / set (set refreshes the BF16 copy). */
 int mpdg_unet_get_params(mpdg_unet *u, float *dst);
 int mpdg_unet_set_params(mpdg_unet *u, const float *src);
+/* Enqueued on the network's stream without a host synchronisation; an expired wait of a
+ * tensor-core convolution (a hardware fault path, with bounded waits) is reported as
+ * MPDG_ERR_CUDA by the next mpdg_unet_forward or by mpdg_unet_train_step. */
 int mpdg_unet_forward(mpdg_unet *u, const float *input, float *output);
 /* Gradient of sum(grad_output * output) w.r.t. the parameters after a forward. */
 int mpdg_unet_backward(mpdg_unet *u, const float *grad_output, float *grad_params);

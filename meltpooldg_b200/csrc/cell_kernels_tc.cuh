@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(optc::kThreads, 1)
     after_sync();
   }
   if (!ok && lt == 0) {
-    atomicExch(err, 1);
+    *(volatile int *)err = 1;  // page-locked host memory: a plain store
     if (a.st) {
       a.st->status = MPDG_ERR_CUDA;
       a.st->done = 2;

@@ -4026,12 +4026,19 @@ extern "C" int mpdg_heat_l2_norm_noalloc(mpdg_heat *h, const double *u, double *
 // ---------------------------------------------------------------------------
 // learned initial guess: sampling onto the network grid and prolongation back
 // ---------------------------------------------------------------------------
+// scale_sum (nullable, device): the increment scale is then sqrt(scale_sum[0] * inv_n) for
+// s0 and s1, computed on the device (a zero scale gives zero features)
 __global__ void k_learned_input(MeshDims d, int stride, int cx, int cy, int cz,
                                 const double *__restrict__ T, const double *__restrict__ To,
                                 const double *__restrict__ q, double dt, double s0, double s1,
-                                double s2, float *in)
+                                double s2, const double *__restrict__ scale_sum, double inv_n,
+                                float *in)
 {
   const int64_t nc = (int64_t)cx * cy * cz;
+  if (scale_sum) {
+    s0 = s1 = sqrt(scale_sum[0] * inv_n);
+    if (!(s0 > 0.0)) s0 = s1 = INFINITY;  // zero features
+  }
   GRID_STRIDE(t, nc)
   {
     const int X = (int)(t % cx), Y = (int)((t / cx) % cy), Z = (int)(t / ((int64_t)cx * cy));
@@ -4078,8 +4085,10 @@ __global__ void k_learned_guess(int64_t N, MeshDims d, int stride, int cx, int c
 
 // the network's increment direction s3 P(y), zero at the Dirichlet DoFs
 __global__ void k_learned_direction(int64_t N, MeshDims d, int stride, int cx, int cy, int cz,
-                                    const float *__restrict__ y, double s3, double *g)
+                                    const float *__restrict__ y, double s3,
+                                    const double *__restrict__ scale_sum, double inv_n, double *g)
 {
+  if (scale_sum) s3 = sqrt(scale_sum[0] * inv_n);
   GRID_STRIDE(i, N)
   {
     const int I = (int)(i % d.nd[0]), J = (int)((i / d.nd[0]) % d.nd[1]),
@@ -4124,7 +4133,7 @@ extern "C" int mpdg_heat_learned_input(mpdg_heat *h, int stride, const double *T
   const int64_t nc = (int64_t)c[0] * c[1] * c[2];
   k_learned_input<<<vgrid(h, nc), VT, 0, h->stream>>>(h->dims, stride, c[0], c[1], c[2], T, T_old,
                                                      heat_source, dt, scales[0], scales[1],
-                                                     scales[2], input);
+                                                     scales[2], nullptr, 0.0, input);
   CU(cudaGetLastError());
   ++h->launches;
   return MPDG_OK;
@@ -4246,21 +4255,23 @@ extern "C" int mpdg_heat_learned_direction(mpdg_heat *h, mpdg_unet *u, int strid
   TRY(dalloc(h, reinterpret_cast<void **>(&h->nn_buf), sizeof(float) * 4 * nc));
   if (h->nn_buf_n == 0) h->nn_buf_n = nc;
   if (h->nn_buf_n != nc) return fail(MPDG_ERR_INVALID_ARGUMENT, "network grid changed");
-  // per-sample scale: RMS of the time increment
+  // per-sample scale: RMS of the time increment, kept on the device (no host round trip: the
+  // feature and direction kernels take the square root themselves; a zero increment gives
+  // zero features and a zero direction)
   k_diff_sq<<<vgrid(h, N), VT, 0, h->stream>>>(N, T, T_old, h->partials, h->counter, h->scal);
   ++h->launches;
   CU(cudaGetLastError());
-  TRY(read_to_host(h, h->scal_map, h->scal, sizeof(double)));
-  const double a = std::sqrt(h->scal_host[0] / (double)N);
-  if (!(a > 0.0)) return zero_async(h, direction, sizeof(double) * N, h->stream) == cudaSuccess
-                           ? MPDG_OK : fail(MPDG_ERR_CUDA, "zero fill");
-  const double scales[3] = {a, a, T_scale};
-  TRY(mpdg_heat_learned_input(h, stride, T, T_old, heat_source, dt, scales, h->nn_buf));
+  k_learned_input<<<vgrid(h, nc), VT, 0, h->stream>>>(h->dims, stride, c[0], c[1], c[2], T, T_old,
+                                                     heat_source, dt, 1.0, 1.0, T_scale, h->scal,
+                                                     1.0 / (double)N, h->nn_buf);
+  ++h->launches;
+  CU(cudaGetLastError());
   mpdg_unet_set_stream(u, h->stream);
   const int rc = mpdg_unet_forward(u, h->nn_buf, h->nn_buf + 3 * nc);
   if (rc != MPDG_OK) return fail(rc, "network forward failed");
   k_learned_direction<<<vgrid(h, N), VT, 0, h->stream>>>(N, h->dims, stride, c[0], c[1], c[2],
-                                                         h->nn_buf + 3 * nc, a, direction);
+                                                         h->nn_buf + 3 * nc, 0.0, h->scal,
+                                                         1.0 / (double)N, direction);
   ++h->launches;
   CU(cudaGetLastError());
   return MPDG_OK;

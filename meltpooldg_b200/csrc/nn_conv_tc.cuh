@@ -3,7 +3,8 @@
 // output channels (padded to 16/32/48/64), K = 27 taps x the input channels.
 //
 // No im2col: a CTA stages the halo of its 8 x 16 x 1 output tile for all input
-// channels in shared memory as 8-channel chunks, [chunk][hz][hy][hx] x 16 bytes,
+// channels in shared memory as 8-channel chunks, [chunk][hz][hy][hx] x 16 bytes (one
+// 16-byte load per point and chunk from the channel-chunked activations),
 // which is the canonical no-swizzle K-major UMMA layout for ANY tap shift: the 8
 // rows of a core matrix are 8 consecutive x points (16 bytes apart), row groups
 // are the 16 y rows (stride 16 * 10 bytes), the two K halves of a 16-channel
@@ -14,7 +15,8 @@
 // [tap][16-channel group][K half][Cout][8] and kept in shared memory for the
 // whole persistent CTA when they fit (else streamed 9 taps at a time). The
 // epilogue reads the accumulator with tcgen05.ld (one output point per thread),
-// adds bias and the skip input, applies ReLU and stores planar [C][points].
+// adds bias and the skip input, applies ReLU and stores the BF16 activations channel-chunked
+// ([C/8][points][8], one 16-byte vector per point and chunk; FP32 outputs planar [C][points]).
 //
 // Waits on the MMA-completion barrier are bounded; on expiry the kernel raises
 // *err, skips its stores, frees its tensor memory and returns.
@@ -89,6 +91,7 @@ template <int NPAD, bool RELU, bool ADD, typename TO>
 __global__ void __launch_bounds__(kThreads, 1) k_conv3d_tc(ConvArgs a)
 {
   static_assert(NPAD % 16 == 0 && NPAD >= 16 && NPAD <= 64, "N = 16, 32, 48, 64");
+  static_assert(!(ADD && sizeof(TO) == 4), "the skip input is added to BF16 activations only");
   constexpr uint32_t TCOLS = tmem_cols(NPAD);
   constexpr uint32_t IDESC = idesc_bf16_m128(NPAD);
   extern __shared__ __align__(128) unsigned char smem[];
@@ -124,7 +127,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3d_tc(ConvArgs a)
   if (resident)
     for (int i = tid; i < wstage; i += kThreads) wsm[i] = a.wp[i];
   const uint32_t halo_a = smem_u32(halo), w_a = smem_u32(wsm);
-  const unsigned short *src = reinterpret_cast<const unsigned short *>(a.in);
+  // activations are channel-chunked, [C/8][points][8] BF16: one 16-byte vector per point and
+  // 8-channel chunk (chunks past ceil(Ci/8) are zero)
+  const uint4 *src = reinterpret_cast<const uint4 *>(a.in);
   const int64_t snp = a.up ? (int64_t)a.sx * a.sy * a.sz : np;  // input plane size
   uint32_t phase = 0;
   bool ok = true;
@@ -146,17 +151,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3d_tc(ConvArgs a)
         const int c = i / THP, hp = i - c * THP;
         const int hx = hp % THX, hy = (hp / THX) % THY, hz = hp / (THX * THY);
         const int gx = bx + hx - 1, gy = by + hy - 1, gz = bz + hz - 1;
-        if (i < nitems && gx >= 0 && gx < a.nx && gy >= 0 && gy < a.ny && gz >= 0 && gz < a.nz) {
+        if (i < nitems && 8 * c < a.ci && gx >= 0 && gx < a.nx && gy >= 0 && gy < a.ny && gz >= 0 &&
+            gz < a.nz) {
           // the input lives on the grid itself or, with a.up, on the coarse grid it is
           // nearest-neighbour upsampled from
           const int64_t gp = a.up ? (gx >> 1) + (int64_t)a.sx * ((gy >> 1) + (int64_t)a.sy * (gz >> 1))
                                   : gx + (int64_t)a.nx * (gy + (int64_t)a.ny * gz);
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int ch = 8 * c + e;
-            const uint32_t v = ch < a.ci ? (uint32_t)__ldg(src + (int64_t)ch * snp + gp) : 0u;
-            w4[u][e >> 1] |= v << (16 * (e & 1));
-          }
+          const uint4 v = __ldg(src + (int64_t)c * snp + gp);
+          w4[u][0] = v.x;
+          w4[u][1] = v.y;
+          w4[u][2] = v.z;
+          w4[u][3] = v.w;
         }
       }
 #pragma unroll
@@ -219,19 +224,42 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3d_tc(ConvArgs a)
           "=r"(r[7])
         : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (inside) {
+      if (inside && c0 < a.co) {
+        if constexpr (sizeof(TO) == 4) {
+          // FP32 outputs (the network's output, data gradients) are planar [C][points]
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int co = c0 + j;
-          if (co < a.co) {
-            float v = __uint_as_float(r[j]) + a.bias[co];
-            if (ADD) v += __bfloat162float(a.add[(int64_t)co * np + p]);
-            if (RELU) v = fmaxf(v, 0.f);
-            if constexpr (sizeof(TO) == 4)
+          for (int j = 0; j < 8; ++j) {
+            const int co = c0 + j;
+            if (co < a.co) {
+              float v = __uint_as_float(r[j]) + a.bias[co];
+              if (RELU) v = fmaxf(v, 0.f);
               reinterpret_cast<float *>(a.out)[(int64_t)co * np + p] = v;
-            else
-              reinterpret_cast<__nv_bfloat16 *>(a.out)[(int64_t)co * np + p] = __float2bfloat16(v);
+            }
           }
+        } else {
+          // BF16 activations: the chunk's 8 channels as one 16-byte vector (zero past Co)
+          uint4 sk = make_uint4(0u, 0u, 0u, 0u);
+          if (ADD) sk = __ldg(reinterpret_cast<const uint4 *>(a.add) + (int64_t)(c0 >> 3) * np + p);
+          const __nv_bfloat16 *skh = reinterpret_cast<const __nv_bfloat16 *>(&sk);
+          uint32_t o4[4];
+#pragma unroll
+          for (int j = 0; j < 8; j += 2) {
+            float v[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int co = c0 + j + e;
+              v[e] = 0.f;
+              if (co < a.co) {
+                v[e] = __uint_as_float(r[j + e]) + a.bias[co];
+                if (ADD) v[e] += __bfloat162float(skh[j + e]);
+                if (RELU) v[e] = fmaxf(v[e], 0.f);
+              }
+            }
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[0], v[1]);
+            o4[j >> 1] = *reinterpret_cast<const uint32_t *>(&h2);
+          }
+          reinterpret_cast<uint4 *>(a.out)[(int64_t)(c0 >> 3) * np + p] =
+            make_uint4(o4[0], o4[1], o4[2], o4[3]);
         }
       }
     }
@@ -239,7 +267,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3d_tc(ConvArgs a)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
   }
-  if (!ok && tid == 0) atomicExch(a.err, 1);
+  if (!ok && tid == 0) *(volatile int *)a.err = 1;  // page-locked host memory: a plain store
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

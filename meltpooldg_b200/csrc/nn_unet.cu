@@ -77,6 +77,23 @@ template <typename T> __device__ __forceinline__ T fromf(float v);
 template <> __device__ __forceinline__ float fromf<float>(float v) { return v; }
 template <> __device__ __forceinline__ __nv_bfloat16 fromf<__nv_bfloat16>(float v) { return __float2bfloat16(v); }
 
+// BF16 activations are channel-chunked, [ceil(C/8)][points][8] (one 16-byte vector per point and
+// 8-channel chunk, pad channels zero); FP32 tensors (gradients, the output) are planar [C][points]
+__host__ __device__ __forceinline__ int64_t aidx(int c, int64_t p, int64_t np)
+{
+  return ((int64_t)(c >> 3) * np + p) * 8 + (c & 7);
+}
+template <typename T> __device__ __forceinline__ int64_t tidx(int c, int64_t p, int64_t np);
+template <> __device__ __forceinline__ int64_t tidx<float>(int c, int64_t p, int64_t np)
+{
+  return (int64_t)c * np + p;
+}
+template <> __device__ __forceinline__ int64_t tidx<__nv_bfloat16>(int c, int64_t p, int64_t np)
+{
+  return aidx(c, p, np);
+}
+__host__ __device__ constexpr int pad8(int c) { return (c + 7) & ~7; }
+
 // out[co][p] = bias[co] + sum_ci sum_o w[co][ci][o] in[ci][p + o - 1]
 //   (+ add[co][p]) ; relu ; (* (mask[co][p] > 0))
 // flip: use w[ci][co][26 - o] (the transposed convolution of the backward pass)
@@ -102,13 +119,12 @@ __global__ void __launch_bounds__(TP) k_conv3d(Grid3 g, int Ci, int Co, const TI
 #pragma unroll
   for (int c = 0; c < COB; ++c) acc[c] = 0.f;
   for (int ci = 0; ci < Ci; ++ci) {
-    const TI *src = in + (int64_t)ci * np;
     for (int i = threadIdx.x; i < HP; i += TP) {
       const int hx = i % HX, hy = (i / HX) % HY, hz = i / (HX * HY);
       const int gx = bx + hx - 1, gy = by + hy - 1, gz = bz + hz - 1;
       float v = 0.f;
       if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz)
-        v = tof<TI>(src[(int64_t)gx + (int64_t)g.nx * (gy + (int64_t)g.ny * gz)]);
+        v = tof<TI>(in[tidx<TI>(ci, (int64_t)gx + (int64_t)g.nx * (gy + (int64_t)g.ny * gz), np)]);
       s_in[i] = v;
     }
     for (int i = threadIdx.x; i < COB * 27; i += TP) {
@@ -145,10 +161,10 @@ __global__ void __launch_bounds__(TP) k_conv3d(Grid3 g, int Ci, int Co, const TI
     const int co = co0 + c;
     if (co >= Co) break;
     float r = acc[c] + (bias ? bias[co] : 0.f);
-    if (ADD) r += __bfloat162float(add[(int64_t)co * np + p]);
+    if (ADD) r += __bfloat162float(add[aidx(co, p, np)]);
     if (RELU) r = fmaxf(r, 0.f);
-    if (MASK) r = __bfloat162float(mask[(int64_t)co * np + p]) > 0.f ? r : 0.f;
-    out[(int64_t)co * np + p] = fromf<TO>(r);
+    if (MASK) r = __bfloat162float(mask[aidx(co, p, np)]) > 0.f ? r : 0.f;
+    out[tidx<TO>(co, p, np)] = fromf<TO>(r);
   }
 }
 
@@ -184,7 +200,7 @@ __global__ void __launch_bounds__(COB * CIB) k_conv3d_wgrad(Grid3 g, int Ci, int
     const int ci = ci0 + c;
     float v = 0.f;
     if (ci < Ci && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz)
-      v = __bfloat162float(in[(int64_t)ci * np + gx + (int64_t)g.nx * (gy + (int64_t)g.ny * gz)]);
+      v = __bfloat162float(in[aidx(ci, gx + (int64_t)g.nx * (gy + (int64_t)g.ny * gz), np)]);
     s_in[i] = v;
   }
   __syncthreads();
@@ -232,11 +248,11 @@ __global__ void k_pool(Grid3 f, int C, const __nv_bfloat16 *__restrict__ in, __n
         for (int dx = 0; dx < 2; ++dx) {
           const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
           if (x < f.nx && y < f.ny && z < f.nz) {
-            s += __bfloat162float(in[(int64_t)ch * f.n() + x + (int64_t)f.nx * (y + (int64_t)f.ny * z)]);
+            s += __bfloat162float(in[aidx(ch, x + (int64_t)f.nx * (y + (int64_t)f.ny * z), f.n())]);
             ++cnt;
           }
         }
-    out[t] = __float2bfloat16(s / cnt);
+    out[aidx(ch, p, c.n())] = __float2bfloat16(s / cnt);
   }
 }
 
@@ -264,7 +280,7 @@ __global__ void k_up(Grid3 f, int C, const __nv_bfloat16 *__restrict__ in, __nv_
     const int ch = (int)(t / f.n());
     const int64_t p = t % f.n();
     const int x = (int)(p % f.nx), y = (int)((p / f.nx) % f.ny), z = (int)(p / ((int64_t)f.nx * f.ny));
-    out[t] = in[(int64_t)ch * c.n() + x / 2 + (int64_t)c.nx * (y / 2 + (int64_t)c.ny * (z / 2))];
+    out[aidx(ch, p, f.n())] = in[aidx(ch, x / 2 + (int64_t)c.nx * (y / 2 + (int64_t)c.ny * (z / 2)), c.n())];
   }
 }
 
@@ -289,11 +305,12 @@ __global__ void k_up_bwd(Grid3 f, int C, const float *__restrict__ gout, float *
   }
 }
 
-// g *= (y > 0)
-__global__ void k_relu_mask(int64_t n, const __nv_bfloat16 *__restrict__ y, float *g)
+// g[c][p] *= (y[c][p] > 0) for C channels of np points (y chunked, g planar)
+__global__ void k_relu_mask(int64_t np, int C, const __nv_bfloat16 *__restrict__ y, float *g)
 {
+  const int64_t n = np * C;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-    if (!(__bfloat162float(y[t]) > 0.f)) g[t] = 0.f;
+    if (!(__bfloat162float(y[aidx((int)(t / np), t % np, np)]) > 0.f)) g[t] = 0.f;
 }
 
 __global__ void k_add_inplace(int64_t n, float *a, const float *__restrict__ b)
@@ -306,6 +323,17 @@ __global__ void k_f32_to_bf16(int64_t n, const float *__restrict__ a, __nv_bfloa
 {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
     b[t] = __float2bfloat16(a[t]);
+}
+
+// planar FP32 [C][np] -> chunked BF16 [ceil(C/8)][np][8], pad channels zero
+__global__ void k_f32_to_chunked(int64_t np, int C, const float *__restrict__ a, __nv_bfloat16 *b)
+{
+  const int64_t n = np * pad8(C);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t & 7) + 8 * (int)(t / (8 * np));
+    const int64_t p = (t >> 3) % np;
+    b[t] = __float2bfloat16(c < C ? a[(int64_t)c * np + p] : 0.f);
+  }
 }
 
 // loss = mean (y - target)^2 ; g = 2 (y - target) / n
@@ -367,7 +395,9 @@ struct mpdg_unet {
   bool use_tc = true;         // forward convolutions on the tensor cores
   bool training = false;      // forward keeps what the backward pass reads
   bool ups_valid = false;     // u2, u1, u0 hold the upsampled decoder inputs
-  int *tc_err = nullptr;      // raised by a tensor-core convolution whose wait expired
+  // raised by a tensor-core convolution whose wait expired: page-locked mapped host memory
+  // (tc_err is its device address), read by the host without a synchronisation
+  int *tc_err = nullptr, *tc_err_host = nullptr;
   int sm_count = 148;
   int64_t step = 0;
   // activations (BF16) and gradients (FP32)
@@ -534,7 +564,7 @@ int dgrad_tc(mpdg_unet *u, int l, Grid3 g, const float *gout, float *gin,
   if (u->wpk_dirty) NNTRY(pack_weights(u));
   const int ci = u->L[l].ci, co = u->L[l].co;
   const int64_t n = g.n();
-  k_f32_to_bf16<<<grid1d((int64_t)co * n), 256, 0, u->stream>>>((int64_t)co * n, gout, u->gbf);
+  k_f32_to_chunked<<<grid1d((int64_t)pad8(co) * n), 256, 0, u->stream>>>(n, co, gout, u->gbf);
   NNCU(cudaGetLastError());
   const uint4 *wp = u->wpkt + u->wpkt_off[l];
   int rc;
@@ -547,7 +577,7 @@ int dgrad_tc(mpdg_unet *u, int l, Grid3 g, const float *gout, float *gin,
   }
   NNTRY(rc);
   if (mask) {
-    k_relu_mask<<<grid1d((int64_t)ci * n), 256, 0, u->stream>>>((int64_t)ci * n, mask, gin);
+    k_relu_mask<<<grid1d((int64_t)ci * n), 256, 0, u->stream>>>(n, ci, mask, gin);
     NNCU(cudaGetLastError());
   }
   return MPDG_OK;
@@ -560,6 +590,17 @@ int dgrad(mpdg_unet *u, int l, Grid3 g, const float *gout, float *gin, const __n
   if (mask)
     return conv<float, float, false, false, true, true>(u, g, u->L[l].co, u->L[l].ci, gout, W(u, l), nullptr, nullptr, mask, gin);
   return conv<float, float, false, false, false, true>(u, g, u->L[l].co, u->L[l].ci, gout, W(u, l), nullptr, nullptr, nullptr, gin);
+}
+
+// the error flag of the tensor-core convolutions, read (and cleared) without a synchronisation:
+// a forward's expired wait is reported by the next call that checks
+int check_tc_err(mpdg_unet *u)
+{
+  if (u->tc_err_host && *(volatile int *)u->tc_err_host) {
+    *(volatile int *)u->tc_err_host = 0;
+    return nn_fail(MPDG_ERR_CUDA, "tensor-core convolution: wait for the MMAs expired");
+  }
+  return MPDG_OK;
 }
 
 int forward(mpdg_unet *u)
@@ -626,8 +667,8 @@ int backward(mpdg_unet *u, const float *gy)
   }
   NNCU(cudaMemsetAsync(u->grad, 0, sizeof(float) * u->n_params, u->stream));
   float *gA = u->gA, *gB = u->gB, *gC = u->gC;
-  auto relu_mask = [&](int64_t n, const __nv_bfloat16 *y, float *gg) -> int {
-    k_relu_mask<<<grid1d(n), 256, 0, u->stream>>>(n, y, gg);
+  auto relu_mask = [&](Grid3 gr, int C, const __nv_bfloat16 *y, float *gg) -> int {
+    k_relu_mask<<<grid1d(gr.n() * C), 256, 0, u->stream>>>(gr.n(), C, y, gg);
     NNCU(cudaGetLastError());
     return MPDG_OK;
   };
@@ -655,39 +696,39 @@ int backward(mpdg_unet *u, const float *gy)
   NNCU(cudaMemcpyAsync(u->gE0, gB, sizeof(float) * 16 * g[0].n(), cudaMemcpyDeviceToDevice, u->stream));
   NNTRY(dgrad(u, D0A, g[0], gB, gC, nullptr));          // gC: d u0 (32 @ g0)
   NNTRY(up_bwd(g[0], 32, gC, gA));                      // gA: d d1 (32 @ g1)
-  NNTRY(relu_mask(32 * g[1].n(), u->d1, gA));
+  NNTRY(relu_mask(g[1], 32, u->d1, gA));
   NNTRY(wgrad(u, g[1], D1B, u->s1, gA));
   NNTRY(dgrad(u, D1B, g[1], gA, gB, u->s1));
   NNTRY(wgrad(u, g[1], D1A, u->u1, gB));
   NNCU(cudaMemcpyAsync(u->gE1, gB, sizeof(float) * 32 * g[1].n(), cudaMemcpyDeviceToDevice, u->stream));
   NNTRY(dgrad(u, D1A, g[1], gB, gC, nullptr));          // d u1 (48 @ g1)
   NNTRY(up_bwd(g[1], 48, gC, gA));                      // d d2 (48 @ g2)
-  NNTRY(relu_mask(48 * g[2].n(), u->d2, gA));
+  NNTRY(relu_mask(g[2], 48, u->d2, gA));
   NNTRY(wgrad(u, g[2], D2B, u->s2, gA));
   NNTRY(dgrad(u, D2B, g[2], gA, gB, u->s2));
   NNTRY(wgrad(u, g[2], D2A, u->u2, gB));
   NNCU(cudaMemcpyAsync(u->gE2, gB, sizeof(float) * 48 * g[2].n(), cudaMemcpyDeviceToDevice, u->stream));
   NNTRY(dgrad(u, D2A, g[2], gB, gC, nullptr));          // d u2 (64 @ g2)
   NNTRY(up_bwd(g[2], 64, gC, gA));                      // d e3 (64 @ g3)
-  NNTRY(relu_mask(64 * g[3].n(), u->e3, gA));
+  NNTRY(relu_mask(g[3], 64, u->e3, gA));
   NNTRY(wgrad(u, g[3], E3B, u->a3, gA));
   NNTRY(dgrad(u, E3B, g[3], gA, gB, u->a3));
   NNTRY(wgrad(u, g[3], E3A, u->p2, gB));
   NNTRY(dgrad(u, E3A, g[3], gB, gC, nullptr));          // d p2 (48 @ g3)
   NNTRY(pool_bwd(g[2], 48, gC, u->gE2));                // d e2 += pool^T
-  NNTRY(relu_mask(48 * g[2].n(), u->e2, u->gE2));
+  NNTRY(relu_mask(g[2], 48, u->e2, u->gE2));
   NNTRY(wgrad(u, g[2], E2B, u->a2, u->gE2));
   NNTRY(dgrad(u, E2B, g[2], u->gE2, gB, u->a2));
   NNTRY(wgrad(u, g[2], E2A, u->p1, gB));
   NNTRY(dgrad(u, E2A, g[2], gB, gC, nullptr));          // d p1 (32 @ g2)
   NNTRY(pool_bwd(g[1], 32, gC, u->gE1));
-  NNTRY(relu_mask(32 * g[1].n(), u->e1, u->gE1));
+  NNTRY(relu_mask(g[1], 32, u->e1, u->gE1));
   NNTRY(wgrad(u, g[1], E1B, u->a1, u->gE1));
   NNTRY(dgrad(u, E1B, g[1], u->gE1, gB, u->a1));
   NNTRY(wgrad(u, g[1], E1A, u->p0, gB));
   NNTRY(dgrad(u, E1A, g[1], gB, gC, nullptr));          // d p0 (16 @ g1)
   NNTRY(pool_bwd(g[0], 16, gC, u->gE0));
-  NNTRY(relu_mask(16 * g[0].n(), u->e0, u->gE0));
+  NNTRY(relu_mask(g[0], 16, u->e0, u->gE0));
   NNTRY(wgrad(u, g[0], E0B, u->a0, u->gE0));
   NNTRY(dgrad(u, E0B, g[0], u->gE0, gB, u->a0));
   NNTRY(wgrad(u, g[0], E0A, u->x0, gB));
@@ -725,12 +766,13 @@ extern "C" int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet
   u->n_params = off;
   auto fail_free = [&](int rc) {
     for (void *p : u->owned) cudaFree(p);
+    if (u->tc_err_host) cudaFreeHost(u->tc_err_host);
     delete u;
     return rc;
   };
   const int64_t n0 = u->g[0].n(), n1 = u->g[1].n(), n2 = u->g[2].n(), n3 = u->g[3].n();
   struct A { __nv_bfloat16 **p; int64_t n; } acts[] = {
-    {&u->x0, 3 * n0}, {&u->a0, 16 * n0}, {&u->e0, 16 * n0}, {&u->p0, 16 * n1}, {&u->a1, 32 * n1},
+    {&u->x0, 8 * n0}, {&u->a0, 16 * n0}, {&u->e0, 16 * n0}, {&u->p0, 16 * n1}, {&u->a1, 32 * n1},
     {&u->e1, 32 * n1}, {&u->p1, 32 * n2}, {&u->a2, 48 * n2}, {&u->e2, 48 * n2}, {&u->p2, 48 * n3},
     {&u->a3, 64 * n3}, {&u->e3, 64 * n3}, {&u->u2, 64 * n2}, {&u->s2, 48 * n2}, {&u->d2, 48 * n2},
     {&u->u1, 48 * n1}, {&u->s1, 32 * n1}, {&u->d1, 32 * n1}, {&u->u0, 32 * n0}, {&u->s0, 16 * n0},
@@ -753,9 +795,13 @@ extern "C" int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet
       (rc = ualloc(u, (void **)&u->pb, sizeof(__nv_bfloat16) * u->n_params)) != MPDG_OK ||
       (rc = ualloc(u, (void **)&u->partials, sizeof(double) * 148 * 16)) != MPDG_OK ||
       (rc = ualloc(u, (void **)&u->lossd, sizeof(double) * 2)) != MPDG_OK ||
-      (rc = ualloc(u, (void **)&u->counter, sizeof(unsigned) * 4)) != MPDG_OK ||
-      (rc = ualloc(u, (void **)&u->tc_err, sizeof(int))) != MPDG_OK)
+      (rc = ualloc(u, (void **)&u->counter, sizeof(unsigned) * 4)) != MPDG_OK)
     return fail_free(rc);
+  if (cudaHostAlloc((void **)&u->tc_err_host, sizeof(int), cudaHostAllocMapped) != cudaSuccess)
+    return fail_free(nn_fail(MPDG_ERR_OUT_OF_MEMORY, "cudaHostAlloc (unet)"));
+  *u->tc_err_host = 0;
+  if (cudaHostGetDevicePointer((void **)&u->tc_err, u->tc_err_host, 0) != cudaSuccess)
+    return fail_free(nn_fail(MPDG_ERR_CUDA, "cudaHostGetDevicePointer (unet)"));
   int64_t wtot = 0;
   for (int l = 0; l < 15; ++l) {
     u->wpk_off[l] = wtot;
@@ -766,14 +812,13 @@ extern "C" int mpdg_unet_create(int nx, int ny, int nz, uint64_t seed, mpdg_unet
   for (int l = 0; l < 15; ++l) {
     u->wpkt_off[l] = wtot_t;
     wtot_t += (int64_t)27 * cg_of(kCo[l]) * 2 * npad_of(kCi[l]);
-    gbf_n = std::max(gbf_n, (int64_t)kCo[l] * u->g[kLevel[l]].n());  // an output gradient
+    gbf_n = std::max(gbf_n, (int64_t)pad8(kCo[l]) * u->g[kLevel[l]].n());  // an output gradient
   }
   if ((rc = ualloc(u, (void **)&u->wpkt, sizeof(uint4) * wtot_t)) != MPDG_OK ||
       (rc = ualloc(u, (void **)&u->gbf, sizeof(__nv_bfloat16) * gbf_n)) != MPDG_OK ||
       (rc = ualloc(u, (void **)&u->zero_bias, sizeof(float) * 64)) != MPDG_OK)
     return fail_free(rc);
   cudaMemset(u->zero_bias, 0, sizeof(float) * 64);
-  cudaMemset(u->tc_err, 0, sizeof(int));
   {
     const char *e = getenv("MPDG_UNET_TC");
     u->use_tc = !(e && e[0] == '0');
@@ -807,6 +852,7 @@ extern "C" int mpdg_unet_destroy(mpdg_unet *u)
   if (!u) return MPDG_OK;
   if (u->stream) cudaStreamSynchronize(u->stream);
   for (void *p : u->owned) cudaFree(p);
+  if (u->tc_err_host) cudaFreeHost(u->tc_err_host);
   delete u;
   return MPDG_OK;
 }
@@ -855,20 +901,12 @@ extern "C" int mpdg_unet_set_params(mpdg_unet *u, const float *src)
 extern "C" int mpdg_unet_forward(mpdg_unet *u, const float *input, float *output)
 {
   if (!u || !input) return nn_fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  NNTRY(check_tc_err(u));  // raised by an earlier forward's convolutions
   const int64_t n0 = u->g[0].n();
-  k_f32_to_bf16<<<grid1d(3 * n0), 256, 0, u->stream>>>(3 * n0, input, u->x0);
+  k_f32_to_chunked<<<grid1d(8 * n0), 256, 0, u->stream>>>(n0, 3, input, u->x0);
   NNCU(cudaGetLastError());
   NNTRY(forward(u));
   if (output) NNCU(cudaMemcpyAsync(output, u->y, sizeof(float) * n0, cudaMemcpyDeviceToDevice, u->stream));
-  if (u->use_tc) {
-    int err = 0;
-    NNCU(cudaMemcpyAsync(&err, u->tc_err, sizeof(int), cudaMemcpyDeviceToHost, u->stream));
-    NNCU(cudaStreamSynchronize(u->stream));
-    if (err) {
-      cudaMemsetAsync(u->tc_err, 0, sizeof(int), u->stream);
-      return nn_fail(MPDG_ERR_CUDA, "tensor-core convolution: wait for the MMAs expired");
-    }
-  }
   return MPDG_OK;
 }
 
@@ -912,6 +950,7 @@ extern "C" int mpdg_unet_train_step(mpdg_unet *u, const float *input, const floa
     NNCU(cudaMemcpyAsync(&l, u->lossd, sizeof(double), cudaMemcpyDeviceToHost, u->stream));
     NNCU(cudaStreamSynchronize(u->stream));
     *loss = l;
+    NNTRY(check_tc_err(u));
   }
   return MPDG_OK;
 }

@@ -33,7 +33,10 @@ template <int n> __host__ __device__ constexpr int v2_cell_stride()
   while (s % 16 != 4) ++s;
   return s;
 }
-template <int LAW> __host__ __device__ constexpr int v2_ncoef() { return (LAW == 1) ? 4 : (LAW == 2 ? 5 : 0); }
+template <int LAW> __host__ __device__ constexpr int v2_ncoef()
+{
+  return (LAW == 1) ? 4 : (LAW == 2 ? 5 : (LAW == 8 ? 1 : 0));
+}
 constexpr int kV2Warps = 2;  // warps per CTA
 template <int n, typename T, int LAW> __host__ __device__ constexpr size_t v2_smem_per_warp()
 {
@@ -246,8 +249,11 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
   constexpr int CS = v2_cell_stride<n>();
   constexpr int NCOEF = v2_ncoef<LAW>();
   // LAW 3: conductivity field k(q), no tangent; LAW 4: coefficient fields a.cf; LAW 6: the
-  // tangent coefficient fields of LAW 5 built at the linearisation point (8 per point)
+  // tangent coefficient fields of LAW 5 built at the linearisation point (8 per point); LAW 8:
+  // the Picard operator of the linear-k law with k(T_lin(q)) interpolated from the gathered
+  // T_lin (k is affine in T, so this is the conductivity field of LAW 3 without storing it)
   constexpr bool TDEP = LAW == 1 || LAW == 2;
+  constexpr bool TLIN = TDEP || LAW == 8;
   if (a.st && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -276,7 +282,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
     T Pu[n][n];
     gather_plane<n>(d, base, pm, true, a.src, Pu, active);
     T Pt[n][n];
-    if (TDEP) gather_plane<n>(d, base, pm, false, a.Tl, Pt, active);
+    if (TLIN) gather_plane<n>(d, base, pm, false, a.Tl, Pt, active);
 
     // L2 prefetch of the next group's rows (and geometry) while this one computes
     {
@@ -288,7 +294,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
         const int64_t nbase =
           (int64_t)d.nd[0] * (d.p * ncy + (int64_t)d.nd[1] * (d.p * ncz + t)) + d.p * ncx;
         prefetch_plane<n>(a.src, nbase, d.nd[0]);
-        if (TDEP) prefetch_plane<n>(a.Tl, nbase, d.nd[0]);
+        if (TLIN) prefetch_plane<n>(a.Tl, nbase, d.nd[0]);
         if (LAW == 3) {
           const char *kq = reinterpret_cast<const char *>(a.kq + ncell * (n * n * n));
           for (int off = t * 128; off < n * n * n * 4; off += n * 128)
@@ -311,6 +317,23 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
       }
     }
 
+    if (LAW == 8) {
+      // ---- linearisation point: values at the q-points -> k(T_lin) (thread-private columns)
+      T (&P)[n][n] = Pt;
+      psweep_b<n, kS, false>(P, P);
+      psweep_a<n, kS, false>(P, P);
+      T Tq[n][n];
+      z_to_x1<n>(P, Tq, bufA, t);
+      psweep_a<n, kS, false>(Tq, Tq);
+#pragma unroll
+      for (int k = 0; k < n; ++k)
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          T rhocp, kk, drhocp, dk;
+          mat_eval<1>(a.m, Tq[k][j], rhocp, kk, drhocp, dk);
+          coef[(k * n + j) * 32 + lane] = kk;
+        }
+    }
     if (TDEP) {
       // ---- linearisation point: values and reference gradients at the q-points
       T (&P)[n][n] = Pt;
@@ -419,6 +442,8 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
         } else {
           if (LAW == 3)
             kk = (T)__ldg(a.kq + cc * (n * n * n) + t + n * (j + n * k));
+          else if (LAW == 8)
+            kk = coef[(k * n + j) * 32 + lane];
           else
             kk = a.m.k_l;
           f0 = kk * Ux[k][j];

@@ -138,6 +138,13 @@ struct DegreeOps {
         return cudaErrorNotSupported;
       }
     }
+    if (law == 8) {  // the Picard operator from the gathered T_lin (linear-k law)
+      if constexpr (use_v2<T>()) {
+        return geo == 0 ? vmult_t<T, 0, 8>(a, s, sm) : vmult_t<T, 1, 8>(a, s, sm);
+      } else {
+        return cudaErrorNotSupported;
+      }
+    }
     if (law == 4) return geo == 0 ? vmult_t<T, 0, 4>(a, s, sm) : vmult_t<T, 1, 4>(a, s, sm);
     if (law == 5) return geo == 0 ? vmult_t<T, 0, 5>(a, s, sm) : vmult_t<T, 1, 5>(a, s, sm);
     if (law == 7) return geo == 0 ? vmult_t<T, 0, 7>(a, s, sm) : vmult_t<T, 1, 7>(a, s, sm);

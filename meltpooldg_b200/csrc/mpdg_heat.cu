@@ -1493,6 +1493,18 @@ static bool picard_tc_on(const mpdg_heat *h)
   return on && h->geo == 0 && h->p == 3 && h->tab.vmult_picard_tc != nullptr;
 }
 
+// The Picard operator with k(T_lin(q)) interpolated in the kernel from the gathered FP32 T_lin
+// instead of read from the stored per-point field (LAW 8; the same operator for the linear-k
+// law, which is affine in T): MPDG_PICARD_NODAL=1, register-resident kernel degrees only
+static bool picard_nodal(const mpdg_heat *h)
+{
+  static const int env_on = [] {
+    const char *e = getenv("MPDG_PICARD_NODAL");
+    return (e && e[0] == '1') ? 1 : 0;
+  }();
+  return env_on && h->law == MPDG_LAW_LINEAR_K && h->tab.v2_f;
+}
+
 static int ensure_picard_tc(mpdg_heat *h)
 {
   if (!h->gmat_tc) {
@@ -1522,7 +1534,7 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
   CellArgs<float> a = cell_args<float>(h);
   a.kq = h->kq;
   a.cf = h->cf_f;
-  int law = picard ? 3 : klaw(h);
+  int law = picard ? (picard_nodal(h) ? 8 : 3) : klaw(h);
   if (law == 5 && h->tab.v2_f) {
     TRY(ensure_tangent(h));
     const int64_t nt = h->n_cells * 8 * h->npt;

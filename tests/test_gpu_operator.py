@@ -143,6 +143,24 @@ def test_line_per_thread_tangent_fields_match_oracle():
     assert " passed" in r.stdout
 
 
+def test_picard_operator_from_nodal_linearisation_point_matches_oracle():
+    """The FP32 Picard operator with k(T_lin(q)) interpolated in the kernel from the gathered
+    T_lin (MPDG_PICARD_NODAL=1) on the cell-pair meshes, and the benchmark step at 48^3 with
+    the multigrid built on it, in a child process because the choice is read once per process."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(__file__)
+    env = dict(os.environ, MPDG_PICARD_NODAL="1")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p",
+                        "no:cacheprovider", __file__,
+                        os.path.join(here, "test_gpu_bench_size.py"), "-k",
+                        "fp32_operator_cell_pairs or benchmark_step_at_48cubed"],
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert " passed" in r.stdout
+
+
 def test_picard_operator_rejects_other_laws():
     _, g = pair(2, (2, 2, 2), 0.0, "constant")
     g.set_linearization(g.new_vector(), g.new_vector())

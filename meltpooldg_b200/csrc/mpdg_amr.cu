@@ -48,6 +48,9 @@ struct AmrArgs {
   const double *src;
   const double *Tl;
   const double *q;  // create_rhs: the nodal heat source (nullable)
+  // the linearisation point's values and reference gradients at the q-points, [cell][4][n^3],
+  // built once per solve (nullable: the operator evaluates T_lin itself)
+  const double *tf;
   double *dst;
   int64_t n_cells;
   double h[3];
@@ -79,6 +82,21 @@ __device__ __forceinline__ double line_sum(const double *M, const double *in, in
   double v = 0.0;
 #pragma unroll
   for (int a = 0; a < n; ++a) v += (transpose ? M[a * n + o] : M[o * n + a]) * in[base + a * st];
+  return v;
+}
+
+// transposed line sum with the element-wise product of two 1D matrices:
+// out_o = sum_a A[a][o] B[a][o] in[line(a)] (the closed-form diagonal's contractions)
+template <int n>
+__device__ __forceinline__ double line_sum_pp(const double *A, const double *B, const double *in,
+                                              int t, int dir)
+{
+  const int st = dir == 0 ? 1 : (dir == 1 ? n : n * n);
+  const int o = (t / st) % n;
+  const int base = t - o * st;
+  double v = 0.0;
+#pragma unroll
+  for (int a = 0; a < n; ++a) v += A[a * n + o] * B[a * n + o] * in[base + a * st];
   return v;
 }
 
@@ -187,22 +205,55 @@ __global__ void k_amr_vmult(const AmrArgs a)
     const int dof = a.idx[c * n3 + t];
     const bool hang = (code & 0x1F8) != 0;
     const double size = cell_size(code);
+    const bool eval_T = a.tangent && !a.tf;
     u[t] = a.mask[dof] ? 0.0 : a.src[dof];
-    if (a.tangent) T[t] = a.Tl[dof];
+    if (eval_T) T[t] = a.Tl[dof];
+    if (a.tangent && a.tf) {
+      const double *f = a.tf + c * 4 * n3;
+      Tv[t] = f[t];
+      Tx[t] = f[n3 + t];
+      Ty[t] = f[2 * n3 + t];
+      Tz[t] = f[3 * n3 + t];
+    }
     __syncthreads();
     if (hang) {
       for (int d = 0; d < 3; ++d) {
         const double *I = a.I[(code >> d) & 1];
         hang_dir<n>(u, tmp, code, d, I, false, t);
-        if (a.tangent) hang_dir<n>(T, tmp, code, d, I, false, t);
+        if (eval_T) hang_dir<n>(T, tmp, code, d, I, false, t);
       }
     }
-    if (a.tangent) evaluate<n>(a, T, Tv, Tx, Ty, Tz, t1, t2, s1, s2, s3, t);
+    if (eval_T) evaluate<n>(a, T, Tv, Tx, Ty, Tz, t1, t2, s1, s2, s3, t);
     apply_cell<n>(a, size, u, Tv, Tx, Ty, Tz, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
     if (hang) {
       for (int d = 2; d >= 0; --d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], true, t);
     }
     if (!a.mask[dof]) atomicAdd(a.dst + dof, u[t]);
+    __syncthreads();
+  }
+}
+
+// the linearisation point's values and reference gradients at the q-points of every cell
+// (hanging interpolation applied), [cell][4][n^3]: the operator's T_lin evaluation, once per solve
+template <int n>
+__global__ void k_amr_tfields(const AmrArgs a, double *tf)
+{
+  constexpr int n3 = n * n * n;
+  __shared__ double T[n3], tmp[n3], t1[n3], t2[n3], s1[n3], s2[n3], s3[n3];
+  __shared__ double Tv[n3], Tx[n3], Ty[n3], Tz[n3];
+  const int t = threadIdx.x;
+  for (int64_t c = blockIdx.x; c < a.n_cells; c += gridDim.x) {
+    const int code = a.code[c];
+    T[t] = a.Tl[a.idx[c * n3 + t]];
+    __syncthreads();
+    if ((code & 0x1F8) != 0)
+      for (int d = 0; d < 3; ++d) hang_dir<n>(T, tmp, code, d, a.I[(code >> d) & 1], false, t);
+    evaluate<n>(a, T, Tv, Tx, Ty, Tz, t1, t2, s1, s2, s3, t);
+    double *f = tf + c * 4 * n3;
+    f[t] = Tv[t];
+    f[n3 + t] = Tx[t];
+    f[2 * n3 + t] = Ty[t];
+    f[3 * n3 + t] = Tz[t];
     __syncthreads();
   }
 }
@@ -229,16 +280,55 @@ __global__ void k_amr_diag(const AmrArgs a)
       evaluate<n>(a, T, Tv, Tx, Ty, Tz, t1, t2, s1, s2, s3, t);
     }
     double mine = 0.0;
-    for (int j = 0; j < n3; ++j) {
-      u[t] = t == j ? 1.0 : 0.0;
+    if (!hang) {
+      // closed form: diag_i = sum_q [F0 P P P + F_x Q P P + F_y P Q P + F_z P P Q
+      //                              + G_x R P P + G_y P R P + G_z P P R](q, i)
+      // with P = S o S, Q = Sd o Sd, R = S o Sd (element-wise, [q][i]) along x, y, z and the
+      // point factors of apply_cell: F0 = JxW rho_cp/dt, F_d = JxW k / h_d^2,
+      // G_d = JxW k1 dT/dxi_d / h_d^2 (the tangent's k1 grad(T_lin) u term)
+      {
+        const int qx = t % n, qy = (t / n) % n, qz = t / (n * n);
+        const double hx = a.h[0] * size, hy = a.h[1] * size, hz = a.h[2] * size;
+        const double jxw = a.w[qx] * a.w[qy] * a.w[qz] * hx * hy * hz;
+        const double k = a.tangent ? a.k0 + a.k1 * Tv[t] : a.k0;
+        val[t] = jxw * a.cval;
+        gx[t] = jxw * k / (hx * hx);
+        gy[t] = jxw * k / (hy * hy);
+        gz[t] = jxw * k / (hz * hz);
+        t1[t] = a.tangent ? jxw * a.k1 * Tx[t] / (hx * hx) : 0.0;
+        t2[t] = a.tangent ? jxw * a.k1 * Ty[t] / (hy * hy) : 0.0;
+        s1[t] = a.tangent ? jxw * a.k1 * Tz[t] / (hz * hz) : 0.0;
+      }
       __syncthreads();
-      if (hang)
+      const double *S = a.S, *D = a.Sd;
+      // along z: the five (x, y) matrix pairs that remain
+      s2[t] = line_sum_pp<n>(S, S, val, t, 2) + line_sum_pp<n>(D, D, gz, t, 2) +
+              line_sum_pp<n>(S, D, s1, t, 2);            // (P, P)
+      s3[t] = line_sum_pp<n>(S, S, gx, t, 2);            // (Q, P)
+      u[t] = line_sum_pp<n>(S, S, gy, t, 2);             // (P, Q)
+      tmp[t] = line_sum_pp<n>(S, S, t1, t, 2);           // (R, P)
+      T[t] = line_sum_pp<n>(S, S, t2, t, 2);             // (P, R)
+      __syncthreads();
+      // along y
+      val[t] = line_sum_pp<n>(S, S, s2, t, 1) + line_sum_pp<n>(D, D, u, t, 1) +
+               line_sum_pp<n>(S, D, T, t, 1);            // x: P
+      gx[t] = line_sum_pp<n>(S, S, s3, t, 1);            // x: Q
+      gy[t] = line_sum_pp<n>(S, S, tmp, t, 1);           // x: R
+      __syncthreads();
+      mine = line_sum_pp<n>(S, S, val, t, 0) + line_sum_pp<n>(D, D, gx, t, 0) +
+             line_sum_pp<n>(S, D, gy, t, 0);
+      __syncthreads();
+    } else {
+      // a cell on a hanging interface: the cell operator applied to its unit vectors
+      for (int j = 0; j < n3; ++j) {
+        u[t] = t == j ? 1.0 : 0.0;
+        __syncthreads();
         for (int d = 0; d < 3; ++d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], false, t);
-      apply_cell<n>(a, size, u, Tv, Tx, Ty, Tz, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
-      if (hang)
+        apply_cell<n>(a, size, u, Tv, Tx, Ty, Tz, val, gx, gy, gz, t1, t2, s1, s2, s3, t);
         for (int d = 2; d >= 0; --d) hang_dir<n>(u, tmp, code, d, a.I[(code >> d) & 1], true, t);
-      if (t == j) mine = u[t];
-      __syncthreads();
+        if (t == j) mine = u[t];
+        __syncthreads();
+      }
     }
     if (!a.mask[dof]) atomicAdd(a.dst + dof, mine);
     __syncthreads();
@@ -382,6 +472,7 @@ struct mpdg_amr {
   // Krylov / step workspace (n_dofs each) and a device scalar for the sums
   double *w[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   double *d_sum = nullptr;
+  double *tf = nullptr;  // tangent fields of the solve's linearisation point, [cell][4][n^3]
 };
 
 namespace {
@@ -408,6 +499,8 @@ void release(mpdg_amr *h)
   }
   if (h->d_sum) cudaFree(h->d_sum);
   h->d_sum = nullptr;
+  if (h->tf) cudaFree(h->tf);
+  h->tf = nullptr;
 }
 
 // the host description: active cells, node numbering, hanging nodes, DoFs, cell data
@@ -850,11 +943,37 @@ int sync_status()
 
 int vgrid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
 
-int vmult_impl(mpdg_amr *h, double *dst, const double *src, const double *T_lin)
+// the tangent fields of T_lin into h->tf (for the applications of one solve)
+int tfields_impl(mpdg_amr *h, const double *T_lin)
+{
+  const int64_t nf = h->n_cells * 4 * (int64_t)h->n * h->n * h->n;
+  if (!h->tf) {
+    const cudaError_t e = cudaMalloc(&h->tf, sizeof(double) * (size_t)nf);
+    if (e != cudaSuccess) {
+      h->tf = nullptr;
+      return fail(MPDG_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+  }
+  AmrArgs a = make_args(h, T_lin);
+  const int grid = (int)std::min<int64_t>(h->n_cells, 148 * 16);
+  switch (h->n) {
+    case 2: k_amr_tfields<2><<<grid, 8>>>(a, h->tf); break;
+    case 3: k_amr_tfields<3><<<grid, 27>>>(a, h->tf); break;
+    case 4: k_amr_tfields<4><<<grid, 64>>>(a, h->tf); break;
+    case 5: k_amr_tfields<5><<<grid, 125>>>(a, h->tf); break;
+    default: return fail(MPDG_ERR_INVALID_ARGUMENT, "degree");
+  }
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MPDG_OK : fail(MPDG_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int vmult_impl(mpdg_amr *h, double *dst, const double *src, const double *T_lin,
+               const double *tf = nullptr)
 {
   AmrArgs a = make_args(h, T_lin);
   a.src = src;
   a.dst = dst;
+  a.tf = a.tangent ? tf : nullptr;
   if (!a.tangent) a.Tl = src;
   k_amr_zero<<<vgrid(h->n_dofs), 256>>>(h->n_dofs, dst);
   return launch_cells(h, CELL_VMULT, a);
@@ -927,8 +1046,14 @@ int cg_impl(mpdg_amr *h, double *x, const double *b, const double *inv, const do
   const double tol = std::max(abs_tol, rel_tol * std::sqrt(rr));
   *iterations = 0;
   if (std::sqrt(rr) <= tol) return MPDG_OK;
+  // T_lin is fixed during the solve: its values and gradients at the q-points once
+  const double *tf = nullptr;
+  if (T_lin && h->mat.law == MPDG_LAW_LINEAR_K && h->mat.k1 != 0.0) {
+    TRY_AMR(tfields_impl(h, T_lin));
+    tf = h->tf;
+  }
   for (int it = 1; it <= max_it; ++it) {
-    TRY_AMR(vmult_impl(h, Ap, p, T_lin));
+    TRY_AMR(vmult_impl(h, Ap, p, T_lin, tf));
     double pap = 0.0;
     TRY_AMR(dot(h, p, Ap, &pap));
     if (!(pap > 0.0)) return fail(MPDG_ERR_BREAKDOWN, "CG breakdown: p.Ap <= 0");

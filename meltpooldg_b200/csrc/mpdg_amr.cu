@@ -27,6 +27,8 @@
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "../../include/mpdg_heat.h"
@@ -904,23 +906,53 @@ AmrArgs make_args(const mpdg_amr *h, const double *T_lin)
 
 enum { CELL_VMULT = 0, CELL_DIAG = 1, CELL_RHS = 2 };
 
+// a persistent grid of as many CTAs (one cell each at a time) as the SMs hold at once
+template <typename K> int resident_grid(K kernel, int threads, int64_t n_cells)
+{
+  static std::mutex mu;
+  static std::map<const void *, int> per_sm_of;  // per kernel
+  static int sms = 0;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (sms == 0) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    auto it = per_sm_of.find(reinterpret_cast<const void *>(kernel));
+    if (it == per_sm_of.end()) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 16;
+      per_sm_of[reinterpret_cast<const void *>(kernel)] = per_sm;
+    } else {
+      per_sm = it->second;
+    }
+  }
+  return (int)std::min<int64_t>(n_cells, (int64_t)per_sm * sms);
+}
+
 template <int n>
-void launch_n(int kind, const AmrArgs &a, int grid)
+void launch_n(int kind, const AmrArgs &a)
 {
   constexpr int n3 = n * n * n;
-  if (kind == CELL_VMULT) k_amr_vmult<n><<<grid, n3>>>(a);
-  else if (kind == CELL_DIAG) k_amr_diag<n><<<grid, n3>>>(a);
-  else k_amr_rhs<n><<<grid, n3>>>(a);
+  if (kind == CELL_VMULT) {
+    k_amr_vmult<n><<<resident_grid(k_amr_vmult<n>, n3, a.n_cells), n3>>>(a);
+  } else if (kind == CELL_DIAG) {
+    k_amr_diag<n><<<resident_grid(k_amr_diag<n>, n3, a.n_cells), n3>>>(a);
+  } else {
+    k_amr_rhs<n><<<resident_grid(k_amr_rhs<n>, n3, a.n_cells), n3>>>(a);
+  }
 }
 
 int launch_cells(const mpdg_amr *h, int kind, const AmrArgs &a)
 {
-  const int grid = (int)std::min<int64_t>(h->n_cells, 148 * 16);
   switch (h->n) {
-    case 2: launch_n<2>(kind, a, grid); break;
-    case 3: launch_n<3>(kind, a, grid); break;
-    case 4: launch_n<4>(kind, a, grid); break;
-    case 5: launch_n<5>(kind, a, grid); break;
+    case 2: launch_n<2>(kind, a); break;
+    case 3: launch_n<3>(kind, a); break;
+    case 4: launch_n<4>(kind, a); break;
+    case 5: launch_n<5>(kind, a); break;
     default: return fail(MPDG_ERR_INVALID_ARGUMENT, "degree");
   }
   const cudaError_t e = cudaGetLastError();
@@ -955,12 +987,12 @@ int tfields_impl(mpdg_amr *h, const double *T_lin)
     }
   }
   AmrArgs a = make_args(h, T_lin);
-  const int grid = (int)std::min<int64_t>(h->n_cells, 148 * 16);
+  const int64_t nc = h->n_cells;
   switch (h->n) {
-    case 2: k_amr_tfields<2><<<grid, 8>>>(a, h->tf); break;
-    case 3: k_amr_tfields<3><<<grid, 27>>>(a, h->tf); break;
-    case 4: k_amr_tfields<4><<<grid, 64>>>(a, h->tf); break;
-    case 5: k_amr_tfields<5><<<grid, 125>>>(a, h->tf); break;
+    case 2: k_amr_tfields<2><<<resident_grid(k_amr_tfields<2>, 8, nc), 8>>>(a, h->tf); break;
+    case 3: k_amr_tfields<3><<<resident_grid(k_amr_tfields<3>, 27, nc), 27>>>(a, h->tf); break;
+    case 4: k_amr_tfields<4><<<resident_grid(k_amr_tfields<4>, 64, nc), 64>>>(a, h->tf); break;
+    case 5: k_amr_tfields<5><<<resident_grid(k_amr_tfields<5>, 125, nc), 125>>>(a, h->tf); break;
     default: return fail(MPDG_ERR_INVALID_ARGUMENT, "degree");
   }
   const cudaError_t e = cudaGetLastError();

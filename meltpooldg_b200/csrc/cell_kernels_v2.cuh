@@ -242,7 +242,10 @@ __device__ __forceinline__ void gather_plane(const MeshDims &d, int64_t base, co
   }
 }
 
-template <int n, typename T, int GEO, int LAW>
+// GPRE (deformed meshes, where the 7 x n^2 factors of a thread's points fit the registers): the
+// per-point geometry is loaded when the cell group starts, so its loads overlap the gathers and
+// the evaluation sweeps instead of stalling the quadrature-point loop
+template <int n, typename T, int GEO, int LAW, bool GPRE = false>
 __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
 {
   constexpr int CW = v2_cells_per_warp<n>();
@@ -281,6 +284,17 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
     // both gathers first so their latencies overlap
     T Pu[n][n];
     gather_plane<n>(d, base, pm, true, a.src, Pu, active);
+    T gpre[GPRE ? 7 : 1][GPRE ? n : 1][GPRE ? n : 1];
+    if constexpr (GPRE && GEO == 1) {
+      constexpr int npt = n * n * n;
+      const T *gb = a.g.q + cc * 7 * npt + t;
+#pragma unroll
+      for (int f = 0; f < 7; ++f)
+#pragma unroll
+        for (int k = 0; k < n; ++k)
+#pragma unroll
+          for (int j = 0; j < n; ++j) gpre[f][k][j] = active ? __ldg(gb + f * npt + n * (j + n * k)) : T(0);
+    }
     T Pt[n][n];
     if (TLIN) gather_plane<n>(d, base, pm, false, a.Tl, Pt, active);
 
@@ -396,7 +410,13 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
 #pragma unroll
       for (int j = 0; j < n; ++j) {
         T jxw, G[6];
-        geo_at<n, GEO>(a.g, cc, t, j, k, jxw, G);
+        if constexpr (GPRE && GEO == 1) {
+          jxw = gpre[0][k][j];
+#pragma unroll
+          for (int f = 0; f < 6; ++f) G[f] = gpre[1 + f][k][j];
+        } else {
+          geo_at<n, GEO>(a.g, cc, t, j, k, jxw, G);
+        }
         const T uu = U[k][j];
         T kk, cval;
         T f0, f1, f2;

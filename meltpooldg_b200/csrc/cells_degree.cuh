@@ -47,6 +47,25 @@ static inline bool fp32_packed()
   return on != 0;
 }
 
+// Register-resident operator on deformed meshes, p <= 2: a thread's 7 x n^2 geometry factors
+// preloaded when the cell group starts or loaded in the quadrature-point loop. Mode 1 (the
+// default) preloads where it measured faster: the k(T) tangents (FP64 1.4-1.5x, FP32
+// 1.4-2.4x at p = 1, 2) and every FP64 law at p = 1 (1.12x); the constant-coefficient and
+// Picard FP32 operators keep the loop loads (the preload measured up to 15 % slower there).
+// MPDG_GEO_PRELOAD_V2=0 never preloads, =1 everywhere eligible.
+static inline int geo_preload_v2()
+{
+  static const int mode = [] {
+    const char *e = getenv("MPDG_GEO_PRELOAD_V2");
+    return !e ? 1 : (e[0] == '0' ? 0 : (e[0] == '1' ? 2 : 1));
+  }();
+  return mode;
+}
+template <int n, typename T, int LAW> constexpr bool geo_preload_v2_default()
+{
+  return (sizeof(T) == 8 && n == 2) || LAW == 1 || LAW == 2 || LAW == 7;
+}
+
 // Line-per-thread operator on deformed meshes: the batch's per-point geometry
 // preloaded into registers (default) or loaded in the quadrature-point loop
 // (MPDG_GEO_PRELOAD=0); both compute the same operator.
@@ -101,6 +120,19 @@ struct DegreeOps {
       }
     }
     if constexpr (use_v2<T, LAW>()) {
+      if constexpr (GEO == 1 && n <= 3) {
+        const int mode = geo_preload_v2();
+        if (mode == 2 || (mode == 1 && geo_preload_v2_default<n, T, LAW>())) {
+          static int cachep = 0;
+          auto kp = k_vmult2<n, T, GEO, LAW, true>;
+          const size_t smemp = v2_smem<n, T, LAW>();
+          const int64_t ng = (a.n_cells + v2_cells_per_warp<n>() - 1) / v2_cells_per_warp<n>();
+          const int gp = persistent_grid(kp, 32 * kV2Warps, smemp, (ng + kV2Warps - 1) / kV2Warps,
+                                         sm, &cachep);
+          kp<<<gp, 32 * kV2Warps, smemp, s>>>(a);
+          return cudaGetLastError();
+        }
+      }
       static int cache2 = 0;
       auto k2 = k_vmult2<n, T, GEO, LAW>;
       const size_t smem2 = v2_smem<n, T, LAW>();

@@ -143,6 +143,24 @@ def test_line_per_thread_tangent_fields_match_oracle():
     assert " passed" in r.stdout
 
 
+def test_register_kernel_geometry_preload_matches_oracle():
+    """The register-resident operator on deformed meshes with its per-point geometry preloaded
+    when the cell group starts for every eligible case (MPDG_GEO_PRELOAD_V2=1: FP32 and FP64,
+    p <= 2, every law; the default preloads for FP64 p = 1 and the FP64 k(T) tangents at p = 2),
+    on the same cases, in a child process because the choice is read once per process."""
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ, MPDG_GEO_PRELOAD_V2="1")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p",
+                        "no:cacheprovider", __file__, "-k",
+                        "(vmult_diag_rhs_match_oracle or fp32_operator_cell_pairs) and 0.2 and "
+                        "(1 or 2)"],
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert " passed" in r.stdout
+
+
 def test_picard_operator_from_nodal_linearisation_point_matches_oracle():
     """The FP32 Picard operator with k(T_lin(q)) interpolated in the kernel from the gathered
     T_lin (MPDG_PICARD_NODAL=1) on the cell-pair meshes, and the benchmark step at 48^3 with

@@ -471,13 +471,21 @@ def run_mine(args):
     picard_dominant = cnt["vmult32_ms"] >= cnt["vmult64_ms"]
     if picard_dominant:
         # FP32 Picard operator of the preconditioner: src + dst + conductivity per q-point
+        # (the operand in cell rows when the step's smoother kept its iterate there: the
+        # algorithmic bytes stay those of the lexicographic vectors)
         kname = ("k_vmult_picard_tc<4>" if op.picard_tensor_cores
-                 else "k_vmult2<4,float,affine,conductivity_field>")
+                 else "k_vmult2<4,float,affine,conductivity_field,cell_rows>"
+                 if op.picard_cell_rows else "k_vmult2<4,float,affine,conductivity_field>")
         kms = cnt["vmult32_ms"]
         alg_bytes = 2 * 4 * N + 4 * nq
         xs = torch.rand(N, dtype=torch.float32, device=dev)
         ys = torch.empty_like(xs)
-        run = lambda: op.vmult_picard_f32(ys, xs)
+        if op.picard_cell_rows:
+            rows = torch.empty(op.cell_rows_size(), dtype=torch.float32, device=dev)
+            op.to_cell_rows_f32(rows, xs)
+            run = lambda: op.vmult_picard_f32_rows(ys, rows)
+        else:
+            run = lambda: op.vmult_picard_f32(ys, xs)
     else:
         kname = "k_vmult2<4,double,affine,linear_k_tangent_fields>"
         kms = cnt["vmult64_ms"]

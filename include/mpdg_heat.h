@@ -227,6 +227,23 @@ int mpdg_heat_vmult_f32(mpdg_heat *h, float *dst, const float *src);
  * k(T_lin) frozen at the quadrature points. Boundary-face terms as in
  * mpdg_heat_vmult_f32. MPDG_ERR_INVALID_ARGUMENT for the other laws. */
 int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float *src);
+/* The cell-row layout of an FP32 nodal vector on an FE_Q(3) mesh, in which the multigrid's fine
+ * level keeps its Chebyshev iterate so that the FP32 Picard operator gathers a cell's x-row of
+ * 4 nodes with one aligned 16-byte load (no reference counterpart): x-row r = j + nd1 k of the
+ * nodal grid holds 4 slots per cell column c, slot s = node 3c + s, so the node shared by
+ * columns c - 1 and c is stored in both. *n_floats = 4 m0 nd1 nd2 (m0 cells and nd0 = 3 m0 + 1
+ * nodes per x-row). MPDG_ERR_NOT_SUPPORTED for the other degrees. */
+int mpdg_heat_cell_rows_size(const mpdg_heat *h, int64_t *n_floats);
+/* rows = the cell-row copy of the lexicographic FP32 vector lex (device pointers). */
+int mpdg_heat_to_cell_rows_f32(mpdg_heat *h, float *rows, const float *lex);
+/* dst = the FP32 Picard operator of mpdg_heat_vmult_f32_picard applied to an operand given in
+ * cell rows: the CUDA-core kernel of the multigrid's fine level. FE_Q(3) without Robin/Neumann
+ * faces; not with the tensor-core or nodal-conductivity forms (MPDG_ERR_INVALID_ARGUMENT). */
+int mpdg_heat_vmult_f32_picard_rows(mpdg_heat *h, float *dst, const float *src_rows);
+/* 1 when the handle's last FP64 CG with the FP32 Chebyshev or multigrid preconditioner kept the
+ * fine level's Chebyshev iterate in cell rows (opt-in: the environment sets MPDG_PICARD_ROWS=1;
+ * FE_Q(3), Picard operator on the CUDA cores, no Robin/Neumann faces), else 0. */
+int mpdg_heat_picard_cell_rows(const mpdg_heat *h);
 /* The FP32 Picard operator (mpdg_heat_vmult_f32_picard and the multigrid fine level) on the
  * tensor cores: tcgen05 TF32 GEMMs over bricks of 128 cells, operands rounded to TF32
  * (relative error ~5e-4 against the oracle), FP32 accumulation. Exists for uniform box meshes

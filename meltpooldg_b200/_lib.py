@@ -117,6 +117,10 @@ _SIGS = {
     "mpdg_heat_vmult": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult_f32": (C.c_int, [_H, _D, _D]),
     "mpdg_heat_vmult_f32_picard": (C.c_int, [_H, _D, _D]),
+    "mpdg_heat_cell_rows_size": (C.c_int, [_H, C.POINTER(C.c_int64)]),
+    "mpdg_heat_to_cell_rows_f32": (C.c_int, [_H, _D, _D]),
+    "mpdg_heat_vmult_f32_picard_rows": (C.c_int, [_H, _D, _D]),
+    "mpdg_heat_picard_cell_rows": (C.c_int, [_H]),
     "mpdg_heat_inverse_diagonal_f32_picard": (C.c_int, [_H, _D]),
     "mpdg_heat_set_picard_tensor_cores": (C.c_int, [_H, C.c_int]),
     "mpdg_heat_picard_tensor_cores": (C.c_int, [_H]),

@@ -245,9 +245,15 @@ __device__ __forceinline__ void gather_plane(const MeshDims &d, int64_t base, co
 // GPRE (deformed meshes, where the 7 x n^2 factors of a thread's points fit the registers): the
 // per-point geometry is loaded when the cell group starts, so its loads overlap the gathers and
 // the evaluation sweeps instead of stalling the quadrature-point loop
-template <int n, typename T, int GEO, int LAW, bool GPRE = false>
+// ROWS (FP32 Picard operator at p = 3): the operand is in the cell-row layout, in which the n = 4
+// nodes of a cell's x-row are one aligned float4 and a node shared by x-neighbours is stored in
+// both cells' rows (cell_row_index below); a plane is then gathered with 4 vector loads instead
+// of 16 scalar ones. The result is scattered into the lexicographic dst as usual; no src.dst
+// partial (the host passes FIN_NONE).
+template <int n, typename T, int GEO, int LAW, bool GPRE = false, bool ROWS = false>
 __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
 {
+  static_assert(!ROWS || (n == 4 && sizeof(T) == 4 && LAW == 3), "cell rows: FP32 Picard, p = 3");
   constexpr int CW = v2_cells_per_warp<n>();
   constexpr int CS = v2_cell_stride<n>();
   constexpr int NCOEF = v2_ncoef<LAW>();
@@ -283,7 +289,21 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
 
     // both gathers first so their latencies overlap
     T Pu[n][n];
-    gather_plane<n>(d, base, pm, true, a.src, Pu, active);
+    if constexpr (ROWS) {
+      const int64_t RS = 4 * (int64_t)d.m[0];
+      const int64_t rb = ((int64_t)K * d.nd[1] + J0) * RS + 4 * cx;
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (active) v = __ldg(reinterpret_cast<const float4 *>(a.src + rb + RS * j));
+        Pu[j][0] = pm.template at<n>(0, j) ? T(0) : v.x;
+        Pu[j][1] = pm.template at<n>(1, j) ? T(0) : v.y;
+        Pu[j][2] = pm.template at<n>(2, j) ? T(0) : v.z;
+        Pu[j][3] = pm.template at<n>(3, j) ? T(0) : v.w;
+      }
+    } else {
+      gather_plane<n>(d, base, pm, true, a.src, Pu, active);
+    }
     T gpre[GPRE ? 7 : 1][GPRE ? n : 1][GPRE ? n : 1];
     if constexpr (GPRE && GEO == 1) {
       constexpr int npt = n * n * n;
@@ -307,9 +327,11 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
         const int ncz = (int)(ncell / ((int64_t)d.m[0] * d.m[1]));
         const int64_t nbase =
           (int64_t)d.nd[0] * (d.p * ncy + (int64_t)d.nd[1] * (d.p * ncz + t)) + d.p * ncx;
-        prefetch_plane<n>(a.src, nbase, d.nd[0]);
+        // (cell rows: the vector gathers measured faster without the operand's and the
+        // conductivity's prefetch)
+        if (!ROWS) prefetch_plane<n>(a.src, nbase, d.nd[0]);
         if (TLIN) prefetch_plane<n>(a.Tl, nbase, d.nd[0]);
-        if (LAW == 3) {
+        if (LAW == 3 && !ROWS) {
           const char *kq = reinterpret_cast<const char *>(a.kq + ncell * (n * n * n));
           for (int off = t * 128; off < n * n * n * 4; off += n * 128)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(kq + off));
@@ -492,7 +514,7 @@ __global__ void __launch_bounds__(32 * kV2Warps) k_vmult2(CellArgs<T> a)
 
     // ---- scatter (constrained rows skipped) and the optional src.dst partial
     if (active) {
-      const bool want_dot = a.fin != FIN_NONE;
+      const bool want_dot = !ROWS && a.fin != FIN_NONE;
 #pragma unroll
       for (int j = 0; j < n; ++j) {
         const int64_t row = base + (int64_t)d.nd[0] * j;

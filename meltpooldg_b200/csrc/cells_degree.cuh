@@ -305,6 +305,26 @@ struct DegreeOps {
   {
     return geo == 0 ? diag_picard_t<0>(a, s, sm) : diag_picard_t<1>(a, s, sm);
   }
+  template <int GEO>
+  static cudaError_t vmult_picard_rows_t(const CellArgs<float> &a, cudaStream_t s, int sm)
+  {
+    static int cache = 0;
+    auto k = k_vmult2<n, float, GEO, 3, false, true>;
+    const size_t smem = v2_smem<n, float, 3>();
+    const int64_t ng = (a.n_cells + v2_cells_per_warp<n>() - 1) / v2_cells_per_warp<n>();
+    const int g = persistent_grid(k, 32 * kV2Warps, smem, (ng + kV2Warps - 1) / kV2Warps, sm, &cache);
+    k<<<g, 32 * kV2Warps, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t vmult_picard_rows(const CellArgs<float> &a, int geo, cudaStream_t s, int sm)
+  {
+    if constexpr (n == 4) {
+      return geo == 0 ? vmult_picard_rows_t<0>(a, s, sm) : vmult_picard_rows_t<1>(a, s, sm);
+    } else {
+      (void)a, (void)geo, (void)s, (void)sm;
+      return cudaErrorNotSupported;
+    }
+  }
   static cudaError_t vmult_picard_tc(const CellArgs<float> &a, const float *gmat, int *err,
                                      cudaStream_t s, int sm)
   {
@@ -397,7 +417,10 @@ struct DegreeOps {
       t.conductivity_q = &conductivity_q;
       t.diag_picard = &diag_picard;
     }
-    if constexpr (n == 4) t.vmult_picard_tc = &vmult_picard_tc;
+    if constexpr (n == 4) {
+      t.vmult_picard_tc = &vmult_picard_tc;
+      t.vmult_picard_rows = &vmult_picard_rows;
+    }
     return t;
   }
 };

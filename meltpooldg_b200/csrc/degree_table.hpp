@@ -36,6 +36,9 @@ struct DegreeTable {
   // the 128 KB of optc::build_gmat in device memory, err: raised on a timed-out wait)
   cudaError_t (*vmult_picard_tc)(const CellArgs<float> &, const float *gmat, int *err,
                                  cudaStream_t, int sm) = nullptr;
+  // a.dst += the FP32 Picard operator with a.src in the cell-row layout (FE_Q(3) only)
+  cudaError_t (*vmult_picard_rows)(const CellArgs<float> &, int geo, cudaStream_t,
+                                   int sm) = nullptr;
 };
 
 DegreeTable degree_table_2();

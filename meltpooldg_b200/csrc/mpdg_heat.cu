@@ -152,6 +152,10 @@ struct mpdg_heat {
   double *r = nullptr, *pv = nullptr, *Ap = nullptr, *z = nullptr, *w1 = nullptr, *w2 = nullptr,
          *w3 = nullptr;
   float *r32 = nullptr, *x32 = nullptr, *d32 = nullptr, *Ax32 = nullptr;
+  // the fine level's Chebyshev iterate in the cell-row layout (instead of x32) during a mixed
+  // solve whose preconditioner applies the FP32 Picard operator of FE_Q(3) (rows_on)
+  float *x32_rows = nullptr;
+  bool rows_on = false;
   double *host_T = nullptr, *host_To = nullptr, *host_q = nullptr;  // device buffers for *_host
   // host-vector verbs: device mirrors of the linearisation point and of the verb's vectors,
   // and the caller's DoF numbering (lex[i] = lexicographic index of the caller's DoF i)
@@ -653,13 +657,65 @@ __global__ void k_cg_update_p(int64_t N, const double *__restrict__ r, double *p
   }
 }
 
+// ---- the cell-row layout of the fine level's FP32 iterate -------------------
+// FE_Q(3): x-row r of the nodal grid (r = j + nd1 k) holds 4 slots per cell column c, slot s
+// holding node 3c + s, so that a cell's 4 x-nodes are one aligned float4 (the operator's
+// gather, k_vmult2 with ROWS); node 3c, shared by columns c - 1 and c, is in both (slot 3 of
+// c - 1 and slot 0 of c). rows == nullptr: the iterate is the lexicographic x32. Node indices
+// are below 2^32 (checked where the layout is enabled).
+struct CellRows {
+  float *rows = nullptr;
+  unsigned nd0 = 0;  // nodes per x-row, 3 m0 + 1
+  unsigned rs = 0;   // slots per x-row, 4 m0
+};
+
+__device__ __forceinline__ float *cell_row_of(const CellRows &c, int64_t i, unsigned &ix)
+{
+  const unsigned ii = (unsigned)i, r = ii / c.nd0;
+  ix = ii - r * c.nd0;
+  return c.rows + (int64_t)r * c.rs;
+}
+// x[i] into every slot of node i
+__device__ __forceinline__ void cell_rows_store(const CellRows &c, int64_t i, float v)
+{
+  unsigned ix;
+  float *row = cell_row_of(c, i, ix);
+  const unsigned q = ix / 3u, s = ix - 3u * q;
+  if (ix + 1u < c.nd0) row[ix + q] = v;  // slot s of column q (the row's last node has none)
+  if (s == 0u && q > 0u) row[ix + q - 1u] = v;  // slot 3 of column q - 1
+}
+__device__ __forceinline__ float cell_rows_load(const CellRows &c, int64_t i)
+{
+  unsigned ix;
+  const float *row = cell_row_of(c, i, ix);
+  const unsigned q = ix / 3u;
+  return row[ix + 1u < c.nd0 ? ix + q : ix + q - 1u];
+}
+
+// the handle's fine-level iterate: its cell rows while rows_on, else the lexicographic x32
+static CellRows cell_rows_of(const mpdg_heat *h)
+{
+  CellRows c;
+  if (h->rows_on) {
+    c.rows = h->x32_rows;
+    c.nd0 = (unsigned)h->dims.nd[0];
+    c.rs = 4u * (unsigned)h->dims.m[0];
+  }
+  return c;
+}
+static int64_t cell_rows_size(const mpdg_heat *h)
+{
+  return (int64_t)4 * h->dims.m[0] * h->dims.nd[1] * h->dims.nd[2];
+}
+
 // ---- FP64 CG with the FP32 Chebyshev-Jacobi preconditioner ------------------
 // init: r = b - Ax ; rr ; r32 = r ; x32 = D32 r32 / theta ; d32 = x32 ; Ap = 0 ; Ax32 = 0
+// (x32 into xr's cell rows instead when xr.rows is set)
 __global__ void k_cgm_init(int64_t N, const double *__restrict__ b, double *r, double *Ap,
                            float *r32, float *x32, float *d32, float *Ax32,
                            const float *__restrict__ D32, float inv_theta, SolverState *st,
                            double *partials, unsigned *counter, double rel, double abs_tol,
-                           double ref_norm, int max_it)
+                           double ref_norm, int max_it, CellRows xr)
 {
   double v[1] = {0.0};
   GRID_STRIDE(i, N)
@@ -670,7 +726,10 @@ __global__ void k_cgm_init(int64_t N, const double *__restrict__ b, double *r, d
     const float rf = (float)ri;
     r32[i] = rf;
     const float xf = D32[i] * rf * inv_theta;
-    x32[i] = xf;
+    if (xr.rows)
+      cell_rows_store(xr, i, xf);
+    else
+      x32[i] = xf;
     d32[i] = xf;
     Ax32[i] = 0.0f;
     v[0] += ri * ri;
@@ -701,16 +760,20 @@ __global__ void k_cgm_init(int64_t N, const double *__restrict__ b, double *r, d
 }
 
 // Chebyshev step: d = c1 d + c2 D32 (r32 - Ax32) ; x32 += d ; Ax32 = 0
+// (x in xr's cell rows instead of x32 when xr.rows is set)
 __global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32, float *d32,
                             float *Ax32, const float *__restrict__ D32, float c1, float c2,
-                            const SolverState *st)
+                            const SolverState *st, CellRows xr)
 {
   if (st->done) return;
   GRID_STRIDE(i, N)
   {
     const float dn = c1 * d32[i] + c2 * D32[i] * (r32[i] - Ax32[i]);
     d32[i] = dn;
-    x32[i] += dn;
+    if (xr.rows)
+      cell_rows_store(xr, i, cell_rows_load(xr, i) + dn);
+    else
+      x32[i] += dn;
     Ax32[i] = 0.0f;
   }
 }
@@ -721,14 +784,14 @@ __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const floa
                             const float *__restrict__ d32, float *Ax32,
                             const float *__restrict__ D32, float c1, float c2,
                             const double *__restrict__ r, const double *__restrict__ Ap, double *z,
-                            SolverState *st, double *partials, unsigned *counter)
+                            SolverState *st, double *partials, unsigned *counter, CellRows xr)
 {
   if (st->done) return;
   double v[2] = {0.0, 0.0};
   GRID_STRIDE(i, N)
   {
     const float dn = c1 * d32[i] + c2 * D32[i] * (r32[i] - Ax32[i]);
-    const double zi = (double)(x32[i] + dn);
+    const double zi = (double)((xr.rows ? cell_rows_load(xr, i) : x32[i]) + dn);
     Ax32[i] = 0.0f;
     z[i] = zi;
     v[0] += zi * r[i];
@@ -751,7 +814,7 @@ __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const floa
 __global__ void k_cgm_update_xr(int64_t N, double *x, double *r, const double *__restrict__ p,
                                 const double *__restrict__ Ap, float *r32, float *x32, float *d32,
                                 const float *__restrict__ D32, float inv_theta, SolverState *st,
-                                double *partials, unsigned *counter)
+                                double *partials, unsigned *counter, CellRows xr)
 {
   if (st->done) return;
   const double alpha = st->alpha;
@@ -764,7 +827,10 @@ __global__ void k_cgm_update_xr(int64_t N, double *x, double *r, const double *_
     const float rf = (float)ri;
     r32[i] = rf;
     const float xf = D32[i] * rf * inv_theta;
-    x32[i] = xf;
+    if (xr.rows)
+      cell_rows_store(xr, i, xf);
+    else
+      x32[i] = xf;
     d32[i] = xf;
     v[0] += ri * ri;
   }
@@ -858,10 +924,11 @@ __global__ void k_restrict_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
 
 // interpolation along one axis: out[.., I, ..] = (1 - xi_a) in[.., V, ..] + xi_a in[.., V + 1, ..]
 // with V = I / r, a = I % r; add: accumulate into out; masked rows are left untouched;
-// zero (optional): an array of out's shape set to zero on the way
+// zero (optional): an array of out's shape set to zero on the way; out in xr's cell rows
+// instead when xr.rows is set
 __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
                                const float *__restrict__ in, float *out, int add, MeshDims md,
-                               int masked, float *zero, const SolverState *st)
+                               int masked, float *zero, const SolverState *st, CellRows xr)
 {
   if (st && st->done) return;
   TRANSFER_LOOP(i, dout)
@@ -870,7 +937,12 @@ __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
     transfer_index(dout, i, o);
     if (zero) zero[i] = 0.f;
     if (masked && constrained(md, o[0], o[1], o[2])) {
-      if (!add) out[i] = 0.f;
+      if (!add) {
+        if (xr.rows)
+          cell_rows_store(xr, i, 0.f);
+        else
+          out[i] = 0.f;
+      }
       continue;
     }
     const int I = o[axis], V = I / t.r, a = I - V * t.r;
@@ -882,7 +954,10 @@ __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
       v = (1.f - t.xi[a]) * v +
           t.xi[a] * in[(unsigned)p[0] + (unsigned)di.n[0] * ((unsigned)p[1] + (unsigned)di.n[1] * (unsigned)p[2])];
     }
-    out[i] = add ? out[i] + v : v;
+    if (xr.rows)
+      cell_rows_store(xr, i, add ? cell_rows_load(xr, i) + v : v);
+    else
+      out[i] = add ? out[i] + v : v;
   }
 }
 
@@ -1524,8 +1599,10 @@ static int ensure_picard_tc(mpdg_heat *h)
   return MPDG_OK;
 }
 
+// src_rows (optional): the operand in the cell-row layout (FP32 Picard operator of FE_Q(3),
+// no boundary-face terms); src is then not read
 static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *st,
-                      bool picard = false)
+                      bool picard = false, const float *src_rows = nullptr)
 {
   TRY(ensure_dt(h));
   TRY(ensure_lin(h));
@@ -1560,12 +1637,20 @@ static int op_apply_f(mpdg_heat *h, float *dst, const float *src, SolverState *s
     cudaEventRecord(e0, h->stream);
   }
   const bool tc = law == 3 && picard_tc_on(h);
+  if (src_rows && (law != 3 || tc || any_faces(h) || !h->tab.vmult_picard_rows))
+    return fail(MPDG_ERR_INVALID_ARGUMENT,
+                "cell-row operand: FP32 Picard operator of FE_Q(3) without boundary faces only");
   if (tc) TRY(ensure_picard_tc(h));
   if (any_faces(h)) TRY(launch_faces<float>(h, 0, dst, src, h->T_lin_f, nullptr, st));
-  if (tc)
+  if (src_rows) {
+    a.src = src_rows;
+    a.fin = FIN_NONE;
+    CU(h->tab.vmult_picard_rows(a, h->geo, h->stream, h->sm_count));
+  } else if (tc) {
     CU(h->tab.vmult_picard_tc(a, h->gmat_tc, h->tc_err_map, h->stream, h->sm_count));
-  else
+  } else {
     CU(h->tab.vmult_f(a, h->geo, law, h->stream, h->sm_count));
+  }
   if (h->timing) {
     cudaEventRecord(e1, h->stream);
     h->ev32.push_back({e0, e1});
@@ -2015,8 +2100,10 @@ static int mg_restrict(mpdg_heat *h, int l, const float *fine_Ax, const float *f
   return MPDG_OK;
 }
 
-// fine += P coarse (constrained rows untouched); zero_fine (fine-shaped) is set to zero
-static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine, float *zero_fine)
+// fine += P coarse (constrained rows untouched); zero_fine (fine-shaped) is set to zero;
+// fine in fine_rows' cell rows instead when fine_rows.rows is set
+static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine, float *zero_fine,
+                          CellRows fine_rows = CellRows())
 {
   const MGLevel &f = h->mg[l], &c = h->mg[l + 1];
   const Dims3 F = nodal_dims(f.h), C = nodal_dims(c.h);
@@ -2025,11 +2112,14 @@ static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine,
   t.r = f.ratio;
   for (int a = 0; a < 8; ++a) t.xi[a] = f.xi[a];
   k_prolong_axis<<<vgrid(h, E2.size()), VT, 0, h->stream>>>(2, C, E2, t, coarse, h->mg_t2, 0,
-                                                            f.h->dims, 0, nullptr, h->st);
+                                                            f.h->dims, 0, nullptr, h->st,
+                                                            CellRows());
   k_prolong_axis<<<vgrid(h, E1.size()), VT, 0, h->stream>>>(1, E2, E1, t, h->mg_t2, h->mg_t1, 0,
-                                                            f.h->dims, 0, nullptr, h->st);
+                                                            f.h->dims, 0, nullptr, h->st,
+                                                            CellRows());
   k_prolong_axis<<<vgrid(h, F.size()), VT, 0, h->stream>>>(0, E1, F, t, h->mg_t1, fine, 1,
-                                                           f.h->dims, 1, zero_fine, h->st);
+                                                           f.h->dims, 1, zero_fine, h->st,
+                                                           fine_rows);
   h->launches += 3;
   CU(cudaGetLastError());
   return MPDG_OK;
@@ -2037,16 +2127,17 @@ static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine,
 
 __global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32, float *d32,
                             float *Ax32, const float *__restrict__ D32, float c1, float c2,
-                            const SolverState *st);
+                            const SolverState *st, CellRows xr);
 __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const float *__restrict__ x32,
                             const float *__restrict__ d32, float *Ax32,
                             const float *__restrict__ D32, float c1, float c2,
                             const double *__restrict__ r, const double *__restrict__ Ap, double *z,
-                            SolverState *st, double *partials, unsigned *counter);
+                            SolverState *st, double *partials, unsigned *counter, CellRows xr);
 
 // one V-cycle on the FP32 residual in level 0's b (= r32), whose first smoothing step
 // (x = d = D b / theta_0) the caller has taken; ends with z = x (FP64) and the dots of
-// the flexible CG, like the last Chebyshev step
+// the flexible CG, like the last Chebyshev step. Level 0's iterate is in the handle's cell
+// rows while rows_on (the caller's first step wrote it there).
 static int mg_vcycle(mpdg_heat *h, bool picard)
 {
   const int L = (int)h->mg.size();
@@ -2056,21 +2147,22 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
     mpdg_heat *c = v.h;
     const int64_t N = c->n_dofs;
     const int g = vgrid(c, N);
+    const CellRows xr = l == 0 ? cell_rows_of(h) : CellRows();
     if (l > 0) {
       k_cheb_init<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, c->inv_diag_f, (float)(1.0 / v.theta),
                                            st);
       ++h->launches;
     }
     for (int j = 1; j <= v.pre; ++j) {
-      TRY(op_apply_f(c, v.Ax, v.x, st, picard));
+      TRY(op_apply_f(c, v.Ax, v.x, st, picard, xr.rows));
       k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, v.c1[j],
-                                           v.c2[j], st);
+                                           v.c2[j], st, xr);
       ++h->launches;
     }
     if (l == L - 1) break;
     // residual b - A x restricted (formed inside the first pass); Ax is reset to zero by
     // the last prolongation pass on the way back up
-    TRY(op_apply_f(c, v.Ax, v.x, st, picard));
+    TRY(op_apply_f(c, v.Ax, v.x, st, picard, xr.rows));
     TRY(mg_restrict(h, l, v.Ax, v.b, h->mg[l + 1].b));
   }
   for (int l = L - 2; l >= 0; --l) {
@@ -2078,17 +2170,19 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
     mpdg_heat *c = v.h;
     const int64_t N = c->n_dofs;
     const int g = vgrid(c, N);
-    TRY(mg_prolong_add(h, l, h->mg[l + 1].x, v.x, v.Ax));
+    const CellRows xr = l == 0 ? cell_rows_of(h) : CellRows();
+    TRY(mg_prolong_add(h, l, h->mg[l + 1].x, v.x, v.Ax, xr));
     // post-smoothing: the Chebyshev recurrence restarted from the corrected iterate
     for (int j = 0; j <= v.post; ++j) {
-      TRY(op_apply_f(c, v.Ax, v.x, st, picard));
+      TRY(op_apply_f(c, v.Ax, v.x, st, picard, xr.rows));
       const float c1 = j == 0 ? 0.f : v.c1[j];
       const float c2 = j == 0 ? (float)(1.0 / v.theta) : v.c2[j];
       if (l == 0 && j == v.post) {
         k_cheb_last<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, h->r,
-                                             h->Ap, h->z, st, h->partials, h->counter);
+                                             h->Ap, h->z, st, h->partials, h->counter, xr);
       } else {
-        k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, st);
+        k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, st,
+                                             xr);
       }
       ++h->launches;
     }
@@ -2186,6 +2280,33 @@ static bool record_body(mpdg_heat *h, F &&body)
   return ok;
 }
 
+// The fine level's Chebyshev iterate in the cell-row layout (opt-in, MPDG_PICARD_ROWS=1), so
+// that the FP32 Picard operator gathers each cell row with one vector load: FE_Q(3), the Picard
+// operator on the CUDA cores (not the nodal-conductivity or tensor-core forms, not the
+// packed-pair kernel), no boundary faces (their kernel reads the lexicographic operand), fewer
+// than 2^32 DoFs. Both layouts compute the same iterates. The operator is faster from cell rows
+// (0.60 against 0.69 ms at 57 M DoFs), but the Chebyshev, update and prolongation kernels that
+// keep the iterate there cost more than that (a benchmark step 86.1 against 84.3 ms).
+static bool picard_rows_env()
+{
+  static const int on = [] {
+    const char *e = getenv("MPDG_PICARD_ROWS");
+    const char *pk = getenv("MPDG_FP32_PACKED");
+    return (e && e[0] == '1' && !(pk && pk[0] == '1')) ? 1 : 0;
+  }();
+  return on != 0;
+}
+static int enable_cell_rows(mpdg_heat *h, bool picard)
+{
+  h->rows_on = false;
+  if (!picard || !picard_rows_env() || !h->tab.vmult_picard_rows || picard_nodal(h) ||
+      picard_tc_on(h) || any_faces(h) || h->n_dofs >= ((int64_t)1 << 32))
+    return MPDG_OK;
+  TRY(dvec(h, &h->x32_rows, cell_rows_size(h)));
+  h->rows_on = true;
+  return MPDG_OK;
+}
+
 // ---------------------------------------------------------------------------
 // FP64 flexible CG with the FP32 Chebyshev-Jacobi or p-multigrid preconditioner
 // ---------------------------------------------------------------------------
@@ -2241,6 +2362,8 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   }
   const float inv_theta = (float)(1.0 / theta);
   const int g = vgrid(h, N);
+  TRY(enable_cell_rows(h, picard));
+  const CellRows xr = cell_rows_of(h);
   int total_it = 0, restarts = 0;
   double res0 = -1.0, true_res = 0.0;
   int graph_state = 0;  // 0 not recorded yet, 1 replaying, -1 direct launches
@@ -2254,7 +2377,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
                                         res0 > 0.0 && prm->tol_reference_norm <= 0.0
                                           ? res0
                                           : prm->tol_reference_norm,
-                                        prm->max_iterations - total_it); ++h->launches;
+                                        prm->max_iterations - total_it, xr); ++h->launches;
     CU(cudaGetLastError());
     TRY(poll(h));
     if (res0 < 0.0) res0 = h->st_host->res0;
@@ -2266,14 +2389,14 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
         return MPDG_OK;
       }
       for (int j = 1; j <= k; ++j) {
-        TRY(op_apply_f(h, h->Ax32, h->x32, h->st, picard));
+        TRY(op_apply_f(h, h->Ax32, h->x32, h->st, picard, xr.rows));
         if (j < k) {
           k_cheb_step<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
-                                               c1[j], c2[j], h->st);
+                                               c1[j], c2[j], h->st, xr);
         } else {
           k_cheb_last<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
                                                c1[j], c2[j], h->r, h->Ap, h->z, h->st,
-                                               h->partials, h->counter);
+                                               h->partials, h->counter, xr);
         }
         ++h->launches;
       }
@@ -2286,7 +2409,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
       TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
       k_cgm_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, h->r32, h->x32, h->d32,
                                                h->inv_diag_f, inv_theta, h->st, h->partials,
-                                               h->counter); ++h->launches;
+                                               h->counter, xr); ++h->launches;
       TRY(precondition());
       return MPDG_OK;
     };
@@ -2409,7 +2532,7 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
     for (int s = 1; s <= kdeg; ++s) {
       TRY(op_apply_f(h, h->Ax32, zj, nullptr, false));
       k_cheb_step<<<gg32, VT, 0, h->stream>>>(N, h->r32, zj, h->d32, h->Ax32, h->inv_diag_f,
-                                              c1[s], c2[s], h->st_run);
+                                              c1[s], c2[s], h->st_run, CellRows());
       ++h->launches;
     }
     k_widen<<<gg32, VT, 0, h->stream>>>(N, zj, h->z);
@@ -3014,6 +3137,55 @@ extern "C" int mpdg_heat_vmult_f32_picard(mpdg_heat *h, float *dst, const float 
   CU(zero_async(h, dst, sizeof(float) * h->n_dofs, h->stream));
   return op_apply_f(h, dst, src, nullptr, true);
 }
+
+__global__ void k_to_cell_rows(int64_t N, CellRows c, const float *__restrict__ lex)
+{
+  GRID_STRIDE(i, N) cell_rows_store(c, i, lex[i]);
+}
+
+extern "C" int mpdg_heat_cell_rows_size(const mpdg_heat *h, int64_t *n_floats)
+{
+  if (!h || !n_floats) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (h->p != 3) return fail(MPDG_ERR_NOT_SUPPORTED, "cell rows: FE_Q(3) only");
+  *n_floats = cell_rows_size(h);
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_to_cell_rows_f32(mpdg_heat *h, float *rows, const float *lex)
+{
+  if (!h || !rows || !lex) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (h->p != 3) return fail(MPDG_ERR_NOT_SUPPORTED, "cell rows: FE_Q(3) only");
+  if (h->n_dofs >= ((int64_t)1 << 32)) return fail(MPDG_ERR_NOT_SUPPORTED, "cell rows: >= 2^32 DoFs");
+  CU(cudaSetDevice(h->device));
+  CellRows c;
+  c.rows = rows;
+  c.nd0 = (unsigned)h->dims.nd[0];
+  c.rs = 4u * (unsigned)h->dims.m[0];
+  k_to_cell_rows<<<vgrid(h, h->n_dofs), VT, 0, h->stream>>>(h->n_dofs, c, lex);
+  ++h->launches;
+  CU(cudaGetLastError());
+  return MPDG_OK;
+}
+
+extern "C" int mpdg_heat_vmult_f32_picard_rows(mpdg_heat *h, float *dst, const float *src_rows)
+{
+  if (!h || !dst || !src_rows) return fail(MPDG_ERR_INVALID_ARGUMENT, "null argument");
+  if (h->law != MPDG_LAW_LINEAR_K || !h->tab.conductivity_q)
+    return fail(MPDG_ERR_INVALID_ARGUMENT, "Picard operator: linear-k law, degree <= 4 only");
+  if (h->p != 3 || !h->tab.vmult_picard_rows)
+    return fail(MPDG_ERR_NOT_SUPPORTED, "cell rows: FE_Q(3) only");
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_lin(h));
+  TRY(dvec(h, &h->kq, h->n_cells * h->npt));
+  CellArgs<double> a = cell_args<double>(h);
+  a.Tl = h->T_lin;
+  CU(h->tab.conductivity_q(a, h->kq, h->law, h->stream, h->sm_count));
+  ++h->launches;
+  CU(zero_async(h, dst, sizeof(float) * h->n_dofs, h->stream));
+  return op_apply_f(h, dst, nullptr, nullptr, true, src_rows);
+}
+
+extern "C" int mpdg_heat_picard_cell_rows(const mpdg_heat *h) { return h && h->rows_on ? 1 : 0; }
 
 extern "C" int mpdg_heat_set_picard_tensor_cores(mpdg_heat *h, int on)
 {

@@ -328,6 +328,32 @@ class HeatDiffuseOperator:
                                                   _ptr(src, torch.float32)))
         return dst
 
+    def cell_rows_size(self) -> int:
+        """Floats of an FP32 vector in the cell-row layout (FE_Q(3)): 4 slots per cell of each
+        x-row of the nodal grid, the node shared by x-neighbouring cells stored in both."""
+        n = C.c_int64(0)
+        check(self._L.mpdg_heat_cell_rows_size(self.h, C.byref(n)))
+        return int(n.value)
+
+    def to_cell_rows_f32(self, rows, lex):
+        """rows = the cell-row copy of the lexicographic FP32 vector lex."""
+        check(self._L.mpdg_heat_to_cell_rows_f32(self.h, _ptr(rows, torch.float32),
+                                                  _ptr(lex, torch.float32)))
+        return rows
+
+    def vmult_picard_f32_rows(self, dst, src_rows):
+        """The FP32 Picard operator applied to an operand in the cell-row layout (the kernel of
+        the multigrid's fine level); dst is lexicographic."""
+        check(self._L.mpdg_heat_vmult_f32_picard_rows(self.h, _ptr(dst, torch.float32),
+                                                       _ptr(src_rows, torch.float32)))
+        return dst
+
+    @property
+    def picard_cell_rows(self) -> bool:
+        """True when the last mixed-precision solve kept the fine level's Chebyshev iterate in
+        the cell-row layout (the Picard operator's vector gather)."""
+        return bool(self._L.mpdg_heat_picard_cell_rows(self.h))
+
     def set_picard_tensor_cores(self, on: bool):
         """Apply the FP32 Picard operator on the tensor cores (TF32 operands) where the kernel
         exists (uniform box, FE_Q(3)); off (the default) keeps the CUDA-core kernel."""

@@ -94,6 +94,11 @@ def check_bench_kernels(o, g, tol64=TOL64):
     tc = g.picard_tensor_cores
     g.set_picard_tensor_cores(False)
     assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), pref) <= TOL32
+    if o.degree == 3:  # the same operator from the cell-row layout (the multigrid fine level)
+        rows = torch.empty(g.cell_rows_size(), dtype=torch.float32, device="cuda")
+        g.to_cell_rows_f32(rows, s32)
+        assert rel(g.vmult_picard_f32_rows(g.new_vector(torch.float32), rows), pref) <= TOL32
+        del rows
     if tc:  # the tensor-core kernel (opt-in) on the benchmark's mesh
         g.set_picard_tensor_cores(True)
         assert rel(g.vmult_picard_f32(g.new_vector(torch.float32), s32), pref) <= TOL_TF32
@@ -158,6 +163,28 @@ def test_benchmark_step_at_48cubed_matches_oracle(precond):
           f"rel L2 {e_l2:.2e}, rel max {e_max:.2e}")
     assert e_l2 <= TOL_STEP and e_max <= TOL_STEP
     assert 0 < st.linear_iterations < its_ref
+    # the fine level's iterate in cell rows exactly when the opt-in asks for it
+    assert g.picard_cell_rows == (__import__("os").environ.get("MPDG_PICARD_ROWS") == "1")
+
+
+def test_benchmark_step_with_cell_row_smoother_iterate():
+    """The 48^3 benchmark step with the multigrid fine level's iterate kept in the cell-row
+    layout (opt-in, MPDG_PICARD_ROWS=1) instead of the lexicographic one, in a child process
+    because the choice is read once per process: the same oracle bounds, and the Chebyshev
+    preconditioner on the same layout."""
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ, MPDG_PICARD_ROWS="1")
+    here = os.path.dirname(__file__)
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p",
+                        "no:cacheprovider", __file__,
+                        os.path.join(here, "test_gpu_operator.py"), "-k",
+                        "benchmark_step_at_48cubed or multigrid_mixed_precision_cg or "
+                        "chebyshev_mixed_precision_cg"],
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert " passed" in r.stdout
 
 
 # the vmult sweep's small meshes (bench_vmult_sweep.py --size small, ~2 M DoFs each)

@@ -179,6 +179,44 @@ def test_picard_operator_from_nodal_linearisation_point_matches_oracle():
     assert " passed" in r.stdout
 
 
+@pytest.mark.parametrize("cells", [(4, 3, 3), (1, 2, 3), (5, 4, 3)])
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+@pytest.mark.parametrize("dirichlet", [0x3F, 0b110000, 0])
+def test_picard_operator_from_cell_rows(cells, perturb, dirichlet):
+    """The cell-row layout of FE_Q(3) (slot s of cell column c of x-row r holds node 3c + s,
+    checked bit for bit) and the FP32 Picard operator applied from it: against the oracle's
+    Picard form (2e-5) and the lexicographic kernel (1e-6, both FP32)."""
+    o, g = pair(3, cells, perturb, "linear_k", dirichlet=dirichlet)
+    rng = np.random.default_rng(sum(cells) + dirichlet)
+    N = o.n_dofs
+    src, Tl, To = rng.uniform(-1, 1, N), rng.uniform(0.5, 1.5, N), rng.uniform(0.5, 1.5, N)
+    g.set_linearization(cuda(Tl), cuda(To))
+    s32 = cuda(src, torch.float32)
+    nd = [3 * c + 1 for c in cells]
+    assert g.cell_rows_size() == 4 * cells[0] * nd[1] * nd[2]
+    rows = torch.full((g.cell_rows_size(),), float("nan"), dtype=torch.float32, device="cuda")
+    g.to_cell_rows_f32(rows, s32)
+    lex = s32.cpu().numpy().reshape(nd[2] * nd[1], nd[0])
+    expect = np.stack([lex[:, 3 * c:3 * c + 4] for c in range(cells[0])], axis=1).reshape(-1)
+    assert np.array_equal(rows.cpu().numpy(), expect)
+    y = g.vmult_picard_f32_rows(g.new_vector(torch.float32), rows)
+    assert rel(y, o.vmult(src, Tl, To, form=2)) <= TOL32
+    ylex = g.vmult_picard_f32(g.new_vector(torch.float32), s32)
+    assert rel(y, ylex.cpu().double().numpy()) <= 1e-6
+
+
+def test_cell_rows_reject_other_degrees_and_boundary_faces():
+    _, g = pair(2, (2, 2, 2), 0.0, "linear_k")
+    with pytest.raises(H.ExcNotImplemented):
+        g.cell_rows_size()
+    o, g = pair(3, (2, 2, 2), 0.0, "linear_k", dirichlet=0b110000)
+    g.set_boundary(0, convection=(5.0, 300.0))
+    g.set_linearization(g.new_vector(), g.new_vector())
+    rows = torch.zeros(g.cell_rows_size(), dtype=torch.float32, device="cuda")
+    with pytest.raises(H.ExcInvalidArgument):
+        g.vmult_picard_f32_rows(g.new_vector(torch.float32), rows)
+
+
 def test_picard_operator_rejects_other_laws():
     _, g = pair(2, (2, 2, 2), 0.0, "constant")
     g.set_linearization(g.new_vector(), g.new_vector())
@@ -368,7 +406,7 @@ def test_chebyshev_mixed_precision_cg_larger_mesh(picard):
 
 @pytest.mark.parametrize("degree,cells,perturb,picard", [
     (3, (24, 24, 24), 0.0, True), (3, (24, 24, 24), 0.0, False), (2, (16, 24, 20), 0.15, True),
-    (1, (32, 32, 32), 0.0, True), (4, (12, 12, 12), 0.2, True)])
+    (1, (32, 32, 32), 0.0, True), (4, (12, 12, 12), 0.2, True), (3, (16, 16, 16), 0.2, True)])
 def test_multigrid_mixed_precision_cg(degree, cells, perturb, picard):
     """Flexible CG + FP32 p-multigrid V-cycle (FE_Q(p) -> FE_Q(1) -> h-coarsened FE_Q(1))
     on the k(T) tangent: converges to the FP64 tolerance (true residual) to the same

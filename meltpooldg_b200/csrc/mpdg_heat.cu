@@ -710,7 +710,8 @@ static int64_t cell_rows_size(const mpdg_heat *h)
 
 // ---- FP64 CG with the FP32 Chebyshev-Jacobi preconditioner ------------------
 // init: r = b - Ax ; rr ; r32 = r ; x32 = D32 r32 / theta ; d32 = x32 ; Ap = 0 ; Ax32 = 0
-// (x32 into xr's cell rows instead when xr.rows is set)
+// (x32 into xr's cell rows instead with ROWS)
+template <bool ROWS>
 __global__ void k_cgm_init(int64_t N, const double *__restrict__ b, double *r, double *Ap,
                            float *r32, float *x32, float *d32, float *Ax32,
                            const float *__restrict__ D32, float inv_theta, SolverState *st,
@@ -726,7 +727,7 @@ __global__ void k_cgm_init(int64_t N, const double *__restrict__ b, double *r, d
     const float rf = (float)ri;
     r32[i] = rf;
     const float xf = D32[i] * rf * inv_theta;
-    if (xr.rows)
+    if constexpr (ROWS)
       cell_rows_store(xr, i, xf);
     else
       x32[i] = xf;
@@ -760,7 +761,8 @@ __global__ void k_cgm_init(int64_t N, const double *__restrict__ b, double *r, d
 }
 
 // Chebyshev step: d = c1 d + c2 D32 (r32 - Ax32) ; x32 += d ; Ax32 = 0
-// (x in xr's cell rows instead of x32 when xr.rows is set)
+// (x in xr's cell rows instead of x32 with ROWS)
+template <bool ROWS>
 __global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32, float *d32,
                             float *Ax32, const float *__restrict__ D32, float c1, float c2,
                             const SolverState *st, CellRows xr)
@@ -770,7 +772,7 @@ __global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32
   {
     const float dn = c1 * d32[i] + c2 * D32[i] * (r32[i] - Ax32[i]);
     d32[i] = dn;
-    if (xr.rows)
+    if constexpr (ROWS)
       cell_rows_store(xr, i, cell_rows_load(xr, i) + dn);
     else
       x32[i] += dn;
@@ -780,6 +782,8 @@ __global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32
 
 // last Chebyshev step, then z = x32 (FP64), rz = r.z, zAp = z.Ap and the
 // flexible (Polak-Ribiere) beta = z.(r - r_old) / rz_old = -alpha z.Ap / rz_old
+// (x in xr's cell rows instead of x32 with ROWS)
+template <bool ROWS>
 __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const float *__restrict__ x32,
                             const float *__restrict__ d32, float *Ax32,
                             const float *__restrict__ D32, float c1, float c2,
@@ -791,7 +795,12 @@ __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const floa
   GRID_STRIDE(i, N)
   {
     const float dn = c1 * d32[i] + c2 * D32[i] * (r32[i] - Ax32[i]);
-    const double zi = (double)((xr.rows ? cell_rows_load(xr, i) : x32[i]) + dn);
+    float xi;
+    if constexpr (ROWS)
+      xi = cell_rows_load(xr, i);
+    else
+      xi = x32[i];
+    const double zi = (double)(xi + dn);
     Ax32[i] = 0.0f;
     z[i] = zi;
     v[0] += zi * r[i];
@@ -811,6 +820,7 @@ __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const floa
 }
 
 // x += alpha p ; r -= alpha Ap ; rr ; r32 = r ; x32 = D32 r32 / theta ; d32 = x32
+template <bool ROWS>
 __global__ void k_cgm_update_xr(int64_t N, double *x, double *r, const double *__restrict__ p,
                                 const double *__restrict__ Ap, float *r32, float *x32, float *d32,
                                 const float *__restrict__ D32, float inv_theta, SolverState *st,
@@ -827,7 +837,7 @@ __global__ void k_cgm_update_xr(int64_t N, double *x, double *r, const double *_
     const float rf = (float)ri;
     r32[i] = rf;
     const float xf = D32[i] * rf * inv_theta;
-    if (xr.rows)
+    if constexpr (ROWS)
       cell_rows_store(xr, i, xf);
     else
       x32[i] = xf;
@@ -925,7 +935,8 @@ __global__ void k_restrict_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
 // interpolation along one axis: out[.., I, ..] = (1 - xi_a) in[.., V, ..] + xi_a in[.., V + 1, ..]
 // with V = I / r, a = I % r; add: accumulate into out; masked rows are left untouched;
 // zero (optional): an array of out's shape set to zero on the way; out in xr's cell rows
-// instead when xr.rows is set
+// instead with ROWS
+template <bool ROWS>
 __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
                                const float *__restrict__ in, float *out, int add, MeshDims md,
                                int masked, float *zero, const SolverState *st, CellRows xr)
@@ -938,7 +949,7 @@ __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
     if (zero) zero[i] = 0.f;
     if (masked && constrained(md, o[0], o[1], o[2])) {
       if (!add) {
-        if (xr.rows)
+        if constexpr (ROWS)
           cell_rows_store(xr, i, 0.f);
         else
           out[i] = 0.f;
@@ -954,7 +965,7 @@ __global__ void k_prolong_axis(int axis, Dims3 di, Dims3 dout, Transfer1D t,
       v = (1.f - t.xi[a]) * v +
           t.xi[a] * in[(unsigned)p[0] + (unsigned)di.n[0] * ((unsigned)p[1] + (unsigned)di.n[1] * (unsigned)p[2])];
     }
-    if (xr.rows)
+    if constexpr (ROWS)
       cell_rows_store(xr, i, add ? cell_rows_load(xr, i) + v : v);
     else
       out[i] = add ? out[i] + v : v;
@@ -2111,13 +2122,14 @@ static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine,
   Transfer1D t;
   t.r = f.ratio;
   for (int a = 0; a < 8; ++a) t.xi[a] = f.xi[a];
-  k_prolong_axis<<<vgrid(h, E2.size()), VT, 0, h->stream>>>(2, C, E2, t, coarse, h->mg_t2, 0,
+  k_prolong_axis<false><<<vgrid(h, E2.size()), VT, 0, h->stream>>>(2, C, E2, t, coarse, h->mg_t2, 0,
                                                             f.h->dims, 0, nullptr, h->st,
                                                             CellRows());
-  k_prolong_axis<<<vgrid(h, E1.size()), VT, 0, h->stream>>>(1, E2, E1, t, h->mg_t2, h->mg_t1, 0,
+  k_prolong_axis<false><<<vgrid(h, E1.size()), VT, 0, h->stream>>>(1, E2, E1, t, h->mg_t2, h->mg_t1, 0,
                                                             f.h->dims, 0, nullptr, h->st,
                                                             CellRows());
-  k_prolong_axis<<<vgrid(h, F.size()), VT, 0, h->stream>>>(0, E1, F, t, h->mg_t1, fine, 1,
+  auto kp = fine_rows.rows ? k_prolong_axis<true> : k_prolong_axis<false>;
+  kp<<<vgrid(h, F.size()), VT, 0, h->stream>>>(0, E1, F, t, h->mg_t1, fine, 1,
                                                            f.h->dims, 1, zero_fine, h->st,
                                                            fine_rows);
   h->launches += 3;
@@ -2125,9 +2137,11 @@ static int mg_prolong_add(mpdg_heat *h, int l, const float *coarse, float *fine,
   return MPDG_OK;
 }
 
+template <bool ROWS>
 __global__ void k_cheb_step(int64_t N, const float *__restrict__ r32, float *x32, float *d32,
                             float *Ax32, const float *__restrict__ D32, float c1, float c2,
                             const SolverState *st, CellRows xr);
+template <bool ROWS>
 __global__ void k_cheb_last(int64_t N, const float *__restrict__ r32, const float *__restrict__ x32,
                             const float *__restrict__ d32, float *Ax32,
                             const float *__restrict__ D32, float c1, float c2,
@@ -2155,7 +2169,8 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
     }
     for (int j = 1; j <= v.pre; ++j) {
       TRY(op_apply_f(c, v.Ax, v.x, st, picard, xr.rows));
-      k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, v.c1[j],
+      (xr.rows ? k_cheb_step<true> : k_cheb_step<false>)<<<g, VT, 0, h->stream>>>(
+        N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, v.c1[j],
                                            v.c2[j], st, xr);
       ++h->launches;
     }
@@ -2178,10 +2193,12 @@ static int mg_vcycle(mpdg_heat *h, bool picard)
       const float c1 = j == 0 ? 0.f : v.c1[j];
       const float c2 = j == 0 ? (float)(1.0 / v.theta) : v.c2[j];
       if (l == 0 && j == v.post) {
-        k_cheb_last<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, h->r,
+        (xr.rows ? k_cheb_last<true> : k_cheb_last<false>)<<<g, VT, 0, h->stream>>>(
+          N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, h->r,
                                              h->Ap, h->z, st, h->partials, h->counter, xr);
       } else {
-        k_cheb_step<<<g, VT, 0, h->stream>>>(N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, st,
+        (xr.rows ? k_cheb_step<true> : k_cheb_step<false>)<<<g, VT, 0, h->stream>>>(
+          N, v.b, v.x, v.d, v.Ax, c->inv_diag_f, c1, c2, st,
                                              xr);
       }
       ++h->launches;
@@ -2371,7 +2388,8 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   if (any_faces(h)) TRY(dvec(h, &h->face_dot, 1));
   for (;;) {
     TRY(initial_Ax(h, x));
-    k_cgm_init<<<g, VT, 0, h->stream>>>(N, b, h->r, h->Ap, h->r32, h->x32, h->d32, h->Ax32,
+    (xr.rows ? k_cgm_init<true> : k_cgm_init<false>)<<<g, VT, 0, h->stream>>>(
+      N, b, h->r, h->Ap, h->r32, h->x32, h->d32, h->Ax32,
                                         h->inv_diag_f, inv_theta, h->st, h->partials, h->counter,
                                         prm->rel_tolerance, prm->abs_tolerance,
                                         res0 > 0.0 && prm->tol_reference_norm <= 0.0
@@ -2391,10 +2409,12 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
       for (int j = 1; j <= k; ++j) {
         TRY(op_apply_f(h, h->Ax32, h->x32, h->st, picard, xr.rows));
         if (j < k) {
-          k_cheb_step<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
+          (xr.rows ? k_cheb_step<true> : k_cheb_step<false>)<<<g, VT, 0, h->stream>>>(
+            N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
                                                c1[j], c2[j], h->st, xr);
         } else {
-          k_cheb_last<<<g, VT, 0, h->stream>>>(N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
+          (xr.rows ? k_cheb_last<true> : k_cheb_last<false>)<<<g, VT, 0, h->stream>>>(
+            N, h->r32, h->x32, h->d32, h->Ax32, h->inv_diag_f,
                                                c1[j], c2[j], h->r, h->Ap, h->z, h->st,
                                                h->partials, h->counter, xr);
         }
@@ -2407,7 +2427,8 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     if (!h->st_host->done) TRY(precondition());
     auto iteration = [&]() -> int {
       TRY(op_apply_d(h, h->Ap, h->pv, FIN_CG_ALPHA, nullptr, h->st));
-      k_cgm_update_xr<<<g, VT, 0, h->stream>>>(N, x, h->r, h->pv, h->Ap, h->r32, h->x32, h->d32,
+      (xr.rows ? k_cgm_update_xr<true> : k_cgm_update_xr<false>)<<<g, VT, 0, h->stream>>>(
+        N, x, h->r, h->pv, h->Ap, h->r32, h->x32, h->d32,
                                                h->inv_diag_f, inv_theta, h->st, h->partials,
                                                h->counter, xr); ++h->launches;
       TRY(precondition());
@@ -2531,7 +2552,7 @@ static int gmres(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const d
     ++h->launches;
     for (int s = 1; s <= kdeg; ++s) {
       TRY(op_apply_f(h, h->Ax32, zj, nullptr, false));
-      k_cheb_step<<<gg32, VT, 0, h->stream>>>(N, h->r32, zj, h->d32, h->Ax32, h->inv_diag_f,
+      k_cheb_step<false><<<gg32, VT, 0, h->stream>>>(N, h->r32, zj, h->d32, h->Ax32, h->inv_diag_f,
                                               c1[s], c2[s], h->st_run, CellRows());
       ++h->launches;
     }

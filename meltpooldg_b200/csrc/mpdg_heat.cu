@@ -183,6 +183,7 @@ struct mpdg_heat {
   float *mg_t1 = nullptr, *mg_t2 = nullptr;
   int mg_min_cells = -1;
   bool x_zero = false;  // the next solve starts from x = 0 (its A x is skipped)
+  bool mixed_ready = false;  // mixed_prepare ran at the current linearisation point
   // host-buffer time step: a copy stream for the transfers that overlap the step, and the
   // events the step records / waits on (null outside mpdg_heat_time_step_host)
   cudaStream_t copy_stream = nullptr;
@@ -2327,8 +2328,11 @@ static int enable_cell_rows(mpdg_heat *h, bool picard)
 // ---------------------------------------------------------------------------
 // FP64 flexible CG with the FP32 Chebyshev-Jacobi or p-multigrid preconditioner
 // ---------------------------------------------------------------------------
-static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
-                        mpdg_solve_stats *stats)
+// the preconditioner's set-up at the current linearisation point: FP32 copies, the Picard
+// conductivity field, the eigenvalue estimate (first time, or without reuse) and the multigrid
+// levels. It needs no right-hand side, so a time step issues it before it waits for the
+// source's upload (h->mixed_ready: the next cg_chebyshev call skips it)
+static int mixed_prepare(mpdg_heat *h, const mpdg_solver_params *prm)
 {
   const int64_t N = h->n_dofs;
   const bool use_mg = prm->preconditioner == MPDG_PRECOND_MG_F32;
@@ -2336,8 +2340,6 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     return fail(MPDG_ERR_INVALID_ARGUMENT,
                 "multigrid preconditioner: not available with the gas-liquid laws or a velocity field");
   const bool picard = prm->cheb_picard && h->law == MPDG_LAW_LINEAR_K && h->tab.conductivity_q;
-  // the FP64 inverse diagonal feeds the Lanczos estimate and the Chebyshev smoother; the
-  // multigrid smoothers of the Picard operator use that operator's own FP32 diagonal
   const bool need_diag = !(use_mg && picard) || !h->eig_valid || !prm->cheb_eig_reuse;
   if (need_diag && !h->diag_valid)
     return fail(MPDG_ERR_INVALID_ARGUMENT, "preconditioner not updated");
@@ -2364,6 +2366,22 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     TRY(estimate_eigenvalues(h, prm->cheb_eig_iterations, &h->eig_min, &h->eig_max));
     h->eig_valid = true;
   }
+  if (use_mg) {
+    TRY(mg_build(h, prm));
+    TRY(mg_setup(h, prm, picard));
+  }
+  h->mixed_ready = true;
+  return MPDG_OK;
+}
+
+static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, const double *b,
+                        mpdg_solve_stats *stats)
+{
+  const int64_t N = h->n_dofs;
+  const bool use_mg = prm->preconditioner == MPDG_PRECOND_MG_F32;
+  const bool picard = prm->cheb_picard && h->law == MPDG_LAW_LINEAR_K && h->tab.conductivity_q;
+  if (!h->mixed_ready) TRY(mixed_prepare(h, prm));
+  h->mixed_ready = false;
   double bmax = prm->cheb_max_factor * h->eig_max;
   double amin = std::max(h->eig_min, prm->cheb_min_fraction * bmax);
   double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin);
@@ -2371,8 +2389,6 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
   std::vector<float> c1, c2;
   cheb_coefficients(theta, delta, k, c1, c2);
   if (use_mg) {
-    TRY(mg_build(h, prm));
-    TRY(mg_setup(h, prm, picard));
     theta = h->mg[0].theta;
     bmax = theta + h->mg[0].delta;
     amin = theta - h->mg[0].delta;
@@ -3696,6 +3712,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
   mpdg_step_stats s;
   memset(&s, 0, sizeof(s));
   int rc = MPDG_OK;
+  h->mixed_ready = false;
   do {
     // the Chebyshev / multigrid interval: kept across steps with cheb_eig_reuse until dt (or
     // the material or the mesh) changes; a solve that does not use it leaves it alone
@@ -3761,6 +3778,14 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
       // J T_g first: it does not need the source, whose upload may still be running
       zero_async(h, h->z, vb, h->stream);
       if ((rc = op_apply_d(h, h->z, T_cur, FIN_NONE, nullptr, nullptr)) != MPDG_OK) break;
+      // so is the mixed-precision preconditioner's set-up (it depends on T_lin only), unless it
+      // has to estimate the fine level's interval (its Lanczos CG uses z, which holds J T_g)
+      if (h->wait_source && h->eig_valid && prm->linear.cheb_eig_reuse &&
+          prm->linear.solver == MPDG_SOLVER_CG &&
+          (prm->linear.preconditioner == MPDG_PRECOND_CHEBYSHEV_JACOBI_F32 ||
+           prm->linear.preconditioner == MPDG_PRECOND_MG_F32) &&
+          (rc = mixed_prepare(h, &prm->linear)) != MPDG_OK)
+        break;
       zero_async(h, h->w2, vb, h->stream);
       if (h->wait_source) cudaStreamWaitEvent(h->stream, h->ev_source, 0);
       if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
@@ -3832,6 +3857,7 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
         rc = fail(MPDG_ERR_NEWTON_NOT_CONVERGED, "Newton-Raphson did not converge");
     }
   } while (0);
+  h->mixed_ready = false;
   cudaEventRecord(e1, h->stream);
   cudaEventSynchronize(e1);
   float ms = 0.f;
@@ -3939,8 +3965,8 @@ extern "C" int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params
     TRY(dvec(h, &h->host_q, N));
     TRY(ensure_copy_stream(h));
     // the source is first needed by create_rhs: its upload overlaps the predictor, the history
-    // commit and the first operator application (the previous source buffer is free: every
-    // call ends synchronised)
+    // commit, the first operator application and the mixed-precision preconditioner's set-up
+    // (the previous source buffer is free: every call ends synchronised)
     CU(cudaEventRecord(h->ev_inputs, h->stream));
     CU(cudaStreamWaitEvent(h->copy_stream, h->ev_inputs, 0));
     CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->copy_stream));

@@ -1371,14 +1371,17 @@ static bool tangent_fields_enabled()
 }
 
 // line-per-thread kernel (FP64, p >= 4) on deformed meshes: the linear-k tangent from the
-// fields (preloaded with the geometry) instead of evaluating T_lin
-static bool tangent_fields_lpt()
+// fields (preloaded with the geometry) instead of evaluating T_lin. The default at p = 4 and 6,
+// where it measured faster per application (3.84 -> 3.26 ms and 4.64 -> 4.00 ms at ~57 M DoFs)
+// and per production step with the fields' build included; at p = 5 its 200 registers make it
+// slower (4.23 -> 5.91 ms). MPDG_TANGENT_FIELDS_LPT=1 takes it at every degree, =0 at none.
+static bool tangent_fields_lpt(int p)
 {
-  static const int on = [] {
+  static const int mode = [] {
     const char *e = getenv("MPDG_TANGENT_FIELDS_LPT");
-    return (e && e[0] == '1') ? 1 : 0;
+    return e ? (e[0] == '1' ? 1 : (e[0] == '0' ? 0 : 2)) : 2;
   }();
-  return on != 0;
+  return mode == 1 || (mode == 2 && (p == 4 || p == 6));
 }
 
 static int ensure_lineark(mpdg_heat *h)
@@ -1496,9 +1499,9 @@ static int op_apply_d(mpdg_heat *h, double *dst, const double *src, int fin, dou
     a.cf = h->tf;
     law = 6;
   } else if (law == MPDG_LAW_LINEAR_K && h->tab.coef_lineark && tangent_fields_enabled() &&
-             (h->tab.v2_d || (h->geo == 1 && tangent_fields_lpt()))) {
-    // the line-per-thread kernel (p >= 4) takes them on deformed meshes only with
-    // MPDG_TANGENT_FIELDS_LPT=1: 4 more loads per point against the 6 T_lin sweeps
+             (h->tab.v2_d || (h->geo == 1 && tangent_fields_lpt(h->p)))) {
+    // the line-per-thread kernel (p >= 4) takes them on deformed meshes (4 more loads per
+    // point against the 6 T_lin sweeps) where that measured faster
     TRY(ensure_lineark(h));
     a.cf = h->tk;
     law = 7;

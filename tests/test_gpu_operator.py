@@ -127,14 +127,16 @@ def test_fp32_packed_kernel_matches_oracle():
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
 
 
-def test_line_per_thread_tangent_fields_match_oracle():
-    """The line-per-thread FP64 k(T) tangent from the fields built once per linearisation
-    (MPDG_TANGENT_FIELDS_LPT=1, deformed meshes at p >= 4) on the same cases, in a child process
-    because the choice is read once per process."""
+@pytest.mark.parametrize("mode", ["1", "0"])
+def test_line_per_thread_tangent_fields_match_oracle(mode):
+    """The line-per-thread FP64 k(T) tangent on deformed meshes at p >= 4 from the fields built
+    once per linearisation at every degree (MPDG_TANGENT_FIELDS_LPT=1; the default takes them at
+    p = 4 and 6) or at none (=0: T_lin evaluated in every application), on the same cases, in a
+    child process because the choice is read once per process."""
     import os
     import subprocess
     import sys
-    env = dict(os.environ, MPDG_TANGENT_FIELDS_LPT="1")
+    env = dict(os.environ, MPDG_TANGENT_FIELDS_LPT=mode)
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p",
                         "no:cacheprovider", __file__, "-k",
                         "vmult_diag_rhs_match_oracle and linear_k and 0.2 and (4 or 5 or 6)"],

@@ -309,8 +309,9 @@ int mpdg_heat_l2_norm(mpdg_heat *h, const double *u, double *norm);
  * scratch is a fixed 128 KiB array in the library (at most 16384 partial sums;
  * larger reductions are rejected with MPDG_ERR_INVALID_ARGUMENT), so the call calls
  * no cudaMalloc/cudaFree. The first call on a device looks up that array's device
- * address and caches it (the cached address is not valid after cudaDeviceReset).
- * Calls share the array: calls that overlap on the GPU race. */
+ * address (cudaGetSymbolAddress) and caches it: make that first call before any
+ * stream capture. The cached address is not valid after cudaDeviceReset. Calls
+ * share the array: calls that overlap on the GPU race. */
 int mpdg_heat_l2_norm_noalloc(mpdg_heat *h, const double *u, double *norm);
 /* DoF support point coordinates, xyz[3*i + d] (device pointer, 3*n_dofs doubles). */
 int mpdg_heat_support_points(mpdg_heat *h, double *xyz);

@@ -4200,7 +4200,7 @@ extern "C" int mpdg_heat_invert_diagonal(mpdg_heat *h, double *d)
 // so calls that overlap on the GPU (different streams, or different host
 // threads on one device) race and must be serialised by the caller. The first
 // call on a device looks up the array's device address (cudaGetSymbolAddress)
-// and caches it per device.
+// and caches it per device; that first call should come before any stream capture.
 // The cached address is not valid after cudaDeviceReset on that device.
 // ---------------------------------------------------------------------------
 static constexpr int kNoAllocSlots = 16384;

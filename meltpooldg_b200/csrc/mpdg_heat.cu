@@ -190,6 +190,13 @@ struct mpdg_heat {
   cudaEvent_t ev_source = nullptr, ev_commit = nullptr, ev_inputs = nullptr;
   bool wait_source = false, record_commit = false;
   double *told_host = nullptr;  // host destination of the committed T_old (copy stream)
+  // resident host step: the new T = T_g + x formed in t_out as soon as the increment solve has
+  // converged and sent to early_host on the copy stream, so that the download overlaps the FP64
+  // residual recheck (early_T: the step's T_g; early_sent: that download holds the final T, no
+  // restart changed the increment after it)
+  double *early_host = nullptr, *early_T = nullptr, *t_out = nullptr;
+  bool early_sent = false;
+  cudaEvent_t ev_early = nullptr;
   double *res_T = nullptr, *res_To = nullptr;  // device-resident history (time_step_resident)
   // the resident step swaps the roles of its two history buffers instead of copying T into
   // T_old (the predictor writes in place over T_{n-1}); rotated reports that the swap happened
@@ -518,6 +525,12 @@ __global__ void k_predict_inplace(int64_t N, const double *__restrict__ T, doubl
 __global__ void k_axpy(int64_t N, double *y, double a, const double *__restrict__ x)
 {
   GRID_STRIDE(i, N) y[i] += a * x[i];
+}
+// out = a + b (the same sum k_axpy forms with a = 1)
+__global__ void k_sum(int64_t N, double *out, const double *__restrict__ a,
+                      const double *__restrict__ b)
+{
+  GRID_STRIDE(i, N) out[i] = a[i] + b[i];
 }
 __global__ void k_masked_random(int64_t N, MeshDims d, double *b)
 {
@@ -2331,6 +2344,8 @@ static int enable_cell_rows(mpdg_heat *h, bool picard)
 // ---------------------------------------------------------------------------
 // FP64 flexible CG with the FP32 Chebyshev-Jacobi or p-multigrid preconditioner
 // ---------------------------------------------------------------------------
+static int distribute(mpdg_heat *h, double *u);
+
 // the preconditioner's set-up at the current linearisation point: FP32 copies, the Picard
 // conductivity field, the eigenvalue estimate (first time, or without reuse) and the multigrid
 // levels. It needs no right-hand side, so a time step issues it before it waits for the
@@ -2481,6 +2496,18 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     total_it += h->st_host->it;
     const int done = h->st_host->done, status = h->st_host->status;
     const double tol = h->st_host->tol;
+    if (h->early_host && h->early_T && done == 1 && restarts == 0) {
+      // the step's new T (T_g + x, Dirichlet values set, as the step forms it after the
+      // solve), sent to the host now so that the download overlaps the recheck
+      TRY(dvec(h, &h->t_out, N));
+      k_sum<<<g, VT, 0, h->stream>>>(N, h->t_out, h->early_T, x); ++h->launches;
+      TRY(distribute(h, h->t_out));
+      CU(cudaEventRecord(h->ev_early, h->stream));
+      CU(cudaStreamWaitEvent(h->copy_stream, h->ev_early, 0));
+      CU(cudaMemcpyAsync(h->early_host, h->t_out, sizeof(double) * N, cudaMemcpyDeviceToHost,
+                         h->copy_stream));
+      h->early_sent = true;
+    }
     // true residual recheck in FP64
     CU(zero_async(h, h->Ap, sizeof(double) * N, h->stream));
     TRY(op_apply_d(h, h->Ap, x, FIN_NONE, nullptr, nullptr));
@@ -2492,6 +2519,7 @@ static int cg_chebyshev(mpdg_heat *h, const mpdg_solver_params *prm, double *x, 
     true_res = std::sqrt(rr);
     if (done == 1 && true_res > tol && total_it < prm->max_iterations && restarts < 5) {
       ++restarts;
+      h->early_sent = false;  // the increment changes: the step downloads T itself
       continue;
     }
     if (stats) {
@@ -2746,6 +2774,7 @@ static void release(mpdg_heat *h)
     cudaEventDestroy(h->ev_source);
     cudaEventDestroy(h->ev_commit);
     cudaEventDestroy(h->ev_inputs);
+    cudaEventDestroy(h->ev_early);
     h->copy_stream = nullptr;
   }
   for (MGLevel &lv : h->mg)
@@ -3818,7 +3847,9 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
         zero_async(h, h->w1, vb, h->stream);
         h->x_zero = true;
       }
+      h->early_T = h->early_host ? T_cur : nullptr;  // T_g, for the early download of T
       rc = linear_solve(h, &lp, h->w1, h->w2, &ls);
+      h->early_T = nullptr;
       h->x_zero = false;
       h->x_Ax = nullptr;
       if (rc != MPDG_OK) break;
@@ -3883,6 +3914,7 @@ static int ensure_copy_stream(mpdg_heat *h)
     CU(cudaEventCreateWithFlags(&h->ev_source, cudaEventDisableTiming));
     CU(cudaEventCreateWithFlags(&h->ev_commit, cudaEventDisableTiming));
     CU(cudaEventCreateWithFlags(&h->ev_inputs, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&h->ev_early, cudaEventDisableTiming));
   }
   return MPDG_OK;
 }
@@ -3979,17 +4011,31 @@ extern "C" int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params
   h->wait_source = heat_source != nullptr;
   h->rotate = true;
   h->rotated = false;
+  // with the mixed-precision CG the new T is downloaded as soon as the increment has converged,
+  // during the solver's FP64 residual recheck (on the copy stream)
+  if (T_out) {
+    TRY(ensure_copy_stream(h));
+    h->early_host = T_out;
+  }
+  h->early_sent = false;
   const int rc = mpdg_heat_time_step(h, prm, dt, dt_old, h->res_T, h->res_To,
                                      heat_source ? h->host_q : nullptr, stats);
+  h->early_host = nullptr;
   h->wait_source = false;
   h->rotate = false;
   if (h->rotated) std::swap(h->res_T, h->res_To);
   h->rotated = false;
   if (rc != MPDG_OK) {
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+    h->early_sent = false;
     return rc;
   }
-  if (T_out) CU(cudaMemcpyAsync(T_out, h->res_T, vb, cudaMemcpyDeviceToHost, h->stream));
+  if (T_out && !h->early_sent) {
+    // an early download invalidated by a restart still writes T_out: let it finish first
+    if (h->copy_stream) CU(cudaStreamSynchronize(h->copy_stream));
+    CU(cudaMemcpyAsync(T_out, h->res_T, vb, cudaMemcpyDeviceToHost, h->stream));
+  }
+  h->early_sent = false;
   if (h->copy_stream) CU(cudaStreamSynchronize(h->copy_stream));
   CU(cudaStreamSynchronize(h->stream));
   return MPDG_OK;

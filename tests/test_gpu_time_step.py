@@ -186,11 +186,14 @@ def test_host_buffer_step_matches_device_step(precond):
         assert ref.abs().max() > 0.0
 
 
-@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_MG_F32])
+@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_MG_F32,
+                                     L.PRECOND_CHEBYSHEV_JACOBI_F32])
 def test_resident_history_step_matches_device_step(precond):
     """mpdg_heat_time_step_resident (history on the device, pinned host source in, new T
     out) follows mpdg_heat_time_step on device vectors over three steps; store_history
-    returns both history vectors."""
+    returns both history vectors, and the T the step downloaded (with the mixed-precision
+    solvers as soon as the increment converged, during the residual recheck) equals the
+    resident T bit for bit."""
     op = H.HeatDiffuseOperator(H.box_mesh(3, (8, 8, 8)))
     op.set_material(H.material(law=L.LAW_LINEAR_K, k=1.0, k1=0.5))
     lin = H.LinearSolverData(preconditioner_type=precond, rel_tolerance=1e-10,

@@ -197,6 +197,13 @@ struct mpdg_heat {
   double *early_host = nullptr, *early_T = nullptr, *t_out = nullptr;
   bool early_sent = false;
   cudaEvent_t ev_early = nullptr;
+  // host-buffer steps: the source uploaded in n_slabs z-slabs of node planes (event ev_slab[k]
+  // after slab k), so that create_rhs applies the cells of cell layers [slab_cz[k],
+  // slab_cz[k + 1]) as soon as slab k has arrived (0: one upload, ev_source)
+  static constexpr int kMaxSlabs = 4;
+  int n_slabs = 0;
+  int slab_cz[kMaxSlabs + 1] = {0};
+  cudaEvent_t ev_slab[kMaxSlabs] = {};
   double *res_T = nullptr, *res_To = nullptr;  // device-resident history (time_step_resident)
   // the resident step swaps the roles of its two history buffers instead of copying T into
   // T_old (the predictor writes in place over T_{n-1}); rotated reports that the swap happened
@@ -2775,6 +2782,7 @@ static void release(mpdg_heat *h)
     cudaEventDestroy(h->ev_commit);
     cudaEventDestroy(h->ev_inputs);
     cudaEventDestroy(h->ev_early);
+    for (int k = 0; k < mpdg_heat::kMaxSlabs; ++k) cudaEventDestroy(h->ev_slab[k]);
     h->copy_stream = nullptr;
   }
   for (MGLevel &lv : h->mg)
@@ -3353,6 +3361,68 @@ static int create_rhs(mpdg_heat *h, double *dst, const double *src, const double
   return MPDG_OK;
 }
 
+// create_rhs with the nodal source arriving in z-slabs on the copy stream (upload_source): the
+// cells of layers [slab_cz[k], slab_cz[k + 1]) are applied as a sub-box of the mesh (base
+// pointers at its first node plane, per-cell fields at its first cell, the z faces Dirichlet only
+// where they are the mesh's) once slab k has arrived; the nodes shared by two sub-boxes receive
+// both contributions through the atomic scatter, as from neighbouring cells of one launch
+static int create_rhs_slabs(mpdg_heat *h, double *dst, const double *src, const double *q)
+{
+  TRY(ensure_dt(h));
+  if (!h->T_lin) return fail(MPDG_ERR_INVALID_ARGUMENT, "create_rhs needs set_linearization");
+  TRY(ensure_lin(h));
+  TRY(ensure_fields(h));
+  CellArgs<double> a = cell_args<double>(h);
+  const MeshDims d = a.d;
+  const int64_t layer_cells = (int64_t)d.m[0] * d.m[1];
+  const int64_t plane = (int64_t)d.nd[0] * d.nd[1];
+  for (int k = 0; k < h->n_slabs; ++k) {
+    const int cz0 = h->slab_cz[k], cz1 = h->slab_cz[k + 1];
+    CU(cudaStreamWaitEvent(h->stream, h->ev_slab[k], 0));
+    if (cz1 <= cz0) continue;
+    CellArgs<double> b = a;
+    const int64_t c0 = (int64_t)cz0 * layer_cells, n0 = (int64_t)d.p * cz0 * plane;
+    b.n_cells = (int64_t)(cz1 - cz0) * layer_cells;
+    b.d.m[2] = cz1 - cz0;
+    b.d.nd[2] = d.p * (cz1 - cz0) + 1;
+    if (cz0 > 0) b.d.dmask &= ~16;
+    if (cz1 < d.m[2]) b.d.dmask &= ~32;
+    b.g.q = h->geoq ? h->geoq + c0 * 7 * h->npt : nullptr;
+    b.cf = h->cf ? h->cf + c0 * 5 * h->npt : nullptr;
+    b.dst = dst + n0;
+    b.Tl = h->T_lin + n0;
+    b.To = src + n0;
+    b.qs = q + n0;
+    CU(h->tab.rhs(b, h->geo, klaw(h), h->stream, h->sm_count));
+    ++h->launches;
+  }
+  if (any_faces(h)) TRY(launch_faces<double>(h, 1, dst, nullptr, h->T_lin, nullptr, nullptr));
+  return MPDG_OK;
+}
+
+// the host source into host_q on the copy stream in z-slabs of node planes (slab k holds the
+// planes up to p slab_cz[k + 1], so it completes every cell of layers below slab_cz[k + 1]),
+// ev_slab[k] after each and ev_source after the last
+static int upload_source(mpdg_heat *h, const double *host_src)
+{
+  const MeshDims &d = h->dims;
+  const int K = std::max(1, std::min(mpdg_heat::kMaxSlabs, d.m[2]));
+  const int64_t plane = (int64_t)d.nd[0] * d.nd[1];
+  int64_t pl0 = 0;
+  for (int k = 0; k <= K; ++k) h->slab_cz[k] = (int)(((int64_t)k * d.m[2]) / K);
+  for (int k = 0; k < K; ++k) {
+    const int64_t pl1 = k + 1 < K ? (int64_t)d.p * h->slab_cz[k + 1] + 1 : d.nd[2];
+    CU(cudaMemcpyAsync(h->host_q + pl0 * plane, host_src + pl0 * plane,
+                       sizeof(double) * (size_t)((pl1 - pl0) * plane), cudaMemcpyHostToDevice,
+                       h->copy_stream));
+    CU(cudaEventRecord(h->ev_slab[k], h->copy_stream));
+    pl0 = pl1;
+  }
+  CU(cudaEventRecord(h->ev_source, h->copy_stream));
+  h->n_slabs = K;
+  return MPDG_OK;
+}
+
 extern "C" int mpdg_heat_create_rhs(mpdg_heat *h, double *dst, const double *src,
                                     const double *heat_source)
 {
@@ -3819,8 +3889,12 @@ extern "C" int mpdg_heat_time_step(mpdg_heat *h, const mpdg_step_params *prm, do
           (rc = mixed_prepare(h, &prm->linear)) != MPDG_OK)
         break;
       zero_async(h, h->w2, vb, h->stream);
-      if (h->wait_source) cudaStreamWaitEvent(h->stream, h->ev_source, 0);
-      if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
+      if (h->wait_source && h->n_slabs > 0 && heat_source) {
+        if ((rc = create_rhs_slabs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
+      } else {
+        if (h->wait_source) cudaStreamWaitEvent(h->stream, h->ev_source, 0);
+        if ((rc = create_rhs(h, h->w2, T_old, heat_source)) != MPDG_OK) break;
+      }
       double rr = 0.0, bb = 0.0;
       if ((rc = norms(h, h->w2, h->z, &rr, &bb)) != MPDG_OK) break;
       mpdg_solver_params lp = prm->linear;
@@ -3915,6 +3989,8 @@ static int ensure_copy_stream(mpdg_heat *h)
     CU(cudaEventCreateWithFlags(&h->ev_commit, cudaEventDisableTiming));
     CU(cudaEventCreateWithFlags(&h->ev_inputs, cudaEventDisableTiming));
     CU(cudaEventCreateWithFlags(&h->ev_early, cudaEventDisableTiming));
+    for (int k = 0; k < mpdg_heat::kMaxSlabs; ++k)
+      CU(cudaEventCreateWithFlags(&h->ev_slab[k], cudaEventDisableTiming));
   }
   return MPDG_OK;
 }
@@ -3938,8 +4014,7 @@ extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *pr
   CU(cudaEventRecord(h->ev_inputs, h->stream));
   if (heat_source) {
     CU(cudaStreamWaitEvent(h->copy_stream, h->ev_inputs, 0));  // one transfer at a time
-    CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->copy_stream));
-    CU(cudaEventRecord(h->ev_source, h->copy_stream));
+    TRY(upload_source(h, heat_source));
   }
   // the new T_old (= the input T) is final once the step has committed the history: the
   // step starts its copy back then, so it runs while the solve computes; T follows at the end
@@ -3949,6 +4024,7 @@ extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *pr
   const int rc = mpdg_heat_time_step(h, prm, dt, dt_old, h->host_T, h->host_To,
                                      heat_source ? h->host_q : nullptr, stats);
   h->wait_source = false;
+  h->n_slabs = 0;
   h->record_commit = false;
   h->told_host = nullptr;
   if (rc != MPDG_OK) {
@@ -4004,8 +4080,7 @@ extern "C" int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params
     // (the previous source buffer is free: every call ends synchronised)
     CU(cudaEventRecord(h->ev_inputs, h->stream));
     CU(cudaStreamWaitEvent(h->copy_stream, h->ev_inputs, 0));
-    CU(cudaMemcpyAsync(h->host_q, heat_source, vb, cudaMemcpyHostToDevice, h->copy_stream));
-    CU(cudaEventRecord(h->ev_source, h->copy_stream));
+    TRY(upload_source(h, heat_source));
   }
   // the two history buffers swap roles: the predictor overwrites T_{n-1} in place
   h->wait_source = heat_source != nullptr;
@@ -4022,6 +4097,7 @@ extern "C" int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params
                                      heat_source ? h->host_q : nullptr, stats);
   h->early_host = nullptr;
   h->wait_source = false;
+  h->n_slabs = 0;
   h->rotate = false;
   if (h->rotated) std::swap(h->res_T, h->res_To);
   h->rotated = false;

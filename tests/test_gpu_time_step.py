@@ -186,6 +186,51 @@ def test_host_buffer_step_matches_device_step(precond):
         assert ref.abs().max() > 0.0
 
 
+@pytest.mark.parametrize("cells,perturb", [((6, 4, 5), 0.2), ((4, 4, 3), 0.0)])
+@pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_MG_F32])
+def test_host_buffer_steps_with_slab_upload_match_device_step(cells, perturb, precond):
+    """The host-buffer steps upload the source in z-slabs and apply the residual to the cells of
+    each slab as it arrives (sub-boxes of the mesh, their z faces Dirichlet only at the mesh's
+    ends): on a deformed mesh with an odd number of cell layers and a Robin face, and on a mesh
+    with fewer layers than slabs, the stateless and the resident steps follow the device step."""
+    import ctypes as C
+    mesh = H.box_mesh(3, cells, perturb=perturb, seed=6,
+                      dirichlet=("x-", "y-", "y+", "z-", "z+"))
+    op = H.HeatDiffuseOperator(mesh)
+    op.set_material(H.material(law=L.LAW_LINEAR_K, k=1.0, k1=0.5))
+    op.set_boundary(1, convection=(5.0, 0.2))
+    lin = H.LinearSolverData(preconditioner_type=precond, rel_tolerance=1e-10,
+                             abs_tolerance=0.0, cheb_picard=True)
+    dev = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    res = H.HeatDiffuseOperation(op, lin, predictor=L.PREDICTOR_LINEAR, single_linearization=True)
+    N, dt = op.n_dofs, 5e-4
+    T0 = torch.rand(N, dtype=torch.float64, device="cuda", generator=torch.Generator(
+        device="cuda").manual_seed(8))
+    op.distribute_constraints(T0)
+    dev.set_initial_condition(T0.clone())
+    res.load_history_host(T0.cpu().contiguous(), T0.cpu().contiguous())
+    hT, hTo = T0.cpu().pin_memory(), T0.cpu().pin_memory()
+    hq = torch.empty(N, dtype=torch.float64).pin_memory()
+    hR = torch.empty(N, dtype=torch.float64).pin_memory()
+    q = op.new_vector()
+    dev.heat_source = q
+    for s in range(2):
+        op.gaussian_source(q, 200.0, (0.4, 0.5, 0.2 + 0.5 * s), 0.2)
+        hq.copy_(q)
+        dev.solve(dt)
+        step = L.StepStats()
+        H.check(op._L.mpdg_heat_time_step_host(op.h, C.byref(dev.params), dt,
+                                                0.0 if s == 0 else dt,
+                                                C.c_void_p(hT.data_ptr()),
+                                                C.c_void_p(hTo.data_ptr()),
+                                                C.c_void_p(hq.data_ptr()), C.byref(step)))
+        res.solve_resident(dt, hq, hR)
+        ref = dev.T.cpu()
+        assert ref.abs().max() > 0.0
+        assert (hT - ref).abs().max() <= 1e-8 * ref.abs().max()
+        assert (hR - ref).abs().max() <= 1e-8 * ref.abs().max()
+
+
 @pytest.mark.parametrize("precond", [L.PRECOND_JACOBI, L.PRECOND_MG_F32,
                                      L.PRECOND_CHEBYSHEV_JACOBI_F32])
 def test_resident_history_step_matches_device_step(precond):

@@ -4075,9 +4075,10 @@ extern "C" int mpdg_heat_time_step_resident(mpdg_heat *h, const mpdg_step_params
   if (heat_source) {
     TRY(dvec(h, &h->host_q, N));
     TRY(ensure_copy_stream(h));
-    // the source is first needed by create_rhs: its upload overlaps the predictor, the history
-    // commit, the first operator application and the mixed-precision preconditioner's set-up
-    // (the previous source buffer is free: every call ends synchronised)
+    // the source is first needed by create_rhs: its upload (in z-slabs, each applied by the
+    // residual as it arrives) overlaps the predictor, the history commit, the first operator
+    // application and the mixed-precision preconditioner's set-up (the previous source buffer
+    // is free: every call ends synchronised)
     CU(cudaEventRecord(h->ev_inputs, h->stream));
     CU(cudaStreamWaitEvent(h->copy_stream, h->ev_inputs, 0));
     TRY(upload_source(h, heat_source));

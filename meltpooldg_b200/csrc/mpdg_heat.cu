@@ -4021,17 +4021,28 @@ extern "C" int mpdg_heat_time_step_host(mpdg_heat *h, const mpdg_step_params *pr
   h->wait_source = heat_source != nullptr;
   h->record_commit = true;
   h->told_host = T_old;
+  // with the mixed-precision CG the new T goes back during the solver's residual recheck
+  // (copy stream; the T input was read from this buffer at the start of the call)
+  h->early_host = T_cur;
+  h->early_sent = false;
   const int rc = mpdg_heat_time_step(h, prm, dt, dt_old, h->host_T, h->host_To,
                                      heat_source ? h->host_q : nullptr, stats);
+  h->early_host = nullptr;
   h->wait_source = false;
   h->n_slabs = 0;
   h->record_commit = false;
   h->told_host = nullptr;
   if (rc != MPDG_OK) {
     cudaStreamSynchronize(h->copy_stream);
+    h->early_sent = false;
     return rc;
   }
-  CU(cudaMemcpyAsync(T_cur, h->host_T, vb, cudaMemcpyDeviceToHost, h->stream));
+  if (!h->early_sent) {
+    // an early download invalidated by a restart still writes T_cur: let it finish first
+    CU(cudaStreamSynchronize(h->copy_stream));
+    CU(cudaMemcpyAsync(T_cur, h->host_T, vb, cudaMemcpyDeviceToHost, h->stream));
+  }
+  h->early_sent = false;
   CU(cudaStreamSynchronize(h->copy_stream));
   CU(cudaStreamSynchronize(h->stream));
   return MPDG_OK;
